@@ -1,0 +1,184 @@
+/*
+ * wnlqg_b200.h - C ABI of the B200 k-mesh response engine.
+ *
+ * The engine evaluates the WannierNLQG k-mesh response hot path on one NVIDIA B200:
+ * Fourier interpolation of H(R), (iR)^n H(R) and A(R) onto k-points, the per-k Hermitian
+ * eigensolve, the sum-over-states integrands and the k-mesh reduction.
+ *
+ * Every array crossing this boundary is plain host (or, for *_device entry points, device)
+ * memory described by pointers and sizes.  Complex numbers are two interleaved doubles
+ * (re, im), exactly like Julia's ComplexF64.  Multi-dimensional arrays use the memory layout
+ * of the reference's column-major Julia arrays, so a Julia `ccall` can pass its arrays
+ * without copying:
+ *   hamiltonian_r[nw, nw, NR]    element (i, j, R) at complex offset i + nw*(j + nw*R)
+ *   position_r[nw, nw, 3, NR]    element (i, j, a, R) at i + nw*(j + nw*(a + 3*R))
+ *   overlap_r[nw, nw, NR]        like hamiltonian_r
+ *   r_vectors[3, NR] (int64)     element (a, R) at a + 3*R
+ *   lattice[3, 3]                element (i, j) at i + 3*j; row i is lattice vector i (Angstrom)
+ *
+ * Errors: every entry point returns a wnlqg_status; the message of the last failure on the
+ * calling thread is available through wnlqg_b200_last_error.  Handles are reentrant per
+ * handle; calls on one handle must not overlap.
+ */
+#ifndef WNLQG_B200_H
+#define WNLQG_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define WNLQG_API __attribute__((visibility("default")))
+#else
+#define WNLQG_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum wnlqg_status {
+    WNLQG_OK = 0,
+    WNLQG_ERR_INVALID_ARGUMENT = 1,   /* reference: ArgumentError */
+    WNLQG_ERR_DIMENSION_MISMATCH = 2, /* reference: DimensionMismatch */
+    WNLQG_ERR_NONFINITE = 3,          /* non-finite model data or results */
+    WNLQG_ERR_CUDA = 4,               /* a CUDA runtime call failed */
+    WNLQG_ERR_OUT_OF_MEMORY = 5,
+    WNLQG_ERR_UNSUPPORTED = 6,        /* request outside what this build implements */
+    WNLQG_ERR_DEVICE_TIMEOUT = 7      /* a bounded device-side wait gave up */
+} wnlqg_status;
+
+/* Response kinds (one per reference task family). */
+typedef enum wnlqg_response_kind {
+    WNLQG_SHIFT_CURRENT = 1,      /* sigma^{abc}(omega), ConventionalShiftCurrent.jl */
+    WNLQG_INJECTION_CURRENT = 2,  /* eta^{abc}(omega), ConventionalInjectionCurrent.jl */
+    WNLQG_BERRY_CURVATURE = 3,    /* occupied-sum Omega^{ab}, ConventionalQuantumGeometry.jl:188-215 */
+    WNLQG_QUANTUM_METRIC = 4,     /* band-sum internal g^{ab}, ConventionalQuantumGeometry.jl:321-355 */
+    WNLQG_INTRINSIC_AHC = 5,      /* sigma^{ab} Fermi sea over the mu axis, IntrinsicHallOccupations.jl */
+    WNLQG_BERRY_DIPOLE = 6,       /* D^{abc} Fermi surface over the mu axis, BerryMultipoleMoments.jl */
+    WNLQG_JERK_CURRENT = 8        /* ordered jerk (abcd)(omega), ConventionalJerkCurrent.jl */
+} wnlqg_response_kind;
+
+typedef enum wnlqg_broadening {
+    WNLQG_GAUSSIAN = 0,
+    WNLQG_LORENTZIAN = 1
+} wnlqg_broadening;
+
+typedef enum wnlqg_precision {
+    WNLQG_PRECISION_FP64 = 0,   /* plain FP64 throughout */
+    WNLQG_PRECISION_MIXED = 1   /* FP32 bulk arithmetic, FP64 where accuracy needs it */
+} wnlqg_precision;
+
+#define WNLQG_MAX_RESPONSES 8
+#define WNLQG_MAX_COMPONENTS 81
+
+/* Model description (mirrors TightBindingModel, src/Core/Models.jl:11-75). */
+typedef struct wnlqg_model_desc {
+    int64_t num_orbitals;
+    int64_t num_r_vectors;
+    const double *lattice;         /* [3,3] */
+    const int64_t *r_vectors;      /* [3,NR] */
+    const int64_t *r_degeneracies; /* [NR] */
+    const double *hamiltonian_r;   /* complex [nw,nw,NR], eV */
+    const double *position_r;      /* complex [nw,nw,3,NR], Angstrom; may be NULL (zero) */
+    const double *overlap_r;       /* complex [nw,nw,NR]; NULL for orthogonal models */
+} wnlqg_model_desc;
+
+/* One requested response and its Cartesian components (0-based axes). */
+typedef struct wnlqg_response_request {
+    int32_t kind;                                   /* wnlqg_response_kind */
+    int32_t num_components;
+    int32_t components[WNLQG_MAX_COMPONENTS][4];    /* (a,b,c,d); unused slots ignored */
+} wnlqg_response_request;
+
+/* Task description (the fields of EffectiveTaskConfig, src/Runtime/Config.jl:95-175, that the
+ * hot path reads). */
+typedef struct wnlqg_task_desc {
+    int32_t num_responses;
+    wnlqg_response_request responses[WNLQG_MAX_RESPONSES];
+    double fermi_energy;               /* eV */
+    double temperature;                /* K */
+    int32_t broadening_type;           /* wnlqg_broadening */
+    double broadening;                 /* eV */
+    double transition_window_factor;
+    double denominator_regularization; /* eV; 0 selects the bare inverse */
+    double degeneracy_threshold;       /* eV */
+    int64_t num_photon_energies;
+    const double *photon_energies;     /* eV */
+    int64_t num_fermi_energies;        /* mu axis for AHC / Berry dipole */
+    const double *fermi_energies;      /* eV */
+    int32_t precision;                 /* wnlqg_precision */
+} wnlqg_task_desc;
+
+typedef struct wnlqg_model wnlqg_model;   /* device-resident model */
+typedef struct wnlqg_plan wnlqg_plan;     /* compiled task: channels, tiles, workspaces */
+
+/* Library version string. */
+WNLQG_API const char *wnlqg_b200_version(void);
+
+/* Message of the last error on the calling thread (always NUL-terminated; may be empty). */
+WNLQG_API wnlqg_status wnlqg_b200_last_error(char *buffer, size_t capacity);
+
+/* Number of visible CUDA devices (0 when no driver or device). */
+WNLQG_API int32_t wnlqg_b200_device_count(void);
+
+/* Copy a model to device `device`.  Replaces the model load of read_wannier_tb /
+ * TightBindingModel (src/IO/WannierTB.jl:53-127, src/Core/Models.jl:11-75). */
+WNLQG_API wnlqg_status wnlqg_b200_model_create(const wnlqg_model_desc *desc, int32_t device,
+                                     wnlqg_model **out_model);
+WNLQG_API wnlqg_status wnlqg_b200_model_destroy(wnlqg_model *model);
+
+/* Compile a task for a model: Fourier channel plan and real-space tiles
+ * (prepare_real_space!, HamiltonianMatrixElements.jl:92-198 and PositionMatrixElements.jl:8-84),
+ * per-batch workspaces sized for `max_batch` k-points.
+ * Replaces the setup half of _run_integral_bundle_owned! (Runtime/Execution/IntegralDriver.jl:92-560). */
+WNLQG_API wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *task,
+                                    int64_t max_batch, wnlqg_plan **out_plan);
+WNLQG_API wnlqg_status wnlqg_b200_plan_destroy(wnlqg_plan *plan);
+
+/* Number of complex values one k-point contributes (all responses concatenated).
+ * Per response: shift/injection/jerk [num_photon_energies x num_components],
+ * curvature/metric [num_components], AHC/dipole [num_fermi_energies x num_components];
+ * the energy axis is fastest. */
+WNLQG_API int64_t wnlqg_b200_plan_value_count(const wnlqg_plan *plan);
+
+/* Sum over the Gamma-centred mesh points k_begin <= idx < k_end of (1/Nk) * value(k), the
+ * reference's lane tensor (consume_point!, IntegralDriver.jl:820-874, with the mesh of
+ * CalculationUtils.jl:265-292, first axis fastest).  `out` (host) receives
+ * plan_value_count complex values.  Replaces the per-worker k loop of
+ * execute_prepared_tasks! (TaskSamplingScheduler.jl:151-217) for one lane. */
+WNLQG_API wnlqg_status wnlqg_b200_eval_mesh(wnlqg_plan *plan, const int64_t mesh[3], int64_t k_begin,
+                                  int64_t k_end, double *out);
+
+/* Same as wnlqg_b200_eval_mesh with a device output pointer, on `stream` (a cudaStream_t, or
+ * NULL for the legacy default stream).  Asynchronous: the caller synchronises the stream. */
+WNLQG_API wnlqg_status wnlqg_b200_eval_mesh_device(wnlqg_plan *plan, const int64_t mesh[3],
+                                         int64_t k_begin, int64_t k_end, double *out_device,
+                                         void *stream);
+
+/* Per-point values at arbitrary fractional k-points: k[3*n] (host), out[n*value_count]
+ * complex (host).  This is the ResponsePointEvaluator / ResponseNodeEvaluator contract
+ * (Runtime/Execution/ResponsePointEvaluation.jl:8-64) batched over n points, used by the
+ * adaptive integrator (ResponseIntegration.jl:100-198). */
+WNLQG_API wnlqg_status wnlqg_b200_eval_points(wnlqg_plan *plan, const double *kpoints, int64_t n,
+                                    double *out);
+
+/* Per-k band data for diagnostics and tests: energies [n*nw] (ascending) and the
+ * canonicalised eigenvectors [n*nw*nw] complex, column-major per k
+ * (compute_spectrum!, HamiltonianMatrixElements.jl:279-300 and :6-25). */
+WNLQG_API wnlqg_status wnlqg_b200_eval_spectrum(wnlqg_plan *plan, const double *kpoints, int64_t n,
+                                      double *energies, double *eigenvectors);
+
+/* Device time in milliseconds of the last eval_mesh* call's dominant kernel and of the
+ * whole call (CUDA events on the plan's stream). */
+WNLQG_API wnlqg_status wnlqg_b200_plan_last_timing(const wnlqg_plan *plan, double *fourier_ms,
+                                         double *eigen_ms, double *response_ms,
+                                         double *total_ms);
+
+/* Number of kernel launches issued by the last eval_mesh* call. */
+WNLQG_API int64_t wnlqg_b200_plan_last_launch_count(const wnlqg_plan *plan);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WNLQG_B200_H */

@@ -1,0 +1,766 @@
+// wnlqg_oracle.cpp -- CPU FP64 restatement of the WannierNLQG k-mesh response hot path.
+//
+// TEST INFRASTRUCTURE ONLY.  This file is the parity oracle: tests/, __graft_entry__.smoke()
+// and the CPU-baseline leg of bench.py call it as the checker and as the timed CPU path.  The
+// product (wanniernlqg_b200) never links, imports or calls it.
+//
+// Each routine restates the reference's Julia code (paths relative to the WannierNLQG project)
+// with plain loops in the reference's own summation order, FP64 / complex<double> throughout:
+//   Fourier factors             src/MatrixElements/Interpolated/HamiltonianMatrixElements.jl:28-39
+//   direct Fourier sums         HamiltonianMatrixElements.jl:42-58, 426-462; PositionMatrixElements.jl:239-334
+//   real-space derivative tiles HamiltonianMatrixElements.jl:92-177; PositionMatrixElements.jl:8-84
+//   Hermitian eigensolve        src/Core/ESKernel/DenseSpectra.jl:14-16 (LAPACK there; cyclic Jacobi here)
+//   phase canonicalisation      HamiltonianMatrixElements.jl:6-25
+//   gauge rotation U'XU         HamiltonianMatrixElements.jl:61-71
+//   gauge correction, r, F      PositionMatrixElements.jl:416-556; PositionVertexRegularization.jl:7-29
+//   transition screen           src/Runtime/Execution/TransitionScreening.jl:32-94; CalculationUtils.jl:21-46
+//   shift current               src/Responses/ShiftCurrent/ConventionalShiftCurrent.jl:191-229, 686-884
+//   injection current           src/Responses/InjectionCurrent/ConventionalInjectionCurrent.jl:23-211
+//   prefactors                  src/Runtime/Execution/ConventionalCurrentIntegralExecution.jl:241-245, 294-298
+//   Berry curvature / metric    src/Responses/QuantumGeometry/ConventionalQuantumGeometry.jl:188-215, 321-355
+//   jerk                        src/Responses/JerkCurrent/ConventionalJerkCurrent.jl:14-65;
+//                               MatrixElements/Interpolated/ThirdOrderGeometry.jl:28-41, 131-160
+//   mesh + lanes                src/Core/CalculationUtils.jl:280-292; Runtime/Setup/BundleAssembly.jl:35-53;
+//                               Runtime/Execution/IntegralDriver.jl:820-874; Reduction/DeterministicReduction.jl:2-38
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <omp.h>
+
+#include "../include/wnlqg_b200.h"
+
+namespace {
+
+using cd = std::complex<double>;
+const cd I1(0.0, 1.0);
+const double PI = 3.14159265358979323846;
+
+// Constants of src/Core/Constants.jl:1-4.
+const double ELEMENTARY_CHARGE_C = 1.602176634e-19;
+const double REDUCED_PLANCK_CONSTANT_J_S = 1.054571817e-34;
+const double REDUCED_PLANCK_CONSTANT_EV_S = 6.582119569e-16;
+const double BOLTZMANN_CONSTANT_EV_K = 8.617333262e-5;
+
+thread_local std::string g_error;
+
+struct Mat {
+    int n = 0;
+    std::vector<cd> v;
+    void init(int size) { n = size; v.assign((size_t)size * size, cd(0.0, 0.0)); }
+    cd &operator()(int i, int j) { return v[(size_t)i + (size_t)n * j]; }
+    const cd &operator()(int i, int j) const { return v[(size_t)i + (size_t)n * j]; }
+};
+
+struct Model {
+    int nw = 0, nr = 0;
+    double lattice[9];
+    std::vector<int64_t> rvec;    // [3*NR]
+    std::vector<int64_t> deg;     // [NR]
+    std::vector<cd> H;            // [nw*nw*NR]
+    std::vector<cd> A;            // [nw*nw*3*NR] (zeros when absent)
+    bool has_position = false;
+};
+
+// Which Cartesian channels a task needs (the reference's MatrixElementPlan direction
+// requirements, MatrixElementPlan.jl:1-18, restated as masks).
+struct Needs {
+    bool dH[3] = {false, false, false};
+    bool ddH[3][3] = {};
+    bool A[3] = {false, false, false};
+    bool dA[3][3] = {};   // [position][derivative]
+    bool F[3][3] = {};
+    void need_r(int a) { A[a] = true; dH[a] = true; }
+    void need_gder(int p, int d) {   // r^p_{nm;d}
+        dA[p][d] = true; ddH[p][d] = true; ddH[d][p] = true;
+        need_r(p); need_r(d);
+    }
+};
+
+struct KData {
+    int nw = 0;
+    std::vector<double> E;
+    Mat U, Uadj;
+    Mat dH[3], ddH[3][3], Aint[3], dA[3][3], F[3][3], inv, D[3], r[3];
+};
+
+void set_error(const std::string &s) { g_error = s; }
+
+// _r_vector_cartesian (HamiltonianMatrixElements.jl:74-83): R_cart = sum_i r_i * lattice[i,:].
+void r_cartesian(const Model &m, int ir, double out[3]) {
+    const int64_t *r = &m.rvec[3 * (size_t)ir];
+    for (int j = 0; j < 3; ++j)
+        out[j] = (double)r[0] * m.lattice[0 + 3 * j] + (double)r[1] * m.lattice[1 + 3 * j] +
+                 (double)r[2] * m.lattice[2 + 3 * j];
+}
+
+// U' * X * U (transform_to_hamiltonian_gauge!, HamiltonianMatrixElements.jl:61-71).
+void rotate(const KData &d, const Mat &x, Mat &out) {
+    int n = d.nw;
+    Mat t; t.init(n);
+    for (int j = 0; j < n; ++j)
+        for (int l = 0; l < n; ++l) {
+            cd xl = x(l, j);
+            for (int i = 0; i < n; ++i) t(i, j) += d.Uadj(i, l) * xl;
+        }
+    out.init(n);
+    for (int j = 0; j < n; ++j)
+        for (int l = 0; l < n; ++l) {
+            cd ul = d.U(l, j);
+            for (int i = 0; i < n; ++i) out(i, j) += t(i, l) * ul;
+        }
+}
+
+// Cyclic Jacobi eigensolver for the Hermitian matrix given by the upper triangle of `h`
+// (Julia's Hermitian(H, :U) view), FP64.  Eigenvalues ascending (stable for ties),
+// eigenvector columns in U.  Stands in for LAPACK (DenseSpectra.jl:14-16); both are
+// backward stable, so eigenvalues agree to O(eps*||H||).
+void hermitian_eigen(const Mat &h, std::vector<double> &evals, Mat &U) {
+    int n = h.n;
+    Mat a; a.init(n);
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i <= j; ++i) {
+            if (i == j) a(i, i) = cd(h(i, i).real(), 0.0);
+            else { a(i, j) = h(i, j); a(j, i) = std::conj(h(i, j)); }
+        }
+    Mat v; v.init(n);
+    for (int i = 0; i < n; ++i) v(i, i) = 1.0;
+    double fro = 0.0;
+    for (auto &z : a.v) fro += std::norm(z);
+    fro = std::sqrt(fro);
+    const double tol = fro * 8.673617379884035e-19;  // 2^-60 * ||H||_F
+    for (int sweep = 0; sweep < 60; ++sweep) {
+        bool rotated = false;
+        for (int p = 0; p < n - 1; ++p)
+            for (int q = p + 1; q < n; ++q) {
+                cd apq = a(p, q);
+                double g = std::abs(apq);
+                if (!(g > tol)) continue;
+                rotated = true;
+                double app = a(p, p).real(), aqq = a(q, q).real();
+                cd ph = apq / g;   // e^{i phi}
+                double theta = (aqq - app) / (2.0 * g);
+                double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+                double c = 1.0 / std::sqrt(t * t + 1.0);
+                double s = t * c;
+                cd sp = s * ph, sm = s * std::conj(ph);
+                // A <- A J, J = [[c, s e^{i phi}], [-s e^{-i phi}, c]] on (p,q)
+                for (int i = 0; i < n; ++i) {
+                    cd aip = a(i, p), aiq = a(i, q);
+                    a(i, p) = c * aip - sm * aiq;
+                    a(i, q) = sp * aip + c * aiq;
+                }
+                // A <- J^H A
+                for (int j = 0; j < n; ++j) {
+                    cd apj = a(p, j), aqj = a(q, j);
+                    a(p, j) = c * apj - sp * aqj;
+                    a(q, j) = sm * apj + c * aqj;
+                }
+                a(p, q) = 0.0; a(q, p) = 0.0;
+                a(p, p) = cd(a(p, p).real(), 0.0);
+                a(q, q) = cd(a(q, q).real(), 0.0);
+                for (int i = 0; i < n; ++i) {
+                    cd vip = v(i, p), viq = v(i, q);
+                    v(i, p) = c * vip - sm * viq;
+                    v(i, q) = sp * vip + c * viq;
+                }
+            }
+        if (!rotated) break;
+    }
+    std::vector<int> order(n);
+    for (int i = 0; i < n; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int x, int y) { return a(x, x).real() < a(y, y).real(); });
+    evals.resize(n);
+    U.init(n);
+    for (int j = 0; j < n; ++j) {
+        evals[j] = a(order[j], order[j]).real();
+        for (int i = 0; i < n; ++i) U(i, j) = v(i, order[j]);
+    }
+}
+
+// canonicalize_eigenvectors! (HamiltonianMatrixElements.jl:6-25).
+void canonicalize(Mat &U) {
+    int n = U.n;
+    for (int j = 0; j < n; ++j) {
+        int pivot = 0;
+        double pm = std::abs(U(0, j));
+        for (int i = 1; i < n; ++i) {
+            double m = std::abs(U(i, j));
+            if (m > pm) { pivot = i; pm = m; }
+        }
+        if (pm > 0.0) {
+            cd phase = std::conj(U(pivot, j)) / pm;
+            for (int i = 0; i < n; ++i) U(i, j) *= phase;
+        }
+    }
+}
+
+// regularized_energy_inverse (PositionVertexRegularization.jl:17-29).
+double regularized_inverse(double d, double eta) {
+    double den = d * d + eta * eta;
+    if (std::isfinite(den) && den != 0.0) return d / den;
+    if (!(std::isfinite(d) && std::isfinite(eta) && eta > 0)) return d / den;
+    double scale = std::max(std::fabs(d), eta);
+    double sd = d / scale, sw = eta / scale;
+    return (sd / (sd * sd + sw * sw)) / scale;
+}
+
+// Fourier interpolation, eigensolve and Hamiltonian-gauge geometry at one k
+// (compute_spectrum! + compute_remaining!, HamiltonianMatrixElements.jl:279-300, 532-563).
+void compute_kpoint(const Model &m, const Needs &need, const double k[3], double eta, KData &d) {
+    int n = m.nw;
+    d.nw = n;
+    size_t nn = (size_t)n * n;
+    // Fourier factors exp(2 pi i R.k)/deg (HamiltonianMatrixElements.jl:28-39).
+    std::vector<cd> f(m.nr);
+    for (int ir = 0; ir < m.nr; ++ir) {
+        const int64_t *r = &m.rvec[3 * (size_t)ir];
+        double phase = (double)r[0] * k[0] + (double)r[1] * k[1] + (double)r[2] * k[2];
+        f[ir] = std::polar(1.0, 2.0 * PI * phase) / (double)m.deg[ir];
+    }
+    Mat Hw; Hw.init(n);
+    Mat dHw[3], ddHw[3][3], Aw[3], dAw[3][3];
+    bool needAw[3];
+    for (int a = 0; a < 3; ++a) {
+        needAw[a] = need.A[a];
+        for (int b = 0; b < 3; ++b) if (need.F[a][b]) { needAw[a] = true; needAw[b] = true; }
+    }
+    bool needdAw[3][3];
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b)
+            needdAw[a][b] = need.dA[a][b] || need.F[a][b] || need.F[b][a];
+    for (int a = 0; a < 3; ++a) {
+        if (need.dH[a]) dHw[a].init(n);
+        if (needAw[a]) Aw[a].init(n);
+        for (int b = 0; b < 3; ++b) {
+            if (need.ddH[a][b]) ddHw[a][b].init(n);
+            if (needdAw[a][b]) dAw[a][b].init(n);
+        }
+    }
+    // Direct sums in R order (HamiltonianMatrixElements.jl:42-58, 428-460; PositionMatrixElements.jl:294-332).
+    for (int ir = 0; ir < m.nr; ++ir) {
+        double rc[3];
+        r_cartesian(m, ir, rc);
+        const cd fr = f[ir];
+        const cd *h = &m.H[nn * ir];
+        for (size_t e = 0; e < nn; ++e) {
+            cd fh = fr * h[e];
+            Hw.v[e] += fh;
+        }
+        for (int a = 0; a < 3; ++a) {
+            if (need.dH[a]) {
+                for (size_t e = 0; e < nn; ++e) dHw[a].v[e] += fr * (I1 * rc[a] * h[e]);
+            }
+            for (int b = 0; b < 3; ++b)
+                if (need.ddH[a][b])
+                    for (size_t e = 0; e < nn; ++e) ddHw[a][b].v[e] += fr * (-rc[a] * rc[b] * h[e]);
+        }
+        if (m.has_position) {
+            for (int a = 0; a < 3; ++a) {
+                const cd *pa = &m.A[nn * (a + 3 * (size_t)ir)];
+                if (needAw[a])
+                    for (size_t e = 0; e < nn; ++e) Aw[a].v[e] += fr * pa[e];
+                for (int b = 0; b < 3; ++b)
+                    if (needdAw[a][b])
+                        for (size_t e = 0; e < nn; ++e) dAw[a][b].v[e] += fr * (I1 * rc[b] * pa[e]);
+            }
+        }
+    }
+    std::vector<double> ev;
+    hermitian_eigen(Hw, ev, d.U);
+    canonicalize(d.U);
+    d.E = ev;
+    d.Uadj.init(n);
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) d.Uadj(i, j) = std::conj(d.U(j, i));
+    for (int a = 0; a < 3; ++a) {
+        if (need.dH[a]) rotate(d, dHw[a], d.dH[a]);
+        if (needAw[a]) rotate(d, Aw[a], d.Aint[a]);
+        for (int b = 0; b < 3; ++b) {
+            if (need.ddH[a][b]) rotate(d, ddHw[a][b], d.ddH[a][b]);
+            if (need.dA[a][b]) rotate(d, dAw[a][b], d.dA[a][b]);
+        }
+    }
+    // Wannier curvature F_ab = dA_b/dk_a - dA_a/dk_b - i[A_a, A_b], then U'FU
+    // (PositionMatrixElements.jl:485-556, non-curl branch).
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+            if (!need.F[a][b]) continue;
+            Mat fw; fw.init(n);
+            for (int col = 0; col < n; ++col)
+                for (int row = 0; row < n; ++row) {
+                    cd val = dAw[b][a](row, col) - dAw[a][b](row, col);
+                    for (int l = 0; l < n; ++l)
+                        val -= I1 * (Aw[a](row, l) * Aw[b](l, col) - Aw[b](row, l) * Aw[a](l, col));
+                    fw(row, col) = val;
+                }
+            rotate(d, fw, d.F[a][b]);
+        }
+    // Inverse energy differences (PositionMatrixElements.jl:444-461).
+    d.inv.init(n);
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i) {
+            double diff = d.E[i] - d.E[j];
+            if (eta == 0.0) d.inv(i, j) = diff == 0.0 ? 0.0 : 1.0 / diff;
+            else d.inv(i, j) = regularized_inverse(diff, eta);
+        }
+    for (int a = 0; a < 3; ++a) {
+        if (!need.dH[a]) continue;
+        d.D[a].init(n);
+        for (size_t e = 0; e < nn; ++e) d.D[a].v[e] = -d.dH[a].v[e] * d.inv.v[e];
+        if (need.A[a]) {
+            d.r[a].init(n);
+            for (size_t e = 0; e < nn; ++e) d.r[a].v[e] = d.Aint[a].v[e] + I1 * d.D[a].v[e];
+        }
+    }
+}
+
+// conventional_generalized_position_derivative_element (ConventionalShiftCurrent.jl:191-229):
+// r^a_{nm;b} with a the position axis and b the derivative axis.
+cd gder(const KData &d, int n, int m, int a, int b) {
+    cd sum_AD(0.0, 0.0), sum_HD(0.0, 0.0);
+    for (int l = 0; l < d.nw; ++l) {
+        if (l != n && l != m) {
+            sum_AD += d.Aint[a](n, l) * d.D[b](l, m) - d.D[b](n, l) * d.Aint[a](l, m);
+            sum_HD += d.dH[a](n, l) * d.D[b](l, m) - d.D[b](n, l) * d.dH[a](l, m);
+        }
+    }
+    cd AD_bit = (d.Aint[b](n, n) - d.Aint[b](m, m)) * d.D[a](n, m) +
+                (d.Aint[a](n, n) - d.Aint[a](m, m)) * d.D[b](n, m);
+    cd AA_bit = (d.Aint[b](n, n) - d.Aint[b](m, m)) * d.Aint[a](n, m);
+    cd DV_bit = (d.dH[b](n, n) - d.dH[b](m, m)) * d.D[a](n, m) +
+                (d.dH[a](n, n) - d.dH[a](m, m)) * d.D[b](n, m);
+    return d.dA[a][b](n, m) + AD_bit - I1 * AA_bit + sum_AD +
+           I1 * (d.ddH[a][b](n, m) + sum_HD + DV_bit) * (-d.inv(n, m));
+}
+
+// fermi_dirac! (CalculationUtils.jl:28-46).
+void fermi(const std::vector<double> &E, double mu, double T, std::vector<double> &f) {
+    double kt = BOLTZMANN_CONSTANT_EV_K * T;
+    f.resize(E.size());
+    for (size_t i = 0; i < E.size(); ++i) {
+        if (kt == 0.0) f[i] = E[i] <= mu ? 1.0 : 0.0;
+        else {
+            double arg = std::min(700.0, std::max(-700.0, (E[i] - mu) / kt));
+            f[i] = 1.0 / (std::exp(arg) + 1.0);
+        }
+    }
+}
+
+struct Screen {
+    bool active = false;
+    std::vector<double> fnm;     // [n + nw*m]
+    std::vector<double> delta;   // [w + nom*(n + nw*m)]
+    std::vector<char> mask;      // [n + nw*m]
+};
+
+// _fill_transition_screen! (TransitionScreening.jl:32-94) with the full band window.
+void fill_screen(const std::vector<double> &E, const std::vector<double> &f,
+                 const wnlqg_task_desc &t, Screen &s) {
+    int n = (int)E.size();
+    int64_t nom = t.num_photon_energies;
+    bool gaussian = t.broadening_type == WNLQG_GAUSSIAN;
+    double eta = t.broadening;
+    double cutoff = eta * std::sqrt(200.0);
+    double gscale = gaussian ? 1.0 / (std::sqrt(PI) * eta) : 0.0;
+    double thr = t.transition_window_factor * eta;
+    s.active = false;
+    s.fnm.assign((size_t)n * n, 0.0);
+    s.delta.assign((size_t)nom * n * n, 0.0);
+    s.mask.assign((size_t)n * n, 0);
+    for (int a = 0; a < n; ++a)
+        for (int b = 0; b < n; ++b) {
+            double od = f[a] - f[b];
+            s.fnm[a + (size_t)n * b] = od;
+            double te = E[b] - E[a];
+            bool occ = std::fabs(od) > 1.0e-10;
+            bool pair_active = occ && !gaussian;
+            if (occ && !gaussian && thr <= 0) s.active = true;
+            for (int64_t w = 0; w < nom; ++w) {
+                double x = te - t.photon_energies[w];
+                bool inside = false;
+                double dv;
+                if (gaussian) {
+                    inside = std::fabs(x) < cutoff;
+                    dv = inside ? gscale * std::exp(-(x / eta) * (x / eta)) : 0.0;
+                    pair_active = pair_active || (occ && inside);
+                } else {
+                    dv = (eta / PI) / (x * x + eta * eta);
+                }
+                s.delta[w + nom * (a + (size_t)n * b)] = dv;
+                if (occ && (gaussian ? inside : (thr > 0 && std::fabs(x) < thr))) s.active = true;
+            }
+            s.mask[a + (size_t)n * b] = pair_active ? 1 : 0;
+        }
+}
+
+struct Task {
+    wnlqg_task_desc desc;
+    std::vector<double> omegas, mus;
+    Needs need;
+    int64_t value_count = 0;
+};
+
+bool build_task(const wnlqg_task_desc *t, Task &task) {
+    task.desc = *t;
+    if (t->num_photon_energies < 0 || t->num_fermi_energies < 0) { set_error("negative axis length"); return false; }
+    task.omegas.assign(t->photon_energies, t->photon_energies + t->num_photon_energies);
+    if (t->num_fermi_energies > 0) task.mus.assign(t->fermi_energies, t->fermi_energies + t->num_fermi_energies);
+    task.desc.photon_energies = task.omegas.data();
+    task.desc.fermi_energies = task.mus.data();
+    if (!(t->broadening > 0) || !std::isfinite(t->broadening)) { set_error("broadening must be finite and positive"); return false; }
+    if (!(t->denominator_regularization >= 0)) { set_error("denominator_regularization must be >= 0"); return false; }
+    if (t->num_responses < 1 || t->num_responses > WNLQG_MAX_RESPONSES) { set_error("num_responses out of range"); return false; }
+    int64_t count = 0;
+    for (int r = 0; r < t->num_responses; ++r) {
+        const wnlqg_response_request &q = t->responses[r];
+        if (q.num_components < 1 || q.num_components > WNLQG_MAX_COMPONENTS) { set_error("num_components out of range"); return false; }
+        for (int c = 0; c < q.num_components; ++c) {
+            const int32_t *x = q.components[c];
+            for (int i = 0; i < 4; ++i)
+                if (x[i] < 0 || x[i] > 2) { set_error("component axis out of range"); return false; }
+            int a = x[0], b = x[1], cc = x[2], dd = x[3];
+            switch (q.kind) {
+            case WNLQG_SHIFT_CURRENT:
+                task.need.need_gder(cc, a); task.need.need_gder(b, a);
+                task.need.need_r(b); task.need.need_r(cc);
+                break;
+            case WNLQG_INJECTION_CURRENT:
+                task.need.dH[a] = true; task.need.need_r(b); task.need.need_r(cc);
+                break;
+            case WNLQG_BERRY_CURVATURE:
+                task.need.F[a][b] = true; task.need.need_r(a); task.need.need_r(b);
+                break;
+            case WNLQG_QUANTUM_METRIC:
+                task.need.need_r(a); task.need.need_r(b);
+                break;
+            case WNLQG_JERK_CURRENT:
+                task.need.need_r(b); task.need.need_r(cc);
+                task.need.dH[a] = true; task.need.dH[dd] = true;
+                task.need.ddH[a][dd] = true;
+                break;
+            default:
+                set_error("response kind not implemented by the oracle"); return false;
+            }
+        }
+        if (q.kind == WNLQG_SHIFT_CURRENT || q.kind == WNLQG_INJECTION_CURRENT || q.kind == WNLQG_JERK_CURRENT)
+            count += q.num_components * t->num_photon_energies;
+        else
+            count += q.num_components;
+    }
+    task.value_count = count;
+    return true;
+}
+
+// Jerk Eq. 9.20 from prepared band data (ConventionalJerkCurrent.jl:14-65 with
+// prepare_third_order_band_geometry!, ThirdOrderGeometry.jl:131-160, and
+// _fill_jerk_current_dipoles!, ThirdOrderGeometry.jl:28-41).  B = dH, A = internal
+// connection, C = ddH, all in the Hamiltonian gauge; out[w + nom*comp].
+void jerk_response(int n, const double *E, const cd *B, const cd *A, const cd *C, int64_t nom,
+                   const double *om, double mu, double T, double width, bool gaussian, double reg,
+                   double window, int ncomp, const int32_t (*comps)[4], cd *out) {
+    auto b3 = [&](int i, int j, int a) { return B[i + n * (j + n * a)]; };
+    auto a3 = [&](int i, int j, int a) { return A[i + n * (j + n * a)]; };
+    auto c4 = [&](int i, int j, int a, int dd) { return C[i + n * (j + n * (a + 3 * dd))]; };
+    std::vector<double> hess((size_t)n * 9);
+    std::vector<cd> dip((size_t)n * n * 3);
+    for (int nn = 0; nn < n; ++nn)
+        for (int a = 0; a < 3; ++a)
+            for (int dd = 0; dd < 3; ++dd) {
+                double value = c4(nn, nn, a, dd).real();
+                for (int l = 0; l < n; ++l) {
+                    if (l == nn) continue;
+                    double gap = E[nn] - E[l];
+                    double inverse = gap / (gap * gap + reg * reg);
+                    value += 2.0 * (b3(nn, l, a) * b3(l, nn, dd)).real() * inverse;
+                }
+                hess[nn + n * (a + 3 * dd)] = value;
+            }
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j)
+            for (int a = 0; a < 3; ++a) {
+                double gap = E[i] - E[j];
+                dip[i + n * (j + n * a)] = i == j ? cd(0.0, 0.0)
+                                                  : a3(i, j, a) - I1 * b3(i, j, a) * gap / (gap * gap + reg * reg);
+            }
+    std::vector<double> occ;
+    std::vector<double> Ev(E, E + n);
+    fermi(Ev, mu, T, occ);
+    for (int64_t e = 0; e < nom * ncomp; ++e) out[e] = 0.0;
+    for (int m = 0; m < n; ++m)
+        for (int nn = 0; nn < n; ++nn) {
+            double gap = E[nn] - E[m];
+            if (!(gap > 0)) continue;
+            double o = occ[m] - occ[nn];
+            for (int64_t w = 0; w < nom; ++w) {
+                double energy = om[w];
+                if (window > 0 && std::fabs(gap - energy) > window * width) continue;
+                double x = (gap - energy) / width;
+                double delta = gaussian ? std::exp(-x * x) / (std::sqrt(PI) * width)
+                                        : 1.0 / (PI * width * (1 + x * x));
+                double weight = o * delta;
+                for (int c = 0; c < ncomp; ++c) {
+                    int a = comps[c][0], b = comps[c][1], cc = comps[c][2], dd = comps[c][3];
+                    cd optical = dip[nn + n * (m + n * b)] * dip[m + n * (nn + n * cc)];
+                    out[w + nom * c] += weight * optical *
+                                        (hess[nn + n * (a + 3 * dd)] - hess[m + n * (a + 3 * dd)]);
+                }
+            }
+        }
+}
+
+// One k-point's concatenated response values (point_value!, IntegralDriver.jl:596-...), with
+// num_kpoints = 1 in every prefactor (the 1/Nk scale is applied by the lane consumer).
+void point_values(const Model &m, const Task &task, const double k[3], cd *out) {
+    const wnlqg_task_desc &t = task.desc;
+    KData d;
+    compute_kpoint(m, task.need, k, t.denominator_regularization, d);
+    int n = d.nw;
+    std::vector<double> f;
+    fermi(d.E, t.fermi_energy, t.temperature, f);
+    Screen s;
+    bool need_screen = false;
+    for (int r = 0; r < t.num_responses; ++r)
+        need_screen |= t.responses[r].kind == WNLQG_SHIFT_CURRENT || t.responses[r].kind == WNLQG_INJECTION_CURRENT;
+    if (need_screen) fill_screen(d.E, f, t, s);
+    double vol = 0.0;
+    {
+        const double *L = m.lattice;  // det of lattice[i,j] = L[i + 3j]
+        auto e = [&](int i, int j) { return L[i + 3 * j]; };
+        vol = e(0, 0) * (e(1, 1) * e(2, 2) - e(1, 2) * e(2, 1)) - e(0, 1) * (e(1, 0) * e(2, 2) - e(1, 2) * e(2, 0)) +
+              e(0, 2) * (e(1, 0) * e(2, 1) - e(1, 1) * e(2, 0));
+    }
+    int64_t nom = t.num_photon_energies;
+    cd *o = out;
+    for (int r = 0; r < t.num_responses; ++r) {
+        const wnlqg_response_request &q = t.responses[r];
+        int nc = q.num_components;
+        if (q.kind == WNLQG_SHIFT_CURRENT || q.kind == WNLQG_INJECTION_CURRENT) {
+            for (int64_t e = 0; e < nom * nc; ++e) o[e] = 0.0;
+            if (s.active) {
+                double P = q.kind == WNLQG_SHIFT_CURRENT
+                               ? REDUCED_PLANCK_CONSTANT_EV_S * PI * std::pow(-ELEMENTARY_CHARGE_C, 3) /
+                                     (2.0 * REDUCED_PLANCK_CONSTANT_J_S * REDUCED_PLANCK_CONSTANT_J_S * vol)
+                               : -PI * std::pow(ELEMENTARY_CHARGE_C, 3) /
+                                     (REDUCED_PLANCK_CONSTANT_J_S * REDUCED_PLANCK_CONSTANT_J_S * vol);
+                // Per-pair kernels for the requested components (compute_*_kernel!).
+                std::vector<cd> kern((size_t)n * n * nc, cd(0.0, 0.0));
+                for (int c = 0; c < nc; ++c) {
+                    int a = q.components[c][0], b = q.components[c][1], cc = q.components[c][2];
+                    for (int nn = 0; nn < n; ++nn)
+                        for (int mm = 0; mm < n; ++mm) {
+                            if (!s.mask[nn + (size_t)n * mm]) continue;
+                            cd val;
+                            if (q.kind == WNLQG_SHIFT_CURRENT) {
+                                cd dnm = gder(d, nn, mm, cc, a);
+                                cd dmn = gder(d, mm, nn, b, a);
+                                val = -I1 * (dnm * d.r[b](mm, nn) - dmn * d.r[cc](nn, mm));
+                            } else {
+                                // (v_mm^a - v_nn^a) r^c_nm r^b_mn with v = diag dH (ConventionalInjectionCurrent.jl:4-5).
+                                cd vdc = d.dH[a](mm, mm) - d.dH[a](nn, nn);
+                                val = vdc * d.r[cc](nn, mm) * d.r[b](mm, nn);
+                            }
+                            kern[nn + (size_t)n * (mm + (size_t)n * c)] = val;
+                        }
+                }
+                // accumulate_conventional_response! (ConventionalShiftCurrent.jl:864-882).
+                for (int64_t w = 0; w < nom; ++w)
+                    for (int mm = 0; mm < n; ++mm)
+                        for (int nn = 0; nn < n; ++nn) {
+                            if (!s.mask[nn + (size_t)n * mm]) continue;
+                            double weight = s.fnm[nn + (size_t)n * mm] * s.delta[w + nom * (nn + (size_t)n * mm)];
+                            if (weight == 0.0) continue;
+                            double cw = P * weight;
+                            for (int c = 0; c < nc; ++c)
+                                o[w + nom * c] += cw * kern[nn + (size_t)n * (mm + (size_t)n * c)];
+                        }
+            }
+            o += nom * nc;
+        } else if (q.kind == WNLQG_BERRY_CURVATURE) {
+            for (int c = 0; c < nc; ++c) {
+                int a = q.components[c][0], b = q.components[c][1];
+                cd value(0.0, 0.0);
+                for (int nn = 0; nn < n; ++nn) {
+                    double fn = f[nn];
+                    value += fn * d.F[a][b](nn, nn);
+                    for (int mm = 0; mm < n; ++mm) {
+                        if (mm == nn) continue;
+                        value += (fn - f[mm]) * I1 * d.r[a](nn, mm) * d.r[b](mm, nn);
+                    }
+                }
+                o[c] = cd(value.real(), 0.0);
+            }
+            o += nc;
+        } else if (q.kind == WNLQG_QUANTUM_METRIC) {
+            for (int c = 0; c < nc; ++c) {
+                int a = q.components[c][0], b = q.components[c][1];
+                double value = 0.0;
+                for (int nn = 0; nn < n; ++nn)
+                    for (int mm = 0; mm < n; ++mm) {
+                        if (mm == nn) continue;
+                        value += 0.5 * (f[nn] + f[mm]) * (d.r[a](nn, mm) * d.r[b](mm, nn)).real();
+                    }
+                o[c] = cd(value, 0.0);
+            }
+            o += nc;
+        } else if (q.kind == WNLQG_JERK_CURRENT) {
+            std::vector<cd> B((size_t)n * n * 3, 0.0), A((size_t)n * n * 3, 0.0), C((size_t)n * n * 9, 0.0);
+            for (int a = 0; a < 3; ++a) {
+                if (task.need.dH[a])
+                    for (size_t e = 0; e < (size_t)n * n; ++e) B[e + (size_t)n * n * a] = d.dH[a].v[e];
+                if (task.need.A[a])
+                    for (size_t e = 0; e < (size_t)n * n; ++e) A[e + (size_t)n * n * a] = d.Aint[a].v[e];
+                for (int b = 0; b < 3; ++b)
+                    if (task.need.ddH[a][b])
+                        for (size_t e = 0; e < (size_t)n * n; ++e) C[e + (size_t)n * n * (a + 3 * b)] = d.ddH[a][b].v[e];
+            }
+            jerk_response(n, d.E.data(), B.data(), A.data(), C.data(), nom, t.photon_energies, t.fermi_energy,
+                          t.temperature, t.broadening, t.broadening_type == WNLQG_GAUSSIAN,
+                          t.denominator_regularization > 0 ? t.denominator_regularization : 0.001,
+                          t.transition_window_factor, nc, q.components, o);
+            o += nom * nc;
+        }
+    }
+}
+
+bool build_model(const wnlqg_model_desc *desc, Model &m) {
+    if (!desc || desc->num_orbitals <= 0 || desc->num_r_vectors <= 0) { set_error("invalid model dimensions"); return false; }
+    if (!desc->lattice || !desc->r_vectors || !desc->r_degeneracies || !desc->hamiltonian_r) { set_error("null model array"); return false; }
+    m.nw = (int)desc->num_orbitals;
+    m.nr = (int)desc->num_r_vectors;
+    std::memcpy(m.lattice, desc->lattice, sizeof(m.lattice));
+    m.rvec.assign(desc->r_vectors, desc->r_vectors + 3 * (size_t)m.nr);
+    m.deg.assign(desc->r_degeneracies, desc->r_degeneracies + m.nr);
+    size_t nn = (size_t)m.nw * m.nw;
+    m.H.resize(nn * m.nr);
+    for (size_t e = 0; e < nn * m.nr; ++e) m.H[e] = cd(desc->hamiltonian_r[2 * e], desc->hamiltonian_r[2 * e + 1]);
+    m.has_position = desc->position_r != nullptr;
+    if (m.has_position) {
+        m.A.resize(nn * 3 * m.nr);
+        for (size_t e = 0; e < nn * 3 * m.nr; ++e) m.A[e] = cd(desc->position_r[2 * e], desc->position_r[2 * e + 1]);
+    }
+    for (auto &z : m.H) if (!std::isfinite(z.real()) || !std::isfinite(z.imag())) { set_error("hamiltonian_r contains non-finite values"); return false; }
+    for (int64_t g : m.deg) if (g <= 0) { set_error("r_degeneracies must be positive"); return false; }
+    return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *oracle_last_error(void) { return g_error.c_str(); }
+
+int64_t oracle_value_count(const wnlqg_task_desc *t) {
+    Task task;
+    if (!build_task(t, task)) return -1;
+    return task.value_count;
+}
+
+// Per-point values: k[3*n] -> out[n*value_count] complex (interleaved).
+int oracle_point_values(const wnlqg_model_desc *md, const wnlqg_task_desc *td, const double *k,
+                        int64_t n, int threads, double *out) {
+    Model m; Task task;
+    if (!build_model(md, m) || !build_task(td, task)) return WNLQG_ERR_INVALID_ARGUMENT;
+    int64_t vc = task.value_count;
+    if (threads <= 0) threads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads)
+    for (int64_t i = 0; i < n; ++i) {
+        std::vector<cd> vals((size_t)vc);
+        point_values(m, task, &k[3 * i], vals.data());
+        for (int64_t e = 0; e < vc; ++e) { out[2 * (i * vc + e)] = vals[e].real(); out[2 * (i * vc + e) + 1] = vals[e].imag(); }
+    }
+    return WNLQG_OK;
+}
+
+// Uniform Gamma-centred mesh integral with the reference's 64 deterministic lanes:
+// lane L owns the contiguous indices [fld((L-1)Nk, NL)+1, fld(L Nk, NL)] (1-based), adds
+// value/Nk in k order; lanes are summed in lane order.  Only indices in [k_begin, k_end)
+// are evaluated (a bounded sample when the range is a sub-range); Nk stays the full mesh size.
+int oracle_integrate_mesh(const wnlqg_model_desc *md, const wnlqg_task_desc *td, const int64_t mesh[3],
+                          int64_t k_begin, int64_t k_end, int threads, double *out) {
+    Model m; Task task;
+    if (!build_model(md, m) || !build_task(td, task)) return WNLQG_ERR_INVALID_ARGUMENT;
+    int64_t nk = mesh[0] * mesh[1] * mesh[2];
+    if (nk <= 0 || k_begin < 0 || k_end > nk || k_begin > k_end) { set_error("invalid mesh range"); return WNLQG_ERR_INVALID_ARGUMENT; }
+    int64_t vc = task.value_count;
+    int64_t lanes = std::min<int64_t>(nk, 64);
+    std::vector<std::vector<cd>> lane_sum((size_t)lanes, std::vector<cd>((size_t)vc, cd(0.0, 0.0)));
+    if (threads <= 0) threads = omp_get_max_threads();
+    const double scale = 1.0 / (double)nk;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads)
+    for (int64_t L = 0; L < lanes; ++L) {
+        int64_t first = (L * nk) / lanes;          // 0-based inclusive
+        int64_t last = ((L + 1) * nk) / lanes;      // exclusive
+        first = std::max(first, k_begin);
+        last = std::min(last, k_end);
+        std::vector<cd> vals((size_t)vc);
+        for (int64_t idx = first; idx < last; ++idx) {
+            double k[3];
+            k[0] = (double)(idx % mesh[0]) / (double)mesh[0];
+            k[1] = (double)((idx / mesh[0]) % mesh[1]) / (double)mesh[1];
+            k[2] = (double)(idx / (mesh[0] * mesh[1])) / (double)mesh[2];
+            point_values(m, task, k, vals.data());
+            for (int64_t e = 0; e < vc; ++e) lane_sum[L][e] += scale * vals[e];
+        }
+    }
+    for (int64_t e = 0; e < vc; ++e) {
+        cd acc(0.0, 0.0);
+        for (int64_t L = 0; L < lanes; ++L) acc += lane_sum[L][e];
+        out[2 * e] = acc.real();
+        out[2 * e + 1] = acc.imag();
+    }
+    return WNLQG_OK;
+}
+
+// Band data at one k for tests: energies[nw], U[nw*nw] (canonical, column-major complex),
+// and the Hamiltonian-gauge velocity matrices dH[a] (complex [nw,nw,3]).
+int oracle_kpoint_spectrum(const wnlqg_model_desc *md, const double k[3], double *energies,
+                           double *eigenvectors, double *dh) {
+    Model m;
+    if (!build_model(md, m)) return WNLQG_ERR_INVALID_ARGUMENT;
+    Needs need;
+    for (int a = 0; a < 3; ++a) need.dH[a] = true;
+    KData d;
+    compute_kpoint(m, need, k, 0.001, d);
+    size_t nn = (size_t)m.nw * m.nw;
+    for (int i = 0; i < m.nw; ++i) energies[i] = d.E[i];
+    for (size_t e = 0; e < nn; ++e) { eigenvectors[2 * e] = d.U.v[e].real(); eigenvectors[2 * e + 1] = d.U.v[e].imag(); }
+    if (dh)
+        for (int a = 0; a < 3; ++a)
+            for (size_t e = 0; e < nn; ++e) { dh[2 * (e + nn * a)] = d.dH[a].v[e].real(); dh[2 * (e + nn * a) + 1] = d.dH[a].v[e].imag(); }
+    return WNLQG_OK;
+}
+
+// Hermitian eigensolve of one matrix (upper triangle), canonicalised: for pinning the
+// eigensolver against LAPACK through numpy.
+int oracle_hermitian_eigen(int64_t n, const double *h, double *energies, double *eigenvectors) {
+    Mat a; a.init((int)n);
+    for (int64_t e = 0; e < n * n; ++e) a.v[e] = cd(h[2 * e], h[2 * e + 1]);
+    std::vector<double> ev; Mat U;
+    hermitian_eigen(a, ev, U);
+    canonicalize(U);
+    for (int64_t i = 0; i < n; ++i) energies[i] = ev[i];
+    for (int64_t e = 0; e < n * n; ++e) { eigenvectors[2 * e] = U.v[e].real(); eigenvectors[2 * e + 1] = U.v[e].imag(); }
+    return WNLQG_OK;
+}
+
+// Jerk Eq. 9.20 on prepared Hamiltonian-gauge inputs (the reference's algebra fixture form):
+// B, A complex [n,n,3]; C complex [n,n,3,3]; out complex [nom, ncomp].
+int oracle_jerk_algebra(int64_t n, const double *E, const double *B, const double *A, const double *C,
+                        int64_t nom, const double *omegas, double mu, double T, double width, int gaussian,
+                        double reg, double window, int64_t ncomp, const int32_t *comps, double *out) {
+    std::vector<cd> b((size_t)n * n * 3), a((size_t)n * n * 3), c((size_t)n * n * 9), o((size_t)nom * ncomp);
+    for (size_t e = 0; e < b.size(); ++e) { b[e] = cd(B[2 * e], B[2 * e + 1]); a[e] = cd(A[2 * e], A[2 * e + 1]); }
+    for (size_t e = 0; e < c.size(); ++e) c[e] = cd(C[2 * e], C[2 * e + 1]);
+    jerk_response((int)n, E, b.data(), a.data(), c.data(), nom, omegas, mu, T, width, gaussian != 0, reg, window,
+                  (int)ncomp, reinterpret_cast<const int32_t(*)[4]>(comps), o.data());
+    for (size_t e = 0; e < o.size(); ++e) { out[2 * e] = o[e].real(); out[2 * e + 1] = o[e].imag(); }
+    return WNLQG_OK;
+}
+
+}  // extern "C"

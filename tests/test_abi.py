@@ -1,0 +1,54 @@
+"""The C-ABI library loads and exports every symbol include/wnlqg_b200.h declares (no compute)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from conftest import ROOT
+
+
+def header_functions():
+    text = open(os.path.join(ROOT, "include", "wnlqg_b200.h")).read()
+    return sorted(set(re.findall(r"\b(wnlqg_b200_[a-z_]+)\s*\(", text)))
+
+
+def test_header_and_loader_agree():
+    from wanniernlqg_b200 import _lib
+    assert sorted(_lib.EXPORTED_SYMBOLS) == header_functions()
+
+
+def test_library_exports_all_symbols():
+    from wanniernlqg_b200 import build, _lib
+    build.build()
+    lib = ctypes.CDLL(_lib.LIB_PATH)
+    for name in header_functions():
+        assert hasattr(lib, name), name
+    L = _lib.load()
+    assert L.wnlqg_b200_version().startswith(b"wnlqg-b200")
+
+
+def test_struct_sizes_match_c():
+    """ctypes layouts equal the C layouts (compiled with the same header)."""
+    import subprocess
+    import tempfile
+    from wanniernlqg_b200 import _abi
+    src = r'''
+#include <stdio.h>
+#include <stddef.h>
+#include "wnlqg_b200.h"
+int main(void) {
+  printf("%zu %zu %zu %zu %zu\n", sizeof(wnlqg_model_desc), sizeof(wnlqg_response_request), sizeof(wnlqg_task_desc),
+         offsetof(wnlqg_task_desc, fermi_energy), offsetof(wnlqg_task_desc, precision));
+  return 0;
+}
+'''
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "t.c")
+        open(c, "w").write(src)
+        exe = os.path.join(d, "t")
+        subprocess.run(["/usr/bin/gcc", "-I", os.path.join(ROOT, "include"), c, "-o", exe], check=True)
+        out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()
+    got = [ctypes.sizeof(_abi.ModelDesc), ctypes.sizeof(_abi.ResponseRequest), ctypes.sizeof(_abi.TaskDesc),
+           _abi.TaskDesc.fermi_energy.offset, _abi.TaskDesc.precision.offset]
+    assert [int(x) for x in out] == got

@@ -1,0 +1,141 @@
+"""GPU parity of the FP64 path against the CPU FP64 oracle, through the C ABI.
+
+Tolerance: 1e-10 relative in the max norm over frequencies and components (relative to the
+oracle's max norm), the plain-FP64 bar for this path.
+"""
+import numpy as np
+import pytest
+
+from wanniernlqg_b200 import _abi
+from wanniernlqg_b200.model import reference_workload_model, synthetic_orthogonal_model
+
+pytestmark = pytest.mark.gpu
+RTOL = 1e-10
+
+
+def rel_err(got, ref):
+    scale = np.max(np.abs(ref))
+    return np.max(np.abs(got - ref)) / (scale if scale > 0 else 1.0)
+
+
+@pytest.fixture(scope="module")
+def engine_cls():
+    from wanniernlqg_b200 import build
+    build.build()
+    from wanniernlqg_b200.engine import ResponseEngine
+    return ResponseEngine
+
+
+def nw4_task(kind=_abi.LORENTZIAN, width=0.02, nom=128, **kw):
+    return _abi.TaskArrays([(_abi.SHIFT_CURRENT, ["xyy"]), (_abi.INJECTION_CURRENT, ["xyy"])],
+                           broadening_type=kind, broadening=width, photon_energies=np.linspace(0, 3, nom), **kw)
+
+
+def nw32_task(nom=512, **kw):
+    return _abi.TaskArrays([(_abi.SHIFT_CURRENT, ["xyy"]), (_abi.BERRY_CURVATURE, ["xy"]),
+                            (_abi.QUANTUM_METRIC, ["xx"])],
+                           broadening_type=_abi.LORENTZIAN, broadening=0.01, photon_energies=np.linspace(0, 4, nom), **kw)
+
+
+@pytest.mark.parametrize("name", ["nw4", "nw32"])
+def test_spectrum_matches_oracle(engine_cls, oracle_mod, name):
+    model = reference_workload_model(name)
+    task = nw4_task() if name == "nw4" else nw32_task()
+    rng = np.random.default_rng(11)
+    k = rng.random((24, 3))
+    with engine_cls(model, task) as eng:
+        e, u = eng.spectrum(k)
+    for i in range(k.shape[0]):
+        eo, uo, _ = oracle_mod.kpoint_spectrum(model, k[i])
+        assert np.max(np.abs(e[i] - eo)) < 1e-12 * max(1.0, np.abs(eo).max())
+        # Gauge-invariant comparison of eigenvectors: |<u_gpu|u_oracle>| = 1 column by column.
+        ov = np.abs(np.sum(u[i].conj() * uo, axis=0))
+        assert np.max(np.abs(ov - 1.0)) < 1e-9
+
+
+@pytest.mark.parametrize("name", ["nw4", "nw32"])
+def test_point_values_match_oracle(engine_cls, oracle_mod, name):
+    model = reference_workload_model(name)
+    task = nw4_task() if name == "nw4" else nw32_task()
+    rng = np.random.default_rng(12)
+    k = rng.random((16, 3))
+    with engine_cls(model, task) as eng:
+        got = eng.point_values(k)
+    ref = oracle_mod.point_values(model, task, k)
+    for g, r in zip(task.split(got), task.split(ref)):
+        assert rel_err(g, r) < RTOL
+
+
+@pytest.mark.parametrize("kind", [_abi.LORENTZIAN, _abi.GAUSSIAN])
+def test_nw4_mesh_matches_oracle(engine_cls, oracle_mod, kind):
+    model = reference_workload_model("nw4")
+    task = nw4_task(kind=kind, width=0.02 if kind == _abi.LORENTZIAN else 0.04)
+    mesh = (8, 8, 8)
+    with engine_cls(model, task, max_batch=192) as eng:
+        got = eng.integrate_mesh(mesh)
+    ref = oracle_mod.integrate_mesh(model, task, mesh)
+    for g, r in zip(task.split(got), task.split(ref)):
+        assert rel_err(g, r) < RTOL
+
+
+def test_nw32_mesh_matches_oracle(engine_cls, oracle_mod):
+    model = reference_workload_model("nw32")
+    task = nw32_task(nom=96)
+    mesh = (4, 4, 3)
+    with engine_cls(model, task) as eng:
+        got = eng.integrate_mesh(mesh)
+    ref = oracle_mod.integrate_mesh(model, task, mesh)
+    for g, r in zip(task.split(got), task.split(ref)):
+        assert rel_err(g, r) < RTOL
+
+
+def test_full_shift_tensor_multi_pass(engine_cls, oracle_mod):
+    """All 27 shift components and 27 injection components (several response passes)."""
+    import itertools
+    comps = ["".join(c) for c in itertools.product("xyz", repeat=3)]
+    model = synthetic_orthogonal_model(8, 1, 4, full_position=True)
+    task = _abi.TaskArrays([(_abi.SHIFT_CURRENT, comps), (_abi.INJECTION_CURRENT, comps)],
+                           broadening_type=_abi.GAUSSIAN, broadening=0.05, photon_energies=np.linspace(0.1, 2.5, 24))
+    k = np.random.default_rng(13).random((8, 3))
+    with engine_cls(model, task) as eng:
+        got = eng.point_values(k)
+    ref = oracle_mod.point_values(model, task, k)
+    for g, r in zip(task.split(got), task.split(ref)):
+        assert rel_err(g, r) < RTOL
+
+
+def test_sub_range_and_batches(engine_cls, oracle_mod):
+    model = reference_workload_model("nw4")
+    task = nw4_task(nom=32)
+    mesh = (6, 5, 4)
+    with engine_cls(model, task, max_batch=64) as eng:
+        part = eng.integrate_mesh(mesh, 17, 101)
+        whole = eng.integrate_mesh(mesh)
+    assert rel_err(part, oracle_mod.integrate_mesh(model, task, mesh, 17, 101)) < RTOL
+    assert rel_err(whole, oracle_mod.integrate_mesh(model, task, mesh)) < RTOL
+
+
+def test_run_to_run_bitwise_deterministic(engine_cls):
+    model = reference_workload_model("nw4")
+    task = nw4_task()
+    with engine_cls(model, task, max_batch=128) as eng:
+        a = eng.integrate_mesh((8, 8, 4))
+        b = eng.integrate_mesh((8, 8, 4))
+    assert np.array_equal(a, b)
+
+
+def test_nonfinite_model_rejected(engine_cls):
+    from wanniernlqg_b200._lib import EngineError
+    model = reference_workload_model("nw4")
+    model.hamiltonian_r[0, 0, 3] = np.nan
+    with pytest.raises(EngineError) as ei:
+        engine_cls(model, nw4_task())
+    assert ei.value.status == 3
+
+
+def test_invalid_task_rejected(engine_cls):
+    from wanniernlqg_b200._lib import EngineError
+    model = reference_workload_model("nw4")
+    with pytest.raises(EngineError) as ei:
+        engine_cls(model, nw4_task(width=0.0))
+    assert ei.value.status == 1

@@ -1,0 +1,743 @@
+// wnlqg_b200.cu - C ABI of the B200 k-mesh response engine (declarations in include/wnlqg_b200.h).
+//
+// A model is copied to the device once; a plan compiles a task into Fourier channels, real-space
+// tiles and response passes, and owns the batch workspaces.  Each batch runs
+//   phase_kernel -> fourier_gemm -> jacobi_eigh -> response pass(es)
+// on the plan's stream; mesh evaluation ends with one ordered reduction of the per-CTA partials.
+#include "../../include/wnlqg_b200.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "eigh.cuh"
+#include "fourier.cuh"
+#include "response.cuh"
+
+namespace {
+
+thread_local std::string g_error;
+
+wnlqg_status fail(wnlqg_status st, const std::string &msg) {
+    g_error = msg;
+    return st;
+}
+
+#define WNLQG_CUDA(call)                                                                                  \
+    do {                                                                                                  \
+        cudaError_t err_ = (call);                                                                        \
+        if (err_ != cudaSuccess)                                                                          \
+            return fail(err_ == cudaErrorMemoryAllocation ? WNLQG_ERR_OUT_OF_MEMORY : WNLQG_ERR_CUDA,       \
+                        std::string(#call) + ": " + cudaGetErrorString(err_));                            \
+    } while (0)
+
+enum ChannelOp { CH_H = 0, CH_DH = 1, CH_DDH = 2, CH_A = 3, CH_DA = 4 };
+
+struct Channel {
+    int op;
+    int p;   // dH/ddH: first derivative axis; A/dA: position axis
+    int d;   // ddH: second derivative axis; dA: derivative axis
+};
+
+}  // namespace
+
+struct wnlqg_model {
+    int device = 0;
+    int nw = 0, nr = 0;
+    double lattice[9];
+    std::vector<int64_t> rvec, deg;
+    std::vector<double2> H, A, S;
+    bool has_position = false, has_overlap = false;
+    int64_t *d_rvec = nullptr, *d_deg = nullptr;
+};
+
+struct Pass {
+    RespParams params;   // template; batch-dependent fields set per launch
+    size_t smem = 0;
+    int threads = 0;
+    int grid = 0;
+};
+
+struct wnlqg_plan {
+    wnlqg_model *model = nullptr;
+    wnlqg_task_desc task;
+    std::vector<double> omegas, mus;
+    std::vector<Channel> channels;
+    int ch_H = 0;
+    int ch_dH[3], ch_A[3], ch_ddH[9], ch_dA[9];
+    int nw = 0, nr = 0, C = 0;
+    int64_t nn = 0, vc = 0, max_batch = 0;
+    double2 *d_tiles = nullptr, *d_phase = nullptr, *d_xw = nullptr, *d_U = nullptr, *d_out = nullptr;
+    double2 *d_points = nullptr;
+    double *d_E = nullptr, *d_kpts = nullptr, *d_omegas = nullptr, *d_partials = nullptr;
+    int partial_slots = 0;
+    std::vector<Pass> passes;
+    int eigh_threads = 32;
+    size_t eigh_smem = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<cudaEvent_t> events;
+    size_t timing_batches = 0;
+    int64_t launches = 0;
+    bool timing_valid = false;
+};
+
+namespace {
+
+int find_channel(const std::vector<Channel> &chs, int op, int p, int d) {
+    for (size_t i = 0; i < chs.size(); ++i)
+        if (chs[i].op == op && chs[i].p == p && chs[i].d == d) return (int)i;
+    return -1;
+}
+
+int add_channel(std::vector<Channel> &chs, int op, int p, int d) {
+    if (op == CH_DDH && p > d) std::swap(p, d);
+    int idx = find_channel(chs, op, p, d);
+    if (idx >= 0) return idx;
+    chs.push_back(Channel{op, p, d});
+    return (int)chs.size() - 1;
+}
+
+bool finite_array(const double *a, size_t n) {
+    for (size_t i = 0; i < n; ++i)
+        if (!std::isfinite(a[i])) return false;
+    return true;
+}
+
+double lattice_det(const double *L) {
+    auto e = [&](int i, int j) { return L[i + 3 * j]; };
+    return e(0, 0) * (e(1, 1) * e(2, 2) - e(1, 2) * e(2, 1)) - e(0, 1) * (e(1, 0) * e(2, 2) - e(1, 2) * e(2, 0)) +
+           e(0, 2) * (e(1, 0) * e(2, 1) - e(1, 1) * e(2, 0));
+}
+
+int eigh_block_threads(int nw) {
+    int np = nw + (nw & 1);
+    int blocks = (np / 2) * (np / 2);
+    int t = ((blocks + 31) / 32) * 32;
+    return std::max(32, std::min(256, t));
+}
+
+int response_threads(int nw) {
+    int t = ((nw * nw / 4 + 31) / 32) * 32;
+    return std::max(32, std::min(256, t));
+}
+
+// Build the response passes: group the requested components so that each pass fits the
+// per-pass limits and the shared-memory budget.
+wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
+    const wnlqg_task_desc &t = pl->task;
+    struct Item { int kind; int a, b, c; int64_t out; };
+    std::vector<Item> items;
+    int64_t off = 0;
+    for (int r = 0; r < t.num_responses; ++r) {
+        const wnlqg_response_request &q = t.responses[r];
+        for (int c = 0; c < q.num_components; ++c) {
+            const int32_t *x = q.components[c];
+            if (q.kind == WNLQG_SHIFT_CURRENT || q.kind == WNLQG_INJECTION_CURRENT) {
+                items.push_back({q.kind, x[0], x[1], x[2], off + (int64_t)c * t.num_photon_energies});
+            } else {
+                items.push_back({q.kind, x[0], x[1], 0, off + c});
+            }
+        }
+        if (q.kind == WNLQG_SHIFT_CURRENT || q.kind == WNLQG_INJECTION_CURRENT)
+            off += (int64_t)q.num_components * t.num_photon_energies;
+        else
+            off += q.num_components;
+    }
+    const double vol = lattice_det(pl->model->lattice);
+    const double e3 = WNLQG_ELEMENTARY_CHARGE_C * WNLQG_ELEMENTARY_CHARGE_C * WNLQG_ELEMENTARY_CHARGE_C;
+    const double P_sc = WNLQG_HBAR_EV_S * WNLQG_PI * (-e3) / (2.0 * WNLQG_HBAR_J_S * WNLQG_HBAR_J_S * vol);
+    const double P_ic = -WNLQG_PI * e3 / (WNLQG_HBAR_J_S * WNLQG_HBAR_J_S * vol);
+
+    // Photon-energy window test: exact interval form when consecutive sorted energies are
+    // closer than twice the half-width.
+    std::vector<double> sorted = pl->omegas;
+    std::sort(sorted.begin(), sorted.end());
+    double max_gap = 0.0;
+    for (size_t i = 1; i < sorted.size(); ++i) max_gap = std::max(max_gap, sorted[i] - sorted[i - 1]);
+    const bool gaussian = t.broadening_type == WNLQG_GAUSSIAN;
+    const double width = t.broadening;
+    const double cutoff = width * std::sqrt(200.0);
+    const double thr = t.transition_window_factor * width;
+    const double half = gaussian ? cutoff : thr;
+    const int interval_ok = !sorted.empty() && (sorted.size() == 1 || max_gap < 2.0 * half) ? 1 : 0;
+
+    size_t i = 0;
+    while (i < items.size()) {
+        Pass ps;
+        RespParams &p = ps.params;
+        std::memset(&p, 0, sizeof(p));
+        p.nw = pl->nw;
+        p.ld = pl->nw + 1;
+        for (int a = 0; a < 3; ++a) { p.slot_dH[a] = -1; p.slot_A[a] = -1; p.ch_dH[a] = pl->ch_dH[a]; p.ch_A[a] = pl->ch_A[a]; }
+        for (int a = 0; a < 9; ++a) { p.ch_ddH[a] = pl->ch_ddH[a]; p.ch_dA[a] = pl->ch_dA[a]; }
+        bool needH[3] = {false, false, false}, needA[3] = {false, false, false};
+        std::vector<std::pair<int, int>> gl;
+        auto gindex = [&](int pp, int dd, bool commit) {
+            for (size_t g = 0; g < gl.size(); ++g)
+                if (gl[g].first == pp && gl[g].second == dd) return (int)g;
+            if (!commit) return (int)gl.size();
+            gl.push_back({pp, dd});
+            return (int)gl.size() - 1;
+        };
+        size_t start = i;
+        while (i < items.size()) {
+            const Item &it = items[i];
+            // Tentatively add the item and check limits.
+            bool tH[3], tA[3];
+            std::copy(needH, needH + 3, tH);
+            std::copy(needA, needA + 3, tA);
+            int newg = 0;
+            auto need_r = [&](int a) { tH[a] = true; tA[a] = true; };
+            bool freq = it.kind == WNLQG_SHIFT_CURRENT || it.kind == WNLQG_INJECTION_CURRENT;
+            if (it.kind == WNLQG_SHIFT_CURRENT) {
+                need_r(it.a); need_r(it.b); need_r(it.c);
+                if (gindex(it.c, it.a, false) == (int)gl.size()) ++newg;
+                if (!(it.b == it.c) && gindex(it.b, it.a, false) == (int)gl.size()) ++newg;
+            } else if (it.kind == WNLQG_INJECTION_CURRENT) {
+                tH[it.a] = true; need_r(it.b); need_r(it.c);
+            } else {
+                need_r(it.a); need_r(it.b);
+            }
+            int nslots = (int)gl.size() + newg;
+            for (int a = 0; a < 3; ++a) nslots += (tH[a] ? 1 : 0) + (tA[a] ? 1 : 0);
+            int nfc = p.n_fc + (freq ? 1 : 0);
+            int nsc = p.n_sc + (freq ? 0 : 1);
+            size_t smem = RespSmem::layout(pl->nw, nslots, nfc, 1, sizeof(double2)).total;
+            bool fits = nfc <= RS_MAX_FREQ && nsc <= RS_MAX_SCALAR && (int)gl.size() + newg <= RS_MAX_G && smem <= smem_limit;
+            if (!fits) {
+                if (i == start)
+                    return fail(WNLQG_ERR_UNSUPPORTED, "one response component does not fit the shared-memory budget for nw=" +
+                                                           std::to_string(pl->nw));
+                break;
+            }
+            std::copy(tH, tH + 3, needH);
+            std::copy(tA, tA + 3, needA);
+            if (it.kind == WNLQG_SHIFT_CURRENT) {
+                int g1 = gindex(it.c, it.a, true);
+                int g2 = gindex(it.b, it.a, true);
+                int c = p.n_fc++;
+                p.fc_kind[c] = RS_FC_SHIFT; p.fc_a[c] = it.a; p.fc_b[c] = it.b; p.fc_c[c] = it.c;
+                p.fc_g1[c] = g1; p.fc_g2[c] = g2; p.fc_pref[c] = P_sc; p.fc_out[c] = it.out;
+            } else if (it.kind == WNLQG_INJECTION_CURRENT) {
+                int c = p.n_fc++;
+                p.fc_kind[c] = RS_FC_INJECTION; p.fc_a[c] = it.a; p.fc_b[c] = it.b; p.fc_c[c] = it.c;
+                p.fc_g1[c] = 0; p.fc_g2[c] = 0; p.fc_pref[c] = P_ic; p.fc_out[c] = it.out;
+            } else {
+                int s = p.n_sc++;
+                p.sc_kind[s] = it.kind == WNLQG_BERRY_CURVATURE ? RS_SC_BERRY : RS_SC_METRIC;
+                p.sc_a[s] = it.a; p.sc_b[s] = it.b; p.sc_out[s] = it.out;
+            }
+            ++i;
+        }
+        int slot = 0;
+        for (int a = 0; a < 3; ++a) if (needH[a]) p.slot_dH[a] = slot++;
+        for (int a = 0; a < 3; ++a) if (needA[a]) p.slot_A[a] = slot++;
+        p.n_g = (int)gl.size();
+        for (int g = 0; g < p.n_g; ++g) { p.g_p[g] = gl[g].first; p.g_d[g] = gl[g].second; p.g_slot[g] = slot++; }
+        p.n_slots = slot;
+        p.nom = (int)t.num_photon_energies;
+        p.omegas = pl->d_omegas;
+        p.mu = t.fermi_energy;
+        p.kT = WNLQG_KB_EV_K * t.temperature;
+        p.gaussian = gaussian ? 1 : 0;
+        p.width = width;
+        p.cutoff = cutoff;
+        p.gscale = gaussian ? 1.0 / (std::sqrt(WNLQG_PI) * width) : 0.0;
+        p.thr = thr;
+        p.window_interval = interval_ok;
+        p.om_lo = sorted.empty() ? 0.0 : sorted.front();
+        p.om_hi = sorted.empty() ? 0.0 : sorted.back();
+        p.eta_reg = t.denominator_regularization;
+        p.vc = pl->vc;
+        p.xw_stride = (int64_t)pl->C * pl->nn;
+        ps.smem = RespSmem::layout(pl->nw, p.n_slots, p.n_fc, 1, sizeof(double2)).total;
+        ps.threads = response_threads(pl->nw);
+        if (ps.smem > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute(response_kernel_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps.smem);
+            if (e != cudaSuccess) return fail(WNLQG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+        }
+        int per_sm = 0;
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, response_kernel_f64, ps.threads, ps.smem);
+        if (e != cudaSuccess) return fail(WNLQG_ERR_CUDA, std::string("occupancy query: ") + cudaGetErrorString(e));
+        if (per_sm < 1) return fail(WNLQG_ERR_UNSUPPORTED, "response kernel cannot be resident with its shared memory");
+        ps.grid = sm_count * per_sm;
+        pl->passes.push_back(ps);
+    }
+    return WNLQG_OK;
+}
+
+wnlqg_status record_event(wnlqg_plan *pl, size_t idx) {
+    while (pl->events.size() <= idx) {
+        cudaEvent_t ev;
+        WNLQG_CUDA(cudaEventCreate(&ev));
+        pl->events.push_back(ev);
+    }
+    WNLQG_CUDA(cudaEventRecord(pl->events[idx], pl->stream));
+    return WNLQG_OK;
+}
+
+// One batch: phases, Fourier GEMM, eigensolve.  kpts_device == nullptr selects mesh mode.
+wnlqg_status run_front(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const int64_t *mesh, const double *kpts_device,
+                       size_t ev_base) {
+    const int nr = pl->nr;
+    int64_t total = nb * nr;
+    int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 32);
+    phase_kernel<<<blocks, 256, 0, pl->stream>>>(pl->d_phase, pl->model->d_rvec, pl->model->d_deg, nr, nb, k_begin,
+                                                 mesh ? mesh[0] : 1, mesh ? mesh[1] : 1, mesh ? mesh[2] : 1, kpts_device);
+    int64_t N = (int64_t)pl->C * pl->nn;
+    dim3 grid((unsigned)((N + FG_BN - 1) / FG_BN), (unsigned)((nb + FG_BM - 1) / FG_BM));
+    fourier_gemm_f64<<<grid, 256, 0, pl->stream>>>(pl->d_phase, pl->d_tiles, pl->d_xw, nb, N, nr);
+    wnlqg_status st = record_event(pl, ev_base + 1);
+    if (st != WNLQG_OK) return st;
+    jacobi_eigh_kernel<double><<<(unsigned)nb, pl->eigh_threads, pl->eigh_smem, pl->stream>>>(
+        pl->d_xw + (int64_t)pl->ch_H * pl->nn, N, nb, pl->nw, pl->d_E, pl->d_U, 8.673617379884035e-19);
+    st = record_event(pl, ev_base + 2);
+    if (st != WNLQG_OK) return st;
+    pl->launches += 3;
+    WNLQG_CUDA(cudaGetLastError());
+    return WNLQG_OK;
+}
+
+wnlqg_status run_passes(wnlqg_plan *pl, int64_t nb, int mode, double scale, int64_t point_offset) {
+    for (Pass &ps : pl->passes) {
+        RespParams p = ps.params;
+        p.batch = nb;
+        p.xw = pl->d_xw;
+        p.E = pl->d_E;
+        p.U = pl->d_U;
+        p.mode = mode;
+        p.scale = scale;
+        p.partials = pl->d_partials;
+        p.out_points = pl->d_points;
+        p.point_offset = point_offset;
+        response_kernel_f64<<<ps.grid, ps.threads, ps.smem, pl->stream>>>(p);
+        pl->launches += 1;
+    }
+    WNLQG_CUDA(cudaGetLastError());
+    return WNLQG_OK;
+}
+
+wnlqg_status check_plan(const wnlqg_plan *pl) {
+    if (!pl) return fail(WNLQG_ERR_INVALID_ARGUMENT, "plan is NULL");
+    return WNLQG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *wnlqg_b200_version(void) { return "wnlqg-b200 0.1.0 (sm_100a)"; }
+
+wnlqg_status wnlqg_b200_last_error(char *buffer, size_t capacity) {
+    if (!buffer || capacity == 0) return WNLQG_ERR_INVALID_ARGUMENT;
+    size_t n = std::min(capacity - 1, g_error.size());
+    std::memcpy(buffer, g_error.data(), n);
+    buffer[n] = '\0';
+    return WNLQG_OK;
+}
+
+int32_t wnlqg_b200_device_count(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+wnlqg_status wnlqg_b200_model_create(const wnlqg_model_desc *desc, int32_t device, wnlqg_model **out_model) {
+    if (!desc || !out_model) return fail(WNLQG_ERR_INVALID_ARGUMENT, "NULL argument");
+    *out_model = nullptr;
+    if (desc->num_orbitals <= 0 || desc->num_r_vectors <= 0)
+        return fail(WNLQG_ERR_DIMENSION_MISMATCH, "num_orbitals and num_r_vectors must be positive");
+    if (desc->num_orbitals > 32)
+        return fail(WNLQG_ERR_UNSUPPORTED, "this build supports num_orbitals <= 32");
+    if (!desc->lattice || !desc->r_vectors || !desc->r_degeneracies || !desc->hamiltonian_r)
+        return fail(WNLQG_ERR_INVALID_ARGUMENT, "lattice, r_vectors, r_degeneracies and hamiltonian_r are required");
+    if (desc->overlap_r) return fail(WNLQG_ERR_UNSUPPORTED, "nonorthogonal models (overlap_r) are not supported by this build");
+    const int nw = (int)desc->num_orbitals, nr = (int)desc->num_r_vectors;
+    const size_t nn = (size_t)nw * nw;
+    if (!finite_array(desc->lattice, 9)) return fail(WNLQG_ERR_NONFINITE, "lattice contains non-finite values");
+    if (!finite_array(desc->hamiltonian_r, 2 * nn * nr)) return fail(WNLQG_ERR_NONFINITE, "hamiltonian_r contains non-finite values");
+    if (desc->position_r && !finite_array(desc->position_r, 2 * nn * 3 * nr))
+        return fail(WNLQG_ERR_NONFINITE, "position_r contains non-finite values");
+    for (int r = 0; r < nr; ++r)
+        if (desc->r_degeneracies[r] <= 0) return fail(WNLQG_ERR_INVALID_ARGUMENT, "r_degeneracies must be positive");
+    int ndev = 0;
+    WNLQG_CUDA(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) return fail(WNLQG_ERR_INVALID_ARGUMENT, "device index out of range");
+    WNLQG_CUDA(cudaSetDevice(device));
+    wnlqg_model *m = new wnlqg_model();
+    m->device = device;
+    m->nw = nw;
+    m->nr = nr;
+    std::memcpy(m->lattice, desc->lattice, sizeof(m->lattice));
+    m->rvec.assign(desc->r_vectors, desc->r_vectors + 3 * (size_t)nr);
+    m->deg.assign(desc->r_degeneracies, desc->r_degeneracies + nr);
+    m->H.resize(nn * nr);
+    std::memcpy(m->H.data(), desc->hamiltonian_r, sizeof(double2) * nn * nr);
+    m->has_position = desc->position_r != nullptr;
+    if (m->has_position) {
+        m->A.resize(nn * 3 * nr);
+        std::memcpy(m->A.data(), desc->position_r, sizeof(double2) * nn * 3 * nr);
+    }
+    cudaError_t e1 = cudaMalloc(&m->d_rvec, sizeof(int64_t) * 3 * nr);
+    cudaError_t e2 = cudaMalloc(&m->d_deg, sizeof(int64_t) * nr);
+    if (e1 != cudaSuccess || e2 != cudaSuccess) {
+        cudaFree(m->d_rvec);
+        cudaFree(m->d_deg);
+        delete m;
+        return fail(WNLQG_ERR_OUT_OF_MEMORY, "cudaMalloc failed for the model");
+    }
+    WNLQG_CUDA(cudaMemcpy(m->d_rvec, m->rvec.data(), sizeof(int64_t) * 3 * nr, cudaMemcpyHostToDevice));
+    WNLQG_CUDA(cudaMemcpy(m->d_deg, m->deg.data(), sizeof(int64_t) * nr, cudaMemcpyHostToDevice));
+    *out_model = m;
+    return WNLQG_OK;
+}
+
+wnlqg_status wnlqg_b200_model_destroy(wnlqg_model *model) {
+    if (!model) return WNLQG_OK;
+    cudaSetDevice(model->device);
+    cudaFree(model->d_rvec);
+    cudaFree(model->d_deg);
+    delete model;
+    return WNLQG_OK;
+}
+
+wnlqg_status wnlqg_b200_plan_destroy(wnlqg_plan *pl) {
+    if (!pl) return WNLQG_OK;
+    cudaSetDevice(pl->model->device);
+    if (pl->stream) cudaStreamSynchronize(pl->stream);
+    for (void *ptr : {(void *)pl->d_tiles, (void *)pl->d_phase, (void *)pl->d_xw, (void *)pl->d_U, (void *)pl->d_out,
+                      (void *)pl->d_points, (void *)pl->d_E, (void *)pl->d_kpts, (void *)pl->d_omegas,
+                      (void *)pl->d_partials})
+        if (ptr) cudaFree(ptr);
+    for (cudaEvent_t ev : pl->events) cudaEventDestroy(ev);
+    if (pl->stream) cudaStreamDestroy(pl->stream);
+    delete pl;
+    return WNLQG_OK;
+}
+
+wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *task, int64_t max_batch,
+                                    wnlqg_plan **out_plan) {
+    if (!model || !task || !out_plan) return fail(WNLQG_ERR_INVALID_ARGUMENT, "NULL argument");
+    *out_plan = nullptr;
+    const wnlqg_task_desc &t = *task;
+    if (t.num_responses < 1 || t.num_responses > WNLQG_MAX_RESPONSES)
+        return fail(WNLQG_ERR_INVALID_ARGUMENT, "num_responses must be in 1..8");
+    if (!(t.broadening > 0) || !std::isfinite(t.broadening))
+        return fail(WNLQG_ERR_INVALID_ARGUMENT, "broadening must be finite and positive");
+    if (t.broadening_type != WNLQG_GAUSSIAN && t.broadening_type != WNLQG_LORENTZIAN)
+        return fail(WNLQG_ERR_INVALID_ARGUMENT, "Unknown smearing type");
+    if (!(t.denominator_regularization >= 0) || !std::isfinite(t.denominator_regularization))
+        return fail(WNLQG_ERR_INVALID_ARGUMENT, "denominator_regularization must be finite and >= 0");
+    if (!std::isfinite(t.fermi_energy) || !(t.temperature >= 0) || !std::isfinite(t.temperature))
+        return fail(WNLQG_ERR_INVALID_ARGUMENT, "fermi_energy and temperature must be finite (temperature >= 0)");
+    if (t.num_photon_energies < 0 || (t.num_photon_energies > 0 && !t.photon_energies))
+        return fail(WNLQG_ERR_INVALID_ARGUMENT, "photon energies missing");
+    if (t.num_photon_energies > 0 && !finite_array(t.photon_energies, (size_t)t.num_photon_energies))
+        return fail(WNLQG_ERR_NONFINITE, "photon energies must be finite");
+    if (t.precision != WNLQG_PRECISION_FP64 && t.precision != WNLQG_PRECISION_MIXED)
+        return fail(WNLQG_ERR_INVALID_ARGUMENT, "unknown precision");
+    WNLQG_CUDA(cudaSetDevice(model->device));
+
+    wnlqg_plan *pl = new wnlqg_plan();
+    pl->model = model;
+    pl->task = t;
+    pl->omegas.assign(t.photon_energies, t.photon_energies + t.num_photon_energies);
+    if (t.num_fermi_energies > 0 && t.fermi_energies) pl->mus.assign(t.fermi_energies, t.fermi_energies + t.num_fermi_energies);
+    pl->task.photon_energies = pl->omegas.data();
+    pl->task.fermi_energies = pl->mus.data();
+    pl->nw = model->nw;
+    pl->nr = model->nr;
+    pl->nn = (int64_t)pl->nw * pl->nw;
+    auto bail = [&](wnlqg_status st) { wnlqg_b200_plan_destroy(pl); return st; };
+
+    // Channels required by the requested components.
+    for (int a = 0; a < 3; ++a) { pl->ch_dH[a] = -1; pl->ch_A[a] = -1; }
+    for (int a = 0; a < 9; ++a) { pl->ch_ddH[a] = -1; pl->ch_dA[a] = -1; }
+    std::vector<Channel> &ch = pl->channels;
+    pl->ch_H = add_channel(ch, CH_H, 0, 0);
+    auto need_r = [&](int a) { pl->ch_dH[a] = add_channel(ch, CH_DH, a, 0); pl->ch_A[a] = add_channel(ch, CH_A, a, 0); };
+    int64_t vc = 0;
+    for (int r = 0; r < t.num_responses; ++r) {
+        const wnlqg_response_request &q = t.responses[r];
+        if (q.num_components < 1 || q.num_components > WNLQG_MAX_COMPONENTS)
+            return bail(fail(WNLQG_ERR_INVALID_ARGUMENT, "num_components must be in 1..81"));
+        for (int c = 0; c < q.num_components; ++c) {
+            const int32_t *x = q.components[c];
+            for (int i = 0; i < 4; ++i)
+                if (x[i] < 0 || x[i] > 2) return bail(fail(WNLQG_ERR_INVALID_ARGUMENT, "component axis out of range"));
+            int a = x[0], b = x[1], cc = x[2];
+            switch (q.kind) {
+            case WNLQG_SHIFT_CURRENT: {
+                need_r(a); need_r(b); need_r(cc);
+                for (auto pd : {std::make_pair(cc, a), std::make_pair(b, a)}) {
+                    int pp = pd.first, dd = pd.second;
+                    pl->ch_dA[pp * 3 + dd] = add_channel(ch, CH_DA, pp, dd);
+                    int hidx = add_channel(ch, CH_DDH, pp, dd);
+                    pl->ch_ddH[pp * 3 + dd] = hidx;
+                    pl->ch_ddH[dd * 3 + pp] = hidx;
+                }
+                break;
+            }
+            case WNLQG_INJECTION_CURRENT:
+                pl->ch_dH[a] = add_channel(ch, CH_DH, a, 0);
+                need_r(b); need_r(cc);
+                break;
+            case WNLQG_BERRY_CURVATURE:
+                need_r(a); need_r(b);
+                pl->ch_dA[b * 3 + a] = add_channel(ch, CH_DA, b, a);
+                pl->ch_dA[a * 3 + b] = add_channel(ch, CH_DA, a, b);
+                break;
+            case WNLQG_QUANTUM_METRIC:
+                need_r(a); need_r(b);
+                break;
+            default:
+                return bail(fail(WNLQG_ERR_UNSUPPORTED, "response kind not supported by this build"));
+            }
+        }
+        if (q.kind == WNLQG_SHIFT_CURRENT || q.kind == WNLQG_INJECTION_CURRENT) {
+            if (t.num_photon_energies < 1) return bail(fail(WNLQG_ERR_INVALID_ARGUMENT, "photon energies required"));
+            vc += (int64_t)q.num_components * t.num_photon_energies;
+        } else {
+            vc += q.num_components;
+        }
+    }
+    pl->vc = vc;
+    pl->C = (int)ch.size();
+
+    // Real-space tiles T[R][c][i + nw j] (prepare_hamiltonian_real_space!,
+    // HamiltonianMatrixElements.jl:92-177; prepare_position_real_space!, PositionMatrixElements.jl:8-84;
+    // Convention II displacements).
+    const int nw = pl->nw, nr = pl->nr;
+    const int64_t nn = pl->nn;
+    std::vector<double2> tiles((size_t)nr * pl->C * nn);
+    for (int r = 0; r < nr; ++r) {
+        double rc[3];
+        const int64_t *rv = &model->rvec[3 * (size_t)r];
+        for (int j = 0; j < 3; ++j)
+            rc[j] = (double)rv[0] * model->lattice[0 + 3 * j] + (double)rv[1] * model->lattice[1 + 3 * j] +
+                    (double)rv[2] * model->lattice[2 + 3 * j];
+        for (int c = 0; c < pl->C; ++c) {
+            const Channel &cc = ch[c];
+            double2 *dst = &tiles[((size_t)r * pl->C + c) * nn];
+            for (int64_t e = 0; e < nn; ++e) {
+                double2 h = model->H[(size_t)r * nn + e];
+                double2 v = make_double2(0.0, 0.0);
+                switch (cc.op) {
+                case CH_H: v = h; break;
+                case CH_DH: v = cmuli(cscale(h, rc[cc.p])); break;
+                case CH_DDH: v = cscale(h, -rc[cc.p] * rc[cc.d]); break;
+                case CH_A:
+                    if (model->has_position) v = model->A[((size_t)r * 3 + cc.p) * nn + e];
+                    break;
+                case CH_DA:
+                    if (model->has_position) v = cmuli(cscale(model->A[((size_t)r * 3 + cc.p) * nn + e], rc[cc.d]));
+                    break;
+                }
+                dst[e] = v;
+            }
+        }
+    }
+
+    int sm_count = 148;
+    int dev = model->device;
+    cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev);
+    int smem_optin = 0;
+    cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (smem_optin <= 0) smem_optin = 48 * 1024;
+
+    if (max_batch <= 0) {
+        int64_t per_k = (int64_t)pl->C * nn * 16 + (int64_t)nr * 16 + nn * 16 + nw * 8;
+        max_batch = std::max<int64_t>(256, std::min<int64_t>(1 << 20, ((int64_t)1 << 30) / per_k));
+        max_batch = (max_batch / 64) * 64;
+    }
+    pl->max_batch = max_batch;
+    WNLQG_CUDA(cudaStreamCreateWithFlags(&pl->stream, cudaStreamNonBlocking));
+    auto alloc = [&](void **ptr, size_t bytes) -> wnlqg_status {
+        cudaError_t e = cudaMalloc(ptr, std::max<size_t>(bytes, 16));
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(WNLQG_ERR_OUT_OF_MEMORY, std::string("cudaMalloc of ") + std::to_string(bytes) + " bytes failed");
+        }
+        return WNLQG_OK;
+    };
+    wnlqg_status st;
+    if ((st = alloc((void **)&pl->d_tiles, tiles.size() * sizeof(double2))) != WNLQG_OK) return bail(st);
+    if ((st = alloc((void **)&pl->d_phase, (size_t)max_batch * nr * sizeof(double2))) != WNLQG_OK) return bail(st);
+    if ((st = alloc((void **)&pl->d_xw, (size_t)max_batch * pl->C * nn * sizeof(double2))) != WNLQG_OK) return bail(st);
+    if ((st = alloc((void **)&pl->d_U, (size_t)max_batch * nn * sizeof(double2))) != WNLQG_OK) return bail(st);
+    if ((st = alloc((void **)&pl->d_E, (size_t)max_batch * nw * sizeof(double))) != WNLQG_OK) return bail(st);
+    if ((st = alloc((void **)&pl->d_kpts, (size_t)max_batch * 3 * sizeof(double))) != WNLQG_OK) return bail(st);
+    if ((st = alloc((void **)&pl->d_points, (size_t)max_batch * vc * sizeof(double2))) != WNLQG_OK) return bail(st);
+    if ((st = alloc((void **)&pl->d_out, (size_t)vc * sizeof(double2))) != WNLQG_OK) return bail(st);
+    if ((st = alloc((void **)&pl->d_omegas, std::max<size_t>(1, pl->omegas.size()) * sizeof(double))) != WNLQG_OK) return bail(st);
+    WNLQG_CUDA(cudaMemcpy(pl->d_tiles, tiles.data(), tiles.size() * sizeof(double2), cudaMemcpyHostToDevice));
+    if (!pl->omegas.empty())
+        WNLQG_CUDA(cudaMemcpy(pl->d_omegas, pl->omegas.data(), pl->omegas.size() * sizeof(double), cudaMemcpyHostToDevice));
+
+    pl->eigh_threads = eigh_block_threads(nw);
+    pl->eigh_smem = EighSmem::bytes(nw, sizeof(double2));
+    if (pl->eigh_smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(jacobi_eigh_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)pl->eigh_smem);
+        if (e != cudaSuccess) return bail(fail(WNLQG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e)));
+    }
+    if ((st = build_passes(pl, sm_count, (size_t)smem_optin)) != WNLQG_OK) return bail(st);
+    for (const Pass &ps : pl->passes) pl->partial_slots = std::max(pl->partial_slots, ps.grid);
+    if ((st = alloc((void **)&pl->d_partials, (size_t)pl->partial_slots * vc * 4 * sizeof(double))) != WNLQG_OK)
+        return bail(st);
+    *out_plan = pl;
+    return WNLQG_OK;
+}
+
+int64_t wnlqg_b200_plan_value_count(const wnlqg_plan *plan) { return plan ? plan->vc : -1; }
+
+wnlqg_status wnlqg_b200_eval_mesh_device(wnlqg_plan *pl, const int64_t mesh[3], int64_t k_begin, int64_t k_end,
+                                         double *out_device, void *stream) {
+    wnlqg_status st = check_plan(pl);
+    if (st != WNLQG_OK) return st;
+    if (!mesh || !out_device) return fail(WNLQG_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (mesh[0] <= 0 || mesh[1] <= 0 || mesh[2] <= 0) return fail(WNLQG_ERR_INVALID_ARGUMENT, "mesh counts must be positive");
+    const int64_t nk = mesh[0] * mesh[1] * mesh[2];
+    if (k_begin < 0 || k_end > nk || k_begin > k_end) return fail(WNLQG_ERR_INVALID_ARGUMENT, "k range outside the mesh");
+    WNLQG_CUDA(cudaSetDevice(pl->model->device));
+    cudaStream_t user = static_cast<cudaStream_t>(stream);
+    // Order the plan stream after the caller's stream.
+    if ((st = record_event(pl, 0)) != WNLQG_OK) return st;
+    if (user) {
+        cudaEvent_t ev;
+        WNLQG_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        WNLQG_CUDA(cudaEventRecord(ev, user));
+        WNLQG_CUDA(cudaStreamWaitEvent(pl->stream, ev, 0));
+        cudaEventDestroy(ev);
+    }
+    pl->launches = 0;
+    WNLQG_CUDA(cudaMemsetAsync(pl->d_partials, 0, (size_t)pl->partial_slots * pl->vc * 4 * sizeof(double), pl->stream));
+    const double scale = 1.0 / (double)nk;
+    size_t nbatch = 0;
+    for (int64_t s = k_begin; s < k_end; s += pl->max_batch, ++nbatch) {
+        int64_t nb = std::min(pl->max_batch, k_end - s);
+        size_t base = 1 + 3 * nbatch;
+        if ((st = record_event(pl, base)) != WNLQG_OK) return st;
+        if ((st = run_front(pl, nb, s, mesh, nullptr, base)) != WNLQG_OK) return st;
+        if ((st = run_passes(pl, nb, 0, scale, 0)) != WNLQG_OK) return st;
+    }
+    // Events: [0] start, per batch b: [1+3b] batch start, [2+3b] after Fourier, [3+3b] after eigh,
+    // next batch start (or the final event) closes the response stage.
+    size_t final_ev = 1 + 3 * nbatch;
+    if ((st = record_event(pl, final_ev)) != WNLQG_OK) return st;
+    reduce_partials_kernel<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((pl->vc + 255) / 256, 1024)), 256, 0,
+                             pl->stream>>>(pl->d_partials, pl->partial_slots, pl->vc, reinterpret_cast<double2 *>(out_device));
+    pl->launches += 1;
+    WNLQG_CUDA(cudaGetLastError());
+    if ((st = record_event(pl, final_ev + 1)) != WNLQG_OK) return st;
+    pl->timing_valid = false;
+    if (user) {
+        cudaEvent_t ev;
+        WNLQG_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        WNLQG_CUDA(cudaEventRecord(ev, pl->stream));
+        WNLQG_CUDA(cudaStreamWaitEvent(user, ev, 0));
+        cudaEventDestroy(ev);
+    }
+    pl->timing_valid = true;
+    pl->timing_batches = nbatch;
+    return WNLQG_OK;
+}
+
+wnlqg_status wnlqg_b200_eval_mesh(wnlqg_plan *pl, const int64_t mesh[3], int64_t k_begin, int64_t k_end, double *out) {
+    wnlqg_status st = check_plan(pl);
+    if (st != WNLQG_OK) return st;
+    if (!out) return fail(WNLQG_ERR_INVALID_ARGUMENT, "NULL output");
+    if ((st = wnlqg_b200_eval_mesh_device(pl, mesh, k_begin, k_end, reinterpret_cast<double *>(pl->d_out), nullptr)) != WNLQG_OK)
+        return st;
+    WNLQG_CUDA(cudaMemcpyAsync(out, pl->d_out, (size_t)pl->vc * sizeof(double2), cudaMemcpyDeviceToHost, pl->stream));
+    WNLQG_CUDA(cudaStreamSynchronize(pl->stream));
+    for (int64_t v = 0; v < 2 * pl->vc; ++v)
+        if (!std::isfinite(out[v])) return fail(WNLQG_ERR_NONFINITE, "response contains non-finite values");
+    return WNLQG_OK;
+}
+
+wnlqg_status wnlqg_b200_eval_points(wnlqg_plan *pl, const double *kpoints, int64_t n, double *out) {
+    wnlqg_status st = check_plan(pl);
+    if (st != WNLQG_OK) return st;
+    if (n < 0 || (n > 0 && (!kpoints || !out))) return fail(WNLQG_ERR_INVALID_ARGUMENT, "invalid points");
+    if (!finite_array(kpoints, 3 * (size_t)n)) return fail(WNLQG_ERR_NONFINITE, "k-points must be finite");
+    WNLQG_CUDA(cudaSetDevice(pl->model->device));
+    pl->launches = 0;
+    for (int64_t s = 0; s < n; s += pl->max_batch) {
+        int64_t nb = std::min(pl->max_batch, n - s);
+        WNLQG_CUDA(cudaMemcpyAsync(pl->d_kpts, kpoints + 3 * s, (size_t)nb * 3 * sizeof(double), cudaMemcpyHostToDevice,
+                                   pl->stream));
+        if ((st = run_front(pl, nb, 0, nullptr, pl->d_kpts, 1)) != WNLQG_OK) return st;
+        if ((st = run_passes(pl, nb, 1, 1.0, 0)) != WNLQG_OK) return st;
+        WNLQG_CUDA(cudaMemcpyAsync(out + 2 * s * pl->vc, pl->d_points, (size_t)nb * pl->vc * sizeof(double2),
+                                   cudaMemcpyDeviceToHost, pl->stream));
+    }
+    WNLQG_CUDA(cudaStreamSynchronize(pl->stream));
+    pl->timing_valid = false;
+    for (int64_t v = 0; v < 2 * n * pl->vc; ++v)
+        if (!std::isfinite(out[v])) return fail(WNLQG_ERR_NONFINITE, "response contains non-finite values");
+    return WNLQG_OK;
+}
+
+wnlqg_status wnlqg_b200_eval_spectrum(wnlqg_plan *pl, const double *kpoints, int64_t n, double *energies,
+                                      double *eigenvectors) {
+    wnlqg_status st = check_plan(pl);
+    if (st != WNLQG_OK) return st;
+    if (n < 0 || (n > 0 && (!kpoints || !energies))) return fail(WNLQG_ERR_INVALID_ARGUMENT, "invalid points");
+    if (!finite_array(kpoints, 3 * (size_t)n)) return fail(WNLQG_ERR_NONFINITE, "k-points must be finite");
+    WNLQG_CUDA(cudaSetDevice(pl->model->device));
+    for (int64_t s = 0; s < n; s += pl->max_batch) {
+        int64_t nb = std::min(pl->max_batch, n - s);
+        WNLQG_CUDA(cudaMemcpyAsync(pl->d_kpts, kpoints + 3 * s, (size_t)nb * 3 * sizeof(double), cudaMemcpyHostToDevice,
+                                   pl->stream));
+        if ((st = run_front(pl, nb, 0, nullptr, pl->d_kpts, 1)) != WNLQG_OK) return st;
+        WNLQG_CUDA(cudaMemcpyAsync(energies + s * pl->nw, pl->d_E, (size_t)nb * pl->nw * sizeof(double),
+                                   cudaMemcpyDeviceToHost, pl->stream));
+        if (eigenvectors)
+            WNLQG_CUDA(cudaMemcpyAsync(eigenvectors + 2 * s * pl->nn, pl->d_U, (size_t)nb * pl->nn * sizeof(double2),
+                                       cudaMemcpyDeviceToHost, pl->stream));
+    }
+    WNLQG_CUDA(cudaStreamSynchronize(pl->stream));
+    pl->timing_valid = false;
+    return WNLQG_OK;
+}
+
+wnlqg_status wnlqg_b200_plan_last_timing(const wnlqg_plan *pl_const, double *fourier_ms, double *eigen_ms,
+                                         double *response_ms, double *total_ms) {
+    wnlqg_plan *pl = const_cast<wnlqg_plan *>(pl_const);
+    wnlqg_status st = check_plan(pl);
+    if (st != WNLQG_OK) return st;
+    if (!pl->timing_valid) return fail(WNLQG_ERR_INVALID_ARGUMENT, "no mesh evaluation to report");
+    WNLQG_CUDA(cudaSetDevice(pl->model->device));
+    WNLQG_CUDA(cudaStreamSynchronize(pl->stream));
+    size_t nbatch = pl->timing_batches;
+    double f = 0, e = 0, r = 0;
+    for (size_t b = 0; b < nbatch; ++b) {
+        float ms = 0;
+        size_t base = 1 + 3 * b;
+        WNLQG_CUDA(cudaEventElapsedTime(&ms, pl->events[base], pl->events[base + 1]));
+        f += ms;
+        WNLQG_CUDA(cudaEventElapsedTime(&ms, pl->events[base + 1], pl->events[base + 2]));
+        e += ms;
+        WNLQG_CUDA(cudaEventElapsedTime(&ms, pl->events[base + 2], pl->events[base + 3]));
+        r += ms;
+    }
+    float tot = 0;
+    WNLQG_CUDA(cudaEventElapsedTime(&tot, pl->events[0], pl->events[1 + 3 * nbatch + 1]));
+    if (fourier_ms) *fourier_ms = f;
+    if (eigen_ms) *eigen_ms = e;
+    if (response_ms) *response_ms = r;
+    if (total_ms) *total_ms = tot;
+    return WNLQG_OK;
+}
+
+int64_t wnlqg_b200_plan_last_launch_count(const wnlqg_plan *plan) { return plan ? plan->launches : -1; }
+
+}  // extern "C"

@@ -1,0 +1,111 @@
+"""Host side of the B200 engine: a device-resident model plus a compiled task (plan).
+
+``ResponseEngine`` is the drop-in for the reference's per-worker k loop: ``integrate_mesh``
+returns the lane tensor sum_k value(k)/Nk over a range of the Gamma-centred mesh (the
+contract of consume_point!, Runtime/Execution/IntegralDriver.jl:820-874), ``point_values`` is
+the batched ResponsePointEvaluator / ResponseNodeEvaluator
+(Runtime/Execution/ResponsePointEvaluation.jl:8-64), and ``spectrum`` exposes compute_spectrum!
+(MatrixElements/Interpolated/HamiltonianMatrixElements.jl:279-300).
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _abi, _lib
+from .model import TightBindingModel
+
+
+class ResponseEngine:
+    def __init__(self, model: TightBindingModel, task: _abi.TaskArrays, *, device: int = 0, max_batch: int = 0):
+        L = _lib.load()
+        self._L = L
+        self.model = model
+        self.task = task
+        self._marrays = _abi.ModelArrays(model)
+        self._model = ctypes.c_void_p()
+        self._plan = ctypes.c_void_p()
+        _lib.check(L.wnlqg_b200_model_create(ctypes.byref(self._marrays.desc), device, ctypes.byref(self._model)))
+        try:
+            _lib.check(L.wnlqg_b200_plan_create(self._model, ctypes.byref(task.desc), max_batch,
+                                                ctypes.byref(self._plan)))
+        except Exception:
+            L.wnlqg_b200_model_destroy(self._model)
+            self._model = ctypes.c_void_p()
+            raise
+        self.value_count = int(L.wnlqg_b200_plan_value_count(self._plan))
+
+    # -- lifetime ------------------------------------------------------------------------
+    def close(self) -> None:
+        if self._plan:
+            self._L.wnlqg_b200_plan_destroy(self._plan)
+            self._plan = ctypes.c_void_p()
+        if self._model:
+            self._L.wnlqg_b200_model_destroy(self._model)
+            self._model = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- evaluation ----------------------------------------------------------------------
+    def integrate_mesh(self, mesh: Sequence[int], k_begin: int = 0, k_end: Optional[int] = None) -> np.ndarray:
+        """sum over mesh indices [k_begin, k_end) of value(k)/Nk, complex [value_count]."""
+        mesh_a = np.ascontiguousarray(np.asarray(mesh, dtype=np.int64))
+        if mesh_a.shape != (3,):
+            raise ValueError("mesh must have three counts")
+        if k_end is None:
+            k_end = int(np.prod(mesh_a))
+        out = np.zeros(self.value_count, dtype=np.complex128)
+        _lib.check(self._L.wnlqg_b200_eval_mesh(self._plan, mesh_a.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                                                int(k_begin), int(k_end),
+                                                out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return out
+
+    def integrate_mesh_device(self, mesh: Sequence[int], k_begin: int, k_end: int, out_device_ptr: int,
+                              stream_ptr: int = 0) -> None:
+        """Asynchronous variant writing value_count complex values to a device pointer."""
+        mesh_a = np.ascontiguousarray(np.asarray(mesh, dtype=np.int64))
+        _lib.check(self._L.wnlqg_b200_eval_mesh_device(self._plan,
+                                                       mesh_a.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                                                       int(k_begin), int(k_end), ctypes.c_void_p(out_device_ptr),
+                                                       ctypes.c_void_p(stream_ptr)))
+
+    def point_values(self, kpoints) -> np.ndarray:
+        """Per-point values at fractional k-points [n, 3] -> complex [n, value_count]."""
+        k = np.ascontiguousarray(np.asarray(kpoints, dtype=np.float64).reshape(-1, 3))
+        out = np.zeros((k.shape[0], self.value_count), dtype=np.complex128)
+        _lib.check(self._L.wnlqg_b200_eval_points(self._plan, k.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                                  k.shape[0], out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return out
+
+    def spectrum(self, kpoints):
+        """(energies [n, nw], canonical eigenvectors [n, nw, nw]) at fractional k-points."""
+        k = np.ascontiguousarray(np.asarray(kpoints, dtype=np.float64).reshape(-1, 3))
+        nw = self.model.num_orbitals
+        e = np.zeros((k.shape[0], nw))
+        # Column-major per k: store as [n, col, row] and transpose.
+        u = np.zeros((k.shape[0], nw, nw), dtype=np.complex128)
+        _lib.check(self._L.wnlqg_b200_eval_spectrum(self._plan, k.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                                    k.shape[0], e.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                                    u.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return e, np.ascontiguousarray(u.transpose(0, 2, 1))
+
+    def last_timing(self):
+        """Device milliseconds (fourier, eigen, response, total) of the last mesh evaluation."""
+        vals = [ctypes.c_double() for _ in range(4)]
+        _lib.check(self._L.wnlqg_b200_plan_last_timing(self._plan, *[ctypes.byref(v) for v in vals]))
+        return tuple(v.value for v in vals)
+
+    def last_launch_count(self) -> int:
+        return int(self._L.wnlqg_b200_plan_last_launch_count(self._plan))
