@@ -165,6 +165,12 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
     const double half = gaussian ? cutoff : thr;
     const int interval_ok = !sorted.empty() && (sorted.size() == 1 || max_gap < 2.0 * half) ? 1 : 0;
 
+    // The dynamic shared-memory ceiling is a per-function attribute: raise it once to the device
+    // maximum so that passes of different sizes can all launch.
+    {
+        cudaError_t e = cudaFuncSetAttribute(response_kernel_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_limit);
+        if (e != cudaSuccess) return fail(WNLQG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+    }
     size_t i = 0;
     while (i < items.size()) {
         Pass ps;
@@ -256,10 +262,6 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
         p.xw_stride = (int64_t)pl->C * pl->nn;
         ps.smem = RespSmem::layout(pl->nw, p.n_slots, p.n_fc, 1, sizeof(double2)).total;
         ps.threads = response_threads(pl->nw);
-        if (ps.smem > 48 * 1024) {
-            cudaError_t e = cudaFuncSetAttribute(response_kernel_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps.smem);
-            if (e != cudaSuccess) return fail(WNLQG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
-        }
         int per_sm = 0;
         cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, response_kernel_f64, ps.threads, ps.smem);
         if (e != cudaSuccess) return fail(WNLQG_ERR_CUDA, std::string("occupancy query: ") + cudaGetErrorString(e));
