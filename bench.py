@@ -1,0 +1,310 @@
+#!/usr/bin/env python
+"""Throughput of the WannierNLQG k-mesh response hot path on B200s, in k-points/s.
+
+Workload (one GPU): the nw=32 synthetic orthogonal Wannier model (|R_i| <= 4, 729 R-vectors,
+full off-diagonal position operator, seed 0) evaluated on its 256^3 Gamma-centred mesh:
+Berry curvature Omega^z (occupied sum), quantum metric g^xx (band sum) and the shift current
+sigma^xyy(omega) on 512 photon energies in [0, 4] eV with Lorentzian eta = 0.01 eV, mu = 0, T = 0.
+A step is one contiguous block of `--batch` mesh points pushed through the whole path
+(phases -> Fourier -> eigensolve -> integrands -> deterministic reduction).  With N ranks each rank
+takes its own blocks (weak scaling, no data-path collective); the lane tensors are combined
+once at the end with one NCCL all-reduce outside the timed region.
+
+`--impl reference` times the reference algorithm's CPU restatement (the FP64 oracle, all host
+threads) on a bounded sample of the same mesh.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from wanniernlqg_b200 import _abi  # noqa: E402
+from wanniernlqg_b200.model import reference_workload_model  # noqa: E402
+
+METRIC = "k-points/s"
+WORKLOAD = "nw32_R729_fullA_mesh256^3_sigma_xyy_512w_OmegaZ_gxx"
+MESH = (256, 256, 256)
+
+
+def make_task(precision: int) -> _abi.TaskArrays:
+    return _abi.TaskArrays([(_abi.SHIFT_CURRENT, ["xyy"]), (_abi.BERRY_CURVATURE, ["xy"]),
+                            (_abi.QUANTUM_METRIC, ["xx"])],
+                           broadening_type=_abi.LORENTZIAN, broadening=0.01,
+                           photon_energies=np.linspace(0.0, 4.0, 512), fermi_energy=0.0, temperature=0.0,
+                           precision=precision)
+
+
+def mesh_kpoints(start: int, count: int) -> np.ndarray:
+    idx = np.arange(start, start + count, dtype=np.int64)
+    n1, n2, n3 = MESH
+    return np.stack([(idx % n1) / n1, ((idx // n1) % n2) / n2, (idx // (n1 * n2)) / n3], axis=1)
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device_index = device_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            p = json.load(fh)
+        return p, "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+def cpu_baseline_run(model, task, target_seconds: float, threads: int):
+    """Time the FP64 oracle on a bounded sample of the workload mesh (contiguous points from the
+    start of a lane)."""
+    from oracle import oracle
+    oracle.build()
+    probe = max(4, threads)
+    start = 1_000_003
+    t0 = time.perf_counter()
+    oracle.integrate_mesh(model, task, MESH, start, start + probe, threads=threads)
+    per_point = (time.perf_counter() - t0) / probe
+    n = int(max(probe, min(200_000, target_seconds / max(per_point, 1e-9))))
+    t0 = time.perf_counter()
+    oracle.integrate_mesh(model, task, MESH, start, start + n, threads=threads)
+    dt = time.perf_counter() - t0
+    return n / dt, n, dt
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    model = reference_workload_model("nw32")
+    task = make_task(_abi.PRECISION_FP64)
+    threads = os.cpu_count() or 1
+    from oracle import oracle
+    oracle.build()
+    # Calibrate a step of about 4 s of CPU work.
+    probe = max(4, threads)
+    t0 = time.perf_counter()
+    oracle.integrate_mesh(model, task, MESH, 0, probe, threads=threads)
+    per_point = (time.perf_counter() - t0) / probe
+    n = int(max(probe, min(200_000, 4.0 / max(per_point, 1e-9))))
+    for w in range(args.warmup):
+        oracle.integrate_mesh(model, task, MESH, w * n, (w + 1) * n, threads=threads)
+    t0 = time.perf_counter()
+    for s in range(args.steps):
+        b = (args.warmup + s) * n
+        oracle.integrate_mesh(model, task, MESH, b, b + n, threads=threads)
+    dt = time.perf_counter() - t0
+    value = n * args.steps / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded model; no dataset)",
+        "config": {"workload": WORKLOAD, "k_per_step": n, "mesh": list(MESH)},
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "port",
+                         "sample": f"{n} contiguous mesh points per step, oracle FP64 with {threads} OpenMP threads"},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--batch", type=int, default=65536, help="mesh points per step and rank")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample length")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    from wanniernlqg_b200 import build
+    from wanniernlqg_b200.engine import ResponseEngine
+    build.build()
+    precision = _abi.PRECISION_FP64 if args.precision == "fp64" else _abi.PRECISION_MIXED
+    model = reference_workload_model("nw32")
+    task = make_task(precision)
+    nk = int(np.prod(MESH))
+    batch = args.batch
+    engine = ResponseEngine(model, task, device=local_rank)
+    vc = engine.value_count
+    out = torch.zeros(2 * vc, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def block(step):
+        b = ((step * world + rank) * batch) % nk
+        return b, min(nk, b + batch)
+
+    for s in range(args.warmup):
+        kb, ke = block(s)
+        engine.integrate_mesh_device(MESH, kb, ke, out.data_ptr(), stream.cuda_stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    time.sleep(0.4)
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    launches = 0
+    for s in range(args.steps):
+        kb, ke = block(args.warmup + s)
+        engine.integrate_mesh_device(MESH, kb, ke, out.data_ptr(), stream.cuda_stream)
+        launches += engine.last_launch_count()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    elapsed_ms = ev0.elapsed_time(ev1)
+    fourier_ms, eigen_ms, response_ms, total_ms = engine.last_timing()
+    if dist:
+        t = torch.tensor([elapsed_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+        dist.barrier()
+    value = world * batch * args.steps / (elapsed_ms / 1e3)
+
+    # End to end through the public host API: host k-points (H2D) -> weighted mesh sum -> host
+    # result (D2H), synchronous, wall clock.
+    e2e_steps = max(1, min(args.steps, 3))
+    kb, _ = block(args.warmup + args.steps)
+    kpts = mesh_kpoints(kb, batch)
+    w = np.full(batch, 1.0 / nk)
+    engine.weighted_sum(kpts, w)
+    t0 = time.perf_counter()
+    for s in range(e2e_steps):
+        engine.weighted_sum(kpts, w)
+    e2e_dt = (time.perf_counter() - t0) / e2e_steps
+    e2e_value = world * batch / e2e_dt
+
+    # Roofline of the dominant kernel (Fourier stage) from the last step's CUDA events.
+    peaks, peak_src = load_peaks()
+    launches_per_step = launches // max(1, args.steps)
+    C = fourier_channels(task)
+    flop_per_k = 8.0 * model.num_r_vectors * model.num_orbitals ** 2 * C
+    fourier_tflops = flop_per_k * batch / (fourier_ms / 1e3) / 1e12 if fourier_ms > 0 else None
+    fp64_peak = 37.0   # nominal B200 dense FP64 TFLOP/s; no measured FP64 peak on this pool
+    roofline = {
+        "bound": "fp64" if precision == _abi.PRECISION_FP64 else "tensor",
+        "kernel": "fourier (phase table + complex GEMM)",
+        "achieved": fourier_tflops, "peak": fp64_peak, "unit": "TFLOP/s",
+        "frac": (fourier_tflops / fp64_peak) if fourier_tflops else None,
+        "peak_source": "nominal B200 FP64 (not in the measured peaks file)",
+        "traffic": None, "launches_per_step": launches_per_step,
+        "stage_ms_last_step": {"fourier": fourier_ms, "eigen": eigen_ms, "response": response_ms, "total": total_ms},
+        "flop_per_k": flop_per_k,
+    }
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if precision == _abi.PRECISION_FP64 else "f32+f64",
+        "data": "synthetic (seeded nw=32 model, 256^3 mesh blocks; no dataset)",
+        "config": {"workload": WORKLOAD, "k_per_step_per_gpu": batch, "mesh": list(MESH),
+                   "precision": args.precision, "l2": "inputs larger than L2 (per-step workspace >> 126 MB)",
+                   "parallelism": f"k-blocks x{world}"},
+        "roofline": roofline,
+        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": int(kpts.nbytes + w.nbytes),
+                "d2h_bytes_per_step": int(16 * vc)},
+        "clocks": clocks,
+        "gpu_launches": launches,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        v, n, dt = cpu_baseline_run(model, make_task(_abi.PRECISION_FP64), args.cpu_seconds, threads)
+        line["cpu_baseline"] = {"value": v, "unit": METRIC, "cores": threads, "kind": "port",
+                                "sample": f"{n} contiguous mesh points, FP64 oracle, {threads} OpenMP threads, {dt:.1f} s"}
+    engine.close()
+    if dist:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def fourier_channels(task) -> int:
+    # H, dH_x, dH_y, A_x, A_y, dA[y][x], ddH_xy, dA[x][y]  for sigma^xyy + Omega^xy + g^xx.
+    return 8
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -162,6 +162,13 @@ WNLQG_API wnlqg_status wnlqg_b200_eval_mesh_device(wnlqg_plan *plan, const int64
 WNLQG_API wnlqg_status wnlqg_b200_eval_points(wnlqg_plan *plan, const double *kpoints, int64_t n,
                                     double *out);
 
+/* Weighted sum over arbitrary points: out = sum_i weights[i] * value(k_i), with k[3*n] and
+ * weights[n] on the host.  This is the lane contract for a symmetry-reduced mesh
+ * (representatives with multiplicities / Nk, consume_point!, IntegralDriver.jl:820-874) and for
+ * a batch of adaptive nodes whose rule weights are known. */
+WNLQG_API wnlqg_status wnlqg_b200_eval_points_weighted(wnlqg_plan *plan, const double *kpoints,
+                                             const double *weights, int64_t n, double *out);
+
 /* Per-k band data for diagnostics and tests: energies [n*nw] (ascending) and the
  * canonicalised eigenvectors [n*nw*nw] complex, column-major per k
  * (compute_spectrum!, HamiltonianMatrixElements.jl:279-300 and :6-25). */

@@ -59,6 +59,7 @@ struct RespParams {
     double om_lo, om_hi;
     double eta_reg;
     double scale;               // 1/Nk (mesh mode) or 1 (point mode)
+    const double *weights;      // per-k weights (mode 0); nullptr: every k uses `scale`
     int mode;                   // 0: accumulate into partials[cta]; 1: write per-point values
     int64_t vc;                 // values per k
     double *partials;           // [gridDim][vc][4]: (sum re, sum im, comp re, comp im)
@@ -183,6 +184,7 @@ __global__ void __launch_bounds__(256) response_kernel_f64(RespParams p) {
     const int64_t ke = (p.batch * (blockIdx.x + 1)) / gridDim.x;
     for (int64_t b = kb; b < ke; ++b) {
         const double2 *xw = p.xw + b * p.xw_stride;
+        const double wk = p.weights ? p.weights[b] * p.scale : p.scale;
         for (int e = threadIdx.x; e < nn; e += blockDim.x) {
             int i = e % nw, j = e / nw;
             sU[i + ld * j] = p.U[b * nn + e];
@@ -279,7 +281,7 @@ __global__ void __launch_bounds__(256) response_kernel_f64(RespParams p) {
             if (threadIdx.x == 0) {
                 if (p.mode == 0) {
                     double *acc = p.partials + ((int64_t)blockIdx.x * p.vc + p.sc_out[s]) * 4;
-                    neumaier_add(acc[0], acc[2], total * p.scale);
+                    neumaier_add(acc[0], acc[2], total * wk);
                 } else {
                     p.out_points[(p.point_offset + b) * p.vc + p.sc_out[s]] = make_double2(total * p.scale, 0.0);
                 }
@@ -380,8 +382,8 @@ __global__ void __launch_bounds__(256) response_kernel_f64(RespParams p) {
                     if (p.mode == 0) {
                         if (active) {
                             double *a4 = p.partials + ((int64_t)blockIdx.x * p.vc + idx) * 4;
-                            neumaier_add(a4[0], a4[2], acc[c].x * p.scale);
-                            neumaier_add(a4[1], a4[3], acc[c].y * p.scale);
+                            neumaier_add(a4[0], a4[2], acc[c].x * wk);
+                            neumaier_add(a4[1], a4[3], acc[c].y * wk);
                         }
                     } else {
                         p.out_points[(p.point_offset + b) * p.vc + idx] = cscale(acc[c], p.scale);

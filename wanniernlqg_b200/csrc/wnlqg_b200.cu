@@ -73,7 +73,7 @@ struct wnlqg_plan {
     int64_t nn = 0, vc = 0, max_batch = 0;
     double2 *d_tiles = nullptr, *d_phase = nullptr, *d_xw = nullptr, *d_U = nullptr, *d_out = nullptr;
     double2 *d_points = nullptr;
-    double *d_E = nullptr, *d_kpts = nullptr, *d_omegas = nullptr, *d_partials = nullptr;
+    double *d_E = nullptr, *d_kpts = nullptr, *d_omegas = nullptr, *d_partials = nullptr, *d_weights = nullptr;
     int partial_slots = 0;
     std::vector<Pass> passes;
     int eigh_threads = 32;
@@ -304,7 +304,8 @@ wnlqg_status run_front(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const int64_
     return WNLQG_OK;
 }
 
-wnlqg_status run_passes(wnlqg_plan *pl, int64_t nb, int mode, double scale, int64_t point_offset) {
+wnlqg_status run_passes(wnlqg_plan *pl, int64_t nb, int mode, double scale, int64_t point_offset,
+                        const double *weights = nullptr) {
     for (Pass &ps : pl->passes) {
         RespParams p = ps.params;
         p.batch = nb;
@@ -313,6 +314,7 @@ wnlqg_status run_passes(wnlqg_plan *pl, int64_t nb, int mode, double scale, int6
         p.U = pl->d_U;
         p.mode = mode;
         p.scale = scale;
+        p.weights = weights;
         p.partials = pl->d_partials;
         p.out_points = pl->d_points;
         p.point_offset = point_offset;
@@ -416,7 +418,7 @@ wnlqg_status wnlqg_b200_plan_destroy(wnlqg_plan *pl) {
     if (pl->stream) cudaStreamSynchronize(pl->stream);
     for (void *ptr : {(void *)pl->d_tiles, (void *)pl->d_phase, (void *)pl->d_xw, (void *)pl->d_U, (void *)pl->d_out,
                       (void *)pl->d_points, (void *)pl->d_E, (void *)pl->d_kpts, (void *)pl->d_omegas,
-                      (void *)pl->d_partials})
+                      (void *)pl->d_partials, (void *)pl->d_weights})
         if (ptr) cudaFree(ptr);
     for (cudaEvent_t ev : pl->events) cudaEventDestroy(ev);
     if (pl->stream) cudaStreamDestroy(pl->stream);
@@ -576,6 +578,7 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
     if ((st = alloc((void **)&pl->d_U, (size_t)max_batch * nn * sizeof(double2))) != WNLQG_OK) return bail(st);
     if ((st = alloc((void **)&pl->d_E, (size_t)max_batch * nw * sizeof(double))) != WNLQG_OK) return bail(st);
     if ((st = alloc((void **)&pl->d_kpts, (size_t)max_batch * 3 * sizeof(double))) != WNLQG_OK) return bail(st);
+    if ((st = alloc((void **)&pl->d_weights, (size_t)max_batch * sizeof(double))) != WNLQG_OK) return bail(st);
     if ((st = alloc((void **)&pl->d_points, (size_t)max_batch * vc * sizeof(double2))) != WNLQG_OK) return bail(st);
     if ((st = alloc((void **)&pl->d_out, (size_t)vc * sizeof(double2))) != WNLQG_OK) return bail(st);
     if ((st = alloc((void **)&pl->d_omegas, std::max<size_t>(1, pl->omegas.size()) * sizeof(double))) != WNLQG_OK) return bail(st);
@@ -684,6 +687,37 @@ wnlqg_status wnlqg_b200_eval_points(wnlqg_plan *pl, const double *kpoints, int64
     WNLQG_CUDA(cudaStreamSynchronize(pl->stream));
     pl->timing_valid = false;
     for (int64_t v = 0; v < 2 * n * pl->vc; ++v)
+        if (!std::isfinite(out[v])) return fail(WNLQG_ERR_NONFINITE, "response contains non-finite values");
+    return WNLQG_OK;
+}
+
+wnlqg_status wnlqg_b200_eval_points_weighted(wnlqg_plan *pl, const double *kpoints, const double *weights,
+                                             int64_t n, double *out) {
+    wnlqg_status st = check_plan(pl);
+    if (st != WNLQG_OK) return st;
+    if (n < 0 || (n > 0 && (!kpoints || !weights)) || !out) return fail(WNLQG_ERR_INVALID_ARGUMENT, "invalid points");
+    if (!finite_array(kpoints, 3 * (size_t)n) || !finite_array(weights, (size_t)n))
+        return fail(WNLQG_ERR_NONFINITE, "k-points and weights must be finite");
+    WNLQG_CUDA(cudaSetDevice(pl->model->device));
+    pl->launches = 0;
+    WNLQG_CUDA(cudaMemsetAsync(pl->d_partials, 0, (size_t)pl->partial_slots * pl->vc * 4 * sizeof(double), pl->stream));
+    for (int64_t s = 0; s < n; s += pl->max_batch) {
+        int64_t nb = std::min(pl->max_batch, n - s);
+        WNLQG_CUDA(cudaMemcpyAsync(pl->d_kpts, kpoints + 3 * s, (size_t)nb * 3 * sizeof(double), cudaMemcpyHostToDevice,
+                                   pl->stream));
+        WNLQG_CUDA(cudaMemcpyAsync(pl->d_weights, weights + s, (size_t)nb * sizeof(double), cudaMemcpyHostToDevice,
+                                   pl->stream));
+        if ((st = run_front(pl, nb, 0, nullptr, pl->d_kpts, 1)) != WNLQG_OK) return st;
+        if ((st = run_passes(pl, nb, 0, 1.0, 0, pl->d_weights)) != WNLQG_OK) return st;
+    }
+    reduce_partials_kernel<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((pl->vc + 255) / 256, 1024)), 256, 0,
+                             pl->stream>>>(pl->d_partials, pl->partial_slots, pl->vc, pl->d_out);
+    pl->launches += 1;
+    WNLQG_CUDA(cudaGetLastError());
+    WNLQG_CUDA(cudaMemcpyAsync(out, pl->d_out, (size_t)pl->vc * sizeof(double2), cudaMemcpyDeviceToHost, pl->stream));
+    WNLQG_CUDA(cudaStreamSynchronize(pl->stream));
+    pl->timing_valid = false;
+    for (int64_t v = 0; v < 2 * pl->vc; ++v)
         if (!std::isfinite(out[v])) return fail(WNLQG_ERR_NONFINITE, "response contains non-finite values");
     return WNLQG_OK;
 }

@@ -89,6 +89,19 @@ class ResponseEngine:
                                                   k.shape[0], out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
         return out
 
+    def weighted_sum(self, kpoints, weights) -> np.ndarray:
+        """sum_i weights[i] * value(k_i) over host k-points [n, 3], complex [value_count]."""
+        k = np.ascontiguousarray(np.asarray(kpoints, dtype=np.float64).reshape(-1, 3))
+        w = np.ascontiguousarray(np.asarray(weights, dtype=np.float64).reshape(-1))
+        if w.shape[0] != k.shape[0]:
+            raise ValueError("one weight per k-point")
+        out = np.zeros(self.value_count, dtype=np.complex128)
+        _lib.check(self._L.wnlqg_b200_eval_points_weighted(
+            self._plan, k.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+            w.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), k.shape[0],
+            out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return out
+
     def spectrum(self, kpoints):
         """(energies [n, nw], canonical eigenvectors [n, nw, nw]) at fractional k-points."""
         k = np.ascontiguousarray(np.asarray(kpoints, dtype=np.float64).reshape(-1, 3))
