@@ -612,16 +612,18 @@ wnlqg_status wnlqg_b200_eval_mesh_device(wnlqg_plan *pl, const int64_t mesh[3], 
     const int64_t nk = mesh[0] * mesh[1] * mesh[2];
     if (k_begin < 0 || k_end > nk || k_begin > k_end) return fail(WNLQG_ERR_INVALID_ARGUMENT, "k range outside the mesh");
     WNLQG_CUDA(cudaSetDevice(pl->model->device));
+    // The caller's stream (NULL = the legacy default stream) and the plan's non-blocking stream
+    // are ordered both ways with events: the work starts after everything queued on the caller's
+    // stream and the caller's stream resumes after the result is written.
     cudaStream_t user = static_cast<cudaStream_t>(stream);
-    // Order the plan stream after the caller's stream.
-    if ((st = record_event(pl, 0)) != WNLQG_OK) return st;
-    if (user) {
+    {
         cudaEvent_t ev;
         WNLQG_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
         WNLQG_CUDA(cudaEventRecord(ev, user));
         WNLQG_CUDA(cudaStreamWaitEvent(pl->stream, ev, 0));
         cudaEventDestroy(ev);
     }
+    if ((st = record_event(pl, 0)) != WNLQG_OK) return st;
     pl->launches = 0;
     WNLQG_CUDA(cudaMemsetAsync(pl->d_partials, 0, (size_t)pl->partial_slots * pl->vc * 4 * sizeof(double), pl->stream));
     const double scale = 1.0 / (double)nk;
@@ -643,7 +645,7 @@ wnlqg_status wnlqg_b200_eval_mesh_device(wnlqg_plan *pl, const int64_t mesh[3], 
     WNLQG_CUDA(cudaGetLastError());
     if ((st = record_event(pl, final_ev + 1)) != WNLQG_OK) return st;
     pl->timing_valid = false;
-    if (user) {
+    {
         cudaEvent_t ev;
         WNLQG_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
         WNLQG_CUDA(cudaEventRecord(ev, pl->stream));
