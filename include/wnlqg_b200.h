@@ -175,6 +175,23 @@ WNLQG_API wnlqg_status wnlqg_b200_eval_points_weighted(wnlqg_plan *plan, const d
 WNLQG_API wnlqg_status wnlqg_b200_eval_spectrum(wnlqg_plan *plan, const double *kpoints, int64_t n,
                                       double *energies, double *eigenvectors);
 
+/* Allocation-free spectrum (no counterpart in the reference).  For callers that cannot let this
+ * library allocate device memory (their memory belongs to another pool allocator under a fixed
+ * budget).  Inputs and outputs are caller-owned DEVICE arrays on the current device:
+ * hamiltonian_r complex [nw,nw,NR], r_vectors int64 [3,NR], r_degeneracies int64 [NR],
+ * kpoints [3*n] fractional; energies [n*nw] ascending, eigenvectors complex [n*nw*nw]
+ * (canonical phases, column-major per k).  Scratch is a fixed 8 MiB device array inside the
+ * library, so n*(NR + nw^2)*16 bytes must stay below 8 MiB (larger n is rejected with
+ * WNLQG_ERR_INVALID_ARGUMENT); nw <= 32.  The first call on a device looks up the scratch
+ * address (cudaGetSymbolAddress); make that first call before any stream capture.  All calls
+ * share the one scratch array: calls whose GPU work overlaps (other streams, other threads)
+ * race on it.  Asynchronous on `stream` (NULL = legacy default stream); allocates nothing. */
+WNLQG_API wnlqg_status wnlqg_b200_spectrum_noalloc(int64_t num_orbitals, int64_t num_r_vectors,
+                                         const double *hamiltonian_r, const int64_t *r_vectors,
+                                         const int64_t *r_degeneracies, const double *kpoints,
+                                         int64_t n, double *energies, double *eigenvectors,
+                                         void *stream);
+
 /* Device time in milliseconds of the last eval_mesh* call's dominant kernel and of the
  * whole call (CUDA events on the plan's stream). */
 WNLQG_API wnlqg_status wnlqg_b200_plan_last_timing(const wnlqg_plan *plan, double *fourier_ms,

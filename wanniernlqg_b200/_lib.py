@@ -20,6 +20,7 @@ EXPORTED_SYMBOLS = (
     "wnlqg_b200_eval_mesh", "wnlqg_b200_eval_mesh_device", "wnlqg_b200_eval_points",
     "wnlqg_b200_eval_points_weighted",
     "wnlqg_b200_eval_spectrum", "wnlqg_b200_plan_last_timing", "wnlqg_b200_plan_last_launch_count",
+    "wnlqg_b200_spectrum_noalloc",
 )
 
 _lib = None
@@ -61,6 +62,9 @@ def load():
     L.wnlqg_b200_eval_points_weighted.argtypes = [vp, dp, dp, ctypes.c_int64, dp]
     L.wnlqg_b200_eval_spectrum.argtypes = [vp, dp, ctypes.c_int64, dp, dp]
     L.wnlqg_b200_plan_last_timing.argtypes = [vp, dp, dp, dp, dp]
+    L.wnlqg_b200_spectrum_noalloc.argtypes = [ctypes.c_int64, ctypes.c_int64, vp, vp, vp, vp, ctypes.c_int64, vp, vp,
+                                              vp]
+    L.wnlqg_b200_spectrum_noalloc.restype = ctypes.c_int
     L.wnlqg_b200_plan_last_launch_count.restype = ctypes.c_int64
     L.wnlqg_b200_plan_last_launch_count.argtypes = [vp]
     for name in ("wnlqg_b200_last_error", "wnlqg_b200_model_create", "wnlqg_b200_model_destroy",

@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -779,3 +780,79 @@ wnlqg_status wnlqg_b200_plan_last_timing(const wnlqg_plan *pl_const, double *fou
 int64_t wnlqg_b200_plan_last_launch_count(const wnlqg_plan *plan) { return plan ? plan->launches : -1; }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// Allocation-free spectrum entry point.
+//
+// Some callers cannot let this library call cudaMalloc: applications whose device memory is
+// owned by another pool allocator under a hard budget (a Julia CUDA.jl pool, PyTorch's caching
+// allocator, a serving process that reserves all HBM up front), where an allocation behind the
+// pool's back fails or evicts the pool's own buffers.  wnlqg_b200_spectrum_noalloc serves them:
+// the caller passes device inputs and outputs, and the only scratch (phase table and H(k)) lives
+// in the fixed file-scope array below, which every GPU that loads the library keeps until exit.
+// ---------------------------------------------------------------------------------------------
+#define WNLQG_NOALLOC_SCRATCH_BYTES ((size_t)8 << 20)   // 8 MiB per device
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[WNLQG_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+constexpr int kNoallocMaxDevices = 64;
+void *g_noalloc_ptr[kNoallocMaxDevices] = {nullptr};
+std::mutex g_noalloc_mutex;
+
+// Device address of the scratch array on the current device, looked up once per device.  In
+// host code the array's name is only a host-side stand-in, never a device address.
+wnlqg_status noalloc_scratch(int device, void **out) {
+    if (device < 0 || device >= kNoallocMaxDevices) return fail(WNLQG_ERR_UNSUPPORTED, "device index too large");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[device]) {
+        void *ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess || !ptr)
+            return fail(WNLQG_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+        g_noalloc_ptr[device] = ptr;
+    }
+    *out = g_noalloc_ptr[device];
+    return WNLQG_OK;
+}
+}  // namespace
+
+extern "C" wnlqg_status wnlqg_b200_spectrum_noalloc(int64_t num_orbitals, int64_t num_r_vectors,
+                                                    const double *hamiltonian_r, const int64_t *r_vectors,
+                                                    const int64_t *r_degeneracies, const double *kpoints,
+                                                    int64_t n, double *energies, double *eigenvectors,
+                                                    void *stream) {
+    if (num_orbitals <= 0 || num_orbitals > 32 || num_r_vectors <= 0)
+        return fail(WNLQG_ERR_UNSUPPORTED, "spectrum_noalloc supports 1 <= num_orbitals <= 32 and num_r_vectors >= 1");
+    if (n < 0) return fail(WNLQG_ERR_INVALID_ARGUMENT, "negative point count");
+    if (n == 0) return WNLQG_OK;
+    if (!hamiltonian_r || !r_vectors || !r_degeneracies || !kpoints || !energies || !eigenvectors)
+        return fail(WNLQG_ERR_INVALID_ARGUMENT, "NULL device pointer");
+    const int nw = (int)num_orbitals, nr = (int)num_r_vectors;
+    const int64_t nn = (int64_t)nw * nw;
+    // Scratch: phase table [n][NR] then H(k) [n][nw*nw], complex double, 256-byte aligned parts.
+    const size_t phase_bytes = (((size_t)n * nr * sizeof(double2)) + 255) & ~(size_t)255;
+    const size_t hk_bytes = (size_t)n * nn * sizeof(double2);
+    if (phase_bytes + hk_bytes > WNLQG_NOALLOC_SCRATCH_BYTES)
+        return fail(WNLQG_ERR_INVALID_ARGUMENT,
+                    "spectrum_noalloc: n*(NR + nw^2)*16 bytes exceeds the 8 MiB scratch; pass fewer points per call (at most " +
+                        std::to_string(WNLQG_NOALLOC_SCRATCH_BYTES / ((size_t)(nr + nn) * sizeof(double2) + 256)) + ")");
+    int device = 0;
+    WNLQG_CUDA(cudaGetDevice(&device));
+    void *scratch = nullptr;
+    wnlqg_status st = noalloc_scratch(device, &scratch);
+    if (st != WNLQG_OK) return st;
+    double2 *phases = reinterpret_cast<double2 *>(scratch);
+    double2 *hk = reinterpret_cast<double2 *>(static_cast<unsigned char *>(scratch) + phase_bytes);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int64_t total = n * nr;
+    const int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 32);
+    // Every scratch element is overwritten before it is read, so nothing needs clearing.
+    phase_kernel<<<blocks, 256, 0, s>>>(phases, r_vectors, r_degeneracies, nr, n, 0, 1, 1, 1, kpoints);
+    dim3 grid((unsigned)((nn + FG_BN - 1) / FG_BN), (unsigned)((n + FG_BM - 1) / FG_BM));
+    fourier_gemm_f64<<<grid, 256, 0, s>>>(phases, reinterpret_cast<const double2 *>(hamiltonian_r), hk, n, nn, nr);
+    jacobi_eigh_kernel<double><<<(unsigned)n, eigh_block_threads(nw), EighSmem::bytes(nw, sizeof(double2)), s>>>(
+        hk, nn, n, nw, energies, reinterpret_cast<double2 *>(eigenvectors), 8.673617379884035e-19);
+    WNLQG_CUDA(cudaGetLastError());
+    return WNLQG_OK;
+}
