@@ -139,3 +139,20 @@ def test_invalid_task_rejected(engine_cls):
     with pytest.raises(EngineError) as ei:
         engine_cls(model, nw4_task(width=0.0))
     assert ei.value.status == 1
+
+
+@pytest.mark.parametrize("name,mesh,batch", [("nw4", (5, 3, 4), 7), ("nw4", (16, 2, 3), 40), ("nw32", (9, 2, 2), 10)])
+def test_staged_mesh_fourier_batches_crossing_lines(engine_cls, oracle_mod, name, mesh, batch):
+    """The staged (separable) mesh contraction, with plan batches that start and end mid-line
+    and mid-plane, equals the oracle's direct Fourier sum."""
+    model = reference_workload_model(name)
+    task = nw4_task(nom=24) if name == "nw4" else nw32_task(nom=24)
+    with engine_cls(model, task, max_batch=batch) as eng:
+        got = eng.integrate_mesh(mesh)
+        part = eng.integrate_mesh(mesh, 3, int(np.prod(mesh)) - 2)
+    ref = oracle_mod.integrate_mesh(model, task, mesh)
+    ref_part = oracle_mod.integrate_mesh(model, task, mesh, 3, int(np.prod(mesh)) - 2)
+    for g, r in zip(task.split(got), task.split(ref)):
+        assert rel_err(g, r) < RTOL
+    for g, r in zip(task.split(part), task.split(ref_part)):
+        assert rel_err(g, r) < RTOL

@@ -92,3 +92,129 @@ __global__ void __launch_bounds__(256) fourier_gemm_f64(const double2 *__restric
         }
     }
 }
+
+// ---------------------------------------------------------------------------------------------
+// Staged (separable) Fourier contraction on the uniform Gamma-centred mesh.
+//
+// exp(2 pi i R.k) = exp(2 pi i r1 i1/N1) exp(2 pi i r2 i2/N2) exp(2 pi i r3 i3/N3), so
+//   Y[i3][(r1,r2)] = sum_{r3} e3 T(R)/deg          (once per k3 plane touched by the batch)
+//   Z[line][r1]    = sum_{r2} e2 Y[i3][(r1,r2)]     (once per (i2,i3) line touched)
+//   X[k]           = sum_{r1} e1 Z[line(k)][r1]     (per k-point)
+// give the direct sum of HamiltonianMatrixElements.jl:42-58 on every mesh point with
+// 8*P1*C*nw^2 flops per k instead of 8*NR*C*nw^2 (P1 = number of distinct r1).  This is the
+// dense-mesh role of the reference's Mixed-FFT backend (MixedFourierMatrixElements.jl:954-1126).
+// R-vectors are grouped on the host: q12 = distinct (r1,r2) with its R list, q1 = distinct r1
+// with its q12 list.
+// ---------------------------------------------------------------------------------------------
+struct StagedGroups {
+    int P12, P1;
+    const int *q12_start;   // [P12+1] offsets into q12_ridx
+    const int *q12_ridx;    // [NR] R indices grouped by (r1,r2)
+    const int *q12_r2;      // [P12]
+    const int *q1_start;    // [P1+1] offsets into q1_q12
+    const int *q1_q12;      // [P12] q12 indices grouped by r1
+    const int *q1_r1;       // [P1]
+};
+
+WNLQG_D double2 mesh_phase(int64_t r, int64_t i, int64_t n) {
+    int64_t p = ((r * i) % n + n) % n;
+    double s, c;
+    sincospi(2.0 * (double)p / (double)n, &s, &c);
+    return make_double2(c, s);
+}
+
+// Y[t3][q12][col] for t3 = 0..n3-1 (i3 = i3_first + t3).  Grid: (col blocks, P12, n3).
+__global__ void staged_r3_kernel(const double2 *__restrict__ T, int64_t N, StagedGroups g,
+                                 const int64_t *__restrict__ rvec, const int64_t *__restrict__ deg, int64_t i3_first,
+                                 int64_t n3mesh, double2 *__restrict__ Y) {
+    const int q12 = blockIdx.y, t3 = blockIdx.z;
+    const int64_t col = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t i3 = i3_first + t3;
+    __shared__ double2 ph[64];
+    const int s0 = g.q12_start[q12], s1 = g.q12_start[q12 + 1];
+    double2 acc = make_double2(0.0, 0.0);
+    for (int base = s0; base < s1; base += 64) {
+        const int cnt = min(64, s1 - base);
+        __syncthreads();
+        if (threadIdx.x < cnt) {
+            const int r = g.q12_ridx[base + threadIdx.x];
+            ph[threadIdx.x] = cscale(mesh_phase(rvec[3 * r + 2], i3, n3mesh), 1.0 / (double)deg[r]);
+        }
+        __syncthreads();
+        if (col < N)
+            for (int j = 0; j < cnt; ++j) acc = cfma(ph[j], T[(int64_t)g.q12_ridx[base + j] * N + col], acc);
+    }
+    if (col < N) Y[((int64_t)t3 * g.P12 + q12) * N + col] = acc;
+}
+
+// Z[l][q1][col] for lines l = 0..nlines-1 (global line = line_first + l, i2 = line % N2,
+// i3 = line / N2).  Grid: (col blocks, P1, nlines).
+__global__ void staged_r2_kernel(const double2 *__restrict__ Y, int64_t N, StagedGroups g, int64_t line_first,
+                                 int64_t n2mesh, int64_t i3_first, double2 *__restrict__ Z) {
+    const int q1 = blockIdx.y;
+    const int64_t l = blockIdx.z;
+    const int64_t col = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t line = line_first + l;
+    const int64_t i2 = line % n2mesh, t3 = line / n2mesh - i3_first;
+    __shared__ double2 ph[64];
+    __shared__ int qq[64];
+    const int s0 = g.q1_start[q1], s1 = g.q1_start[q1 + 1];
+    double2 acc = make_double2(0.0, 0.0);
+    for (int base = s0; base < s1; base += 64) {
+        const int cnt = min(64, s1 - base);
+        __syncthreads();
+        if (threadIdx.x < cnt) {
+            const int q12 = g.q1_q12[base + threadIdx.x];
+            qq[threadIdx.x] = q12;
+            ph[threadIdx.x] = mesh_phase(g.q12_r2[q12], i2, n2mesh);
+        }
+        __syncthreads();
+        if (col < N)
+            for (int j = 0; j < cnt; ++j) acc = cfma(ph[j], Y[((int64_t)t3 * g.P12 + qq[j]) * N + col], acc);
+    }
+    if (col < N) Z[((int64_t)l * g.P1 + q1) * N + col] = acc;
+}
+
+// X[b][col] = sum_q1 e1(b, q1) Z[line(b)][q1][col] for batch entries b (mesh index k_begin + b).
+// Grid: (col blocks, ceil(nb / 16)); each CTA handles 16 consecutive batch entries.
+constexpr int STAGED_BT = 16;
+constexpr int STAGED_MAX_P1 = 32;
+
+__global__ void __launch_bounds__(256) staged_r1_kernel(const double2 *__restrict__ Z, int64_t N, StagedGroups g,
+                                                        int64_t k_begin, int64_t nb, int64_t n1mesh,
+                                                        int64_t line_first, double2 *__restrict__ X) {
+    __shared__ double2 ph[STAGED_BT][STAGED_MAX_P1];
+    const int64_t b0 = (int64_t)blockIdx.y * STAGED_BT;
+    const int64_t col = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int P1 = g.P1;
+    for (int e = threadIdx.x; e < STAGED_BT * P1; e += blockDim.x) {
+        const int bb = e / P1, q1 = e % P1;
+        const int64_t idx = k_begin + b0 + bb;
+        ph[bb][q1] = mesh_phase(g.q1_r1[q1], idx % n1mesh, n1mesh);
+    }
+    __syncthreads();
+    if (col >= N) return;
+    const int64_t bend = min((int64_t)STAGED_BT, nb - b0);
+    const int64_t l_first = (k_begin + b0) / n1mesh - line_first;
+    const int64_t l_last = (k_begin + b0 + bend - 1) / n1mesh - line_first;
+    if (l_first == l_last) {
+        double2 z[STAGED_MAX_P1];
+        const double2 *zl = Z + (l_first * P1) * N + col;
+#pragma unroll 4
+        for (int q1 = 0; q1 < P1; ++q1) z[q1] = zl[(int64_t)q1 * N];
+        for (int bb = 0; bb < bend; ++bb) {
+            double2 acc = make_double2(0.0, 0.0);
+#pragma unroll 4
+            for (int q1 = 0; q1 < P1; ++q1) acc = cfma(ph[bb][q1], z[q1], acc);
+            X[(b0 + bb) * N + col] = acc;
+        }
+    } else {
+        for (int bb = 0; bb < bend; ++bb) {
+            const int64_t l = (k_begin + b0 + bb) / n1mesh - line_first;
+            const double2 *zl = Z + (l * P1) * N + col;
+            double2 acc = make_double2(0.0, 0.0);
+            for (int q1 = 0; q1 < P1; ++q1) acc = cfma(ph[bb][q1], zl[(int64_t)q1 * N], acc);
+            X[(b0 + bb) * N + col] = acc;
+        }
+    }
+}

@@ -76,6 +76,13 @@ struct wnlqg_plan {
     double2 *d_points = nullptr;
     double *d_E = nullptr, *d_kpts = nullptr, *d_omegas = nullptr, *d_partials = nullptr, *d_weights = nullptr;
     int partial_slots = 0;
+    // Staged mesh Fourier: R grouping (device) and lazily sized Y/Z workspaces.
+    int P12 = 0, P1 = 0;
+    int *d_groups = nullptr;        // q12_start | q12_ridx | q12_r2 | q1_start | q1_q12 | q1_r1
+    StagedGroups groups;
+    double2 *d_stageY = nullptr, *d_stageZ = nullptr;
+    size_t stageY_elems = 0, stageZ_elems = 0;
+    bool use_staged_last = false;
     std::vector<Pass> passes;
     int eigh_threads = 32;
     size_t eigh_smem = 0;
@@ -287,20 +294,54 @@ wnlqg_status record_event(wnlqg_plan *pl, size_t idx) {
 wnlqg_status run_front(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const int64_t *mesh, const double *kpts_device,
                        size_t ev_base) {
     const int nr = pl->nr;
-    int64_t total = nb * nr;
-    int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 32);
-    phase_kernel<<<blocks, 256, 0, pl->stream>>>(pl->d_phase, pl->model->d_rvec, pl->model->d_deg, nr, nb, k_begin,
-                                                 mesh ? mesh[0] : 1, mesh ? mesh[1] : 1, mesh ? mesh[2] : 1, kpts_device);
     int64_t N = (int64_t)pl->C * pl->nn;
-    dim3 grid((unsigned)((N + FG_BN - 1) / FG_BN), (unsigned)((nb + FG_BM - 1) / FG_BM));
-    fourier_gemm_f64<<<grid, 256, 0, pl->stream>>>(pl->d_phase, pl->d_tiles, pl->d_xw, nb, N, nr);
+    const bool staged = mesh != nullptr && kpts_device == nullptr && pl->P1 <= STAGED_MAX_P1 && mesh[0] >= pl->P1;
+    pl->use_staged_last = staged;
+    if (staged) {
+        const int64_t n1 = mesh[0], n2 = mesh[1], n3 = mesh[2];
+        const int64_t line_first = k_begin / n1, line_last = (k_begin + nb - 1) / n1;
+        const int64_t nlines = line_last - line_first + 1;
+        const int64_t i3_first = line_first / n2, i3_last = line_last / n2;
+        const int64_t n3t = i3_last - i3_first + 1;
+        const size_t needY = (size_t)n3t * pl->P12 * N, needZ = (size_t)nlines * pl->P1 * N;
+        if (needY > pl->stageY_elems) {
+            if (pl->d_stageY) WNLQG_CUDA(cudaFree(pl->d_stageY));
+            pl->d_stageY = nullptr;
+            pl->stageY_elems = 0;
+            WNLQG_CUDA(cudaMalloc(&pl->d_stageY, needY * sizeof(double2)));
+            pl->stageY_elems = needY;
+        }
+        if (needZ > pl->stageZ_elems) {
+            if (pl->d_stageZ) WNLQG_CUDA(cudaFree(pl->d_stageZ));
+            pl->d_stageZ = nullptr;
+            pl->stageZ_elems = 0;
+            WNLQG_CUDA(cudaMalloc(&pl->d_stageZ, needZ * sizeof(double2)));
+            pl->stageZ_elems = needZ;
+        }
+        const unsigned cb = (unsigned)((N + 255) / 256);
+        staged_r3_kernel<<<dim3(cb, pl->P12, (unsigned)n3t), 256, 0, pl->stream>>>(
+            pl->d_tiles, N, pl->groups, pl->model->d_rvec, pl->model->d_deg, i3_first, n3, pl->d_stageY);
+        staged_r2_kernel<<<dim3(cb, pl->P1, (unsigned)nlines), 256, 0, pl->stream>>>(pl->d_stageY, N, pl->groups,
+                                                                                       line_first, n2, i3_first,
+                                                                                       pl->d_stageZ);
+        staged_r1_kernel<<<dim3(cb, (unsigned)((nb + STAGED_BT - 1) / STAGED_BT)), 256, 0, pl->stream>>>(
+            pl->d_stageZ, N, pl->groups, k_begin, nb, n1, line_first, pl->d_xw);
+    } else {
+        int64_t total = nb * nr;
+        int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 32);
+        phase_kernel<<<blocks, 256, 0, pl->stream>>>(pl->d_phase, pl->model->d_rvec, pl->model->d_deg, nr, nb,
+                                                     k_begin, mesh ? mesh[0] : 1, mesh ? mesh[1] : 1,
+                                                     mesh ? mesh[2] : 1, kpts_device);
+        dim3 grid((unsigned)((N + FG_BN - 1) / FG_BN), (unsigned)((nb + FG_BM - 1) / FG_BM));
+        fourier_gemm_f64<<<grid, 256, 0, pl->stream>>>(pl->d_phase, pl->d_tiles, pl->d_xw, nb, N, nr);
+    }
     wnlqg_status st = record_event(pl, ev_base + 1);
     if (st != WNLQG_OK) return st;
     jacobi_eigh_kernel<double><<<(unsigned)nb, pl->eigh_threads, pl->eigh_smem, pl->stream>>>(
         pl->d_xw + (int64_t)pl->ch_H * pl->nn, N, nb, pl->nw, pl->d_E, pl->d_U, 8.673617379884035e-19);
     st = record_event(pl, ev_base + 2);
     if (st != WNLQG_OK) return st;
-    pl->launches += 3;
+    pl->launches += staged ? 4 : 3;
     WNLQG_CUDA(cudaGetLastError());
     return WNLQG_OK;
 }
@@ -419,7 +460,8 @@ wnlqg_status wnlqg_b200_plan_destroy(wnlqg_plan *pl) {
     if (pl->stream) cudaStreamSynchronize(pl->stream);
     for (void *ptr : {(void *)pl->d_tiles, (void *)pl->d_phase, (void *)pl->d_xw, (void *)pl->d_U, (void *)pl->d_out,
                       (void *)pl->d_points, (void *)pl->d_E, (void *)pl->d_kpts, (void *)pl->d_omegas,
-                      (void *)pl->d_partials, (void *)pl->d_weights})
+                      (void *)pl->d_partials, (void *)pl->d_weights, (void *)pl->d_groups, (void *)pl->d_stageY,
+                      (void *)pl->d_stageZ})
         if (ptr) cudaFree(ptr);
     for (cudaEvent_t ev : pl->events) cudaEventDestroy(ev);
     if (pl->stream) cudaStreamDestroy(pl->stream);
@@ -586,6 +628,55 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
     WNLQG_CUDA(cudaMemcpy(pl->d_tiles, tiles.data(), tiles.size() * sizeof(double2), cudaMemcpyHostToDevice));
     if (!pl->omegas.empty())
         WNLQG_CUDA(cudaMemcpy(pl->d_omegas, pl->omegas.data(), pl->omegas.size() * sizeof(double), cudaMemcpyHostToDevice));
+
+    // Group the R-vectors for the staged mesh contraction.
+    {
+        std::vector<std::pair<std::pair<int64_t, int64_t>, int>> keyed;
+        for (int r = 0; r < nr; ++r) keyed.push_back({{model->rvec[3 * r], model->rvec[3 * r + 1]}, r});
+        std::stable_sort(keyed.begin(), keyed.end(),
+                         [](const auto &x, const auto &y) { return x.first < y.first; });
+        std::vector<int> q12_start, q12_ridx, q12_r2, q12_r1;
+        for (size_t i = 0; i < keyed.size(); ++i) {
+            if (i == 0 || keyed[i].first != keyed[i - 1].first) {
+                q12_start.push_back((int)i);
+                q12_r1.push_back((int)keyed[i].first.first);
+                q12_r2.push_back((int)keyed[i].first.second);
+            }
+            q12_ridx.push_back(keyed[i].second);
+        }
+        const int P12 = (int)q12_r2.size();
+        q12_start.push_back(nr);
+        std::vector<int> q1_start, q1_q12, q1_r1;
+        for (int q = 0; q < P12; ++q) {   // q12 are sorted by (r1, r2): r1 groups are contiguous
+            if (q == 0 || q12_r1[q] != q12_r1[q - 1]) {
+                q1_start.push_back(q);
+                q1_r1.push_back(q12_r1[q]);
+            }
+            q1_q12.push_back(q);
+        }
+        const int P1 = (int)q1_r1.size();
+        q1_start.push_back(P12);
+        std::vector<int> packed;
+        packed.insert(packed.end(), q12_start.begin(), q12_start.end());
+        packed.insert(packed.end(), q12_ridx.begin(), q12_ridx.end());
+        packed.insert(packed.end(), q12_r2.begin(), q12_r2.end());
+        packed.insert(packed.end(), q1_start.begin(), q1_start.end());
+        packed.insert(packed.end(), q1_q12.begin(), q1_q12.end());
+        packed.insert(packed.end(), q1_r1.begin(), q1_r1.end());
+        if ((st = alloc((void **)&pl->d_groups, packed.size() * sizeof(int))) != WNLQG_OK) return bail(st);
+        WNLQG_CUDA(cudaMemcpy(pl->d_groups, packed.data(), packed.size() * sizeof(int), cudaMemcpyHostToDevice));
+        pl->P12 = P12;
+        pl->P1 = P1;
+        int *base = pl->d_groups;
+        pl->groups.P12 = P12;
+        pl->groups.P1 = P1;
+        pl->groups.q12_start = base; base += P12 + 1;
+        pl->groups.q12_ridx = base; base += nr;
+        pl->groups.q12_r2 = base; base += P12;
+        pl->groups.q1_start = base; base += P1 + 1;
+        pl->groups.q1_q12 = base; base += P12;
+        pl->groups.q1_r1 = base;
+    }
 
     pl->eigh_threads = eigh_block_threads(nw);
     pl->eigh_smem = EighSmem::bytes(nw, sizeof(double2));
