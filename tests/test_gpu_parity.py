@@ -156,3 +156,34 @@ def test_staged_mesh_fourier_batches_crossing_lines(engine_cls, oracle_mod, name
         assert rel_err(g, r) < RTOL
     for g, r in zip(task.split(part), task.split(ref_part)):
         assert rel_err(g, r) < RTOL
+
+
+# Mixed path (FP32 per-k matrices; FP64 energies, denominators, occupations and k-sums).
+# Stated bound: 1e-4 relative (max norm over frequencies/components, relative to the oracle's
+# max norm) for every response; the bench workload's sigma^xyy target is 1e-4.
+MIXED_RTOL = 1e-4
+
+
+@pytest.mark.parametrize("name", ["nw4", "nw32"])
+def test_mixed_point_values_within_bound(engine_cls, oracle_mod, name):
+    model = reference_workload_model(name)
+    task = (nw4_task(precision=_abi.PRECISION_MIXED) if name == "nw4"
+            else nw32_task(precision=_abi.PRECISION_MIXED))
+    k = np.random.default_rng(14).random((16, 3))
+    with engine_cls(model, task) as eng:
+        got = eng.point_values(k)
+    ref = oracle_mod.point_values(model, task, k)
+    for g, r in zip(task.split(got), task.split(ref)):
+        assert rel_err(g, r) < MIXED_RTOL
+
+
+@pytest.mark.parametrize("name,mesh", [("nw4", (8, 8, 8)), ("nw32", (9, 4, 3))])
+def test_mixed_mesh_within_bound(engine_cls, oracle_mod, name, mesh):
+    model = reference_workload_model(name)
+    task = (nw4_task(precision=_abi.PRECISION_MIXED) if name == "nw4"
+            else nw32_task(nom=64, precision=_abi.PRECISION_MIXED))
+    with engine_cls(model, task) as eng:
+        got = eng.integrate_mesh(mesh)
+    ref = oracle_mod.integrate_mesh(model, task, mesh)
+    for g, r in zip(task.split(got), task.split(ref)):
+        assert rel_err(g, r) < MIXED_RTOL

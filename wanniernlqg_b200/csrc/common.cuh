@@ -39,6 +39,9 @@ WNLQG_HD float2 cfmaconj(float2 a, float2 b, float2 acc) {
     return make_float2(fmaf(a.x, b.x, fmaf(a.y, b.y, acc.x)), fmaf(a.x, b.y, fmaf(-a.y, b.x, acc.y)));
 }
 
+WNLQG_HD double2 make_neg(double2 a) { return make_double2(-a.x, -a.y); }
+WNLQG_HD float2 make_neg(float2 a) { return make_float2(-a.x, -a.y); }
+
 // Complex type traits for templated kernels: real type R, complex type C.
 template <typename R> struct cplx_of;
 template <> struct cplx_of<double> { typedef double2 type; };

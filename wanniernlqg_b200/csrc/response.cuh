@@ -36,7 +36,7 @@ struct RespParams {
     // Channel index inside xw (-1: absent).
     int ch_dH[3], ch_A[3], ch_ddH[9], ch_dA[9];   // [p*3+d]: position p, derivative d
     // Shared-memory matrix slots (-1: absent).
-    int slot_dH[3], slot_A[3];
+    int slot_dH[3], slot_A[3], slot_D[3];
     int n_g;
     int g_p[RS_MAX_G], g_d[RS_MAX_G], g_slot[RS_MAX_G];
     // Frequency-axis components (shift / injection).
@@ -86,8 +86,8 @@ struct RespSmem {
         s.f = take(nw * sizeof(double));
         s.te = take((size_t)nw * nw * sizeof(double));
         s.fnm = take((size_t)nw * nw * sizeof(double));
-        s.Q = take((size_t)nw * nw * (n_fc > 0 ? n_fc : 1) * sizeof(double2));
-        s.fd = take((size_t)nw * (n_berry > 0 ? n_berry : 1) * sizeof(double2));
+        s.Q = take((size_t)nw * nw * (n_fc > 0 ? n_fc : 1) * csize);
+        s.fd = take((size_t)2 * nw * (n_berry > 0 ? n_berry : 1) * sizeof(double2));
         s.red = take(64 * sizeof(double) + 64 * sizeof(int));
         s.total = off;
         return s;
@@ -110,28 +110,105 @@ WNLQG_D double fermi_occ(double e, double mu, double kT) {
     return 1.0 / (exp(arg) + 1.0);
 }
 
-// dst = U^H X U for one Wannier-gauge matrix X read from global memory (column-major nw x nw).
-// All threads participate; shared matrices use leading dimension ld = nw + 1.
-WNLQG_D void rotate_to_hamiltonian(const double2 *__restrict__ src, double2 *T1, double2 *T2, const double2 *U,
-                                   double2 *dst, int nw, int ld) {
+// ---- shared-memory matrix products (all threads participate; ld = nw + 1) -------------------
+// Work item w -> row i = w % nw and four columns 4*(w / nw) .. +3: the row operand is read
+// conflict-free across lanes, the column operand is a broadcast.
+#define RS_JB 4
+
+WNLQG_D double2 load_c(const double2 *p) { return *p; }
+template <typename C> WNLQG_D C conv_c(double2 v);
+template <> WNLQG_D double2 conv_c<double2>(double2 v) { return v; }
+template <> WNLQG_D float2 conv_c<float2>(double2 v) { return make_float2((float)v.x, (float)v.y); }
+
+// out = X * Y
+template <typename C> WNLQG_D void mm_xy(const C *X, const C *Y, C *out, int nw, int ld) {
+    const int ng = (nw + RS_JB - 1) / RS_JB;
+    for (int w = threadIdx.x; w < nw * ng; w += blockDim.x) {
+        const int i = w % nw, j0 = (w / nw) * RS_JB;
+        C acc[RS_JB];
+#pragma unroll
+        for (int q = 0; q < RS_JB; ++q) acc[q] = czero<C>();
+        for (int l = 0; l < nw; ++l) {
+            const C x = X[i + ld * l];
+#pragma unroll
+            for (int q = 0; q < RS_JB; ++q)
+                if (j0 + q < nw) acc[q] = cfma(x, Y[l + ld * (j0 + q)], acc[q]);
+        }
+#pragma unroll
+        for (int q = 0; q < RS_JB; ++q)
+            if (j0 + q < nw) out[i + ld * (j0 + q)] = acc[q];
+    }
+}
+
+// out = X^H * Y
+template <typename C> WNLQG_D void mm_xhy(const C *X, const C *Y, C *out, int nw, int ld) {
+    const int ng = (nw + RS_JB - 1) / RS_JB;
+    for (int w = threadIdx.x; w < nw * ng; w += blockDim.x) {
+        const int i = w % nw, j0 = (w / nw) * RS_JB;
+        C acc[RS_JB];
+#pragma unroll
+        for (int q = 0; q < RS_JB; ++q) acc[q] = czero<C>();
+        for (int l = 0; l < nw; ++l) {
+            const C x = X[l + ld * i];
+#pragma unroll
+            for (int q = 0; q < RS_JB; ++q)
+                if (j0 + q < nw) acc[q] = cfmaconj(x, Y[l + ld * (j0 + q)], acc[q]);
+        }
+#pragma unroll
+        for (int q = 0; q < RS_JB; ++q)
+            if (j0 + q < nw) out[i + ld * (j0 + q)] = acc[q];
+    }
+}
+
+// out = X * Y - Y * X
+template <typename C> WNLQG_D void mm_comm(const C *X, const C *Y, C *out, int nw, int ld) {
+    const int ng = (nw + RS_JB - 1) / RS_JB;
+    for (int w = threadIdx.x; w < nw * ng; w += blockDim.x) {
+        const int i = w % nw, j0 = (w / nw) * RS_JB;
+        C acc[RS_JB];
+#pragma unroll
+        for (int q = 0; q < RS_JB; ++q) acc[q] = czero<C>();
+        for (int l = 0; l < nw; ++l) {
+            const C x = X[i + ld * l], y = Y[i + ld * l];
+#pragma unroll
+            for (int q = 0; q < RS_JB; ++q)
+                if (j0 + q < nw) {
+                    acc[q] = cfma(x, Y[l + ld * (j0 + q)], acc[q]);
+                    const C xl = X[l + ld * (j0 + q)];
+                    acc[q] = cfma(make_neg(y), xl, acc[q]);
+                }
+        }
+#pragma unroll
+        for (int q = 0; q < RS_JB; ++q)
+            if (j0 + q < nw) out[i + ld * (j0 + q)] = acc[q];
+    }
+}
+
+// dst = U^H X U for a Wannier-gauge matrix X in global memory (FP64, column-major nw x nw).
+// dst may alias T1.
+template <typename C>
+WNLQG_D void rotate_to_hamiltonian(const double2 *__restrict__ src, C *T1, C *T2, const C *U, C *dst, int nw, int ld) {
     const int nn = nw * nw;
-    for (int e = threadIdx.x; e < nn; e += blockDim.x) {
-        int i = e % nw, j = e / nw;
-        T1[i + ld * j] = src[e];
-    }
+    for (int e = threadIdx.x; e < nn; e += blockDim.x) T1[(e % nw) + ld * (e / nw)] = conv_c<C>(src[e]);
     __syncthreads();
-    for (int e = threadIdx.x; e < nn; e += blockDim.x) {
-        int i = e % nw, j = e / nw;
-        double2 acc = make_double2(0.0, 0.0);
-        for (int l = 0; l < nw; ++l) acc = cfma(T1[i + ld * l], U[l + ld * j], acc);
-        T2[i + ld * j] = acc;
-    }
+    mm_xy(T1, U, T2, nw, ld);
     __syncthreads();
-    for (int e = threadIdx.x; e < nn; e += blockDim.x) {
-        int i = e % nw, j = e / nw;
+    mm_xhy(U, T2, dst, nw, ld);
+    __syncthreads();
+}
+
+// diag[n] = (U^H X U)_nn; uses T1, T2.
+template <typename C>
+WNLQG_D void rotate_diagonal(const double2 *__restrict__ src, C *T1, C *T2, const C *U, double2 *diag, int nw, int ld) {
+    const int nn = nw * nw;
+    for (int e = threadIdx.x; e < nn; e += blockDim.x) T1[(e % nw) + ld * (e / nw)] = conv_c<C>(src[e]);
+    __syncthreads();
+    mm_xy(T1, U, T2, nw, ld);
+    __syncthreads();
+    for (int n = threadIdx.x; n < nw; n += blockDim.x) {
         double2 acc = make_double2(0.0, 0.0);
-        for (int l = 0; l < nw; ++l) acc = cfmaconj(U[l + ld * i], T2[l + ld * j], acc);
-        dst[i + ld * j] = acc;
+        for (int l = 0; l < nw; ++l) acc = cfmaconj(to_c64(U[l + ld * n]), to_c64(T2[l + ld * n]), acc);
+        diag[n] = acc;
     }
     __syncthreads();
 }
@@ -160,124 +237,138 @@ WNLQG_D bool any_within(double te, double half, const RespParams &p) {
     return false;
 }
 
-__global__ void __launch_bounds__(256) response_kernel_f64(RespParams p) {
+#define RS_OMB 4   // photon energies per thread per pass of the pair loop
+
+// R: storage/arithmetic type of the per-k matrices (double: plain FP64 path; float: mixed path).
+// Energies, inverse energy differences, occupations and every accumulation across pairs of a
+// scalar response and across k-points stay FP64.
+template <typename R>
+__global__ void __launch_bounds__(256) response_kernel(RespParams p) {
+    typedef typename cplx_of<R>::type C;
     extern __shared__ __align__(16) unsigned char sm[];
     const int nw = p.nw, ld = p.ld, nn = nw * nw;
-    const RespSmem L = RespSmem::layout(nw, p.n_slots, p.n_fc, 1, sizeof(double2));
-    double2 *sU = reinterpret_cast<double2 *>(sm + L.U);
-    double2 *T1 = reinterpret_cast<double2 *>(sm + L.T1);
-    double2 *T2 = reinterpret_cast<double2 *>(sm + L.T2);
-    double2 *slots = reinterpret_cast<double2 *>(sm + L.slots);
+    const RespSmem L = RespSmem::layout(nw, p.n_slots, p.n_fc, 1, sizeof(C));
+    C *sU = reinterpret_cast<C *>(sm + L.U);
+    C *T1 = reinterpret_cast<C *>(sm + L.T1);
+    C *T2 = reinterpret_cast<C *>(sm + L.T2);
+    C *slots = reinterpret_cast<C *>(sm + L.slots);
     double *sinv = reinterpret_cast<double *>(sm + L.inv);
     double *sE = reinterpret_cast<double *>(sm + L.E);
     double *sf = reinterpret_cast<double *>(sm + L.f);
     double *ste = reinterpret_cast<double *>(sm + L.te);
     double *sfnm = reinterpret_cast<double *>(sm + L.fnm);
-    double2 *sQ = reinterpret_cast<double2 *>(sm + L.Q);
+    C *sQ = reinterpret_cast<C *>(sm + L.Q);
     double2 *sFd = reinterpret_cast<double2 *>(sm + L.fd);
     double *red = reinterpret_cast<double *>(sm + L.red);
     int *ired = reinterpret_cast<int *>(red + 64);
     const size_t matsz = (size_t)nw * ld;
     auto slot = [&](int s) { return slots + matsz * s; };
+    // r_a[n,m] = A_a[n,m] + i D_a[n,m], D_a = -dH_a .* inv
+    auto r_elem = [&](int a, int n, int m) -> C {
+        const C A = slot(p.slot_A[a])[n + ld * m];
+        const C H = slot(p.slot_dH[a])[n + ld * m];
+        const R s = (R)(-sinv[n + nw * m]);
+        return cadd(A, cmuli(cscale(H, s)));
+    };
 
     const int64_t kb = (p.batch * blockIdx.x) / gridDim.x;
     const int64_t ke = (p.batch * (blockIdx.x + 1)) / gridDim.x;
     for (int64_t b = kb; b < ke; ++b) {
         const double2 *xw = p.xw + b * p.xw_stride;
         const double wk = p.weights ? p.weights[b] * p.scale : p.scale;
-        for (int e = threadIdx.x; e < nn; e += blockDim.x) {
-            int i = e % nw, j = e / nw;
-            sU[i + ld * j] = p.U[b * nn + e];
-        }
+        for (int e = threadIdx.x; e < nn; e += blockDim.x) sU[(e % nw) + ld * (e / nw)] = conv_c<C>(p.U[b * nn + e]);
         for (int i = threadIdx.x; i < nw; i += blockDim.x) {
-            double e = p.E[b * nw + i];
+            const double e = p.E[b * nw + i];
             sE[i] = e;
             sf[i] = fermi_occ(e, p.mu, p.kT);
         }
         __syncthreads();
         for (int e = threadIdx.x; e < nn; e += blockDim.x) {
-            int i = e % nw, j = e / nw;
-            double d = sE[i] - sE[j];
+            const int i = e % nw, j = e / nw;
+            const double d = sE[i] - sE[j];
             sinv[e] = p.eta_reg == 0.0 ? (d == 0.0 ? 0.0 : 1.0 / d) : reg_inverse(d, p.eta_reg);
         }
         for (int a = 0; a < 3; ++a)
             if (p.slot_dH[a] >= 0) rotate_to_hamiltonian(xw + (int64_t)p.ch_dH[a] * nn, T1, T2, sU, slot(p.slot_dH[a]), nw, ld);
         for (int a = 0; a < 3; ++a)
             if (p.slot_A[a] >= 0) rotate_to_hamiltonian(xw + (int64_t)p.ch_A[a] * nn, T1, T2, sU, slot(p.slot_A[a]), nw, ld);
+        // Gauge corrections D_d = -dH_d .* inv for the derivative axes of the generalised derivatives.
+        for (int a = 0; a < 3; ++a)
+            if (p.slot_D[a] >= 0) {
+                C *D = slot(p.slot_D[a]);
+                const C *H = slot(p.slot_dH[a]);
+                for (int e = threadIdx.x; e < nn; e += blockDim.x) {
+                    const int i = e % nw, j = e / nw;
+                    D[i + ld * j] = cscale(H[i + ld * j], (R)(-sinv[e]));
+                }
+            }
+        __syncthreads();
 
-        // Generalised derivatives r^p_{nm;d} (ConventionalShiftCurrent.jl:191-229).
+        // Generalised derivatives r^p_{nm;d} (ConventionalShiftCurrent.jl:191-229), with the
+        // l != n,m sums written as commutators (exact: D_nn = 0):
+        //   sum_AD + AD_bit = [A_p, D_d]_nm + (A_d,nn - A_d,mm) D_p,nm
+        //   sum_HD + DV_bit = [dH_p, D_d]_nm + (dH_d,nn - dH_d,mm) D_p,nm
         for (int g = 0; g < p.n_g; ++g) {
             const int pp = p.g_p[g], dd = p.g_d[g];
-            double2 *G = slot(p.g_slot[g]);
+            C *G = slot(p.g_slot[g]);
             rotate_to_hamiltonian(xw + (int64_t)p.ch_dA[pp * 3 + dd] * nn, T1, T2, sU, G, nw, ld);
             rotate_to_hamiltonian(xw + (int64_t)p.ch_ddH[pp * 3 + dd] * nn, T1, T2, sU, T1, nw, ld);
-            const double2 *Ap = slot(p.slot_A[pp]), *Ad = slot(p.slot_A[dd]);
-            const double2 *Hp = slot(p.slot_dH[pp]), *Hd = slot(p.slot_dH[dd]);
+            const C *Ap = slot(p.slot_A[pp]), *Ad = slot(p.slot_A[dd]);
+            const C *Hp = slot(p.slot_dH[pp]), *Hd = slot(p.slot_dH[dd]);
+            const C *Dd = slot(p.slot_D[dd]);
+            mm_comm(Ap, Dd, T2, nw, ld);
+            __syncthreads();
             for (int e = threadIdx.x; e < nn; e += blockDim.x) {
                 const int n = e % nw, m = e / nw;
-                double2 sum_AD = make_double2(0.0, 0.0), sum_HD = make_double2(0.0, 0.0);
-                for (int l = 0; l < nw; ++l) {
-                    if (l == n || l == m) continue;
-                    // D_d[l,m] = -dH_d[l,m] inv[l,m];  D_d[n,l] = -dH_d[n,l] inv[n,l]
-                    double2 Dlm = cscale(Hd[l + ld * m], -sinv[l + nw * m]);
-                    double2 Dnl = cscale(Hd[n + ld * l], -sinv[n + nw * l]);
-                    sum_AD = cadd(sum_AD, csub(cmul(Ap[n + ld * l], Dlm), cmul(Dnl, Ap[l + ld * m])));
-                    sum_HD = cadd(sum_HD, csub(cmul(Hp[n + ld * l], Dlm), cmul(Dnl, Hp[l + ld * m])));
-                }
-                const double inm = sinv[n + nw * m];
-                double2 Da = cscale(Hp[n + ld * m], -inm);   // D_p[n,m]
-                double2 Db = cscale(Hd[n + ld * m], -inm);   // D_d[n,m]
-                double2 dAdn = csub(Ad[n + ld * n], Ad[m + ld * m]);
-                double2 dApn = csub(Ap[n + ld * n], Ap[m + ld * m]);
-                double2 AD_bit = cadd(cmul(dAdn, Da), cmul(dApn, Db));
-                double2 AA_bit = cmul(dAdn, Ap[n + ld * m]);
-                double2 DV_bit = cadd(cmul(csub(Hd[n + ld * n], Hd[m + ld * m]), Da),
-                                      cmul(csub(Hp[n + ld * n], Hp[m + ld * m]), Db));
-                double2 h = cadd(cadd(T1[n + ld * m], sum_HD), DV_bit);
-                double2 v = cadd(cadd(G[n + ld * m], AD_bit), csub(sum_AD, cmuli(AA_bit)));
-                v = cadd(v, cmuli(cscale(h, -inm)));
-                G[n + ld * m] = v;
+                const int o = n + ld * m;
+                const C Dp = cscale(Hp[o], (R)(-sinv[e]));
+                const C dAd = csub(Ad[n + ld * n], Ad[m + ld * m]);
+                const C dHd = csub(Hd[n + ld * n], Hd[m + ld * m]);
+                // G <- dA + (A_d,nn - A_d,mm)(D_p - i A_p) + [A_p, D_d]
+                G[o] = cadd(cadd(G[o], cmul(dAd, csub(Dp, cmuli(Ap[o])))), T2[o]);
+                // T1 <- ddH + (dH_d,nn - dH_d,mm) D_p
+                T1[o] = cadd(T1[o], cmul(dHd, Dp));
+            }
+            __syncthreads();
+            mm_comm(Hp, Dd, T2, nw, ld);
+            __syncthreads();
+            for (int e = threadIdx.x; e < nn; e += blockDim.x) {
+                const int n = e % nw, m = e / nw;
+                const int o = n + ld * m;
+                const C h = cadd(T1[o], T2[o]);
+                G[o] = cadd(G[o], cmuli(cscale(h, (R)(-sinv[e]))));
             }
             __syncthreads();
         }
 
-        // Scalar responses.
+        // Scalar responses (FP64 block sums).
         for (int s = 0; s < p.n_sc; ++s) {
             const int a = p.sc_a[s], bb = p.sc_b[s];
-            const double2 *Aa = slot(p.slot_A[a]), *Ab = slot(p.slot_A[bb]);
-            const double2 *Ha = slot(p.slot_dH[a]), *Hb = slot(p.slot_dH[bb]);
-            double local = 0.0;
             if (p.sc_kind[s] == RS_SC_BERRY) {
-                // Diagonals of U^H (dA_b/dk_a) U (kept in sFd) and U^H (dA_a/dk_b) U (left in T1).
-                rotate_to_hamiltonian(xw + (int64_t)p.ch_dA[bb * 3 + a] * nn, T1, T2, sU, T1, nw, ld);
-                for (int n = threadIdx.x; n < nw; n += blockDim.x) sFd[n] = T1[n + ld * n];
-                __syncthreads();
-                rotate_to_hamiltonian(xw + (int64_t)p.ch_dA[a * 3 + bb] * nn, T1, T2, sU, T1, nw, ld);
+                // F_nn = (U' dA_b/dk_a U)_nn - (U' dA_a/dk_b U)_nn - i [A_a, A_b]_nn
+                rotate_diagonal(xw + (int64_t)p.ch_dA[bb * 3 + a] * nn, T1, T2, sU, sFd, nw, ld);
+                rotate_diagonal(xw + (int64_t)p.ch_dA[a * 3 + bb] * nn, T1, T2, sU, sFd + nw, nw, ld);
             }
+            double local = 0.0;
             for (int e = threadIdx.x; e < nn; e += blockDim.x) {
                 const int n = e % nw, m = e / nw;
-                const double inm = sinv[e];
-                double2 ra = cadd(Aa[n + ld * m], cmuli(cscale(Ha[n + ld * m], -inm)));
-                const double imn = sinv[m + nw * n];
-                double2 rb = cadd(Ab[m + ld * n], cmuli(cscale(Hb[m + ld * n], -imn)));
                 if (p.sc_kind[s] == RS_SC_BERRY) {
                     if (n == m) {
-                        // F_nn = (U'dA_b/dk_a U)_nn - (U'dA_a/dk_b U)_nn - i sum_l (A_a[n,l]A_b[l,n] - A_b[n,l]A_a[l,n])
-                        double2 fnn = csub(sFd[n], T1[n + ld * n]);
                         double2 comm = make_double2(0.0, 0.0);
+                        const C *Aa = slot(p.slot_A[a]), *Ab = slot(p.slot_A[bb]);
                         for (int l = 0; l < nw; ++l)
-                            comm = cadd(comm, csub(cmul(Aa[n + ld * l], Ab[l + ld * n]), cmul(Ab[n + ld * l], Aa[l + ld * n])));
-                        fnn = csub(fnn, cmuli(comm));
+                            comm = cadd(comm, to_c64(csub(cmul(Aa[n + ld * l], Ab[l + ld * n]), cmul(Ab[n + ld * l], Aa[l + ld * n]))));
+                        const double2 fnn = csub(csub(sFd[n], sFd[nw + n]), cmuli(comm));
                         local += sf[n] * fnn.x;
                     } else {
-                        double2 t = cmuli(cmul(ra, rb));
+                        const double2 t = cmuli(to_c64(cmul(r_elem(a, n, m), r_elem(bb, m, n))));
                         local += (sf[n] - sf[m]) * t.x;
                     }
                 } else if (n != m) {
-                    local += 0.5 * (sf[n] + sf[m]) * cmul(ra, rb).x;
+                    local += 0.5 * (sf[n] + sf[m]) * (double)cmul(r_elem(a, n, m), r_elem(bb, m, n)).x;
                 }
             }
-            double total = block_sum(local, red);
+            const double total = block_sum(local, red);
             if (threadIdx.x == 0) {
                 if (p.mode == 0) {
                     double *acc = p.partials + ((int64_t)blockIdx.x * p.vc + p.sc_out[s]) * 4;
@@ -289,7 +380,7 @@ __global__ void __launch_bounds__(256) response_kernel_f64(RespParams p) {
         }
 
         if (p.n_fc > 0) {
-            // Transition screen and per-pair kernels, pairs in column-major (n fastest) order.
+            // Transition screen and per-pair kernels; pairs kept in column-major (n fastest) order.
             if (threadIdx.x == 0) { ired[0] = 0; ired[1] = 0; }
             __syncthreads();
             for (int base = 0; base < nn; base += blockDim.x) {
@@ -301,8 +392,7 @@ __global__ void __launch_bounds__(256) response_kernel_f64(RespParams p) {
                     n = e % nw; m = e / nw;
                     fnm = sf[n] - sf[m];
                     te = sE[m] - sE[n];
-                    const bool occ = fabs(fnm) > 1.0e-10;
-                    if (occ) {
+                    if (fabs(fnm) > 1.0e-10) {
                         if (p.gaussian) {
                             keep = any_within(te, p.cutoff, p);
                             if (keep) ired[1] = 1;
@@ -312,9 +402,8 @@ __global__ void __launch_bounds__(256) response_kernel_f64(RespParams p) {
                         }
                     }
                 }
-                // Ordered compaction: warp ballots, warps in order.
-                unsigned ball = __ballot_sync(0xffffffffu, keep);
-                int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+                const unsigned ball = __ballot_sync(0xffffffffu, keep);
+                const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
                 if (lane == 0) ired[8 + wid] = __popc(ball);
                 __syncthreads();
                 int before = ired[0];
@@ -325,19 +414,14 @@ __global__ void __launch_bounds__(256) response_kernel_f64(RespParams p) {
                     sfnm[before] = fnm;
                     for (int c = 0; c < p.n_fc; ++c) {
                         const int a = p.fc_a[c], bb = p.fc_b[c], cc = p.fc_c[c];
-                        const double2 *Ab = slot(p.slot_A[bb]), *Ac = slot(p.slot_A[cc]);
-                        const double2 *Hb = slot(p.slot_dH[bb]), *Hc = slot(p.slot_dH[cc]);
-                        // r_c[n,m] and r_b[m,n]
-                        double2 rc_nm = cadd(Ac[n + ld * m], cmuli(cscale(Hc[n + ld * m], -sinv[n + nw * m])));
-                        double2 rb_mn = cadd(Ab[m + ld * n], cmuli(cscale(Hb[m + ld * n], -sinv[m + nw * n])));
-                        double2 q;
+                        const C rc_nm = r_elem(cc, n, m), rb_mn = r_elem(bb, m, n);
+                        C q;
                         if (p.fc_kind[c] == RS_FC_SHIFT) {
-                            const double2 *G1 = slot(p.g_slot[p.fc_g1[c]]), *G2 = slot(p.g_slot[p.fc_g2[c]]);
+                            const C *G1 = slot(p.g_slot[p.fc_g1[c]]), *G2 = slot(p.g_slot[p.fc_g2[c]]);
                             q = cmulmi(csub(cmul(G1[n + ld * m], rb_mn), cmul(G2[m + ld * n], rc_nm)));
                         } else {
-                            const double2 *Ha = slot(p.slot_dH[a]);
-                            double2 vd = csub(Ha[m + ld * m], Ha[n + ld * n]);
-                            q = cmul(cmul(vd, rc_nm), rb_mn);
+                            const C *Ha = slot(p.slot_dH[a]);
+                            q = cmul(cmul(csub(Ha[m + ld * m], Ha[n + ld * n]), rc_nm), rb_mn);
                         }
                         sQ[(size_t)c * nn + before] = q;
                     }
@@ -352,41 +436,70 @@ __global__ void __launch_bounds__(256) response_kernel_f64(RespParams p) {
             }
             const int npairs = ired[0];
             const bool active = ired[1] != 0;
-            for (int w = threadIdx.x; w < p.nom; w += blockDim.x) {
-                const double om = p.omegas[w];
-                double2 acc[RS_MAX_FREQ];
-                for (int c = 0; c < RS_MAX_FREQ; ++c) acc[c] = make_double2(0.0, 0.0);
-                if (active) {
-                    for (int q = 0; q < npairs; ++q) {
-                        const double x = ste[q] - om;
-                        double delta;
-                        if (p.gaussian) {
-                            if (!(fabs(x) < p.cutoff)) continue;
-                            const double y = x / p.width;
-                            delta = p.gscale * exp(-y * y);
-                        } else {
-                            delta = (p.width / WNLQG_PI) / (x * x + p.width * p.width);
-                        }
-                        const double weight = sfnm[q] * delta;
-                        if (weight == 0.0) continue;
-                        for (int c = 0; c < p.n_fc; ++c) {
-                            const double cw = p.fc_pref[c] * weight;
-                            const double2 qq = sQ[(size_t)c * nn + q];
-                            acc[c].x = fma(cw, qq.x, acc[c].x);
-                            acc[c].y = fma(cw, qq.y, acc[c].y);
+            // Frequency contraction: each thread owns up to RS_OMB photon energies per pass and
+            // streams the pair list once per pass.
+            const R w2 = (R)(p.width * p.width), lor = (R)(p.width / WNLQG_PI);
+            const R gsc = (R)p.gscale, cut = (R)p.cutoff, invw = (R)(1.0 / p.width);
+            for (int w0 = 0; w0 < p.nom; w0 += RS_OMB * blockDim.x) {
+                double om[RS_OMB];
+#pragma unroll
+                for (int j = 0; j < RS_OMB; ++j) {
+                    const int w = w0 + threadIdx.x + j * blockDim.x;
+                    om[j] = w < p.nom ? p.omegas[w] : 0.0;
+                }
+                // Components in chunks of two keep the accumulators in registers.
+                for (int c0 = 0; c0 < p.n_fc; c0 += 2) {
+                    const bool two = c0 + 1 < p.n_fc;
+                    C acc[RS_OMB][2];
+#pragma unroll
+                    for (int j = 0; j < RS_OMB; ++j) { acc[j][0] = czero<C>(); acc[j][1] = czero<C>(); }
+                    if (active) {
+                        const C *Q0 = sQ + (size_t)c0 * nn;
+                        const C *Q1 = sQ + (size_t)(two ? c0 + 1 : c0) * nn;
+                        for (int q = 0; q < npairs; ++q) {
+                            const double te = ste[q];
+                            const R fq = (R)sfnm[q];
+                            const C q0 = Q0[q], q1 = Q1[q];
+#pragma unroll
+                            for (int j = 0; j < RS_OMB; ++j) {
+                                const R x = (R)(te - om[j]);
+                                R delta;
+                                if (p.gaussian) {
+                                    if (!(fabs(x) < cut)) continue;
+                                    const R y = x * invw;
+                                    delta = gsc * exp(-y * y);
+                                } else {
+                                    delta = lor / (x * x + w2);
+                                }
+                                const R weight = fq * delta;
+                                if (weight == (R)0) continue;
+                                acc[j][0].x = fma(weight, q0.x, acc[j][0].x);
+                                acc[j][0].y = fma(weight, q0.y, acc[j][0].y);
+                                acc[j][1].x = fma(weight, q1.x, acc[j][1].x);
+                                acc[j][1].y = fma(weight, q1.y, acc[j][1].y);
+                            }
                         }
                     }
-                }
-                for (int c = 0; c < p.n_fc; ++c) {
-                    const int64_t idx = p.fc_out[c] + w;
-                    if (p.mode == 0) {
-                        if (active) {
-                            double *a4 = p.partials + ((int64_t)blockIdx.x * p.vc + idx) * 4;
-                            neumaier_add(a4[0], a4[2], acc[c].x * wk);
-                            neumaier_add(a4[1], a4[3], acc[c].y * wk);
+#pragma unroll
+                    for (int j = 0; j < RS_OMB; ++j) {
+                        const int w = w0 + threadIdx.x + j * blockDim.x;
+                        if (w >= p.nom) continue;
+#pragma unroll
+                        for (int cc = 0; cc < 2; ++cc) {
+                            if (cc == 1 && !two) continue;
+                            const int c = c0 + cc;
+                            const int64_t idx = p.fc_out[c] + w;
+                            const double2 v = cscale(to_c64(acc[j][cc]), p.fc_pref[c]);
+                            if (p.mode == 0) {
+                                if (active) {
+                                    double *a4 = p.partials + ((int64_t)blockIdx.x * p.vc + idx) * 4;
+                                    neumaier_add(a4[0], a4[2], v.x * wk);
+                                    neumaier_add(a4[1], a4[3], v.y * wk);
+                                }
+                            } else {
+                                p.out_points[(p.point_offset + b) * p.vc + idx] = cscale(v, p.scale);
+                            }
                         }
-                    } else {
-                        p.out_points[(p.point_offset + b) * p.vc + idx] = cscale(acc[c], p.scale);
                     }
                 }
             }

@@ -175,8 +175,12 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
 
     // The dynamic shared-memory ceiling is a per-function attribute: raise it once to the device
     // maximum so that passes of different sizes can all launch.
+    const bool mixed = t.precision == WNLQG_PRECISION_MIXED;
+    const int csize = mixed ? (int)sizeof(float2) : (int)sizeof(double2);
     {
-        cudaError_t e = cudaFuncSetAttribute(response_kernel_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_limit);
+        cudaError_t e = cudaFuncSetAttribute(response_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_limit);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(response_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_limit);
         if (e != cudaSuccess) return fail(WNLQG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
     }
     size_t i = 0;
@@ -186,9 +190,12 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
         std::memset(&p, 0, sizeof(p));
         p.nw = pl->nw;
         p.ld = pl->nw + 1;
-        for (int a = 0; a < 3; ++a) { p.slot_dH[a] = -1; p.slot_A[a] = -1; p.ch_dH[a] = pl->ch_dH[a]; p.ch_A[a] = pl->ch_A[a]; }
+        for (int a = 0; a < 3; ++a) {
+            p.slot_dH[a] = -1; p.slot_A[a] = -1; p.slot_D[a] = -1;
+            p.ch_dH[a] = pl->ch_dH[a]; p.ch_A[a] = pl->ch_A[a];
+        }
         for (int a = 0; a < 9; ++a) { p.ch_ddH[a] = pl->ch_ddH[a]; p.ch_dA[a] = pl->ch_dA[a]; }
-        bool needH[3] = {false, false, false}, needA[3] = {false, false, false};
+        bool needH[3] = {false, false, false}, needA[3] = {false, false, false}, needD[3] = {false, false, false};
         std::vector<std::pair<int, int>> gl;
         auto gindex = [&](int pp, int dd, bool commit) {
             for (size_t g = 0; g < gl.size(); ++g)
@@ -201,14 +208,16 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
         while (i < items.size()) {
             const Item &it = items[i];
             // Tentatively add the item and check limits.
-            bool tH[3], tA[3];
+            bool tH[3], tA[3], tD[3];
             std::copy(needH, needH + 3, tH);
             std::copy(needA, needA + 3, tA);
+            std::copy(needD, needD + 3, tD);
             int newg = 0;
             auto need_r = [&](int a) { tH[a] = true; tA[a] = true; };
             bool freq = it.kind == WNLQG_SHIFT_CURRENT || it.kind == WNLQG_INJECTION_CURRENT;
             if (it.kind == WNLQG_SHIFT_CURRENT) {
                 need_r(it.a); need_r(it.b); need_r(it.c);
+                tD[it.a] = true;
                 if (gindex(it.c, it.a, false) == (int)gl.size()) ++newg;
                 if (!(it.b == it.c) && gindex(it.b, it.a, false) == (int)gl.size()) ++newg;
             } else if (it.kind == WNLQG_INJECTION_CURRENT) {
@@ -217,10 +226,10 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
                 need_r(it.a); need_r(it.b);
             }
             int nslots = (int)gl.size() + newg;
-            for (int a = 0; a < 3; ++a) nslots += (tH[a] ? 1 : 0) + (tA[a] ? 1 : 0);
+            for (int a = 0; a < 3; ++a) nslots += (tH[a] ? 1 : 0) + (tA[a] ? 1 : 0) + (tD[a] ? 1 : 0);
             int nfc = p.n_fc + (freq ? 1 : 0);
             int nsc = p.n_sc + (freq ? 0 : 1);
-            size_t smem = RespSmem::layout(pl->nw, nslots, nfc, 1, sizeof(double2)).total;
+            size_t smem = RespSmem::layout(pl->nw, nslots, nfc, 1, csize).total;
             bool fits = nfc <= RS_MAX_FREQ && nsc <= RS_MAX_SCALAR && (int)gl.size() + newg <= RS_MAX_G && smem <= smem_limit;
             if (!fits) {
                 if (i == start)
@@ -230,6 +239,7 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
             }
             std::copy(tH, tH + 3, needH);
             std::copy(tA, tA + 3, needA);
+            std::copy(tD, tD + 3, needD);
             if (it.kind == WNLQG_SHIFT_CURRENT) {
                 int g1 = gindex(it.c, it.a, true);
                 int g2 = gindex(it.b, it.a, true);
@@ -250,6 +260,7 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
         int slot = 0;
         for (int a = 0; a < 3; ++a) if (needH[a]) p.slot_dH[a] = slot++;
         for (int a = 0; a < 3; ++a) if (needA[a]) p.slot_A[a] = slot++;
+        for (int a = 0; a < 3; ++a) if (needD[a]) p.slot_D[a] = slot++;
         p.n_g = (int)gl.size();
         for (int g = 0; g < p.n_g; ++g) { p.g_p[g] = gl[g].first; p.g_d[g] = gl[g].second; p.g_slot[g] = slot++; }
         p.n_slots = slot;
@@ -268,10 +279,11 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
         p.eta_reg = t.denominator_regularization;
         p.vc = pl->vc;
         p.xw_stride = (int64_t)pl->C * pl->nn;
-        ps.smem = RespSmem::layout(pl->nw, p.n_slots, p.n_fc, 1, sizeof(double2)).total;
+        ps.smem = RespSmem::layout(pl->nw, p.n_slots, p.n_fc, 1, csize).total;
         ps.threads = response_threads(pl->nw);
         int per_sm = 0;
-        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, response_kernel_f64, ps.threads, ps.smem);
+        cudaError_t e = mixed ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, response_kernel<float>, ps.threads, ps.smem)
+                              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, response_kernel<double>, ps.threads, ps.smem);
         if (e != cudaSuccess) return fail(WNLQG_ERR_CUDA, std::string("occupancy query: ") + cudaGetErrorString(e));
         if (per_sm < 1) return fail(WNLQG_ERR_UNSUPPORTED, "response kernel cannot be resident with its shared memory");
         ps.grid = sm_count * per_sm;
@@ -360,7 +372,10 @@ wnlqg_status run_passes(wnlqg_plan *pl, int64_t nb, int mode, double scale, int6
         p.partials = pl->d_partials;
         p.out_points = pl->d_points;
         p.point_offset = point_offset;
-        response_kernel_f64<<<ps.grid, ps.threads, ps.smem, pl->stream>>>(p);
+        if (pl->task.precision == WNLQG_PRECISION_MIXED)
+            response_kernel<float><<<ps.grid, ps.threads, ps.smem, pl->stream>>>(p);
+        else
+            response_kernel<double><<<ps.grid, ps.threads, ps.smem, pl->stream>>>(p);
         pl->launches += 1;
     }
     WNLQG_CUDA(cudaGetLastError());
