@@ -187,3 +187,18 @@ def test_mixed_mesh_within_bound(engine_cls, oracle_mod, name, mesh):
     ref = oracle_mod.integrate_mesh(model, task, mesh)
     for g, r in zip(task.split(got), task.split(ref)):
         assert rel_err(g, r) < MIXED_RTOL
+
+
+@pytest.mark.parametrize("name", ["nw4", "nw32"])
+def test_mixed_eigensolver_refined_to_fp64(engine_cls, oracle_mod, name):
+    """FP32 Jacobi + one FP64 Rayleigh-Ritz refinement reaches FP64-level eigenvalues."""
+    model = reference_workload_model(name)
+    task = nw4_task(precision=_abi.PRECISION_MIXED) if name == "nw4" else nw32_task(precision=_abi.PRECISION_MIXED)
+    k = np.random.default_rng(15).random((24, 3))
+    with engine_cls(model, task) as eng:
+        e, u = eng.spectrum(k)
+    for i in range(k.shape[0]):
+        eo, uo, _ = oracle_mod.kpoint_spectrum(model, k[i])
+        assert np.max(np.abs(e[i] - eo)) < 1e-11 * max(1.0, np.abs(eo).max())
+        ov = np.abs(np.sum(u[i].conj() * uo, axis=0))
+        assert np.max(np.abs(ov - 1.0)) < 1e-8

@@ -27,6 +27,118 @@ struct EighSmem {
     }
 };
 
+// One parallel-Jacobi sweep on (A, V) of real type T.  Returns after np-1 rounds; the caller
+// measures convergence.  Pairs are computed by threads tid < np/2.
+template <typename T>
+WNLQG_D void jacobi_sweep(typename cplx_of<T>::type *A, typename cplx_of<T>::type *V, int np, int ld, T tol,
+                          typename cplx_of<T>::type *rot_s, T *rot_c, int *rot_p, int *rot_q) {
+    typedef typename cplx_of<T>::type C;
+    const int half = np / 2;
+    const int tid = threadIdx.x;
+    for (int round = 0; round < np - 1; ++round) {
+        if (tid < half) {
+            int s1 = tid, s2 = np - 1 - tid;
+            int i1 = s1 == 0 ? 0 : ((s1 - 1 + round) % (np - 1)) + 1;
+            int i2 = ((s2 - 1 + round) % (np - 1)) + 1;
+            int p = min(i1, i2), q = max(i1, i2);
+            C apq = A[p + ld * q];
+            T g = (T)hypot((double)apq.x, (double)apq.y);
+            T c = (T)1;
+            C sp = czero<C>();
+            if (g > tol) {
+                T app = A[p + ld * p].x, aqq = A[q + ld * q].x;
+                T theta = (aqq - app) / ((T)2 * g);
+                T t = (theta >= (T)0 ? (T)1 : (T)-1) / (fabs(theta) + sqrt(theta * theta + (T)1));
+                c = (T)1 / sqrt(t * t + (T)1);
+                T s = t * c;
+                sp.x = s * (apq.x / g);
+                sp.y = s * (apq.y / g);
+            }
+            rot_c[tid] = c;
+            rot_s[tid] = sp;
+            rot_p[tid] = p;
+            rot_q[tid] = q;
+        }
+        __syncthreads();
+        const int nblk = half * (half + 1) / 2;
+        for (int w = tid; w < nblk + half * half; w += blockDim.x) {
+            if (w < nblk) {
+                // Upper-triangular block index (k1 <= k2) of the pair grid.
+                int k2 = (int)((sqrtf(8.0f * w + 1.0f) - 1.0f) * 0.5f);
+                while (k2 * (k2 + 1) / 2 > w) --k2;
+                while ((k2 + 1) * (k2 + 2) / 2 <= w) ++k2;
+                const int k1 = w - k2 * (k2 + 1) / 2;
+                const int p1 = rot_p[k1], q1 = rot_q[k1], p2 = rot_p[k2], q2 = rot_q[k2];
+                const T c1 = rot_c[k1], c2 = rot_c[k2];
+                const C s1 = rot_s[k1], s2 = rot_s[k2];
+                const C s2c = cconj(s2), s1c = cconj(s1);
+                C a00 = A[p1 + ld * p2], a01 = A[p1 + ld * q2], a10 = A[q1 + ld * p2], a11 = A[q1 + ld * q2];
+                C t00 = csub(cscale(a00, c2), cmul(a01, s2c));
+                C t01 = cadd(cmul(a00, s2), cscale(a01, c2));
+                C t10 = csub(cscale(a10, c2), cmul(a11, s2c));
+                C t11 = cadd(cmul(a10, s2), cscale(a11, c2));
+                C o00 = csub(cscale(t00, c1), cmul(s1, t10));
+                C o01 = csub(cscale(t01, c1), cmul(s1, t11));
+                C o10 = cadd(cmul(s1c, t00), cscale(t10, c1));
+                C o11 = cadd(cmul(s1c, t01), cscale(t11, c1));
+                if (k1 == k2) {
+                    if (s1.x != (T)0 || s1.y != (T)0) {
+                        o01 = czero<C>();
+                        o10 = czero<C>();
+                    } else {
+                        o10 = cconj(o01);
+                    }
+                    o00.y = (T)0;
+                    o11.y = (T)0;
+                    A[p1 + ld * p2] = o00; A[p1 + ld * q2] = o01; A[q1 + ld * p2] = o10; A[q1 + ld * q2] = o11;
+                } else {
+                    A[p1 + ld * p2] = o00; A[p1 + ld * q2] = o01; A[q1 + ld * p2] = o10; A[q1 + ld * q2] = o11;
+                    // Mirrored block (rows of pair k2, columns of pair k1) = conjugate transpose.
+                    A[p2 + ld * p1] = cconj(o00); A[q2 + ld * p1] = cconj(o01);
+                    A[p2 + ld * q1] = cconj(o10); A[q2 + ld * q1] = cconj(o11);
+                }
+            } else {
+                const int v = w - nblk;
+                const int k1 = v % half, k2 = v / half;
+                const int p1 = rot_p[k1], q1 = rot_q[k1], p2 = rot_p[k2], q2 = rot_q[k2];
+                const T c2 = rot_c[k2];
+                const C s2 = rot_s[k2], s2c = cconj(s2);
+                C v00 = V[p1 + ld * p2], v01 = V[p1 + ld * q2], v10 = V[q1 + ld * p2], v11 = V[q1 + ld * q2];
+                V[p1 + ld * p2] = csub(cscale(v00, c2), cmul(v01, s2c));
+                V[p1 + ld * q2] = cadd(cmul(v00, s2), cscale(v01, c2));
+                V[q1 + ld * p2] = csub(cscale(v10, c2), cmul(v11, s2c));
+                V[q1 + ld * q2] = cadd(cmul(v10, s2), cscale(v11, c2));
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Off-diagonal Frobenius norm (fixed-order block reduction); all threads get the value.
+template <typename C>
+WNLQG_D double offdiag_norm(const C *A, int np, int ld, double *red) {
+    double local = 0.0;
+    for (int e = threadIdx.x; e < np * np; e += blockDim.x) {
+        const int i = e % np, j = e / np;
+        if (i != j) {
+            const double2 z = to_c64(A[i + ld * j]);
+            local += z.x * z.x + z.y * z.y;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xffffffffu, local, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = local;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+        red[40] = sqrt(s);
+    }
+    __syncthreads();
+    const double r = red[40];
+    __syncthreads();
+    return r;
+}
+
 // T: real type of the iteration (double for the FP64 path, float for the mixed path).
 // Input H(k) for batch entry b at h_in + b*h_stride (complex double, column-major nw x nw).
 // Outputs: energies E[b*nw + n] (double) and U[b*nw*nw + i + nw*n] (complex double).
@@ -45,8 +157,7 @@ __global__ void jacobi_eigh_kernel(const double2 *__restrict__ h_in, int64_t h_s
     T *rot_c = reinterpret_cast<T *>(scratch + 2);           // c per pair
     int *rot_p = reinterpret_cast<int *>(rot_c + half);
     int *rot_q = rot_p + half;
-    __shared__ int any_rotation;
-    __shared__ double red[32];
+    __shared__ double red[48];
 
     const int tid = threadIdx.x;
     for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) {
@@ -77,73 +188,8 @@ __global__ void jacobi_eigh_kernel(const double2 *__restrict__ h_in, int64_t h_s
         const T tol = (T)scratch[0];
 
         for (int sweep = 0; sweep < WNLQG_JACOBI_MAX_SWEEPS; ++sweep) {
-            if (tid == 0) any_rotation = 0;
-            __syncthreads();
-            for (int round = 0; round < np - 1; ++round) {
-                if (tid < half) {
-                    // Circle method: slot 0 holds index 0, slots 1..np-1 hold ((j-1+round) mod (np-1)) + 1.
-                    int s1 = tid, s2 = np - 1 - tid;
-                    int i1 = s1 == 0 ? 0 : ((s1 - 1 + round) % (np - 1)) + 1;
-                    int i2 = ((s2 - 1 + round) % (np - 1)) + 1;
-                    int p = min(i1, i2), q = max(i1, i2);
-                    C apq = A[p + ld * q];
-                    T g = (T)hypot((double)apq.x, (double)apq.y);
-                    T c = (T)1, s = (T)0;
-                    C ph = from_c64<C>(make_double2(1.0, 0.0));
-                    if (g > tol) {
-                        T app = A[p + ld * p].x, aqq = A[q + ld * q].x;
-                        T theta = (aqq - app) / ((T)2 * g);
-                        T t = (theta >= (T)0 ? (T)1 : (T)-1) / (fabs(theta) + sqrt(theta * theta + (T)1));
-                        c = (T)1 / sqrt(t * t + (T)1);
-                        s = t * c;
-                        ph.x = apq.x / g;
-                        ph.y = apq.y / g;
-                        any_rotation = 1;
-                    }
-                    rot_c[tid] = c;
-                    rot_s[tid] = cscale(ph, s);
-                    rot_p[tid] = p;
-                    rot_q[tid] = q;
-                }
-                __syncthreads();
-                for (int blk = tid; blk < half * half; blk += blockDim.x) {
-                    int k1 = blk % half, k2 = blk / half;
-                    int p1 = rot_p[k1], q1 = rot_q[k1], p2 = rot_p[k2], q2 = rot_q[k2];
-                    T c1 = rot_c[k1], c2 = rot_c[k2];
-                    C s1 = rot_s[k1], s2 = rot_s[k2];
-                    C s2c = cconj(s2), s1c = cconj(s1);
-                    // A block rows (p1,q1), cols (p2,q2): J1^H * a * J2.
-                    C a00 = A[p1 + ld * p2], a01 = A[p1 + ld * q2], a10 = A[q1 + ld * p2], a11 = A[q1 + ld * q2];
-                    C t00 = csub(cscale(a00, c2), cmul(a01, s2c));
-                    C t01 = cadd(cmul(a00, s2), cscale(a01, c2));
-                    C t10 = csub(cscale(a10, c2), cmul(a11, s2c));
-                    C t11 = cadd(cmul(a10, s2), cscale(a11, c2));
-                    C o00 = csub(cscale(t00, c1), cmul(s1, t10));
-                    C o01 = csub(cscale(t01, c1), cmul(s1, t11));
-                    C o10 = cadd(cmul(s1c, t00), cscale(t10, c1));
-                    C o11 = cadd(cmul(s1c, t01), cscale(t11, c1));
-                    if (k1 == k2) {
-                        // Diagonal 2x2 block: the rotated pair's coupling is zero by construction.
-                        if (rot_s[k1].x != (T)0 || rot_s[k1].y != (T)0) {
-                            o01 = czero<C>();
-                            o10 = czero<C>();
-                        }
-                        o00.y = (T)0;
-                        o11.y = (T)0;
-                    }
-                    A[p1 + ld * p2] = o00; A[p1 + ld * q2] = o01; A[q1 + ld * p2] = o10; A[q1 + ld * q2] = o11;
-                    // V rows (p1,q1), cols (p2,q2): v * J2.
-                    C v00 = V[p1 + ld * p2], v01 = V[p1 + ld * q2], v10 = V[q1 + ld * p2], v11 = V[q1 + ld * q2];
-                    V[p1 + ld * p2] = csub(cscale(v00, c2), cmul(v01, s2c));
-                    V[p1 + ld * q2] = cadd(cmul(v00, s2), cscale(v01, c2));
-                    V[q1 + ld * p2] = csub(cscale(v10, c2), cmul(v11, s2c));
-                    V[q1 + ld * q2] = cadd(cmul(v10, s2), cscale(v11, c2));
-                }
-                __syncthreads();
-            }
-            int done = any_rotation == 0;
-            __syncthreads();
-            if (done) break;
+            if (offdiag_norm(A, np, ld, red) <= (double)tol) break;
+            jacobi_sweep<T>(A, V, np, ld, tol, rot_s, rot_c, rot_p, rot_q);
         }
         // Ascending order (stable), then phase canonicalisation per column.
         for (int i = tid; i < nw; i += blockDim.x) {
@@ -167,10 +213,160 @@ __global__ void jacobi_eigh_kernel(const double2 *__restrict__ h_in, int64_t h_s
             E_out[b * nw + rank] = (double)di;
             double2 *u = U_out + b * (int64_t)nw * nw + (int64_t)nw * rank;
             for (int r = 0; r < nw; ++r) {
-                double2 v = cmul(to_c64(V[r + ld * i]), phase);
-                if (r == pivot) v.y = 0.0;
-                u[r] = v;
+                u[r] = cmul(to_c64(V[r + ld * i]), phase);
             }
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Mixed-precision eigensolver: FP32 parallel Jacobi to FP32 accuracy, then one FP64
+// Rayleigh-Ritz refinement: H' = V^H H V in FP64 (V the FP32 eigenvectors promoted) followed
+// by FP64 Jacobi sweeps on the nearly diagonal H' (quadratic convergence: one sweep takes the
+// 1e-7 off-diagonal to rounding level, a second is taken only if needed), U = V J.
+// The A update is Hermitian-aware: only blocks k1 <= k2 are computed and the conjugate block is
+// mirrored.  A sweep stops the iteration once the off-diagonal Frobenius norm is below tol.
+// ---------------------------------------------------------------------------------------------
+struct EighMixedSmem {
+    static __host__ __device__ size_t bytes(int nw) {
+        int np = nw + (nw & 1);
+        int ld = np + 1;
+        size_t s = 2 * (size_t)np * ld * sizeof(float2);    // A32, V32
+        s += 2 * (size_t)np * ld * sizeof(double2);         // A64, V64
+        s += (size_t)(np / 2) * (sizeof(double2) + sizeof(double) + 2 * sizeof(int));
+        s += 256;
+        return s;
+    }
+};
+
+__global__ void jacobi_eigh_mixed_kernel(const double2 *__restrict__ h_in, int64_t h_stride, int64_t batch, int nw,
+                                         double *__restrict__ E_out, double2 *__restrict__ U_out) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int np = nw + (nw & 1);
+    const int ld = np + 1;
+    const int half = np / 2;
+    double2 *A64 = reinterpret_cast<double2 *>(smraw);
+    double2 *V64 = A64 + (size_t)np * ld;
+    float2 *A32 = reinterpret_cast<float2 *>(V64 + (size_t)np * ld);
+    float2 *V32 = A32 + (size_t)np * ld;
+    double2 *rot_s = reinterpret_cast<double2 *>(V32 + (size_t)np * ld);
+    double *rot_c = reinterpret_cast<double *>(rot_s + half);
+    int *rot_p = reinterpret_cast<int *>(rot_c + half);
+    int *rot_q = rot_p + half;
+    __shared__ double red[48];
+    const int tid = threadIdx.x;
+    for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) {
+        const double2 *h = h_in + b * h_stride;
+        double local = 0.0;
+        for (int e = tid; e < np * np; e += blockDim.x) {
+            const int i = e % np, j = e / np;
+            double2 v = make_double2(0.0, 0.0);
+            if (i < nw && j < nw) {
+                if (i < j) v = h[i + (size_t)nw * j];
+                else if (i > j) v = cconj(h[j + (size_t)nw * i]);
+                else v = make_double2(h[i + (size_t)nw * i].x, 0.0);
+            }
+            local += v.x * v.x + v.y * v.y;
+            A64[i + ld * j] = v;                     // FP64 copy of H (kept for Rayleigh-Ritz)
+            A32[i + ld * j] = make_float2((float)v.x, (float)v.y);
+            V32[i + ld * j] = make_float2(i == j ? 1.0f : 0.0f, 0.0f);
+        }
+        for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xffffffffu, local, o);
+        if ((tid & 31) == 0) red[tid >> 5] = local;
+        __syncthreads();
+        if (tid == 0) {
+            double s = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+            red[41] = sqrt(s);
+        }
+        __syncthreads();
+        const double fro = red[41];
+        // FP32 phase: rotate while |a_pq| > 2^-26 ||H||, stop at off(A) <= 2^-22 ||H||.
+        const float tol32 = (float)(fro * 1.4901161193847656e-08);
+        for (int sweep = 0; sweep < WNLQG_JACOBI_MAX_SWEEPS; ++sweep) {
+            jacobi_sweep<float>(A32, V32, np, ld, tol32, reinterpret_cast<float2 *>(rot_s),
+                                reinterpret_cast<float *>(rot_c), rot_p, rot_q);
+            if (offdiag_norm(A32, np, ld, red) <= fro * 2.384185791015625e-07) break;
+        }
+        // Rayleigh-Ritz in FP64: H' = V^H H V.  A64 holds H; use A32/V32 storage as FP64 scratch
+        // only through V64 (V promoted) and a product written back into A64.
+        for (int e = tid; e < np * np; e += blockDim.x) {
+            const int i = e % np, j = e / np;
+            V64[i + ld * j] = to_c64(V32[i + ld * j]);
+        }
+        __syncthreads();
+        // T = H V kept in registers per thread, then A64 <- V^H T (after a barrier).
+        {
+            const int nel = np * np;
+            const int per = (nel + blockDim.x - 1) / blockDim.x;   // <= 4 for np <= 32 and 256 threads
+            double2 tv[4];
+            for (int r = 0; r < per && r < 4; ++r) {
+                const int e = tid + r * blockDim.x;
+                double2 acc = make_double2(0.0, 0.0);
+                if (e < nel) {
+                    const int i = e % np, j = e / np;
+                    for (int l = 0; l < np; ++l) acc = cfma(A64[i + ld * l], V64[l + ld * j], acc);
+                }
+                tv[r] = acc;
+            }
+            __syncthreads();
+            // Stage T into the FP32 area reinterpreted as FP64 is too small; write T into A64.
+            for (int r = 0; r < per && r < 4; ++r) {
+                const int e = tid + r * blockDim.x;
+                if (e < nel) A64[(e % np) + ld * (e / np)] = tv[r];
+            }
+            __syncthreads();
+            for (int r = 0; r < per && r < 4; ++r) {
+                const int e = tid + r * blockDim.x;
+                double2 acc = make_double2(0.0, 0.0);
+                if (e < nel) {
+                    const int i = e % np, j = e / np;
+                    for (int l = 0; l < np; ++l) acc = cfmaconj(V64[l + ld * i], A64[l + ld * j], acc);
+                }
+                tv[r] = acc;
+            }
+            __syncthreads();
+            for (int r = 0; r < per && r < 4; ++r) {
+                const int e = tid + r * blockDim.x;
+                if (e < nel) {
+                    const int i = e % np, j = e / np;
+                    double2 v = tv[r];
+                    if (i == j) v.y = 0.0;
+                    A64[i + ld * j] = v;
+                }
+            }
+            __syncthreads();
+        }
+        // Symmetrise H' from its upper triangle (Hermitian up to rounding).
+        for (int e = tid; e < np * np; e += blockDim.x) {
+            const int i = e % np, j = e / np;
+            if (i > j) A64[i + ld * j] = cconj(A64[j + ld * i]);
+        }
+        __syncthreads();
+        const double tol64 = fro * 8.673617379884035e-19;
+        for (int sweep = 0; sweep < 4; ++sweep) {
+            if (offdiag_norm(A64, np, ld, red) <= tol64) break;
+            jacobi_sweep<double>(A64, V64, np, ld, tol64, rot_s, rot_c, rot_p, rot_q);
+        }
+        for (int i = tid; i < nw; i += blockDim.x) {
+            const double di = A64[i + ld * i].x;
+            int rank = 0;
+            for (int j = 0; j < nw; ++j) {
+                const double dj = A64[j + ld * j].x;
+                rank += (dj < di) || (dj == di && j < i);
+            }
+            int pivot = 0;
+            double pm = hypot(V64[0 + ld * i].x, V64[0 + ld * i].y);
+            for (int r = 1; r < nw; ++r) {
+                const double mg = hypot(V64[r + ld * i].x, V64[r + ld * i].y);
+                if (mg > pm) { pm = mg; pivot = r; }
+            }
+            double2 phase = make_double2(1.0, 0.0);
+            if (pm > 0.0) phase = make_double2(V64[pivot + ld * i].x / pm, -V64[pivot + ld * i].y / pm);
+            E_out[b * nw + rank] = di;
+            double2 *u = U_out + b * (int64_t)nw * nw + (int64_t)nw * rank;
+            for (int r = 0; r < nw; ++r) u[r] = cmul(V64[r + ld * i], phase);
         }
         __syncthreads();
     }

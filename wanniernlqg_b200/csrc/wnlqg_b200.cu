@@ -349,8 +349,12 @@ wnlqg_status run_front(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const int64_
     }
     wnlqg_status st = record_event(pl, ev_base + 1);
     if (st != WNLQG_OK) return st;
-    jacobi_eigh_kernel<double><<<(unsigned)nb, pl->eigh_threads, pl->eigh_smem, pl->stream>>>(
-        pl->d_xw + (int64_t)pl->ch_H * pl->nn, N, nb, pl->nw, pl->d_E, pl->d_U, 8.673617379884035e-19);
+    if (pl->task.precision == WNLQG_PRECISION_MIXED)
+        jacobi_eigh_mixed_kernel<<<(unsigned)nb, pl->eigh_threads, pl->eigh_smem, pl->stream>>>(
+            pl->d_xw + (int64_t)pl->ch_H * pl->nn, N, nb, pl->nw, pl->d_E, pl->d_U);
+    else
+        jacobi_eigh_kernel<double><<<(unsigned)nb, pl->eigh_threads, pl->eigh_smem, pl->stream>>>(
+            pl->d_xw + (int64_t)pl->ch_H * pl->nn, N, nb, pl->nw, pl->d_E, pl->d_U, 8.673617379884035e-19);
     st = record_event(pl, ev_base + 2);
     if (st != WNLQG_OK) return st;
     pl->launches += staged ? 4 : 3;
@@ -694,11 +698,20 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
     }
 
     pl->eigh_threads = eigh_block_threads(nw);
-    pl->eigh_smem = EighSmem::bytes(nw, sizeof(double2));
-    if (pl->eigh_smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(jacobi_eigh_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)pl->eigh_smem);
-        if (e != cudaSuccess) return bail(fail(WNLQG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e)));
+    if (t.precision == WNLQG_PRECISION_MIXED) {
+        pl->eigh_smem = EighMixedSmem::bytes(nw);
+        if (pl->eigh_smem > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute(jacobi_eigh_mixed_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)pl->eigh_smem);
+            if (e != cudaSuccess) return bail(fail(WNLQG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e)));
+        }
+    } else {
+        pl->eigh_smem = EighSmem::bytes(nw, sizeof(double2));
+        if (pl->eigh_smem > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute(jacobi_eigh_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)pl->eigh_smem);
+            if (e != cudaSuccess) return bail(fail(WNLQG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e)));
+        }
     }
     if ((st = build_passes(pl, sm_count, (size_t)smem_optin)) != WNLQG_OK) return bail(st);
     for (const Pass &ps : pl->passes) pl->partial_slots = std::max(pl->partial_slots, ps.grid);
