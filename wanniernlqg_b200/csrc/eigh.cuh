@@ -31,7 +31,7 @@ struct EighSmem {
 // measures convergence.  Pairs are computed by threads tid < np/2.
 template <typename T>
 WNLQG_D void jacobi_sweep(typename cplx_of<T>::type *A, typename cplx_of<T>::type *V, int np, int ld, T tol,
-                          typename cplx_of<T>::type *rot_s, T *rot_c, int *rot_p, int *rot_q) {
+                          typename cplx_of<T>::type *rot_s, T *rot_c, int *rot_p, int *rot_q, int *rotated) {
     typedef typename cplx_of<T>::type C;
     const int half = np / 2;
     const int tid = threadIdx.x;
@@ -53,6 +53,7 @@ WNLQG_D void jacobi_sweep(typename cplx_of<T>::type *A, typename cplx_of<T>::typ
                 T s = t * c;
                 sp.x = s * (apq.x / g);
                 sp.y = s * (apq.y / g);
+                *rotated = 1;
             }
             rot_c[tid] = c;
             rot_s[tid] = sp;
@@ -158,6 +159,7 @@ __global__ void jacobi_eigh_kernel(const double2 *__restrict__ h_in, int64_t h_s
     int *rot_p = reinterpret_cast<int *>(rot_c + half);
     int *rot_q = rot_p + half;
     __shared__ double red[48];
+    __shared__ int rot_flag;
 
     const int tid = threadIdx.x;
     for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) {
@@ -187,9 +189,16 @@ __global__ void jacobi_eigh_kernel(const double2 *__restrict__ h_in, int64_t h_s
         __syncthreads();
         const T tol = (T)scratch[0];
 
+        // Sweep until a sweep applies no rotation (every |a_pq| <= tol) or the off-diagonal norm is
+        // below np * tol (then every element is too).
         for (int sweep = 0; sweep < WNLQG_JACOBI_MAX_SWEEPS; ++sweep) {
-            if (offdiag_norm(A, np, ld, red) <= (double)tol) break;
-            jacobi_sweep<T>(A, V, np, ld, tol, rot_s, rot_c, rot_p, rot_q);
+            if (offdiag_norm(A, np, ld, red) <= (double)tol * np) break;
+            if (tid == 0) rot_flag = 0;
+            __syncthreads();
+            jacobi_sweep<T>(A, V, np, ld, tol, rot_s, rot_c, rot_p, rot_q, &rot_flag);
+            const int any = rot_flag;
+            __syncthreads();
+            if (!any) break;
         }
         // Ascending order (stable), then phase canonicalisation per column.
         for (int i = tid; i < nw; i += blockDim.x) {
@@ -240,6 +249,34 @@ struct EighMixedSmem {
     }
 };
 
+// out = op(X) * Y in FP64 for np x np shared matrices (op = conjugate transpose when xh), with
+// every thread's results held in registers until all reads are done, so out may alias X or Y.
+// Needs blockDim.x >= np*np/4 (true for the eigensolver's launch shape).
+WNLQG_D void small_product(const double2 *X, const double2 *Y, double2 *out, int np, int ld, bool xh) {
+    const int nel = np * np;
+    double2 tv[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const int e = threadIdx.x + r * blockDim.x;
+        double2 acc = make_double2(0.0, 0.0);
+        if (e < nel) {
+            const int i = e % np, j = e / np;
+            if (xh)
+                for (int l = 0; l < np; ++l) acc = cfmaconj(X[l + ld * i], Y[l + ld * j], acc);
+            else
+                for (int l = 0; l < np; ++l) acc = cfma(X[i + ld * l], Y[l + ld * j], acc);
+        }
+        tv[r] = acc;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const int e = threadIdx.x + r * blockDim.x;
+        if (e < nel) out[(e % np) + ld * (e / np)] = tv[r];
+    }
+    __syncthreads();
+}
+
 __global__ void jacobi_eigh_mixed_kernel(const double2 *__restrict__ h_in, int64_t h_stride, int64_t batch, int nw,
                                          double *__restrict__ E_out, double2 *__restrict__ U_out) {
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -255,6 +292,7 @@ __global__ void jacobi_eigh_mixed_kernel(const double2 *__restrict__ h_in, int64
     int *rot_p = reinterpret_cast<int *>(rot_c + half);
     int *rot_q = rot_p + half;
     __shared__ double red[48];
+    __shared__ int rot_flag;
     const int tid = threadIdx.x;
     for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) {
         const double2 *h = h_in + b * h_stride;
@@ -285,59 +323,36 @@ __global__ void jacobi_eigh_mixed_kernel(const double2 *__restrict__ h_in, int64
         // FP32 phase: rotate while |a_pq| > 2^-26 ||H||, stop at off(A) <= 2^-22 ||H||.
         const float tol32 = (float)(fro * 1.4901161193847656e-08);
         for (int sweep = 0; sweep < WNLQG_JACOBI_MAX_SWEEPS; ++sweep) {
+            if (tid == 0) rot_flag = 0;
+            __syncthreads();
             jacobi_sweep<float>(A32, V32, np, ld, tol32, reinterpret_cast<float2 *>(rot_s),
-                                reinterpret_cast<float *>(rot_c), rot_p, rot_q);
-            if (offdiag_norm(A32, np, ld, red) <= fro * 2.384185791015625e-07) break;
+                                reinterpret_cast<float *>(rot_c), rot_p, rot_q, &rot_flag);
+            const int any = rot_flag;
+            __syncthreads();
+            if (!any || offdiag_norm(A32, np, ld, red) <= fro * 2.384185791015625e-07) break;
         }
-        // Rayleigh-Ritz in FP64: H' = V^H H V.  A64 holds H; use A32/V32 storage as FP64 scratch
-        // only through V64 (V promoted) and a product written back into A64.
+        // Rayleigh-Ritz in FP64.  The FP32 eigenvectors are orthonormal only to ~1e-7, so they are
+        // first re-orthonormalised with one Newton-Schulz (Loewdin) step W = V (3I - V^H V)/2
+        // (error 1e-7 -> 1e-14); then H' = W^H H W, which is similar to H to FP64 accuracy.
+        // The dead FP32 A/V area holds one FP64 scratch matrix S.
+        double2 *S64 = reinterpret_cast<double2 *>(A32);
         for (int e = tid; e < np * np; e += blockDim.x) {
             const int i = e % np, j = e / np;
             V64[i + ld * j] = to_c64(V32[i + ld * j]);
         }
         __syncthreads();
-        // T = H V kept in registers per thread, then A64 <- V^H T (after a barrier).
-        {
-            const int nel = np * np;
-            const int per = (nel + blockDim.x - 1) / blockDim.x;   // <= 4 for np <= 32 and 256 threads
-            double2 tv[4];
-            for (int r = 0; r < per && r < 4; ++r) {
-                const int e = tid + r * blockDim.x;
-                double2 acc = make_double2(0.0, 0.0);
-                if (e < nel) {
-                    const int i = e % np, j = e / np;
-                    for (int l = 0; l < np; ++l) acc = cfma(A64[i + ld * l], V64[l + ld * j], acc);
-                }
-                tv[r] = acc;
-            }
-            __syncthreads();
-            // Stage T into the FP32 area reinterpreted as FP64 is too small; write T into A64.
-            for (int r = 0; r < per && r < 4; ++r) {
-                const int e = tid + r * blockDim.x;
-                if (e < nel) A64[(e % np) + ld * (e / np)] = tv[r];
-            }
-            __syncthreads();
-            for (int r = 0; r < per && r < 4; ++r) {
-                const int e = tid + r * blockDim.x;
-                double2 acc = make_double2(0.0, 0.0);
-                if (e < nel) {
-                    const int i = e % np, j = e / np;
-                    for (int l = 0; l < np; ++l) acc = cfmaconj(V64[l + ld * i], A64[l + ld * j], acc);
-                }
-                tv[r] = acc;
-            }
-            __syncthreads();
-            for (int r = 0; r < per && r < 4; ++r) {
-                const int e = tid + r * blockDim.x;
-                if (e < nel) {
-                    const int i = e % np, j = e / np;
-                    double2 v = tv[r];
-                    if (i == j) v.y = 0.0;
-                    A64[i + ld * j] = v;
-                }
-            }
-            __syncthreads();
+        small_product(V64, V64, S64, np, ld, true);            // S = V^H V
+        for (int e = tid; e < np * np; e += blockDim.x) {
+            const int i = e % np, j = e / np;
+            const double2 v = S64[i + ld * j];
+            S64[i + ld * j] = make_double2((i == j ? 1.5 : 0.0) - 0.5 * v.x, -0.5 * v.y);
         }
+        __syncthreads();
+        small_product(V64, S64, V64, np, ld, false);           // W = V (3I - S)/2 (in place)
+        small_product(A64, V64, A64, np, ld, false);           // T = H W (in place over H)
+        small_product(V64, A64, A64, np, ld, true);            // H' = W^H T
+        for (int i = tid; i < np; i += blockDim.x) A64[i + ld * i].y = 0.0;
+        __syncthreads();
         // Symmetrise H' from its upper triangle (Hermitian up to rounding).
         for (int e = tid; e < np * np; e += blockDim.x) {
             const int i = e % np, j = e / np;
@@ -346,8 +361,13 @@ __global__ void jacobi_eigh_mixed_kernel(const double2 *__restrict__ h_in, int64
         __syncthreads();
         const double tol64 = fro * 8.673617379884035e-19;
         for (int sweep = 0; sweep < 4; ++sweep) {
-            if (offdiag_norm(A64, np, ld, red) <= tol64) break;
-            jacobi_sweep<double>(A64, V64, np, ld, tol64, rot_s, rot_c, rot_p, rot_q);
+            if (offdiag_norm(A64, np, ld, red) <= tol64 * np) break;
+            if (tid == 0) rot_flag = 0;
+            __syncthreads();
+            jacobi_sweep<double>(A64, V64, np, ld, tol64, rot_s, rot_c, rot_p, rot_q, &rot_flag);
+            const int any = rot_flag;
+            __syncthreads();
+            if (!any) break;
         }
         for (int i = tid; i < nw; i += blockDim.x) {
             const double di = A64[i + ld * i].x;
