@@ -199,6 +199,7 @@ def test_mixed_eigensolver_refined_to_fp64(engine_cls, oracle_mod, name):
         e, u = eng.spectrum(k)
     for i in range(k.shape[0]):
         eo, uo, _ = oracle_mod.kpoint_spectrum(model, k[i])
-        assert np.max(np.abs(e[i] - eo)) < 1e-11 * max(1.0, np.abs(eo).max())
+        err = np.max(np.abs(e[i] - eo))
+        assert err < 1e-11 * max(1.0, np.abs(eo).max()), (i, err, np.min(np.diff(eo)))
         ov = np.abs(np.sum(u[i].conj() * uo, axis=0))
-        assert np.max(np.abs(ov - 1.0)) < 1e-8
+        assert np.max(np.abs(ov - 1.0)) < 1e-8, (i, np.max(np.abs(ov - 1.0)), np.min(np.diff(eo)))

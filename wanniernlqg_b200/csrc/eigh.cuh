@@ -237,26 +237,15 @@ __global__ void jacobi_eigh_kernel(const double2 *__restrict__ h_in, int64_t h_s
 // The A update is Hermitian-aware: only blocks k1 <= k2 are computed and the conjugate block is
 // mirrored.  A sweep stops the iteration once the off-diagonal Frobenius norm is below tol.
 // ---------------------------------------------------------------------------------------------
-struct EighMixedSmem {
-    static __host__ __device__ size_t bytes(int nw) {
-        int np = nw + (nw & 1);
-        int ld = np + 1;
-        size_t s = 2 * (size_t)np * ld * sizeof(float2);    // A32, V32
-        s += 2 * (size_t)np * ld * sizeof(double2);         // A64, V64
-        s += (size_t)(np / 2) * (sizeof(double2) + sizeof(double) + 2 * sizeof(int));
-        s += 256;
-        return s;
-    }
-};
 
 // out = op(X) * Y in FP64 for np x np shared matrices (op = conjugate transpose when xh), with
 // every thread's results held in registers until all reads are done, so out may alias X or Y.
-// Needs blockDim.x >= np*np/4 (true for the eigensolver's launch shape).
+// Needs blockDim.x * 8 >= np*np.
 WNLQG_D void small_product(const double2 *X, const double2 *Y, double2 *out, int np, int ld, bool xh) {
     const int nel = np * np;
-    double2 tv[4];
+    double2 tv[8];
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {
+    for (int r = 0; r < 8; ++r) {
         const int e = threadIdx.x + r * blockDim.x;
         double2 acc = make_double2(0.0, 0.0);
         if (e < nel) {
@@ -270,25 +259,33 @@ WNLQG_D void small_product(const double2 *X, const double2 *Y, double2 *out, int
     }
     __syncthreads();
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {
+    for (int r = 0; r < 8; ++r) {
         const int e = threadIdx.x + r * blockDim.x;
         if (e < nel) out[(e % np) + ld * (e / np)] = tv[r];
     }
     __syncthreads();
 }
 
-__global__ void jacobi_eigh_mixed_kernel(const double2 *__restrict__ h_in, int64_t h_stride, int64_t batch, int nw,
-                                         double *__restrict__ E_out, double2 *__restrict__ U_out) {
+// Stage 1 of the mixed eigensolver: FP32 parallel Jacobi (17 KB of shared memory at nw = 32, so
+// several CTAs share an SM).  Writes the FP32 eigenvector estimate V [b][np][np] to global memory.
+struct EighF32Smem {
+    static __host__ __device__ size_t bytes(int nw) {
+        int np = nw + (nw & 1);
+        int ld = np + 1;
+        return 2 * (size_t)np * ld * sizeof(float2) + (size_t)(np / 2) * (sizeof(float2) + sizeof(float) + 2 * sizeof(int)) + 64;
+    }
+};
+
+__global__ void jacobi_eigh_f32_kernel(const double2 *__restrict__ h_in, int64_t h_stride, int64_t batch, int nw,
+                                       float2 *__restrict__ V_out) {
     extern __shared__ __align__(16) unsigned char smraw[];
     const int np = nw + (nw & 1);
     const int ld = np + 1;
     const int half = np / 2;
-    double2 *A64 = reinterpret_cast<double2 *>(smraw);
-    double2 *V64 = A64 + (size_t)np * ld;
-    float2 *A32 = reinterpret_cast<float2 *>(V64 + (size_t)np * ld);
+    float2 *A32 = reinterpret_cast<float2 *>(smraw);
     float2 *V32 = A32 + (size_t)np * ld;
-    double2 *rot_s = reinterpret_cast<double2 *>(V32 + (size_t)np * ld);
-    double *rot_c = reinterpret_cast<double *>(rot_s + half);
+    float2 *rot_s = V32 + (size_t)np * ld;
+    float *rot_c = reinterpret_cast<float *>(rot_s + half);
     int *rot_p = reinterpret_cast<int *>(rot_c + half);
     int *rot_q = rot_p + half;
     __shared__ double red[48];
@@ -306,7 +303,6 @@ __global__ void jacobi_eigh_mixed_kernel(const double2 *__restrict__ h_in, int64
                 else v = make_double2(h[i + (size_t)nw * i].x, 0.0);
             }
             local += v.x * v.x + v.y * v.y;
-            A64[i + ld * j] = v;                     // FP64 copy of H (kept for Rayleigh-Ritz)
             A32[i + ld * j] = make_float2((float)v.x, (float)v.y);
             V32[i + ld * j] = make_float2(i == j ? 1.0f : 0.0f, 0.0f);
         }
@@ -314,33 +310,80 @@ __global__ void jacobi_eigh_mixed_kernel(const double2 *__restrict__ h_in, int64
         if ((tid & 31) == 0) red[tid >> 5] = local;
         __syncthreads();
         if (tid == 0) {
-            double s = 0.0;
-            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
-            red[41] = sqrt(s);
+            double sum = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) sum += red[w];
+            red[41] = sqrt(sum);
         }
         __syncthreads();
         const double fro = red[41];
-        // FP32 phase: rotate while |a_pq| > 2^-26 ||H||, stop at off(A) <= 2^-22 ||H||.
-        const float tol32 = (float)(fro * 1.4901161193847656e-08);
+        const float tol32 = (float)(fro * 1.4901161193847656e-08);   // rotate while |a_pq| > 2^-26 ||H||
         for (int sweep = 0; sweep < WNLQG_JACOBI_MAX_SWEEPS; ++sweep) {
             if (tid == 0) rot_flag = 0;
             __syncthreads();
-            jacobi_sweep<float>(A32, V32, np, ld, tol32, reinterpret_cast<float2 *>(rot_s),
-                                reinterpret_cast<float *>(rot_c), rot_p, rot_q, &rot_flag);
+            jacobi_sweep<float>(A32, V32, np, ld, tol32, rot_s, rot_c, rot_p, rot_q, &rot_flag);
             const int any = rot_flag;
             __syncthreads();
             if (!any || offdiag_norm(A32, np, ld, red) <= fro * 2.384185791015625e-07) break;
         }
-        // Rayleigh-Ritz in FP64.  The FP32 eigenvectors are orthonormal only to ~1e-7, so they are
-        // first re-orthonormalised with one Newton-Schulz (Loewdin) step W = V (3I - V^H V)/2
-        // (error 1e-7 -> 1e-14); then H' = W^H H W, which is similar to H to FP64 accuracy.
-        // The dead FP32 A/V area holds one FP64 scratch matrix S.
-        double2 *S64 = reinterpret_cast<double2 *>(A32);
+        float2 *vo = V_out + b * (int64_t)np * np;
+        for (int e = tid; e < np * np; e += blockDim.x) vo[e] = V32[(e % np) + ld * (e / np)];
+        __syncthreads();
+    }
+}
+
+// Stage 2: FP64 refinement.  W = V (3I - V^H V)/2 (Newton-Schulz orthonormalisation of the FP32
+// eigenvectors), H' = W^H H W, FP64 Jacobi sweeps on the nearly diagonal H' (usually one), then
+// ascending order and canonical phases.
+struct EighRefineSmem {
+    static __host__ __device__ size_t bytes(int nw) {
+        int np = nw + (nw & 1);
+        int ld = np + 1;
+        return 3 * (size_t)np * ld * sizeof(double2) + (size_t)(np / 2) * (sizeof(double2) + sizeof(double) + 2 * sizeof(int)) + 64;
+    }
+};
+
+__global__ void eigh_refine_f64_kernel(const double2 *__restrict__ h_in, int64_t h_stride, const float2 *__restrict__ V_in,
+                                       int64_t batch, int nw, double *__restrict__ E_out, double2 *__restrict__ U_out) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int np = nw + (nw & 1);
+    const int ld = np + 1;
+    const int half = np / 2;
+    double2 *A64 = reinterpret_cast<double2 *>(smraw);
+    double2 *V64 = A64 + (size_t)np * ld;
+    double2 *S64 = V64 + (size_t)np * ld;
+    double2 *rot_s = S64 + (size_t)np * ld;
+    double *rot_c = reinterpret_cast<double *>(rot_s + half);
+    int *rot_p = reinterpret_cast<int *>(rot_c + half);
+    int *rot_q = rot_p + half;
+    __shared__ double red[48];
+    __shared__ int rot_flag;
+    const int tid = threadIdx.x;
+    for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) {
+        const double2 *h = h_in + b * h_stride;
+        const float2 *vi = V_in + b * (int64_t)np * np;
+        double local = 0.0;
         for (int e = tid; e < np * np; e += blockDim.x) {
             const int i = e % np, j = e / np;
-            V64[i + ld * j] = to_c64(V32[i + ld * j]);
+            double2 v = make_double2(0.0, 0.0);
+            if (i < nw && j < nw) {
+                if (i < j) v = h[i + (size_t)nw * j];
+                else if (i > j) v = cconj(h[j + (size_t)nw * i]);
+                else v = make_double2(h[i + (size_t)nw * i].x, 0.0);
+            }
+            local += v.x * v.x + v.y * v.y;
+            A64[i + ld * j] = v;
+            V64[i + ld * j] = to_c64(vi[e]);
+        }
+        for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xffffffffu, local, o);
+        if ((tid & 31) == 0) red[tid >> 5] = local;
+        __syncthreads();
+        if (tid == 0) {
+            double sum = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) sum += red[w];
+            red[41] = sqrt(sum);
         }
         __syncthreads();
+        const double fro = red[41];
         small_product(V64, V64, S64, np, ld, true);            // S = V^H V
         for (int e = tid; e < np * np; e += blockDim.x) {
             const int i = e % np, j = e / np;
@@ -348,15 +391,13 @@ __global__ void jacobi_eigh_mixed_kernel(const double2 *__restrict__ h_in, int64
             S64[i + ld * j] = make_double2((i == j ? 1.5 : 0.0) - 0.5 * v.x, -0.5 * v.y);
         }
         __syncthreads();
-        small_product(V64, S64, V64, np, ld, false);           // W = V (3I - S)/2 (in place)
-        small_product(A64, V64, A64, np, ld, false);           // T = H W (in place over H)
+        small_product(V64, S64, V64, np, ld, false);           // W = V (3I - S)/2
+        small_product(A64, V64, A64, np, ld, false);           // T = H W
         small_product(V64, A64, A64, np, ld, true);            // H' = W^H T
-        for (int i = tid; i < np; i += blockDim.x) A64[i + ld * i].y = 0.0;
-        __syncthreads();
-        // Symmetrise H' from its upper triangle (Hermitian up to rounding).
         for (int e = tid; e < np * np; e += blockDim.x) {
             const int i = e % np, j = e / np;
             if (i > j) A64[i + ld * j] = cconj(A64[j + ld * i]);
+            if (i == j) A64[i + ld * i].y = 0.0;
         }
         __syncthreads();
         const double tol64 = fro * 8.673617379884035e-19;
@@ -391,3 +432,4 @@ __global__ void jacobi_eigh_mixed_kernel(const double2 *__restrict__ h_in, int64
         __syncthreads();
     }
 }
+

@@ -86,6 +86,9 @@ struct wnlqg_plan {
     std::vector<Pass> passes;
     int eigh_threads = 32;
     size_t eigh_smem = 0;
+    int refine_threads = 32;
+    size_t refine_smem = 0;
+    float2 *d_V32 = nullptr;
     cudaStream_t stream = nullptr;
     std::vector<cudaEvent_t> events;
     size_t timing_batches = 0;
@@ -349,10 +352,13 @@ wnlqg_status run_front(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const int64_
     }
     wnlqg_status st = record_event(pl, ev_base + 1);
     if (st != WNLQG_OK) return st;
-    if (pl->task.precision == WNLQG_PRECISION_MIXED)
-        jacobi_eigh_mixed_kernel<<<(unsigned)nb, pl->eigh_threads, pl->eigh_smem, pl->stream>>>(
-            pl->d_xw + (int64_t)pl->ch_H * pl->nn, N, nb, pl->nw, pl->d_E, pl->d_U);
-    else
+    if (pl->task.precision == WNLQG_PRECISION_MIXED) {
+        jacobi_eigh_f32_kernel<<<(unsigned)nb, pl->eigh_threads, pl->eigh_smem, pl->stream>>>(
+            pl->d_xw + (int64_t)pl->ch_H * pl->nn, N, nb, pl->nw, pl->d_V32);
+        eigh_refine_f64_kernel<<<(unsigned)nb, pl->refine_threads, pl->refine_smem, pl->stream>>>(
+            pl->d_xw + (int64_t)pl->ch_H * pl->nn, N, pl->d_V32, nb, pl->nw, pl->d_E, pl->d_U);
+        pl->launches += 1;
+    } else
         jacobi_eigh_kernel<double><<<(unsigned)nb, pl->eigh_threads, pl->eigh_smem, pl->stream>>>(
             pl->d_xw + (int64_t)pl->ch_H * pl->nn, N, nb, pl->nw, pl->d_E, pl->d_U, 8.673617379884035e-19);
     st = record_event(pl, ev_base + 2);
@@ -480,7 +486,7 @@ wnlqg_status wnlqg_b200_plan_destroy(wnlqg_plan *pl) {
     for (void *ptr : {(void *)pl->d_tiles, (void *)pl->d_phase, (void *)pl->d_xw, (void *)pl->d_U, (void *)pl->d_out,
                       (void *)pl->d_points, (void *)pl->d_E, (void *)pl->d_kpts, (void *)pl->d_omegas,
                       (void *)pl->d_partials, (void *)pl->d_weights, (void *)pl->d_groups, (void *)pl->d_stageY,
-                      (void *)pl->d_stageZ})
+                      (void *)pl->d_stageZ, (void *)pl->d_V32})
         if (ptr) cudaFree(ptr);
     for (cudaEvent_t ev : pl->events) cudaEventDestroy(ev);
     if (pl->stream) cudaStreamDestroy(pl->stream);
@@ -699,12 +705,15 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
 
     pl->eigh_threads = eigh_block_threads(nw);
     if (t.precision == WNLQG_PRECISION_MIXED) {
-        pl->eigh_smem = EighMixedSmem::bytes(nw);
-        if (pl->eigh_smem > 48 * 1024) {
-            cudaError_t e = cudaFuncSetAttribute(jacobi_eigh_mixed_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)pl->eigh_smem);
-            if (e != cudaSuccess) return bail(fail(WNLQG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e)));
-        }
+        const int np = nw + (nw & 1);
+        pl->eigh_smem = EighF32Smem::bytes(nw);
+        pl->refine_smem = EighRefineSmem::bytes(nw);
+        pl->refine_threads = std::max(32, std::min(256, ((np * np / 8 + 31) / 32) * 32));
+        pl->refine_threads = std::max(pl->refine_threads, pl->eigh_threads);
+        if ((st = alloc((void **)&pl->d_V32, (size_t)max_batch * np * np * sizeof(float2))) != WNLQG_OK) return bail(st);
+        cudaError_t e = cudaFuncSetAttribute(eigh_refine_f64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)std::max<size_t>(pl->refine_smem, 48 * 1024));
+        if (e != cudaSuccess) return bail(fail(WNLQG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e)));
     } else {
         pl->eigh_smem = EighSmem::bytes(nw, sizeof(double2));
         if (pl->eigh_smem > 48 * 1024) {
