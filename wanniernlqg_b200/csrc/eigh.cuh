@@ -384,14 +384,33 @@ __global__ void eigh_refine_f64_kernel(const double2 *__restrict__ h_in, int64_t
         }
         __syncthreads();
         const double fro = red[41];
+        // Loewdin orthonormalisation to second order: E = V^H V - I (about 1e-6 after the FP32
+        // sweeps), W = V (I - E/2 + 3E^2/8), so that W^H W - I = O(|E|^3).
         small_product(V64, V64, S64, np, ld, true);            // S = V^H V
         for (int e = tid; e < np * np; e += blockDim.x) {
             const int i = e % np, j = e / np;
-            const double2 v = S64[i + ld * j];
-            S64[i + ld * j] = make_double2((i == j ? 1.5 : 0.0) - 0.5 * v.x, -0.5 * v.y);
+            if (i == j) S64[i + ld * i].x -= 1.0;                // E = S - I
         }
         __syncthreads();
-        small_product(V64, S64, V64, np, ld, false);           // W = V (3I - S)/2
+        small_product(S64, S64, A64, np, ld, false);           // A64 <- E^2 (H is reloaded below)
+        for (int e = tid; e < np * np; e += blockDim.x) {
+            const int i = e % np, j = e / np;
+            const double2 ev = S64[i + ld * j], e2 = A64[i + ld * j];
+            S64[i + ld * j] = make_double2((i == j ? 1.0 : 0.0) - 0.5 * ev.x + 0.375 * e2.x, -0.5 * ev.y + 0.375 * e2.y);
+        }
+        __syncthreads();
+        small_product(V64, S64, V64, np, ld, false);           // W = V M
+        for (int e = tid; e < np * np; e += blockDim.x) {
+            const int i = e % np, j = e / np;
+            double2 v = make_double2(0.0, 0.0);
+            if (i < nw && j < nw) {
+                if (i < j) v = h[i + (size_t)nw * j];
+                else if (i > j) v = cconj(h[j + (size_t)nw * i]);
+                else v = make_double2(h[i + (size_t)nw * i].x, 0.0);
+            }
+            A64[i + ld * j] = v;
+        }
+        __syncthreads();
         small_product(A64, V64, A64, np, ld, false);           // T = H W
         small_product(V64, A64, A64, np, ld, true);            // H' = W^H T
         for (int e = tid; e < np * np; e += blockDim.x) {

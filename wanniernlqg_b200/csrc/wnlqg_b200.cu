@@ -710,6 +710,7 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
         pl->refine_smem = EighRefineSmem::bytes(nw);
         pl->refine_threads = std::max(32, std::min(256, ((np * np / 8 + 31) / 32) * 32));
         pl->refine_threads = std::max(pl->refine_threads, pl->eigh_threads);
+        pl->eigh_threads = std::max(32, std::min(pl->eigh_threads, 128));   // FP32 stage: more CTAs per SM
         if ((st = alloc((void **)&pl->d_V32, (size_t)max_batch * np * np * sizeof(float2))) != WNLQG_OK) return bail(st);
         cudaError_t e = cudaFuncSetAttribute(eigh_refine_f64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)std::max<size_t>(pl->refine_smem, 48 * 1024));
