@@ -243,16 +243,17 @@ def main():
         dist.barrier()
     value = world * batch * args.steps / (elapsed_ms / 1e3)
 
-    # End to end through the public host API: host k-points (H2D) -> weighted mesh sum -> host
-    # result (D2H), synchronous, wall clock.
+    # End to end through the public host API: the step's mesh indices and weights in pinned
+    # host memory (H2D), the weighted mesh sum, and the result read back (D2H); synchronous,
+    # wall clock.
     e2e_steps = max(1, min(args.steps, 3))
     kb, _ = block(args.warmup + args.steps)
-    kpts = mesh_kpoints(kb, batch)
-    w = np.full(batch, 1.0 / nk)
-    engine.weighted_sum(kpts, w)
+    idx = torch.arange(kb, kb + batch, dtype=torch.int64).pin_memory().numpy()
+    w = torch.full((batch,), 1.0 / nk, dtype=torch.float64).pin_memory().numpy()
+    engine.mesh_weighted_sum(MESH, idx, w)
     t0 = time.perf_counter()
     for s in range(e2e_steps):
-        engine.weighted_sum(kpts, w)
+        engine.mesh_weighted_sum(MESH, idx, w)
     e2e_dt = (time.perf_counter() - t0) / e2e_steps
     e2e_value = world * batch / e2e_dt
 
@@ -283,7 +284,7 @@ def main():
                    "precision": args.precision, "l2": "inputs larger than L2 (per-step workspace >> 126 MB)",
                    "parallelism": f"k-blocks x{world}"},
         "roofline": roofline,
-        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": int(kpts.nbytes + w.nbytes),
+        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": int(idx.nbytes + w.nbytes),
                 "d2h_bytes_per_step": int(16 * vc)},
         "clocks": clocks,
         "gpu_launches": launches,

@@ -169,6 +169,15 @@ WNLQG_API wnlqg_status wnlqg_b200_eval_points(wnlqg_plan *plan, const double *kp
 WNLQG_API wnlqg_status wnlqg_b200_eval_points_weighted(wnlqg_plan *plan, const double *kpoints,
                                              const double *weights, int64_t n, double *out);
 
+/* Weighted sum over mesh indices: out = sum_i weights[i] * value(k(indices[i])) with k the
+ * Gamma-centred mesh point of each index (first axis fastest).  Indices and weights are host
+ * arrays.  This is the symmetry-reduced mesh contract (representatives and multiplicities/Nk,
+ * numerical_response_symmetry_plan in IntegralDriver.jl:169-180, 820-874); runs of consecutive
+ * indices use the staged mesh contraction. */
+WNLQG_API wnlqg_status wnlqg_b200_eval_mesh_weighted(wnlqg_plan *plan, const int64_t mesh[3],
+                                           const int64_t *indices, const double *weights, int64_t n,
+                                           double *out);
+
 /* Per-k band data for diagnostics and tests: energies [n*nw] (ascending) and the
  * canonicalised eigenvectors [n*nw*nw] complex, column-major per k
  * (compute_spectrum!, HamiltonianMatrixElements.jl:279-300 and :6-25). */

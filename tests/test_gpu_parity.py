@@ -203,3 +203,25 @@ def test_mixed_eigensolver_refined_to_fp64(engine_cls, oracle_mod, name):
         assert err < 1e-11 * max(1.0, np.abs(eo).max()), (i, err, np.min(np.diff(eo)))
         ov = np.abs(np.sum(u[i].conj() * uo, axis=0))
         assert np.max(np.abs(ov - 1.0)) < 1e-8, (i, np.max(np.abs(ov - 1.0)), np.min(np.diff(eo)))
+
+
+def test_mesh_weighted_sum_contiguous_and_scattered(engine_cls, oracle_mod):
+    """Host mesh indices + weights: a contiguous run (staged path) equals the lane sum, and a
+    scattered representative set with multiplicities equals the weighted oracle point sum."""
+    model = reference_workload_model("nw4")
+    task = nw4_task(nom=32)
+    mesh = (8, 6, 4)
+    nk = int(np.prod(mesh))
+    rng = np.random.default_rng(16)
+    with engine_cls(model, task, max_batch=50) as eng:
+        idx = np.arange(10, 150)
+        got = eng.mesh_weighted_sum(mesh, idx, np.full(idx.size, 1.0 / nk))
+        ref = eng.integrate_mesh(mesh, 10, 150)
+        assert rel_err(got, ref) < 1e-13
+        sidx = rng.choice(nk, 37, replace=False)
+        w = rng.integers(1, 9, sidx.size) / nk
+        got2 = eng.mesh_weighted_sum(mesh, sidx, w)
+    k = np.stack([(sidx % 8) / 8, ((sidx // 8) % 6) / 6, (sidx // 48) / 4], axis=1)
+    ref2 = (oracle_mod.point_values(model, task, k) * w[:, None]).sum(axis=0)
+    for g, r in zip(task.split(got2), task.split(ref2)):
+        assert rel_err(g, r) < RTOL

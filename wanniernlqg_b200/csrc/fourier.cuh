@@ -7,11 +7,12 @@
 #include "common.cuh"
 
 // Phase table F[k, R] for a batch.  Mesh mode (kpts == nullptr): batch entry b is mesh index
-// k_begin + b of the Gamma-centred mesh (first axis fastest, CalculationUtils.jl:280-292); the
+// kidx[b] (or k_begin + b without an index list) of the Gamma-centred mesh (first axis fastest, CalculationUtils.jl:280-292); the
 // phase R.k is reduced exactly with integer arithmetic before sincospi.  Point mode: k from kpts.
 __global__ void phase_kernel(double2 *__restrict__ phases, const int64_t *__restrict__ rvec,
                              const int64_t *__restrict__ deg, int nr, int64_t batch, int64_t k_begin,
-                             int64_t n1, int64_t n2, int64_t n3, const double *__restrict__ kpts) {
+                             int64_t n1, int64_t n2, int64_t n3, const double *__restrict__ kpts,
+                             const int64_t *__restrict__ kidx = nullptr) {
     int64_t total = batch * (int64_t)nr;
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
          e += (int64_t)gridDim.x * blockDim.x) {
@@ -20,7 +21,7 @@ __global__ void phase_kernel(double2 *__restrict__ phases, const int64_t *__rest
         int64_t r1 = rvec[3 * r], r2 = rvec[3 * r + 1], r3 = rvec[3 * r + 2];
         double x;
         if (kpts == nullptr) {
-            int64_t idx = k_begin + b;
+            int64_t idx = kidx ? kidx[b] : k_begin + b;
             int64_t i1 = idx % n1, i2 = (idx / n1) % n2, i3 = idx / (n1 * n2);
             int64_t p1 = ((r1 * i1) % n1 + n1) % n1, p2 = ((r2 * i2) % n2 + n2) % n2, p3 = ((r3 * i3) % n3 + n3) % n3;
             x = (double)p1 / (double)n1 + (double)p2 / (double)n2 + (double)p3 / (double)n3;

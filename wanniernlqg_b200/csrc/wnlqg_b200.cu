@@ -75,6 +75,7 @@ struct wnlqg_plan {
     double2 *d_tiles = nullptr, *d_phase = nullptr, *d_xw = nullptr, *d_U = nullptr, *d_out = nullptr;
     double2 *d_points = nullptr;
     double *d_E = nullptr, *d_kpts = nullptr, *d_omegas = nullptr, *d_partials = nullptr, *d_weights = nullptr;
+    int64_t *d_kidx = nullptr;
     int partial_slots = 0;
     // Staged mesh Fourier: R grouping (device) and lazily sized Y/Z workspaces.
     int P12 = 0, P1 = 0;
@@ -307,10 +308,11 @@ wnlqg_status record_event(wnlqg_plan *pl, size_t idx) {
 
 // One batch: phases, Fourier GEMM, eigensolve.  kpts_device == nullptr selects mesh mode.
 wnlqg_status run_front(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const int64_t *mesh, const double *kpts_device,
-                       size_t ev_base) {
+                       size_t ev_base, const int64_t *kidx_device = nullptr) {
     const int nr = pl->nr;
     int64_t N = (int64_t)pl->C * pl->nn;
-    const bool staged = mesh != nullptr && kpts_device == nullptr && pl->P1 <= STAGED_MAX_P1 && mesh[0] >= pl->P1;
+    const bool staged = mesh != nullptr && kpts_device == nullptr && kidx_device == nullptr && pl->P1 <= STAGED_MAX_P1 &&
+                        mesh[0] >= pl->P1;
     pl->use_staged_last = staged;
     if (staged) {
         const int64_t n1 = mesh[0], n2 = mesh[1], n3 = mesh[2];
@@ -346,7 +348,7 @@ wnlqg_status run_front(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const int64_
         int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 32);
         phase_kernel<<<blocks, 256, 0, pl->stream>>>(pl->d_phase, pl->model->d_rvec, pl->model->d_deg, nr, nb,
                                                      k_begin, mesh ? mesh[0] : 1, mesh ? mesh[1] : 1,
-                                                     mesh ? mesh[2] : 1, kpts_device);
+                                                     mesh ? mesh[2] : 1, kpts_device, kidx_device);
         dim3 grid((unsigned)((N + FG_BN - 1) / FG_BN), (unsigned)((nb + FG_BM - 1) / FG_BM));
         fourier_gemm_f64<<<grid, 256, 0, pl->stream>>>(pl->d_phase, pl->d_tiles, pl->d_xw, nb, N, nr);
     }
@@ -486,7 +488,7 @@ wnlqg_status wnlqg_b200_plan_destroy(wnlqg_plan *pl) {
     for (void *ptr : {(void *)pl->d_tiles, (void *)pl->d_phase, (void *)pl->d_xw, (void *)pl->d_U, (void *)pl->d_out,
                       (void *)pl->d_points, (void *)pl->d_E, (void *)pl->d_kpts, (void *)pl->d_omegas,
                       (void *)pl->d_partials, (void *)pl->d_weights, (void *)pl->d_groups, (void *)pl->d_stageY,
-                      (void *)pl->d_stageZ, (void *)pl->d_V32})
+                      (void *)pl->d_stageZ, (void *)pl->d_V32, (void *)pl->d_kidx})
         if (ptr) cudaFree(ptr);
     for (cudaEvent_t ev : pl->events) cudaEventDestroy(ev);
     if (pl->stream) cudaStreamDestroy(pl->stream);
@@ -647,6 +649,7 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
     if ((st = alloc((void **)&pl->d_E, (size_t)max_batch * nw * sizeof(double))) != WNLQG_OK) return bail(st);
     if ((st = alloc((void **)&pl->d_kpts, (size_t)max_batch * 3 * sizeof(double))) != WNLQG_OK) return bail(st);
     if ((st = alloc((void **)&pl->d_weights, (size_t)max_batch * sizeof(double))) != WNLQG_OK) return bail(st);
+    if ((st = alloc((void **)&pl->d_kidx, (size_t)max_batch * sizeof(int64_t))) != WNLQG_OK) return bail(st);
     if ((st = alloc((void **)&pl->d_points, (size_t)max_batch * vc * sizeof(double2))) != WNLQG_OK) return bail(st);
     if ((st = alloc((void **)&pl->d_out, (size_t)vc * sizeof(double2))) != WNLQG_OK) return bail(st);
     if ((st = alloc((void **)&pl->d_omegas, std::max<size_t>(1, pl->omegas.size()) * sizeof(double))) != WNLQG_OK) return bail(st);
@@ -840,6 +843,47 @@ wnlqg_status wnlqg_b200_eval_points_weighted(wnlqg_plan *pl, const double *kpoin
         WNLQG_CUDA(cudaMemcpyAsync(pl->d_weights, weights + s, (size_t)nb * sizeof(double), cudaMemcpyHostToDevice,
                                    pl->stream));
         if ((st = run_front(pl, nb, 0, nullptr, pl->d_kpts, 1)) != WNLQG_OK) return st;
+        if ((st = run_passes(pl, nb, 0, 1.0, 0, pl->d_weights)) != WNLQG_OK) return st;
+    }
+    reduce_partials_kernel<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((pl->vc + 255) / 256, 1024)), 256, 0,
+                             pl->stream>>>(pl->d_partials, pl->partial_slots, pl->vc, pl->d_out);
+    pl->launches += 1;
+    WNLQG_CUDA(cudaGetLastError());
+    WNLQG_CUDA(cudaMemcpyAsync(out, pl->d_out, (size_t)pl->vc * sizeof(double2), cudaMemcpyDeviceToHost, pl->stream));
+    WNLQG_CUDA(cudaStreamSynchronize(pl->stream));
+    pl->timing_valid = false;
+    for (int64_t v = 0; v < 2 * pl->vc; ++v)
+        if (!std::isfinite(out[v])) return fail(WNLQG_ERR_NONFINITE, "response contains non-finite values");
+    return WNLQG_OK;
+}
+
+wnlqg_status wnlqg_b200_eval_mesh_weighted(wnlqg_plan *pl, const int64_t mesh[3], const int64_t *indices,
+                                           const double *weights, int64_t n, double *out) {
+    wnlqg_status st = check_plan(pl);
+    if (st != WNLQG_OK) return st;
+    if (!mesh || !out || n < 0 || (n > 0 && (!indices || !weights))) return fail(WNLQG_ERR_INVALID_ARGUMENT, "invalid arguments");
+    if (mesh[0] <= 0 || mesh[1] <= 0 || mesh[2] <= 0) return fail(WNLQG_ERR_INVALID_ARGUMENT, "mesh counts must be positive");
+    const int64_t nk = mesh[0] * mesh[1] * mesh[2];
+    for (int64_t i = 0; i < n; ++i)
+        if (indices[i] < 0 || indices[i] >= nk) return fail(WNLQG_ERR_INVALID_ARGUMENT, "mesh index out of range");
+    if (!finite_array(weights, (size_t)n)) return fail(WNLQG_ERR_NONFINITE, "weights must be finite");
+    WNLQG_CUDA(cudaSetDevice(pl->model->device));
+    pl->launches = 0;
+    WNLQG_CUDA(cudaMemsetAsync(pl->d_partials, 0, (size_t)pl->partial_slots * pl->vc * 4 * sizeof(double), pl->stream));
+    for (int64_t s = 0; s < n; s += pl->max_batch) {
+        const int64_t nb = std::min(pl->max_batch, n - s);
+        bool contiguous = true;
+        for (int64_t i = 1; i < nb && contiguous; ++i) contiguous = indices[s + i] == indices[s] + i;
+        WNLQG_CUDA(cudaMemcpyAsync(pl->d_weights, weights + s, (size_t)nb * sizeof(double), cudaMemcpyHostToDevice,
+                                   pl->stream));
+        if (contiguous) {
+            // A run of consecutive mesh indices takes the staged mesh contraction.
+            if ((st = run_front(pl, nb, indices[s], mesh, nullptr, 1)) != WNLQG_OK) return st;
+        } else {
+            WNLQG_CUDA(cudaMemcpyAsync(pl->d_kidx, indices + s, (size_t)nb * sizeof(int64_t), cudaMemcpyHostToDevice,
+                                       pl->stream));
+            if ((st = run_front(pl, nb, 0, mesh, nullptr, 1, pl->d_kidx)) != WNLQG_OK) return st;
+        }
         if ((st = run_passes(pl, nb, 0, 1.0, 0, pl->d_weights)) != WNLQG_OK) return st;
     }
     reduce_partials_kernel<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((pl->vc + 255) / 256, 1024)), 256, 0,

@@ -102,6 +102,21 @@ class ResponseEngine:
             out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
         return out
 
+    def mesh_weighted_sum(self, mesh: Sequence[int], indices, weights) -> np.ndarray:
+        """sum_i weights[i] * value(mesh point indices[i]) from host arrays, complex [value_count]."""
+        mesh_a = np.ascontiguousarray(np.asarray(mesh, dtype=np.int64))
+        idx = np.ascontiguousarray(np.asarray(indices, dtype=np.int64).reshape(-1))
+        w = np.ascontiguousarray(np.asarray(weights, dtype=np.float64).reshape(-1))
+        if idx.shape != w.shape:
+            raise ValueError("one weight per index")
+        out = np.zeros(self.value_count, dtype=np.complex128)
+        ip = ctypes.POINTER(ctypes.c_int64)
+        _lib.check(self._L.wnlqg_b200_eval_mesh_weighted(
+            self._plan, mesh_a.ctypes.data_as(ip), idx.ctypes.data_as(ip),
+            w.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), idx.shape[0],
+            out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return out
+
     def spectrum(self, kpoints):
         """(energies [n, nw], canonical eigenvectors [n, nw, nw]) at fractional k-points."""
         k = np.ascontiguousarray(np.asarray(kpoints, dtype=np.float64).reshape(-1, 3))
