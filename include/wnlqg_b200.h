@@ -107,6 +107,7 @@ typedef struct wnlqg_task_desc {
     int64_t num_fermi_energies;        /* mu axis for AHC / Berry dipole */
     const double *fermi_energies;      /* eV */
     int32_t precision;                 /* wnlqg_precision */
+    double fermi_surface_broadening;   /* eV; Gaussian width of -f' at T = 0 (Berry dipole) */
 } wnlqg_task_desc;
 
 typedef struct wnlqg_model wnlqg_model;   /* device-resident model */

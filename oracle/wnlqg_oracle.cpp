@@ -18,6 +18,11 @@
 //   injection current           src/Responses/InjectionCurrent/ConventionalInjectionCurrent.jl:23-211
 //   prefactors                  src/Runtime/Execution/ConventionalCurrentIntegralExecution.jl:241-245, 294-298
 //   Berry curvature / metric    src/Responses/QuantumGeometry/ConventionalQuantumGeometry.jl:188-215, 321-355
+//   intrinsic AHC (T = 0)       src/Responses/IntrinsicHall/IntrinsicHallOccupations.jl:8-44,
+//                               IntrinsicHallCurvature.jl:2-29; MatrixElements/IntrinsicHallGeometry.jl:117-136
+//   Berry-curvature dipole      src/Responses/QuantumGeometry/BerryMultipoleMoments.jl:7-47,
+//                               BerryMultipoleGeometry.jl:66-161, BerryMultipoleDC.jl:64-75;
+//                               Responses/Shared/ResponseOccupations.jl:10-36
 //   jerk                        src/Responses/JerkCurrent/ConventionalJerkCurrent.jl:14-65;
 //                               MatrixElements/Interpolated/ThirdOrderGeometry.jl:28-41, 131-160
 //   mesh + lanes                src/Core/CalculationUtils.jl:280-292; Runtime/Setup/BundleAssembly.jl:35-53;
@@ -45,6 +50,7 @@ const double ELEMENTARY_CHARGE_C = 1.602176634e-19;
 const double REDUCED_PLANCK_CONSTANT_J_S = 1.054571817e-34;
 const double REDUCED_PLANCK_CONSTANT_EV_S = 6.582119569e-16;
 const double BOLTZMANN_CONSTANT_EV_K = 8.617333262e-5;
+const double RESPONSE_KB_EV = 8.617333262145e-5;   // Responses/Shared/ResponseOccupations.jl:4
 
 thread_local std::string g_error;
 
@@ -439,6 +445,11 @@ bool build_task(const wnlqg_task_desc *t, Task &task) {
             case WNLQG_QUANTUM_METRIC:
                 task.need.need_r(a); task.need.need_r(b);
                 break;
+            case WNLQG_INTRINSIC_AHC:
+            case WNLQG_BERRY_DIPOLE:
+                task.need.F[a][b] = true; task.need.need_r(a); task.need.need_r(b);
+                if (q.kind == WNLQG_BERRY_DIPOLE) task.need.dH[cc] = true;
+                break;
             case WNLQG_JERK_CURRENT:
                 task.need.need_r(b); task.need.need_r(cc);
                 task.need.dH[a] = true; task.need.dH[dd] = true;
@@ -450,7 +461,13 @@ bool build_task(const wnlqg_task_desc *t, Task &task) {
         }
         if (q.kind == WNLQG_SHIFT_CURRENT || q.kind == WNLQG_INJECTION_CURRENT || q.kind == WNLQG_JERK_CURRENT)
             count += q.num_components * t->num_photon_energies;
-        else
+        else if (q.kind == WNLQG_INTRINSIC_AHC || q.kind == WNLQG_BERRY_DIPOLE) {
+            if (t->num_fermi_energies < 1) { set_error("a Fermi-energy axis is required"); return false; }
+            if (q.kind == WNLQG_BERRY_DIPOLE && t->temperature == 0.0 && !(t->fermi_surface_broadening > 0)) {
+                set_error("T=0 requires positive eta_fs_ev"); return false;
+            }
+            count += q.num_components * t->num_fermi_energies;
+        } else
             count += q.num_components;
     }
     task.value_count = count;
@@ -608,6 +625,64 @@ void point_values(const Model &m, const Task &task, const double k[3], cd *out) 
                 o[c] = cd(value, 0.0);
             }
             o += nc;
+        } else if (q.kind == WNLQG_INTRINSIC_AHC || q.kind == WNLQG_BERRY_DIPOLE) {
+            const int64_t nmu = t.num_fermi_energies;
+            for (int c = 0; c < nc; ++c) {
+                const int a = q.components[c][0], b = q.components[c][1], cc = q.components[c][2];
+                for (int64_t im = 0; im < nmu; ++im) {
+                    const double mu = t.fermi_energies[im];
+                    double value = 0.0;
+                    if (q.kind == WNLQG_INTRINSIC_AHC && t.temperature == 0.0) {
+                        // Occupied-space matrix curvature with bare occupied/empty links
+                        // r_lm = A_lm - i dH_lm/(E_l - E_m) (IntrinsicHallGeometry.jl:117-136).
+                        int occ = 0;
+                        while (occ < n && d.E[occ] <= mu) ++occ;
+                        for (int l = 0; l < occ; ++l) {
+                            value += d.F[a][b](l, l).real();
+                            for (int m = occ; m < n; ++m) {
+                                auto link = [&](int x, int y, int ax) {
+                                    return d.Aint[ax](x, y) - I1 * d.dH[ax](x, y) / (d.E[x] - d.E[y]);
+                                };
+                                cd left = link(l, m, a) * link(m, l, b);
+                                cd right = link(l, m, b) * link(m, l, a);
+                                value -= (left - right).imag();
+                            }
+                        }
+                    } else if (q.kind == WNLQG_INTRINSIC_AHC) {
+                        // Finite temperature: occupation-weighted Berry curvature (the Fermi-sea
+                        // form of berry_curvature_occupied_sum_component, ConventionalQuantumGeometry.jl:188-215).
+                        std::vector<double> fm;
+                        fermi(d.E, mu, t.temperature, fm);
+                        cd v(0.0, 0.0);
+                        for (int nn = 0; nn < n; ++nn) {
+                            v += fm[nn] * d.F[a][b](nn, nn);
+                            for (int mm = 0; mm < n; ++mm)
+                                if (mm != nn) v += (fm[nn] - fm[mm]) * I1 * d.r[a](nn, mm) * d.r[b](mm, nn);
+                        }
+                        value = v.real();
+                    } else {
+                        // D[mu,a,b,c] = sum_n (-f'(E_n)) Omega_n^{ab} dE_n/dk_c.
+                        for (int nn = 0; nn < n; ++nn) {
+                            double omega = 0.0;
+                            for (int mm = 0; mm < n; ++mm)
+                                if (mm != nn) omega += -(d.r[a](nn, mm) * d.r[b](mm, nn)).imag();
+                            omega = 2.0 * omega + d.F[a][b](nn, nn).real();
+                            double w;
+                            if (t.temperature > 0) {
+                                const double scale = RESPONSE_KB_EV * t.temperature;
+                                const double z = std::exp(-std::fabs((d.E[nn] - mu) / scale));
+                                w = z / (scale * (1 + z) * (1 + z));
+                            } else {
+                                const double x = (d.E[nn] - mu) / t.fermi_surface_broadening;
+                                w = std::exp(-x * x) / (std::sqrt(PI) * t.fermi_surface_broadening);
+                            }
+                            value += w * omega * d.dH[cc](nn, nn).real();
+                        }
+                    }
+                    o[im + nmu * c] = cd(value, 0.0);
+                }
+            }
+            o += nmu * nc;
         } else if (q.kind == WNLQG_JERK_CURRENT) {
             std::vector<cd> B((size_t)n * n * 3, 0.0), A((size_t)n * n * 3, 0.0), C((size_t)n * n * 9, 0.0);
             for (int a = 0; a < 3; ++a) {

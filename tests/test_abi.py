@@ -38,8 +38,9 @@ def test_struct_sizes_match_c():
 #include <stddef.h>
 #include "wnlqg_b200.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu\n", sizeof(wnlqg_model_desc), sizeof(wnlqg_response_request), sizeof(wnlqg_task_desc),
-         offsetof(wnlqg_task_desc, fermi_energy), offsetof(wnlqg_task_desc, precision));
+  printf("%zu %zu %zu %zu %zu %zu\n", sizeof(wnlqg_model_desc), sizeof(wnlqg_response_request), sizeof(wnlqg_task_desc),
+         offsetof(wnlqg_task_desc, fermi_energy), offsetof(wnlqg_task_desc, precision),
+         offsetof(wnlqg_task_desc, fermi_surface_broadening));
   return 0;
 }
 '''
@@ -50,5 +51,6 @@ int main(void) {
         subprocess.run(["/usr/bin/gcc", "-I", os.path.join(ROOT, "include"), c, "-o", exe], check=True)
         out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()
     got = [ctypes.sizeof(_abi.ModelDesc), ctypes.sizeof(_abi.ResponseRequest), ctypes.sizeof(_abi.TaskDesc),
-           _abi.TaskDesc.fermi_energy.offset, _abi.TaskDesc.precision.offset]
+           _abi.TaskDesc.fermi_energy.offset, _abi.TaskDesc.precision.offset,
+           _abi.TaskDesc.fermi_surface_broadening.offset]
     assert [int(x) for x in out] == got

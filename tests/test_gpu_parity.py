@@ -225,3 +225,42 @@ def test_mesh_weighted_sum_contiguous_and_scattered(engine_cls, oracle_mod):
     ref2 = (oracle_mod.point_values(model, task, k) * w[:, None]).sum(axis=0)
     for g, r in zip(task.split(got2), task.split(ref2)):
         assert rel_err(g, r) < RTOL
+
+
+@pytest.mark.parametrize("precision", [_abi.PRECISION_FP64, _abi.PRECISION_MIXED])
+@pytest.mark.parametrize("temperature", [0.0, 50.0])
+def test_ahc_and_berry_dipole_match_oracle(engine_cls, oracle_mod, precision, temperature):
+    model = synthetic_orthogonal_model(8, 1, 6, full_position=True)
+    task = _abi.TaskArrays([(_abi.INTRINSIC_AHC, ["xy", "zx"]), (_abi.BERRY_DIPOLE, ["xyz", "xzx", "yzy"])],
+                           fermi_energies=[-0.5, 0.0, 0.5], temperature=temperature,
+                           fermi_surface_broadening=0.05, precision=precision)
+    tol = RTOL if precision == _abi.PRECISION_FP64 else MIXED_RTOL
+    k = np.random.default_rng(17).random((12, 3))
+    with engine_cls(model, task) as eng:
+        got = eng.point_values(k)
+        gm = eng.integrate_mesh((6, 4, 4))
+    ref = oracle_mod.point_values(model, task, k)
+    rm = oracle_mod.integrate_mesh(model, task, (6, 4, 4))
+    for g, r in zip(task.split(got), task.split(ref)):
+        assert rel_err(g, r) < tol
+    for g, r in zip(task.split(gm), task.split(rm)):
+        assert rel_err(g, r) < tol
+
+
+@pytest.mark.parametrize("precision", [_abi.PRECISION_FP64, _abi.PRECISION_MIXED])
+@pytest.mark.parametrize("kind", [_abi.GAUSSIAN, _abi.LORENTZIAN])
+def test_jerk_matches_oracle(engine_cls, oracle_mod, precision, kind):
+    import itertools
+    comps = ["".join(c) for c in itertools.product("xyz", repeat=4)][::7]
+    model = synthetic_orthogonal_model(8, 1, 9, full_position=True)
+    task = _abi.TaskArrays([(_abi.JERK_CURRENT, comps)], broadening_type=kind, broadening=0.05,
+                           photon_energies=np.linspace(0.2, 3.0, 20), precision=precision)
+    tol = RTOL if precision == _abi.PRECISION_FP64 else MIXED_RTOL
+    k = np.random.default_rng(18).random((10, 3))
+    with engine_cls(model, task) as eng:
+        got = eng.point_values(k)
+        gm = eng.integrate_mesh((5, 3, 3))
+    ref = oracle_mod.point_values(model, task, k)
+    rm = oracle_mod.integrate_mesh(model, task, (5, 3, 3))
+    assert rel_err(got, ref) < tol
+    assert rel_err(gm, rm) < tol

@@ -114,3 +114,27 @@ def test_generalized_derivative_finite_difference(oracle_mod):
                            photon_energies=[1.0], denominator_regularization=0.0)
     val = oracle_mod.point_values(model, task, k0)[0, 0]
     assert np.isfinite(val)
+
+
+def test_ahc_zero_temperature_matches_occupied_curvature(oracle_mod):
+    """T=0 intrinsic AHC (bare occupied/empty links) equals the occupied-sum Berry curvature up to
+    the eta^2/gap^2 difference between bare and regularised links."""
+    model = synthetic_orthogonal_model(6, 1, 2, full_position=True)
+    mus = [-0.3, 0.0, 0.4]
+    k = np.random.default_rng(8).random((6, 3))
+    ahc = _abi.TaskArrays([(_abi.INTRINSIC_AHC, ["xy", "yz"])], fermi_energies=mus)
+    a = oracle_mod.point_values(model, ahc, k)
+    for i, mu in enumerate(mus):
+        bc = _abi.TaskArrays([(_abi.BERRY_CURVATURE, ["xy", "yz"])], fermi_energy=mu, denominator_regularization=1e-7)
+        b = oracle_mod.point_values(model, bc, k)
+        np.testing.assert_allclose(a[:, [i, 3 + i]].real, b.real, rtol=1e-6, atol=1e-9)
+
+
+def test_berry_dipole_finite_temperature_weight_integrates_to_one():
+    """-f'(E) of the dipole weight (ResponseOccupations.jl:24-36) integrates to one over E."""
+    kb = 8.617333262145e-5
+    T = 50.0
+    e = np.linspace(-1, 1, 200001)
+    z = np.exp(-np.abs(e / (kb * T)))
+    w = z / (kb * T * (1 + z) ** 2)
+    assert abs(np.trapezoid(w, e) - 1.0) < 1e-6

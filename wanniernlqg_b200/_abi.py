@@ -77,6 +77,7 @@ class TaskDesc(ctypes.Structure):
         ("num_fermi_energies", ctypes.c_int64),
         ("fermi_energies", ctypes.POINTER(ctypes.c_double)),
         ("precision", ctypes.c_int32),
+        ("fermi_surface_broadening", ctypes.c_double),
     ]
 
 
@@ -127,7 +128,8 @@ class TaskArrays:
     def __init__(self, responses: Sequence[tuple], *, fermi_energy=0.0, temperature=0.0,
                  broadening_type=GAUSSIAN, broadening=0.040, transition_window_factor=5.0,
                  denominator_regularization=0.001, degeneracy_threshold=2.0e-3,
-                 photon_energies=(0.10,), fermi_energies=(), precision=PRECISION_FP64):
+                 photon_energies=(0.10,), fermi_energies=(), precision=PRECISION_FP64,
+                 fermi_surface_broadening=0.0):
         if not 1 <= len(responses) <= MAX_RESPONSES:
             raise ValueError("between 1 and 8 responses are supported per task")
         self.photon_energies = np.ascontiguousarray(np.asarray(photon_energies, dtype=np.float64))
@@ -158,6 +160,7 @@ class TaskArrays:
         d.num_fermi_energies = self.fermi_energies.size
         d.fermi_energies = _dptr(self.fermi_energies) if self.fermi_energies.size else None
         d.precision = int(precision)
+        d.fermi_surface_broadening = float(fermi_surface_broadening)
         self.desc = d
 
     def value_count(self) -> int:

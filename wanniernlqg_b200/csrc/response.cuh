@@ -23,8 +23,11 @@
 #define RS_MAX_SCALAR 16
 #define RS_MAX_G 9
 
-enum { RS_FC_SHIFT = 1, RS_FC_INJECTION = 2 };
+enum { RS_FC_SHIFT = 1, RS_FC_INJECTION = 2, RS_FC_JERK = 3 };
 enum { RS_SC_BERRY = 1, RS_SC_METRIC = 2 };
+enum { RS_MU_AHC = 1, RS_MU_DIPOLE = 2 };
+#define RS_MAX_HESS 9
+#define RS_MU_CHUNK 8
 
 struct RespParams {
     int nw, ld;
@@ -45,6 +48,19 @@ struct RespParams {
     int fc_g1[RS_MAX_FREQ], fc_g2[RS_MAX_FREQ];   // index into the g list: G(c,a), G(b,a)
     double fc_pref[RS_MAX_FREQ];
     int64_t fc_out[RS_MAX_FREQ];
+    // Pair family of the frequency components: 0 = transition screen (shift/injection),
+    // 1 = positive-gap pairs with a windowed delta (jerk).
+    int pair_mode;
+    int fc_hess[RS_MAX_FREQ];                     // jerk: index into the Hessian list (a,d)
+    int n_hess;
+    int hess_a[RS_MAX_HESS], hess_d[RS_MAX_HESS];
+    // Fermi-energy-axis components (intrinsic AHC, Berry-curvature dipole).
+    int n_mu;
+    int mu_kind[RS_MAX_SCALAR], mu_a[RS_MAX_SCALAR], mu_b[RS_MAX_SCALAR], mu_c[RS_MAX_SCALAR];
+    int64_t mu_out[RS_MAX_SCALAR];
+    int nmu;
+    const double *mus;
+    double temperature, fs_width;
     // Scalar components (Berry curvature, quantum metric).
     int n_sc;
     int sc_kind[RS_MAX_SCALAR], sc_a[RS_MAX_SCALAR], sc_b[RS_MAX_SCALAR];
@@ -70,7 +86,7 @@ struct RespParams {
 
 struct RespSmem {
     // Byte offsets inside the dynamic shared memory.
-    size_t U, T1, T2, slots, inv, E, f, te, fnm, Q, fd, red, total;
+    size_t U, T1, T2, slots, inv, E, f, te, fnm, Q, fd, hess, red, total;
     static __host__ __device__ RespSmem layout(int nw, int n_slots, int n_fc, int n_berry, int csize) {
         RespSmem s;
         int ld = nw + 1;
@@ -87,7 +103,8 @@ struct RespSmem {
         s.te = take((size_t)nw * nw * sizeof(double));
         s.fnm = take((size_t)nw * nw * sizeof(double));
         s.Q = take((size_t)nw * nw * (n_fc > 0 ? n_fc : 1) * csize);
-        s.fd = take((size_t)2 * nw * (n_berry > 0 ? n_berry : 1) * sizeof(double2));
+        s.fd = take((size_t)4 * nw * (n_berry > 0 ? n_berry : 1) * sizeof(double2));
+        s.hess = take((size_t)RS_MAX_HESS * nw * sizeof(double));
         s.red = take(64 * sizeof(double) + 64 * sizeof(int));
         s.total = off;
         return s;
@@ -259,6 +276,7 @@ __global__ void __launch_bounds__(256) response_kernel(RespParams p) {
     double *sfnm = reinterpret_cast<double *>(sm + L.fnm);
     C *sQ = reinterpret_cast<C *>(sm + L.Q);
     double2 *sFd = reinterpret_cast<double2 *>(sm + L.fd);
+    double *sHess = reinterpret_cast<double *>(sm + L.hess);
     double *red = reinterpret_cast<double *>(sm + L.red);
     int *ired = reinterpret_cast<int *>(red + 64);
     const size_t matsz = (size_t)nw * ld;
@@ -379,6 +397,141 @@ __global__ void __launch_bounds__(256) response_kernel(RespParams p) {
             }
         }
 
+
+        // Fermi-energy-axis responses.
+        for (int s = 0; s < p.n_mu; ++s) {
+            const int a = p.mu_a[s], bb = p.mu_b[s], cc = p.mu_c[s];
+            // F_nn^{ab} (Hamiltonian-gauge Wannier curvature diagonal) into sFd[2nw .. 3nw).
+            rotate_diagonal(xw + (int64_t)p.ch_dA[bb * 3 + a] * nn, T1, T2, sU, sFd, nw, ld);
+            rotate_diagonal(xw + (int64_t)p.ch_dA[a * 3 + bb] * nn, T1, T2, sU, sFd + nw, nw, ld);
+            const C *Aa = slot(p.slot_A[a]), *Ab = slot(p.slot_A[bb]);
+            const C *Ha = slot(p.slot_dH[a]), *Hb = slot(p.slot_dH[bb]);
+            for (int n = threadIdx.x; n < nw; n += blockDim.x) {
+                double2 comm = make_double2(0.0, 0.0);
+                for (int l = 0; l < nw; ++l)
+                    comm = cadd(comm, to_c64(csub(cmul(Aa[n + ld * l], Ab[l + ld * n]), cmul(Ab[n + ld * l], Aa[l + ld * n]))));
+                sFd[2 * nw + n] = csub(csub(sFd[n], sFd[nw + n]), cmuli(comm));
+            }
+            __syncthreads();
+            if (p.mu_kind[s] == RS_MU_DIPOLE) {
+                // Band Berry curvature Omega_n = -2 sum_m Im(r^a_nm r^b_mn) + Re F_nn
+                // (berry_curvature_component, ConventionalQuantumGeometry.jl:166-180) into sFd[3nw..).
+                for (int n = threadIdx.x; n < nw; n += blockDim.x) {
+                    double om = 0.0;
+                    for (int m = 0; m < nw; ++m)
+                        if (m != n) om += -to_c64(cmul(r_elem(a, n, m), r_elem(bb, m, n))).y;
+                    sFd[3 * nw + n] = make_double2(2.0 * om + sFd[2 * nw + n].x, 0.0);
+                }
+                __syncthreads();
+                if (threadIdx.x == 0) {
+                    const C *Hc = slot(p.slot_dH[cc]);
+                    for (int im = 0; im < p.nmu; ++im) {
+                        const double mu = p.mus[im];
+                        double value = 0.0;
+                        for (int n = 0; n < nw; ++n) {
+                            double w;
+                            if (p.temperature > 0.0) {
+                                const double scale = 8.617333262145e-5 * p.temperature;
+                                const double z = exp(-fabs((sE[n] - mu) / scale));
+                                w = z / (scale * (1.0 + z) * (1.0 + z));
+                            } else {
+                                const double x = (sE[n] - mu) / p.fs_width;
+                                w = exp(-x * x) / (sqrt(WNLQG_PI) * p.fs_width);
+                            }
+                            value += w * sFd[3 * nw + n].x * (double)Hc[n + ld * n].x;
+                        }
+                        const int64_t idx = p.mu_out[s] + im;
+                        if (p.mode == 0) {
+                            double *a4 = p.partials + ((int64_t)blockIdx.x * p.vc + idx) * 4;
+                            neumaier_add(a4[0], a4[2], value * wk);
+                        } else {
+                            p.out_points[(p.point_offset + b) * p.vc + idx] = make_double2(value * p.scale, 0.0);
+                        }
+                    }
+                }
+                __syncthreads();
+            } else {
+                for (int m0 = 0; m0 < p.nmu; m0 += RS_MU_CHUNK) {
+                    double loc[RS_MU_CHUNK];
+                    int nocc[RS_MU_CHUNK];
+#pragma unroll
+                    for (int j = 0; j < RS_MU_CHUNK; ++j) {
+                        loc[j] = 0.0;
+                        nocc[j] = 0;
+                        if (m0 + j < p.nmu) {
+                            const double mu = p.mus[m0 + j];
+                            for (int n = 0; n < nw; ++n) nocc[j] += sE[n] <= mu ? 1 : 0;
+                        }
+                    }
+                    for (int e = threadIdx.x; e < nn; e += blockDim.x) {
+                        const int l = e % nw, m = e / nw;
+                        if (p.temperature == 0.0) {
+                            // Matrix curvature with bare occupied/empty links
+                            // (IntrinsicHallCurvature.jl:2-29, IntrinsicHallGeometry.jl:117-136).
+                            double pair = 0.0;
+                            if (l != m) {
+                                const double g = sE[l] - sE[m];
+                                auto link = [&](int ax, int x, int y, double inv) {
+                                    const double2 A = to_c64(slot(p.slot_A[ax])[x + ld * y]);
+                                    const double2 H = to_c64(slot(p.slot_dH[ax])[x + ld * y]);
+                                    return cadd(A, cmuli(cscale(H, -inv)));
+                                };
+                                const double ilm = 1.0 / g, iml = -1.0 / g;
+                                const double2 left = cmul(link(a, l, m, ilm), link(bb, m, l, iml));
+                                const double2 right = cmul(link(bb, l, m, ilm), link(a, m, l, iml));
+                                pair = -(left.y - right.y);
+                            }
+#pragma unroll
+                            for (int j = 0; j < RS_MU_CHUNK; ++j) {
+                                if (m0 + j >= p.nmu) continue;
+                                if (l == m) { if (l < nocc[j]) loc[j] += sFd[2 * nw + l].x; }
+                                else if (l < nocc[j] && m >= nocc[j]) loc[j] += pair;
+                            }
+                        } else {
+                            // Finite temperature: occupation-weighted Berry curvature.
+                            const double2 t = l == m ? make_double2(0.0, 0.0)
+                                                     : cmuli(to_c64(cmul(r_elem(a, l, m), r_elem(bb, m, l))));
+#pragma unroll
+                            for (int j = 0; j < RS_MU_CHUNK; ++j) {
+                                if (m0 + j >= p.nmu) continue;
+                                const double mu = p.mus[m0 + j];
+                                const double fl = fermi_occ(sE[l], mu, p.kT);
+                                if (l == m) loc[j] += fl * sFd[2 * nw + l].x;
+                                else loc[j] += (fl - fermi_occ(sE[m], mu, p.kT)) * t.x;
+                            }
+                        }
+                    }
+                    for (int j = 0; j < RS_MU_CHUNK && m0 + j < p.nmu; ++j) {
+                        const double total = block_sum(loc[j], red);
+                        if (threadIdx.x == 0) {
+                            const int64_t idx = p.mu_out[s] + m0 + j;
+                            if (p.mode == 0) {
+                                double *a4 = p.partials + ((int64_t)blockIdx.x * p.vc + idx) * 4;
+                                neumaier_add(a4[0], a4[2], total * wk);
+                            } else {
+                                p.out_points[(p.point_offset + b) * p.vc + idx] = make_double2(total * p.scale, 0.0);
+                            }
+                        }
+                    }
+                }
+            }
+        }
+
+        // Band Hessians for jerk: H_n^{ad} = Re ddH_ad[n,n] + 2 sum_{l!=n} Re(dH_a[n,l] dH_d[l,n]) reg(E_n-E_l)
+        // (prepare_third_order_band_geometry!, ThirdOrderGeometry.jl:131-160).
+        for (int h = 0; h < p.n_hess; ++h) {
+            const int a = p.hess_a[h], dd = p.hess_d[h];
+            rotate_diagonal(xw + (int64_t)p.ch_ddH[a * 3 + dd] * nn, T1, T2, sU, sFd, nw, ld);
+            const C *Ha = slot(p.slot_dH[a]), *Hd = slot(p.slot_dH[dd]);
+            for (int n = threadIdx.x; n < nw; n += blockDim.x) {
+                double v = sFd[n].x;
+                for (int l = 0; l < nw; ++l)
+                    if (l != n) v += 2.0 * to_c64(cmul(Ha[n + ld * l], Hd[l + ld * n])).x * sinv[n + nw * l];
+                sHess[h * nw + n] = v;
+            }
+            __syncthreads();
+        }
+
         if (p.n_fc > 0) {
             // Transition screen and per-pair kernels; pairs kept in column-major (n fastest) order.
             if (threadIdx.x == 0) { ired[0] = 0; ired[1] = 0; }
@@ -388,7 +541,15 @@ __global__ void __launch_bounds__(256) response_kernel(RespParams p) {
                 bool keep = false;
                 int n = 0, m = 0;
                 double fnm = 0.0, te = 0.0;
-                if (e < nn) {
+                if (e < nn && p.pair_mode == 1) {
+                    // Jerk: ordered pairs with E_n > E_m, weight (f_m - f_n) delta(E_n - E_m - omega)
+                    // (ConventionalJerkCurrent.jl:39-61); exactly-zero occupation differences add zero.
+                    n = e % nw; m = e / nw;
+                    te = sE[n] - sE[m];
+                    fnm = sf[m] - sf[n];
+                    keep = te > 0.0 && fnm != 0.0;
+                    if (keep) ired[1] = 1;
+                } else if (e < nn) {
                     n = e % nw; m = e / nw;
                     fnm = sf[n] - sf[m];
                     te = sE[m] - sE[n];
@@ -416,7 +577,11 @@ __global__ void __launch_bounds__(256) response_kernel(RespParams p) {
                         const int a = p.fc_a[c], bb = p.fc_b[c], cc = p.fc_c[c];
                         const C rc_nm = r_elem(cc, n, m), rb_mn = r_elem(bb, m, n);
                         C q;
-                        if (p.fc_kind[c] == RS_FC_SHIFT) {
+                        if (p.fc_kind[c] == RS_FC_JERK) {
+                            const int hh = p.fc_hess[c];
+                            const R dh = (R)(sHess[hh * nw + n] - sHess[hh * nw + m]);
+                            q = cscale(cmul(r_elem(bb, n, m), r_elem(cc, m, n)), dh);
+                        } else if (p.fc_kind[c] == RS_FC_SHIFT) {
                             const C *G1 = slot(p.g_slot[p.fc_g1[c]]), *G2 = slot(p.g_slot[p.fc_g2[c]]);
                             q = cmulmi(csub(cmul(G1[n + ld * m], rb_mn), cmul(G2[m + ld * n], rc_nm)));
                         } else {
@@ -440,6 +605,7 @@ __global__ void __launch_bounds__(256) response_kernel(RespParams p) {
             // streams the pair list once per pass.
             const R w2 = (R)(p.width * p.width), lor = (R)(p.width / WNLQG_PI);
             const R gsc = (R)p.gscale, cut = (R)p.cutoff, invw = (R)(1.0 / p.width);
+            const R win = (R)(p.thr > 0.0 ? p.thr : 0.0);
             for (int w0 = 0; w0 < p.nom; w0 += RS_OMB * blockDim.x) {
                 double om[RS_OMB];
 #pragma unroll
@@ -464,7 +630,12 @@ __global__ void __launch_bounds__(256) response_kernel(RespParams p) {
                             for (int j = 0; j < RS_OMB; ++j) {
                                 const R x = (R)(te - om[j]);
                                 R delta;
-                                if (p.gaussian) {
+                                if (p.pair_mode == 1) {
+                                    // second_harmonic_delta with the transition window (SecondHarmonicKernels.jl:86-89).
+                                    if (win > (R)0 && fabs(x) > win) continue;
+                                    const R y = x * invw;
+                                    delta = p.gaussian ? gsc * exp(-y * y) : lor / (x * x + w2);
+                                } else if (p.gaussian) {
                                     if (!(fabs(x) < cut)) continue;
                                     const R y = x * invw;
                                     delta = gsc * exp(-y * y);

@@ -75,6 +75,7 @@ struct wnlqg_plan {
     double2 *d_tiles = nullptr, *d_phase = nullptr, *d_xw = nullptr, *d_U = nullptr, *d_out = nullptr;
     double2 *d_points = nullptr;
     double *d_E = nullptr, *d_kpts = nullptr, *d_omegas = nullptr, *d_partials = nullptr, *d_weights = nullptr;
+    double *d_mus = nullptr;
     int64_t *d_kidx = nullptr;
     int partial_slots = 0;
     // Staged mesh Fourier: R grouping (device) and lazily sized Y/Z workspaces.
@@ -141,21 +142,25 @@ int response_threads(int nw) {
 // per-pass limits and the shared-memory budget.
 wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
     const wnlqg_task_desc &t = pl->task;
-    struct Item { int kind; int a, b, c; int64_t out; };
+    struct Item { int kind; int a, b, c, d; int64_t out; };
     std::vector<Item> items;
     int64_t off = 0;
     for (int r = 0; r < t.num_responses; ++r) {
         const wnlqg_response_request &q = t.responses[r];
         for (int c = 0; c < q.num_components; ++c) {
             const int32_t *x = q.components[c];
-            if (q.kind == WNLQG_SHIFT_CURRENT || q.kind == WNLQG_INJECTION_CURRENT) {
-                items.push_back({q.kind, x[0], x[1], x[2], off + (int64_t)c * t.num_photon_energies});
+            if (q.kind == WNLQG_SHIFT_CURRENT || q.kind == WNLQG_INJECTION_CURRENT || q.kind == WNLQG_JERK_CURRENT) {
+                items.push_back({q.kind, x[0], x[1], x[2], x[3], off + (int64_t)c * t.num_photon_energies});
+            } else if (q.kind == WNLQG_INTRINSIC_AHC || q.kind == WNLQG_BERRY_DIPOLE) {
+                items.push_back({q.kind, x[0], x[1], x[2], 0, off + (int64_t)c * t.num_fermi_energies});
             } else {
-                items.push_back({q.kind, x[0], x[1], 0, off + c});
+                items.push_back({q.kind, x[0], x[1], 0, 0, off + c});
             }
         }
-        if (q.kind == WNLQG_SHIFT_CURRENT || q.kind == WNLQG_INJECTION_CURRENT)
+        if (q.kind == WNLQG_SHIFT_CURRENT || q.kind == WNLQG_INJECTION_CURRENT || q.kind == WNLQG_JERK_CURRENT)
             off += (int64_t)q.num_components * t.num_photon_energies;
+        else if (q.kind == WNLQG_INTRINSIC_AHC || q.kind == WNLQG_BERRY_DIPOLE)
+            off += (int64_t)q.num_components * t.num_fermi_energies;
         else
             off += q.num_components;
     }
@@ -200,7 +205,14 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
         }
         for (int a = 0; a < 9; ++a) { p.ch_ddH[a] = pl->ch_ddH[a]; p.ch_dA[a] = pl->ch_dA[a]; }
         bool needH[3] = {false, false, false}, needA[3] = {false, false, false}, needD[3] = {false, false, false};
-        std::vector<std::pair<int, int>> gl;
+        std::vector<std::pair<int, int>> gl, hl;
+        auto hindex = [&](int aa, int dd, bool commit) {
+            for (size_t h = 0; h < hl.size(); ++h)
+                if (hl[h].first == aa && hl[h].second == dd) return (int)h;
+            if (!commit) return (int)hl.size();
+            hl.push_back({aa, dd});
+            return (int)hl.size() - 1;
+        };
         auto gindex = [&](int pp, int dd, bool commit) {
             for (size_t g = 0; g < gl.size(); ++g)
                 if (gl[g].first == pp && gl[g].second == dd) return (int)g;
@@ -216,9 +228,13 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
             std::copy(needH, needH + 3, tH);
             std::copy(needA, needA + 3, tA);
             std::copy(needD, needD + 3, tD);
-            int newg = 0;
+            int newg = 0, newh = 0;
             auto need_r = [&](int a) { tH[a] = true; tA[a] = true; };
-            bool freq = it.kind == WNLQG_SHIFT_CURRENT || it.kind == WNLQG_INJECTION_CURRENT;
+            const bool freq = it.kind == WNLQG_SHIFT_CURRENT || it.kind == WNLQG_INJECTION_CURRENT ||
+                              it.kind == WNLQG_JERK_CURRENT;
+            const bool muaxis = it.kind == WNLQG_INTRINSIC_AHC || it.kind == WNLQG_BERRY_DIPOLE;
+            const int mode = it.kind == WNLQG_JERK_CURRENT ? 1 : 0;
+            if (freq && p.n_fc > 0 && p.pair_mode != mode) break;   // one pair family per pass
             if (it.kind == WNLQG_SHIFT_CURRENT) {
                 need_r(it.a); need_r(it.b); need_r(it.c);
                 tD[it.a] = true;
@@ -226,15 +242,21 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
                 if (!(it.b == it.c) && gindex(it.b, it.a, false) == (int)gl.size()) ++newg;
             } else if (it.kind == WNLQG_INJECTION_CURRENT) {
                 tH[it.a] = true; need_r(it.b); need_r(it.c);
+            } else if (it.kind == WNLQG_JERK_CURRENT) {
+                tH[it.a] = true; tH[it.d] = true; need_r(it.b); need_r(it.c);
+                if (hindex(it.a, it.d, false) == (int)hl.size()) ++newh;
             } else {
                 need_r(it.a); need_r(it.b);
+                if (it.kind == WNLQG_BERRY_DIPOLE) tH[it.c] = true;
             }
             int nslots = (int)gl.size() + newg;
             for (int a = 0; a < 3; ++a) nslots += (tH[a] ? 1 : 0) + (tA[a] ? 1 : 0) + (tD[a] ? 1 : 0);
             int nfc = p.n_fc + (freq ? 1 : 0);
-            int nsc = p.n_sc + (freq ? 0 : 1);
+            int nsc = p.n_sc + ((!freq && !muaxis) ? 1 : 0);
+            int nmi = p.n_mu + (muaxis ? 1 : 0);
             size_t smem = RespSmem::layout(pl->nw, nslots, nfc, 1, csize).total;
-            bool fits = nfc <= RS_MAX_FREQ && nsc <= RS_MAX_SCALAR && (int)gl.size() + newg <= RS_MAX_G && smem <= smem_limit;
+            bool fits = nfc <= RS_MAX_FREQ && nsc <= RS_MAX_SCALAR && nmi <= RS_MAX_SCALAR &&
+                        (int)gl.size() + newg <= RS_MAX_G && (int)hl.size() + newh <= RS_MAX_HESS && smem <= smem_limit;
             if (!fits) {
                 if (i == start)
                     return fail(WNLQG_ERR_UNSUPPORTED, "one response component does not fit the shared-memory budget for nw=" +
@@ -250,10 +272,22 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
                 int c = p.n_fc++;
                 p.fc_kind[c] = RS_FC_SHIFT; p.fc_a[c] = it.a; p.fc_b[c] = it.b; p.fc_c[c] = it.c;
                 p.fc_g1[c] = g1; p.fc_g2[c] = g2; p.fc_pref[c] = P_sc; p.fc_out[c] = it.out;
+                p.pair_mode = 0;
             } else if (it.kind == WNLQG_INJECTION_CURRENT) {
                 int c = p.n_fc++;
                 p.fc_kind[c] = RS_FC_INJECTION; p.fc_a[c] = it.a; p.fc_b[c] = it.b; p.fc_c[c] = it.c;
                 p.fc_g1[c] = 0; p.fc_g2[c] = 0; p.fc_pref[c] = P_ic; p.fc_out[c] = it.out;
+                p.pair_mode = 0;
+            } else if (it.kind == WNLQG_JERK_CURRENT) {
+                int c = p.n_fc++;
+                p.fc_kind[c] = RS_FC_JERK; p.fc_a[c] = it.a; p.fc_b[c] = it.b; p.fc_c[c] = it.c;
+                p.fc_g1[c] = 0; p.fc_g2[c] = 0; p.fc_pref[c] = 1.0; p.fc_out[c] = it.out;
+                p.fc_hess[c] = hindex(it.a, it.d, true);
+                p.pair_mode = 1;
+            } else if (muaxis) {
+                int m = p.n_mu++;
+                p.mu_kind[m] = it.kind == WNLQG_INTRINSIC_AHC ? RS_MU_AHC : RS_MU_DIPOLE;
+                p.mu_a[m] = it.a; p.mu_b[m] = it.b; p.mu_c[m] = it.c; p.mu_out[m] = it.out;
             } else {
                 int s = p.n_sc++;
                 p.sc_kind[s] = it.kind == WNLQG_BERRY_CURVATURE ? RS_SC_BERRY : RS_SC_METRIC;
@@ -268,6 +302,12 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
         p.n_g = (int)gl.size();
         for (int g = 0; g < p.n_g; ++g) { p.g_p[g] = gl[g].first; p.g_d[g] = gl[g].second; p.g_slot[g] = slot++; }
         p.n_slots = slot;
+        p.n_hess = (int)hl.size();
+        for (int h = 0; h < p.n_hess; ++h) { p.hess_a[h] = hl[h].first; p.hess_d[h] = hl[h].second; }
+        p.nmu = (int)t.num_fermi_energies;
+        p.mus = pl->d_mus;
+        p.temperature = t.temperature;
+        p.fs_width = t.fermi_surface_broadening;
         p.nom = (int)t.num_photon_energies;
         p.omegas = pl->d_omegas;
         p.mu = t.fermi_energy;
@@ -488,7 +528,7 @@ wnlqg_status wnlqg_b200_plan_destroy(wnlqg_plan *pl) {
     for (void *ptr : {(void *)pl->d_tiles, (void *)pl->d_phase, (void *)pl->d_xw, (void *)pl->d_U, (void *)pl->d_out,
                       (void *)pl->d_points, (void *)pl->d_E, (void *)pl->d_kpts, (void *)pl->d_omegas,
                       (void *)pl->d_partials, (void *)pl->d_weights, (void *)pl->d_groups, (void *)pl->d_stageY,
-                      (void *)pl->d_stageZ, (void *)pl->d_V32, (void *)pl->d_kidx})
+                      (void *)pl->d_stageZ, (void *)pl->d_V32, (void *)pl->d_kidx, (void *)pl->d_mus})
         if (ptr) cudaFree(ptr);
     for (cudaEvent_t ev : pl->events) cudaEventDestroy(ev);
     if (pl->stream) cudaStreamDestroy(pl->stream);
@@ -571,13 +611,40 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
             case WNLQG_QUANTUM_METRIC:
                 need_r(a); need_r(b);
                 break;
+            case WNLQG_INTRINSIC_AHC:
+            case WNLQG_BERRY_DIPOLE:
+                need_r(a); need_r(b);
+                pl->ch_dA[b * 3 + a] = add_channel(ch, CH_DA, b, a);
+                pl->ch_dA[a * 3 + b] = add_channel(ch, CH_DA, a, b);
+                if (q.kind == WNLQG_BERRY_DIPOLE) pl->ch_dH[cc] = add_channel(ch, CH_DH, cc, 0);
+                break;
+            case WNLQG_JERK_CURRENT: {
+                const int dd = x[3];
+                need_r(b); need_r(cc);
+                pl->ch_dH[a] = add_channel(ch, CH_DH, a, 0);
+                pl->ch_dH[dd] = add_channel(ch, CH_DH, dd, 0);
+                const int hidx = add_channel(ch, CH_DDH, a, dd);
+                pl->ch_ddH[a * 3 + dd] = hidx;
+                pl->ch_ddH[dd * 3 + a] = hidx;
+                break;
+            }
             default:
                 return bail(fail(WNLQG_ERR_UNSUPPORTED, "response kind not supported by this build"));
             }
         }
-        if (q.kind == WNLQG_SHIFT_CURRENT || q.kind == WNLQG_INJECTION_CURRENT) {
+        if (q.kind == WNLQG_SHIFT_CURRENT || q.kind == WNLQG_INJECTION_CURRENT || q.kind == WNLQG_JERK_CURRENT) {
             if (t.num_photon_energies < 1) return bail(fail(WNLQG_ERR_INVALID_ARGUMENT, "photon energies required"));
+            if (q.kind == WNLQG_JERK_CURRENT && !(t.denominator_regularization > 0))
+                return bail(fail(WNLQG_ERR_INVALID_ARGUMENT, "third-order matrix width must be finite and positive"));
             vc += (int64_t)q.num_components * t.num_photon_energies;
+        } else if (q.kind == WNLQG_INTRINSIC_AHC || q.kind == WNLQG_BERRY_DIPOLE) {
+            if (t.num_fermi_energies < 1 || !t.fermi_energies)
+                return bail(fail(WNLQG_ERR_INVALID_ARGUMENT, "finite nonempty Fermi energy axis required"));
+            if (!finite_array(t.fermi_energies, (size_t)t.num_fermi_energies))
+                return bail(fail(WNLQG_ERR_INVALID_ARGUMENT, "finite nonempty Fermi energy axis required"));
+            if (q.kind == WNLQG_BERRY_DIPOLE && t.temperature == 0.0 && !(t.fermi_surface_broadening > 0))
+                return bail(fail(WNLQG_ERR_INVALID_ARGUMENT, "T=0 requires positive eta_fs_ev"));
+            vc += (int64_t)q.num_components * t.num_fermi_energies;
         } else {
             vc += q.num_components;
         }
@@ -653,6 +720,9 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
     if ((st = alloc((void **)&pl->d_points, (size_t)max_batch * vc * sizeof(double2))) != WNLQG_OK) return bail(st);
     if ((st = alloc((void **)&pl->d_out, (size_t)vc * sizeof(double2))) != WNLQG_OK) return bail(st);
     if ((st = alloc((void **)&pl->d_omegas, std::max<size_t>(1, pl->omegas.size()) * sizeof(double))) != WNLQG_OK) return bail(st);
+    if ((st = alloc((void **)&pl->d_mus, std::max<size_t>(1, pl->mus.size()) * sizeof(double))) != WNLQG_OK) return bail(st);
+    if (!pl->mus.empty())
+        WNLQG_CUDA(cudaMemcpy(pl->d_mus, pl->mus.data(), pl->mus.size() * sizeof(double), cudaMemcpyHostToDevice));
     WNLQG_CUDA(cudaMemcpy(pl->d_tiles, tiles.data(), tiles.size() * sizeof(double2), cudaMemcpyHostToDevice));
     if (!pl->omegas.empty())
         WNLQG_CUDA(cudaMemcpy(pl->d_omegas, pl->omegas.data(), pl->omegas.size() * sizeof(double), cudaMemcpyHostToDevice));
