@@ -202,6 +202,23 @@ WNLQG_API wnlqg_status wnlqg_b200_spectrum_noalloc(int64_t num_orbitals, int64_t
                                          int64_t n, double *energies, double *eigenvectors,
                                          void *stream);
 
+/* Refinement-proposer MLP (no counterpart in the reference: it ranks adaptive cells for
+ * subdivision and never supplies an integrand value).  8 input features -> 3 tanh layers of
+ * 64 -> 1 output; FP32 master parameters, BF16 weight copies in the products, FP32 accumulation;
+ * mean-squared-error loss; Adam.  Arrays are host arrays: x[n*8], targets/outputs[n],
+ * params/grad[wnlqg_b200_mlp_param_count()]. */
+typedef struct wnlqg_mlp wnlqg_mlp;
+WNLQG_API int64_t wnlqg_b200_mlp_param_count(void);
+WNLQG_API wnlqg_status wnlqg_b200_mlp_create(int32_t device, uint64_t seed, wnlqg_mlp **out_mlp);
+WNLQG_API wnlqg_status wnlqg_b200_mlp_destroy(wnlqg_mlp *mlp);
+WNLQG_API wnlqg_status wnlqg_b200_mlp_get_params(wnlqg_mlp *mlp, float *params);
+WNLQG_API wnlqg_status wnlqg_b200_mlp_set_params(wnlqg_mlp *mlp, const float *params);
+WNLQG_API wnlqg_status wnlqg_b200_mlp_forward(wnlqg_mlp *mlp, const float *x, int64_t n, float *y);
+WNLQG_API wnlqg_status wnlqg_b200_mlp_loss_grad(wnlqg_mlp *mlp, const float *x, const float *target, int64_t n,
+                                      float *loss, float *grad);
+WNLQG_API wnlqg_status wnlqg_b200_mlp_train(wnlqg_mlp *mlp, const float *x, const float *target, int64_t n,
+                                  int32_t steps, float learning_rate, float *final_loss);
+
 /* Device time in milliseconds of the last eval_mesh* call's dominant kernel and of the
  * whole call (CUDA events on the plan's stream). */
 WNLQG_API wnlqg_status wnlqg_b200_plan_last_timing(const wnlqg_plan *plan, double *fourier_ms,

@@ -138,3 +138,27 @@ def test_berry_dipole_finite_temperature_weight_integrates_to_one():
     z = np.exp(-np.abs(e / (kb * T)))
     w = z / (kb * T * (1 + z) ** 2)
     assert abs(np.trapezoid(w, e) - 1.0) < 1e-6
+
+
+def test_mlp_oracle_gradient_matches_finite_differences():
+    """Pins the oracle's backpropagation: with weights that are exact BF16 values, central
+    differences of the float64 loss equal the analytic gradient."""
+    from oracle import mlp_oracle as M
+    rng = np.random.default_rng(4)
+    p = M.bf16_round(rng.normal(0, 0.3, M.COUNT).astype(np.float32)).astype(np.float64)
+    x = rng.normal(size=(40, M.F))
+    t = rng.normal(size=40)
+
+    def loss_at(q):
+        y, _ = M.forward(q.astype(np.float32), x)   # q holds exact BF16 values for weights
+        return np.mean((y - t) ** 2)
+
+    _, g = M.loss_grad(p.astype(np.float32), x, t)
+    # Probe biases (no BF16 rounding) with central differences.
+    for name in ("b1", "b2", "b3", "b4"):
+        o, size = M.OFF[name]
+        for i in range(min(size, 5)):
+            e = np.zeros(M.COUNT)
+            e[o + i] = 1e-3
+            fd = (loss_at(p + e) - loss_at(p - e)) / 2e-3
+            assert abs(fd - g[o + i]) < 1e-4 * max(1.0, abs(fd))

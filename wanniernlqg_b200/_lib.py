@@ -21,6 +21,8 @@ EXPORTED_SYMBOLS = (
     "wnlqg_b200_eval_points_weighted", "wnlqg_b200_eval_mesh_weighted",
     "wnlqg_b200_eval_spectrum", "wnlqg_b200_plan_last_timing", "wnlqg_b200_plan_last_launch_count",
     "wnlqg_b200_spectrum_noalloc",
+    "wnlqg_b200_mlp_param_count", "wnlqg_b200_mlp_create", "wnlqg_b200_mlp_destroy", "wnlqg_b200_mlp_get_params",
+    "wnlqg_b200_mlp_set_params", "wnlqg_b200_mlp_forward", "wnlqg_b200_mlp_loss_grad", "wnlqg_b200_mlp_train",
 )
 
 _lib = None
@@ -66,6 +68,20 @@ def load():
     L.wnlqg_b200_spectrum_noalloc.argtypes = [ctypes.c_int64, ctypes.c_int64, vp, vp, vp, vp, ctypes.c_int64, vp, vp,
                                               vp]
     L.wnlqg_b200_spectrum_noalloc.restype = ctypes.c_int
+    fp = ctypes.POINTER(ctypes.c_float)
+    L.wnlqg_b200_mlp_param_count.restype = ctypes.c_int64
+    L.wnlqg_b200_mlp_param_count.argtypes = []
+    L.wnlqg_b200_mlp_create.argtypes = [ctypes.c_int32, ctypes.c_uint64, ctypes.POINTER(vp)]
+    L.wnlqg_b200_mlp_destroy.argtypes = [vp]
+    L.wnlqg_b200_mlp_get_params.argtypes = [vp, fp]
+    L.wnlqg_b200_mlp_set_params.argtypes = [vp, fp]
+    L.wnlqg_b200_mlp_forward.argtypes = [vp, fp, ctypes.c_int64, fp]
+    L.wnlqg_b200_mlp_loss_grad.argtypes = [vp, fp, fp, ctypes.c_int64, fp, fp]
+    L.wnlqg_b200_mlp_train.argtypes = [vp, fp, fp, ctypes.c_int64, ctypes.c_int32, ctypes.c_float, fp]
+    for name in ("wnlqg_b200_mlp_create", "wnlqg_b200_mlp_destroy", "wnlqg_b200_mlp_get_params",
+                 "wnlqg_b200_mlp_set_params", "wnlqg_b200_mlp_forward", "wnlqg_b200_mlp_loss_grad",
+                 "wnlqg_b200_mlp_train"):
+        getattr(L, name).restype = ctypes.c_int
     L.wnlqg_b200_plan_last_launch_count.restype = ctypes.c_int64
     L.wnlqg_b200_plan_last_launch_count.argtypes = [vp]
     for name in ("wnlqg_b200_last_error", "wnlqg_b200_model_create", "wnlqg_b200_model_destroy",

@@ -1,0 +1,241 @@
+"""Cell-adaptive k-space integration with an optional learned refinement proposer.
+
+Scheme (this engine's own; the reference's adaptive integrator is the HCubature controller in
+:mod:`wanniernlqg_b200.integration`):
+
+* The unit cell [0,1)^3 starts as N0^3 cubic cells.  Every leaf cell has a coarse value,
+  its volume times the integrand at its centre.
+* A cell is *checked* by evaluating the integrand at the centres of its 8 octants; its fine
+  value is their mean times the volume and its error estimate is ||fine - coarse|| (maximum
+  absolute complex entry, the reference's norm).  A checked cell contributes its fine value.
+* Each round splits the checked cells with the largest errors into their octants (whose coarse
+  values are the parent's octant values, so no evaluation is repeated) until the error of the
+  cells left unsplit fits the tolerance budget, up to `max_level` levels of refinement.
+* Stop when sum(errors) <= rtol * ||I||.
+
+The plain method checks every leaf.  The learned method (``MlpProposer``) predicts log10 of each
+unchecked leaf's error from cheap features (cell centre, size, parent error, the centre value
+and the distance of the centre's spectrum to the Fermi level and to the photon window) and
+checks only the leaves predicted above the threshold plus a random audit sample; if the audit
+finds a leaf whose true error exceeds its predicted error by more than ``audit_factor``, the
+round falls back to checking every leaf.  Unchecked leaves keep their coarse value (an actual
+integrand value) and count their predicted error in the total.  The network never supplies an
+integrand value; it only decides which cells are checked first.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import time
+from typing import Callable, Optional
+
+import numpy as np
+
+from . import _lib
+
+OCTANTS = np.array([[i, j, k] for k in (0, 1) for j in (0, 1) for i in (0, 1)], dtype=np.float64) - 0.5
+
+
+@dataclasses.dataclass
+class AdaptiveResult:
+    value: np.ndarray
+    error_estimate: float
+    evaluations: int
+    leaves: int
+    checked_cells: int
+    rounds: int
+    converged: bool
+    seconds: float
+    fallbacks: int = 0
+
+
+def _norm(x) -> float:
+    return float(np.max(np.abs(x))) if np.size(x) else 0.0
+
+
+class MlpProposer:
+    """Feature builder plus the GPU MLP (wnlqg_b200_mlp_*) trained online on checked cells."""
+
+    def __init__(self, fermi_energy: float, omegas, spectrum_fn: Callable, *, device: int = 0, seed: int = 1,
+                 train_steps: int = 200, learning_rate: float = 3e-3):
+        self.L = _lib.load()
+        self.m = ctypes.c_void_p()
+        _lib.check(self.L.wnlqg_b200_mlp_create(device, seed, ctypes.byref(self.m)))
+        self.mu = float(fermi_energy)
+        om = np.asarray(omegas, dtype=np.float64)
+        self.om_lo, self.om_hi = (float(om.min()), float(om.max())) if om.size else (0.0, 0.0)
+        self.spectrum_fn = spectrum_fn
+        self.train_steps = train_steps
+        self.lr = learning_rate
+        self.X = []
+        self.Y = []
+        self.spectrum_evaluations = 0
+
+    def close(self):
+        if self.m:
+            self.L.wnlqg_b200_mlp_destroy(self.m)
+            self.m = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def features(self, centers, sizes, parent_err, coarse_norm) -> np.ndarray:
+        e, _ = self.spectrum_fn(centers)
+        self.spectrum_evaluations += centers.shape[0]
+        dmu = np.min(np.abs(e - self.mu), axis=1)
+        occ = e <= self.mu
+        # Smallest distance of an occupied -> empty transition energy to the photon window.
+        emax_occ = np.where(occ, e, -np.inf).max(axis=1)
+        emin_emp = np.where(~occ, e, np.inf).min(axis=1)
+        gap = emin_emp - emax_occ
+        dwin = np.where(gap < self.om_lo, self.om_lo - gap, np.where(gap > self.om_hi, gap - self.om_hi, 0.0))
+        f = np.stack([
+            np.sin(2 * np.pi * centers[:, 0]), np.sin(2 * np.pi * centers[:, 1]), np.sin(2 * np.pi * centers[:, 2]),
+            np.log2(sizes) / 8.0,
+            np.log10(np.maximum(parent_err, 1e-30)) / 10.0,
+            np.log10(np.maximum(coarse_norm, 1e-30)) / 10.0,
+            np.log10(np.maximum(dmu, 1e-6)),
+            np.log10(np.maximum(dwin, 1e-6)),
+        ], axis=1)
+        return np.ascontiguousarray(f, dtype=np.float32)
+
+    def observe(self, feats: np.ndarray, errors: np.ndarray):
+        self.X.append(feats)
+        self.Y.append(np.log10(np.maximum(errors, 1e-30)).astype(np.float32) / 10.0)
+
+    def train(self):
+        X = np.ascontiguousarray(np.concatenate(self.X), dtype=np.float32)
+        Y = np.ascontiguousarray(np.concatenate(self.Y), dtype=np.float32)
+        loss = ctypes.c_float()
+        fp = ctypes.POINTER(ctypes.c_float)
+        _lib.check(self.L.wnlqg_b200_mlp_train(self.m, X.ctypes.data_as(fp), Y.ctypes.data_as(fp), X.shape[0],
+                                               self.train_steps, self.lr, ctypes.byref(loss)))
+        return loss.value
+
+    def predict(self, feats: np.ndarray) -> np.ndarray:
+        y = np.zeros(feats.shape[0], dtype=np.float32)
+        fp = ctypes.POINTER(ctypes.c_float)
+        _lib.check(self.L.wnlqg_b200_mlp_forward(self.m, feats.ctypes.data_as(fp), feats.shape[0],
+                                                 y.ctypes.data_as(fp)))
+        return 10.0 ** (10.0 * y.astype(np.float64))
+
+
+def integrate_cells(point_values: Callable, *, n0: int = 16, rtol: float = 1e-4, max_level: int = 8,
+                    max_evaluations: int = 50_000_000, proposer: Optional[MlpProposer] = None,
+                    warmup_fraction: float = 0.15, audit_fraction: float = 0.05, audit_factor: float = 10.0,
+                    safety: float = 4.0, seed: int = 0, component=None) -> AdaptiveResult:
+    """Integrate the domain average of point_values(k[n,3]) -> [n, V] over [0,1)^3.
+
+    `component` (index array) restricts the error norm to those value entries (for example the
+    sigma^xyy(omega) block); the integral covers all entries."""
+    t0 = time.perf_counter()
+    rng = np.random.default_rng(seed)
+    g = (np.arange(n0) + 0.5) / n0
+    cz, cy, cx = np.meshgrid(g, g, g, indexing="ij")
+    centers = np.stack([cx.ravel(), cy.ravel(), cz.ravel()], axis=1)
+    half = np.full(centers.shape[0], 0.5 / n0)
+    level = np.zeros(centers.shape[0], dtype=np.int64)
+    vol = (2 * half) ** 3
+    coarse = point_values(centers) * vol[:, None]
+    evaluations = centers.shape[0]
+    sel = slice(None) if component is None else component
+    nv = coarse.shape[1]
+    fine = np.zeros_like(coarse)
+    octv = np.zeros((centers.shape[0], 8, nv), dtype=coarse.dtype)
+    err = np.full(centers.shape[0], np.nan)
+    pred = np.full(centers.shape[0], np.nan)
+    checked = np.zeros(centers.shape[0], dtype=bool)
+    parent_err = np.full(centers.shape[0], 1e-30)
+    rounds = 0
+    fallbacks = 0
+    checked_total = 0
+
+    def check(idx):
+        nonlocal evaluations
+        if idx.size == 0:
+            return
+        pts = (centers[idx, None, :] + OCTANTS[None, :, :] * half[idx, None, None]).reshape(-1, 3)
+        vals = point_values(pts % 1.0).reshape(idx.size, 8, nv)
+        evaluations += pts.shape[0]
+        octv[idx] = vals
+        fine[idx] = vals.mean(axis=1) * vol[idx, None]
+        err[idx] = np.max(np.abs((fine[idx] - coarse[idx])[:, sel]), axis=1)
+        checked[idx] = True
+
+    while True:
+        rounds += 1
+        todo = np.where(~checked)[0]
+        if proposer is None or todo.size == 0:
+            check(todo)
+            checked_total += todo.size
+        else:
+            feats = proposer.features(centers[todo], 2 * half[todo], parent_err[todo],
+                                      np.max(np.abs(coarse[todo][:, sel]), axis=1) / vol[todo])
+            if not proposer.X:
+                first = rng.random(todo.size) < warmup_fraction
+                check(todo[first])
+                checked_total += int(first.sum())
+                proposer.observe(feats[first], err[todo[first]])
+                proposer.train()
+            p = proposer.predict(feats)
+            pred[todo] = p * vol[todo] / vol[todo].max()
+            value_now = np.where(checked[:, None], fine, coarse).sum(axis=0)
+            budget = rtol * _norm(value_now[sel]) / safety
+            rest = todo[~checked[todo]]
+            order = np.argsort(-pred[rest], kind="stable")
+            csum = np.cumsum(pred[rest][order][::-1])[::-1]
+            must = order[csum > budget * 0.5]
+            audit = rng.random(rest.size) < audit_fraction
+            pick = np.zeros(rest.size, dtype=bool)
+            pick[must] = True
+            pick |= audit
+            chosen = rest[pick]
+            check(chosen)
+            checked_total += chosen.size
+            proposer.observe(proposer.features(centers[chosen], 2 * half[chosen], parent_err[chosen],
+                                               np.max(np.abs(coarse[chosen][:, sel]), axis=1) / vol[chosen]),
+                             err[chosen])
+            aud = rest[audit & ~np.isin(np.arange(rest.size), must)]
+            if aud.size and np.any(err[aud] > audit_factor * np.maximum(pred[aud], 1e-300)):
+                fallbacks += 1
+                left = np.where(~checked)[0]
+                check(left)
+                checked_total += left.size
+            proposer.train()
+        value = np.where(checked[:, None], fine, coarse).sum(axis=0)
+        est = np.where(checked, err, np.nan_to_num(pred, nan=0.0))
+        total_err = float(est.sum())
+        inorm = _norm(value[sel])
+        if total_err <= rtol * inorm:
+            return AdaptiveResult(value, total_err, evaluations, centers.shape[0], checked_total, rounds, True,
+                                  time.perf_counter() - t0, fallbacks)
+        splittable = np.where(checked & (level < max_level))[0]
+        if splittable.size == 0 or evaluations >= max_evaluations:
+            return AdaptiveResult(value, total_err, evaluations, centers.shape[0], checked_total, rounds, False,
+                                  time.perf_counter() - t0, fallbacks)
+        order = splittable[np.argsort(-est[splittable], kind="stable")]
+        keep_err = total_err - np.cumsum(est[order])
+        nsplit = int(np.searchsorted(-keep_err, -0.5 * rtol * inorm)) + 1
+        split = order[:min(nsplit, order.size)]
+        # Children: octant centres of each split cell, coarse values from the parent's octants.
+        ch_c = (centers[split, None, :] + OCTANTS[None, :, :] * half[split, None, None]).reshape(-1, 3)
+        ch_h = np.repeat(half[split] / 2, 8)
+        ch_l = np.repeat(level[split] + 1, 8)
+        ch_v = octv[split].reshape(-1, nv) * ((2 * ch_h) ** 3)[:, None]
+        ch_pe = np.repeat(err[split] / 8.0, 8)
+        keep = np.ones(centers.shape[0], dtype=bool)
+        keep[split] = False
+        centers = np.concatenate([centers[keep], ch_c])
+        half = np.concatenate([half[keep], ch_h])
+        level = np.concatenate([level[keep], ch_l])
+        vol = (2 * half) ** 3
+        coarse = np.concatenate([coarse[keep], ch_v])
+        fine = np.concatenate([fine[keep], np.zeros_like(ch_v)])
+        octv = np.concatenate([octv[keep], np.zeros((ch_c.shape[0], 8, nv), dtype=coarse.dtype)])
+        err = np.concatenate([err[keep], np.full(ch_c.shape[0], np.nan)])
+        pred = np.concatenate([pred[keep], np.full(ch_c.shape[0], np.nan)])
+        checked = np.concatenate([checked[keep], np.zeros(ch_c.shape[0], dtype=bool)])
+        parent_err = np.concatenate([parent_err[keep], ch_pe])

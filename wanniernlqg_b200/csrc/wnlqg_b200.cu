@@ -1099,3 +1099,191 @@ extern "C" wnlqg_status wnlqg_b200_spectrum_noalloc(int64_t num_orbitals, int64_
     WNLQG_CUDA(cudaGetLastError());
     return WNLQG_OK;
 }
+
+// ---------------------------------------------------------------------------------------------
+// Refinement-proposer MLP (no counterpart in the reference; it only ranks cells for refinement).
+// ---------------------------------------------------------------------------------------------
+#include "mlp.cuh"
+
+struct wnlqg_mlp {
+    int device = 0;
+    float *d_master = nullptr, *d_m = nullptr, *d_v = nullptr, *d_grad = nullptr, *d_partial = nullptr;
+    __nv_bfloat16 *d_wb = nullptr;
+    float *d_x = nullptr, *d_y = nullptr, *d_out = nullptr;
+    int64_t cap = 0;
+    int slots = 0;
+    int64_t step = 0;
+    cudaStream_t stream = nullptr;
+};
+
+namespace {
+wnlqg_status mlp_reserve(wnlqg_mlp *m, int64_t n) {
+    if (n <= m->cap) return WNLQG_OK;
+    cudaFree(m->d_x);
+    cudaFree(m->d_y);
+    cudaFree(m->d_out);
+    m->d_x = m->d_y = m->d_out = nullptr;
+    m->cap = 0;
+    WNLQG_CUDA(cudaMalloc(&m->d_x, (size_t)n * MLP_F * sizeof(float)));
+    WNLQG_CUDA(cudaMalloc(&m->d_y, (size_t)n * sizeof(float)));
+    WNLQG_CUDA(cudaMalloc(&m->d_out, (size_t)n * sizeof(float)));
+    m->cap = n;
+    return WNLQG_OK;
+}
+
+int mlp_grid(int64_t n, int maxslots) {
+    return (int)std::max<int64_t>(1, std::min<int64_t>((n + MLP_TILE - 1) / MLP_TILE, maxslots));
+}
+
+wnlqg_status mlp_loss_grad_device(wnlqg_mlp *m, int64_t n) {
+    const int grid = mlp_grid(n, m->slots);
+    mlp_backward_kernel<<<grid, MLP_H, 0, m->stream>>>(m->d_wb, m->d_master, m->d_x, m->d_y, n, m->d_partial);
+    mlp_reduce_kernel<<<(MlpLayout::COUNT + 256) / 256, 256, 0, m->stream>>>(m->d_partial, grid, m->d_grad);
+    WNLQG_CUDA(cudaGetLastError());
+    return WNLQG_OK;
+}
+}  // namespace
+
+extern "C" int64_t wnlqg_b200_mlp_param_count(void) { return MlpLayout::COUNT; }
+
+extern "C" wnlqg_status wnlqg_b200_mlp_create(int32_t device, uint64_t seed, wnlqg_mlp **out) {
+    if (!out) return fail(WNLQG_ERR_INVALID_ARGUMENT, "NULL argument");
+    *out = nullptr;
+    WNLQG_CUDA(cudaSetDevice(device));
+    wnlqg_mlp *m = new wnlqg_mlp();
+    m->device = device;
+    m->slots = 148 * 4;
+    // Glorot-uniform weights from a seeded 64-bit LCG, zero biases.
+    std::vector<float> p(MlpLayout::COUNT, 0.0f);
+    uint64_t state = seed * 6364136223846793005ULL + 1442695040888963407ULL;
+    auto uni = [&]() {
+        state = state * 6364136223846793005ULL + 1442695040888963407ULL;
+        return (double)(state >> 11) * (1.0 / 9007199254740992.0);
+    };
+    auto fill = [&](int off, int fan_out, int fan_in) {
+        const double lim = std::sqrt(6.0 / (fan_in + fan_out));
+        for (int i = 0; i < fan_out * fan_in; ++i) p[off + i] = (float)((2.0 * uni() - 1.0) * lim);
+    };
+    fill(MlpLayout::W1, MLP_H, MLP_F);
+    fill(MlpLayout::W2, MLP_H, MLP_H);
+    fill(MlpLayout::W3, MLP_H, MLP_H);
+    fill(MlpLayout::W4, 1, MLP_H);
+    auto cleanup = [&]() {
+        cudaFree(m->d_master); cudaFree(m->d_m); cudaFree(m->d_v); cudaFree(m->d_grad);
+        cudaFree(m->d_partial); cudaFree(m->d_wb);
+        delete m;
+    };
+    const size_t pb = (size_t)MlpLayout::COUNT * sizeof(float);
+    if (cudaMalloc(&m->d_master, pb) != cudaSuccess || cudaMalloc(&m->d_m, pb) != cudaSuccess ||
+        cudaMalloc(&m->d_v, pb) != cudaSuccess || cudaMalloc(&m->d_grad, pb + sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&m->d_partial, (size_t)m->slots * (MlpLayout::COUNT + 1) * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&m->d_wb, (size_t)MlpLayout::COUNT * sizeof(__nv_bfloat16)) != cudaSuccess) {
+        cudaGetLastError();
+        cleanup();
+        return fail(WNLQG_ERR_OUT_OF_MEMORY, "cudaMalloc failed for the MLP");
+    }
+    if (cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cleanup();
+        return fail(WNLQG_ERR_CUDA, "cudaStreamCreate failed");
+    }
+    WNLQG_CUDA(cudaMemcpy(m->d_master, p.data(), pb, cudaMemcpyHostToDevice));
+    WNLQG_CUDA(cudaMemset(m->d_m, 0, pb));
+    WNLQG_CUDA(cudaMemset(m->d_v, 0, pb));
+    mlp_to_bf16_kernel<<<(MlpLayout::COUNT + 255) / 256, 256, 0, m->stream>>>(m->d_master, m->d_wb, MlpLayout::COUNT);
+    WNLQG_CUDA(cudaStreamSynchronize(m->stream));
+    *out = m;
+    return WNLQG_OK;
+}
+
+extern "C" wnlqg_status wnlqg_b200_mlp_destroy(wnlqg_mlp *m) {
+    if (!m) return WNLQG_OK;
+    cudaSetDevice(m->device);
+    if (m->stream) cudaStreamSynchronize(m->stream);
+    for (void *ptr : {(void *)m->d_master, (void *)m->d_m, (void *)m->d_v, (void *)m->d_grad, (void *)m->d_partial,
+                      (void *)m->d_wb, (void *)m->d_x, (void *)m->d_y, (void *)m->d_out})
+        if (ptr) cudaFree(ptr);
+    if (m->stream) cudaStreamDestroy(m->stream);
+    delete m;
+    return WNLQG_OK;
+}
+
+extern "C" wnlqg_status wnlqg_b200_mlp_get_params(wnlqg_mlp *m, float *params) {
+    if (!m || !params) return fail(WNLQG_ERR_INVALID_ARGUMENT, "NULL argument");
+    WNLQG_CUDA(cudaSetDevice(m->device));
+    WNLQG_CUDA(cudaMemcpyAsync(params, m->d_master, (size_t)MlpLayout::COUNT * sizeof(float), cudaMemcpyDeviceToHost,
+                               m->stream));
+    WNLQG_CUDA(cudaStreamSynchronize(m->stream));
+    return WNLQG_OK;
+}
+
+extern "C" wnlqg_status wnlqg_b200_mlp_set_params(wnlqg_mlp *m, const float *params) {
+    if (!m || !params) return fail(WNLQG_ERR_INVALID_ARGUMENT, "NULL argument");
+    for (int i = 0; i < MlpLayout::COUNT; ++i)
+        if (!std::isfinite(params[i])) return fail(WNLQG_ERR_NONFINITE, "parameters must be finite");
+    WNLQG_CUDA(cudaSetDevice(m->device));
+    WNLQG_CUDA(cudaMemcpyAsync(m->d_master, params, (size_t)MlpLayout::COUNT * sizeof(float), cudaMemcpyHostToDevice,
+                               m->stream));
+    mlp_to_bf16_kernel<<<(MlpLayout::COUNT + 255) / 256, 256, 0, m->stream>>>(m->d_master, m->d_wb, MlpLayout::COUNT);
+    WNLQG_CUDA(cudaStreamSynchronize(m->stream));
+    return WNLQG_OK;
+}
+
+extern "C" wnlqg_status wnlqg_b200_mlp_forward(wnlqg_mlp *m, const float *x, int64_t n, float *y) {
+    if (!m || n < 0 || (n > 0 && (!x || !y))) return fail(WNLQG_ERR_INVALID_ARGUMENT, "invalid arguments");
+    if (n == 0) return WNLQG_OK;
+    WNLQG_CUDA(cudaSetDevice(m->device));
+    wnlqg_status st = mlp_reserve(m, n);
+    if (st != WNLQG_OK) return st;
+    WNLQG_CUDA(cudaMemcpyAsync(m->d_x, x, (size_t)n * MLP_F * sizeof(float), cudaMemcpyHostToDevice, m->stream));
+    mlp_forward_kernel<<<mlp_grid(n, 148 * 8), MLP_H, 0, m->stream>>>(m->d_wb, m->d_master, m->d_x, n, m->d_out);
+    WNLQG_CUDA(cudaGetLastError());
+    WNLQG_CUDA(cudaMemcpyAsync(y, m->d_out, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, m->stream));
+    WNLQG_CUDA(cudaStreamSynchronize(m->stream));
+    return WNLQG_OK;
+}
+
+extern "C" wnlqg_status wnlqg_b200_mlp_loss_grad(wnlqg_mlp *m, const float *x, const float *target, int64_t n,
+                                                 float *loss, float *grad) {
+    if (!m || n <= 0 || !x || !target) return fail(WNLQG_ERR_INVALID_ARGUMENT, "invalid arguments");
+    WNLQG_CUDA(cudaSetDevice(m->device));
+    wnlqg_status st = mlp_reserve(m, n);
+    if (st != WNLQG_OK) return st;
+    WNLQG_CUDA(cudaMemcpyAsync(m->d_x, x, (size_t)n * MLP_F * sizeof(float), cudaMemcpyHostToDevice, m->stream));
+    WNLQG_CUDA(cudaMemcpyAsync(m->d_y, target, (size_t)n * sizeof(float), cudaMemcpyHostToDevice, m->stream));
+    if ((st = mlp_loss_grad_device(m, n)) != WNLQG_OK) return st;
+    std::vector<float> g(MlpLayout::COUNT + 1);
+    WNLQG_CUDA(cudaMemcpyAsync(g.data(), m->d_grad, g.size() * sizeof(float), cudaMemcpyDeviceToHost, m->stream));
+    WNLQG_CUDA(cudaStreamSynchronize(m->stream));
+    if (loss) *loss = g[MlpLayout::COUNT];
+    if (grad) std::memcpy(grad, g.data(), (size_t)MlpLayout::COUNT * sizeof(float));
+    return WNLQG_OK;
+}
+
+extern "C" wnlqg_status wnlqg_b200_mlp_train(wnlqg_mlp *m, const float *x, const float *target, int64_t n,
+                                             int32_t steps, float lr, float *final_loss) {
+    if (!m || n <= 0 || !x || !target || steps < 0 || !(lr > 0))
+        return fail(WNLQG_ERR_INVALID_ARGUMENT, "invalid arguments");
+    WNLQG_CUDA(cudaSetDevice(m->device));
+    wnlqg_status st = mlp_reserve(m, n);
+    if (st != WNLQG_OK) return st;
+    WNLQG_CUDA(cudaMemcpyAsync(m->d_x, x, (size_t)n * MLP_F * sizeof(float), cudaMemcpyHostToDevice, m->stream));
+    WNLQG_CUDA(cudaMemcpyAsync(m->d_y, target, (size_t)n * sizeof(float), cudaMemcpyHostToDevice, m->stream));
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    for (int s = 0; s < steps; ++s) {
+        if ((st = mlp_loss_grad_device(m, n)) != WNLQG_OK) return st;
+        m->step += 1;
+        const float bc1 = 1.0f - std::pow(b1, (float)m->step), bc2 = 1.0f - std::pow(b2, (float)m->step);
+        mlp_adam_kernel<<<(MlpLayout::COUNT + 255) / 256, 256, 0, m->stream>>>(m->d_master, m->d_grad, m->d_m, m->d_v,
+                                                                               m->d_wb, lr, b1, b2, eps, bc1, bc2);
+    }
+    WNLQG_CUDA(cudaGetLastError());
+    if (final_loss) {
+        if ((st = mlp_loss_grad_device(m, n)) != WNLQG_OK) return st;
+        float l = 0.f;
+        WNLQG_CUDA(cudaMemcpyAsync(&l, m->d_grad + MlpLayout::COUNT, sizeof(float), cudaMemcpyDeviceToHost, m->stream));
+        WNLQG_CUDA(cudaStreamSynchronize(m->stream));
+        *final_loss = l;
+    }
+    WNLQG_CUDA(cudaStreamSynchronize(m->stream));
+    return WNLQG_OK;
+}
