@@ -10,15 +10,17 @@ Scheme (this engine's own; the reference's adaptive integrator is the HCubature 
   absolute complex entry, the reference's norm).  A checked cell contributes its fine value.
 * Each round splits the checked cells with the largest errors into their octants (whose coarse
   values are the parent's octant values, so no evaluation is repeated) until the error of the
-  cells left unsplit fits the tolerance budget, up to `max_level` levels of refinement.
+  cells left unsplit fits the tolerance budget, up to `max_level` levels of refinement.  The
+  octant rule is second order, so the fine value's error is estimated as |fine - coarse| / 3.
 * Stop when sum(errors) <= rtol * ||I||.
 
 The plain method checks every leaf.  The learned method (``MlpProposer``) predicts log10 of each
 unchecked leaf's error from cheap features (cell centre, size, parent error, the centre value
 and the distance of the centre's spectrum to the Fermi level and to the photon window) and
 checks only the leaves predicted above the threshold plus a random audit sample; if the audit
-finds a leaf whose true error exceeds its predicted error by more than ``audit_factor``, the
-round falls back to checking every leaf.  Unchecked leaves keep their coarse value (an actual
+finds a leaf whose true error exceeds its prediction by more than ``audit_factor``, every
+prediction is scaled up by the worst audited ratio and the leaves the rescaled budget requires
+are checked (every leaf, when the ratio exceeds audit_factor^3).  Unchecked leaves keep their coarse value (an actual
 integrand value) and count their predicted error in the total.  The network never supplies an
 integrand value; it only decides which cells are checked first.
 """
@@ -162,7 +164,8 @@ def integrate_cells(point_values: Callable, *, n0: int = 16, rtol: float = 1e-4,
         evaluations += pts.shape[0]
         octv[idx] = vals
         fine[idx] = vals.mean(axis=1) * vol[idx, None]
-        err[idx] = np.max(np.abs((fine[idx] - coarse[idx])[:, sel]), axis=1)
+        # Midpoint rules converge as h^2: the fine value's error is |fine - coarse| / 3.
+        err[idx] = np.max(np.abs((fine[idx] - coarse[idx])[:, sel]), axis=1) / 3.0
         checked[idx] = True
 
     while True:
@@ -199,11 +202,25 @@ def integrate_cells(point_values: Callable, *, n0: int = 16, rtol: float = 1e-4,
                                                np.max(np.abs(coarse[chosen][:, sel]), axis=1) / vol[chosen]),
                              err[chosen])
             aud = rest[audit & ~np.isin(np.arange(rest.size), must)]
-            if aud.size and np.any(err[aud] > audit_factor * np.maximum(pred[aud], 1e-300)):
-                fallbacks += 1
-                left = np.where(~checked)[0]
-                check(left)
-                checked_total += left.size
+            if aud.size:
+                ratio = float(np.max(err[aud] / np.maximum(pred[aud], 1e-300)))
+                if ratio > audit_factor:
+                    # The audit found under-predicted errors: recalibrate every prediction by the
+                    # worst audited ratio and check what the recalibrated budget requires; fall back
+                    # to checking every leaf if the network is off by more than audit_factor^3.
+                    fallbacks += 1
+                    left = np.where(~checked)[0]
+                    if ratio > audit_factor ** 3:
+                        check(left)
+                        checked_total += left.size
+                    else:
+                        pl = pred[left] * ratio
+                        pred[left] = pl
+                        order2 = np.argsort(-pl, kind="stable")
+                        csum2 = np.cumsum(pl[order2][::-1])[::-1]
+                        extra = left[order2[csum2 > budget * 0.5]]
+                        check(extra)
+                        checked_total += extra.size
             proposer.train()
         value = np.where(checked[:, None], fine, coarse).sum(axis=0)
         est = np.where(checked, err, np.nan_to_num(pred, nan=0.0))
