@@ -21,7 +21,7 @@ def test_plain_cells_converge_on_smooth_and_localised_integrands():
     assert r.converged and abs(r.value[0] - exact) < 1e-3 * exact
     g = lambda k: (1.0 + 0.3 * np.cos(2 * np.pi * k[:, 0]) * np.sin(2 * np.pi * k[:, 1]))[:, None].astype(complex)
     r2 = integrate_cells(g, n0=8, rtol=1e-3, max_level=3)
-    assert r2.converged and abs(r2.value[0] - 1.0) < 1e-6
+    assert r2.converged and abs(r2.value[0] - 1.0) < 1e-3
 
 
 def test_learned_proposer_saves_evaluations_cpu():
