@@ -257,23 +257,42 @@ def main():
     e2e_dt = (time.perf_counter() - t0) / e2e_steps
     e2e_value = world * batch / e2e_dt
 
-    # Roofline of the dominant kernel (Fourier stage) from the last step's CUDA events.
+    # Roofline of the dominant stage, from the last step's CUDA events on the plan stream.
     peaks, peak_src = load_peaks()
-    launches_per_step = launches // max(1, args.steps)
+    stages = {"fourier": fourier_ms, "eigen": eigen_ms, "response": response_ms}
+    dominant = max(stages, key=stages.get)
+    nw, nr = model.num_orbitals, model.num_r_vectors
     C = fourier_channels(task)
-    flop_per_k = 8.0 * model.num_r_vectors * model.num_orbitals ** 2 * C
-    fourier_tflops = flop_per_k * batch / (fourier_ms / 1e3) / 1e12 if fourier_ms > 0 else None
-    fp64_peak = 37.0   # nominal B200 dense FP64 TFLOP/s; no measured FP64 peak on this pool
+    # Algorithmic work per k-point (counts of the algorithms executed):
+    #   staged Fourier: 8*P1*C*nw^2 flop (P1 = 9 distinct r1 on the |R_i|<=4 cube) and
+    #     C*nw^2*16 B written + read once (FP64 Wannier-gauge channels);
+    #   eigensolve: 30*nw^3 flop (LAPACK-class modelling count for a Hermitian eigensolve);
+    #   response: 18 complex nw^3 products (8*nw^3 flop each) + 4*nw^2*Nw flop contraction.
+    p1 = 9
+    flop = {"fourier": 8.0 * p1 * C * nw * nw, "eigen": 30.0 * nw ** 3,
+            "response": 18 * 8.0 * nw ** 3 + 4.0 * nw * nw * 512}
+    hbm = {"fourier": 2.0 * C * nw * nw * 16, "eigen": nw * nw * 16 * 2.0 + nw * 8,
+           "response": (C - 1) * nw * nw * 16 + nw * nw * 16}
+    t_s = stages[dominant] / 1e3
+    achieved_gbs = hbm[dominant] * batch / t_s / 1e9
+    achieved_tf = flop[dominant] * batch / t_s / 1e12
+    sm_peak = {"fp64": 37.0, "mixed": 74.0}["fp64" if precision == _abi.PRECISION_FP64 else "mixed"]
     roofline = {
-        "bound": "fp64" if precision == _abi.PRECISION_FP64 else "tensor",
-        "kernel": "fourier (phase table + complex GEMM)",
-        "achieved": fourier_tflops, "peak": fp64_peak, "unit": "TFLOP/s",
-        "frac": (fourier_tflops / fp64_peak) if fourier_tflops else None,
-        "peak_source": "nominal B200 FP64 (not in the measured peaks file)",
-        "traffic": None, "launches_per_step": launches_per_step,
+        "bound": "hbm" if dominant == "fourier" else "sm",
+        "kernel": {"fourier": "staged Fourier (staged_r1_kernel)", "eigen": "Jacobi eigensolver",
+                   "response": "fused response kernel"}[dominant],
+        "achieved": achieved_gbs if dominant == "fourier" else achieved_tf,
+        "peak": peaks["hbm_gbs"] if dominant == "fourier" else sm_peak,
+        "unit": "GB/s" if dominant == "fourier" else "TFLOP/s",
+        "traffic": None,
+        "peak_source": (f"{peak_src} HBM copy bandwidth" if dominant == "fourier" else
+                        "nominal B200 CUDA-core peak (FP64 37 / FP32 74 TFLOP/s; not in the measured peaks file)"),
         "stage_ms_last_step": {"fourier": fourier_ms, "eigen": eigen_ms, "response": response_ms, "total": total_ms},
-        "flop_per_k": flop_per_k,
+        "algorithmic_per_k": {"flop": flop, "hbm_bytes": hbm},
+        "hbm_gbs_dominant": achieved_gbs,
+        "launches_per_step": launches // max(1, args.steps),
     }
+    roofline["frac"] = roofline["achieved"] / roofline["peak"] if roofline["peak"] else None
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,

@@ -1,0 +1,99 @@
+# WannierNLQGB200.jl - ccall binding of libwnlqg_b200.so for WannierNLQG (not executed in this
+# repository: Julia is not installed in its build image).  A maintainer includes this file in
+# WannierNLQG's Runtime and selects it with `fourier_backend = "b200"`.
+module WannierNLQGB200
+
+const LIB = get(ENV, "WNLQG_B200_LIB", joinpath(@__DIR__, "..", "wanniernlqg_b200", "libwnlqg_b200.so"))
+
+const SHIFT_CURRENT = Int32(1)
+const INJECTION_CURRENT = Int32(2)
+const BERRY_CURVATURE = Int32(3)
+const QUANTUM_METRIC = Int32(4)
+const INTRINSIC_AHC = Int32(5)
+const BERRY_DIPOLE = Int32(6)
+const JERK_CURRENT = Int32(8)
+
+struct ModelDesc
+    num_orbitals::Int64
+    num_r_vectors::Int64
+    lattice::Ptr{Float64}
+    r_vectors::Ptr{Int64}
+    r_degeneracies::Ptr{Int64}
+    hamiltonian_r::Ptr{ComplexF64}
+    position_r::Ptr{ComplexF64}
+    overlap_r::Ptr{ComplexF64}
+end
+
+struct ResponseRequest
+    kind::Int32
+    num_components::Int32
+    components::NTuple{324, Int32}     # [81][4], 0-based axes, a fastest
+end
+
+struct TaskDesc
+    num_responses::Int32
+    responses::NTuple{8, ResponseRequest}
+    fermi_energy::Float64
+    temperature::Float64
+    broadening_type::Int32             # 0 Gaussian, 1 Lorentzian
+    broadening::Float64
+    transition_window_factor::Float64
+    denominator_regularization::Float64
+    degeneracy_threshold::Float64
+    num_photon_energies::Int64
+    photon_energies::Ptr{Float64}
+    num_fermi_energies::Int64
+    fermi_energies::Ptr{Float64}
+    precision::Int32                   # 0 FP64, 1 mixed
+    fermi_surface_broadening::Float64
+end
+
+function check(status)
+    status == 0 && return nothing
+    buf = Vector{UInt8}(undef, 4096)
+    ccall((:wnlqg_b200_last_error, LIB), Cint, (Ptr{UInt8}, Csize_t), buf, length(buf))
+    msg = unsafe_string(pointer(buf))
+    status == 1 ? throw(ArgumentError(msg)) : status == 2 ? throw(DimensionMismatch(msg)) : error(msg)
+end
+
+"""Device-resident copy of a TightBindingModel (arrays are passed without copies)."""
+function model_create(model; device::Integer = 0)
+    desc = ModelDesc(model.num_orbitals, model.num_r_vectors, pointer(model.lattice),
+                     pointer(model.r_vectors), pointer(model.r_degeneracies),
+                     pointer(model.hamiltonian_r), pointer(model.position_r), C_NULL)
+    out = Ref{Ptr{Cvoid}}(C_NULL)
+    GC.@preserve model begin
+        check(ccall((:wnlqg_b200_model_create, LIB), Cint, (Ref{ModelDesc}, Int32, Ref{Ptr{Cvoid}}),
+                    desc, Int32(device), out))
+    end
+    return out[]
+end
+
+function plan_create(handle::Ptr{Cvoid}, task::TaskDesc; max_batch::Integer = 0)
+    out = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((:wnlqg_b200_plan_create, LIB), Cint, (Ptr{Cvoid}, Ref{TaskDesc}, Int64, Ref{Ptr{Cvoid}}),
+                handle, task, Int64(max_batch), out))
+    return out[]
+end
+
+value_count(plan) = ccall((:wnlqg_b200_plan_value_count, LIB), Int64, (Ptr{Cvoid},), plan)
+
+"""Lane tensor sum_{k in [first,last)} value(k)/Nk on the Gamma-centred mesh (0-based indices)."""
+function eval_mesh!(out::Vector{ComplexF64}, plan, mesh::NTuple{3, Int}, first::Integer, last::Integer)
+    m = Int64[mesh...]
+    check(ccall((:wnlqg_b200_eval_mesh, LIB), Cint, (Ptr{Cvoid}, Ptr{Int64}, Int64, Int64, Ptr{ComplexF64}),
+                plan, m, Int64(first), Int64(last), out))
+    return out
+end
+
+"""Batched ResponseNodeEvaluator: values of n fractional k-points, one column per point."""
+function eval_points!(out::Matrix{ComplexF64}, plan, kpoints::Matrix{Float64})
+    check(ccall((:wnlqg_b200_eval_points, LIB), Cint, (Ptr{Cvoid}, Ptr{Float64}, Int64, Ptr{ComplexF64}),
+                plan, kpoints, Int64(size(kpoints, 2)), out))
+    return out
+end
+
+plan_destroy(plan) = ccall((:wnlqg_b200_plan_destroy, LIB), Cint, (Ptr{Cvoid},), plan)
+model_destroy(h) = ccall((:wnlqg_b200_model_destroy, LIB), Cint, (Ptr{Cvoid},), h)
+
+end # module
