@@ -51,7 +51,7 @@ def test_gpu_trained_proposer_saves_evaluations_on_a_localised_integrand():
     f, exact = _bump()
     spec = lambda k: (np.zeros((k.shape[0], 2)) + np.array([-1.0, 1.0]), None)
     plain = integrate_cells(f, n0=16, rtol=1e-2, max_level=6)
-    prop = MlpProposer(0.0, [1.0], spec, seed=2, train_steps=150)
+    prop = MlpProposer(0.0, [1.0], spec, seed=2, train_steps=300)
     try:
         learned = integrate_cells(f, n0=16, rtol=1e-2, max_level=6, proposer=prop)
     finally:
@@ -59,4 +59,4 @@ def test_gpu_trained_proposer_saves_evaluations_on_a_localised_integrand():
     assert plain.converged and learned.converged
     assert abs(plain.value[0] - exact) < 1e-2 * exact
     assert abs(learned.value[0] - exact) < 1e-2 * exact
-    assert learned.evaluations < 0.7 * plain.evaluations
+    assert learned.evaluations < 0.7 * plain.evaluations, (learned, plain)

@@ -256,6 +256,41 @@ WNLQG_D bool any_within(double te, double half, const RespParams &p) {
 
 #define RS_OMB 4   // photon energies per thread per pass of the pair loop
 
+// Frequency contraction of one thread's RS_OMB photon energies over the pair list.
+// KIND 0: Gaussian with the sqrt(200) cutoff (transition screen); 1: Lorentzian; 2: jerk's
+// windowed delta (Gaussian or Lorentzian by `gaussian`).
+template <typename R, typename C, int KIND>
+WNLQG_D void contract_pairs(const double *ste, const double *sfnm, const C *Q0, const C *Q1, int npairs,
+                            const double *om, C (*acc)[2], R gsc, R cut, R invw, R w2, R lor, R win, int gaussian) {
+    for (int q = 0; q < npairs; ++q) {
+        const double te = ste[q];
+        const R fq = (R)sfnm[q];
+        const C q0 = Q0[q], q1 = Q1[q];
+#pragma unroll
+        for (int j = 0; j < RS_OMB; ++j) {
+            const R x = (R)(te - om[j]);
+            R delta;
+            if (KIND == 0) {
+                if (!(fabs(x) < cut)) continue;
+                const R y = x * invw;
+                delta = gsc * exp(-y * y);
+            } else if (KIND == 1) {
+                delta = lor / (x * x + w2);
+            } else {
+                if (win > (R)0 && fabs(x) > win) continue;
+                const R y = x * invw;
+                delta = gaussian ? gsc * exp(-y * y) : lor / (x * x + w2);
+            }
+            const R weight = fq * delta;
+            if (weight == (R)0) continue;
+            acc[j][0].x = fma(weight, q0.x, acc[j][0].x);
+            acc[j][0].y = fma(weight, q0.y, acc[j][0].y);
+            acc[j][1].x = fma(weight, q1.x, acc[j][1].x);
+            acc[j][1].y = fma(weight, q1.y, acc[j][1].y);
+        }
+    }
+}
+
 // R: storage/arithmetic type of the per-k matrices (double: plain FP64 path; float: mixed path).
 // Energies, inverse energy differences, occupations and every accumulation across pairs of a
 // scalar response and across k-points stay FP64.
@@ -622,34 +657,13 @@ __global__ void __launch_bounds__(256) response_kernel(RespParams p) {
                     if (active) {
                         const C *Q0 = sQ + (size_t)c0 * nn;
                         const C *Q1 = sQ + (size_t)(two ? c0 + 1 : c0) * nn;
-                        for (int q = 0; q < npairs; ++q) {
-                            const double te = ste[q];
-                            const R fq = (R)sfnm[q];
-                            const C q0 = Q0[q], q1 = Q1[q];
-#pragma unroll
-                            for (int j = 0; j < RS_OMB; ++j) {
-                                const R x = (R)(te - om[j]);
-                                R delta;
-                                if (p.pair_mode == 1) {
-                                    // second_harmonic_delta with the transition window (SecondHarmonicKernels.jl:86-89).
-                                    if (win > (R)0 && fabs(x) > win) continue;
-                                    const R y = x * invw;
-                                    delta = p.gaussian ? gsc * exp(-y * y) : lor / (x * x + w2);
-                                } else if (p.gaussian) {
-                                    if (!(fabs(x) < cut)) continue;
-                                    const R y = x * invw;
-                                    delta = gsc * exp(-y * y);
-                                } else {
-                                    delta = lor / (x * x + w2);
-                                }
-                                const R weight = fq * delta;
-                                if (weight == (R)0) continue;
-                                acc[j][0].x = fma(weight, q0.x, acc[j][0].x);
-                                acc[j][0].y = fma(weight, q0.y, acc[j][0].y);
-                                acc[j][1].x = fma(weight, q1.x, acc[j][1].x);
-                                acc[j][1].y = fma(weight, q1.y, acc[j][1].y);
-                            }
-                        }
+                        // The delta kind is fixed per pass: one specialised loop each.
+                        if (p.pair_mode == 1)
+                            contract_pairs<R, C, 2>(ste, sfnm, Q0, Q1, npairs, om, acc, gsc, cut, invw, w2, lor, win, p.gaussian);
+                        else if (p.gaussian)
+                            contract_pairs<R, C, 0>(ste, sfnm, Q0, Q1, npairs, om, acc, gsc, cut, invw, w2, lor, win, 1);
+                        else
+                            contract_pairs<R, C, 1>(ste, sfnm, Q0, Q1, npairs, om, acc, gsc, cut, invw, w2, lor, win, 0);
                     }
 #pragma unroll
                     for (int j = 0; j < RS_OMB; ++j) {
