@@ -16,7 +16,7 @@ class NumpyMlpProposer(MlpProposer):
         self.spectrum_fn = spectrum_fn
         self.train_steps = train_steps
         self.lr = learning_rate
-        self.X, self.Y = [], []
+        self.X, self.E = [], []
         self.spectrum_evaluations = 0
         rng = np.random.default_rng(seed)
         p = np.zeros(M.COUNT)
@@ -34,7 +34,7 @@ class NumpyMlpProposer(MlpProposer):
 
     def train(self):
         X = np.concatenate(self.X)
-        Y = np.concatenate(self.Y)
+        Y = self._targets()
         p = self.p.astype(np.float64)
         for _ in range(self.train_steps):
             _, g = M.loss_grad(p.astype(np.float32), X, Y)

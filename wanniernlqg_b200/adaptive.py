@@ -17,10 +17,10 @@ Scheme (this engine's own; the reference's adaptive integrator is the HCubature 
 The plain method checks every leaf.  The learned method (``MlpProposer``) predicts log10 of each
 unchecked leaf's error from cheap features (cell centre, size, parent error, the centre value
 and the distance of the centre's spectrum to the Fermi level and to the photon window) and
-checks only the leaves predicted above the threshold plus a random audit sample; if the audit
-finds a leaf whose true error exceeds its prediction by more than ``audit_factor``, every
-prediction is scaled up by the worst audited ratio and the leaves the rescaled budget requires
-are checked (every leaf, when the ratio exceeds audit_factor^3).  Unchecked leaves keep their coarse value (an actual
+checks only the leaves predicted above the threshold plus a random audit sample.  The audit
+estimates the error mass the network missed (audited under-prediction divided by the audit
+fraction); if that mass exceeds the tolerance budget, the round falls back to the plain method
+and checks every leaf.  Unchecked leaves keep their coarse value (an actual
 integrand value) and count their predicted error in the total.  The network never supplies an
 integrand value; it only decides which cells are checked first.
 """
@@ -70,7 +70,7 @@ class MlpProposer:
         self.train_steps = train_steps
         self.lr = learning_rate
         self.X = []
-        self.Y = []
+        self.E = []
         self.spectrum_evaluations = 0
 
     def close(self):
@@ -106,11 +106,18 @@ class MlpProposer:
 
     def observe(self, feats: np.ndarray, errors: np.ndarray):
         self.X.append(feats)
-        self.Y.append(np.log10(np.maximum(errors, 1e-30)).astype(np.float32) / 10.0)
+        self.E.append(np.asarray(errors, dtype=np.float64))
+
+    def _targets(self):
+        # Errors far below the largest one never decide a refinement: clip them at 1e-6 of the
+        # largest so that the fit spends its capacity on the decisive range.
+        e = np.concatenate(self.E)
+        floor = max(float(np.max(e)) * 1e-6, 1e-300)
+        return (np.log10(np.maximum(e, floor)) / 10.0).astype(np.float32)
 
     def train(self):
         X = np.ascontiguousarray(np.concatenate(self.X), dtype=np.float32)
-        Y = np.ascontiguousarray(np.concatenate(self.Y), dtype=np.float32)
+        Y = np.ascontiguousarray(self._targets(), dtype=np.float32)
         loss = ctypes.c_float()
         fp = ctypes.POINTER(ctypes.c_float)
         _lib.check(self.L.wnlqg_b200_mlp_train(self.m, X.ctypes.data_as(fp), Y.ctypes.data_as(fp), X.shape[0],
@@ -127,7 +134,7 @@ class MlpProposer:
 
 def integrate_cells(point_values: Callable, *, n0: int = 16, rtol: float = 1e-4, max_level: int = 8,
                     max_evaluations: int = 50_000_000, proposer: Optional[MlpProposer] = None,
-                    warmup_fraction: float = 0.15, audit_fraction: float = 0.05, audit_factor: float = 10.0,
+                    warmup_fraction: float = 0.15, audit_fraction: float = 0.05,
                     safety: float = 4.0, seed: int = 0, component=None) -> AdaptiveResult:
     """Integrate the domain average of point_values(k[n,3]) -> [n, V] over [0,1)^3.
 
@@ -178,7 +185,11 @@ def integrate_cells(point_values: Callable, *, n0: int = 16, rtol: float = 1e-4,
             feats = proposer.features(centers[todo], 2 * half[todo], parent_err[todo],
                                       np.max(np.abs(coarse[todo][:, sel]), axis=1) / vol[todo])
             if not proposer.X:
+                # Warm-up labels: a random sample plus the leaves with the largest centre values,
+                # so that the first training set contains the cells that matter.
                 first = rng.random(todo.size) < warmup_fraction
+                mag = np.max(np.abs(coarse[todo][:, sel]), axis=1) / vol[todo]
+                first[np.argsort(-mag, kind="stable")[:max(1, int(0.05 * todo.size))]] = True
                 check(todo[first])
                 checked_total += int(first.sum())
                 proposer.observe(feats[first], err[todo[first]])
@@ -203,24 +214,15 @@ def integrate_cells(point_values: Callable, *, n0: int = 16, rtol: float = 1e-4,
                              err[chosen])
             aud = rest[audit & ~np.isin(np.arange(rest.size), must)]
             if aud.size:
-                ratio = float(np.max(err[aud] / np.maximum(pred[aud], 1e-300)))
-                if ratio > audit_factor:
-                    # The audit found under-predicted errors: recalibrate every prediction by the
-                    # worst audited ratio and check what the recalibrated budget requires; fall back
-                    # to checking every leaf if the network is off by more than audit_factor^3.
+                # The audit estimates the error mass the network missed among the unchecked leaves
+                # (the audited under-prediction scaled by the audit fraction).  If it does not fit
+                # the budget, the plain method takes over for the round: every leaf is checked.
+                missed = float(np.sum(np.maximum(err[aud] - pred[aud], 0.0))) / audit_fraction
+                if missed > 0.5 * budget * safety:
                     fallbacks += 1
                     left = np.where(~checked)[0]
-                    if ratio > audit_factor ** 3:
-                        check(left)
-                        checked_total += left.size
-                    else:
-                        pl = pred[left] * ratio
-                        pred[left] = pl
-                        order2 = np.argsort(-pl, kind="stable")
-                        csum2 = np.cumsum(pl[order2][::-1])[::-1]
-                        extra = left[order2[csum2 > budget * 0.5]]
-                        check(extra)
-                        checked_total += extra.size
+                    check(left)
+                    checked_total += left.size
             proposer.train()
         value = np.where(checked[:, None], fine, coarse).sum(axis=0)
         est = np.where(checked, err, np.nan_to_num(pred, nan=0.0))
