@@ -266,15 +266,46 @@ WNLQG_D void small_product(const double2 *X, const double2 *Y, double2 *out, int
     __syncthreads();
 }
 
-// Stage 1 of the mixed eigensolver: FP32 parallel Jacobi (17 KB of shared memory at nw = 32, so
-// several CTAs share an SM).  Writes the FP32 eigenvector estimate V [b][np][np] to global memory.
+// Stage 1 of the mixed eigensolver: FP32 parallel Jacobi.  Each CTA walks a contiguous run of
+// the batch.  Consecutive mesh indices are neighbouring k-points (periodically), so from the
+// second point on the Jacobi iteration starts from the previous point's eigenvectors V: V is
+// re-orthonormalised (first-order Loewdin, V <- V (3I - V^H V)/2) and A = V^H H V is then nearly
+// diagonal, which cuts the sweeps needed to reach FP32 accuracy.  Writes the FP32 eigenvector
+// estimate V [b][np][np] to global memory.
 struct EighF32Smem {
     static __host__ __device__ size_t bytes(int nw) {
         int np = nw + (nw & 1);
         int ld = np + 1;
-        return 2 * (size_t)np * ld * sizeof(float2) + (size_t)(np / 2) * (sizeof(float2) + sizeof(float) + 2 * sizeof(int)) + 64;
+        return 3 * (size_t)np * ld * sizeof(float2) + (size_t)(np / 2) * (sizeof(float2) + sizeof(float) + 2 * sizeof(int)) + 64;
     }
 };
+
+// out = op(X) * Y for np x np FP32 shared matrices, results staged in registers (out may alias).
+// Needs blockDim.x * 8 >= np*np.
+WNLQG_D void small_product_f32(const float2 *X, const float2 *Y, float2 *out, int np, int ld, bool xh) {
+    const int nel = np * np;
+    float2 tv[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        const int e = threadIdx.x + r * blockDim.x;
+        float2 acc = make_float2(0.f, 0.f);
+        if (e < nel) {
+            const int i = e % np, j = e / np;
+            if (xh)
+                for (int l = 0; l < np; ++l) acc = cfmaconj(X[l + ld * i], Y[l + ld * j], acc);
+            else
+                for (int l = 0; l < np; ++l) acc = cfma(X[i + ld * l], Y[l + ld * j], acc);
+        }
+        tv[r] = acc;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        const int e = threadIdx.x + r * blockDim.x;
+        if (e < nel) out[(e % np) + ld * (e / np)] = tv[r];
+    }
+    __syncthreads();
+}
 
 __global__ void jacobi_eigh_f32_kernel(const double2 *__restrict__ h_in, int64_t h_stride, int64_t batch, int nw,
                                        float2 *__restrict__ V_out) {
@@ -284,14 +315,18 @@ __global__ void jacobi_eigh_f32_kernel(const double2 *__restrict__ h_in, int64_t
     const int half = np / 2;
     float2 *A32 = reinterpret_cast<float2 *>(smraw);
     float2 *V32 = A32 + (size_t)np * ld;
-    float2 *rot_s = V32 + (size_t)np * ld;
+    float2 *T32 = V32 + (size_t)np * ld;
+    float2 *rot_s = T32 + (size_t)np * ld;
     float *rot_c = reinterpret_cast<float *>(rot_s + half);
     int *rot_p = reinterpret_cast<int *>(rot_c + half);
     int *rot_q = rot_p + half;
     __shared__ double red[48];
     __shared__ int rot_flag;
     const int tid = threadIdx.x;
-    for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) {
+    const int64_t kb = (batch * blockIdx.x) / gridDim.x;
+    const int64_t ke = (batch * (blockIdx.x + 1)) / gridDim.x;
+    for (int64_t b = kb; b < ke; ++b) {
+        const bool warm = b > kb;
         const double2 *h = h_in + b * h_stride;
         double local = 0.0;
         for (int e = tid; e < np * np; e += blockDim.x) {
@@ -304,7 +339,7 @@ __global__ void jacobi_eigh_f32_kernel(const double2 *__restrict__ h_in, int64_t
             }
             local += v.x * v.x + v.y * v.y;
             A32[i + ld * j] = make_float2((float)v.x, (float)v.y);
-            V32[i + ld * j] = make_float2(i == j ? 1.0f : 0.0f, 0.0f);
+            if (!warm) V32[i + ld * j] = make_float2(i == j ? 1.0f : 0.0f, 0.0f);
         }
         for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xffffffffu, local, o);
         if ((tid & 31) == 0) red[tid >> 5] = local;
@@ -316,14 +351,34 @@ __global__ void jacobi_eigh_f32_kernel(const double2 *__restrict__ h_in, int64_t
         }
         __syncthreads();
         const double fro = red[41];
+        if (warm) {
+            // V <- V (3I - V^H V)/2, then A <- V^H H V.
+            small_product_f32(V32, V32, T32, np, ld, true);
+            for (int e = tid; e < np * np; e += blockDim.x) {
+                const int i = e % np, j = e / np;
+                const float2 v = T32[i + ld * j];
+                T32[i + ld * j] = make_float2((i == j ? 1.5f : 0.0f) - 0.5f * v.x, -0.5f * v.y);
+            }
+            __syncthreads();
+            small_product_f32(V32, T32, V32, np, ld, false);
+            small_product_f32(A32, V32, T32, np, ld, false);
+            small_product_f32(V32, T32, A32, np, ld, true);
+            for (int e = tid; e < np * np; e += blockDim.x) {
+                const int i = e % np, j = e / np;
+                if (i > j) A32[i + ld * j] = cconj(A32[j + ld * i]);
+                if (i == j) A32[i + ld * i].y = 0.0f;
+            }
+            __syncthreads();
+        }
         const float tol32 = (float)(fro * 1.4901161193847656e-08);   // rotate while |a_pq| > 2^-26 ||H||
         for (int sweep = 0; sweep < WNLQG_JACOBI_MAX_SWEEPS; ++sweep) {
+            if (offdiag_norm(A32, np, ld, red) <= fro * 2.384185791015625e-07) break;
             if (tid == 0) rot_flag = 0;
             __syncthreads();
             jacobi_sweep<float>(A32, V32, np, ld, tol32, rot_s, rot_c, rot_p, rot_q, &rot_flag);
             const int any = rot_flag;
             __syncthreads();
-            if (!any || offdiag_norm(A32, np, ld, red) <= fro * 2.384185791015625e-07) break;
+            if (!any) break;
         }
         float2 *vo = V_out + b * (int64_t)np * np;
         for (int e = tid; e < np * np; e += blockDim.x) vo[e] = V32[(e % np) + ld * (e / np)];
@@ -338,7 +393,7 @@ struct EighRefineSmem {
     static __host__ __device__ size_t bytes(int nw) {
         int np = nw + (nw & 1);
         int ld = np + 1;
-        return 3 * (size_t)np * ld * sizeof(double2) + (size_t)(np / 2) * (sizeof(double2) + sizeof(double) + 2 * sizeof(int)) + 64;
+        return 2 * (size_t)np * ld * sizeof(double2) + (size_t)(np / 2) * (sizeof(double2) + sizeof(double) + 2 * sizeof(int)) + 64;
     }
 };
 
@@ -350,8 +405,7 @@ __global__ void eigh_refine_f64_kernel(const double2 *__restrict__ h_in, int64_t
     const int half = np / 2;
     double2 *A64 = reinterpret_cast<double2 *>(smraw);
     double2 *V64 = A64 + (size_t)np * ld;
-    double2 *S64 = V64 + (size_t)np * ld;
-    double2 *rot_s = S64 + (size_t)np * ld;
+    double2 *rot_s = V64 + (size_t)np * ld;
     double *rot_c = reinterpret_cast<double *>(rot_s + half);
     int *rot_p = reinterpret_cast<int *>(rot_c + half);
     int *rot_q = rot_p + half;
@@ -385,21 +439,41 @@ __global__ void eigh_refine_f64_kernel(const double2 *__restrict__ h_in, int64_t
         __syncthreads();
         const double fro = red[41];
         // Loewdin orthonormalisation to second order: E = V^H V - I (about 1e-6 after the FP32
-        // sweeps), W = V (I - E/2 + 3E^2/8), so that W^H W - I = O(|E|^3).
-        small_product(V64, V64, S64, np, ld, true);            // S = V^H V
-        for (int e = tid; e < np * np; e += blockDim.x) {
-            const int i = e % np, j = e / np;
-            if (i == j) S64[i + ld * i].x -= 1.0;                // E = S - I
+        // sweeps), W = V (I - E/2 + 3E^2/8), so that W^H W - I = O(|E|^3).  A64 serves as the
+        // scratch for E and E^2 (every thread keeps its own entries of E in registers); H is
+        // loaded afterwards.
+        small_product(V64, V64, A64, np, ld, true);            // A64 <- V^H V
+        double2 ev[8];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            const int e = tid + r * blockDim.x;
+            ev[r] = make_double2(0.0, 0.0);
+            if (e < np * np) {
+                const int i = e % np, j = e / np;
+                ev[r] = A64[i + ld * j];
+                if (i == j) ev[r].x -= 1.0;
+            }
         }
         __syncthreads();
-        small_product(S64, S64, A64, np, ld, false);           // A64 <- E^2 (H is reloaded below)
-        for (int e = tid; e < np * np; e += blockDim.x) {
-            const int i = e % np, j = e / np;
-            const double2 ev = S64[i + ld * j], e2 = A64[i + ld * j];
-            S64[i + ld * j] = make_double2((i == j ? 1.0 : 0.0) - 0.5 * ev.x + 0.375 * e2.x, -0.5 * ev.y + 0.375 * e2.y);
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            const int e = tid + r * blockDim.x;
+            if (e < np * np) A64[(e % np) + ld * (e / np)] = ev[r];
         }
         __syncthreads();
-        small_product(V64, S64, V64, np, ld, false);           // W = V M
+        small_product(A64, A64, A64, np, ld, false);           // A64 <- E^2
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            const int e = tid + r * blockDim.x;
+            if (e < np * np) {
+                const int i = e % np, j = e / np;
+                const double2 e2 = A64[i + ld * j];
+                A64[i + ld * j] = make_double2((i == j ? 1.0 : 0.0) - 0.5 * ev[r].x + 0.375 * e2.x,
+                                               -0.5 * ev[r].y + 0.375 * e2.y);
+            }
+        }
+        __syncthreads();
+        small_product(V64, A64, V64, np, ld, false);           // W = V M
         for (int e = tid; e < np * np; e += blockDim.x) {
             const int i = e % np, j = e / np;
             double2 v = make_double2(0.0, 0.0);

@@ -89,6 +89,7 @@ struct wnlqg_plan {
     int eigh_threads = 32;
     size_t eigh_smem = 0;
     int refine_threads = 32;
+    int sm_count = 148;
     size_t refine_smem = 0;
     float2 *d_V32 = nullptr;
     cudaStream_t stream = nullptr;
@@ -395,7 +396,10 @@ wnlqg_status run_front(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const int64_
     wnlqg_status st = record_event(pl, ev_base + 1);
     if (st != WNLQG_OK) return st;
     if (pl->task.precision == WNLQG_PRECISION_MIXED) {
-        jacobi_eigh_f32_kernel<<<(unsigned)nb, pl->eigh_threads, pl->eigh_smem, pl->stream>>>(
+        int per_sm = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jacobi_eigh_f32_kernel, pl->eigh_threads, pl->eigh_smem);
+        const int64_t f32_grid = std::min<int64_t>(nb, (int64_t)std::max(1, per_sm) * pl->sm_count);
+        jacobi_eigh_f32_kernel<<<(unsigned)f32_grid, pl->eigh_threads, pl->eigh_smem, pl->stream>>>(
             pl->d_xw + (int64_t)pl->ch_H * pl->nn, N, nb, pl->nw, pl->d_V32);
         eigh_refine_f64_kernel<<<(unsigned)nb, pl->refine_threads, pl->refine_smem, pl->stream>>>(
             pl->d_xw + (int64_t)pl->ch_H * pl->nn, N, pl->d_V32, nb, pl->nw, pl->d_E, pl->d_U);
@@ -689,6 +693,7 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
     int sm_count = 148;
     int dev = model->device;
     cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev);
+    pl->sm_count = sm_count;
     int smem_optin = 0;
     cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     if (smem_optin <= 0) smem_optin = 48 * 1024;
@@ -781,9 +786,10 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
         const int np = nw + (nw & 1);
         pl->eigh_smem = EighF32Smem::bytes(nw);
         pl->refine_smem = EighRefineSmem::bytes(nw);
+        // Both stages need blockDim >= np/2 (pairs) and 8 * blockDim >= np^2 (register-staged products).
         pl->refine_threads = std::max(32, std::min(256, ((np * np / 8 + 31) / 32) * 32));
-        pl->refine_threads = std::max(pl->refine_threads, pl->eigh_threads);
-        pl->eigh_threads = std::max(32, std::min(pl->eigh_threads, 128));   // FP32 stage: more CTAs per SM
+        pl->refine_threads = std::max(pl->refine_threads, ((np / 2 + 31) / 32) * 32);
+        pl->eigh_threads = pl->refine_threads;
         if ((st = alloc((void **)&pl->d_V32, (size_t)max_batch * np * np * sizeof(float2))) != WNLQG_OK) return bail(st);
         cudaError_t e = cudaFuncSetAttribute(eigh_refine_f64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)std::max<size_t>(pl->refine_smem, 48 * 1024));
