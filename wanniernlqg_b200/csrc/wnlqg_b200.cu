@@ -700,7 +700,9 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
 
     if (max_batch <= 0) {
         int64_t per_k = (int64_t)pl->C * nn * 16 + (int64_t)nr * 16 + nn * 16 + nw * 8;
-        max_batch = std::max<int64_t>(256, std::min<int64_t>(1 << 20, ((int64_t)1 << 30) / per_k));
+        // About 4 GiB of batch workspace (HBM is 180 GB): long runs of neighbouring k-points per
+        // CTA for the warm-started eigensolver and few batches per call.
+        max_batch = std::max<int64_t>(256, std::min<int64_t>(1 << 20, ((int64_t)1 << 32) / per_k));
         max_batch = (max_batch / 64) * 64;
     }
     pl->max_batch = max_batch;
