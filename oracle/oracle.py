@@ -42,6 +42,8 @@ def lib():
                                             ctypes.c_int64, ctypes.c_int64, ctypes.c_int, dp]
         L.oracle_kpoint_spectrum.argtypes = [ctypes.POINTER(_abi.ModelDesc), dp, dp, dp, dp]
         L.oracle_hermitian_eigen.argtypes = [ctypes.c_int64, dp, dp, dp]
+        L.oracle_generalized_eigen.argtypes = [ctypes.c_int64, dp, dp, dp, dp]
+        L.oracle_generalized_eigen.restype = ctypes.c_int
         L.oracle_jerk_algebra.argtypes = [ctypes.c_int64, dp, dp, dp, dp, ctypes.c_int64, dp, ctypes.c_double,
                                           ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                           ctypes.c_double, ctypes.c_int64, ctypes.POINTER(ctypes.c_int32), dp]
@@ -107,6 +109,17 @@ def hermitian_eigen(h: np.ndarray):
     u = np.zeros((n, n), dtype=np.complex128, order="F")
     _check(lib().oracle_hermitian_eigen(n, _dp(h), _dp(e), _dp(u)))
     return e, u
+
+
+def generalized_eigen(h: np.ndarray, s: np.ndarray):
+    """Oracle generalised eigensolve (upper triangles): energies and S-orthonormal canonical C."""
+    h = np.asfortranarray(h, dtype=np.complex128)
+    s_ = np.asfortranarray(s, dtype=np.complex128)
+    n = h.shape[0]
+    e = np.zeros(n)
+    c = np.zeros((n, n), dtype=np.complex128, order="F")
+    _check(lib().oracle_generalized_eigen(n, _dp(h), _dp(s_), _dp(e), _dp(c)))
+    return e, c
 
 
 def jerk_algebra(energies, B, A, C, omegas, components, *, mu=0.0, T=0.0, width=0.04, gaussian=True,

@@ -11,6 +11,8 @@
 //   real-space derivative tiles HamiltonianMatrixElements.jl:92-177; PositionMatrixElements.jl:8-84
 //   Hermitian eigensolve        src/Core/ESKernel/DenseSpectra.jl:14-16 (LAPACK there; cyclic Jacobi here)
 //   phase canonicalisation      HamiltonianMatrixElements.jl:6-25
+//   generalised eigensolve      DenseSpectra.jl:33-39 (LAPACK hegv there; Cholesky + Jacobi here),
+//                               NonorthogonalMatrixElements.jl:349-385
 //   gauge rotation U'XU         HamiltonianMatrixElements.jl:61-71
 //   gauge correction, r, F      PositionMatrixElements.jl:416-556; PositionVertexRegularization.jl:7-29
 //   transition screen           src/Runtime/Execution/TransitionScreening.jl:32-94; CalculationUtils.jl:21-46
@@ -69,7 +71,9 @@ struct Model {
     std::vector<int64_t> deg;     // [NR]
     std::vector<cd> H;            // [nw*nw*NR]
     std::vector<cd> A;            // [nw*nw*3*NR] (zeros when absent)
+    std::vector<cd> S;            // [nw*nw*NR] overlap (nonorthogonal models)
     bool has_position = false;
+    bool has_overlap = false;
 };
 
 // Which Cartesian channels a task needs (the reference's MatrixElementPlan direction
@@ -204,6 +208,65 @@ void canonicalize(Mat &U) {
             for (int i = 0; i < n; ++i) U(i, j) *= phase;
         }
     }
+}
+
+// Generalised Hermitian eigensolve of (H, S) from their upper triangles: S = L L^H, Jacobi on
+// L^-1 H L^-H, C = L^-H U (so C^H S C = I), eigenvalues ascending.  Returns false when S is not
+// positive definite.
+bool generalized_eigen(const Mat &h, const Mat &sm, std::vector<double> &evals, Mat &C) {
+    int n = h.n;
+    Mat S; S.init(n);
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i <= j; ++i) {
+            if (i == j) S(i, i) = cd(sm(i, i).real(), 0.0);
+            else { S(i, j) = sm(i, j); S(j, i) = std::conj(sm(i, j)); }
+        }
+    Mat L; L.init(n);
+    for (int j = 0; j < n; ++j) {
+        double d = S(j, j).real();
+        for (int k = 0; k < j; ++k) d -= std::norm(L(j, k));
+        if (!(d > 0)) return false;
+        L(j, j) = std::sqrt(d);
+        for (int i = j + 1; i < n; ++i) {
+            cd v = S(i, j);
+            for (int k = 0; k < j; ++k) v -= L(i, k) * std::conj(L(j, k));
+            L(i, j) = v / L(j, j).real();
+        }
+    }
+    Mat H; H.init(n);
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i <= j; ++i) {
+            if (i == j) H(i, i) = cd(h(i, i).real(), 0.0);
+            else { H(i, j) = h(i, j); H(j, i) = std::conj(h(i, j)); }
+        }
+    Mat X; X.init(n);   // X = L^-1 H
+    for (int c = 0; c < n; ++c)
+        for (int r = 0; r < n; ++r) {
+            cd v = H(r, c);
+            for (int k = 0; k < r; ++k) v -= L(r, k) * X(k, c);
+            X(r, c) = v / L(r, r).real();
+        }
+    Mat Ht; Ht.init(n);   // Ht = X L^-H = (L^-1 X^H)^H
+    for (int c = 0; c < n; ++c) {
+        std::vector<cd> y(n);
+        for (int r = 0; r < n; ++r) {
+            cd v = std::conj(X(c, r));
+            for (int k = 0; k < r; ++k) v -= L(r, k) * y[k];
+            y[r] = v / L(r, r).real();
+        }
+        for (int r = 0; r < n; ++r) Ht(c, r) = std::conj(y[r]);
+    }
+    Mat U;
+    hermitian_eigen(Ht, evals, U);
+    C.init(n);
+    for (int c = 0; c < n; ++c)
+        for (int r = n - 1; r >= 0; --r) {
+            cd v = U(r, c);
+            for (int k = r + 1; k < n; ++k) v -= std::conj(L(k, r)) * C(k, c);
+            C(r, c) = v / L(r, r).real();
+        }
+    canonicalize(C);
+    return true;
 }
 
 // regularized_energy_inverse (PositionVertexRegularization.jl:17-29).
@@ -719,6 +782,11 @@ bool build_model(const wnlqg_model_desc *desc, Model &m) {
         m.A.resize(nn * 3 * m.nr);
         for (size_t e = 0; e < nn * 3 * m.nr; ++e) m.A[e] = cd(desc->position_r[2 * e], desc->position_r[2 * e + 1]);
     }
+    m.has_overlap = desc->overlap_r != nullptr;
+    if (m.has_overlap) {
+        m.S.resize(nn * m.nr);
+        for (size_t e = 0; e < nn * m.nr; ++e) m.S[e] = cd(desc->overlap_r[2 * e], desc->overlap_r[2 * e + 1]);
+    }
     for (auto &z : m.H) if (!std::isfinite(z.real()) || !std::isfinite(z.imag())) { set_error("hamiltonian_r contains non-finite values"); return false; }
     for (int64_t g : m.deg) if (g <= 0) { set_error("r_degeneracies must be positive"); return false; }
     return true;
@@ -798,6 +866,25 @@ int oracle_kpoint_spectrum(const wnlqg_model_desc *md, const double k[3], double
                            double *eigenvectors, double *dh) {
     Model m;
     if (!build_model(md, m)) return WNLQG_ERR_INVALID_ARGUMENT;
+    if (m.has_overlap) {
+        // Nonorthogonal spectrum: H(k), S(k) by the direct sums, then the generalised eigensolve.
+        const size_t nn = (size_t)m.nw * m.nw;
+        Mat Hk, Sk;
+        Hk.init(m.nw);
+        Sk.init(m.nw);
+        for (int ir = 0; ir < m.nr; ++ir) {
+            const int64_t *r = &m.rvec[3 * (size_t)ir];
+            double phase = (double)r[0] * k[0] + (double)r[1] * k[1] + (double)r[2] * k[2];
+            cd f = std::polar(1.0, 2.0 * PI * phase) / (double)m.deg[ir];
+            for (size_t e = 0; e < nn; ++e) { Hk.v[e] += f * m.H[nn * ir + e]; Sk.v[e] += f * m.S[nn * ir + e]; }
+        }
+        std::vector<double> ev;
+        Mat C;
+        if (!generalized_eigen(Hk, Sk, ev, C)) { set_error("effective S(k) is not positive definite"); return WNLQG_ERR_INVALID_ARGUMENT; }
+        for (int i = 0; i < m.nw; ++i) energies[i] = ev[i];
+        for (size_t e = 0; e < nn; ++e) { eigenvectors[2 * e] = C.v[e].real(); eigenvectors[2 * e + 1] = C.v[e].imag(); }
+        return WNLQG_OK;
+    }
     Needs need;
     for (int a = 0; a < 3; ++a) need.dH[a] = true;
     KData d;
@@ -821,6 +908,21 @@ int oracle_hermitian_eigen(int64_t n, const double *h, double *energies, double 
     canonicalize(U);
     for (int64_t i = 0; i < n; ++i) energies[i] = ev[i];
     for (int64_t e = 0; e < n * n; ++e) { eigenvectors[2 * e] = U.v[e].real(); eigenvectors[2 * e + 1] = U.v[e].imag(); }
+    return WNLQG_OK;
+}
+
+// Generalised eigensolve of one (H, S) pair (upper triangles), canonicalised: for pinning
+// against LAPACK hegv through scipy.
+int oracle_generalized_eigen(int64_t n, const double *h, const double *s, double *energies, double *eigenvectors) {
+    Mat a, b;
+    a.init((int)n);
+    b.init((int)n);
+    for (int64_t e = 0; e < n * n; ++e) { a.v[e] = cd(h[2 * e], h[2 * e + 1]); b.v[e] = cd(s[2 * e], s[2 * e + 1]); }
+    std::vector<double> ev;
+    Mat C;
+    if (!generalized_eigen(a, b, ev, C)) { set_error("effective S(k) is not positive definite"); return WNLQG_ERR_INVALID_ARGUMENT; }
+    for (int64_t i = 0; i < n; ++i) energies[i] = ev[i];
+    for (int64_t e = 0; e < n * n; ++e) { eigenvectors[2 * e] = C.v[e].real(); eigenvectors[2 * e + 1] = C.v[e].imag(); }
     return WNLQG_OK;
 }
 

@@ -264,3 +264,38 @@ def test_jerk_matches_oracle(engine_cls, oracle_mod, precision, kind):
     rm = oracle_mod.integrate_mesh(model, task, (5, 3, 3))
     assert rel_err(got, ref) < tol
     assert rel_err(gm, rm) < tol
+
+
+@pytest.mark.parametrize("nw,rmax", [(8, 1), (24, 1)])
+def test_nonorthogonal_generalized_spectrum_matches_oracle(engine_cls, oracle_mod, nw, rmax):
+    from wanniernlqg_b200.model import synthetic_nonorthogonal_model
+    model = synthetic_nonorthogonal_model(nw, rmax, 5)
+    task = _abi.TaskArrays([(_abi.QUANTUM_METRIC, ["xx"])], broadening_type=_abi.LORENTZIAN, broadening=0.01)
+    k = np.random.default_rng(19).random((12, 3))
+    with engine_cls(model, task) as eng:
+        e, c = eng.spectrum(k)
+    for i in range(k.shape[0]):
+        eo, co, _ = oracle_mod.kpoint_spectrum(model, k[i])
+        assert np.max(np.abs(e[i] - eo)) < 1e-11 * max(1.0, np.abs(eo).max())
+        ph = np.exp(2j * np.pi * (model.r_vectors.T @ k[i])) / model.r_degeneracies
+        sk = np.einsum("ijr,r->ij", model.overlap_r, ph)
+        ov = np.abs(np.sum(c[i].conj() * (sk @ co), axis=0))
+        assert np.max(np.abs(ov - 1.0)) < 1e-9
+
+
+def test_nonorthogonal_responses_rejected_and_indefinite_overlap_reported(engine_cls):
+    from wanniernlqg_b200._lib import EngineError
+    from wanniernlqg_b200.model import synthetic_nonorthogonal_model
+    model = synthetic_nonorthogonal_model(6, 1, 2)
+    task = _abi.TaskArrays([(_abi.QUANTUM_METRIC, ["xx"])])
+    with engine_cls(model, task) as eng:
+        with pytest.raises(EngineError) as ei:
+            eng.integrate_mesh((2, 2, 2))
+        assert ei.value.status == 6
+    bad = synthetic_nonorthogonal_model(6, 1, 2)
+    home = int(np.where(np.all(bad.r_vectors == 0, axis=0))[0][0])
+    bad.overlap_r[:, :, home] -= 2.0 * np.eye(6)       # S(k) = -I + small: not positive definite
+    with engine_cls(bad, task) as eng:
+        with pytest.raises(EngineError) as ei:
+            eng.spectrum(np.array([[0.1, 0.2, 0.3]]))
+        assert ei.value.status == 1

@@ -162,3 +162,18 @@ def test_mlp_oracle_gradient_matches_finite_differences():
             e[o + i] = 1e-3
             fd = (loss_at(p + e) - loss_at(p - e)) / 2e-3
             assert abs(fd - g[o + i]) < 1e-4 * max(1.0, abs(fd))
+
+
+@pytest.mark.parametrize("n", [2, 5, 16])
+def test_generalized_eigen_matches_lapack(oracle_mod, n):
+    import scipy.linalg
+    rng = np.random.default_rng(30 + n)
+    a = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    h = a + a.conj().T
+    b = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    s = b @ b.conj().T + n * np.eye(n)
+    e, c = oracle_mod.generalized_eigen(h, s)
+    el = scipy.linalg.eigh(h, s, eigvals_only=True)
+    assert np.max(np.abs(e - el)) < 1e-12 * max(1.0, np.abs(el).max())
+    assert np.max(np.abs(c.conj().T @ s @ c - np.eye(n))) < 1e-12
+    assert np.max(np.abs(h @ c - s @ c * e)) < 1e-11 * max(1.0, np.abs(el).max())

@@ -526,3 +526,154 @@ __global__ void eigh_refine_f64_kernel(const double2 *__restrict__ h_in, int64_t
     }
 }
 
+
+// ---------------------------------------------------------------------------------------------
+// Generalised Hermitian eigensolve H C = S C E for nonorthogonal models, FP64
+// (generalized_hermitian_spectrum, DenseSpectra.jl:33-39: eigen(Hermitian(H,:U), Hermitian(S,:U))).
+// S = L L^H (Cholesky, lower), Ht = L^-1 H L^-H, Jacobi on Ht, C = L^-H Ut, so C^H S C = I; then
+// ascending order and the canonical phase rule (NonorthogonalMatrixElements.jl:382-385).
+// A non-positive pivot of S sets the k-point's status word to 1 (S(k) not positive definite).
+// ---------------------------------------------------------------------------------------------
+struct GenEighSmem {
+    static __host__ __device__ size_t bytes(int nw) {
+        int np = nw + (nw & 1);
+        int ld = np + 1;
+        return 3 * (size_t)np * ld * sizeof(double2) + (size_t)(np / 2) * (sizeof(double2) + sizeof(double) + 2 * sizeof(int)) + 64;
+    }
+};
+
+__global__ void generalized_eigh_kernel(const double2 *__restrict__ h_in, const double2 *__restrict__ s_in,
+                                        int64_t stride, int64_t batch, int nw, double *__restrict__ E_out,
+                                        double2 *__restrict__ U_out, int *__restrict__ status) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int np = nw + (nw & 1);
+    const int ld = np + 1;
+    const int half = np / 2;
+    double2 *A = reinterpret_cast<double2 *>(smraw);     // H, then Ht, then the Jacobi matrix
+    double2 *V = A + (size_t)np * ld;                    // Jacobi eigenvectors
+    double2 *Lm = V + (size_t)np * ld;                   // S, then its Cholesky factor
+    double2 *rot_s = Lm + (size_t)np * ld;
+    double *rot_c = reinterpret_cast<double *>(rot_s + half);
+    int *rot_p = reinterpret_cast<int *>(rot_c + half);
+    int *rot_q = rot_p + half;
+    __shared__ double red[48];
+    __shared__ int rot_flag, bad;
+    const int tid = threadIdx.x;
+    for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) {
+        const double2 *h = h_in + b * stride;
+        const double2 *sk = s_in + b * stride;
+        if (tid == 0) bad = 0;
+        for (int e = tid; e < np * np; e += blockDim.x) {
+            const int i = e % np, j = e / np;
+            double2 hv = make_double2(0.0, 0.0), sv = make_double2(i == j ? 1.0 : 0.0, 0.0);
+            if (i < nw && j < nw) {
+                if (i < j) { hv = h[i + (size_t)nw * j]; sv = sk[i + (size_t)nw * j]; }
+                else if (i > j) { hv = cconj(h[j + (size_t)nw * i]); sv = cconj(sk[j + (size_t)nw * i]); }
+                else { hv = make_double2(h[i + (size_t)nw * i].x, 0.0); sv = make_double2(sk[i + (size_t)nw * i].x, 0.0); }
+            }
+            A[i + ld * j] = hv;
+            Lm[i + ld * j] = sv;
+            V[i + ld * j] = make_double2(i == j ? 1.0 : 0.0, 0.0);
+        }
+        __syncthreads();
+        // Right-looking Cholesky in place (lower triangle of Lm).
+        for (int j = 0; j < np; ++j) {
+            if (tid == 0) {
+                const double d = Lm[j + ld * j].x;
+                if (!(d > 0.0)) bad = 1;
+                Lm[j + ld * j] = make_double2(d > 0.0 ? sqrt(d) : 1.0, 0.0);
+            }
+            __syncthreads();
+            const double ljj = Lm[j + ld * j].x;
+            for (int i = j + 1 + tid; i < np; i += blockDim.x) Lm[i + ld * j] = cscale(Lm[i + ld * j], 1.0 / ljj);
+            __syncthreads();
+            for (int e = tid; e < np * np; e += blockDim.x) {
+                const int r = e % np, c = e / np;
+                if (c > j && r >= c) Lm[r + ld * c] = csub(Lm[r + ld * c], cmul(Lm[r + ld * j], cconj(Lm[c + ld * j])));
+            }
+            __syncthreads();
+        }
+        // X = L^-1 H (forward substitution, one thread per column), stored in V.
+        for (int c = tid; c < np; c += blockDim.x)
+            for (int r = 0; r < np; ++r) {
+                double2 acc = A[r + ld * c];
+                for (int k = 0; k < r; ++k) acc = csub(acc, cmul(Lm[r + ld * k], V[k + ld * c]));
+                V[r + ld * c] = cscale(acc, 1.0 / Lm[r + ld * r].x);
+            }
+        __syncthreads();
+        // Ht = X L^-H = (L^-1 X^H)^H: solve L Y = X^H column by column (column c of X^H is row c
+        // of X, conjugated); Ht[c][r] = conj(Y[r][c]).
+        for (int c = tid; c < np; c += blockDim.x)
+            for (int r = 0; r < np; ++r) {
+                double2 acc = cconj(V[c + ld * r]);
+                for (int k = 0; k < r; ++k) acc = csub(acc, cmul(Lm[r + ld * k], cconj(A[c + ld * k])));
+                A[c + ld * r] = cconj(cscale(acc, 1.0 / Lm[r + ld * r].x));
+            }
+        __syncthreads();
+        // Hermitian part from the upper triangle; identity for the eigenvector accumulation.
+        for (int e = tid; e < np * np; e += blockDim.x) {
+            const int i = e % np, j = e / np;
+            V[i + ld * j] = make_double2(i == j ? 1.0 : 0.0, 0.0);
+        }
+        __syncthreads();
+        for (int e = tid; e < np * np; e += blockDim.x) {
+            const int i = e % np, j = e / np;
+            if (i > j) A[i + ld * j] = cconj(A[j + ld * i]);
+            if (i == j) A[i + ld * i].y = 0.0;
+        }
+        __syncthreads();
+        double local = 0.0;
+        for (int e = tid; e < np * np; e += blockDim.x) {
+            const double2 z = A[(e % np) + ld * (e / np)];
+            local += z.x * z.x + z.y * z.y;
+        }
+        for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xffffffffu, local, o);
+        if ((tid & 31) == 0) red[tid >> 5] = local;
+        __syncthreads();
+        if (tid == 0) {
+            double sum = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) sum += red[w];
+            red[41] = sqrt(sum);
+        }
+        __syncthreads();
+        const double tol = red[41] * 8.673617379884035e-19;
+        for (int sweep = 0; sweep < WNLQG_JACOBI_MAX_SWEEPS; ++sweep) {
+            if (offdiag_norm(A, np, ld, red) <= tol * np) break;
+            if (tid == 0) rot_flag = 0;
+            __syncthreads();
+            jacobi_sweep<double>(A, V, np, ld, tol, rot_s, rot_c, rot_p, rot_q, &rot_flag);
+            const int any = rot_flag;
+            __syncthreads();
+            if (!any) break;
+        }
+        // C = L^-H Ut (back substitution with L^H, one thread per column), in place in V.
+        for (int c = tid; c < np; c += blockDim.x)
+            for (int r = np - 1; r >= 0; --r) {
+                double2 acc = V[r + ld * c];
+                for (int k = r + 1; k < np; ++k) acc = csub(acc, cmul(cconj(Lm[k + ld * r]), V[k + ld * c]));
+                V[r + ld * c] = cscale(acc, 1.0 / Lm[r + ld * r].x);
+            }
+        __syncthreads();
+        for (int i = tid; i < nw; i += blockDim.x) {
+            const double di = A[i + ld * i].x;
+            int rank = 0;
+            for (int j = 0; j < nw; ++j) {
+                const double dj = A[j + ld * j].x;
+                rank += (dj < di) || (dj == di && j < i);
+            }
+            int pivot = 0;
+            double pm = hypot(V[0 + ld * i].x, V[0 + ld * i].y);
+            for (int r = 1; r < nw; ++r) {
+                const double mg = hypot(V[r + ld * i].x, V[r + ld * i].y);
+                if (mg > pm) { pm = mg; pivot = r; }
+            }
+            double2 phase = make_double2(1.0, 0.0);
+            if (pm > 0.0) phase = make_double2(V[pivot + ld * i].x / pm, -V[pivot + ld * i].y / pm);
+            E_out[b * nw + rank] = di;
+            double2 *u = U_out + b * (int64_t)nw * nw + (int64_t)nw * rank;
+            for (int r = 0; r < nw; ++r) u[r] = cmul(V[r + ld * i], phase);
+        }
+        if (tid == 0 && status) status[b] = bad;
+        __syncthreads();
+    }
+}

@@ -36,7 +36,7 @@ wnlqg_status fail(wnlqg_status st, const std::string &msg) {
                         std::string(#call) + ": " + cudaGetErrorString(err_));                            \
     } while (0)
 
-enum ChannelOp { CH_H = 0, CH_DH = 1, CH_DDH = 2, CH_A = 3, CH_DA = 4 };
+enum ChannelOp { CH_H = 0, CH_DH = 1, CH_DDH = 2, CH_A = 3, CH_DA = 4, CH_S = 5 };
 
 struct Channel {
     int op;
@@ -68,7 +68,9 @@ struct wnlqg_plan {
     wnlqg_task_desc task;
     std::vector<double> omegas, mus;
     std::vector<Channel> channels;
-    int ch_H = 0;
+    int ch_H = 0, ch_S = -1;
+    bool nonorth = false;
+    int *d_status = nullptr;
     int ch_dH[3], ch_A[3], ch_ddH[9], ch_dA[9];
     int nw = 0, nr = 0, C = 0;
     int64_t nn = 0, vc = 0, max_batch = 0;
@@ -395,7 +397,11 @@ wnlqg_status run_front(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const int64_
     }
     wnlqg_status st = record_event(pl, ev_base + 1);
     if (st != WNLQG_OK) return st;
-    if (pl->task.precision == WNLQG_PRECISION_MIXED) {
+    if (pl->nonorth) {
+        generalized_eigh_kernel<<<(unsigned)nb, pl->eigh_threads, GenEighSmem::bytes(pl->nw), pl->stream>>>(
+            pl->d_xw + (int64_t)pl->ch_H * pl->nn, pl->d_xw + (int64_t)pl->ch_S * pl->nn, N, nb, pl->nw, pl->d_E,
+            pl->d_U, pl->d_status);
+    } else if (pl->task.precision == WNLQG_PRECISION_MIXED) {
         int per_sm = 1;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jacobi_eigh_f32_kernel, pl->eigh_threads, pl->eigh_smem);
         const int64_t f32_grid = std::min<int64_t>(nb, (int64_t)std::max(1, per_sm) * pl->sm_count);
@@ -475,13 +481,14 @@ wnlqg_status wnlqg_b200_model_create(const wnlqg_model_desc *desc, int32_t devic
         return fail(WNLQG_ERR_UNSUPPORTED, "this build supports num_orbitals <= 32");
     if (!desc->lattice || !desc->r_vectors || !desc->r_degeneracies || !desc->hamiltonian_r)
         return fail(WNLQG_ERR_INVALID_ARGUMENT, "lattice, r_vectors, r_degeneracies and hamiltonian_r are required");
-    if (desc->overlap_r) return fail(WNLQG_ERR_UNSUPPORTED, "nonorthogonal models (overlap_r) are not supported by this build");
     const int nw = (int)desc->num_orbitals, nr = (int)desc->num_r_vectors;
     const size_t nn = (size_t)nw * nw;
     if (!finite_array(desc->lattice, 9)) return fail(WNLQG_ERR_NONFINITE, "lattice contains non-finite values");
     if (!finite_array(desc->hamiltonian_r, 2 * nn * nr)) return fail(WNLQG_ERR_NONFINITE, "hamiltonian_r contains non-finite values");
     if (desc->position_r && !finite_array(desc->position_r, 2 * nn * 3 * nr))
         return fail(WNLQG_ERR_NONFINITE, "position_r contains non-finite values");
+    if (desc->overlap_r && !finite_array(desc->overlap_r, 2 * nn * nr))
+        return fail(WNLQG_ERR_NONFINITE, "overlap_r contains non-finite values");
     for (int r = 0; r < nr; ++r)
         if (desc->r_degeneracies[r] <= 0) return fail(WNLQG_ERR_INVALID_ARGUMENT, "r_degeneracies must be positive");
     int ndev = 0;
@@ -497,6 +504,11 @@ wnlqg_status wnlqg_b200_model_create(const wnlqg_model_desc *desc, int32_t devic
     m->deg.assign(desc->r_degeneracies, desc->r_degeneracies + nr);
     m->H.resize(nn * nr);
     std::memcpy(m->H.data(), desc->hamiltonian_r, sizeof(double2) * nn * nr);
+    m->has_overlap = desc->overlap_r != nullptr;
+    if (m->has_overlap) {
+        m->S.resize(nn * nr);
+        std::memcpy(m->S.data(), desc->overlap_r, sizeof(double2) * nn * nr);
+    }
     m->has_position = desc->position_r != nullptr;
     if (m->has_position) {
         m->A.resize(nn * 3 * nr);
@@ -532,7 +544,7 @@ wnlqg_status wnlqg_b200_plan_destroy(wnlqg_plan *pl) {
     for (void *ptr : {(void *)pl->d_tiles, (void *)pl->d_phase, (void *)pl->d_xw, (void *)pl->d_U, (void *)pl->d_out,
                       (void *)pl->d_points, (void *)pl->d_E, (void *)pl->d_kpts, (void *)pl->d_omegas,
                       (void *)pl->d_partials, (void *)pl->d_weights, (void *)pl->d_groups, (void *)pl->d_stageY,
-                      (void *)pl->d_stageZ, (void *)pl->d_V32, (void *)pl->d_kidx, (void *)pl->d_mus})
+                      (void *)pl->d_stageZ, (void *)pl->d_V32, (void *)pl->d_kidx, (void *)pl->d_mus, (void *)pl->d_status})
         if (ptr) cudaFree(ptr);
     for (cudaEvent_t ev : pl->events) cudaEventDestroy(ev);
     if (pl->stream) cudaStreamDestroy(pl->stream);
@@ -654,6 +666,11 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
         }
     }
     pl->vc = vc;
+    if (model->has_overlap) {
+        // Nonorthogonal model: the spectrum uses S(k); the response kernels are orthogonal-only.
+        pl->nonorth = true;
+        pl->ch_S = add_channel(ch, CH_S, 0, 0);
+    }
     pl->C = (int)ch.size();
 
     // Real-space tiles T[R][c][i + nw j] (prepare_hamiltonian_real_space!,
@@ -683,6 +700,9 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
                     break;
                 case CH_DA:
                     if (model->has_position) v = cmuli(cscale(model->A[((size_t)r * 3 + cc.p) * nn + e], rc[cc.d]));
+                    break;
+                case CH_S:
+                    v = model->S[(size_t)r * nn + e];
                     break;
                 }
                 dst[e] = v;
@@ -724,6 +744,7 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
     if ((st = alloc((void **)&pl->d_kpts, (size_t)max_batch * 3 * sizeof(double))) != WNLQG_OK) return bail(st);
     if ((st = alloc((void **)&pl->d_weights, (size_t)max_batch * sizeof(double))) != WNLQG_OK) return bail(st);
     if ((st = alloc((void **)&pl->d_kidx, (size_t)max_batch * sizeof(int64_t))) != WNLQG_OK) return bail(st);
+    if ((st = alloc((void **)&pl->d_status, (size_t)max_batch * sizeof(int))) != WNLQG_OK) return bail(st);
     if ((st = alloc((void **)&pl->d_points, (size_t)max_batch * vc * sizeof(double2))) != WNLQG_OK) return bail(st);
     if ((st = alloc((void **)&pl->d_out, (size_t)vc * sizeof(double2))) != WNLQG_OK) return bail(st);
     if ((st = alloc((void **)&pl->d_omegas, std::max<size_t>(1, pl->omegas.size()) * sizeof(double))) != WNLQG_OK) return bail(st);
@@ -784,7 +805,12 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
     }
 
     pl->eigh_threads = eigh_block_threads(nw);
-    if (t.precision == WNLQG_PRECISION_MIXED) {
+    if (pl->nonorth) {
+        pl->eigh_threads = std::max(pl->eigh_threads, ((nw + (nw & 1)) / 2 + 31) / 32 * 32);
+        cudaError_t e = cudaFuncSetAttribute(generalized_eigh_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)std::max<size_t>(GenEighSmem::bytes(nw), 48 * 1024));
+        if (e != cudaSuccess) return bail(fail(WNLQG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e)));
+    } else if (t.precision == WNLQG_PRECISION_MIXED) {
         const int np = nw + (nw & 1);
         pl->eigh_smem = EighF32Smem::bytes(nw);
         pl->refine_smem = EighRefineSmem::bytes(nw);
@@ -818,6 +844,7 @@ wnlqg_status wnlqg_b200_eval_mesh_device(wnlqg_plan *pl, const int64_t mesh[3], 
                                          double *out_device, void *stream) {
     wnlqg_status st = check_plan(pl);
     if (st != WNLQG_OK) return st;
+    if (pl->nonorth) return fail(WNLQG_ERR_UNSUPPORTED, "responses of nonorthogonal models are not built yet; eval_spectrum is");
     if (!mesh || !out_device) return fail(WNLQG_ERR_INVALID_ARGUMENT, "NULL argument");
     if (mesh[0] <= 0 || mesh[1] <= 0 || mesh[2] <= 0) return fail(WNLQG_ERR_INVALID_ARGUMENT, "mesh counts must be positive");
     const int64_t nk = mesh[0] * mesh[1] * mesh[2];
@@ -884,6 +911,7 @@ wnlqg_status wnlqg_b200_eval_mesh(wnlqg_plan *pl, const int64_t mesh[3], int64_t
 wnlqg_status wnlqg_b200_eval_points(wnlqg_plan *pl, const double *kpoints, int64_t n, double *out) {
     wnlqg_status st = check_plan(pl);
     if (st != WNLQG_OK) return st;
+    if (pl->nonorth) return fail(WNLQG_ERR_UNSUPPORTED, "responses of nonorthogonal models are not built yet; eval_spectrum is");
     if (n < 0 || (n > 0 && (!kpoints || !out))) return fail(WNLQG_ERR_INVALID_ARGUMENT, "invalid points");
     if (!finite_array(kpoints, 3 * (size_t)n)) return fail(WNLQG_ERR_NONFINITE, "k-points must be finite");
     WNLQG_CUDA(cudaSetDevice(pl->model->device));
@@ -908,6 +936,7 @@ wnlqg_status wnlqg_b200_eval_points_weighted(wnlqg_plan *pl, const double *kpoin
                                              int64_t n, double *out) {
     wnlqg_status st = check_plan(pl);
     if (st != WNLQG_OK) return st;
+    if (pl->nonorth) return fail(WNLQG_ERR_UNSUPPORTED, "responses of nonorthogonal models are not built yet; eval_spectrum is");
     if (n < 0 || (n > 0 && (!kpoints || !weights)) || !out) return fail(WNLQG_ERR_INVALID_ARGUMENT, "invalid points");
     if (!finite_array(kpoints, 3 * (size_t)n) || !finite_array(weights, (size_t)n))
         return fail(WNLQG_ERR_NONFINITE, "k-points and weights must be finite");
@@ -939,6 +968,7 @@ wnlqg_status wnlqg_b200_eval_mesh_weighted(wnlqg_plan *pl, const int64_t mesh[3]
                                            const double *weights, int64_t n, double *out) {
     wnlqg_status st = check_plan(pl);
     if (st != WNLQG_OK) return st;
+    if (pl->nonorth) return fail(WNLQG_ERR_UNSUPPORTED, "responses of nonorthogonal models are not built yet; eval_spectrum is");
     if (!mesh || !out || n < 0 || (n > 0 && (!indices || !weights))) return fail(WNLQG_ERR_INVALID_ARGUMENT, "invalid arguments");
     if (mesh[0] <= 0 || mesh[1] <= 0 || mesh[2] <= 0) return fail(WNLQG_ERR_INVALID_ARGUMENT, "mesh counts must be positive");
     const int64_t nk = mesh[0] * mesh[1] * mesh[2];
@@ -983,11 +1013,15 @@ wnlqg_status wnlqg_b200_eval_spectrum(wnlqg_plan *pl, const double *kpoints, int
     if (n < 0 || (n > 0 && (!kpoints || !energies))) return fail(WNLQG_ERR_INVALID_ARGUMENT, "invalid points");
     if (!finite_array(kpoints, 3 * (size_t)n)) return fail(WNLQG_ERR_NONFINITE, "k-points must be finite");
     WNLQG_CUDA(cudaSetDevice(pl->model->device));
+    std::vector<int> stat(pl->nonorth ? (size_t)n : 0);
     for (int64_t s = 0; s < n; s += pl->max_batch) {
         int64_t nb = std::min(pl->max_batch, n - s);
         WNLQG_CUDA(cudaMemcpyAsync(pl->d_kpts, kpoints + 3 * s, (size_t)nb * 3 * sizeof(double), cudaMemcpyHostToDevice,
                                    pl->stream));
         if ((st = run_front(pl, nb, 0, nullptr, pl->d_kpts, 1)) != WNLQG_OK) return st;
+        if (pl->nonorth)
+            WNLQG_CUDA(cudaMemcpyAsync(stat.data() + s, pl->d_status, (size_t)nb * sizeof(int), cudaMemcpyDeviceToHost,
+                                       pl->stream));
         WNLQG_CUDA(cudaMemcpyAsync(energies + s * pl->nw, pl->d_E, (size_t)nb * pl->nw * sizeof(double),
                                    cudaMemcpyDeviceToHost, pl->stream));
         if (eigenvectors)
@@ -996,6 +1030,9 @@ wnlqg_status wnlqg_b200_eval_spectrum(wnlqg_plan *pl, const double *kpoints, int
     }
     WNLQG_CUDA(cudaStreamSynchronize(pl->stream));
     pl->timing_valid = false;
+    if (pl->nonorth)
+        for (int v : stat)
+            if (v) return fail(WNLQG_ERR_INVALID_ARGUMENT, "effective S(k) is not positive definite");
     return WNLQG_OK;
 }
 
