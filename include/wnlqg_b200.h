@@ -55,6 +55,7 @@ typedef enum wnlqg_response_kind {
     WNLQG_QUANTUM_METRIC = 4,     /* band-sum internal g^{ab}, ConventionalQuantumGeometry.jl:321-355 */
     WNLQG_INTRINSIC_AHC = 5,      /* sigma^{ab} Fermi sea over the mu axis, IntrinsicHallOccupations.jl */
     WNLQG_BERRY_DIPOLE = 6,       /* D^{abc} Fermi surface over the mu axis, BerryMultipoleMoments.jl */
+    WNLQG_SECOND_HARMONIC = 7,    /* seven-term chi/sigma^{abc}(omega; 2 omega), SecondHarmonicKernels.jl */
     WNLQG_JERK_CURRENT = 8        /* ordered jerk (abcd)(omega), ConventionalJerkCurrent.jl */
 } wnlqg_response_kind;
 
@@ -108,6 +109,9 @@ typedef struct wnlqg_task_desc {
     const double *fermi_energies;      /* eV */
     int32_t precision;                 /* wnlqg_precision */
     double fermi_surface_broadening;   /* eV; Gaussian width of -f' at T = 0 (Berry dipole) */
+    double shg_low_frequency_broadening;    /* eV; second harmonic low-frequency width (reference 0.025) */
+    double shg_intermediate_regularization; /* eV; second harmonic eta; 0 selects denominator_regularization */
+    int32_t shg_eta_correction;             /* second harmonic: 1 adds the finite-eta C numerator (reference true) */
 } wnlqg_task_desc;
 
 typedef struct wnlqg_model wnlqg_model;   /* device-resident model */
@@ -138,6 +142,8 @@ WNLQG_API wnlqg_status wnlqg_b200_plan_destroy(wnlqg_plan *plan);
 
 /* Number of complex values one k-point contributes (all responses concatenated).
  * Per response: shift/injection/jerk [num_photon_energies x num_components],
+ * second harmonic [num_photon_energies x num_components x 7 terms x 2 quantities] (the reference's
+ * raw per-k (frequency, component, term, quantity) array of SecondHarmonicDriver.jl:146-171),
  * curvature/metric [num_components], AHC/dipole [num_fermi_energies x num_components];
  * the energy axis is fastest. */
 WNLQG_API int64_t wnlqg_b200_plan_value_count(const wnlqg_plan *plan);

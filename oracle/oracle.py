@@ -47,8 +47,13 @@ def lib():
         L.oracle_jerk_algebra.argtypes = [ctypes.c_int64, dp, dp, dp, dp, ctypes.c_int64, dp, ctypes.c_double,
                                           ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                           ctypes.c_double, ctypes.c_int64, ctypes.POINTER(ctypes.c_int32), dp]
+        L.oracle_kpoint_data.argtypes = [ctypes.POINTER(_abi.ModelDesc), dp, dp, dp, dp, dp, dp]
+        L.oracle_shg_algebra.argtypes = [ctypes.c_int64, dp, dp, dp, dp, dp, ctypes.c_int64, dp, ctypes.c_int64,
+                                         ctypes.POINTER(ctypes.c_int32), ctypes.c_double, ctypes.c_double,
+                                         ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                         ctypes.c_int, ctypes.c_double, dp]
         for name in ("oracle_point_values", "oracle_integrate_mesh", "oracle_kpoint_spectrum",
-                     "oracle_hermitian_eigen", "oracle_jerk_algebra"):
+                     "oracle_hermitian_eigen", "oracle_jerk_algebra", "oracle_kpoint_data", "oracle_shg_algebra"):
             getattr(L, name).restype = ctypes.c_int
         _lib = L
     return _lib
@@ -136,4 +141,36 @@ def jerk_algebra(energies, B, A, C, omegas, components, *, mu=0.0, T=0.0, width=
     _check(lib().oracle_jerk_algebra(n, _dp(e), _dp(Bf), _dp(Af), _dp(Cf), om.size, _dp(om), mu, T, width,
                                      1 if gaussian else 0, reg, window, len(components),
                                      comps.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), _dp(out)))
+    return out
+
+
+def kpoint_data(model: TightBindingModel, k):
+    """Hamiltonian-gauge band data at one k: energies[nw], dH[nw,nw,3], A[nw,nw,3],
+    dA[nw,nw,3,3] (position axis, derivative axis) and ddH[nw,nw,3,3]."""
+    nw = model.num_orbitals
+    m = _abi.ModelArrays(model)
+    kk = np.ascontiguousarray(np.asarray(k, dtype=np.float64))
+    e = np.zeros(nw)
+    dh = np.zeros((nw, nw, 3), dtype=np.complex128, order="F")
+    a = np.zeros((nw, nw, 3), dtype=np.complex128, order="F")
+    da = np.zeros((nw, nw, 3, 3), dtype=np.complex128, order="F")
+    ddh = np.zeros((nw, nw, 3, 3), dtype=np.complex128, order="F")
+    _check(lib().oracle_kpoint_data(ctypes.byref(m.desc), _dp(kk), _dp(e), _dp(dh), _dp(a), _dp(da), _dp(ddh)))
+    return e, dh, a, da, ddh
+
+
+def shg_algebra(energies, V, A, dA, W, omegas, components, *, mu=0.0, T=0.0, broadening=0.025,
+                low_frequency_broadening=0.025, gaussian=True, eta=0.04, eta_correction=True,
+                degeneracy=0.002) -> np.ndarray:
+    """Seven-term SHG on prepared Hamiltonian-gauge inputs: complex [n_omega, n_components, 7, 2]."""
+    e = np.ascontiguousarray(np.asarray(energies, dtype=np.float64))
+    n = e.size
+    arrs = [np.asfortranarray(x, dtype=np.complex128) for x in (V, A, dA, W)]
+    om = np.ascontiguousarray(np.asarray(omegas, dtype=np.float64))
+    comps = np.ascontiguousarray(np.array([_abi._axes(c) for c in components], dtype=np.int32))
+    out = np.zeros((om.size, len(components), 7, 2), dtype=np.complex128, order="F")
+    _check(lib().oracle_shg_algebra(n, _dp(e), *[_dp(x) for x in arrs], om.size, _dp(om), len(components),
+                                    comps.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), mu, T, broadening,
+                                    low_frequency_broadening, 1 if gaussian else 0, eta,
+                                    1 if eta_correction else 0, degeneracy, _dp(out)))
     return out

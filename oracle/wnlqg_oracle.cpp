@@ -25,6 +25,9 @@
 //   Berry-curvature dipole      src/Responses/QuantumGeometry/BerryMultipoleMoments.jl:7-47,
 //                               BerryMultipoleGeometry.jl:66-161, BerryMultipoleDC.jl:64-75;
 //                               Responses/Shared/ResponseOccupations.jl:10-36
+//   second harmonic             src/Responses/SecondHarmonicGeneration/SecondHarmonicKernels.jl:1-294;
+//                               MatrixElements/Interpolated/OpticalPositionDerivatives.jl:13-123,
+//                               PositionVertexRegularization.jl:7-50
 //   jerk                        src/Responses/JerkCurrent/ConventionalJerkCurrent.jl:14-65;
 //                               MatrixElements/Interpolated/ThirdOrderGeometry.jl:28-41, 131-160
 //   mesh + lanes                src/Core/CalculationUtils.jl:280-292; Runtime/Setup/BundleAssembly.jl:35-53;
@@ -513,6 +516,12 @@ bool build_task(const wnlqg_task_desc *t, Task &task) {
                 task.need.F[a][b] = true; task.need.need_r(a); task.need.need_r(b);
                 if (q.kind == WNLQG_BERRY_DIPOLE) task.need.dH[cc] = true;
                 break;
+            case WNLQG_SECOND_HARMONIC:
+                for (int x = 0; x < 3; ++x) {
+                    task.need.dH[x] = true; task.need.A[x] = true;
+                    for (int y = 0; y < 3; ++y) { task.need.dA[x][y] = true; task.need.ddH[x][y] = true; }
+                }
+                break;
             case WNLQG_JERK_CURRENT:
                 task.need.need_r(b); task.need.need_r(cc);
                 task.need.dH[a] = true; task.need.dH[dd] = true;
@@ -524,6 +533,21 @@ bool build_task(const wnlqg_task_desc *t, Task &task) {
         }
         if (q.kind == WNLQG_SHIFT_CURRENT || q.kind == WNLQG_INJECTION_CURRENT || q.kind == WNLQG_JERK_CURRENT)
             count += q.num_components * t->num_photon_energies;
+        else if (q.kind == WNLQG_SECOND_HARMONIC) {
+            // second_harmonic_response! argument checks (SecondHarmonicKernels.jl:129-138).
+            const double eta = t->shg_intermediate_regularization > 0 ? t->shg_intermediate_regularization
+                                                                      : t->denominator_regularization;
+            if (!(std::isfinite(t->shg_low_frequency_broadening) && t->shg_low_frequency_broadening > 0 &&
+                  std::isfinite(eta) && eta > 0)) {
+                set_error("SHG optical widths and intermediate_regularization must be finite and positive in eV");
+                return false;
+            }
+            if (!(std::isfinite(t->degeneracy_threshold) && t->degeneracy_threshold >= 0)) {
+                set_error("SHG degeneracy_threshold must be finite and nonnegative in eV");
+                return false;
+            }
+            count += q.num_components * t->num_photon_energies * 14;
+        }
         else if (q.kind == WNLQG_INTRINSIC_AHC || q.kind == WNLQG_BERRY_DIPOLE) {
             if (t->num_fermi_energies < 1) { set_error("a Fermi-energy axis is required"); return false; }
             if (q.kind == WNLQG_BERRY_DIPOLE && t->temperature == 0.0 && !(t->fermi_surface_broadening > 0)) {
@@ -592,6 +616,202 @@ void jerk_response(int n, const double *E, const cd *B, const cd *A, const cd *C
                 }
             }
         }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Second-harmonic generation (src/Responses/SecondHarmonicGeneration/SecondHarmonicKernels.jl).
+// Inputs are prepared Hamiltonian-gauge band data at one k, all [n,n,...] column-major:
+// V = dH (velocity, [n,n,3]), A = internal connection ([n,n,3]), dA = connection derivatives
+// ([n,n,3,3], position axis then derivative axis), W = second Hamiltonian derivatives ([n,n,3,3]).
+// out[w + nom*(c + nc*(term + 7*q))] for term 0..6 (SECOND_HARMONIC_TERMS order) and quantity q
+// (0 = susceptibility, 1 = conductivity, both before their physical prefactors).
+
+// bare_energy_inverse (PositionVertexRegularization.jl:7-8): zero strictly below 1e-7 eV.
+double bare_inverse(double d) { return std::fabs(d) < 1.0e-7 ? 0.0 : 1.0 / d; }
+
+// regularized_energy_weight (PositionVertexRegularization.jl:37-50): eta^2/(d^2+eta^2).
+double regularized_weight(double d, double eta) {
+    double w2 = eta * eta, den = d * d + w2;
+    if (std::isfinite(den) && den != 0.0 && w2 != 0.0) return w2 / den;
+    if (!(std::isfinite(d) && std::isfinite(eta) && eta > 0)) return w2 / den;
+    double scale = std::max(std::fabs(d), eta), sd = d / scale, sw = eta / scale;
+    return sw * sw / (sd * sd + sw * sw);
+}
+
+// second_harmonic_delta / _principal / _resonance (SecondHarmonicKernels.jl:86-98).
+double shg_delta(double e, double width, bool gaussian) {
+    double x = e / width;
+    return gaussian ? std::exp(-x * x) / (std::sqrt(PI) * width) : 1.0 / (PI * width * (1 + x * x));
+}
+double shg_principal(double e, double width) { return e / (e * e + width * width); }
+cd shg_resonance(double e, double width, bool gaussian) {
+    return cd(shg_principal(e, width), PI * shg_delta(e, width, gaussian));
+}
+
+// second_harmonic_occupation (SecondHarmonicKernels.jl:101-105).
+double shg_occupation(double e, double mu, double T) {
+    if (T <= 1.0e-7) return e <= mu ? 1.0 : 0.0;
+    double x = (e - mu) / (RESPONSE_KB_EV * T);
+    return x >= 0 ? std::exp(-x) / (1 + std::exp(-x)) : 1.0 / (1 + std::exp(x));
+}
+
+struct ShgParams {
+    double mu, T, width, low_width, eta, degeneracy;
+    bool gaussian, eta_correction;
+};
+
+void shg_response(int n, const double *E, const cd *V, const cd *A, const cd *dA, const cd *W, int64_t nom,
+                  const double *om, int nc, const int32_t (*comps)[4], const ShgParams &p, cd *out) {
+    auto v3 = [&](int i, int j, int a) { return V[i + n * (j + n * a)]; };
+    auto a3 = [&](int i, int j, int a) { return A[i + n * (j + n * a)]; };
+    auto da4 = [&](int i, int j, int a, int b) { return dA[i + n * (j + n * (a + 3 * b))]; };
+    auto w4 = [&](int i, int j, int a, int b) { return W[i + n * (j + n * (a + 3 * b))]; };
+    const size_t nn = (size_t)n * n;
+    for (int64_t e = 0; e < nom * nc * 14; ++e) out[e] = 0.0;
+    std::vector<double> occ(n);
+    for (int i = 0; i < n; ++i) occ[i] = shg_occupation(E[i], p.mu, p.T);
+    std::vector<char> active(nn, 0);
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i) active[i + n * j] = i != j && std::fabs(occ[i] - occ[j]) >= 1.0e-10;
+    // optical_position_vertices! (OpticalPositionDerivatives.jl:13-91): bare D0, regularised
+    // D_eta, r0 = A + i D0, r_eta = A + i D_eta and the cutoff derivative G for active pairs.
+    std::vector<cd> D0(nn * 3), Dr(nn * 3), r0(nn * 3), re(nn * 3), G(nn * 9, cd(0.0, 0.0));
+    for (int a = 0; a < 3; ++a)
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) {
+                size_t e = i + n * (j + (size_t)n * a);
+                double inv = bare_inverse(E[j] - E[i]);
+                D0[e] = inv == 0.0 ? cd(0.0, 0.0) : V[e] * inv;
+                Dr[e] = V[e] * regularized_inverse(E[j] - E[i], p.eta);
+                r0[e] = A[e] + I1 * D0[e];
+                re[e] = A[e] + I1 * Dr[e];
+            }
+    auto d0 = [&](int i, int j, int a) { return D0[i + n * (j + n * a)]; };
+    auto dr = [&](int i, int j, int a) { return Dr[i + n * (j + n * a)]; };
+    auto dip = [&](int i, int j, int a) { return r0[i + n * (j + n * a)]; };
+    auto rdip = [&](int i, int j, int a) { return re[i + n * (j + n * a)]; };
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b)
+            for (int m = 0; m < n; ++m)
+                for (int i = 0; i < n; ++i) {
+                    if (!active[i + n * m]) continue;
+                    cd comA(0.0, 0.0), comH(0.0, 0.0);
+                    for (int l = 0; l < n; ++l) {
+                        comA += a3(i, l, a) * dr(l, m, b) - dr(i, l, b) * a3(l, m, a);
+                        comH += v3(i, l, a) * dr(l, m, b) - dr(i, l, b) * v3(l, m, a);
+                    }
+                    cd sum_a = comA - (a3(i, i, a) - a3(m, m, a)) * dr(i, m, b);
+                    cd sum_h = comH - (v3(i, i, a) - v3(m, m, a)) * dr(i, m, b);
+                    cd finite = da4(i, m, a, b) + sum_a + (a3(i, i, a) - a3(m, m, a)) * d0(i, m, b) +
+                                (a3(i, i, b) - a3(m, m, b)) * d0(i, m, a) -
+                                I1 * a3(i, m, a) * (a3(i, i, b) - a3(m, m, b));
+                    cd numerator = I1 * (w4(i, m, a, b) + sum_h +
+                                         d0(i, m, a) * (v3(i, i, b) - v3(m, m, b)).real() +
+                                         d0(i, m, b) * (v3(i, i, a) - v3(m, m, a)).real());
+                    if (p.eta_correction)
+                        for (int q = 0; q < n; ++q) {
+                            if (q == i || q == m) continue;
+                            numerator += regularized_weight(E[q] - E[m], p.eta) *
+                                         (a3(i, q, a) * v3(q, m, b) -
+                                          (v3(i, q, a) + I1 * (E[i] - E[q]) * a3(i, q, a)) * a3(q, m, b));
+                            numerator -= regularized_weight(E[i] - E[q], p.eta) *
+                                         (v3(i, q, b) * a3(q, m, a) -
+                                          a3(i, q, b) * (v3(q, m, a) + I1 * (E[q] - E[m]) * a3(q, m, a)));
+                        }
+                    double inv = bare_inverse(E[m] - E[i]);
+                    G[i + n * (m + n * (a + 3 * (size_t)b))] = inv == 0.0 ? finite : finite + inv * numerator;
+                }
+    auto g4 = [&](int i, int j, int a, int b) { return G[i + n * (j + n * (a + 3 * b))]; };
+    auto o = [&](int64_t w, int c, int term, int q) -> cd & { return out[w + nom * (c + nc * (term + 7 * q))]; };
+    // Pair terms (SecondHarmonicKernels.jl:149-220).
+    for (int i = 0; i < n; ++i)
+        for (int m = 0; m < n; ++m) {
+            if (i == m) continue;
+            const double fo = occ[i] - occ[m];
+            if (std::fabs(fo) < 1.0e-10) continue;
+            const double diff = E[m] - E[i];
+            const double inv = bare_inverse(diff);
+            for (int c = 0; c < nc; ++c) {
+                const int a = comps[c][0], b = comps[c][1], cc = comps[c][2];
+                cd first = dip(i, m, a) * (g4(m, i, b, cc) + g4(m, i, cc, b));
+                cd second = g4(i, m, a, b) * dip(m, i, cc) + g4(i, m, a, cc) * dip(m, i, b);
+                cd third = dip(i, m, a) *
+                           (dip(m, i, b) * (v3(m, m, cc) - v3(i, i, cc)).real() +
+                            dip(m, i, cc) * (v3(m, m, b) - v3(i, i, b)).real()) * inv;
+                cd fourth = g4(i, m, b, a) * dip(m, i, cc) + g4(i, m, cc, a) * dip(m, i, b);
+                cd fifth = (v3(i, i, a) - v3(m, m, a)).real() *
+                           (dip(i, m, b) * dip(m, i, cc) + dip(i, m, cc) * dip(m, i, b));
+                cd tfirst(0.0, 0.0), tother(0.0, 0.0);
+                for (int q = 0; q < n; ++q) {
+                    if (q == i || q == m) continue;
+                    tfirst += dip(i, m, a) * (rdip(m, q, b) * rdip(q, i, cc) + rdip(m, q, cc) * rdip(q, i, b)) *
+                              shg_principal(2 * E[q] - E[i] - E[m], p.eta);
+                    tother += rdip(m, q, a) * (rdip(q, i, b) * dip(i, m, cc) + rdip(q, i, cc) * dip(i, m, b)) *
+                              shg_principal(2 * E[i] - E[m] - E[q], p.eta);
+                    tother += rdip(q, i, a) * (dip(i, m, b) * rdip(m, q, cc) + dip(i, m, cc) * rdip(m, q, b)) *
+                              shg_principal(2 * E[m] - E[q] - E[i], p.eta);
+                }
+                for (int64_t w = 0; w < nom; ++w) {
+                    const double energy = om[w];
+                    cd d1 = shg_resonance(diff - energy, p.width, p.gaussian);
+                    cd d2 = shg_resonance(diff - 2 * energy, p.width, p.gaussian);
+                    cd dn = shg_resonance(-diff - energy, p.width, p.gaussian);
+                    double low = shg_principal(energy, p.low_width);
+                    cd factor = 0.5 * I1 * fo;
+                    o(w, c, 0, 0) += factor * inv * (2.0 * first * d2 + second * d1 + (first + second) * low);
+                    o(w, c, 1, 0) += factor * inv * third * (d1 - 4.0 * d2 - low);
+                    o(w, c, 2, 0) += 0.5 * fo * (2.0 * tfirst * d2 + tother * dn);
+                    o(w, c, 3, 0) -= factor * inv * 0.5 * fourth * (d1 + low);
+                    o(w, c, 4, 0) -= factor * 0.25 * fifth * d1 * (low * low);
+                    o(w, c, 0, 1) += fo * (first * d2 + second * d1);
+                    o(w, c, 1, 1) += fo * third * (d1 - 2.0 * d2);
+                    o(w, c, 2, 1) -= I1 * fo * diff * (tfirst * d2 - tother * dn);
+                    o(w, c, 3, 1) -= fo * 0.5 * fourth * d1;
+                    o(w, c, 4, 1) -= fo * 0.25 * fifth * d1 * low;
+                }
+            }
+        }
+    if (p.T <= 1.0e-7) return;
+    // One-band terms (second_harmonic_one_band!, SecondHarmonicKernels.jl:245-294).
+    const double kt = RESPONSE_KB_EV * p.T;
+    for (int i = 0; i < n; ++i) {
+        const double offset = E[i] - p.mu;
+        if (std::fabs(offset) > 5 * kt) continue;
+        const double fd = -std::exp(-0.5 * (offset / kt) * (offset / kt)) / (kt * std::sqrt(2 * PI));
+        const double sd = -offset / (kt * kt) * fd;
+        // _second_harmonic_bcd_enabled: a singleton of the adjacent-gap partition.
+        const bool isolated = (i == 0 || E[i] - E[i - 1] > p.degeneracy) && (i == n - 1 || E[i + 1] - E[i] > p.degeneracy);
+        double curv[3][3] = {};
+        if (isolated)
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) {
+                    if (a == b) continue;
+                    cd value = da4(i, i, b, a) - da4(i, i, a, b);
+                    for (int q = 0; q < n; ++q)
+                        value += a3(i, q, b) * d0(q, i, a) - d0(i, q, a) * a3(q, i, b) - a3(i, q, a) * d0(q, i, b) +
+                                 d0(i, q, b) * a3(q, i, a) - I1 * (d0(i, q, a) * d0(q, i, b) - d0(i, q, b) * d0(q, i, a));
+                    curv[a][b] = value.real();
+                }
+        for (int c = 0; c < nc; ++c) {
+            const int a = comps[c][0], b = comps[c][1], cc = comps[c][2];
+            double hess = w4(i, i, b, cc).real();
+            for (int q = 0; q < n; ++q) {
+                if (q == i) continue;
+                hess += 2.0 * (v3(i, q, b) * v3(q, i, cc)).real() * shg_principal(E[i] - E[q], p.eta);
+            }
+            const double va = v3(i, i, a).real(), vb = v3(i, i, b).real(), vc = v3(i, i, cc).real();
+            const double semi = sd * va * vb * vc + fd * va * hess;
+            const double bcd = isolated ? fd * (vb * curv[a][cc] + vc * curv[a][b]) : 0.0;
+            for (int64_t w = 0; w < nom; ++w) {
+                const double low = shg_principal(om[w], p.low_width);
+                const cd kernel = low - I1 * shg_delta(om[w], p.low_width, p.gaussian);
+                o(w, c, 5, 0) -= 0.25 * bcd * kernel * low;
+                o(w, c, 5, 1) += 0.5 * I1 * bcd * kernel;
+                o(w, c, 6, 0) -= 0.25 * I1 * semi * kernel * (low * low);
+                o(w, c, 6, 1) -= 0.5 * semi * kernel * low;
+            }
+        }
+    }
 }
 
 // One k-point's concatenated response values (point_value!, IntegralDriver.jl:596-...), with
@@ -746,6 +966,27 @@ void point_values(const Model &m, const Task &task, const double k[3], cd *out) 
                 }
             }
             o += nmu * nc;
+        } else if (q.kind == WNLQG_SECOND_HARMONIC) {
+            const size_t nn = (size_t)n * n;
+            std::vector<cd> V(nn * 3), A(nn * 3), dA(nn * 9), W(nn * 9);
+            for (int a = 0; a < 3; ++a) {
+                for (size_t e = 0; e < nn; ++e) { V[e + nn * a] = d.dH[a].v[e]; A[e + nn * a] = d.Aint[a].v[e]; }
+                for (int b = 0; b < 3; ++b)
+                    for (size_t e = 0; e < nn; ++e) {
+                        dA[e + nn * (a + 3 * b)] = d.dA[a][b].v[e];
+                        W[e + nn * (a + 3 * b)] = d.ddH[a][b].v[e];
+                    }
+            }
+            ShgParams p;
+            p.mu = t.fermi_energy; p.T = t.temperature; p.width = t.broadening;
+            p.low_width = t.shg_low_frequency_broadening;
+            p.eta = t.shg_intermediate_regularization > 0 ? t.shg_intermediate_regularization : t.denominator_regularization;
+            p.degeneracy = t.degeneracy_threshold;
+            p.gaussian = t.broadening_type == WNLQG_GAUSSIAN;
+            p.eta_correction = t.shg_eta_correction != 0;
+            shg_response(n, d.E.data(), V.data(), A.data(), dA.data(), W.data(), nom, t.photon_energies, nc,
+                         q.components, p, o);
+            o += nom * nc * 14;
         } else if (q.kind == WNLQG_JERK_CURRENT) {
             std::vector<cd> B((size_t)n * n * 3, 0.0), A((size_t)n * n * 3, 0.0), C((size_t)n * n * 9, 0.0);
             for (int a = 0; a < 3; ++a) {
@@ -936,6 +1177,64 @@ int oracle_jerk_algebra(int64_t n, const double *E, const double *B, const doubl
     for (size_t e = 0; e < c.size(); ++e) c[e] = cd(C[2 * e], C[2 * e + 1]);
     jerk_response((int)n, E, b.data(), a.data(), c.data(), nom, omegas, mu, T, width, gaussian != 0, reg, window,
                   (int)ncomp, reinterpret_cast<const int32_t(*)[4]>(comps), o.data());
+    for (size_t e = 0; e < o.size(); ++e) { out[2 * e] = o[e].real(); out[2 * e + 1] = o[e].imag(); }
+    return WNLQG_OK;
+}
+
+// Hamiltonian-gauge band data at one k for tests: energies[nw]; dH, A [nw,nw,3]; dA, ddH
+// [nw,nw,3,3] (dA: position axis, then derivative axis), all complex column-major.
+int oracle_kpoint_data(const wnlqg_model_desc *md, const double k[3], double *energies, double *dh, double *a,
+                       double *da, double *ddh) {
+    Model m;
+    if (!build_model(md, m)) return WNLQG_ERR_INVALID_ARGUMENT;
+    if (m.has_overlap) { set_error("orthogonal models only"); return WNLQG_ERR_UNSUPPORTED; }
+    Needs need;
+    for (int x = 0; x < 3; ++x) {
+        need.dH[x] = need.A[x] = true;
+        for (int y = 0; y < 3; ++y) need.dA[x][y] = need.ddH[x][y] = true;
+    }
+    KData d;
+    compute_kpoint(m, need, k, 0.001, d);
+    const size_t nn = (size_t)m.nw * m.nw;
+    for (int i = 0; i < m.nw; ++i) energies[i] = d.E[i];
+    auto put = [](double *dst, size_t off, const Mat &x, size_t nn_) {
+        for (size_t e = 0; e < nn_; ++e) { dst[2 * (off + e)] = x.v[e].real(); dst[2 * (off + e) + 1] = x.v[e].imag(); }
+    };
+    for (int x = 0; x < 3; ++x) {
+        put(dh, nn * x, d.dH[x], nn);
+        put(a, nn * x, d.Aint[x], nn);
+        for (int y = 0; y < 3; ++y) { put(da, nn * (x + 3 * y), d.dA[x][y], nn); put(ddh, nn * (x + 3 * y), d.ddH[x][y], nn); }
+    }
+    return WNLQG_OK;
+}
+
+// Seven-term SHG on prepared Hamiltonian-gauge inputs (the reference's unit-test form):
+// out complex [nom, ncomp, 7, 2].
+int oracle_shg_algebra(int64_t n, const double *E, const double *V, const double *A, const double *dA,
+                       const double *W, int64_t nom, const double *omegas, int64_t ncomp, const int32_t *comps,
+                       double mu, double T, double width, double low_width, int gaussian, double eta,
+                       int eta_correction, double degeneracy, double *out) {
+    if (!(std::isfinite(width) && width > 0 && std::isfinite(low_width) && low_width > 0 && std::isfinite(eta) && eta > 0)) {
+        set_error("SHG optical widths and intermediate_regularization must be finite and positive in eV");
+        return WNLQG_ERR_INVALID_ARGUMENT;
+    }
+    if (!(std::isfinite(degeneracy) && degeneracy >= 0)) {
+        set_error("SHG degeneracy_threshold must be finite and nonnegative in eV");
+        return WNLQG_ERR_INVALID_ARGUMENT;
+    }
+    const size_t nn = (size_t)n * n;
+    auto load = [](const double *src, size_t count) {
+        std::vector<cd> v(count);
+        for (size_t e = 0; e < count; ++e) v[e] = cd(src[2 * e], src[2 * e + 1]);
+        return v;
+    };
+    std::vector<cd> v = load(V, nn * 3), a = load(A, nn * 3), da = load(dA, nn * 9), w = load(W, nn * 9);
+    std::vector<cd> o((size_t)nom * ncomp * 14);
+    ShgParams p;
+    p.mu = mu; p.T = T; p.width = width; p.low_width = low_width; p.eta = eta; p.degeneracy = degeneracy;
+    p.gaussian = gaussian != 0; p.eta_correction = eta_correction != 0;
+    shg_response((int)n, E, v.data(), a.data(), da.data(), w.data(), nom, omegas, (int)ncomp,
+                 reinterpret_cast<const int32_t(*)[4]>(comps), p, o.data());
     for (size_t e = 0; e < o.size(); ++e) { out[2 * e] = o[e].real(); out[2 * e + 1] = o[e].imag(); }
     return WNLQG_OK;
 }

@@ -76,6 +76,64 @@ def test_jerk_golden_fixture(oracle_mod):
     assert np.max(np.abs(out.imag)) > 0.01
 
 
+SHG_COMPONENTS = [(a, b, c) for a in range(3) for (b, c) in ((0, 0), (1, 1), (2, 2), (1, 2), (0, 2), (0, 1))]
+SHG_OPTIONS = dict(mu=0.0, T=0.0, broadening=0.025, low_frequency_broadening=0.025, gaussian=True, eta=0.04,
+                   eta_correction=True, degeneracy=0.002)
+SHG_OMEGAS = [0.0, 0.1, 0.73, 1.7]
+
+
+def _shg_block(data, sel):
+    e, dh, a, da, ddh = data
+    ix = np.ix_(sel, sel)
+    return (e[sel], dh[ix + (slice(None),)], a[ix + (slice(None),)], da[ix + (slice(None), slice(None))],
+            ddh[ix + (slice(None), slice(None))])
+
+
+@pytest.mark.parametrize("bands", [2, 3, 4])
+@pytest.mark.parametrize("point", ["generic", "gamma"])
+@pytest.mark.parametrize("gaussian", [True, False])
+@pytest.mark.parametrize("correction", [True, False])
+def test_shg_golden_fixtures(oracle_mod, bands, point, gaussian, correction):
+    """The reference's 24 frozen SHG tables (test/second_harmonic_unit.jl:29-100): the 4-orbital
+    synthetic_runtime model at one generic k and at Gamma, band subsets 2:3, 1:3 and 1:4, both
+    delta kernels, with and without the finite-eta correction; the table is the sum of the seven
+    terms, flattened (frequency, component, quantity)."""
+    from wanniernlqg_b200.model import read_wannier_tb
+    model = read_wannier_tb(os.path.join(GOLDEN, "synthetic_tb.dat"))
+    k = [0.17, 0.23, 0.31] if point == "generic" else [0.0, 0.0, 0.0]
+    sel = [1, 2] if bands == 2 else list(range(bands))
+    e, V, A, dA, W = _shg_block(oracle_mod.kpoint_data(model, k), sel)
+    opts = dict(SHG_OPTIONS, gaussian=gaussian, eta_correction=correction)
+    out = oracle_mod.shg_algebra(e, V, A, dA, W, SHG_OMEGAS, SHG_COMPONENTS, **opts)
+    name = ("" if bands == 4 else f"{bands}band_") + point + "_" + ("gaussian" if gaussian else "lorentzian") + \
+        "_" + ("corrected" if correction else "uncorrected") + ".dat"
+    ref = read_complex_lines(os.path.join(GOLDEN, "second_harmonic", name)).reshape(4, 18, 2, order="F")
+    np.testing.assert_allclose(out.sum(axis=2), ref, atol=1e-10, rtol=1e-8)
+
+
+def test_shg_contract_properties(oracle_mod):
+    """Structural checks of second_harmonic_unit.jl:101-131: finite values, no one-band terms at
+    T = 0, symmetric incident indices, the 1e-7 K temperature switch, and at 300 K with mu on a
+    band both one-band terms present with a vanishing aaa Berry-curvature-dipole term."""
+    from wanniernlqg_b200.model import read_wannier_tb
+    model = read_wannier_tb(os.path.join(GOLDEN, "synthetic_tb.dat"))
+    data = oracle_mod.kpoint_data(model, [0.17, 0.23, 0.31])
+    out = oracle_mod.shg_algebra(*data, SHG_OMEGAS, SHG_COMPONENTS, **SHG_OPTIONS)
+    assert np.all(np.isfinite(out))
+    assert np.all(out[:, :, 5:7, :] == 0)
+    swapped = oracle_mod.shg_algebra(*data, SHG_OMEGAS, [(a, c, b) for a, b, c in SHG_COMPONENTS], **SHG_OPTIONS)
+    np.testing.assert_allclose(swapped, out, atol=1e-10, rtol=1e-8)
+    tiny = oracle_mod.shg_algebra(*data, SHG_OMEGAS, SHG_COMPONENTS, **dict(SHG_OPTIONS, T=1e-7))
+    assert np.array_equal(tiny, out)
+    metal = oracle_mod.shg_algebra(*data, SHG_OMEGAS, SHG_COMPONENTS, **dict(SHG_OPTIONS, T=300.0, mu=data[0][1]))
+    assert np.any(metal[:, :, 6, :] != 0) and np.any(metal[:, :, 5, :] != 0)
+    for i, (a, b, c) in enumerate(SHG_COMPONENTS):
+        if a == b == c:
+            assert np.all(metal[:, i, 5, :] == 0)
+    with pytest.raises(RuntimeError, match="finite and positive"):
+        oracle_mod.shg_algebra(*data, SHG_OMEGAS, SHG_COMPONENTS, **dict(SHG_OPTIONS, eta=0.0))
+
+
 def _sc_task(**kw):
     args = dict(broadening_type=_abi.LORENTZIAN, broadening=0.02, photon_energies=np.linspace(0, 3, 16))
     args.update(kw)

@@ -24,6 +24,7 @@ BERRY_CURVATURE = 3
 QUANTUM_METRIC = 4
 INTRINSIC_AHC = 5
 BERRY_DIPOLE = 6
+SECOND_HARMONIC = 7
 JERK_CURRENT = 8
 
 GAUSSIAN = 0
@@ -78,6 +79,9 @@ class TaskDesc(ctypes.Structure):
         ("fermi_energies", ctypes.POINTER(ctypes.c_double)),
         ("precision", ctypes.c_int32),
         ("fermi_surface_broadening", ctypes.c_double),
+        ("shg_low_frequency_broadening", ctypes.c_double),
+        ("shg_intermediate_regularization", ctypes.c_double),
+        ("shg_eta_correction", ctypes.c_int32),
     ]
 
 
@@ -129,7 +133,8 @@ class TaskArrays:
                  broadening_type=GAUSSIAN, broadening=0.040, transition_window_factor=5.0,
                  denominator_regularization=0.001, degeneracy_threshold=2.0e-3,
                  photon_energies=(0.10,), fermi_energies=(), precision=PRECISION_FP64,
-                 fermi_surface_broadening=0.0):
+                 fermi_surface_broadening=0.0, shg_low_frequency_broadening=0.025,
+                 shg_intermediate_regularization=0.0, shg_eta_correction=True):
         if not 1 <= len(responses) <= MAX_RESPONSES:
             raise ValueError("between 1 and 8 responses are supported per task")
         self.photon_energies = np.ascontiguousarray(np.asarray(photon_energies, dtype=np.float64))
@@ -161,6 +166,9 @@ class TaskArrays:
         d.fermi_energies = _dptr(self.fermi_energies) if self.fermi_energies.size else None
         d.precision = int(precision)
         d.fermi_surface_broadening = float(fermi_surface_broadening)
+        d.shg_low_frequency_broadening = float(shg_low_frequency_broadening)
+        d.shg_intermediate_regularization = float(shg_intermediate_regularization)
+        d.shg_eta_correction = 1 if shg_eta_correction else 0
         self.desc = d
 
     def value_count(self) -> int:
@@ -168,6 +176,8 @@ class TaskArrays:
         for kind, nc in self.responses:
             if kind in FREQUENCY_KINDS:
                 total += nc * self.photon_energies.size
+            elif kind == SECOND_HARMONIC:
+                total += nc * self.photon_energies.size * 14
             elif kind in FERMI_AXIS_KINDS:
                 total += nc * self.fermi_energies.size
             else:
@@ -175,10 +185,17 @@ class TaskArrays:
         return total
 
     def split(self, values: np.ndarray) -> list:
-        """Split a concatenated value vector into one (axis, component) array per response."""
+        """Split a concatenated value vector into one (axis, component) array per response;
+        second harmonic responses come out as (photon energy, component, term, quantity)."""
         out = []
         off = 0
         for kind, nc in self.responses:
+            if kind == SECOND_HARMONIC:
+                na = self.photon_energies.size
+                block = values[..., off:off + na * nc * 14].reshape(values.shape[:-1] + (2, 7, nc, na))
+                out.append(np.moveaxis(block, (-1, -2, -3, -4), (-4, -3, -2, -1)))
+                off += na * nc * 14
+                continue
             if kind in FREQUENCY_KINDS:
                 na = self.photon_energies.size
             elif kind in FERMI_AXIS_KINDS:
