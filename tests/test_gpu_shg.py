@@ -1,0 +1,131 @@
+"""Second-harmonic generation on the GPU (shg_kernel) through the C ABI.
+
+Checked three ways: directly against the reference's frozen four-band tables
+(test/second_harmonic_unit.jl; the table is the sum of the seven terms), against the CPU oracle
+term by term at arbitrary k-points (FP64: 1e-10 relative in the max norm over each term and
+quantity block), and through the mesh reduction.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, read_complex_lines
+from wanniernlqg_b200 import _abi
+from wanniernlqg_b200.model import read_wannier_tb, reference_workload_model
+
+pytestmark = pytest.mark.gpu
+RTOL = 1e-10
+MIXED_RTOL = 1e-4
+COMPONENTS = [(a, b, c) for a in range(3) for (b, c) in ((0, 0), (1, 1), (2, 2), (1, 2), (0, 2), (0, 1))]
+OMEGAS = [0.0, 0.1, 0.73, 1.7]
+
+
+def shg_task(*, gaussian=True, correction=True, T=0.0, mu=0.0, omegas=OMEGAS, components=COMPONENTS,
+             precision=_abi.PRECISION_FP64, extra=()):
+    return _abi.TaskArrays(list(extra) + [(_abi.SECOND_HARMONIC, components)],
+                           broadening_type=_abi.GAUSSIAN if gaussian else _abi.LORENTZIAN, broadening=0.025,
+                           photon_energies=omegas, fermi_energy=mu, temperature=T, degeneracy_threshold=0.002,
+                           shg_low_frequency_broadening=0.025, shg_intermediate_regularization=0.04,
+                           shg_eta_correction=correction, precision=precision)
+
+
+def block_err(got, ref):
+    """Largest relative error over the (term, quantity) blocks of [.., n_omega, nc, 7, 2] arrays."""
+    worst = 0.0
+    for t in range(7):
+        for q in range(2):
+            g, r = got[..., t, q], ref[..., t, q]
+            scale = np.max(np.abs(r))
+            err = np.max(np.abs(g - r))
+            worst = max(worst, err / scale if scale > 0 else err)
+    return worst
+
+
+@pytest.fixture(scope="module")
+def engine_cls():
+    from wanniernlqg_b200 import build
+    build.build()
+    from wanniernlqg_b200.engine import ResponseEngine
+    return ResponseEngine
+
+
+@pytest.fixture(scope="module")
+def tb4():
+    return read_wannier_tb(os.path.join(GOLDEN, "synthetic_tb.dat"))
+
+
+@pytest.mark.parametrize("gaussian", [True, False])
+@pytest.mark.parametrize("correction", [True, False])
+def test_shg_matches_reference_tables(engine_cls, tb4, gaussian, correction):
+    task = shg_task(gaussian=gaussian, correction=correction)
+    with engine_cls(tb4, task) as eng:
+        got = task.split(eng.point_values([[0.17, 0.23, 0.31], [0.0, 0.0, 0.0]]))[0]
+    for i, point in enumerate(["generic", "gamma"]):
+        name = f"{point}_{'gaussian' if gaussian else 'lorentzian'}_{'corrected' if correction else 'uncorrected'}.dat"
+        ref = read_complex_lines(os.path.join(GOLDEN, "second_harmonic", name)).reshape(4, 18, 2, order="F")
+        np.testing.assert_allclose(got[i].sum(axis=2), ref, atol=1e-10, rtol=1e-8)
+        assert np.all(got[i][:, :, 5:7, :] == 0)
+
+
+@pytest.mark.parametrize("T,mu_band", [(0.0, None), (300.0, 1)])
+@pytest.mark.parametrize("gaussian", [True, False])
+def test_shg_terms_match_oracle_nw4(engine_cls, oracle_mod, tb4, T, mu_band, gaussian):
+    rng = np.random.default_rng(21)
+    k = np.vstack([[0.17, 0.23, 0.31], rng.random((7, 3))])
+    mu = 0.0 if mu_band is None else float(oracle_mod.kpoint_data(tb4, k[0])[0][mu_band])
+    task = shg_task(gaussian=gaussian, T=T, mu=mu, omegas=np.linspace(0.0, 3.0, 37))
+    with engine_cls(tb4, task) as eng:
+        got = task.split(eng.point_values(k))[0]
+    ref = task.split(oracle_mod.point_values(tb4, task, k))[0]
+    assert block_err(got, ref) < RTOL
+    if T > 0:
+        assert np.any(got[:, :, :, 5:7, :] != 0)
+
+
+@pytest.mark.parametrize("T", [0.0, 300.0])
+def test_shg_nw32_matches_oracle(engine_cls, oracle_mod, T):
+    model = reference_workload_model("nw32")
+    rng = np.random.default_rng(22)
+    k = rng.random((4, 3))
+    comps = [(0, 1, 1), (2, 0, 1), (1, 2, 2), (0, 0, 0)]
+    task = shg_task(T=T, omegas=np.linspace(0.0, 4.0, 40), components=comps)
+    with engine_cls(model, task) as eng:
+        got = task.split(eng.point_values(k))[0]
+    ref = task.split(oracle_mod.point_values(model, task, k))[0]
+    assert block_err(got, ref) < RTOL
+
+
+def test_shg_mesh_with_other_responses(engine_cls, oracle_mod, tb4):
+    """SHG beside shift-current and quantum-metric components in one task: value offsets, mesh
+    lanes, staged Fourier."""
+    task = shg_task(gaussian=False, T=150.0, omegas=np.linspace(0.0, 2.5, 21),
+                    extra=[(_abi.SHIFT_CURRENT, ["xyy"]), (_abi.QUANTUM_METRIC, ["xx"])])
+    mesh = (6, 5, 4)
+    with engine_cls(tb4, task, max_batch=37) as eng:
+        got = eng.integrate_mesh(mesh)
+    ref = oracle_mod.integrate_mesh(tb4, task, mesh)
+    g_parts, r_parts = task.split(got), task.split(ref)
+    for g, r in zip(g_parts[:2], r_parts[:2]):
+        scale = np.max(np.abs(r))
+        assert np.max(np.abs(g - r)) <= RTOL * scale
+    assert block_err(g_parts[2], r_parts[2]) < RTOL
+
+
+def test_shg_mixed_precision_within_bound(engine_cls, oracle_mod, tb4):
+    rng = np.random.default_rng(23)
+    k = rng.random((6, 3))
+    task = shg_task(precision=_abi.PRECISION_MIXED, omegas=np.linspace(0.0, 3.0, 13))
+    with engine_cls(tb4, task) as eng:
+        got = task.split(eng.point_values(k))[0]
+    ref = task.split(oracle_mod.point_values(tb4, task, k))[0]
+    assert block_err(got, ref) < MIXED_RTOL
+
+
+def test_shg_invalid_widths_rejected(engine_cls, tb4):
+    from wanniernlqg_b200._lib import EngineError
+    task = shg_task()
+    task.desc.shg_low_frequency_broadening = 0.0
+    with pytest.raises(EngineError) as ei:
+        engine_cls(tb4, task)
+    assert ei.value.status == 1 and "finite and positive" in str(ei.value)

@@ -18,6 +18,7 @@
 #include "eigh.cuh"
 #include "fourier.cuh"
 #include "response.cuh"
+#include "shg.cuh"
 
 namespace {
 
@@ -88,6 +89,11 @@ struct wnlqg_plan {
     size_t stageY_elems = 0, stageZ_elems = 0;
     bool use_staged_last = false;
     std::vector<Pass> passes;
+    // Second-harmonic responses: one shg_kernel launch each, sharing one per-CTA scratch.
+    std::vector<ShgParams> shg;
+    size_t shg_smem = 0;
+    int shg_grid = 0;
+    double2 *d_shg_scratch = nullptr;
     int eigh_threads = 32;
     size_t eigh_smem = 0;
     int refine_threads = 32;
@@ -150,6 +156,10 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
     int64_t off = 0;
     for (int r = 0; r < t.num_responses; ++r) {
         const wnlqg_response_request &q = t.responses[r];
+        if (q.kind == WNLQG_SECOND_HARMONIC) {   // its own kernel (build_shg)
+            off += (int64_t)q.num_components * t.num_photon_energies * 14;
+            continue;
+        }
         for (int c = 0; c < q.num_components; ++c) {
             const int32_t *x = q.components[c];
             if (q.kind == WNLQG_SHIFT_CURRENT || q.kind == WNLQG_INJECTION_CURRENT || q.kind == WNLQG_JERK_CURRENT) {
@@ -339,6 +349,73 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
     return WNLQG_OK;
 }
 
+// Second-harmonic launches: parameters per SHG response, shared-memory size, grid and the per-CTA
+// global scratch (G matrices, pair coefficients, pair data).
+wnlqg_status build_shg(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
+    const wnlqg_task_desc &t = pl->task;
+    int64_t off = 0;
+    int max_nc = 0;
+    for (int r = 0; r < t.num_responses; ++r) {
+        const wnlqg_response_request &q = t.responses[r];
+        int64_t width;
+        if (q.kind == WNLQG_SHIFT_CURRENT || q.kind == WNLQG_INJECTION_CURRENT || q.kind == WNLQG_JERK_CURRENT)
+            width = (int64_t)q.num_components * t.num_photon_energies;
+        else if (q.kind == WNLQG_SECOND_HARMONIC)
+            width = (int64_t)q.num_components * t.num_photon_energies * 14;
+        else if (q.kind == WNLQG_INTRINSIC_AHC || q.kind == WNLQG_BERRY_DIPOLE)
+            width = (int64_t)q.num_components * t.num_fermi_energies;
+        else
+            width = q.num_components;
+        if (q.kind == WNLQG_SECOND_HARMONIC) {
+            ShgParams p;
+            std::memset(&p, 0, sizeof(p));
+            p.nw = pl->nw;
+            p.ld = pl->nw + 1;
+            p.xw_stride = (int64_t)pl->C * pl->nn;
+            for (int a = 0; a < 3; ++a) { p.ch_dH[a] = pl->ch_dH[a]; p.ch_A[a] = pl->ch_A[a]; }
+            for (int a = 0; a < 9; ++a) { p.ch_ddH[a] = pl->ch_ddH[a]; p.ch_dA[a] = pl->ch_dA[a]; }
+            p.nc = q.num_components;
+            for (int c = 0; c < q.num_components; ++c)
+                for (int j = 0; j < 3; ++j) p.comp[c][j] = q.components[c][j];
+            p.out = off;
+            p.nom = (int)t.num_photon_energies;
+            p.omegas = pl->d_omegas;
+            p.mu = t.fermi_energy;
+            p.T = t.temperature;
+            p.width = t.broadening;
+            p.low_width = t.shg_low_frequency_broadening;
+            p.eta = t.shg_intermediate_regularization > 0 ? t.shg_intermediate_regularization : t.denominator_regularization;
+            p.degeneracy = t.degeneracy_threshold;
+            p.gaussian = t.broadening_type == WNLQG_GAUSSIAN ? 1 : 0;
+            p.eta_correction = t.shg_eta_correction ? 1 : 0;
+            p.vc = pl->vc;
+            pl->shg.push_back(p);
+            max_nc = std::max(max_nc, q.num_components);
+        }
+        off += width;
+    }
+    if (pl->shg.empty()) return WNLQG_OK;
+    pl->shg_smem = ShgSmem::layout(pl->nw, max_nc).total;
+    if (pl->shg_smem > smem_limit)
+        return fail(WNLQG_ERR_UNSUPPORTED, "second-harmonic kernel does not fit shared memory for nw=" + std::to_string(pl->nw));
+    cudaError_t e = cudaFuncSetAttribute(shg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)std::max<size_t>(pl->shg_smem, 48 * 1024));
+    if (e != cudaSuccess) return fail(WNLQG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, shg_kernel, 256, pl->shg_smem);
+    if (e != cudaSuccess) return fail(WNLQG_ERR_CUDA, std::string("occupancy query: ") + cudaGetErrorString(e));
+    if (per_sm < 1) return fail(WNLQG_ERR_UNSUPPORTED, "second-harmonic kernel cannot be resident with its shared memory");
+    pl->shg_grid = sm_count * per_sm;
+    const int64_t stride = ShgSmem::scratch_entries(pl->nw, max_nc);
+    for (ShgParams &p : pl->shg) p.scratch_stride = stride;
+    e = cudaMalloc(&pl->d_shg_scratch, (size_t)pl->shg_grid * stride * sizeof(double2));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(WNLQG_ERR_OUT_OF_MEMORY, "cudaMalloc of the second-harmonic scratch failed");
+    }
+    return WNLQG_OK;
+}
+
 wnlqg_status record_event(wnlqg_plan *pl, size_t idx) {
     while (pl->events.size() <= idx) {
         cudaEvent_t ev;
@@ -438,6 +515,22 @@ wnlqg_status run_passes(wnlqg_plan *pl, int64_t nb, int mode, double scale, int6
             response_kernel<float><<<ps.grid, ps.threads, ps.smem, pl->stream>>>(p);
         else
             response_kernel<double><<<ps.grid, ps.threads, ps.smem, pl->stream>>>(p);
+        pl->launches += 1;
+    }
+    for (const ShgParams &tmpl : pl->shg) {
+        ShgParams p = tmpl;
+        p.batch = nb;
+        p.xw = pl->d_xw;
+        p.E = pl->d_E;
+        p.U = pl->d_U;
+        p.mode = mode;
+        p.scale = scale;
+        p.weights = weights;
+        p.partials = pl->d_partials;
+        p.out_points = pl->d_points;
+        p.point_offset = point_offset;
+        p.scratch = pl->d_shg_scratch;
+        shg_kernel<<<pl->shg_grid, 256, pl->shg_smem, pl->stream>>>(p);
         pl->launches += 1;
     }
     WNLQG_CUDA(cudaGetLastError());
@@ -544,7 +637,8 @@ wnlqg_status wnlqg_b200_plan_destroy(wnlqg_plan *pl) {
     for (void *ptr : {(void *)pl->d_tiles, (void *)pl->d_phase, (void *)pl->d_xw, (void *)pl->d_U, (void *)pl->d_out,
                       (void *)pl->d_points, (void *)pl->d_E, (void *)pl->d_kpts, (void *)pl->d_omegas,
                       (void *)pl->d_partials, (void *)pl->d_weights, (void *)pl->d_groups, (void *)pl->d_stageY,
-                      (void *)pl->d_stageZ, (void *)pl->d_V32, (void *)pl->d_kidx, (void *)pl->d_mus, (void *)pl->d_status})
+                      (void *)pl->d_stageZ, (void *)pl->d_V32, (void *)pl->d_kidx, (void *)pl->d_mus, (void *)pl->d_status,
+                      (void *)pl->d_shg_scratch})
         if (ptr) cudaFree(ptr);
     for (cudaEvent_t ev : pl->events) cudaEventDestroy(ev);
     if (pl->stream) cudaStreamDestroy(pl->stream);
@@ -634,6 +728,18 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
                 pl->ch_dA[a * 3 + b] = add_channel(ch, CH_DA, a, b);
                 if (q.kind == WNLQG_BERRY_DIPOLE) pl->ch_dH[cc] = add_channel(ch, CH_DH, cc, 0);
                 break;
+            case WNLQG_SECOND_HARMONIC:
+                // Every Cartesian channel: the nine cutoff derivatives G^{ab} and both one-band terms.
+                for (int u = 0; u < 3; ++u) {
+                    need_r(u);
+                    for (int v = 0; v < 3; ++v) {
+                        pl->ch_dA[u * 3 + v] = add_channel(ch, CH_DA, u, v);
+                        const int hidx = add_channel(ch, CH_DDH, u, v);
+                        pl->ch_ddH[u * 3 + v] = hidx;
+                        pl->ch_ddH[v * 3 + u] = hidx;
+                    }
+                }
+                break;
             case WNLQG_JERK_CURRENT: {
                 const int dd = x[3];
                 need_r(b); need_r(cc);
@@ -653,6 +759,18 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
             if (q.kind == WNLQG_JERK_CURRENT && !(t.denominator_regularization > 0))
                 return bail(fail(WNLQG_ERR_INVALID_ARGUMENT, "third-order matrix width must be finite and positive"));
             vc += (int64_t)q.num_components * t.num_photon_energies;
+        } else if (q.kind == WNLQG_SECOND_HARMONIC) {
+            // second_harmonic_response! argument checks (SecondHarmonicKernels.jl:129-138).
+            if (t.num_photon_energies < 1) return bail(fail(WNLQG_ERR_INVALID_ARGUMENT, "photon energies required"));
+            const double eta = t.shg_intermediate_regularization > 0 ? t.shg_intermediate_regularization
+                                                                      : t.denominator_regularization;
+            if (!(std::isfinite(t.shg_low_frequency_broadening) && t.shg_low_frequency_broadening > 0 &&
+                  std::isfinite(eta) && eta > 0))
+                return bail(fail(WNLQG_ERR_INVALID_ARGUMENT,
+                                 "SHG optical widths and intermediate_regularization must be finite and positive in eV"));
+            if (!(std::isfinite(t.degeneracy_threshold) && t.degeneracy_threshold >= 0))
+                return bail(fail(WNLQG_ERR_INVALID_ARGUMENT, "SHG degeneracy_threshold must be finite and nonnegative in eV"));
+            vc += (int64_t)q.num_components * t.num_photon_energies * 14;
         } else if (q.kind == WNLQG_INTRINSIC_AHC || q.kind == WNLQG_BERRY_DIPOLE) {
             if (t.num_fermi_energies < 1 || !t.fermi_energies)
                 return bail(fail(WNLQG_ERR_INVALID_ARGUMENT, "finite nonempty Fermi energy axis required"));
@@ -719,7 +837,7 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
     if (smem_optin <= 0) smem_optin = 48 * 1024;
 
     if (max_batch <= 0) {
-        int64_t per_k = (int64_t)pl->C * nn * 16 + (int64_t)nr * 16 + nn * 16 + nw * 8;
+        int64_t per_k = (int64_t)pl->C * nn * 16 + (int64_t)nr * 16 + nn * 16 + nw * 8 + vc * 16;
         // About 4 GiB of batch workspace (HBM is 180 GB): long runs of neighbouring k-points per
         // CTA for the warm-started eigensolver and few batches per call.
         max_batch = std::max<int64_t>(256, std::min<int64_t>(1 << 20, ((int64_t)1 << 32) / per_k));
@@ -831,7 +949,9 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
         }
     }
     if ((st = build_passes(pl, sm_count, (size_t)smem_optin)) != WNLQG_OK) return bail(st);
+    if ((st = build_shg(pl, sm_count, (size_t)smem_optin)) != WNLQG_OK) return bail(st);
     for (const Pass &ps : pl->passes) pl->partial_slots = std::max(pl->partial_slots, ps.grid);
+    pl->partial_slots = std::max(pl->partial_slots, pl->shg_grid);
     if ((st = alloc((void **)&pl->d_partials, (size_t)pl->partial_slots * vc * 4 * sizeof(double))) != WNLQG_OK)
         return bail(st);
     *out_plan = pl;
