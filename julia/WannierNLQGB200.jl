@@ -11,6 +11,7 @@ const BERRY_CURVATURE = Int32(3)
 const QUANTUM_METRIC = Int32(4)
 const INTRINSIC_AHC = Int32(5)
 const BERRY_DIPOLE = Int32(6)
+const SECOND_HARMONIC = Int32(7)
 const JERK_CURRENT = Int32(8)
 
 struct ModelDesc
@@ -46,6 +47,9 @@ struct TaskDesc
     fermi_energies::Ptr{Float64}
     precision::Int32                   # 0 FP64, 1 mixed
     fermi_surface_broadening::Float64
+    shg_low_frequency_broadening::Float64      # cfg.shg_low_frequency_broadening
+    shg_intermediate_regularization::Float64   # cfg.shg_intermediate_regularization (0: denominator_regularization)
+    shg_eta_correction::Int32                  # cfg.shg_eta_correction
 end
 
 function check(status)
