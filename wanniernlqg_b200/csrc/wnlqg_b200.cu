@@ -6,9 +6,12 @@
 // on the plan's stream; mesh evaluation ends with one ordered reduction of the per-CTA partials.
 #include "../../include/wnlqg_b200.h"
 
+#include <cuda.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -19,6 +22,7 @@
 #include "fourier.cuh"
 #include "response.cuh"
 #include "shg.cuh"
+#include "tc_fourier.cuh"
 
 namespace {
 
@@ -94,6 +98,15 @@ struct wnlqg_plan {
     size_t shg_smem = 0;
     int shg_grid = 0;
     double2 *d_shg_scratch = nullptr;
+    // Tensor-core Fourier for arbitrary k-points: Ozaki slices of the phases (A, per batch) and of
+    // the channel tiles (B, built once), tcgen05 kind::i8 GEMM.  tc_slices == 0: FP64 CUDA cores.
+    int tc_slices = 0;
+    int64_t tc_kpad = 0, tc_npad = 0, tc_mpad = 0, tc_ncols = 0;
+    int8_t *d_tcA = nullptr, *d_tcB = nullptr;
+    double *d_tc_colscale = nullptr;
+    int *d_tc_err = nullptr;
+    bool tc_used = false;
+    CUtensorMap tc_mapA, tc_mapB;
     int eigh_threads = 32;
     size_t eigh_smem = 0;
     int refine_threads = 32;
@@ -426,6 +439,147 @@ wnlqg_status record_event(wnlqg_plan *pl, size_t idx) {
     return WNLQG_OK;
 }
 
+// Tensor-core Fourier of one batch: phase slices, then the persistent tcgen05 GEMM writing the
+// FP64 channels.
+template <int S>
+wnlqg_status launch_tc_fourier(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const int64_t *mesh,
+                               const double *kpts_device, const int64_t *kidx_device) {
+    typedef tcf::Layout<S> L;
+    const int64_t total = nb * (pl->tc_kpad / 2);
+    const int blocks = (int)std::min<int64_t>((total + 255) / 256, (int64_t)pl->sm_count * 32);
+    tcf::phase_slices_kernel<S><<<blocks, 256, 0, pl->stream>>>(
+        pl->d_tcA, pl->tc_mpad, pl->tc_kpad, pl->model->d_rvec, pl->model->d_deg, pl->nr, nb, k_begin,
+        mesh ? mesh[0] : 1, mesh ? mesh[1] : 1, mesh ? mesh[2] : 1, kpts_device, kidx_device);
+    tcf::TcArgs a;
+    a.colscale = pl->d_tc_colscale;
+    a.xw = pl->d_xw;
+    a.nb = nb;
+    a.ncols = pl->tc_ncols;
+    a.kblocks = (int)(pl->tc_kpad / tcf::BK);
+    a.mtiles = (int)((nb + tcf::BM - 1) / tcf::BM);
+    a.ntiles = (int)(pl->tc_npad / L::NT);
+    a.err = pl->d_tc_err;
+    const int tiles = a.mtiles * a.ntiles;
+    const int grid = std::min(tiles, pl->sm_count);
+    tcf::tc_fourier_kernel<S><<<grid, tcf::THREADS, L::SMEM_BYTES, pl->stream>>>(pl->tc_mapA, pl->tc_mapB, a);
+    pl->launches += 1;
+    pl->tc_used = true;
+    WNLQG_CUDA(cudaGetLastError());
+    return WNLQG_OK;
+}
+
+wnlqg_status run_tc_fourier(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const int64_t *mesh, const double *kpts_device,
+                            const int64_t *kidx_device) {
+    switch (pl->tc_slices) {
+    case 7: return launch_tc_fourier<7>(pl, nb, k_begin, mesh, kpts_device, kidx_device);
+    case 4: return launch_tc_fourier<4>(pl, nb, k_begin, mesh, kpts_device, kidx_device);
+    default: return fail(WNLQG_ERR_UNSUPPORTED, "tensor-core Fourier slice count");
+    }
+}
+
+// Reports (and clears) a bounded-wait failure of the tensor-core Fourier after a synchronised call.
+wnlqg_status tc_check(wnlqg_plan *pl) {
+    if (!pl->tc_used || !pl->d_tc_err) return WNLQG_OK;
+    pl->tc_used = false;
+    int h = 0;
+    WNLQG_CUDA(cudaMemcpy(&h, pl->d_tc_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (h) {
+        cudaMemset(pl->d_tc_err, 0, sizeof(int));
+        return fail(WNLQG_ERR_DEVICE_TIMEOUT, "tensor-core Fourier: a bounded device wait gave up");
+    }
+    return WNLQG_OK;
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// 3D int8 tensor map [slices][rows][kpad] with a box of (64 bytes, box_rows, slices), 64-byte swizzle.
+wnlqg_status encode_slices_map(EncodeTiledFn enc, CUtensorMap *map, int8_t *ptr, int64_t kpad, int64_t rows, int slices,
+                               int box_rows) {
+    cuuint64_t dims[3] = {(cuuint64_t)kpad, (cuuint64_t)rows, (cuuint64_t)slices};
+    cuuint64_t strides[2] = {(cuuint64_t)kpad, (cuuint64_t)(kpad * rows)};
+    cuuint32_t box[3] = {(cuuint32_t)tcf::BK, (cuuint32_t)box_rows, (cuuint32_t)slices};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, ptr, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(WNLQG_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+    return WNLQG_OK;
+}
+
+// Builds the B slices of the channel tiles (host, once per plan), the phase-slice buffer and both
+// tensor maps.  tiles: [NR][C][nw^2] complex.
+template <int S>
+wnlqg_status setup_tc_fourier(wnlqg_plan *pl, const std::vector<double2> &tiles) {
+    typedef tcf::Layout<S> L;
+    const int64_t nr = pl->nr, nn = pl->nn, C = pl->C;
+    const int64_t ncols = 2 * C * nn;
+    const int64_t kpad = ((2 * nr + tcf::BK - 1) / tcf::BK) * tcf::BK;
+    const int64_t npad = ((ncols + L::NT - 1) / L::NT) * L::NT;
+    const int64_t mpad = ((pl->max_batch + tcf::BM - 1) / tcf::BM) * tcf::BM;
+    std::vector<int8_t> Bq((size_t)S * npad * kpad, 0);
+    std::vector<double> colscale((size_t)npad, 0.0);
+    const int64_t row_stride = C * nn;
+    for (int64_t n = 0; n < C * nn; ++n) {
+        double mx = 0.0;
+        for (int64_t r = 0; r < nr; ++r) {
+            const double2 t = tiles[(size_t)(r * row_stride + n)];
+            mx = std::max(mx, std::max(std::fabs(t.x), std::fabs(t.y)));
+        }
+        int e = 0;
+        if (mx > 0.0) std::frexp(mx, &e);
+        for (int sidx = 0; sidx < 2; ++sidx) {
+            const int64_t row = 2 * n + sidx;
+            colscale[(size_t)row] = std::ldexp(1.0, e - 12);
+            for (int64_t r = 0; r < nr; ++r) {
+                const double2 t = tiles[(size_t)(r * row_stride + n)];
+                const double v0 = sidx == 0 ? t.x : t.y;    // multiplies Re F
+                const double v1 = sidx == 0 ? -t.y : t.x;   // multiplies Im F
+                int8_t s0[S], s1[S];
+                tcf::slice_value<S>(std::ldexp(v0, -e), s0);
+                tcf::slice_value<S>(std::ldexp(v1, -e), s1);
+                for (int i = 0; i < S; ++i) {
+                    Bq[(size_t)((i * npad + row) * kpad + 2 * r)] = s0[i];
+                    Bq[(size_t)((i * npad + row) * kpad + 2 * r + 1)] = s1[i];
+                }
+            }
+        }
+    }
+    auto alloc = [&](void **ptr, size_t bytes) -> wnlqg_status {
+        cudaError_t ce = cudaMalloc(ptr, std::max<size_t>(bytes, 16));
+        if (ce != cudaSuccess) {
+            cudaGetLastError();
+            return fail(WNLQG_ERR_OUT_OF_MEMORY, "cudaMalloc of " + std::to_string(bytes) + " bytes failed");
+        }
+        return WNLQG_OK;
+    };
+    wnlqg_status st;
+    if ((st = alloc((void **)&pl->d_tcB, Bq.size())) != WNLQG_OK) return st;
+    if ((st = alloc((void **)&pl->d_tcA, (size_t)S * mpad * kpad)) != WNLQG_OK) return st;
+    if ((st = alloc((void **)&pl->d_tc_colscale, colscale.size() * sizeof(double))) != WNLQG_OK) return st;
+    if ((st = alloc((void **)&pl->d_tc_err, sizeof(int))) != WNLQG_OK) return st;
+    WNLQG_CUDA(cudaMemcpy(pl->d_tcB, Bq.data(), Bq.size(), cudaMemcpyHostToDevice));
+    WNLQG_CUDA(cudaMemcpy(pl->d_tc_colscale, colscale.data(), colscale.size() * sizeof(double), cudaMemcpyHostToDevice));
+    WNLQG_CUDA(cudaMemset(pl->d_tc_err, 0, sizeof(int)));
+    WNLQG_CUDA(cudaMemset(pl->d_tcA, 0, (size_t)S * mpad * kpad));
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn)
+        return fail(WNLQG_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    EncodeTiledFn enc = reinterpret_cast<EncodeTiledFn>(fn);
+    if ((st = encode_slices_map(enc, &pl->tc_mapA, pl->d_tcA, kpad, mpad, S, tcf::BM)) != WNLQG_OK) return st;
+    if ((st = encode_slices_map(enc, &pl->tc_mapB, pl->d_tcB, kpad, npad, S, L::NT)) != WNLQG_OK) return st;
+    WNLQG_CUDA(cudaFuncSetAttribute(tcf::tc_fourier_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)L::SMEM_BYTES));
+    pl->tc_kpad = kpad;
+    pl->tc_npad = npad;
+    pl->tc_mpad = mpad;
+    pl->tc_ncols = ncols;
+    pl->tc_slices = S;
+    return WNLQG_OK;
+}
+
 // One batch: phases, Fourier GEMM, eigensolve.  kpts_device == nullptr selects mesh mode.
 wnlqg_status run_front(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const int64_t *mesh, const double *kpts_device,
                        size_t ev_base, const int64_t *kidx_device = nullptr) {
@@ -463,6 +617,9 @@ wnlqg_status run_front(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const int64_
                                                                                        pl->d_stageZ);
         staged_r1_kernel<<<dim3(cb, (unsigned)((nb + STAGED_BT - 1) / STAGED_BT)), 256, 0, pl->stream>>>(
             pl->d_stageZ, N, pl->groups, k_begin, nb, n1, line_first, pl->d_xw);
+    } else if (pl->tc_slices > 0) {
+        wnlqg_status tst = run_tc_fourier(pl, nb, k_begin, mesh, kpts_device, kidx_device);
+        if (tst != WNLQG_OK) return tst;
     } else {
         int64_t total = nb * nr;
         int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 32);
@@ -638,7 +795,8 @@ wnlqg_status wnlqg_b200_plan_destroy(wnlqg_plan *pl) {
                       (void *)pl->d_points, (void *)pl->d_E, (void *)pl->d_kpts, (void *)pl->d_omegas,
                       (void *)pl->d_partials, (void *)pl->d_weights, (void *)pl->d_groups, (void *)pl->d_stageY,
                       (void *)pl->d_stageZ, (void *)pl->d_V32, (void *)pl->d_kidx, (void *)pl->d_mus, (void *)pl->d_status,
-                      (void *)pl->d_shg_scratch})
+                      (void *)pl->d_shg_scratch, (void *)pl->d_tcA, (void *)pl->d_tcB, (void *)pl->d_tc_colscale,
+                      (void *)pl->d_tc_err})
         if (ptr) cudaFree(ptr);
     for (cudaEvent_t ev : pl->events) cudaEventDestroy(ev);
     if (pl->stream) cudaStreamDestroy(pl->stream);
@@ -948,6 +1106,17 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
             if (e != cudaSuccess) return bail(fail(WNLQG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e)));
         }
     }
+    // Arbitrary-point Fourier on the tcgen05 tensor cores (sm_100): 7 slices (FP64 path) or 4
+    // (mixed path).  WNLQG_B200_DIRECT_FOURIER=1 keeps the FP64 CUDA-core GEMM instead.
+    {
+        int major = 0;
+        cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+        const char *direct = std::getenv("WNLQG_B200_DIRECT_FOURIER");
+        if (major == 10 && !(direct && direct[0] == '1')) {
+            st = t.precision == WNLQG_PRECISION_MIXED ? setup_tc_fourier<4>(pl, tiles) : setup_tc_fourier<7>(pl, tiles);
+            if (st != WNLQG_OK) return bail(st);
+        }
+    }
     if ((st = build_passes(pl, sm_count, (size_t)smem_optin)) != WNLQG_OK) return bail(st);
     if ((st = build_shg(pl, sm_count, (size_t)smem_optin)) != WNLQG_OK) return bail(st);
     for (const Pass &ps : pl->passes) pl->partial_slots = std::max(pl->partial_slots, ps.grid);
@@ -1023,6 +1192,7 @@ wnlqg_status wnlqg_b200_eval_mesh(wnlqg_plan *pl, const int64_t mesh[3], int64_t
         return st;
     WNLQG_CUDA(cudaMemcpyAsync(out, pl->d_out, (size_t)pl->vc * sizeof(double2), cudaMemcpyDeviceToHost, pl->stream));
     WNLQG_CUDA(cudaStreamSynchronize(pl->stream));
+    if ((st = tc_check(pl)) != WNLQG_OK) return st;
     for (int64_t v = 0; v < 2 * pl->vc; ++v)
         if (!std::isfinite(out[v])) return fail(WNLQG_ERR_NONFINITE, "response contains non-finite values");
     return WNLQG_OK;
@@ -1047,6 +1217,7 @@ wnlqg_status wnlqg_b200_eval_points(wnlqg_plan *pl, const double *kpoints, int64
     }
     WNLQG_CUDA(cudaStreamSynchronize(pl->stream));
     pl->timing_valid = false;
+    if ((st = tc_check(pl)) != WNLQG_OK) return st;
     for (int64_t v = 0; v < 2 * n * pl->vc; ++v)
         if (!std::isfinite(out[v])) return fail(WNLQG_ERR_NONFINITE, "response contains non-finite values");
     return WNLQG_OK;
@@ -1079,6 +1250,7 @@ wnlqg_status wnlqg_b200_eval_points_weighted(wnlqg_plan *pl, const double *kpoin
     WNLQG_CUDA(cudaMemcpyAsync(out, pl->d_out, (size_t)pl->vc * sizeof(double2), cudaMemcpyDeviceToHost, pl->stream));
     WNLQG_CUDA(cudaStreamSynchronize(pl->stream));
     pl->timing_valid = false;
+    if ((st = tc_check(pl)) != WNLQG_OK) return st;
     for (int64_t v = 0; v < 2 * pl->vc; ++v)
         if (!std::isfinite(out[v])) return fail(WNLQG_ERR_NONFINITE, "response contains non-finite values");
     return WNLQG_OK;
@@ -1121,6 +1293,7 @@ wnlqg_status wnlqg_b200_eval_mesh_weighted(wnlqg_plan *pl, const int64_t mesh[3]
     WNLQG_CUDA(cudaMemcpyAsync(out, pl->d_out, (size_t)pl->vc * sizeof(double2), cudaMemcpyDeviceToHost, pl->stream));
     WNLQG_CUDA(cudaStreamSynchronize(pl->stream));
     pl->timing_valid = false;
+    if ((st = tc_check(pl)) != WNLQG_OK) return st;
     for (int64_t v = 0; v < 2 * pl->vc; ++v)
         if (!std::isfinite(out[v])) return fail(WNLQG_ERR_NONFINITE, "response contains non-finite values");
     return WNLQG_OK;
@@ -1150,6 +1323,7 @@ wnlqg_status wnlqg_b200_eval_spectrum(wnlqg_plan *pl, const double *kpoints, int
     }
     WNLQG_CUDA(cudaStreamSynchronize(pl->stream));
     pl->timing_valid = false;
+    if ((st = tc_check(pl)) != WNLQG_OK) return st;
     if (pl->nonorth)
         for (int v : stat)
             if (v) return fail(WNLQG_ERR_INVALID_ARGUMENT, "effective S(k) is not positive definite");
