@@ -10,6 +10,10 @@ A step is one contiguous block of `--batch` mesh points pushed through the whole
 takes its own blocks (weak scaling, no data-path collective); the lane tensors are combined
 once at the end with one NCCL all-reduce outside the timed region.
 
+`--sampling random` replaces the mesh blocks by seeded uniformly random k-points (the nodes of an
+adaptive integrator), evaluated through the weighted-points entry point: there the Fourier step
+is the tcgen05 tensor-core GEMM instead of the staged mesh contraction.
+
 `--impl reference` times the reference algorithm's CPU restatement (the FP64 oracle, all host
 threads) on a bounded sample of the same mesh.
 """
@@ -33,6 +37,7 @@ from wanniernlqg_b200.model import reference_workload_model  # noqa: E402
 
 METRIC = "k-points/s"
 WORKLOAD = "nw32_R729_fullA_mesh256^3_sigma_xyy_512w_OmegaZ_gxx"
+WORKLOAD_RANDOM = "nw32_R729_fullA_random_k_sigma_xyy_512w_OmegaZ_gxx"
 MESH = (256, 256, 256)
 
 
@@ -177,6 +182,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--batch", type=int, default=65536, help="mesh points per step and rank")
+    ap.add_argument("--sampling", default="mesh", choices=["mesh", "random"],
+                    help="mesh blocks (staged Fourier) or random k-points (tensor-core Fourier)")
+    ap.add_argument("--max-batch", type=int, default=0, help="plan batch capacity (0: the plan default, ~4 GiB)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -204,7 +212,7 @@ def main():
     task = make_task(precision)
     nk = int(np.prod(MESH))
     batch = args.batch
-    engine = ResponseEngine(model, task, device=local_rank)
+    engine = ResponseEngine(model, task, device=local_rank, max_batch=args.max_batch)
     vc = engine.value_count
     out = torch.zeros(2 * vc, dtype=torch.float64, device="cuda")
     stream = torch.cuda.current_stream()
@@ -213,9 +221,23 @@ def main():
         b = ((step * world + rank) * batch) % nk
         return b, min(nk, b + batch)
 
+    random_mode = args.sampling == "random"
+    if random_mode:
+        gen = torch.Generator(device="cuda")
+        gen.manual_seed(1234 + rank)
+        kdev = torch.rand((args.warmup + args.steps) * batch, 3, dtype=torch.float64, device="cuda", generator=gen)
+        wdev = torch.full((batch,), 1.0 / (world * batch), dtype=torch.float64, device="cuda")
+
+    def run_step(step):
+        if random_mode:
+            engine.weighted_sum_device(kdev.data_ptr() + step * batch * 3 * 8, wdev.data_ptr(), batch,
+                                       out.data_ptr(), stream.cuda_stream)
+        else:
+            kb, ke = block(step)
+            engine.integrate_mesh_device(MESH, kb, ke, out.data_ptr(), stream.cuda_stream)
+
     for s in range(args.warmup):
-        kb, ke = block(s)
-        engine.integrate_mesh_device(MESH, kb, ke, out.data_ptr(), stream.cuda_stream)
+        run_step(s)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -228,8 +250,7 @@ def main():
     ev0.record(stream)
     launches = 0
     for s in range(args.steps):
-        kb, ke = block(args.warmup + s)
-        engine.integrate_mesh_device(MESH, kb, ke, out.data_ptr(), stream.cuda_stream)
+        run_step(args.warmup + s)
         launches += engine.last_launch_count()
     ev1.record(stream)
     torch.cuda.synchronize()
@@ -247,13 +268,20 @@ def main():
     # host memory (H2D), the weighted mesh sum, and the result read back (D2H); synchronous,
     # wall clock.
     e2e_steps = max(1, min(args.steps, 3))
-    kb, _ = block(args.warmup + args.steps)
-    idx = torch.arange(kb, kb + batch, dtype=torch.int64).pin_memory().numpy()
-    w = torch.full((batch,), 1.0 / nk, dtype=torch.float64).pin_memory().numpy()
-    engine.mesh_weighted_sum(MESH, idx, w)
+    if random_mode:
+        # Host k-points and weights (pinned), the weighted-points call, the result read back.
+        idx = kdev[:batch].cpu().pin_memory().numpy()
+        w = torch.full((batch,), 1.0 / batch, dtype=torch.float64).pin_memory().numpy()
+        e2e_call = lambda: engine.weighted_sum(idx, w)  # noqa: E731
+    else:
+        kb, _ = block(args.warmup + args.steps)
+        idx = torch.arange(kb, kb + batch, dtype=torch.int64).pin_memory().numpy()
+        w = torch.full((batch,), 1.0 / nk, dtype=torch.float64).pin_memory().numpy()
+        e2e_call = lambda: engine.mesh_weighted_sum(MESH, idx, w)  # noqa: E731
+    e2e_call()
     t0 = time.perf_counter()
     for s in range(e2e_steps):
-        engine.mesh_weighted_sum(MESH, idx, w)
+        e2e_call()
     e2e_dt = (time.perf_counter() - t0) / e2e_steps
     e2e_value = world * batch / e2e_dt
 
@@ -264,8 +292,10 @@ def main():
     nw, nr = model.num_orbitals, model.num_r_vectors
     C = fourier_channels(task)
     # Algorithmic work per k-point (counts of the algorithms executed):
-    #   staged Fourier: 8*P1*C*nw^2 flop (P1 = 9 distinct r1 on the |R_i|<=4 cube) and
+    #   staged Fourier (mesh): 8*P1*C*nw^2 flop (P1 = 9 distinct r1 on the |R_i|<=4 cube) and
     #     C*nw^2*16 B written + read once (FP64 Wannier-gauge channels);
+    #   tensor-core Fourier (random): S(S+1)/2 int8 slice products of 2*Kpad*Npad ops each
+    #     (Kpad = 2*NR rounded up to 64, Npad = 2*C*nw^2 rounded up to the tile width);
     #   eigensolve: 30*nw^3 flop (LAPACK-class modelling count for a Hermitian eigensolve);
     #   response: 18 complex nw^3 products (8*nw^3 flop each) + 4*nw^2*Nw flop contraction.
     p1 = 9
@@ -273,33 +303,53 @@ def main():
             "response": 18 * 8.0 * nw ** 3 + 4.0 * nw * nw * 512}
     hbm = {"fourier": 2.0 * C * nw * nw * 16, "eigen": nw * nw * 16 * 2.0 + nw * 8,
            "response": (C - 1) * nw * nw * 16 + nw * nw * 16}
-    t_s = stages[dominant] / 1e3
-    achieved_gbs = hbm[dominant] * batch / t_s / 1e9
-    achieved_tf = flop[dominant] * batch / t_s / 1e12
     sm_peak = {"fp64": 37.0, "mixed": 74.0}["fp64" if precision == _abi.PRECISION_FP64 else "mixed"]
-    roofline = {
-        "bound": "hbm" if dominant == "fourier" else "sm",
-        "kernel": {"fourier": "staged Fourier (staged_r1_kernel)", "eigen": "Jacobi eigensolver",
-                   "response": "fused response kernel"}[dominant],
-        "achieved": achieved_gbs if dominant == "fourier" else achieved_tf,
-        "peak": peaks["hbm_gbs"] if dominant == "fourier" else sm_peak,
-        "unit": "GB/s" if dominant == "fourier" else "TFLOP/s",
+    sm_src = "nominal B200 CUDA-core peak (FP64 37 / FP32 74 TFLOP/s; not in the measured peaks file)"
+    slices = 7 if precision == _abi.PRECISION_FP64 else 4
+    tile_n = 64 if slices == 7 else 128
+    kpad = -(-2 * nr // 64) * 64
+    npad = -(-2 * C * nw * nw // tile_n) * tile_n
+    tc_ops = slices * (slices + 1) / 2 * 2.0 * kpad * npad
+
+    def stage_roofline(name):
+        t_s = stages[name] / 1e3
+        if name == "fourier" and random_mode:
+            achieved = tc_ops * batch / t_s / 1e12
+            return {"bound": "tensor", "kernel": "tcgen05 int8 slice GEMM (tc_fourier_kernel)",
+                    "achieved": achieved, "unit": "TOP/s", "peak": 2.0 * peaks["bf16_tflops"],
+                    "peak_source": f"2 x {peak_src} dense bf16 (the dense int8 rate is twice bf16)",
+                    "fp64_equivalent_tflops": 8.0 * nr * C * nw * nw * batch / t_s / 1e12}
+        if name == "fourier":
+            return {"bound": "hbm", "kernel": "staged Fourier (staged_r1_kernel)",
+                    "achieved": hbm[name] * batch / t_s / 1e9, "unit": "GB/s", "peak": peaks["hbm_gbs"],
+                    "peak_source": f"{peak_src} HBM copy bandwidth"}
+        return {"bound": "sm", "kernel": {"eigen": "Jacobi eigensolver", "response": "fused response kernel"}[name],
+                "achieved": flop[name] * batch / t_s / 1e12, "unit": "TFLOP/s", "peak": sm_peak, "peak_source": sm_src,
+                "hbm_gbs": hbm[name] * batch / t_s / 1e9}
+
+    per_stage = {}
+    for name in stages:
+        r = stage_roofline(name)
+        r["frac"] = r["achieved"] / r["peak"] if r["peak"] else None
+        r["ms_last_step"] = stages[name]
+        per_stage[name] = r
+    roofline = dict(per_stage[dominant])
+    roofline.update({
         "traffic": None,
-        "peak_source": (f"{peak_src} HBM copy bandwidth" if dominant == "fourier" else
-                        "nominal B200 CUDA-core peak (FP64 37 / FP32 74 TFLOP/s; not in the measured peaks file)"),
         "stage_ms_last_step": {"fourier": fourier_ms, "eigen": eigen_ms, "response": response_ms, "total": total_ms},
-        "algorithmic_per_k": {"flop": flop, "hbm_bytes": hbm},
-        "hbm_gbs_dominant": achieved_gbs,
+        "stages": per_stage,
+        "algorithmic_per_k": {"flop": flop, "hbm_bytes": hbm, "tensor_int8_ops": tc_ops if random_mode else None},
         "launches_per_step": launches // max(1, args.steps),
-    }
-    roofline["frac"] = roofline["achieved"] / roofline["peak"] if roofline["peak"] else None
+    })
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if precision == _abi.PRECISION_FP64 else "f32+f64",
-        "data": "synthetic (seeded nw=32 model, 256^3 mesh blocks; no dataset)",
-        "config": {"workload": WORKLOAD, "k_per_step_per_gpu": batch, "mesh": list(MESH),
+        "data": ("synthetic (seeded nw=32 model, seeded random k-points; no dataset)" if random_mode else
+                 "synthetic (seeded nw=32 model, 256^3 mesh blocks; no dataset)"),
+        "config": {"workload": WORKLOAD_RANDOM if random_mode else WORKLOAD, "k_per_step_per_gpu": batch,
+                   "mesh": None if random_mode else list(MESH), "sampling": args.sampling,
                    "precision": args.precision, "l2": "inputs larger than L2 (per-step workspace >> 126 MB)",
                    "parallelism": f"k-blocks x{world}"},
         "roofline": roofline,

@@ -176,6 +176,14 @@ WNLQG_API wnlqg_status wnlqg_b200_eval_points(wnlqg_plan *plan, const double *kp
 WNLQG_API wnlqg_status wnlqg_b200_eval_points_weighted(wnlqg_plan *plan, const double *kpoints,
                                              const double *weights, int64_t n, double *out);
 
+/* Same as wnlqg_b200_eval_points_weighted with DEVICE arrays (kpoints_device[3*n],
+ * weights_device[n], out_device complex [value_count]) on `stream` (NULL = legacy default
+ * stream); asynchronous, the caller synchronises.  For adaptive integrators whose nodes are
+ * generated on the device (ResponseCubatureTree.jl:112-143 batch evaluation). */
+WNLQG_API wnlqg_status wnlqg_b200_eval_points_weighted_device(wnlqg_plan *plan, const double *kpoints_device,
+                                                    const double *weights_device, int64_t n,
+                                                    double *out_device, void *stream);
+
 /* Weighted sum over mesh indices: out = sum_i weights[i] * value(k(indices[i])) with k the
  * Gamma-centred mesh point of each index (first axis fastest).  Indices and weights are host
  * arrays.  This is the symmetry-reduced mesh contract (representatives and multiplicities/Nk,

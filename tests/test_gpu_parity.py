@@ -190,8 +190,10 @@ def test_mixed_mesh_within_bound(engine_cls, oracle_mod, name, mesh):
 
 
 @pytest.mark.parametrize("name", ["nw4", "nw32"])
-def test_mixed_eigensolver_refined_to_fp64(engine_cls, oracle_mod, name):
-    """FP32 Jacobi + one FP64 Rayleigh-Ritz refinement reaches FP64-level eigenvalues."""
+def test_mixed_eigensolver_refined_to_fp64(engine_cls, oracle_mod, name, monkeypatch):
+    """FP32 Jacobi + one FP64 Rayleigh-Ritz refinement reaches FP64-level eigenvalues.  The
+    eigensolver is isolated by feeding it the FP64 CUDA-core Fourier sums."""
+    monkeypatch.setenv("WNLQG_B200_DIRECT_FOURIER", "1")
     model = reference_workload_model(name)
     task = nw4_task(precision=_abi.PRECISION_MIXED) if name == "nw4" else nw32_task(precision=_abi.PRECISION_MIXED)
     k = np.random.default_rng(15).random((24, 3))
@@ -203,6 +205,24 @@ def test_mixed_eigensolver_refined_to_fp64(engine_cls, oracle_mod, name):
         assert err < 1e-11 * max(1.0, np.abs(eo).max()), (i, err, np.min(np.diff(eo)))
         ov = np.abs(np.sum(u[i].conj() * uo, axis=0))
         assert np.max(np.abs(ov - 1.0)) < 1e-8, (i, np.max(np.abs(ov - 1.0)), np.min(np.diff(eo)))
+
+
+@pytest.mark.parametrize("name,precision,slices", [("nw4", _abi.PRECISION_FP64, 7), ("nw32", _abi.PRECISION_FP64, 7),
+                                                   ("nw4", _abi.PRECISION_MIXED, 4), ("nw32", _abi.PRECISION_MIXED, 4)])
+def test_tensor_core_fourier_eigenvalues_within_slice_bound(engine_cls, oracle_mod, name, precision, slices):
+    """Arbitrary k-points take the tcgen05 Fourier on S int8 slices: H(k) carries at most
+    16 sqrt(2 NR) 2^(-7S) of each channel column's largest |H(R)|, and so do the eigenvalues
+    (Weyl); the FP64 path (S = 7) stays at the FP64 bar."""
+    model = reference_workload_model(name)
+    task = nw4_task(precision=precision) if name == "nw4" else nw32_task(precision=precision)
+    k = np.random.default_rng(16).random((24, 3))
+    with engine_cls(model, task) as eng:
+        e, _ = eng.spectrum(k)
+    colmax = np.max(np.abs(model.hamiltonian_r), axis=2)
+    bound = 16.0 * np.sqrt(2 * model.num_r_vectors) * 2.0 ** (-7 * slices) * np.linalg.norm(colmax, 2)
+    for i in range(k.shape[0]):
+        eo, _, _ = oracle_mod.kpoint_spectrum(model, k[i])
+        assert np.max(np.abs(e[i] - eo)) < max(bound, 1e-11 * max(1.0, np.abs(eo).max()))
 
 
 def test_mesh_weighted_sum_contiguous_and_scattered(engine_cls, oracle_mod):

@@ -1184,6 +1184,53 @@ wnlqg_status wnlqg_b200_eval_mesh_device(wnlqg_plan *pl, const int64_t mesh[3], 
     return WNLQG_OK;
 }
 
+wnlqg_status wnlqg_b200_eval_points_weighted_device(wnlqg_plan *pl, const double *kpoints_device,
+                                                    const double *weights_device, int64_t n, double *out_device,
+                                                    void *stream) {
+    wnlqg_status st = check_plan(pl);
+    if (st != WNLQG_OK) return st;
+    if (pl->nonorth) return fail(WNLQG_ERR_UNSUPPORTED, "responses of nonorthogonal models are not built yet; eval_spectrum is");
+    if (n < 0 || (n > 0 && (!kpoints_device || !weights_device)) || !out_device)
+        return fail(WNLQG_ERR_INVALID_ARGUMENT, "invalid points");
+    WNLQG_CUDA(cudaSetDevice(pl->model->device));
+    cudaStream_t user = static_cast<cudaStream_t>(stream);
+    {
+        cudaEvent_t ev;
+        WNLQG_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        WNLQG_CUDA(cudaEventRecord(ev, user));
+        WNLQG_CUDA(cudaStreamWaitEvent(pl->stream, ev, 0));
+        cudaEventDestroy(ev);
+    }
+    if ((st = record_event(pl, 0)) != WNLQG_OK) return st;
+    pl->launches = 0;
+    WNLQG_CUDA(cudaMemsetAsync(pl->d_partials, 0, (size_t)pl->partial_slots * pl->vc * 4 * sizeof(double), pl->stream));
+    size_t nbatch = 0;
+    for (int64_t s = 0; s < n; s += pl->max_batch, ++nbatch) {
+        const int64_t nb = std::min(pl->max_batch, n - s);
+        const size_t base = 1 + 3 * nbatch;
+        if ((st = record_event(pl, base)) != WNLQG_OK) return st;
+        if ((st = run_front(pl, nb, 0, nullptr, kpoints_device + 3 * s, base)) != WNLQG_OK) return st;
+        if ((st = run_passes(pl, nb, 0, 1.0, 0, weights_device + s)) != WNLQG_OK) return st;
+    }
+    const size_t final_ev = 1 + 3 * nbatch;
+    if ((st = record_event(pl, final_ev)) != WNLQG_OK) return st;
+    reduce_partials_kernel<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((pl->vc + 255) / 256, 1024)), 256, 0,
+                             pl->stream>>>(pl->d_partials, pl->partial_slots, pl->vc, reinterpret_cast<double2 *>(out_device));
+    pl->launches += 1;
+    WNLQG_CUDA(cudaGetLastError());
+    if ((st = record_event(pl, final_ev + 1)) != WNLQG_OK) return st;
+    {
+        cudaEvent_t ev;
+        WNLQG_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        WNLQG_CUDA(cudaEventRecord(ev, pl->stream));
+        WNLQG_CUDA(cudaStreamWaitEvent(user, ev, 0));
+        cudaEventDestroy(ev);
+    }
+    pl->timing_valid = true;
+    pl->timing_batches = nbatch;
+    return WNLQG_OK;
+}
+
 wnlqg_status wnlqg_b200_eval_mesh(wnlqg_plan *pl, const int64_t mesh[3], int64_t k_begin, int64_t k_end, double *out) {
     wnlqg_status st = check_plan(pl);
     if (st != WNLQG_OK) return st;

@@ -102,6 +102,14 @@ class ResponseEngine:
             out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
         return out
 
+    def weighted_sum_device(self, kpoints_ptr: int, weights_ptr: int, n: int, out_device_ptr: int,
+                            stream_ptr: int = 0) -> None:
+        """Asynchronous weighted sum over n device-resident k-points ([n, 3] doubles) and weights,
+        writing value_count complex values to a device pointer."""
+        _lib.check(self._L.wnlqg_b200_eval_points_weighted_device(
+            self._plan, ctypes.c_void_p(kpoints_ptr), ctypes.c_void_p(weights_ptr), int(n),
+            ctypes.c_void_p(out_device_ptr), ctypes.c_void_p(stream_ptr)))
+
     def mesh_weighted_sum(self, mesh: Sequence[int], indices, weights) -> np.ndarray:
         """sum_i weights[i] * value(mesh point indices[i]) from host arrays, complex [value_count]."""
         mesh_a = np.ascontiguousarray(np.asarray(mesh, dtype=np.int64))
