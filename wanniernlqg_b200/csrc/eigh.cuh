@@ -386,6 +386,229 @@ __global__ void jacobi_eigh_f32_kernel(const double2 *__restrict__ h_in, int64_t
     }
 }
 
+// Stage 1, warp form: one warp per matrix, A and V in the warp's own shared memory, so a round
+// synchronises with __syncwarp only.  Each warp walks a contiguous run of the batch; when the
+// batch is a run of consecutive mesh points (warm_start), every point after the first starts
+// from the previous point's eigenvectors as above.  The Hermitian 2x2 block updates of a round
+// take their (k1 <= k2) pair indices from a fixed table (the order w = k2 (k2 + 1) / 2 + k1 is a
+// prefix for every np <= 32); the V <- V J update runs one row per lane.
+__constant__ unsigned char c_jacobi_blocks[136][2];
+
+struct WarpJacobiSmem {
+    // Per warp: A, V (np x ld complex float), rotation sines, cosines and pair indices.
+    static __host__ __device__ size_t per_warp(int nw) {
+        const int np = nw + (nw & 1);
+        const int ld = np + 1;
+        size_t s = 2 * (size_t)np * ld * sizeof(float2) + 16 * (sizeof(float2) + sizeof(float) + 2 * sizeof(int));
+        return (s + 15) & ~(size_t)15;
+    }
+};
+
+// One warp-synchronous parallel-Jacobi sweep (np - 1 rounds); returns true when a rotation was applied.
+WNLQG_D bool warp_jacobi_sweep_f32(float2 *A, float2 *V, int np, int ld, float tol, float2 *rot_s, float *rot_c,
+                                   int *rot_p, int *rot_q, int lane) {
+    const int half = np / 2;
+    const int nblk = half * (half + 1) / 2;
+    bool rotated = false;
+    for (int round = 0; round < np - 1; ++round) {
+        if (lane < half) {
+            const int s1 = lane, s2 = np - 1 - lane;
+            const int i1 = s1 == 0 ? 0 : ((s1 - 1 + round) % (np - 1)) + 1;
+            const int i2 = ((s2 - 1 + round) % (np - 1)) + 1;
+            const int p = min(i1, i2), q = max(i1, i2);
+            const float2 apq = A[p + ld * q];
+            const float g = hypotf(apq.x, apq.y);
+            float c = 1.0f;
+            float2 sp = make_float2(0.0f, 0.0f);
+            if (g > tol) {
+                const float app = A[p + ld * p].x, aqq = A[q + ld * q].x;
+                const float theta = (aqq - app) / (2.0f * g);
+                const float t = (theta >= 0.0f ? 1.0f : -1.0f) / (fabsf(theta) + sqrtf(theta * theta + 1.0f));
+                c = rsqrtf(t * t + 1.0f);
+                const float sn = t * c;
+                sp = make_float2(sn * (apq.x / g), sn * (apq.y / g));
+                rotated = true;
+            }
+            rot_c[lane] = c;
+            rot_s[lane] = sp;
+            rot_p[lane] = p;
+            rot_q[lane] = q;
+        }
+        __syncwarp();
+        for (int w = lane; w < nblk; w += 32) {
+            const int k1 = c_jacobi_blocks[w][0], k2 = c_jacobi_blocks[w][1];
+            const int p1 = rot_p[k1], q1 = rot_q[k1], p2 = rot_p[k2], q2 = rot_q[k2];
+            const float c1 = rot_c[k1], c2 = rot_c[k2];
+            const float2 s1 = rot_s[k1], s2 = rot_s[k2];
+            const float2 s2c = cconj(s2), s1c = cconj(s1);
+            const float2 a00 = A[p1 + ld * p2], a01 = A[p1 + ld * q2], a10 = A[q1 + ld * p2], a11 = A[q1 + ld * q2];
+            const float2 t00 = csub(cscale(a00, c2), cmul(a01, s2c));
+            const float2 t01 = cadd(cmul(a00, s2), cscale(a01, c2));
+            const float2 t10 = csub(cscale(a10, c2), cmul(a11, s2c));
+            const float2 t11 = cadd(cmul(a10, s2), cscale(a11, c2));
+            float2 o00 = csub(cscale(t00, c1), cmul(s1, t10));
+            float2 o01 = csub(cscale(t01, c1), cmul(s1, t11));
+            float2 o10 = cadd(cmul(s1c, t00), cscale(t10, c1));
+            float2 o11 = cadd(cmul(s1c, t01), cscale(t11, c1));
+            if (k1 == k2) {
+                if (s1.x != 0.0f || s1.y != 0.0f) {
+                    o01 = make_float2(0.0f, 0.0f);
+                    o10 = o01;
+                } else {
+                    o10 = cconj(o01);
+                }
+                o00.y = 0.0f;
+                o11.y = 0.0f;
+                A[p1 + ld * p2] = o00; A[p1 + ld * q2] = o01; A[q1 + ld * p2] = o10; A[q1 + ld * q2] = o11;
+            } else {
+                A[p1 + ld * p2] = o00; A[p1 + ld * q2] = o01; A[q1 + ld * p2] = o10; A[q1 + ld * q2] = o11;
+                A[p2 + ld * p1] = cconj(o00); A[q2 + ld * p1] = cconj(o01);
+                A[p2 + ld * q1] = cconj(o10); A[q2 + ld * q1] = cconj(o11);
+            }
+        }
+        if (lane < np) {
+            for (int k = 0; k < half; ++k) {
+                const int p = rot_p[k], q = rot_q[k];
+                const float c = rot_c[k];
+                const float2 sk = rot_s[k], skc = cconj(sk);
+                const float2 vp = V[lane + ld * p], vq = V[lane + ld * q];
+                V[lane + ld * p] = csub(cscale(vp, c), cmul(vq, skc));
+                V[lane + ld * q] = cadd(cmul(vp, sk), cscale(vq, c));
+            }
+        }
+        __syncwarp();
+    }
+    return __any_sync(0xffffffffu, rotated);
+}
+
+// out = op(X) * Y[:, lane] for the warp's np x np shared matrices (op = conjugate transpose when
+// xh): the lane's column of the product, returned in registers (static indices only).
+WNLQG_D void warp_column_product(const float2 *X, const float2 *Y, float2 (&out)[32], int np, int ld, int lane,
+                                 bool xh) {
+#pragma unroll
+    for (int i = 0; i < 32; ++i) out[i] = make_float2(0.0f, 0.0f);
+    if (lane >= np) return;
+    for (int l = 0; l < np; ++l) {
+        const float2 y = Y[l + ld * lane];
+        if (xh) {
+#pragma unroll
+            for (int i = 0; i < 32; ++i)
+                if (i < np) out[i] = cfmaconj(X[l + ld * i], y, out[i]);
+        } else {
+#pragma unroll
+            for (int i = 0; i < 32; ++i)
+                if (i < np) out[i] = cfma(X[i + ld * l], y, out[i]);
+        }
+    }
+}
+
+WNLQG_D void warp_store_column(float2 *M, const float2 (&v)[32], int np, int ld, int lane) {
+    if (lane < np) {
+#pragma unroll
+        for (int i = 0; i < 32; ++i)
+            if (i < np) M[i + ld * lane] = v[i];
+    }
+}
+
+// A <- H(k) from the upper triangle of the stored matrix (lower = conjugate, real diagonal),
+// zero-padded to np; returns the Frobenius norm.
+WNLQG_D double warp_load_hermitian(float2 *A, const double2 *__restrict__ h, int nw, int np, int ld, int lane) {
+    for (int j = 0; j < np; ++j) {
+        double2 v = make_double2(0.0, 0.0);
+        if (lane < nw && j < nw) v = h[lane + (size_t)nw * j];
+        if (lane < np) A[lane + ld * j] = make_float2((float)v.x, (float)v.y);
+    }
+    __syncwarp();
+    if (lane < np)
+        for (int i = lane; i < np; ++i) {
+            if (i > lane) A[i + ld * lane] = cconj(A[lane + ld * i]);
+            else A[i + ld * i].y = 0.0f;
+        }
+    __syncwarp();
+    double local = 0.0;
+    if (lane < np)
+        for (int i = 0; i < np; ++i) {
+            const float2 z = A[i + ld * lane];
+            local += (double)z.x * z.x + (double)z.y * z.y;
+        }
+    for (int o = 16; o > 0; o >>= 1) local += __shfl_xor_sync(0xffffffffu, local, o);
+    return sqrt(local);
+}
+
+__global__ void __launch_bounds__(128) jacobi_f32_warp_kernel(const double2 *__restrict__ h_in, int64_t h_stride,
+                                                              int64_t batch, int nw, float2 *__restrict__ V_out,
+                                                              int warm_start) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int np = nw + (nw & 1);
+    const int ld = np + 1;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned char *base = smraw + (size_t)warp * WarpJacobiSmem::per_warp(nw);
+    float2 *A = reinterpret_cast<float2 *>(base);
+    float2 *V = A + (size_t)np * ld;
+    float2 *rot_s = V + (size_t)np * ld;
+    float *rot_c = reinterpret_cast<float *>(rot_s + 16);
+    int *rot_p = reinterpret_cast<int *>(rot_c + 16);
+    int *rot_q = rot_p + 16;
+    const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
+    const int64_t kb = (batch * gw) / nwarps, ke = (batch * (gw + 1)) / nwarps;
+    float2 col[32];
+    for (int64_t b = kb; b < ke; ++b) {
+        const double2 *h = h_in + b * h_stride;
+        double fro;
+        if (b == kb || !warm_start) {
+            fro = warp_load_hermitian(A, h, nw, np, ld, lane);
+            if (lane < np)
+                for (int i = 0; i < np; ++i) V[i + ld * lane] = make_float2(i == lane ? 1.0f : 0.0f, 0.0f);
+            __syncwarp();
+        } else {
+            // Warm start from the previous point's V: V <- V (3I - V^H V)/2 and A <- V^H H V; the
+            // second factor of every product is read from shared memory (A serves as scratch).
+            warp_column_product(V, V, col, np, ld, lane, true);                // (V^H V)[:, lane]
+#pragma unroll
+            for (int i = 0; i < 32; ++i)
+                col[i] = make_float2((i == lane ? 1.5f : 0.0f) - 0.5f * col[i].x, -0.5f * col[i].y);
+            warp_store_column(A, col, np, ld, lane);                            // A <- M
+            __syncwarp();
+            warp_column_product(V, A, col, np, ld, lane, false);                // (V M)[:, lane]
+            __syncwarp();
+            warp_store_column(V, col, np, ld, lane);
+            fro = warp_load_hermitian(A, h, nw, np, ld, lane);                  // A <- H
+            warp_column_product(A, V, col, np, ld, lane, false);                // (H V)[:, lane]
+            __syncwarp();
+            warp_store_column(A, col, np, ld, lane);                            // A <- H V
+            __syncwarp();
+            warp_column_product(V, A, col, np, ld, lane, true);                 // (V^H H V)[:, lane]
+            __syncwarp();
+            warp_store_column(A, col, np, ld, lane);
+            __syncwarp();
+            if (lane < np)
+                for (int i = lane; i < np; ++i) {
+                    if (i > lane) A[i + ld * lane] = cconj(A[lane + ld * i]);
+                    else A[i + ld * i].y = 0.0f;
+                }
+            __syncwarp();
+        }
+        const float tol32 = (float)(fro * 1.4901161193847656e-08);   // rotate while |a_pq| > 2^-26 ||H||
+        for (int sweep = 0; sweep < WNLQG_JACOBI_MAX_SWEEPS; ++sweep) {
+            double off = 0.0;
+            if (lane < np)
+                for (int i = 0; i < np; ++i)
+                    if (i != lane) {
+                        const float2 z = A[i + ld * lane];
+                        off += (double)z.x * z.x + (double)z.y * z.y;
+                    }
+            for (int o = 16; o > 0; o >>= 1) off += __shfl_xor_sync(0xffffffffu, off, o);
+            if (sqrt(off) <= fro * 2.384185791015625e-07) break;
+            if (!warp_jacobi_sweep_f32(A, V, np, ld, tol32, rot_s, rot_c, rot_p, rot_q, lane)) break;
+        }
+        float2 *vo = V_out + b * (int64_t)np * np;
+        if (lane < np)
+            for (int j = 0; j < np; ++j) vo[lane + (int64_t)np * j] = V[lane + ld * j];
+        __syncwarp();
+    }
+}
+
 // Stage 2: FP64 refinement.  W = V (3I - V^H V)/2 (Newton-Schulz orthonormalisation of the FP32
 // eigenvectors), H' = W^H H W, FP64 Jacobi sweeps on the nearly diagonal H' (usually one), then
 // ascending order and canonical phases.

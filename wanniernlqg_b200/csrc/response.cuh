@@ -254,20 +254,26 @@ WNLQG_D bool any_within(double te, double half, const RespParams &p) {
     return false;
 }
 
-#define RS_OMB 4   // photon energies per thread per pass of the pair loop
+#define RS_OMB 4   // largest number of photon energies per thread per pass of the pair loop
 
-// Frequency contraction of one thread's RS_OMB photon energies over the pair list.
-// KIND 0: Gaussian with the sqrt(200) cutoff (transition screen); 1: Lorentzian; 2: jerk's
-// windowed delta (Gaussian or Lorentzian by `gaussian`).
-template <typename R, typename C, int KIND>
+// Lorentzian weight numerator / (x^2 + w2): a fast reciprocal on the FP32 path, IEEE division
+// on the FP64 path.
+WNLQG_D float lorentz(float num, float den) { return __fdividef(num, den); }
+WNLQG_D double lorentz(double num, double den) { return num / den; }
+
+// Frequency contraction of one thread's OMB photon energies over the pair list, for one or two
+// components (TWO).  KIND 0: Gaussian with the sqrt(200) cutoff (transition screen);
+// 1: Lorentzian; 2: jerk's windowed delta (Gaussian or Lorentzian by `gaussian`).
+template <typename R, typename C, int KIND, int OMB, bool TWO>
 WNLQG_D void contract_pairs(const double *ste, const double *sfnm, const C *Q0, const C *Q1, int npairs,
                             const double *om, C (*acc)[2], R gsc, R cut, R invw, R w2, R lor, R win, int gaussian) {
     for (int q = 0; q < npairs; ++q) {
         const double te = ste[q];
         const R fq = (R)sfnm[q];
-        const C q0 = Q0[q], q1 = Q1[q];
+        const C q0 = Q0[q];
+        const C q1 = TWO ? Q1[q] : q0;
 #pragma unroll
-        for (int j = 0; j < RS_OMB; ++j) {
+        for (int j = 0; j < OMB; ++j) {
             const R x = (R)(te - om[j]);
             R delta;
             if (KIND == 0) {
@@ -275,20 +281,33 @@ WNLQG_D void contract_pairs(const double *ste, const double *sfnm, const C *Q0, 
                 const R y = x * invw;
                 delta = gsc * exp(-y * y);
             } else if (KIND == 1) {
-                delta = lor / (x * x + w2);
+                delta = lorentz(lor, x * x + w2);
             } else {
                 if (win > (R)0 && fabs(x) > win) continue;
                 const R y = x * invw;
-                delta = gaussian ? gsc * exp(-y * y) : lor / (x * x + w2);
+                delta = gaussian ? gsc * exp(-y * y) : lorentz(lor, x * x + w2);
             }
             const R weight = fq * delta;
-            if (weight == (R)0) continue;
             acc[j][0].x = fma(weight, q0.x, acc[j][0].x);
             acc[j][0].y = fma(weight, q0.y, acc[j][0].y);
-            acc[j][1].x = fma(weight, q1.x, acc[j][1].x);
-            acc[j][1].y = fma(weight, q1.y, acc[j][1].y);
+            if (TWO) {
+                acc[j][1].x = fma(weight, q1.x, acc[j][1].x);
+                acc[j][1].y = fma(weight, q1.y, acc[j][1].y);
+            }
         }
     }
+}
+
+template <typename R, typename C, int OMB, bool TWO>
+WNLQG_D void contract_dispatch(int pair_mode, int gaussian, const double *ste, const double *sfnm, const C *Q0,
+                               const C *Q1, int npairs, const double *om, C (*acc)[2], R gsc, R cut, R invw, R w2,
+                               R lor, R win) {
+    if (pair_mode == 1)
+        contract_pairs<R, C, 2, OMB, TWO>(ste, sfnm, Q0, Q1, npairs, om, acc, gsc, cut, invw, w2, lor, win, gaussian);
+    else if (gaussian)
+        contract_pairs<R, C, 0, OMB, TWO>(ste, sfnm, Q0, Q1, npairs, om, acc, gsc, cut, invw, w2, lor, win, 1);
+    else
+        contract_pairs<R, C, 1, OMB, TWO>(ste, sfnm, Q0, Q1, npairs, om, acc, gsc, cut, invw, w2, lor, win, 0);
 }
 
 // R: storage/arithmetic type of the per-k matrices (double: plain FP64 path; float: mixed path).
@@ -636,17 +655,20 @@ __global__ void __launch_bounds__(256) response_kernel(RespParams p) {
             }
             const int npairs = ired[0];
             const bool active = ired[1] != 0;
-            // Frequency contraction: each thread owns up to RS_OMB photon energies per pass and
-            // streams the pair list once per pass.
+            // Frequency contraction: each thread owns OMB photon energies per pass (OMB = 1, 2 or 4,
+            // the fewest that cover the energy axis with the CTA's threads) and streams the pair list
+            // once per pass; threads past the end of the axis skip the pass.
             const R w2 = (R)(p.width * p.width), lor = (R)(p.width / WNLQG_PI);
             const R gsc = (R)p.gscale, cut = (R)p.cutoff, invw = (R)(1.0 / p.width);
             const R win = (R)(p.thr > 0.0 ? p.thr : 0.0);
-            for (int w0 = 0; w0 < p.nom; w0 += RS_OMB * blockDim.x) {
+            const int omb = p.nom <= (int)blockDim.x ? 1 : (p.nom <= 2 * (int)blockDim.x ? 2 : RS_OMB);
+            for (int w0 = 0; w0 < p.nom; w0 += omb * blockDim.x) {
+                if (w0 + (int)threadIdx.x >= p.nom) continue;
                 double om[RS_OMB];
 #pragma unroll
                 for (int j = 0; j < RS_OMB; ++j) {
                     const int w = w0 + threadIdx.x + j * blockDim.x;
-                    om[j] = w < p.nom ? p.omegas[w] : 0.0;
+                    om[j] = (j < omb && w < p.nom) ? p.omegas[w] : 0.0;
                 }
                 // Components in chunks of two keep the accumulators in registers.
                 for (int c0 = 0; c0 < p.n_fc; c0 += 2) {
@@ -657,18 +679,21 @@ __global__ void __launch_bounds__(256) response_kernel(RespParams p) {
                     if (active) {
                         const C *Q0 = sQ + (size_t)c0 * nn;
                         const C *Q1 = sQ + (size_t)(two ? c0 + 1 : c0) * nn;
-                        // The delta kind is fixed per pass: one specialised loop each.
-                        if (p.pair_mode == 1)
-                            contract_pairs<R, C, 2>(ste, sfnm, Q0, Q1, npairs, om, acc, gsc, cut, invw, w2, lor, win, p.gaussian);
-                        else if (p.gaussian)
-                            contract_pairs<R, C, 0>(ste, sfnm, Q0, Q1, npairs, om, acc, gsc, cut, invw, w2, lor, win, 1);
-                        else
-                            contract_pairs<R, C, 1>(ste, sfnm, Q0, Q1, npairs, om, acc, gsc, cut, invw, w2, lor, win, 0);
+                        if (omb == 1) {
+                            if (two) contract_dispatch<R, C, 1, true>(p.pair_mode, p.gaussian, ste, sfnm, Q0, Q1, npairs, om, acc, gsc, cut, invw, w2, lor, win);
+                            else contract_dispatch<R, C, 1, false>(p.pair_mode, p.gaussian, ste, sfnm, Q0, Q1, npairs, om, acc, gsc, cut, invw, w2, lor, win);
+                        } else if (omb == 2) {
+                            if (two) contract_dispatch<R, C, 2, true>(p.pair_mode, p.gaussian, ste, sfnm, Q0, Q1, npairs, om, acc, gsc, cut, invw, w2, lor, win);
+                            else contract_dispatch<R, C, 2, false>(p.pair_mode, p.gaussian, ste, sfnm, Q0, Q1, npairs, om, acc, gsc, cut, invw, w2, lor, win);
+                        } else {
+                            if (two) contract_dispatch<R, C, RS_OMB, true>(p.pair_mode, p.gaussian, ste, sfnm, Q0, Q1, npairs, om, acc, gsc, cut, invw, w2, lor, win);
+                            else contract_dispatch<R, C, RS_OMB, false>(p.pair_mode, p.gaussian, ste, sfnm, Q0, Q1, npairs, om, acc, gsc, cut, invw, w2, lor, win);
+                        }
                     }
 #pragma unroll
                     for (int j = 0; j < RS_OMB; ++j) {
                         const int w = w0 + threadIdx.x + j * blockDim.x;
-                        if (w >= p.nom) continue;
+                        if (j >= omb || w >= p.nom) continue;
 #pragma unroll
                         for (int cc = 0; cc < 2; ++cc) {
                             if (cc == 1 && !two) continue;

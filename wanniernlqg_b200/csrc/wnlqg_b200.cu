@@ -637,10 +637,12 @@ wnlqg_status run_front(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const int64_
             pl->d_U, pl->d_status);
     } else if (pl->task.precision == WNLQG_PRECISION_MIXED) {
         int per_sm = 1;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jacobi_eigh_f32_kernel, pl->eigh_threads, pl->eigh_smem);
-        const int64_t f32_grid = std::min<int64_t>(nb, (int64_t)std::max(1, per_sm) * pl->sm_count);
-        jacobi_eigh_f32_kernel<<<(unsigned)f32_grid, pl->eigh_threads, pl->eigh_smem, pl->stream>>>(
-            pl->d_xw + (int64_t)pl->ch_H * pl->nn, N, nb, pl->nw, pl->d_V32);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jacobi_f32_warp_kernel, 128, pl->eigh_smem);
+        const int64_t f32_grid = std::min<int64_t>((nb + 3) / 4, (int64_t)std::max(1, per_sm) * pl->sm_count);
+        // Consecutive mesh points are neighbours: warm-start the Jacobi iteration along the run.
+        const int warm = (mesh != nullptr && kpts_device == nullptr && kidx_device == nullptr) ? 1 : 0;
+        jacobi_f32_warp_kernel<<<(unsigned)f32_grid, 128, pl->eigh_smem, pl->stream>>>(
+            pl->d_xw + (int64_t)pl->ch_H * pl->nn, N, nb, pl->nw, pl->d_V32, warm);
         eigh_refine_f64_kernel<<<(unsigned)nb, pl->refine_threads, pl->refine_smem, pl->stream>>>(
             pl->d_xw + (int64_t)pl->ch_H * pl->nn, N, pl->d_V32, nb, pl->nw, pl->d_E, pl->d_U);
         pl->launches += 1;
@@ -1088,8 +1090,18 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
         if (e != cudaSuccess) return bail(fail(WNLQG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e)));
     } else if (t.precision == WNLQG_PRECISION_MIXED) {
         const int np = nw + (nw & 1);
-        pl->eigh_smem = EighF32Smem::bytes(nw);
+        pl->eigh_smem = 4 * WarpJacobiSmem::per_warp(nw);
         pl->refine_smem = EighRefineSmem::bytes(nw);
+        {
+            // Pair-block table of the warp Jacobi: w = k2 (k2 + 1) / 2 + k1, k1 <= k2 < 16.
+            unsigned char tab[136][2];
+            for (int k2 = 0, w = 0; k2 < 16; ++k2)
+                for (int k1 = 0; k1 <= k2; ++k1, ++w) { tab[w][0] = (unsigned char)k1; tab[w][1] = (unsigned char)k2; }
+            WNLQG_CUDA(cudaMemcpyToSymbol(c_jacobi_blocks, tab, sizeof(tab)));
+            cudaError_t ea = cudaFuncSetAttribute(jacobi_f32_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                  (int)std::max<size_t>(pl->eigh_smem, 48 * 1024));
+            if (ea != cudaSuccess) return bail(fail(WNLQG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(ea)));
+        }
         // Both stages need blockDim >= np/2 (pairs) and 8 * blockDim >= np^2 (register-staged products).
         pl->refine_threads = std::max(32, std::min(256, ((np * np / 8 + 31) / 32) * 32));
         pl->refine_threads = std::max(pl->refine_threads, ((np / 2 + 31) / 32) * 32);
