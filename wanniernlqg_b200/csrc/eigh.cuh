@@ -230,168 +230,18 @@ __global__ void jacobi_eigh_kernel(const double2 *__restrict__ h_in, int64_t h_s
 }
 
 // ---------------------------------------------------------------------------------------------
-// Mixed-precision eigensolver: FP32 parallel Jacobi to FP32 accuracy, then one FP64
-// Rayleigh-Ritz refinement: H' = V^H H V in FP64 (V the FP32 eigenvectors promoted) followed
-// by FP64 Jacobi sweeps on the nearly diagonal H' (quadratic convergence: one sweep takes the
-// 1e-7 off-diagonal to rounding level, a second is taken only if needed), U = V J.
-// The A update is Hermitian-aware: only blocks k1 <= k2 are computed and the conjugate block is
-// mirrored.  A sweep stops the iteration once the off-diagonal Frobenius norm is below tol.
+// Mixed-precision eigensolver, one warp per matrix in two kernels:
+//   stage 1 (jacobi_f32_warp_kernel): FP32 parallel Jacobi until the off-diagonal norm is below
+//     2^-17 ||H||, warm-started along runs of consecutive mesh points from the previous point's
+//     eigenvectors (V <- V (3I - V^H V)/2, A <- V^H H V);
+//   stage 2 (eigh_refine_f64_warp_kernel): FP64 Rayleigh-Ritz refinement, W = second-order
+//     Loewdin orthonormalisation of V, H' = W^H H W, one FP64 Jacobi sweep (quadratic
+//     convergence), U = W J, ascending order and canonical phases.
+// A and V sit in the warp's own shared memory, so a round synchronises with __syncwarp only.
+// The Hermitian 2x2 block updates of a round take their (k1 <= k2) pair indices from a fixed
+// table (the order w = k2 (k2 + 1) / 2 + k1 is a prefix for every np <= 32); V <- V J runs one
+// row per lane.
 // ---------------------------------------------------------------------------------------------
-
-// out = op(X) * Y in FP64 for np x np shared matrices (op = conjugate transpose when xh), with
-// every thread's results held in registers until all reads are done, so out may alias X or Y.
-// Needs blockDim.x * 8 >= np*np.
-WNLQG_D void small_product(const double2 *X, const double2 *Y, double2 *out, int np, int ld, bool xh) {
-    const int nel = np * np;
-    double2 tv[8];
-#pragma unroll
-    for (int r = 0; r < 8; ++r) {
-        const int e = threadIdx.x + r * blockDim.x;
-        double2 acc = make_double2(0.0, 0.0);
-        if (e < nel) {
-            const int i = e % np, j = e / np;
-            if (xh)
-                for (int l = 0; l < np; ++l) acc = cfmaconj(X[l + ld * i], Y[l + ld * j], acc);
-            else
-                for (int l = 0; l < np; ++l) acc = cfma(X[i + ld * l], Y[l + ld * j], acc);
-        }
-        tv[r] = acc;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int r = 0; r < 8; ++r) {
-        const int e = threadIdx.x + r * blockDim.x;
-        if (e < nel) out[(e % np) + ld * (e / np)] = tv[r];
-    }
-    __syncthreads();
-}
-
-// Stage 1 of the mixed eigensolver: FP32 parallel Jacobi.  Each CTA walks a contiguous run of
-// the batch.  Consecutive mesh indices are neighbouring k-points (periodically), so from the
-// second point on the Jacobi iteration starts from the previous point's eigenvectors V: V is
-// re-orthonormalised (first-order Loewdin, V <- V (3I - V^H V)/2) and A = V^H H V is then nearly
-// diagonal, which cuts the sweeps needed to reach FP32 accuracy.  Writes the FP32 eigenvector
-// estimate V [b][np][np] to global memory.
-struct EighF32Smem {
-    static __host__ __device__ size_t bytes(int nw) {
-        int np = nw + (nw & 1);
-        int ld = np + 1;
-        return 3 * (size_t)np * ld * sizeof(float2) + (size_t)(np / 2) * (sizeof(float2) + sizeof(float) + 2 * sizeof(int)) + 64;
-    }
-};
-
-// out = op(X) * Y for np x np FP32 shared matrices, results staged in registers (out may alias).
-// Needs blockDim.x * 8 >= np*np.
-WNLQG_D void small_product_f32(const float2 *X, const float2 *Y, float2 *out, int np, int ld, bool xh) {
-    const int nel = np * np;
-    float2 tv[8];
-#pragma unroll
-    for (int r = 0; r < 8; ++r) {
-        const int e = threadIdx.x + r * blockDim.x;
-        float2 acc = make_float2(0.f, 0.f);
-        if (e < nel) {
-            const int i = e % np, j = e / np;
-            if (xh)
-                for (int l = 0; l < np; ++l) acc = cfmaconj(X[l + ld * i], Y[l + ld * j], acc);
-            else
-                for (int l = 0; l < np; ++l) acc = cfma(X[i + ld * l], Y[l + ld * j], acc);
-        }
-        tv[r] = acc;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int r = 0; r < 8; ++r) {
-        const int e = threadIdx.x + r * blockDim.x;
-        if (e < nel) out[(e % np) + ld * (e / np)] = tv[r];
-    }
-    __syncthreads();
-}
-
-__global__ void jacobi_eigh_f32_kernel(const double2 *__restrict__ h_in, int64_t h_stride, int64_t batch, int nw,
-                                       float2 *__restrict__ V_out) {
-    extern __shared__ __align__(16) unsigned char smraw[];
-    const int np = nw + (nw & 1);
-    const int ld = np + 1;
-    const int half = np / 2;
-    float2 *A32 = reinterpret_cast<float2 *>(smraw);
-    float2 *V32 = A32 + (size_t)np * ld;
-    float2 *T32 = V32 + (size_t)np * ld;
-    float2 *rot_s = T32 + (size_t)np * ld;
-    float *rot_c = reinterpret_cast<float *>(rot_s + half);
-    int *rot_p = reinterpret_cast<int *>(rot_c + half);
-    int *rot_q = rot_p + half;
-    __shared__ double red[48];
-    __shared__ int rot_flag;
-    const int tid = threadIdx.x;
-    const int64_t kb = (batch * blockIdx.x) / gridDim.x;
-    const int64_t ke = (batch * (blockIdx.x + 1)) / gridDim.x;
-    for (int64_t b = kb; b < ke; ++b) {
-        const bool warm = b > kb;
-        const double2 *h = h_in + b * h_stride;
-        double local = 0.0;
-        for (int e = tid; e < np * np; e += blockDim.x) {
-            const int i = e % np, j = e / np;
-            double2 v = make_double2(0.0, 0.0);
-            if (i < nw && j < nw) {
-                if (i < j) v = h[i + (size_t)nw * j];
-                else if (i > j) v = cconj(h[j + (size_t)nw * i]);
-                else v = make_double2(h[i + (size_t)nw * i].x, 0.0);
-            }
-            local += v.x * v.x + v.y * v.y;
-            A32[i + ld * j] = make_float2((float)v.x, (float)v.y);
-            if (!warm) V32[i + ld * j] = make_float2(i == j ? 1.0f : 0.0f, 0.0f);
-        }
-        for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xffffffffu, local, o);
-        if ((tid & 31) == 0) red[tid >> 5] = local;
-        __syncthreads();
-        if (tid == 0) {
-            double sum = 0.0;
-            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) sum += red[w];
-            red[41] = sqrt(sum);
-        }
-        __syncthreads();
-        const double fro = red[41];
-        if (warm) {
-            // V <- V (3I - V^H V)/2, then A <- V^H H V.
-            small_product_f32(V32, V32, T32, np, ld, true);
-            for (int e = tid; e < np * np; e += blockDim.x) {
-                const int i = e % np, j = e / np;
-                const float2 v = T32[i + ld * j];
-                T32[i + ld * j] = make_float2((i == j ? 1.5f : 0.0f) - 0.5f * v.x, -0.5f * v.y);
-            }
-            __syncthreads();
-            small_product_f32(V32, T32, V32, np, ld, false);
-            small_product_f32(A32, V32, T32, np, ld, false);
-            small_product_f32(V32, T32, A32, np, ld, true);
-            for (int e = tid; e < np * np; e += blockDim.x) {
-                const int i = e % np, j = e / np;
-                if (i > j) A32[i + ld * j] = cconj(A32[j + ld * i]);
-                if (i == j) A32[i + ld * i].y = 0.0f;
-            }
-            __syncthreads();
-        }
-        const float tol32 = (float)(fro * 1.4901161193847656e-08);   // rotate while |a_pq| > 2^-26 ||H||
-        for (int sweep = 0; sweep < WNLQG_JACOBI_MAX_SWEEPS; ++sweep) {
-            if (offdiag_norm(A32, np, ld, red) <= fro * 2.384185791015625e-07) break;
-            if (tid == 0) rot_flag = 0;
-            __syncthreads();
-            jacobi_sweep<float>(A32, V32, np, ld, tol32, rot_s, rot_c, rot_p, rot_q, &rot_flag);
-            const int any = rot_flag;
-            __syncthreads();
-            if (!any) break;
-        }
-        float2 *vo = V_out + b * (int64_t)np * np;
-        for (int e = tid; e < np * np; e += blockDim.x) vo[e] = V32[(e % np) + ld * (e / np)];
-        __syncthreads();
-    }
-}
-
-// Stage 1, warp form: one warp per matrix, A and V in the warp's own shared memory, so a round
-// synchronises with __syncwarp only.  Each warp walks a contiguous run of the batch; when the
-// batch is a run of consecutive mesh points (warm_start), every point after the first starts
-// from the previous point's eigenvectors as above.  The Hermitian 2x2 block updates of a round
-// take their (k1 <= k2) pair indices from a fixed table (the order w = k2 (k2 + 1) / 2 + k1 is a
-// prefix for every np <= 32); the V <- V J update runs one row per lane.
 __constant__ unsigned char c_jacobi_blocks[136][2];
 
 struct WarpJacobiSmem {
@@ -405,8 +255,13 @@ struct WarpJacobiSmem {
 };
 
 // One warp-synchronous parallel-Jacobi sweep (np - 1 rounds); returns true when a rotation was applied.
-WNLQG_D bool warp_jacobi_sweep_f32(float2 *A, float2 *V, int np, int ld, float tol, float2 *rot_s, float *rot_c,
-                                   int *rot_p, int *rot_q, int lane) {
+WNLQG_D float recip_sqrt(float x) { return rsqrtf(x); }
+WNLQG_D double recip_sqrt(double x) { return 1.0 / sqrt(x); }
+
+template <typename T>
+WNLQG_D bool warp_jacobi_sweep(typename cplx_of<T>::type *A, typename cplx_of<T>::type *V, int np, int ld, T tol,
+                               typename cplx_of<T>::type *rot_s, T *rot_c, int *rot_p, int *rot_q, int lane) {
+    typedef typename cplx_of<T>::type C;
     const int half = np / 2;
     const int nblk = half * (half + 1) / 2;
     bool rotated = false;
@@ -416,17 +271,18 @@ WNLQG_D bool warp_jacobi_sweep_f32(float2 *A, float2 *V, int np, int ld, float t
             const int i1 = s1 == 0 ? 0 : ((s1 - 1 + round) % (np - 1)) + 1;
             const int i2 = ((s2 - 1 + round) % (np - 1)) + 1;
             const int p = min(i1, i2), q = max(i1, i2);
-            const float2 apq = A[p + ld * q];
-            const float g = hypotf(apq.x, apq.y);
-            float c = 1.0f;
-            float2 sp = make_float2(0.0f, 0.0f);
+            const C apq = A[p + ld * q];
+            const T g = hypot(apq.x, apq.y);
+            T c = (T)1;
+            C sp = czero<C>();
             if (g > tol) {
-                const float app = A[p + ld * p].x, aqq = A[q + ld * q].x;
-                const float theta = (aqq - app) / (2.0f * g);
-                const float t = (theta >= 0.0f ? 1.0f : -1.0f) / (fabsf(theta) + sqrtf(theta * theta + 1.0f));
-                c = rsqrtf(t * t + 1.0f);
-                const float sn = t * c;
-                sp = make_float2(sn * (apq.x / g), sn * (apq.y / g));
+                const T app = A[p + ld * p].x, aqq = A[q + ld * q].x;
+                const T theta = (aqq - app) / ((T)2 * g);
+                const T t = (theta >= (T)0 ? (T)1 : (T)-1) / (fabs(theta) + sqrt(theta * theta + (T)1));
+                c = recip_sqrt(t * t + (T)1);
+                const T sn = t * c;
+                sp.x = sn * (apq.x / g);
+                sp.y = sn * (apq.y / g);
                 rotated = true;
             }
             rot_c[lane] = c;
@@ -438,27 +294,27 @@ WNLQG_D bool warp_jacobi_sweep_f32(float2 *A, float2 *V, int np, int ld, float t
         for (int w = lane; w < nblk; w += 32) {
             const int k1 = c_jacobi_blocks[w][0], k2 = c_jacobi_blocks[w][1];
             const int p1 = rot_p[k1], q1 = rot_q[k1], p2 = rot_p[k2], q2 = rot_q[k2];
-            const float c1 = rot_c[k1], c2 = rot_c[k2];
-            const float2 s1 = rot_s[k1], s2 = rot_s[k2];
-            const float2 s2c = cconj(s2), s1c = cconj(s1);
-            const float2 a00 = A[p1 + ld * p2], a01 = A[p1 + ld * q2], a10 = A[q1 + ld * p2], a11 = A[q1 + ld * q2];
-            const float2 t00 = csub(cscale(a00, c2), cmul(a01, s2c));
-            const float2 t01 = cadd(cmul(a00, s2), cscale(a01, c2));
-            const float2 t10 = csub(cscale(a10, c2), cmul(a11, s2c));
-            const float2 t11 = cadd(cmul(a10, s2), cscale(a11, c2));
-            float2 o00 = csub(cscale(t00, c1), cmul(s1, t10));
-            float2 o01 = csub(cscale(t01, c1), cmul(s1, t11));
-            float2 o10 = cadd(cmul(s1c, t00), cscale(t10, c1));
-            float2 o11 = cadd(cmul(s1c, t01), cscale(t11, c1));
+            const T c1 = rot_c[k1], c2 = rot_c[k2];
+            const C s1 = rot_s[k1], s2 = rot_s[k2];
+            const C s2c = cconj(s2), s1c = cconj(s1);
+            const C a00 = A[p1 + ld * p2], a01 = A[p1 + ld * q2], a10 = A[q1 + ld * p2], a11 = A[q1 + ld * q2];
+            const C t00 = csub(cscale(a00, c2), cmul(a01, s2c));
+            const C t01 = cadd(cmul(a00, s2), cscale(a01, c2));
+            const C t10 = csub(cscale(a10, c2), cmul(a11, s2c));
+            const C t11 = cadd(cmul(a10, s2), cscale(a11, c2));
+            C o00 = csub(cscale(t00, c1), cmul(s1, t10));
+            C o01 = csub(cscale(t01, c1), cmul(s1, t11));
+            C o10 = cadd(cmul(s1c, t00), cscale(t10, c1));
+            C o11 = cadd(cmul(s1c, t01), cscale(t11, c1));
             if (k1 == k2) {
-                if (s1.x != 0.0f || s1.y != 0.0f) {
-                    o01 = make_float2(0.0f, 0.0f);
+                if (s1.x != (T)0 || s1.y != (T)0) {
+                    o01 = czero<C>();
                     o10 = o01;
                 } else {
                     o10 = cconj(o01);
                 }
-                o00.y = 0.0f;
-                o11.y = 0.0f;
+                o00.y = (T)0;
+                o11.y = (T)0;
                 A[p1 + ld * p2] = o00; A[p1 + ld * q2] = o01; A[q1 + ld * p2] = o10; A[q1 + ld * q2] = o11;
             } else {
                 A[p1 + ld * p2] = o00; A[p1 + ld * q2] = o01; A[q1 + ld * p2] = o10; A[q1 + ld * q2] = o11;
@@ -469,9 +325,9 @@ WNLQG_D bool warp_jacobi_sweep_f32(float2 *A, float2 *V, int np, int ld, float t
         if (lane < np) {
             for (int k = 0; k < half; ++k) {
                 const int p = rot_p[k], q = rot_q[k];
-                const float c = rot_c[k];
-                const float2 sk = rot_s[k], skc = cconj(sk);
-                const float2 vp = V[lane + ld * p], vq = V[lane + ld * q];
+                const T c = rot_c[k];
+                const C sk = rot_s[k], skc = cconj(sk);
+                const C vp = V[lane + ld * p], vq = V[lane + ld * q];
                 V[lane + ld * p] = csub(cscale(vp, c), cmul(vq, skc));
                 V[lane + ld * q] = cadd(cmul(vp, sk), cscale(vq, c));
             }
@@ -483,13 +339,13 @@ WNLQG_D bool warp_jacobi_sweep_f32(float2 *A, float2 *V, int np, int ld, float t
 
 // out = op(X) * Y[:, lane] for the warp's np x np shared matrices (op = conjugate transpose when
 // xh): the lane's column of the product, returned in registers (static indices only).
-WNLQG_D void warp_column_product(const float2 *X, const float2 *Y, float2 (&out)[32], int np, int ld, int lane,
-                                 bool xh) {
+template <typename C>
+WNLQG_D void warp_column_product(const C *X, const C *Y, C (&out)[32], int np, int ld, int lane, bool xh) {
 #pragma unroll
-    for (int i = 0; i < 32; ++i) out[i] = make_float2(0.0f, 0.0f);
+    for (int i = 0; i < 32; ++i) out[i] = czero<C>();
     if (lane >= np) return;
     for (int l = 0; l < np; ++l) {
-        const float2 y = Y[l + ld * lane];
+        const C y = Y[l + ld * lane];
         if (xh) {
 #pragma unroll
             for (int i = 0; i < 32; ++i)
@@ -502,7 +358,7 @@ WNLQG_D void warp_column_product(const float2 *X, const float2 *Y, float2 (&out)
     }
 }
 
-WNLQG_D void warp_store_column(float2 *M, const float2 (&v)[32], int np, int ld, int lane) {
+template <typename C> WNLQG_D void warp_store_column(C *M, const C (&v)[32], int np, int ld, int lane) {
     if (lane < np) {
 #pragma unroll
         for (int i = 0; i < 32; ++i)
@@ -512,23 +368,24 @@ WNLQG_D void warp_store_column(float2 *M, const float2 (&v)[32], int np, int ld,
 
 // A <- H(k) from the upper triangle of the stored matrix (lower = conjugate, real diagonal),
 // zero-padded to np; returns the Frobenius norm.
-WNLQG_D double warp_load_hermitian(float2 *A, const double2 *__restrict__ h, int nw, int np, int ld, int lane) {
+template <typename C>
+WNLQG_D double warp_load_hermitian(C *A, const double2 *__restrict__ h, int nw, int np, int ld, int lane) {
     for (int j = 0; j < np; ++j) {
         double2 v = make_double2(0.0, 0.0);
         if (lane < nw && j < nw) v = h[lane + (size_t)nw * j];
-        if (lane < np) A[lane + ld * j] = make_float2((float)v.x, (float)v.y);
+        if (lane < np) A[lane + ld * j] = from_c64<C>(v);
     }
     __syncwarp();
     if (lane < np)
         for (int i = lane; i < np; ++i) {
             if (i > lane) A[i + ld * lane] = cconj(A[lane + ld * i]);
-            else A[i + ld * i].y = 0.0f;
+            else A[i + ld * i].y = 0;
         }
     __syncwarp();
     double local = 0.0;
     if (lane < np)
         for (int i = 0; i < np; ++i) {
-            const float2 z = A[i + ld * lane];
+            const C z = A[i + ld * lane];
             local += (double)z.x * z.x + (double)z.y * z.y;
         }
     for (int o = 16; o > 0; o >>= 1) local += __shfl_xor_sync(0xffffffffu, local, o);
@@ -589,7 +446,9 @@ __global__ void __launch_bounds__(128) jacobi_f32_warp_kernel(const double2 *__r
                 }
             __syncwarp();
         }
-        const float tol32 = (float)(fro * 1.4901161193847656e-08);   // rotate while |a_pq| > 2^-26 ||H||
+        // The FP64 stage converges quadratically from here: the FP32 stage stops once the
+        // off-diagonal norm is below 2^-17 ||H|| (rotating elements above 2^-20 ||H||).
+        const float tol32 = (float)(fro * 9.5367431640625e-07);
         for (int sweep = 0; sweep < WNLQG_JACOBI_MAX_SWEEPS; ++sweep) {
             double off = 0.0;
             if (lane < np)
@@ -599,8 +458,8 @@ __global__ void __launch_bounds__(128) jacobi_f32_warp_kernel(const double2 *__r
                         off += (double)z.x * z.x + (double)z.y * z.y;
                     }
             for (int o = 16; o > 0; o >>= 1) off += __shfl_xor_sync(0xffffffffu, off, o);
-            if (sqrt(off) <= fro * 2.384185791015625e-07) break;
-            if (!warp_jacobi_sweep_f32(A, V, np, ld, tol32, rot_s, rot_c, rot_p, rot_q, lane)) break;
+            if (sqrt(off) <= fro * 7.62939453125e-06) break;
+            if (!warp_jacobi_sweep<float>(A, V, np, ld, tol32, rot_s, rot_c, rot_p, rot_q, lane)) break;
         }
         float2 *vo = V_out + b * (int64_t)np * np;
         if (lane < np)
@@ -609,146 +468,115 @@ __global__ void __launch_bounds__(128) jacobi_f32_warp_kernel(const double2 *__r
     }
 }
 
-// Stage 2: FP64 refinement.  W = V (3I - V^H V)/2 (Newton-Schulz orthonormalisation of the FP32
-// eigenvectors), H' = W^H H W, FP64 Jacobi sweeps on the nearly diagonal H' (usually one), then
-// ascending order and canonical phases.
-struct EighRefineSmem {
-    static __host__ __device__ size_t bytes(int nw) {
-        int np = nw + (nw & 1);
-        int ld = np + 1;
-        return 2 * (size_t)np * ld * sizeof(double2) + (size_t)(np / 2) * (sizeof(double2) + sizeof(double) + 2 * sizeof(int)) + 64;
+// Stage 2, warp form: one warp per matrix, FP64 A and W in the warp's shared memory.
+// W = V (I - E/2 + 3E^2/8) with E = V^H V - I (second-order Loewdin), H' = W^H H W, one FP64
+// Jacobi sweep on H' (quadratic convergence: the off-diagonal goes from the FP32 stage's
+// 2^-17 ||H|| to the square of that over the gap), then ascending order and canonical phases.
+struct WarpRefineSmem {
+    static __host__ __device__ size_t per_warp(int nw) {
+        const int np = nw + (nw & 1);
+        const int ld = np + 1;
+        size_t s = 2 * (size_t)np * ld * sizeof(double2) + 16 * (sizeof(double2) + sizeof(double) + 2 * sizeof(int)) +
+                   32 * (sizeof(double2) + sizeof(int));
+        return (s + 15) & ~(size_t)15;
     }
 };
 
-__global__ void eigh_refine_f64_kernel(const double2 *__restrict__ h_in, int64_t h_stride, const float2 *__restrict__ V_in,
-                                       int64_t batch, int nw, double *__restrict__ E_out, double2 *__restrict__ U_out) {
+__global__ void __launch_bounds__(64) eigh_refine_f64_warp_kernel(const double2 *__restrict__ h_in, int64_t h_stride,
+                                                                  const float2 *__restrict__ V_in, int64_t batch, int nw,
+                                                                  double *__restrict__ E_out, double2 *__restrict__ U_out) {
     extern __shared__ __align__(16) unsigned char smraw[];
     const int np = nw + (nw & 1);
     const int ld = np + 1;
-    const int half = np / 2;
-    double2 *A64 = reinterpret_cast<double2 *>(smraw);
-    double2 *V64 = A64 + (size_t)np * ld;
-    double2 *rot_s = V64 + (size_t)np * ld;
-    double *rot_c = reinterpret_cast<double *>(rot_s + half);
-    int *rot_p = reinterpret_cast<int *>(rot_c + half);
-    int *rot_q = rot_p + half;
-    __shared__ double red[48];
-    __shared__ int rot_flag;
-    const int tid = threadIdx.x;
-    for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) {
-        const double2 *h = h_in + b * h_stride;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned char *base = smraw + (size_t)warp * WarpRefineSmem::per_warp(nw);
+    double2 *A = reinterpret_cast<double2 *>(base);
+    double2 *W = A + (size_t)np * ld;
+    double2 *rot_s = W + (size_t)np * ld;
+    double2 *phase = rot_s + 16;
+    double *rot_c = reinterpret_cast<double *>(phase + 32);
+    int *rot_p = reinterpret_cast<int *>(rot_c + 16);
+    int *rot_q = rot_p + 16;
+    int *rank = rot_q + 16;
+    const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    double2 col[32];
+    for (int64_t b = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp; b < batch; b += nwarps) {
         const float2 *vi = V_in + b * (int64_t)np * np;
-        double local = 0.0;
-        for (int e = tid; e < np * np; e += blockDim.x) {
-            const int i = e % np, j = e / np;
-            double2 v = make_double2(0.0, 0.0);
-            if (i < nw && j < nw) {
-                if (i < j) v = h[i + (size_t)nw * j];
-                else if (i > j) v = cconj(h[j + (size_t)nw * i]);
-                else v = make_double2(h[i + (size_t)nw * i].x, 0.0);
-            }
-            local += v.x * v.x + v.y * v.y;
-            A64[i + ld * j] = v;
-            V64[i + ld * j] = to_c64(vi[e]);
-        }
-        for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xffffffffu, local, o);
-        if ((tid & 31) == 0) red[tid >> 5] = local;
-        __syncthreads();
-        if (tid == 0) {
-            double sum = 0.0;
-            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) sum += red[w];
-            red[41] = sqrt(sum);
-        }
-        __syncthreads();
-        const double fro = red[41];
-        // Loewdin orthonormalisation to second order: E = V^H V - I (about 1e-6 after the FP32
-        // sweeps), W = V (I - E/2 + 3E^2/8), so that W^H W - I = O(|E|^3).  A64 serves as the
-        // scratch for E and E^2 (every thread keeps its own entries of E in registers); H is
-        // loaded afterwards.
-        small_product(V64, V64, A64, np, ld, true);            // A64 <- V^H V
-        double2 ev[8];
+        if (lane < np)
+            for (int j = 0; j < np; ++j) W[lane + ld * j] = to_c64(vi[lane + np * j]);
+        __syncwarp();
+        // E = V^H V - I into A; then M = I - E/2 + 3 E^2 / 8 into A; W <- V M.
+        warp_column_product(W, W, col, np, ld, lane, true);
 #pragma unroll
-        for (int r = 0; r < 8; ++r) {
-            const int e = tid + r * blockDim.x;
-            ev[r] = make_double2(0.0, 0.0);
-            if (e < np * np) {
-                const int i = e % np, j = e / np;
-                ev[r] = A64[i + ld * j];
-                if (i == j) ev[r].x -= 1.0;
-            }
-        }
-        __syncthreads();
+        for (int i = 0; i < 32; ++i)
+            if (i == lane) col[i].x -= 1.0;
+        warp_store_column(A, col, np, ld, lane);
+        __syncwarp();
+        warp_column_product(A, A, col, np, ld, lane, false);                 // (E^2)[:, lane]
 #pragma unroll
-        for (int r = 0; r < 8; ++r) {
-            const int e = tid + r * blockDim.x;
-            if (e < np * np) A64[(e % np) + ld * (e / np)] = ev[r];
-        }
-        __syncthreads();
-        small_product(A64, A64, A64, np, ld, false);           // A64 <- E^2
-#pragma unroll
-        for (int r = 0; r < 8; ++r) {
-            const int e = tid + r * blockDim.x;
-            if (e < np * np) {
-                const int i = e % np, j = e / np;
-                const double2 e2 = A64[i + ld * j];
-                A64[i + ld * j] = make_double2((i == j ? 1.0 : 0.0) - 0.5 * ev[r].x + 0.375 * e2.x,
-                                               -0.5 * ev[r].y + 0.375 * e2.y);
+        for (int i = 0; i < 32; ++i) {
+            if (i < np && lane < np) {
+                const double2 e = A[i + ld * lane];
+                col[i] = make_double2((i == lane ? 1.0 : 0.0) - 0.5 * e.x + 0.375 * col[i].x, -0.5 * e.y + 0.375 * col[i].y);
             }
         }
-        __syncthreads();
-        small_product(V64, A64, V64, np, ld, false);           // W = V M
-        for (int e = tid; e < np * np; e += blockDim.x) {
-            const int i = e % np, j = e / np;
-            double2 v = make_double2(0.0, 0.0);
-            if (i < nw && j < nw) {
-                if (i < j) v = h[i + (size_t)nw * j];
-                else if (i > j) v = cconj(h[j + (size_t)nw * i]);
-                else v = make_double2(h[i + (size_t)nw * i].x, 0.0);
+        __syncwarp();
+        warp_store_column(A, col, np, ld, lane);
+        __syncwarp();
+        warp_column_product(W, A, col, np, ld, lane, false);                 // (V M)[:, lane]
+        __syncwarp();
+        warp_store_column(W, col, np, ld, lane);
+        const double fro = warp_load_hermitian(A, h_in + b * h_stride, nw, np, ld, lane);   // A <- H
+        warp_column_product(A, W, col, np, ld, lane, false);                 // (H W)[:, lane]
+        __syncwarp();
+        warp_store_column(A, col, np, ld, lane);
+        __syncwarp();
+        warp_column_product(W, A, col, np, ld, lane, true);                  // (W^H H W)[:, lane]
+        __syncwarp();
+        warp_store_column(A, col, np, ld, lane);
+        __syncwarp();
+        if (lane < np)
+            for (int i = lane; i < np; ++i) {
+                if (i > lane) A[i + ld * lane] = cconj(A[lane + ld * i]);
+                else A[i + ld * i].y = 0.0;
             }
-            A64[i + ld * j] = v;
+        __syncwarp();
+        {
+            double off = 0.0;
+            if (lane < np)
+                for (int i = 0; i < np; ++i)
+                    if (i != lane) off += A[i + ld * lane].x * A[i + ld * lane].x + A[i + ld * lane].y * A[i + ld * lane].y;
+            for (int o = 16; o > 0; o >>= 1) off += __shfl_xor_sync(0xffffffffu, off, o);
+            if (sqrt(off) > fro * 1.0e-13)
+                warp_jacobi_sweep<double>(A, W, np, ld, fro * 8.673617379884035e-19, rot_s, rot_c, rot_p, rot_q, lane);
         }
-        __syncthreads();
-        small_product(A64, V64, A64, np, ld, false);           // T = H W
-        small_product(V64, A64, A64, np, ld, true);            // H' = W^H T
-        for (int e = tid; e < np * np; e += blockDim.x) {
-            const int i = e % np, j = e / np;
-            if (i > j) A64[i + ld * j] = cconj(A64[j + ld * i]);
-            if (i == j) A64[i + ld * i].y = 0.0;
-        }
-        __syncthreads();
-        const double tol64 = fro * 8.673617379884035e-19;
-        for (int sweep = 0; sweep < 4; ++sweep) {
-            if (offdiag_norm(A64, np, ld, red) <= tol64 * np) break;
-            if (tid == 0) rot_flag = 0;
-            __syncthreads();
-            jacobi_sweep<double>(A64, V64, np, ld, tol64, rot_s, rot_c, rot_p, rot_q, &rot_flag);
-            const int any = rot_flag;
-            __syncthreads();
-            if (!any) break;
-        }
-        for (int i = tid; i < nw; i += blockDim.x) {
-            const double di = A64[i + ld * i].x;
-            int rank = 0;
+        // Ascending order (stable) and canonical phases: lane i handles eigenpair i, then the
+        // columns are written row-wise (coalesced).
+        if (lane < nw) {
+            const double di = A[lane + ld * lane].x;
+            int r = 0;
             for (int j = 0; j < nw; ++j) {
-                const double dj = A64[j + ld * j].x;
-                rank += (dj < di) || (dj == di && j < i);
+                const double dj = A[j + ld * j].x;
+                r += (dj < di) || (dj == di && j < lane);
             }
             int pivot = 0;
-            double pm = hypot(V64[0 + ld * i].x, V64[0 + ld * i].y);
-            for (int r = 1; r < nw; ++r) {
-                const double mg = hypot(V64[r + ld * i].x, V64[r + ld * i].y);
-                if (mg > pm) { pm = mg; pivot = r; }
+            double pm = hypot(W[0 + ld * lane].x, W[0 + ld * lane].y);
+            for (int rr = 1; rr < nw; ++rr) {
+                const double mg = hypot(W[rr + ld * lane].x, W[rr + ld * lane].y);
+                if (mg > pm) { pm = mg; pivot = rr; }
             }
-            double2 phase = make_double2(1.0, 0.0);
-            if (pm > 0.0) phase = make_double2(V64[pivot + ld * i].x / pm, -V64[pivot + ld * i].y / pm);
-            E_out[b * nw + rank] = di;
-            double2 *u = U_out + b * (int64_t)nw * nw + (int64_t)nw * rank;
-            for (int r = 0; r < nw; ++r) u[r] = cmul(V64[r + ld * i], phase);
+            phase[lane] = pm > 0.0 ? make_double2(W[pivot + ld * lane].x / pm, -W[pivot + ld * lane].y / pm)
+                                   : make_double2(1.0, 0.0);
+            rank[lane] = r;
+            E_out[b * nw + r] = di;
         }
-        __syncthreads();
+        __syncwarp();
+        double2 *u = U_out + b * (int64_t)nw * nw;
+        for (int c = 0; c < nw; ++c)
+            if (lane < nw) u[lane + (int64_t)nw * rank[c]] = cmul(W[lane + ld * c], phase[c]);
+        __syncwarp();
     }
 }
-
 
 // ---------------------------------------------------------------------------------------------
 // Generalised Hermitian eigensolve H C = S C E for nonorthogonal models, FP64

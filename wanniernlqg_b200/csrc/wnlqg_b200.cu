@@ -643,7 +643,10 @@ wnlqg_status run_front(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const int64_
         const int warm = (mesh != nullptr && kpts_device == nullptr && kidx_device == nullptr) ? 1 : 0;
         jacobi_f32_warp_kernel<<<(unsigned)f32_grid, 128, pl->eigh_smem, pl->stream>>>(
             pl->d_xw + (int64_t)pl->ch_H * pl->nn, N, nb, pl->nw, pl->d_V32, warm);
-        eigh_refine_f64_kernel<<<(unsigned)nb, pl->refine_threads, pl->refine_smem, pl->stream>>>(
+        int per_sm_r = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_r, eigh_refine_f64_warp_kernel, 64, pl->refine_smem);
+        const int64_t r_grid = std::min<int64_t>((nb + 1) / 2, (int64_t)std::max(1, per_sm_r) * pl->sm_count);
+        eigh_refine_f64_warp_kernel<<<(unsigned)r_grid, 64, pl->refine_smem, pl->stream>>>(
             pl->d_xw + (int64_t)pl->ch_H * pl->nn, N, pl->d_V32, nb, pl->nw, pl->d_E, pl->d_U);
         pl->launches += 1;
     } else
@@ -1091,7 +1094,7 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
     } else if (t.precision == WNLQG_PRECISION_MIXED) {
         const int np = nw + (nw & 1);
         pl->eigh_smem = 4 * WarpJacobiSmem::per_warp(nw);
-        pl->refine_smem = EighRefineSmem::bytes(nw);
+        pl->refine_smem = 2 * WarpRefineSmem::per_warp(nw);
         {
             // Pair-block table of the warp Jacobi: w = k2 (k2 + 1) / 2 + k1, k1 <= k2 < 16.
             unsigned char tab[136][2];
@@ -1107,7 +1110,7 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
         pl->refine_threads = std::max(pl->refine_threads, ((np / 2 + 31) / 32) * 32);
         pl->eigh_threads = pl->refine_threads;
         if ((st = alloc((void **)&pl->d_V32, (size_t)max_batch * np * np * sizeof(float2))) != WNLQG_OK) return bail(st);
-        cudaError_t e = cudaFuncSetAttribute(eigh_refine_f64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaError_t e = cudaFuncSetAttribute(eigh_refine_f64_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)std::max<size_t>(pl->refine_smem, 48 * 1024));
         if (e != cudaSuccess) return bail(fail(WNLQG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e)));
     } else {
