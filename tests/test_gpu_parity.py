@@ -319,3 +319,59 @@ def test_nonorthogonal_responses_rejected_and_indefinite_overlap_reported(engine
         with pytest.raises(EngineError) as ei:
             eng.spectrum(np.array([[0.1, 0.2, 0.3]]))
         assert ei.value.status == 1
+
+
+# ---- orbital counts above 32: matrices in a per-CTA global working set ---------------------------
+
+@pytest.mark.parametrize("nw,precision", [(48, _abi.PRECISION_FP64), (64, _abi.PRECISION_FP64),
+                                          (64, _abi.PRECISION_MIXED)])
+def test_large_nw_point_values_match_oracle(engine_cls, oracle_mod, nw, precision):
+    model = synthetic_orthogonal_model(nw, 1, seed=nw, full_position=True)
+    task = _abi.TaskArrays([(_abi.SHIFT_CURRENT, ["xyy", "zxz"]), (_abi.BERRY_CURVATURE, ["xy"]),
+                            (_abi.QUANTUM_METRIC, ["xx"]), (_abi.INJECTION_CURRENT, ["xyy"])],
+                           broadening_type=_abi.LORENTZIAN, broadening=0.02, photon_energies=np.linspace(0, 3, 24),
+                           precision=precision)
+    k = np.random.default_rng(nw).random((3, 3))
+    with engine_cls(model, task) as eng:
+        got = eng.point_values(k)
+    ref = oracle_mod.point_values(model, task, k)
+    tol = RTOL if precision == _abi.PRECISION_FP64 else MIXED_RTOL
+    for g, r in zip(task.split(got), task.split(ref)):
+        assert rel_err(g, r) < tol
+
+
+def test_large_nw_mesh_matches_oracle(engine_cls, oracle_mod):
+    model = synthetic_orthogonal_model(64, 1, seed=5, full_position=True)
+    task = _abi.TaskArrays([(_abi.SHIFT_CURRENT, ["xyy"]), (_abi.QUANTUM_METRIC, ["xx"])],
+                           broadening_type=_abi.GAUSSIAN, broadening=0.05, photon_energies=np.linspace(0, 3, 16))
+    mesh = (4, 3, 2)
+    with engine_cls(model, task, max_batch=10) as eng:
+        got = eng.integrate_mesh(mesh)
+    ref = oracle_mod.integrate_mesh(model, task, mesh)
+    for g, r in zip(task.split(got), task.split(ref)):
+        assert rel_err(g, r) < RTOL
+
+
+@pytest.mark.parametrize("nw", [96])
+def test_large_nw_spectrum_matches_oracle(engine_cls, oracle_mod, nw):
+    model = synthetic_orthogonal_model(nw, 1, seed=3)
+    task = _abi.TaskArrays([(_abi.QUANTUM_METRIC, ["xx"])])
+    k = np.random.default_rng(4).random((4, 3))
+    with engine_cls(model, task) as eng:
+        e, _ = eng.spectrum(k)
+    for i in range(k.shape[0]):
+        eo, _, _ = oracle_mod.kpoint_spectrum(model, k[i])
+        assert np.max(np.abs(e[i] - eo)) < 1e-11 * max(1.0, np.abs(eo).max())
+
+
+@pytest.mark.parametrize("nw", [64, 80])
+def test_large_nw_nonorthogonal_spectrum_matches_oracle(engine_cls, oracle_mod, nw):
+    from wanniernlqg_b200.model import synthetic_nonorthogonal_model
+    model = synthetic_nonorthogonal_model(nw, 1, seed=2)
+    task = _abi.TaskArrays([(_abi.QUANTUM_METRIC, ["xx"])])
+    k = np.random.default_rng(6).random((3, 3))
+    with engine_cls(model, task) as eng:
+        e, _ = eng.spectrum(k)
+    for i in range(k.shape[0]):
+        eo, _, _ = oracle_mod.kpoint_spectrum(model, k[i])
+        assert np.max(np.abs(e[i] - eo)) < 1e-10 * max(1.0, np.abs(eo).max())

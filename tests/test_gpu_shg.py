@@ -129,3 +129,15 @@ def test_shg_invalid_widths_rejected(engine_cls, tb4):
     with pytest.raises(EngineError) as ei:
         engine_cls(tb4, task)
     assert ei.value.status == 1 and "finite and positive" in str(ei.value)
+
+
+def test_shg_large_nw_matches_oracle(engine_cls, oracle_mod):
+    """nw = 48: the SHG matrices live in the per-CTA global working set."""
+    from wanniernlqg_b200.model import synthetic_orthogonal_model
+    model = synthetic_orthogonal_model(48, 1, seed=9, full_position=True)
+    task = shg_task(T=300.0, omegas=np.linspace(0.0, 3.0, 9), components=[(0, 1, 1), (2, 0, 0), (1, 1, 1)])
+    k = np.random.default_rng(24).random((2, 3))
+    with engine_cls(model, task) as eng:
+        got = task.split(eng.point_values(k))[0]
+    ref = task.split(oracle_mod.point_values(model, task, k))[0]
+    assert block_err(got, ref) < RTOL

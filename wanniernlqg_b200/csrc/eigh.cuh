@@ -143,11 +143,15 @@ WNLQG_D double offdiag_norm(const C *A, int np, int ld, double *red) {
 // T: real type of the iteration (double for the FP64 path, float for the mixed path).
 // Input H(k) for batch entry b at h_in + b*h_stride (complex double, column-major nw x nw).
 // Outputs: energies E[b*nw + n] (double) and U[b*nw*nw + i + nw*n] (complex double).
+// gscratch (optional): a per-CTA working set of EighSmem::bytes in global memory, used when the
+// matrices do not fit shared memory (large nw).
 template <typename T>
 __global__ void jacobi_eigh_kernel(const double2 *__restrict__ h_in, int64_t h_stride, int64_t batch, int nw,
-                                   double *__restrict__ E_out, double2 *__restrict__ U_out, T tol_scale) {
+                                   double *__restrict__ E_out, double2 *__restrict__ U_out, T tol_scale,
+                                   unsigned char *gscratch = nullptr, int64_t gscratch_stride = 0) {
     typedef typename cplx_of<T>::type C;
-    extern __shared__ __align__(16) unsigned char smraw[];
+    extern __shared__ __align__(16) unsigned char smem_dyn[];
+    unsigned char *smraw = gscratch ? gscratch + (int64_t)blockIdx.x * gscratch_stride : smem_dyn;
     const int np = nw + (nw & 1);
     const int ld = np + 1;
     const int half = np / 2;
@@ -595,8 +599,10 @@ struct GenEighSmem {
 
 __global__ void generalized_eigh_kernel(const double2 *__restrict__ h_in, const double2 *__restrict__ s_in,
                                         int64_t stride, int64_t batch, int nw, double *__restrict__ E_out,
-                                        double2 *__restrict__ U_out, int *__restrict__ status) {
-    extern __shared__ __align__(16) unsigned char smraw[];
+                                        double2 *__restrict__ U_out, int *__restrict__ status,
+                                        unsigned char *gscratch = nullptr, int64_t gscratch_stride = 0) {
+    extern __shared__ __align__(16) unsigned char smem_dyn[];
+    unsigned char *smraw = gscratch ? gscratch + (int64_t)blockIdx.x * gscratch_stride : smem_dyn;
     const int np = nw + (nw & 1);
     const int ld = np + 1;
     const int half = np / 2;

@@ -82,6 +82,10 @@ struct RespParams {
     double2 *out_points;        // [batch][vc]
     int64_t point_offset;       // global index of batch entry 0 (mode 1)
     int n_slots;
+    // Per-CTA working set in global memory (L1/L2-resident) when it exceeds shared memory
+    // (large nw); nullptr: dynamic shared memory.
+    unsigned char *gscratch;
+    int64_t gscratch_stride;
 };
 
 struct RespSmem {
@@ -316,7 +320,8 @@ WNLQG_D void contract_dispatch(int pair_mode, int gaussian, const double *ste, c
 template <typename R>
 __global__ void __launch_bounds__(256) response_kernel(RespParams p) {
     typedef typename cplx_of<R>::type C;
-    extern __shared__ __align__(16) unsigned char sm[];
+    extern __shared__ __align__(16) unsigned char smem_dyn[];
+    unsigned char *sm = p.gscratch ? p.gscratch + (int64_t)blockIdx.x * p.gscratch_stride : smem_dyn;
     const int nw = p.nw, ld = p.ld, nn = nw * nw;
     const RespSmem L = RespSmem::layout(nw, p.n_slots, p.n_fc, 1, sizeof(C));
     C *sU = reinterpret_cast<C *>(sm + L.U);

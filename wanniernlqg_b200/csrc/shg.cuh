@@ -55,6 +55,8 @@ struct ShgParams {
     int64_t point_offset;
     double2 *scratch;            // per CTA: G[9][nn] | coef[nn][nc][7] | pinfo[nn] (fo, inv, diff, 0)
     int64_t scratch_stride;      // double2 entries per CTA
+    unsigned char *gscratch;     // per-CTA matrix working set in global memory (large nw); nullptr: shared
+    int64_t gscratch_stride;
 };
 
 struct ShgSmem {
@@ -180,7 +182,8 @@ WNLQG_D void shg_contract(const ShgParams &p, const double2 *__restrict__ coef, 
 }
 
 __global__ void __launch_bounds__(256) shg_kernel(ShgParams p) {
-    extern __shared__ __align__(16) unsigned char sm[];
+    extern __shared__ __align__(16) unsigned char smem_dyn[];
+    unsigned char *sm = p.gscratch ? p.gscratch + (int64_t)blockIdx.x * p.gscratch_stride : smem_dyn;
     const int nw = p.nw, ld = p.ld, nn = nw * nw, nc = p.nc;
     const ShgSmem L = ShgSmem::layout(nw, nc);
     double2 *sU = reinterpret_cast<double2 *>(sm + L.U);

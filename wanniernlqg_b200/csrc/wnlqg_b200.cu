@@ -63,6 +63,7 @@ struct wnlqg_model {
 
 struct Pass {
     RespParams params;   // template; batch-dependent fields set per launch
+    bool global = false; // working set in global memory (does not fit shared memory)
     size_t smem = 0;
     int threads = 0;
     int grid = 0;
@@ -98,6 +99,7 @@ struct wnlqg_plan {
     size_t shg_smem = 0;
     int shg_grid = 0;
     double2 *d_shg_scratch = nullptr;
+    unsigned char *d_shg_gscratch = nullptr;
     // Tensor-core Fourier for arbitrary k-points: Ozaki slices of the phases (A, per batch) and of
     // the channel tiles (B, built once), tcgen05 kind::i8 GEMM.  tc_slices == 0: FP64 CUDA cores.
     int tc_slices = 0;
@@ -109,6 +111,12 @@ struct wnlqg_plan {
     CUtensorMap tc_mapA, tc_mapB;
     int eigh_threads = 32;
     size_t eigh_smem = 0;
+    bool warp_eigh = false;                   // mixed path, nw <= 32: warp-per-matrix stages
+    unsigned char *d_eigh_scratch = nullptr;  // per-CTA global working set of the CTA eigensolvers
+    int64_t eigh_scratch_stride = 0;
+    int eigh_grid = 0;
+    unsigned char *d_resp_scratch = nullptr;  // per-CTA global working set of the response passes
+    int64_t resp_scratch_stride = 0;
     int refine_threads = 32;
     int sm_count = 148;
     size_t refine_smem = 0;
@@ -218,6 +226,9 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
             e = cudaFuncSetAttribute(response_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_limit);
         if (e != cudaSuccess) return fail(WNLQG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
     }
+    // Orbital counts whose matrices do not fit shared memory keep each CTA's working set in global
+    // memory (L1/L2-resident); passes are then limited only by the per-pass component limits.
+    const bool global_mode = RespSmem::layout(pl->nw, 4, 1, 1, csize).total > smem_limit;
     size_t i = 0;
     while (i < items.size()) {
         Pass ps;
@@ -282,7 +293,8 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
             int nmi = p.n_mu + (muaxis ? 1 : 0);
             size_t smem = RespSmem::layout(pl->nw, nslots, nfc, 1, csize).total;
             bool fits = nfc <= RS_MAX_FREQ && nsc <= RS_MAX_SCALAR && nmi <= RS_MAX_SCALAR &&
-                        (int)gl.size() + newg <= RS_MAX_G && (int)hl.size() + newh <= RS_MAX_HESS && smem <= smem_limit;
+                        (int)gl.size() + newg <= RS_MAX_G && (int)hl.size() + newh <= RS_MAX_HESS &&
+                        (global_mode || smem <= smem_limit);
             if (!fits) {
                 if (i == start)
                     return fail(WNLQG_ERR_UNSUPPORTED, "one response component does not fit the shared-memory budget for nw=" +
@@ -350,14 +362,30 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
         p.vc = pl->vc;
         p.xw_stride = (int64_t)pl->C * pl->nn;
         ps.smem = RespSmem::layout(pl->nw, p.n_slots, p.n_fc, 1, csize).total;
+        ps.global = global_mode;
         ps.threads = response_threads(pl->nw);
         int per_sm = 0;
-        cudaError_t e = mixed ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, response_kernel<float>, ps.threads, ps.smem)
-                              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, response_kernel<double>, ps.threads, ps.smem);
+        const size_t launch_smem = global_mode ? 0 : ps.smem;
+        cudaError_t e = mixed ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, response_kernel<float>, ps.threads, launch_smem)
+                              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, response_kernel<double>, ps.threads, launch_smem);
         if (e != cudaSuccess) return fail(WNLQG_ERR_CUDA, std::string("occupancy query: ") + cudaGetErrorString(e));
         if (per_sm < 1) return fail(WNLQG_ERR_UNSUPPORTED, "response kernel cannot be resident with its shared memory");
         ps.grid = sm_count * per_sm;
         pl->passes.push_back(ps);
+    }
+    if (global_mode && !pl->passes.empty()) {
+        int64_t grid = 0;
+        size_t bytes = 0;
+        for (const Pass &ps : pl->passes) {
+            grid = std::max<int64_t>(grid, ps.grid);
+            bytes = std::max(bytes, ps.smem);
+        }
+        pl->resp_scratch_stride = (int64_t)((bytes + 255) & ~(size_t)255);
+        cudaError_t e = cudaMalloc(&pl->d_resp_scratch, (size_t)grid * pl->resp_scratch_stride);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(WNLQG_ERR_OUT_OF_MEMORY, "cudaMalloc of the response working set failed");
+        }
     }
     return WNLQG_OK;
 }
@@ -408,9 +436,9 @@ wnlqg_status build_shg(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
         off += width;
     }
     if (pl->shg.empty()) return WNLQG_OK;
-    pl->shg_smem = ShgSmem::layout(pl->nw, max_nc).total;
-    if (pl->shg_smem > smem_limit)
-        return fail(WNLQG_ERR_UNSUPPORTED, "second-harmonic kernel does not fit shared memory for nw=" + std::to_string(pl->nw));
+    const size_t shg_bytes = ShgSmem::layout(pl->nw, max_nc).total;
+    const bool shg_global = shg_bytes > smem_limit;   // large nw: matrices in a per-CTA global working set
+    pl->shg_smem = shg_global ? 0 : shg_bytes;
     cudaError_t e = cudaFuncSetAttribute(shg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)std::max<size_t>(pl->shg_smem, 48 * 1024));
     if (e != cudaSuccess) return fail(WNLQG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
@@ -425,6 +453,15 @@ wnlqg_status build_shg(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
     if (e != cudaSuccess) {
         cudaGetLastError();
         return fail(WNLQG_ERR_OUT_OF_MEMORY, "cudaMalloc of the second-harmonic scratch failed");
+    }
+    if (shg_global) {
+        const int64_t gstride = (int64_t)((shg_bytes + 255) & ~(size_t)255);
+        e = cudaMalloc(&pl->d_shg_gscratch, (size_t)pl->shg_grid * gstride);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(WNLQG_ERR_OUT_OF_MEMORY, "cudaMalloc of the second-harmonic working set failed");
+        }
+        for (ShgParams &p : pl->shg) p.gscratch_stride = gstride;
     }
     return WNLQG_OK;
 }
@@ -631,11 +668,12 @@ wnlqg_status run_front(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const int64_
     }
     wnlqg_status st = record_event(pl, ev_base + 1);
     if (st != WNLQG_OK) return st;
+    const unsigned eigh_grid = (unsigned)(pl->d_eigh_scratch ? std::min<int64_t>(nb, pl->eigh_grid) : nb);
     if (pl->nonorth) {
-        generalized_eigh_kernel<<<(unsigned)nb, pl->eigh_threads, GenEighSmem::bytes(pl->nw), pl->stream>>>(
+        generalized_eigh_kernel<<<eigh_grid, pl->eigh_threads, pl->eigh_smem, pl->stream>>>(
             pl->d_xw + (int64_t)pl->ch_H * pl->nn, pl->d_xw + (int64_t)pl->ch_S * pl->nn, N, nb, pl->nw, pl->d_E,
-            pl->d_U, pl->d_status);
-    } else if (pl->task.precision == WNLQG_PRECISION_MIXED) {
+            pl->d_U, pl->d_status, pl->d_eigh_scratch, pl->eigh_scratch_stride);
+    } else if (pl->warp_eigh) {
         int per_sm = 1;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jacobi_f32_warp_kernel, 128, pl->eigh_smem);
         const int64_t f32_grid = std::min<int64_t>((nb + 3) / 4, (int64_t)std::max(1, per_sm) * pl->sm_count);
@@ -650,8 +688,9 @@ wnlqg_status run_front(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const int64_
             pl->d_xw + (int64_t)pl->ch_H * pl->nn, N, pl->d_V32, nb, pl->nw, pl->d_E, pl->d_U);
         pl->launches += 1;
     } else
-        jacobi_eigh_kernel<double><<<(unsigned)nb, pl->eigh_threads, pl->eigh_smem, pl->stream>>>(
-            pl->d_xw + (int64_t)pl->ch_H * pl->nn, N, nb, pl->nw, pl->d_E, pl->d_U, 8.673617379884035e-19);
+        jacobi_eigh_kernel<double><<<eigh_grid, pl->eigh_threads, pl->eigh_smem, pl->stream>>>(
+            pl->d_xw + (int64_t)pl->ch_H * pl->nn, N, nb, pl->nw, pl->d_E, pl->d_U, 8.673617379884035e-19,
+            pl->d_eigh_scratch, pl->eigh_scratch_stride);
     st = record_event(pl, ev_base + 2);
     if (st != WNLQG_OK) return st;
     pl->launches += staged ? 4 : 3;
@@ -673,10 +712,13 @@ wnlqg_status run_passes(wnlqg_plan *pl, int64_t nb, int mode, double scale, int6
         p.partials = pl->d_partials;
         p.out_points = pl->d_points;
         p.point_offset = point_offset;
+        p.gscratch = ps.global ? pl->d_resp_scratch : nullptr;
+        p.gscratch_stride = pl->resp_scratch_stride;
+        const size_t launch_smem = ps.global ? 0 : ps.smem;
         if (pl->task.precision == WNLQG_PRECISION_MIXED)
-            response_kernel<float><<<ps.grid, ps.threads, ps.smem, pl->stream>>>(p);
+            response_kernel<float><<<ps.grid, ps.threads, launch_smem, pl->stream>>>(p);
         else
-            response_kernel<double><<<ps.grid, ps.threads, ps.smem, pl->stream>>>(p);
+            response_kernel<double><<<ps.grid, ps.threads, launch_smem, pl->stream>>>(p);
         pl->launches += 1;
     }
     for (const ShgParams &tmpl : pl->shg) {
@@ -692,6 +734,7 @@ wnlqg_status run_passes(wnlqg_plan *pl, int64_t nb, int mode, double scale, int6
         p.out_points = pl->d_points;
         p.point_offset = point_offset;
         p.scratch = pl->d_shg_scratch;
+        p.gscratch = pl->d_shg_gscratch;
         shg_kernel<<<pl->shg_grid, 256, pl->shg_smem, pl->stream>>>(p);
         pl->launches += 1;
     }
@@ -732,8 +775,8 @@ wnlqg_status wnlqg_b200_model_create(const wnlqg_model_desc *desc, int32_t devic
     *out_model = nullptr;
     if (desc->num_orbitals <= 0 || desc->num_r_vectors <= 0)
         return fail(WNLQG_ERR_DIMENSION_MISMATCH, "num_orbitals and num_r_vectors must be positive");
-    if (desc->num_orbitals > 32)
-        return fail(WNLQG_ERR_UNSUPPORTED, "this build supports num_orbitals <= 32");
+    if (desc->num_orbitals > 128)
+        return fail(WNLQG_ERR_UNSUPPORTED, "this build supports num_orbitals <= 128");
     if (!desc->lattice || !desc->r_vectors || !desc->r_degeneracies || !desc->hamiltonian_r)
         return fail(WNLQG_ERR_INVALID_ARGUMENT, "lattice, r_vectors, r_degeneracies and hamiltonian_r are required");
     const int nw = (int)desc->num_orbitals, nr = (int)desc->num_r_vectors;
@@ -801,7 +844,8 @@ wnlqg_status wnlqg_b200_plan_destroy(wnlqg_plan *pl) {
                       (void *)pl->d_partials, (void *)pl->d_weights, (void *)pl->d_groups, (void *)pl->d_stageY,
                       (void *)pl->d_stageZ, (void *)pl->d_V32, (void *)pl->d_kidx, (void *)pl->d_mus, (void *)pl->d_status,
                       (void *)pl->d_shg_scratch, (void *)pl->d_tcA, (void *)pl->d_tcB, (void *)pl->d_tc_colscale,
-                      (void *)pl->d_tc_err})
+                      (void *)pl->d_tc_err, (void *)pl->d_shg_gscratch, (void *)pl->d_eigh_scratch,
+                      (void *)pl->d_resp_scratch})
         if (ptr) cudaFree(ptr);
     for (cudaEvent_t ev : pl->events) cudaEventDestroy(ev);
     if (pl->stream) cudaStreamDestroy(pl->stream);
@@ -1086,12 +1130,11 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
     }
 
     pl->eigh_threads = eigh_block_threads(nw);
+    pl->warp_eigh = !pl->nonorth && t.precision == WNLQG_PRECISION_MIXED && nw <= 32;
     if (pl->nonorth) {
         pl->eigh_threads = std::max(pl->eigh_threads, ((nw + (nw & 1)) / 2 + 31) / 32 * 32);
-        cudaError_t e = cudaFuncSetAttribute(generalized_eigh_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)std::max<size_t>(GenEighSmem::bytes(nw), 48 * 1024));
-        if (e != cudaSuccess) return bail(fail(WNLQG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e)));
-    } else if (t.precision == WNLQG_PRECISION_MIXED) {
+        pl->eigh_smem = GenEighSmem::bytes(nw);
+    } else if (pl->warp_eigh) {
         const int np = nw + (nw & 1);
         pl->eigh_smem = 4 * WarpJacobiSmem::per_warp(nw);
         pl->refine_smem = 2 * WarpRefineSmem::per_warp(nw);
@@ -1114,10 +1157,24 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
                                              (int)std::max<size_t>(pl->refine_smem, 48 * 1024));
         if (e != cudaSuccess) return bail(fail(WNLQG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e)));
     } else {
+        // FP64 path, and the mixed path above 32 orbitals: FP64 CTA Jacobi.
         pl->eigh_smem = EighSmem::bytes(nw, sizeof(double2));
-        if (pl->eigh_smem > 48 * 1024) {
-            cudaError_t e = cudaFuncSetAttribute(jacobi_eigh_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)pl->eigh_smem);
+    }
+    if (!pl->warp_eigh) {
+        // CTA eigensolvers keep A, V (and the Cholesky factor) in shared memory when they fit,
+        // else in a per-CTA global working set (large nw).
+        if (pl->eigh_smem > (size_t)smem_optin) {
+            pl->eigh_grid = 4 * sm_count;
+            pl->eigh_scratch_stride = (int64_t)((pl->eigh_smem + 255) & ~(size_t)255);
+            if ((st = alloc((void **)&pl->d_eigh_scratch, (size_t)pl->eigh_grid * pl->eigh_scratch_stride)) != WNLQG_OK)
+                return bail(st);
+            pl->eigh_smem = 0;
+        } else {
+            cudaError_t e = pl->nonorth
+                                ? cudaFuncSetAttribute(generalized_eigh_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                       (int)std::max<size_t>(pl->eigh_smem, 48 * 1024))
+                                : cudaFuncSetAttribute(jacobi_eigh_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                       (int)std::max<size_t>(pl->eigh_smem, 48 * 1024));
             if (e != cudaSuccess) return bail(fail(WNLQG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e)));
         }
     }
