@@ -184,7 +184,8 @@ def main():
     ap.add_argument("--batch", type=int, default=65536, help="mesh points per step and rank")
     ap.add_argument("--sampling", default="mesh", choices=["mesh", "random"],
                     help="mesh blocks (staged Fourier) or random k-points (tensor-core Fourier)")
-    ap.add_argument("--max-batch", type=int, default=0, help="plan batch capacity (0: the plan default, ~4 GiB)")
+    ap.add_argument("--max-batch", type=int, default=0,
+                    help="plan batch capacity (0: one step, --batch points; a 65536-point nw=32 step holds ~11 GB)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-time-to-tolerance", action="store_true",
@@ -214,7 +215,7 @@ def main():
     task = make_task(precision)
     nk = int(np.prod(MESH))
     batch = args.batch
-    engine = ResponseEngine(model, task, device=local_rank, max_batch=args.max_batch)
+    engine = ResponseEngine(model, task, device=local_rank, max_batch=args.max_batch or batch)
     vc = engine.value_count
     out = torch.zeros(2 * vc, dtype=torch.float64, device="cuda")
     stream = torch.cuda.current_stream()

@@ -112,6 +112,9 @@ typedef struct wnlqg_task_desc {
     double shg_low_frequency_broadening;    /* eV; second harmonic low-frequency width (reference 0.025) */
     double shg_intermediate_regularization; /* eV; second harmonic eta; 0 selects denominator_regularization */
     int32_t shg_eta_correction;             /* second harmonic: 1 adds the finite-eta C numerator (reference true) */
+    int32_t band_window_size;               /* shift/injection pairs: bands around mu, widened to complete
+                                               degeneracy groups (select_band_window, CalculationUtils.jl:71-90,
+                                               TransitionScreening.jl:201-233); -1 = all bands */
 } wnlqg_task_desc;
 
 typedef struct wnlqg_model wnlqg_model;   /* device-resident model */

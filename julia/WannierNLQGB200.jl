@@ -50,6 +50,7 @@ struct TaskDesc
     shg_low_frequency_broadening::Float64      # cfg.shg_low_frequency_broadening
     shg_intermediate_regularization::Float64   # cfg.shg_intermediate_regularization (0: denominator_regularization)
     shg_eta_correction::Int32                  # cfg.shg_eta_correction
+    band_window_size::Int32                    # cfg.band_window_size (-1: all bands)
 end
 
 function check(status)

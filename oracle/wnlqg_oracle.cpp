@@ -431,10 +431,38 @@ struct Screen {
     std::vector<char> mask;      // [n + nw*m]
 };
 
-// _fill_transition_screen! (TransitionScreening.jl:32-94) with the full band window.
+// Effective band window [lo, hi) (0-based) of _prepare_transition_selection_window!
+// (TransitionScreening.jl:201-233): select_band_window (CalculationUtils.jl:71-90) around mu, then,
+// for a finite window, widened to whole response degeneracy groups
+// (_mark_response_degeneracy_groups!, ResponseDegeneracyGroups.jl:10-33).  lo = hi = 0: no bands.
+void band_window(const std::vector<double> &E, const wnlqg_task_desc &t, int &lo, int &hi) {
+    const int n = (int)E.size();
+    const int size = t.band_window_size;
+    if (size == -1 || 2 * size > n) { lo = 0; hi = n; return; }
+    int valence = 0;   // searchsortedlast: number of energies <= mu
+    while (valence < n && E[valence] <= t.fermi_energy) ++valence;
+    if (valence < 1 || valence >= n) { lo = 0; hi = 0; return; }
+    int start = std::max(1, valence - size + 1), end = std::min(n, valence + size);   // 1-based inclusive
+    double emax = 0.0;
+    for (double e : E) emax = std::max(emax, std::fabs(e));
+    const double equal = 32.0 * 2.220446049250313e-16 * std::max(1.0, emax);
+    auto joined = [&](int b) {   // bands b and b+1 (1-based) in one group
+        const double gap = E[b] - E[b - 1];
+        return gap < t.degeneracy_threshold || gap <= equal;
+    };
+    while (start > 1 && joined(start - 1)) --start;
+    while (end < n && joined(end)) ++end;
+    lo = start - 1;
+    hi = end;
+}
+
+// _fill_transition_screen! (TransitionScreening.jl:32-94) with the pair lists of
+// _record_active_transition_pairs! (:126-162) restricted to the effective band window.
 void fill_screen(const std::vector<double> &E, const std::vector<double> &f,
                  const wnlqg_task_desc &t, Screen &s) {
     int n = (int)E.size();
+    int wlo = 0, whi = 0;
+    band_window(E, t, wlo, whi);
     int64_t nom = t.num_photon_energies;
     bool gaussian = t.broadening_type == WNLQG_GAUSSIAN;
     double eta = t.broadening;
@@ -450,7 +478,7 @@ void fill_screen(const std::vector<double> &E, const std::vector<double> &f,
             double od = f[a] - f[b];
             s.fnm[a + (size_t)n * b] = od;
             double te = E[b] - E[a];
-            bool occ = std::fabs(od) > 1.0e-10;
+            bool occ = std::fabs(od) > 1.0e-10 && a >= wlo && a < whi && b >= wlo && b < whi;
             bool pair_active = occ && !gaussian;
             if (occ && !gaussian && thr <= 0) s.active = true;
             for (int64_t w = 0; w < nom; ++w) {

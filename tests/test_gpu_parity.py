@@ -375,3 +375,31 @@ def test_large_nw_nonorthogonal_spectrum_matches_oracle(engine_cls, oracle_mod, 
     for i in range(k.shape[0]):
         eo, _, _ = oracle_mod.kpoint_spectrum(model, k[i])
         assert np.max(np.abs(e[i] - eo)) < 1e-10 * max(1.0, np.abs(eo).max())
+
+
+@pytest.mark.parametrize("name,window,mu", [("nw4", 1, 0.0), ("nw4", 2, 0.0), ("nw4", 1, 5.0), ("nw32", 4, 0.0),
+                                             ("nw32", 3, -0.3), ("nw32", 100, 0.0)])
+def test_band_window_matches_oracle(engine_cls, oracle_mod, name, window, mu):
+    """band_window_size restricts the shift/injection pairs to bands around mu (widened to whole
+    degeneracy groups); a window past the spectrum edge leaves no pairs."""
+    model = reference_workload_model(name)
+    task = _abi.TaskArrays([(_abi.SHIFT_CURRENT, ["xyy"]), (_abi.INJECTION_CURRENT, ["xyy"])],
+                           broadening_type=_abi.LORENTZIAN, broadening=0.02, photon_energies=np.linspace(0, 3, 32),
+                           fermi_energy=mu, band_window_size=window, degeneracy_threshold=0.05)
+    full = _abi.TaskArrays([(_abi.SHIFT_CURRENT, ["xyy"]), (_abi.INJECTION_CURRENT, ["xyy"])],
+                           broadening_type=_abi.LORENTZIAN, broadening=0.02, photon_energies=np.linspace(0, 3, 32),
+                           fermi_energy=mu)
+    k = np.random.default_rng(31).random((6, 3))
+    with engine_cls(model, task) as eng:
+        got = eng.point_values(k)
+    ref = oracle_mod.point_values(model, task, k)
+    for g, r in zip(task.split(got), task.split(ref)):
+        scale = np.max(np.abs(r))
+        assert np.max(np.abs(g - r)) <= RTOL * max(scale, 1e-300)
+    ref_full = oracle_mod.point_values(model, full, k)
+    if 2 * window > model.num_orbitals:
+        assert np.array_equal(ref, ref_full)
+    elif mu > 4.0:
+        assert np.all(ref == 0)
+    else:
+        assert not np.allclose(ref, ref_full)

@@ -82,6 +82,7 @@ class TaskDesc(ctypes.Structure):
         ("shg_low_frequency_broadening", ctypes.c_double),
         ("shg_intermediate_regularization", ctypes.c_double),
         ("shg_eta_correction", ctypes.c_int32),
+        ("band_window_size", ctypes.c_int32),
     ]
 
 
@@ -134,7 +135,7 @@ class TaskArrays:
                  denominator_regularization=0.001, degeneracy_threshold=2.0e-3,
                  photon_energies=(0.10,), fermi_energies=(), precision=PRECISION_FP64,
                  fermi_surface_broadening=0.0, shg_low_frequency_broadening=0.025,
-                 shg_intermediate_regularization=0.0, shg_eta_correction=True):
+                 shg_intermediate_regularization=0.0, shg_eta_correction=True, band_window_size=-1):
         if not 1 <= len(responses) <= MAX_RESPONSES:
             raise ValueError("between 1 and 8 responses are supported per task")
         self.photon_energies = np.ascontiguousarray(np.asarray(photon_energies, dtype=np.float64))
@@ -169,6 +170,7 @@ class TaskArrays:
         d.shg_low_frequency_broadening = float(shg_low_frequency_broadening)
         d.shg_intermediate_regularization = float(shg_intermediate_regularization)
         d.shg_eta_correction = 1 if shg_eta_correction else 0
+        d.band_window_size = int(band_window_size)
         self.desc = d
 
     def value_count(self) -> int:

@@ -86,7 +86,28 @@ struct RespParams {
     // (large nw); nullptr: dynamic shared memory.
     unsigned char *gscratch;
     int64_t gscratch_stride;
+    // Shift/injection band window (-1: all bands) and the response degeneracy threshold.
+    int band_window;
+    double degeneracy_threshold;
 };
+
+// Effective band window [lo, hi) (0-based) around mu: select_band_window (CalculationUtils.jl:71-90),
+// widened for a finite window to whole degeneracy groups (TransitionScreening.jl:201-233,
+// ResponseDegeneracyGroups.jl:10-33).  lo = hi = 0: the Fermi level is outside the spectrum.
+WNLQG_D void band_window(const double *E, int n, double mu, int size, double thr, int &lo, int &hi) {
+    if (size == -1 || 2 * size > n) { lo = 0; hi = n; return; }
+    int valence = 0;
+    while (valence < n && E[valence] <= mu) ++valence;
+    if (valence < 1 || valence >= n) { lo = 0; hi = 0; return; }
+    int start = max(1, valence - size + 1), end = min(n, valence + size);
+    double emax = 0.0;
+    for (int i = 0; i < n; ++i) emax = fmax(emax, fabs(E[i]));
+    const double equal = 32.0 * 2.220446049250313e-16 * fmax(1.0, emax);
+    while (start > 1 && (E[start - 1] - E[start - 2] < thr || E[start - 1] - E[start - 2] <= equal)) --start;
+    while (end < n && (E[end] - E[end - 1] < thr || E[end] - E[end - 1] <= equal)) ++end;
+    lo = start - 1;
+    hi = end;
+}
 
 struct RespSmem {
     // Byte offsets inside the dynamic shared memory.
@@ -593,8 +614,16 @@ __global__ void __launch_bounds__(256) response_kernel(RespParams p) {
 
         if (p.n_fc > 0) {
             // Transition screen and per-pair kernels; pairs kept in column-major (n fastest) order.
-            if (threadIdx.x == 0) { ired[0] = 0; ired[1] = 0; }
+            if (threadIdx.x == 0) {
+                ired[0] = 0;
+                ired[1] = 0;
+                int lo = 0, hi = nw;
+                if (p.pair_mode == 0) band_window(sE, nw, p.mu, p.band_window, p.degeneracy_threshold, lo, hi);
+                ired[2] = lo;
+                ired[3] = hi;
+            }
             __syncthreads();
+            const int wlo = ired[2], whi = ired[3];
             for (int base = 0; base < nn; base += blockDim.x) {
                 const int e = base + threadIdx.x;
                 bool keep = false;
@@ -612,7 +641,7 @@ __global__ void __launch_bounds__(256) response_kernel(RespParams p) {
                     n = e % nw; m = e / nw;
                     fnm = sf[n] - sf[m];
                     te = sE[m] - sE[n];
-                    if (fabs(fnm) > 1.0e-10) {
+                    if (fabs(fnm) > 1.0e-10 && n >= wlo && n < whi && m >= wlo && m < whi) {
                         if (p.gaussian) {
                             keep = any_within(te, p.cutoff, p);
                             if (keep) ired[1] = 1;

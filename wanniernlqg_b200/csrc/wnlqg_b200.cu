@@ -359,6 +359,8 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
         p.om_lo = sorted.empty() ? 0.0 : sorted.front();
         p.om_hi = sorted.empty() ? 0.0 : sorted.back();
         p.eta_reg = t.denominator_regularization;
+        p.band_window = t.band_window_size;
+        p.degeneracy_threshold = t.degeneracy_threshold;
         p.vc = pl->vc;
         p.xw_stride = (int64_t)pl->C * pl->nn;
         ps.smem = RespSmem::layout(pl->nw, p.n_slots, p.n_fc, 1, csize).total;
@@ -874,6 +876,8 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
         return fail(WNLQG_ERR_NONFINITE, "photon energies must be finite");
     if (t.precision != WNLQG_PRECISION_FP64 && t.precision != WNLQG_PRECISION_MIXED)
         return fail(WNLQG_ERR_INVALID_ARGUMENT, "unknown precision");
+    if (t.band_window_size < -1 || t.band_window_size == 0)
+        return fail(WNLQG_ERR_INVALID_ARGUMENT, "band_window_size must be -1 or positive");
     WNLQG_CUDA(cudaSetDevice(model->device));
 
     wnlqg_plan *pl = new wnlqg_plan();
