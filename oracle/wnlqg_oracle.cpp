@@ -99,6 +99,10 @@ struct KData {
     std::vector<double> E;
     Mat U, Uadj;
     Mat dH[3], ddH[3][3], Aint[3], dA[3][3], F[3][3], inv, D[3], r[3];
+    // Nonorthogonal models: r = Berry connection, dH diagonal = Hellmann-Feynman slopes and the
+    // metric generalized derivatives G[p][d] (position p, derivative d) replace gder.
+    bool nonorth = false;
+    Mat G[3][3];
 };
 
 void set_error(const std::string &s) { g_error = s; }
@@ -284,7 +288,10 @@ double regularized_inverse(double d, double eta) {
 
 // Fourier interpolation, eigensolve and Hamiltonian-gauge geometry at one k
 // (compute_spectrum! + compute_remaining!, HamiltonianMatrixElements.jl:279-300, 532-563).
+void nonorth_kpoint(const Model &m, const Needs &need, const double k[3], double eta, KData &d);
+
 void compute_kpoint(const Model &m, const Needs &need, const double k[3], double eta, KData &d) {
+    if (m.has_overlap) { nonorth_kpoint(m, need, k, eta, d); return; }
     int n = m.nw;
     d.nw = n;
     size_t nn = (size_t)n * n;
@@ -392,9 +399,144 @@ void compute_kpoint(const Model &m, const Needs &need, const double k[3], double
     }
 }
 
+// Nonorthogonal k-point geometry for the conventional currents: the localized operator sums of
+// nonorthogonal_operator_matrices (NonorthogonalMatrixElements.jl:223-283, Convention II), the
+// S-orthonormal canonical eigenvectors C, and _nonorthogonal_geometry (:560-817): band-frame
+// dH, dS and connection B = r + i dS, the metric eigenvector derivative D, the Berry connection
+// i D + B (-> d.r), the Hellmann-Feynman slopes Re(dH_ll - E_l dS_ll) (-> diagonal of d.dH) and
+// the generalized derivatives for the requested (position, derivative) pairs (-> d.G).
+void nonorth_kpoint(const Model &m, const Needs &need, const double k[3], double eta, KData &d) {
+    const int n = m.nw;
+    const size_t nn = (size_t)n * n;
+    d.nw = n;
+    d.nonorth = true;
+    Mat h, sm, r[3], dh[3], ds[3], d2h[3][3], d2s[3][3], dr[3][3];
+    h.init(n); sm.init(n);
+    for (int a = 0; a < 3; ++a) {
+        r[a].init(n); dh[a].init(n); ds[a].init(n);
+        for (int b = 0; b < 3; ++b) { d2h[a][b].init(n); d2s[a][b].init(n); dr[a][b].init(n); }
+    }
+    for (int ir = 0; ir < m.nr; ++ir) {
+        const int64_t *rv = &m.rvec[3 * (size_t)ir];
+        const double phase = (double)rv[0] * k[0] + (double)rv[1] * k[1] + (double)rv[2] * k[2];
+        const cd f = std::polar(1.0, 2.0 * PI * phase) / (double)m.deg[ir];
+        double rc[3];
+        r_cartesian(m, ir, rc);
+        const cd *H = &m.H[nn * ir];
+        const cd *S = &m.S[nn * ir];
+        for (size_t e = 0; e < nn; ++e) { h.v[e] += f * H[e]; sm.v[e] += f * S[e]; }
+        for (int a = 0; a < 3; ++a) {
+            const cd fa = f * (I1 * rc[a]);
+            for (size_t e = 0; e < nn; ++e) { dh[a].v[e] += fa * H[e]; ds[a].v[e] += fa * S[e]; }
+            if (m.has_position) {
+                const cd *A = &m.A[nn * (a + 3 * (size_t)ir)];
+                for (size_t e = 0; e < nn; ++e) r[a].v[e] += f * A[e];
+            }
+            for (int b = 0; b < 3; ++b) {
+                const cd fab = f * (-rc[a] * rc[b]);
+                for (size_t e = 0; e < nn; ++e) { d2h[a][b].v[e] += fab * H[e]; d2s[a][b].v[e] += fab * S[e]; }
+                if (m.has_position) {
+                    const cd *A = &m.A[nn * (a + 3 * (size_t)ir)];
+                    const cd fb = f * (I1 * rc[b]);
+                    for (size_t e = 0; e < nn; ++e) dr[a][b].v[e] += fb * A[e];
+                }
+            }
+        }
+    }
+    std::vector<double> ev;
+    Mat C;
+    if (!generalized_eigen(h, sm, ev, C)) {
+        for (double &x : ev) x = std::nan("");
+        d.E.assign(n, std::nan(""));
+        return;
+    }
+    d.E = ev;
+    d.U = C;
+    d.Uadj.init(n);
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) d.Uadj(i, j) = std::conj(C(j, i));
+    auto mulh = [&](const Mat &X, const Mat &Y) {   // X^H Y
+        Mat o; o.init(n);
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) {
+                cd v(0.0, 0.0);
+                for (int l = 0; l < n; ++l) v += std::conj(X(l, i)) * Y(l, j);
+                o(i, j) = v;
+            }
+        return o;
+    };
+    auto mul = [&](const Mat &X, const Mat &Y) {
+        Mat o; o.init(n);
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) {
+                cd v(0.0, 0.0);
+                for (int l = 0; l < n; ++l) v += X(i, l) * Y(l, j);
+                o(i, j) = v;
+            }
+        return o;
+    };
+    auto f_of = [&](double gap) { return eta == 0.0 ? 1.0 / gap : gap / (gap * gap + eta * eta); };
+    auto fp_of = [&](double gap) {
+        return eta == 0.0 ? -1.0 / (gap * gap) : (eta * eta - gap * gap) / ((gap * gap + eta * eta) * (gap * gap + eta * eta));
+    };
+    Mat dhb[3], dsb[3], conn[3], numer[3];
+    std::vector<double> ed((size_t)n * 3);
+    for (int a = 0; a < 3; ++a) {
+        rotate(d, dh[a], dhb[a]);
+        rotate(d, ds[a], dsb[a]);
+        Mat B; B.init(n);
+        for (size_t e = 0; e < nn; ++e) B.v[e] = r[a].v[e] + I1 * ds[a].v[e];
+        rotate(d, B, conn[a]);
+        numer[a].init(n);
+        d.D[a].init(n);
+        for (int mm = 0; mm < n; ++mm)
+            for (int l = 0; l < n; ++l) {
+                numer[a](l, mm) = dhb[a](l, mm) - (ev[l] + ev[mm]) * dsb[a](l, mm) / 2.0;
+                if (l == mm) d.D[a](l, l) = -dsb[a](l, l) / 2.0 + I1 * conn[a](l, l).real();
+                else d.D[a](l, mm) = -dsb[a](l, mm) / 2.0 + numer[a](l, mm) * f_of(ev[mm] - ev[l]);
+            }
+        for (int l = 0; l < n; ++l) ed[l + (size_t)n * a] = (dhb[a](l, l) - ev[l] * dsb[a](l, l)).real();
+        d.r[a].init(n);
+        for (size_t e = 0; e < nn; ++e) d.r[a].v[e] = I1 * d.D[a].v[e] + conn[a].v[e];
+        d.dH[a] = dhb[a];
+        for (int l = 0; l < n; ++l) d.dH[a](l, l) = ed[l + (size_t)n * a];
+        d.Aint[a] = conn[a];
+    }
+    for (int p = 0; p < 3; ++p)
+        for (int q = 0; q < 3; ++q) {
+            if (!need.dA[p][q]) continue;
+            const Mat &Dd = d.D[q];
+            Mat hd = mulh(Dd, dhb[p]), sd = mulh(Dd, dsb[p]), bd = mulh(Dd, conn[p]);
+            Mat t1 = mul(dhb[p], Dd), t2 = mul(dsb[p], Dd), t3 = mul(conn[p], Dd);
+            Mat rh, rs, rb, X;
+            rotate(d, d2h[p][q], rh);
+            rotate(d, d2s[p][q], rs);
+            X.init(n);
+            for (size_t e = 0; e < nn; ++e) X.v[e] = dr[p][q].v[e] + I1 * d2s[p][q].v[e];
+            rotate(d, X, rb);
+            for (size_t e = 0; e < nn; ++e) {
+                hd.v[e] += t1.v[e] + rh.v[e];
+                sd.v[e] += t2.v[e] + rs.v[e];
+                bd.v[e] += t3.v[e] + rb.v[e];
+            }
+            Mat &G = d.G[p][q];
+            G.init(n);
+            for (int mm = 0; mm < n; ++mm)
+                for (int l = 0; l < n; ++l) {
+                    if (l == mm) continue;
+                    const double gap = ev[mm] - ev[l];
+                    const double edl = ed[l + (size_t)n * q], edm = ed[mm + (size_t)n * q];
+                    const cd nd = hd(l, mm) - (ev[l] + ev[mm]) * sd(l, mm) / 2.0 - (edl + edm) * dsb[p](l, mm) / 2.0;
+                    const cd dd = -sd(l, mm) / 2.0 + nd * f_of(gap) + numer[p](l, mm) * fp_of(gap) * (edm - edl);
+                    G(l, mm) = I1 * dd + bd(l, mm) - I1 * (d.r[q](l, l) - d.r[q](mm, mm)) * d.r[p](l, mm);
+                }
+        }
+}
+
 // conventional_generalized_position_derivative_element (ConventionalShiftCurrent.jl:191-229):
 // r^a_{nm;b} with a the position axis and b the derivative axis.
 cd gder(const KData &d, int n, int m, int a, int b) {
+    if (d.nonorth) return d.G[a][b](n, m);
     cd sum_AD(0.0, 0.0), sum_HD(0.0, 0.0);
     for (int l = 0; l < d.nw; ++l) {
         if (l != n && l != m) {
@@ -1074,10 +1216,21 @@ int64_t oracle_value_count(const wnlqg_task_desc *t) {
 }
 
 // Per-point values: k[3*n] -> out[n*value_count] complex (interleaved).
+bool nonorth_kinds_ok(const Model &m, const wnlqg_task_desc *t) {
+    if (!m.has_overlap) return true;
+    for (int r = 0; r < t->num_responses; ++r)
+        if (t->responses[r].kind != WNLQG_SHIFT_CURRENT && t->responses[r].kind != WNLQG_INJECTION_CURRENT) {
+            set_error("nonorthogonal models: shift and injection current only");
+            return false;
+        }
+    return true;
+}
+
 int oracle_point_values(const wnlqg_model_desc *md, const wnlqg_task_desc *td, const double *k,
                         int64_t n, int threads, double *out) {
     Model m; Task task;
     if (!build_model(md, m) || !build_task(td, task)) return WNLQG_ERR_INVALID_ARGUMENT;
+    if (!nonorth_kinds_ok(m, td)) return WNLQG_ERR_UNSUPPORTED;
     int64_t vc = task.value_count;
     if (threads <= 0) threads = omp_get_max_threads();
 #pragma omp parallel for schedule(dynamic, 1) num_threads(threads)
@@ -1097,6 +1250,7 @@ int oracle_integrate_mesh(const wnlqg_model_desc *md, const wnlqg_task_desc *td,
                           int64_t k_begin, int64_t k_end, int threads, double *out) {
     Model m; Task task;
     if (!build_model(md, m) || !build_task(td, task)) return WNLQG_ERR_INVALID_ARGUMENT;
+    if (!nonorth_kinds_ok(m, td)) return WNLQG_ERR_UNSUPPORTED;
     int64_t nk = mesh[0] * mesh[1] * mesh[2];
     if (nk <= 0 || k_begin < 0 || k_end > nk || k_begin > k_end) { set_error("invalid mesh range"); return WNLQG_ERR_INVALID_ARGUMENT; }
     int64_t vc = task.value_count;

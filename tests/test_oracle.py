@@ -235,3 +235,39 @@ def test_generalized_eigen_matches_lapack(oracle_mod, n):
     assert np.max(np.abs(e - el)) < 1e-12 * max(1.0, np.abs(el).max())
     assert np.max(np.abs(c.conj().T @ s @ c - np.eye(n))) < 1e-12
     assert np.max(np.abs(h @ c - s @ c * e)) < 1e-11 * max(1.0, np.abs(el).max())
+
+
+def _overlap_copy(model, M=None):
+    """The same model in a nonorthogonal basis: S = M^H M at R = 0, H' = M^H H M, A' = M^H A M
+    (M = I: the orthogonal model with an identity overlap)."""
+    import copy
+    nw, nr = model.num_orbitals, model.num_r_vectors
+    M = np.eye(nw) if M is None else M
+    out = copy.deepcopy(model)
+    home = int(np.where(np.all(model.r_vectors == 0, axis=0))[0][0])
+    S = np.zeros((nw, nw, nr), dtype=np.complex128, order="F")
+    S[:, :, home] = M.conj().T @ M
+    out.overlap_r = S
+    out.hamiltonian_r = np.asfortranarray(np.einsum("ji,jkr,kl->ilr", M.conj(), model.hamiltonian_r, M))
+    out.position_r = np.asfortranarray(np.einsum("ji,jkar,kl->ilar", M.conj(), model.position_r, M))
+    return out
+
+
+@pytest.mark.parametrize("eta", [0.001, 0.0])
+@pytest.mark.parametrize("transform", ["identity", "constant"])
+def test_nonorthogonal_currents_equal_orthogonal(oracle_mod, eta, transform):
+    """The metric (nonorthogonal) geometry of NonorthogonalMatrixElements.jl:560-817 must give the
+    orthogonal shift and injection currents when the overlap is the identity, and must be invariant
+    under a constant non-unitary change of the orbital basis (the reference has no numeric fixtures
+    for this path; these identities pin it)."""
+    model = synthetic_orthogonal_model(6, 1, seed=3, full_position=True)
+    rng = np.random.default_rng(4)
+    M = None if transform == "identity" else np.eye(6) + 0.2 * (rng.standard_normal((6, 6)) + 1j * rng.standard_normal((6, 6)))
+    other = _overlap_copy(model, M)
+    task = _abi.TaskArrays([(_abi.SHIFT_CURRENT, ["xyy", "zxy", "yyy"]), (_abi.INJECTION_CURRENT, ["xyy", "zzx"])],
+                           broadening_type=_abi.LORENTZIAN, broadening=0.05, photon_energies=np.linspace(0, 3, 16),
+                           denominator_regularization=eta)
+    k = np.random.default_rng(1).random((5, 3))
+    a = oracle_mod.point_values(model, task, k)
+    b = oracle_mod.point_values(other, task, k)
+    assert np.max(np.abs(a - b)) <= 1e-10 * np.max(np.abs(a))
