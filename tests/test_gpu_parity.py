@@ -290,7 +290,7 @@ def test_jerk_matches_oracle(engine_cls, oracle_mod, precision, kind):
 def test_nonorthogonal_generalized_spectrum_matches_oracle(engine_cls, oracle_mod, nw, rmax):
     from wanniernlqg_b200.model import synthetic_nonorthogonal_model
     model = synthetic_nonorthogonal_model(nw, rmax, 5)
-    task = _abi.TaskArrays([(_abi.QUANTUM_METRIC, ["xx"])], broadening_type=_abi.LORENTZIAN, broadening=0.01)
+    task = _abi.TaskArrays([(_abi.SHIFT_CURRENT, ["xyy"])], broadening_type=_abi.LORENTZIAN, broadening=0.01)
     k = np.random.default_rng(19).random((12, 3))
     with engine_cls(model, task) as eng:
         e, c = eng.spectrum(k)
@@ -303,15 +303,16 @@ def test_nonorthogonal_generalized_spectrum_matches_oracle(engine_cls, oracle_mo
         assert np.max(np.abs(ov - 1.0)) < 1e-9
 
 
-def test_nonorthogonal_responses_rejected_and_indefinite_overlap_reported(engine_cls):
+def test_nonorthogonal_other_responses_rejected_and_indefinite_overlap_reported(engine_cls):
+    """Nonorthogonal models take the shift and injection currents; other kinds are refused at plan
+    creation, and a non-positive-definite S(k) is reported, never silently used."""
     from wanniernlqg_b200._lib import EngineError
     from wanniernlqg_b200.model import synthetic_nonorthogonal_model
     model = synthetic_nonorthogonal_model(6, 1, 2)
-    task = _abi.TaskArrays([(_abi.QUANTUM_METRIC, ["xx"])])
-    with engine_cls(model, task) as eng:
-        with pytest.raises(EngineError) as ei:
-            eng.integrate_mesh((2, 2, 2))
-        assert ei.value.status == 6
+    with pytest.raises(EngineError) as ei:
+        engine_cls(model, _abi.TaskArrays([(_abi.QUANTUM_METRIC, ["xx"])]))
+    assert ei.value.status == 6
+    task = _abi.TaskArrays([(_abi.SHIFT_CURRENT, ["xyy"])])
     bad = synthetic_nonorthogonal_model(6, 1, 2)
     home = int(np.where(np.all(bad.r_vectors == 0, axis=0))[0][0])
     bad.overlap_r[:, :, home] -= 2.0 * np.eye(6)       # S(k) = -I + small: not positive definite
@@ -319,6 +320,61 @@ def test_nonorthogonal_responses_rejected_and_indefinite_overlap_reported(engine
         with pytest.raises(EngineError) as ei:
             eng.spectrum(np.array([[0.1, 0.2, 0.3]]))
         assert ei.value.status == 1
+
+
+def _nonorth_full_position(nw, seed):
+    """Nonorthogonal synthetic model with the full off-diagonal position operator."""
+    from wanniernlqg_b200.model import synthetic_nonorthogonal_model
+    m = synthetic_nonorthogonal_model(nw, 1, seed)
+    full = synthetic_orthogonal_model(nw, 1, seed, full_position=True)
+    m.position_r = full.position_r
+    return m
+
+
+def _currents_task(precision=_abi.PRECISION_FP64, kind=_abi.LORENTZIAN, width=0.03):
+    return _abi.TaskArrays([(_abi.SHIFT_CURRENT, ["xyy", "zxy", "yzz"]), (_abi.INJECTION_CURRENT, ["xyy", "zzx"])],
+                           broadening_type=kind, broadening=width, photon_energies=np.linspace(0, 3, 40),
+                           precision=precision)
+
+
+@pytest.mark.parametrize("nw,precision", [(8, _abi.PRECISION_FP64), (8, _abi.PRECISION_MIXED),
+                                          (32, _abi.PRECISION_FP64)])
+def test_nonorthogonal_currents_match_oracle(engine_cls, oracle_mod, nw, precision):
+    """Metric geometry (nonorth_geometry_kernel) + the shared pair contraction against the oracle."""
+    model = _nonorth_full_position(nw, 7)
+    task = _currents_task(precision)
+    k = np.random.default_rng(41).random((5, 3))
+    with engine_cls(model, task) as eng:
+        got = eng.point_values(k)
+    ref = oracle_mod.point_values(model, task, k)
+    tol = RTOL if precision == _abi.PRECISION_FP64 else MIXED_RTOL
+    for g, r in zip(task.split(got), task.split(ref)):
+        assert rel_err(g, r) < tol
+
+
+def test_nonorthogonal_mesh_and_identity_overlap(engine_cls, oracle_mod):
+    """Mesh lanes for a nonorthogonal model against the oracle, and an identity overlap giving the
+    orthogonal engine's result (two different GPU geometries of one model)."""
+    import copy
+    model = _nonorth_full_position(8, 3)
+    task = _currents_task(kind=_abi.GAUSSIAN, width=0.06)
+    mesh = (5, 4, 3)
+    with engine_cls(model, task, max_batch=17) as eng:
+        got = eng.integrate_mesh(mesh)
+    ref = oracle_mod.integrate_mesh(model, task, mesh)
+    for g, r in zip(task.split(got), task.split(ref)):
+        assert rel_err(g, r) < RTOL
+    orth = synthetic_orthogonal_model(8, 1, 3, full_position=True)
+    ident = copy.deepcopy(orth)
+    home = int(np.where(np.all(orth.r_vectors == 0, axis=0))[0][0])
+    ident.overlap_r = np.zeros((8, 8, orth.num_r_vectors), dtype=np.complex128, order="F")
+    ident.overlap_r[:, :, home] = np.eye(8)
+    k = np.random.default_rng(42).random((4, 3))
+    with engine_cls(orth, task) as eng:
+        a = eng.point_values(k)
+    with engine_cls(ident, task) as eng:
+        b = eng.point_values(k)
+    assert np.max(np.abs(a - b)) <= 1e-10 * np.max(np.abs(a))
 
 
 # ---- orbital counts above 32: matrices in a per-CTA global working set ---------------------------
@@ -368,7 +424,7 @@ def test_large_nw_spectrum_matches_oracle(engine_cls, oracle_mod, nw):
 def test_large_nw_nonorthogonal_spectrum_matches_oracle(engine_cls, oracle_mod, nw):
     from wanniernlqg_b200.model import synthetic_nonorthogonal_model
     model = synthetic_nonorthogonal_model(nw, 1, seed=2)
-    task = _abi.TaskArrays([(_abi.QUANTUM_METRIC, ["xx"])])
+    task = _abi.TaskArrays([(_abi.INJECTION_CURRENT, ["xyy"])])
     k = np.random.default_rng(6).random((3, 3))
     with engine_cls(model, task) as eng:
         e, _ = eng.spectrum(k)

@@ -89,6 +89,15 @@ struct RespParams {
     // Shift/injection band window (-1: all bands) and the response degeneracy threshold.
     int band_window;
     double degeneracy_threshold;
+    // Nonorthogonal models: per-k geometry precomputed by nonorth_geometry_kernel (Berry
+    // connection r [batch][3][nn], Hellmann-Feynman slopes v [batch][3][nw], generalized
+    // derivatives [batch][ng_pairs][nn] with g_ng[g] the pair index of G slot g).  nullptr: the
+    // orthogonal geometry of this kernel.
+    const double2 *ng_r;
+    const double *ng_v;
+    const double2 *ng_G;
+    int ng_pairs;
+    int g_ng[RS_MAX_G];
 };
 
 // Effective band window [lo, hi) (0-based) around mu: select_band_window (CalculationUtils.jl:71-90),
@@ -386,57 +395,84 @@ __global__ void __launch_bounds__(256) response_kernel(RespParams p) {
             const double d = sE[i] - sE[j];
             sinv[e] = p.eta_reg == 0.0 ? (d == 0.0 ? 0.0 : 1.0 / d) : reg_inverse(d, p.eta_reg);
         }
-        for (int a = 0; a < 3; ++a)
-            if (p.slot_dH[a] >= 0) rotate_to_hamiltonian(xw + (int64_t)p.ch_dH[a] * nn, T1, T2, sU, slot(p.slot_dH[a]), nw, ld);
-        for (int a = 0; a < 3; ++a)
-            if (p.slot_A[a] >= 0) rotate_to_hamiltonian(xw + (int64_t)p.ch_A[a] * nn, T1, T2, sU, slot(p.slot_A[a]), nw, ld);
-        // Gauge corrections D_d = -dH_d .* inv for the derivative axes of the generalised derivatives.
-        for (int a = 0; a < 3; ++a)
-            if (p.slot_D[a] >= 0) {
-                C *D = slot(p.slot_D[a]);
-                const C *H = slot(p.slot_dH[a]);
-                for (int e = threadIdx.x; e < nn; e += blockDim.x) {
-                    const int i = e % nw, j = e / nw;
-                    D[i + ld * j] = cscale(H[i + ld * j], (R)(-sinv[e]));
+        if (p.ng_r) {
+            // Nonorthogonal model: Berry connection into the A slots, slopes on the dH diagonals,
+            // generalized derivatives into the G slots; r_elem then reads r directly (inv = 0).
+            for (int e = threadIdx.x; e < nn; e += blockDim.x) sinv[e] = 0.0;
+            for (int a = 0; a < 3; ++a) {
+                if (p.slot_A[a] >= 0) {
+                    C *dst = slot(p.slot_A[a]);
+                    const double2 *src = p.ng_r + (b * 3 + a) * (int64_t)nn;
+                    for (int e = threadIdx.x; e < nn; e += blockDim.x) dst[(e % nw) + ld * (e / nw)] = conv_c<C>(src[e]);
+                }
+                if (p.slot_dH[a] >= 0) {
+                    C *dst = slot(p.slot_dH[a]);
+                    const double *v = p.ng_v + (b * 3 + a) * (int64_t)nw;
+                    for (int e = threadIdx.x; e < nn; e += blockDim.x) {
+                        const int i = e % nw, j = e / nw;
+                        dst[i + ld * j] = conv_c<C>(make_double2(i == j ? v[i] : 0.0, 0.0));
+                    }
                 }
             }
-        __syncthreads();
+            for (int g = 0; g < p.n_g; ++g) {
+                C *dst = slot(p.g_slot[g]);
+                const double2 *src = p.ng_G + (b * p.ng_pairs + p.g_ng[g]) * (int64_t)nn;
+                for (int e = threadIdx.x; e < nn; e += blockDim.x) dst[(e % nw) + ld * (e / nw)] = conv_c<C>(src[e]);
+            }
+            __syncthreads();
+        } else {
+            for (int a = 0; a < 3; ++a)
+                if (p.slot_dH[a] >= 0) rotate_to_hamiltonian(xw + (int64_t)p.ch_dH[a] * nn, T1, T2, sU, slot(p.slot_dH[a]), nw, ld);
+            for (int a = 0; a < 3; ++a)
+                if (p.slot_A[a] >= 0) rotate_to_hamiltonian(xw + (int64_t)p.ch_A[a] * nn, T1, T2, sU, slot(p.slot_A[a]), nw, ld);
+            // Gauge corrections D_d = -dH_d .* inv for the derivative axes of the generalised derivatives.
+            for (int a = 0; a < 3; ++a)
+                if (p.slot_D[a] >= 0) {
+                    C *D = slot(p.slot_D[a]);
+                    const C *H = slot(p.slot_dH[a]);
+                    for (int e = threadIdx.x; e < nn; e += blockDim.x) {
+                        const int i = e % nw, j = e / nw;
+                        D[i + ld * j] = cscale(H[i + ld * j], (R)(-sinv[e]));
+                    }
+                }
+            __syncthreads();
 
-        // Generalised derivatives r^p_{nm;d} (ConventionalShiftCurrent.jl:191-229), with the
-        // l != n,m sums written as commutators (exact: D_nn = 0):
-        //   sum_AD + AD_bit = [A_p, D_d]_nm + (A_d,nn - A_d,mm) D_p,nm
-        //   sum_HD + DV_bit = [dH_p, D_d]_nm + (dH_d,nn - dH_d,mm) D_p,nm
-        for (int g = 0; g < p.n_g; ++g) {
-            const int pp = p.g_p[g], dd = p.g_d[g];
-            C *G = slot(p.g_slot[g]);
-            rotate_to_hamiltonian(xw + (int64_t)p.ch_dA[pp * 3 + dd] * nn, T1, T2, sU, G, nw, ld);
-            rotate_to_hamiltonian(xw + (int64_t)p.ch_ddH[pp * 3 + dd] * nn, T1, T2, sU, T1, nw, ld);
-            const C *Ap = slot(p.slot_A[pp]), *Ad = slot(p.slot_A[dd]);
-            const C *Hp = slot(p.slot_dH[pp]), *Hd = slot(p.slot_dH[dd]);
-            const C *Dd = slot(p.slot_D[dd]);
-            mm_comm(Ap, Dd, T2, nw, ld);
-            __syncthreads();
-            for (int e = threadIdx.x; e < nn; e += blockDim.x) {
-                const int n = e % nw, m = e / nw;
-                const int o = n + ld * m;
-                const C Dp = cscale(Hp[o], (R)(-sinv[e]));
-                const C dAd = csub(Ad[n + ld * n], Ad[m + ld * m]);
-                const C dHd = csub(Hd[n + ld * n], Hd[m + ld * m]);
-                // G <- dA + (A_d,nn - A_d,mm)(D_p - i A_p) + [A_p, D_d]
-                G[o] = cadd(cadd(G[o], cmul(dAd, csub(Dp, cmuli(Ap[o])))), T2[o]);
-                // T1 <- ddH + (dH_d,nn - dH_d,mm) D_p
-                T1[o] = cadd(T1[o], cmul(dHd, Dp));
+            // Generalised derivatives r^p_{nm;d} (ConventionalShiftCurrent.jl:191-229), with the
+            // l != n,m sums written as commutators (exact: D_nn = 0):
+            //   sum_AD + AD_bit = [A_p, D_d]_nm + (A_d,nn - A_d,mm) D_p,nm
+            //   sum_HD + DV_bit = [dH_p, D_d]_nm + (dH_d,nn - dH_d,mm) D_p,nm
+            for (int g = 0; g < p.n_g; ++g) {
+                const int pp = p.g_p[g], dd = p.g_d[g];
+                C *G = slot(p.g_slot[g]);
+                rotate_to_hamiltonian(xw + (int64_t)p.ch_dA[pp * 3 + dd] * nn, T1, T2, sU, G, nw, ld);
+                rotate_to_hamiltonian(xw + (int64_t)p.ch_ddH[pp * 3 + dd] * nn, T1, T2, sU, T1, nw, ld);
+                const C *Ap = slot(p.slot_A[pp]), *Ad = slot(p.slot_A[dd]);
+                const C *Hp = slot(p.slot_dH[pp]), *Hd = slot(p.slot_dH[dd]);
+                const C *Dd = slot(p.slot_D[dd]);
+                mm_comm(Ap, Dd, T2, nw, ld);
+                __syncthreads();
+                for (int e = threadIdx.x; e < nn; e += blockDim.x) {
+                    const int n = e % nw, m = e / nw;
+                    const int o = n + ld * m;
+                    const C Dp = cscale(Hp[o], (R)(-sinv[e]));
+                    const C dAd = csub(Ad[n + ld * n], Ad[m + ld * m]);
+                    const C dHd = csub(Hd[n + ld * n], Hd[m + ld * m]);
+                    // G <- dA + (A_d,nn - A_d,mm)(D_p - i A_p) + [A_p, D_d]
+                    G[o] = cadd(cadd(G[o], cmul(dAd, csub(Dp, cmuli(Ap[o])))), T2[o]);
+                    // T1 <- ddH + (dH_d,nn - dH_d,mm) D_p
+                    T1[o] = cadd(T1[o], cmul(dHd, Dp));
+                }
+                __syncthreads();
+                mm_comm(Hp, Dd, T2, nw, ld);
+                __syncthreads();
+                for (int e = threadIdx.x; e < nn; e += blockDim.x) {
+                    const int n = e % nw, m = e / nw;
+                    const int o = n + ld * m;
+                    const C h = cadd(T1[o], T2[o]);
+                    G[o] = cadd(G[o], cmuli(cscale(h, (R)(-sinv[e]))));
+                }
+                __syncthreads();
             }
-            __syncthreads();
-            mm_comm(Hp, Dd, T2, nw, ld);
-            __syncthreads();
-            for (int e = threadIdx.x; e < nn; e += blockDim.x) {
-                const int n = e % nw, m = e / nw;
-                const int o = n + ld * m;
-                const C h = cadd(T1[o], T2[o]);
-                G[o] = cadd(G[o], cmuli(cscale(h, (R)(-sinv[e]))));
-            }
-            __syncthreads();
         }
 
         // Scalar responses (FP64 block sums).

@@ -23,6 +23,7 @@
 #include "response.cuh"
 #include "shg.cuh"
 #include "tc_fourier.cuh"
+#include "nonorth.cuh"
 
 namespace {
 
@@ -41,7 +42,7 @@ wnlqg_status fail(wnlqg_status st, const std::string &msg) {
                         std::string(#call) + ": " + cudaGetErrorString(err_));                            \
     } while (0)
 
-enum ChannelOp { CH_H = 0, CH_DH = 1, CH_DDH = 2, CH_A = 3, CH_DA = 4, CH_S = 5 };
+enum ChannelOp { CH_H = 0, CH_DH = 1, CH_DDH = 2, CH_A = 3, CH_DA = 4, CH_S = 5, CH_DS = 6, CH_DDS = 7 };
 
 struct Channel {
     int op;
@@ -117,6 +118,13 @@ struct wnlqg_plan {
     int eigh_grid = 0;
     unsigned char *d_resp_scratch = nullptr;  // per-CTA global working set of the response passes
     int64_t resp_scratch_stride = 0;
+    // Nonorthogonal responses: metric geometry per batch (Berry connection, slopes, G pairs).
+    NonorthParams ng;
+    int ng_grid = 0;
+    int ng_gidx[9];
+    double2 *d_ng_r = nullptr, *d_ng_G = nullptr;
+    double *d_ng_v = nullptr;
+    unsigned char *d_ng_ws = nullptr;
     int refine_threads = 32;
     int sm_count = 148;
     size_t refine_smem = 0;
@@ -258,6 +266,7 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
             return (int)gl.size() - 1;
         };
         size_t start = i;
+        bool pass_global = global_mode;   // a pass whose first component alone exceeds shared memory
         while (i < items.size()) {
             const Item &it = items[i];
             // Tentatively add the item and check limits.
@@ -294,11 +303,15 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
             size_t smem = RespSmem::layout(pl->nw, nslots, nfc, 1, csize).total;
             bool fits = nfc <= RS_MAX_FREQ && nsc <= RS_MAX_SCALAR && nmi <= RS_MAX_SCALAR &&
                         (int)gl.size() + newg <= RS_MAX_G && (int)hl.size() + newh <= RS_MAX_HESS &&
-                        (global_mode || smem <= smem_limit);
+                        (pass_global || smem <= smem_limit);
             if (!fits) {
-                if (i == start)
-                    return fail(WNLQG_ERR_UNSUPPORTED, "one response component does not fit the shared-memory budget for nw=" +
-                                                           std::to_string(pl->nw));
+                if (i == start) {
+                    if (!pass_global) {
+                        pass_global = true;   // runs from the per-CTA global working set
+                        continue;
+                    }
+                    return fail(WNLQG_ERR_UNSUPPORTED, "one response component exceeds the per-pass limits");
+                }
                 break;
             }
             std::copy(tH, tH + 3, needH);
@@ -364,10 +377,10 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
         p.vc = pl->vc;
         p.xw_stride = (int64_t)pl->C * pl->nn;
         ps.smem = RespSmem::layout(pl->nw, p.n_slots, p.n_fc, 1, csize).total;
-        ps.global = global_mode;
+        ps.global = pass_global;
         ps.threads = response_threads(pl->nw);
         int per_sm = 0;
-        const size_t launch_smem = global_mode ? 0 : ps.smem;
+        const size_t launch_smem = pass_global ? 0 : ps.smem;
         cudaError_t e = mixed ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, response_kernel<float>, ps.threads, launch_smem)
                               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, response_kernel<double>, ps.threads, launch_smem);
         if (e != cudaSuccess) return fail(WNLQG_ERR_CUDA, std::string("occupancy query: ") + cudaGetErrorString(e));
@@ -375,10 +388,13 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
         ps.grid = sm_count * per_sm;
         pl->passes.push_back(ps);
     }
-    if (global_mode && !pl->passes.empty()) {
+    bool any_global = false;
+    for (const Pass &ps : pl->passes) any_global |= ps.global;
+    if (any_global) {
         int64_t grid = 0;
         size_t bytes = 0;
         for (const Pass &ps : pl->passes) {
+            if (!ps.global) continue;
             grid = std::max<int64_t>(grid, ps.grid);
             bytes = std::max(bytes, ps.smem);
         }
@@ -702,8 +718,24 @@ wnlqg_status run_front(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const int64_
 
 wnlqg_status run_passes(wnlqg_plan *pl, int64_t nb, int mode, double scale, int64_t point_offset,
                         const double *weights = nullptr) {
+    if (pl->nonorth) {
+        NonorthParams q = pl->ng;
+        q.batch = nb;
+        q.xw = pl->d_xw;
+        q.E = pl->d_E;
+        q.U = pl->d_U;
+        nonorth_geometry_kernel<<<(unsigned)std::min<int64_t>(nb, pl->ng_grid), 256, 0, pl->stream>>>(q);
+        pl->launches += 1;
+    }
     for (Pass &ps : pl->passes) {
         RespParams p = ps.params;
+        if (pl->nonorth) {
+            p.ng_r = pl->d_ng_r;
+            p.ng_v = pl->d_ng_v;
+            p.ng_G = pl->d_ng_G;
+            p.ng_pairs = pl->ng.npairs;
+            for (int g = 0; g < p.n_g; ++g) p.g_ng[g] = pl->ng_gidx[p.g_p[g] * 3 + p.g_d[g]];
+        }
         p.batch = nb;
         p.xw = pl->d_xw;
         p.E = pl->d_E;
@@ -847,7 +879,8 @@ wnlqg_status wnlqg_b200_plan_destroy(wnlqg_plan *pl) {
                       (void *)pl->d_stageZ, (void *)pl->d_V32, (void *)pl->d_kidx, (void *)pl->d_mus, (void *)pl->d_status,
                       (void *)pl->d_shg_scratch, (void *)pl->d_tcA, (void *)pl->d_tcB, (void *)pl->d_tc_colscale,
                       (void *)pl->d_tc_err, (void *)pl->d_shg_gscratch, (void *)pl->d_eigh_scratch,
-                      (void *)pl->d_resp_scratch})
+                      (void *)pl->d_resp_scratch, (void *)pl->d_ng_r, (void *)pl->d_ng_v, (void *)pl->d_ng_G,
+                      (void *)pl->d_ng_ws})
         if (ptr) cudaFree(ptr);
     for (cudaEvent_t ev : pl->events) cudaEventDestroy(ev);
     if (pl->stream) cudaStreamDestroy(pl->stream);
@@ -908,6 +941,9 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
             for (int i = 0; i < 4; ++i)
                 if (x[i] < 0 || x[i] > 2) return bail(fail(WNLQG_ERR_INVALID_ARGUMENT, "component axis out of range"));
             int a = x[0], b = x[1], cc = x[2];
+            if (model->has_overlap && q.kind != WNLQG_SHIFT_CURRENT && q.kind != WNLQG_INJECTION_CURRENT)
+                return bail(fail(WNLQG_ERR_UNSUPPORTED,
+                                 "nonorthogonal models: shift and injection current are built; other responses are not"));
             switch (q.kind) {
             case WNLQG_SHIFT_CURRENT: {
                 need_r(a); need_r(b); need_r(cc);
@@ -995,10 +1031,32 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
         }
     }
     pl->vc = vc;
+    for (int g = 0; g < 9; ++g) pl->ng_gidx[g] = -1;
     if (model->has_overlap) {
-        // Nonorthogonal model: the spectrum uses S(k); the response kernels are orthogonal-only.
+        // Nonorthogonal model: the spectrum uses S(k); the conventional currents take the metric
+        // geometry (dH, dS, r on all axes; d2H, d2S, dr per generalized-derivative pair).
         pl->nonorth = true;
         pl->ch_S = add_channel(ch, CH_S, 0, 0);
+        if (vc > 0) {
+            NonorthParams &q = pl->ng;
+            std::memset(&q, 0, sizeof(q));
+            for (int a = 0; a < 3; ++a) {
+                q.ch_dH[a] = pl->ch_dH[a] = add_channel(ch, CH_DH, a, 0);
+                q.ch_dS[a] = add_channel(ch, CH_DS, a, 0);
+                q.ch_A[a] = pl->ch_A[a] = add_channel(ch, CH_A, a, 0);
+            }
+            for (int pd = 0; pd < 9; ++pd) {
+                if (pl->ch_dA[pd] < 0) continue;
+                const int pp = pd / 3, dd = pd % 3, g = q.npairs++;
+                q.pair_p[g] = pp;
+                q.pair_d[g] = dd;
+                q.ch_dA[g] = pl->ch_dA[pd];
+                q.ch_ddH[g] = pl->ch_ddH[pd];
+                q.ch_ddS[g] = add_channel(ch, CH_DDS, pp, dd);
+                pl->ng_gidx[pd] = g;
+            }
+            q.eta = t.denominator_regularization;
+        }
     }
     pl->C = (int)ch.size();
 
@@ -1032,6 +1090,12 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
                     break;
                 case CH_S:
                     v = model->S[(size_t)r * nn + e];
+                    break;
+                case CH_DS:
+                    v = cmuli(cscale(model->S[(size_t)r * nn + e], rc[cc.p]));
+                    break;
+                case CH_DDS:
+                    v = cscale(model->S[(size_t)r * nn + e], -rc[cc.p] * rc[cc.d]);
                     break;
                 }
                 dst[e] = v;
@@ -1074,6 +1138,23 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
     if ((st = alloc((void **)&pl->d_weights, (size_t)max_batch * sizeof(double))) != WNLQG_OK) return bail(st);
     if ((st = alloc((void **)&pl->d_kidx, (size_t)max_batch * sizeof(int64_t))) != WNLQG_OK) return bail(st);
     if ((st = alloc((void **)&pl->d_status, (size_t)max_batch * sizeof(int))) != WNLQG_OK) return bail(st);
+    if (pl->nonorth && vc > 0) {
+        NonorthParams &q = pl->ng;
+        q.nw = nw;
+        q.ld = nw + 1;
+        q.xw_stride = (int64_t)pl->C * nn;
+        pl->ng_grid = 2 * sm_count;
+        q.ws_stride = (NonorthWs::bytes(nw) + 255) & ~(int64_t)255;
+        if ((st = alloc((void **)&pl->d_ng_r, (size_t)max_batch * 3 * nn * sizeof(double2))) != WNLQG_OK) return bail(st);
+        if ((st = alloc((void **)&pl->d_ng_v, (size_t)max_batch * 3 * nw * sizeof(double))) != WNLQG_OK) return bail(st);
+        if ((st = alloc((void **)&pl->d_ng_G, (size_t)max_batch * std::max(1, q.npairs) * nn * sizeof(double2))) != WNLQG_OK)
+            return bail(st);
+        if ((st = alloc((void **)&pl->d_ng_ws, (size_t)pl->ng_grid * q.ws_stride)) != WNLQG_OK) return bail(st);
+        q.r_out = pl->d_ng_r;
+        q.v_out = pl->d_ng_v;
+        q.g_out = pl->d_ng_G;
+        q.ws = pl->d_ng_ws;
+    }
     if ((st = alloc((void **)&pl->d_points, (size_t)max_batch * vc * sizeof(double2))) != WNLQG_OK) return bail(st);
     if ((st = alloc((void **)&pl->d_out, (size_t)vc * sizeof(double2))) != WNLQG_OK) return bail(st);
     if ((st = alloc((void **)&pl->d_omegas, std::max<size_t>(1, pl->omegas.size()) * sizeof(double))) != WNLQG_OK) return bail(st);
@@ -1209,7 +1290,6 @@ wnlqg_status wnlqg_b200_eval_mesh_device(wnlqg_plan *pl, const int64_t mesh[3], 
                                          double *out_device, void *stream) {
     wnlqg_status st = check_plan(pl);
     if (st != WNLQG_OK) return st;
-    if (pl->nonorth) return fail(WNLQG_ERR_UNSUPPORTED, "responses of nonorthogonal models are not built yet; eval_spectrum is");
     if (!mesh || !out_device) return fail(WNLQG_ERR_INVALID_ARGUMENT, "NULL argument");
     if (mesh[0] <= 0 || mesh[1] <= 0 || mesh[2] <= 0) return fail(WNLQG_ERR_INVALID_ARGUMENT, "mesh counts must be positive");
     const int64_t nk = mesh[0] * mesh[1] * mesh[2];
@@ -1265,7 +1345,6 @@ wnlqg_status wnlqg_b200_eval_points_weighted_device(wnlqg_plan *pl, const double
                                                     void *stream) {
     wnlqg_status st = check_plan(pl);
     if (st != WNLQG_OK) return st;
-    if (pl->nonorth) return fail(WNLQG_ERR_UNSUPPORTED, "responses of nonorthogonal models are not built yet; eval_spectrum is");
     if (n < 0 || (n > 0 && (!kpoints_device || !weights_device)) || !out_device)
         return fail(WNLQG_ERR_INVALID_ARGUMENT, "invalid points");
     WNLQG_CUDA(cudaSetDevice(pl->model->device));
@@ -1324,7 +1403,6 @@ wnlqg_status wnlqg_b200_eval_mesh(wnlqg_plan *pl, const int64_t mesh[3], int64_t
 wnlqg_status wnlqg_b200_eval_points(wnlqg_plan *pl, const double *kpoints, int64_t n, double *out) {
     wnlqg_status st = check_plan(pl);
     if (st != WNLQG_OK) return st;
-    if (pl->nonorth) return fail(WNLQG_ERR_UNSUPPORTED, "responses of nonorthogonal models are not built yet; eval_spectrum is");
     if (n < 0 || (n > 0 && (!kpoints || !out))) return fail(WNLQG_ERR_INVALID_ARGUMENT, "invalid points");
     if (!finite_array(kpoints, 3 * (size_t)n)) return fail(WNLQG_ERR_NONFINITE, "k-points must be finite");
     WNLQG_CUDA(cudaSetDevice(pl->model->device));
@@ -1350,7 +1428,6 @@ wnlqg_status wnlqg_b200_eval_points_weighted(wnlqg_plan *pl, const double *kpoin
                                              int64_t n, double *out) {
     wnlqg_status st = check_plan(pl);
     if (st != WNLQG_OK) return st;
-    if (pl->nonorth) return fail(WNLQG_ERR_UNSUPPORTED, "responses of nonorthogonal models are not built yet; eval_spectrum is");
     if (n < 0 || (n > 0 && (!kpoints || !weights)) || !out) return fail(WNLQG_ERR_INVALID_ARGUMENT, "invalid points");
     if (!finite_array(kpoints, 3 * (size_t)n) || !finite_array(weights, (size_t)n))
         return fail(WNLQG_ERR_NONFINITE, "k-points and weights must be finite");
@@ -1383,7 +1460,6 @@ wnlqg_status wnlqg_b200_eval_mesh_weighted(wnlqg_plan *pl, const int64_t mesh[3]
                                            const double *weights, int64_t n, double *out) {
     wnlqg_status st = check_plan(pl);
     if (st != WNLQG_OK) return st;
-    if (pl->nonorth) return fail(WNLQG_ERR_UNSUPPORTED, "responses of nonorthogonal models are not built yet; eval_spectrum is");
     if (!mesh || !out || n < 0 || (n > 0 && (!indices || !weights))) return fail(WNLQG_ERR_INVALID_ARGUMENT, "invalid arguments");
     if (mesh[0] <= 0 || mesh[1] <= 0 || mesh[2] <= 0) return fail(WNLQG_ERR_INVALID_ARGUMENT, "mesh counts must be positive");
     const int64_t nk = mesh[0] * mesh[1] * mesh[2];
