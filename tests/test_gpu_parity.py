@@ -459,3 +459,15 @@ def test_band_window_matches_oracle(engine_cls, oracle_mod, name, window, mu):
         assert np.all(ref == 0)
     else:
         assert not np.allclose(ref, ref_full)
+
+
+def test_kslice_map_on_gpu_matches_oracle(engine_cls, oracle_mod):
+    """A Berry-curvature / metric k-slice through one batched device call."""
+    from wanniernlqg_b200.kslice import kslice_map
+    model = reference_workload_model("nw32")
+    task = _abi.TaskArrays([(_abi.BERRY_CURVATURE, ["xy"]), (_abi.QUANTUM_METRIC, ["xx"])])
+    args = ([12, 9], [0.0, 0.0, 0.1], [1.0, 0.0, 0.0], [0.0, 1.0, 0.0])
+    with engine_cls(model, task) as eng:
+        got = kslice_map(eng.point_values, *args)
+    ref = kslice_map(lambda k: oracle_mod.point_values(model, task, k), *args)
+    assert rel_err(got, ref) < RTOL
