@@ -330,15 +330,26 @@ def main():
                 "achieved": flop[name] * batch / t_s / 1e12, "unit": "TFLOP/s", "peak": sm_peak, "peak_source": sm_src,
                 "hbm_gbs": hbm[name] * batch / t_s / 1e9}
 
+    # DRAM bytes per k-point (read + write) of each stage's kernel, from the committed ncu
+    # captures of 8192-point launches (profiles/*.md), scaled to the step's batch: the kernels
+    # stream their inputs point by point, so traffic grows in proportion to the points.
+    traffic_per_k = {
+        ("fp64", "response"): (1.080335e9 + 6.255872e6) / 8192,     # response_kernel_fp64_nw32_mesh.md
+        ("fp64", "eigen"): (0.084022e9 + 84.824064e6) / 8192,       # response_kernel_fp64_nw32_mesh.md
+        ("mixed", "response"): (1.084089e9 + 8.529664e6) / 8192,    # mixed_path_kernels_nw32_mesh.md
+        ("mixed", "fourier_random"): (436.281088e6 + 1.025739e9) / 8192,  # tc_fourier_kernel_nw32_random_k.md
+    }
+    prec_key = "fp64" if precision == _abi.PRECISION_FP64 else "mixed"
     per_stage = {}
     for name in stages:
         r = stage_roofline(name)
         r["frac"] = r["achieved"] / r["peak"] if r["peak"] else None
         r["ms_last_step"] = stages[name]
+        key = (prec_key, "fourier_random" if (name == "fourier" and random_mode) else name)
+        r["traffic"] = traffic_per_k[key] * batch if key in traffic_per_k else None
         per_stage[name] = r
     roofline = dict(per_stage[dominant])
     roofline.update({
-        "traffic": None,
         "stage_ms_last_step": {"fourier": fourier_ms, "eigen": eigen_ms, "response": response_ms, "total": total_ms},
         "stages": per_stage,
         "algorithmic_per_k": {"flop": flop, "hbm_bytes": hbm, "tensor_int8_ops": tc_ops if random_mode else None},
