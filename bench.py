@@ -188,6 +188,8 @@ def main():
                     help="plan batch capacity (0: one step, --batch points; a 65536-point nw=32 step holds ~11 GB)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the batched uneven-models measurement (one GPU only)")
     ap.add_argument("--no-time-to-tolerance", action="store_true",
                     help="skip the time-to-1e-4 convergence study of sigma^xyy (one GPU only)")
     args = ap.parse_args()
@@ -380,6 +382,8 @@ def main():
     engine.close()
     if rank == 0 and world == 1 and not args.no_time_to_tolerance:
         line["time_to_tolerance"] = time_to_tolerance(model, local_rank)
+    if rank == 0 and world == 1 and not args.no_batched:
+        line["batched_uneven"] = batched_uneven(local_rank)
     if dist:
         dist.destroy_process_group()
     if rank == 0:
@@ -417,6 +421,62 @@ def time_to_tolerance(model, device: int, rtol: float = 1e-4, blocks: int = 4, b
             "mixed_vs_fp64_max_rel_error": err, "within_rtol": err <= rtol,
             "fp64_seconds_full_mesh": t64 * scale, "mixed_seconds_full_mesh": tmx * scale,
             "speedup_mixed_vs_fp64": t64 / tmx}
+
+
+def batched_uneven(device: int, mesh: int = 16) -> dict:
+    """Several models of uneven orbital counts through one call: 12 seeded models with
+    nw in {6, 8, 12, 16, 24, 32}, every second one Kramers-doubled (H (x) I_2 + i 1e-3 eV M (x)
+    sigma_z, so nw up to 64), intrinsic AHC sigma^xy and Berry-curvature dipole D^xzz at
+    mu in {-0.5, 0, 0.5} eV and T = 50 K, each on its own mesh^3 mesh.  Timed (CUDA events on the
+    caller's stream) as one concurrent wnlqg_b200_eval_mesh_many call and as the same models one
+    call after another."""
+    import torch
+    from wanniernlqg_b200.engine import ResponseEngine, integrate_meshes_many
+    from wanniernlqg_b200.model import kramers_doubled_model, synthetic_orthogonal_model
+
+    task = _abi.TaskArrays([(_abi.INTRINSIC_AHC, ["xy"]), (_abi.BERRY_DIPOLE, ["xzz"])],
+                           fermi_energies=[-0.5, 0.0, 0.5], temperature=50.0)
+    models = []
+    for i, nw in enumerate([6, 8, 12, 16, 24, 32] * 2):
+        base = synthetic_orthogonal_model(nw, 2 if nw <= 16 else 1, seed=100 + i, full_position=True)
+        models.append(kramers_doubled_model(base, 1e-3, seed=i) if i % 2 else base)
+    nk = mesh ** 3
+    engines = [ResponseEngine(m, task, device=device, max_batch=nk) for m in models]
+    try:
+        outs = [torch.zeros(2 * e.value_count, dtype=torch.float64, device="cuda") for e in engines]
+        meshes = [(mesh, mesh, mesh)] * len(engines)
+        ranges = [(0, nk)] * len(engines)
+        stream = torch.cuda.current_stream()
+        ptrs = [o.data_ptr() for o in outs]
+
+        def concurrent():
+            integrate_meshes_many(engines, meshes, ranges, ptrs, stream.cuda_stream)
+
+        def sequential():
+            for e, o in zip(engines, outs):
+                e.integrate_mesh_device(meshes[0], 0, nk, o.data_ptr(), stream.cuda_stream)
+                torch.cuda.synchronize()
+
+        def timed(fn):
+            fn()
+            torch.cuda.synchronize()
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            fn()
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            return ev0.elapsed_time(ev1)
+
+        t_conc = timed(concurrent)
+        t_seq = timed(sequential)
+    finally:
+        for e in engines:
+            e.close()
+    total = nk * len(models)
+    return {"models": len(models), "orbitals": [m.num_orbitals for m in models], "mesh": mesh,
+            "responses": "AHC xy + Berry dipole xzz at 3 Fermi energies, T = 50 K",
+            "concurrent_ms": t_conc, "sequential_ms": t_seq, "speedup": t_seq / t_conc,
+            "kpoints_per_s": total / (t_conc / 1e3)}
 
 
 def fourier_channels(task) -> int:

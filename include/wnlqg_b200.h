@@ -165,6 +165,17 @@ WNLQG_API wnlqg_status wnlqg_b200_eval_mesh_device(wnlqg_plan *plan, const int64
                                          int64_t k_begin, int64_t k_end, double *out_device,
                                          void *stream);
 
+/* Several plans (for example models of different orbital counts) in one call: plan i sums its
+ * mesh meshes[3*i..3*i+2] over [k_begin[i], k_end[i]) into outs_device[i] (device, plan value
+ * count complex values), exactly as wnlqg_b200_eval_mesh_device.  Every plan works on its own
+ * stream after `stream` (NULL = legacy default stream) and joins back into it, so the models'
+ * kernels overlap on the device.  Asynchronous; all plans must live on one device.  Batches the
+ * per-worker task loop of execute_prepared_tasks! (TaskSamplingScheduler.jl:151-217) across
+ * tasks. */
+WNLQG_API wnlqg_status wnlqg_b200_eval_mesh_many(wnlqg_plan *const *plans, int32_t count, const int64_t *meshes,
+                                       const int64_t *k_begin, const int64_t *k_end,
+                                       double *const *outs_device, void *stream);
+
 /* Per-point values at arbitrary fractional k-points: k[3*n] (host), out[n*value_count]
  * complex (host).  This is the ResponsePointEvaluator / ResponseNodeEvaluator contract
  * (Runtime/Execution/ResponsePointEvaluation.jl:8-64) batched over n points, used by the

@@ -471,3 +471,33 @@ def test_kslice_map_on_gpu_matches_oracle(engine_cls, oracle_mod):
         got = kslice_map(eng.point_values, *args)
     ref = kslice_map(lambda k: oracle_mod.point_values(model, task, k), *args)
     assert rel_err(got, ref) < RTOL
+
+
+def test_eval_mesh_many_uneven_models(engine_cls, oracle_mod):
+    """Models of different orbital counts (half Kramers-doubled with an O(1e-3 eV) splitting) in
+    one concurrent call: each result equals the model's own evaluation and the oracle."""
+    import torch
+    from wanniernlqg_b200.engine import integrate_meshes_many
+    from wanniernlqg_b200.model import kramers_doubled_model
+    models = []
+    for i, nw in enumerate([6, 8, 12, 16]):
+        base = synthetic_orthogonal_model(nw, 1, seed=20 + i, full_position=True)
+        models.append(kramers_doubled_model(base, 1e-3, seed=i) if i % 2 else base)
+    task = _abi.TaskArrays([(_abi.INTRINSIC_AHC, ["xy"]), (_abi.BERRY_DIPOLE, ["xzz"])],
+                           fermi_energies=[-0.5, 0.0, 0.5], temperature=50.0)
+    engines = [engine_cls(m, task) for m in models]
+    try:
+        meshes = [(6, 5, 4), (4, 4, 4), (5, 3, 3), (3, 3, 4)]
+        ranges = [(0, int(np.prod(ms))) for ms in meshes]
+        outs = [torch.zeros(2 * e.value_count, dtype=torch.float64, device="cuda") for e in engines]
+        integrate_meshes_many(engines, meshes, ranges, [o.data_ptr() for o in outs])
+        torch.cuda.synchronize()
+        for e, m, ms, o in zip(engines, models, meshes, outs):
+            got = o.cpu().numpy().view(np.complex128)
+            single = e.integrate_mesh(ms)
+            assert np.array_equal(got, single)
+            ref = oracle_mod.integrate_mesh(m, task, ms)
+            assert rel_err(got, ref) < RTOL
+    finally:
+        for e in engines:
+            e.close()

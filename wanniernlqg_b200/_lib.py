@@ -17,7 +17,7 @@ EXPORTED_SYMBOLS = (
     "wnlqg_b200_version", "wnlqg_b200_last_error", "wnlqg_b200_device_count",
     "wnlqg_b200_model_create", "wnlqg_b200_model_destroy",
     "wnlqg_b200_plan_create", "wnlqg_b200_plan_destroy", "wnlqg_b200_plan_value_count",
-    "wnlqg_b200_eval_mesh", "wnlqg_b200_eval_mesh_device", "wnlqg_b200_eval_points",
+    "wnlqg_b200_eval_mesh", "wnlqg_b200_eval_mesh_device", "wnlqg_b200_eval_mesh_many", "wnlqg_b200_eval_points",
     "wnlqg_b200_eval_points_weighted", "wnlqg_b200_eval_points_weighted_device", "wnlqg_b200_eval_mesh_weighted",
     "wnlqg_b200_eval_spectrum", "wnlqg_b200_plan_last_timing", "wnlqg_b200_plan_last_launch_count",
     "wnlqg_b200_spectrum_noalloc",
@@ -60,6 +60,7 @@ def load():
     L.wnlqg_b200_plan_value_count.argtypes = [vp]
     L.wnlqg_b200_eval_mesh.argtypes = [vp, ip, ctypes.c_int64, ctypes.c_int64, dp]
     L.wnlqg_b200_eval_mesh_device.argtypes = [vp, ip, ctypes.c_int64, ctypes.c_int64, vp, vp]
+    L.wnlqg_b200_eval_mesh_many.argtypes = [ctypes.POINTER(vp), ctypes.c_int32, ip, ip, ip, ctypes.POINTER(vp), vp]
     L.wnlqg_b200_eval_points.argtypes = [vp, dp, ctypes.c_int64, dp]
     L.wnlqg_b200_eval_points_weighted.argtypes = [vp, dp, dp, ctypes.c_int64, dp]
     L.wnlqg_b200_eval_points_weighted_device.argtypes = [vp, vp, vp, ctypes.c_int64, vp, vp]
@@ -87,7 +88,8 @@ def load():
     L.wnlqg_b200_plan_last_launch_count.argtypes = [vp]
     for name in ("wnlqg_b200_last_error", "wnlqg_b200_model_create", "wnlqg_b200_model_destroy",
                  "wnlqg_b200_plan_create", "wnlqg_b200_plan_destroy", "wnlqg_b200_eval_mesh",
-                 "wnlqg_b200_eval_mesh_device", "wnlqg_b200_eval_points", "wnlqg_b200_eval_points_weighted",
+                 "wnlqg_b200_eval_mesh_device", "wnlqg_b200_eval_mesh_many", "wnlqg_b200_eval_points",
+                 "wnlqg_b200_eval_points_weighted",
                  "wnlqg_b200_eval_points_weighted_device", "wnlqg_b200_eval_mesh_weighted", "wnlqg_b200_eval_spectrum",
                  "wnlqg_b200_plan_last_timing"):
         getattr(L, name).restype = ctypes.c_int

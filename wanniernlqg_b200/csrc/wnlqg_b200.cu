@@ -1386,6 +1386,26 @@ wnlqg_status wnlqg_b200_eval_points_weighted_device(wnlqg_plan *pl, const double
     return WNLQG_OK;
 }
 
+wnlqg_status wnlqg_b200_eval_mesh_many(wnlqg_plan *const *plans, int32_t count, const int64_t *meshes,
+                                       const int64_t *k_begin, const int64_t *k_end, double *const *outs_device,
+                                       void *stream) {
+    if (count < 0 || (count > 0 && (!plans || !meshes || !k_begin || !k_end || !outs_device)))
+        return fail(WNLQG_ERR_INVALID_ARGUMENT, "invalid plan list");
+    for (int32_t i = 0; i < count; ++i) {
+        wnlqg_status st = check_plan(plans[i]);
+        if (st != WNLQG_OK) return st;
+        if (i > 0 && plans[i]->model->device != plans[0]->model->device)
+            return fail(WNLQG_ERR_INVALID_ARGUMENT, "all plans of one call must live on one device");
+    }
+    // Each plan runs on its own stream after the caller's stream and joins back into it, so the
+    // models' kernels overlap on the device.
+    for (int32_t i = 0; i < count; ++i) {
+        wnlqg_status st = wnlqg_b200_eval_mesh_device(plans[i], meshes + 3 * i, k_begin[i], k_end[i], outs_device[i], stream);
+        if (st != WNLQG_OK) return st;
+    }
+    return WNLQG_OK;
+}
+
 wnlqg_status wnlqg_b200_eval_mesh(wnlqg_plan *pl, const int64_t mesh[3], int64_t k_begin, int64_t k_end, double *out) {
     wnlqg_status st = check_plan(pl);
     if (st != WNLQG_OK) return st;

@@ -145,3 +145,20 @@ class ResponseEngine:
 
     def last_launch_count(self) -> int:
         return int(self._L.wnlqg_b200_plan_last_launch_count(self._plan))
+
+
+def integrate_meshes_many(engines, meshes, ranges, outs_device, stream_ptr: int = 0) -> None:
+    """Mesh sums of several engines (models) in one asynchronous call (wnlqg_b200_eval_mesh_many):
+    engine i sums meshes[i] over ranges[i] = (k_begin, k_end) into the device pointer outs_device[i];
+    the engines' kernels overlap on the device.  All engines must use one device."""
+    n = len(engines)
+    L = _lib.load()
+    vp = ctypes.c_void_p
+    plans = (vp * n)(*[e._plan for e in engines])
+    mesh_a = np.ascontiguousarray(np.asarray(meshes, dtype=np.int64).reshape(n, 3))
+    kb = np.ascontiguousarray(np.array([r[0] for r in ranges], dtype=np.int64))
+    ke = np.ascontiguousarray(np.array([r[1] for r in ranges], dtype=np.int64))
+    outs = (vp * n)(*[vp(o) for o in outs_device])
+    ip = ctypes.POINTER(ctypes.c_int64)
+    _lib.check(L.wnlqg_b200_eval_mesh_many(plans, n, mesh_a.ctypes.data_as(ip), kb.ctypes.data_as(ip),
+                                           ke.ctypes.data_as(ip), outs, vp(stream_ptr)))

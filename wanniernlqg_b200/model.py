@@ -246,6 +246,29 @@ def synthetic_nonorthogonal_model(nw: int, rmax: int, seed: int = 0, *, overlap_
     return base
 
 
+def kramers_doubled_model(model: TightBindingModel, lam: float = 1e-3, seed: int = 0) -> TightBindingModel:
+    """H (x) I_2 plus the home-cell orbital-mixing term i lam (M (x) sigma_z) with a real
+    antisymmetric M (Hermitian: (i lam M (x) sigma_z)^H = i lam M (x) sigma_z), which splits the
+    doubled bands by O(lam) and so creates near-degenerate pairs; positions A (x) I_2."""
+    rng = np.random.default_rng(seed)
+    nw, nr = model.num_orbitals, model.num_r_vectors
+    x = rng.standard_normal((nw, nw))
+    M = (x - x.T) / 2.0
+    sz = np.diag([1.0, -1.0])
+    ham = np.zeros((2 * nw, 2 * nw, nr), dtype=np.complex128, order="F")
+    for r in range(nr):
+        ham[:, :, r] = np.kron(model.hamiltonian_r[:, :, r], np.eye(2))
+    home = int(np.where(np.all(model.r_vectors == 0, axis=0))[0][0])
+    ham[:, :, home] += 1j * lam * np.kron(M, sz)
+    pos = None
+    if model.position_r is not None:
+        pos = np.zeros((2 * nw, 2 * nw, 3, nr), dtype=np.complex128, order="F")
+        for r in range(nr):
+            for a in range(3):
+                pos[:, :, a, r] = np.kron(model.position_r[:, :, a, r], np.eye(2))
+    return TightBindingModel(model.lattice.copy(), model.r_vectors.copy(), model.r_degeneracies.copy(), ham, pos)
+
+
 def reference_workload_model(name: str) -> TightBindingModel:
     """Models of the reference workloads, by the short name used in tests and the bench.
 
