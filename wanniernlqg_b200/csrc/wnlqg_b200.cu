@@ -1286,26 +1286,34 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
 
 int64_t wnlqg_b200_plan_value_count(const wnlqg_plan *plan) { return plan ? plan->vc : -1; }
 
-wnlqg_status wnlqg_b200_eval_mesh_device(wnlqg_plan *pl, const int64_t mesh[3], int64_t k_begin, int64_t k_end,
-                                         double *out_device, void *stream) {
+}  // extern "C"
+
+namespace {
+
+wnlqg_status check_mesh_args(wnlqg_plan *pl, const int64_t mesh[3], int64_t k_begin, int64_t k_end, const double *out) {
     wnlqg_status st = check_plan(pl);
     if (st != WNLQG_OK) return st;
-    if (!mesh || !out_device) return fail(WNLQG_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (!mesh || !out) return fail(WNLQG_ERR_INVALID_ARGUMENT, "NULL argument");
     if (mesh[0] <= 0 || mesh[1] <= 0 || mesh[2] <= 0) return fail(WNLQG_ERR_INVALID_ARGUMENT, "mesh counts must be positive");
     const int64_t nk = mesh[0] * mesh[1] * mesh[2];
     if (k_begin < 0 || k_end > nk || k_begin > k_end) return fail(WNLQG_ERR_INVALID_ARGUMENT, "k range outside the mesh");
-    WNLQG_CUDA(cudaSetDevice(pl->model->device));
-    // The caller's stream (NULL = the legacy default stream) and the plan's non-blocking stream
-    // are ordered both ways with events: the work starts after everything queued on the caller's
-    // stream and the caller's stream resumes after the result is written.
-    cudaStream_t user = static_cast<cudaStream_t>(stream);
-    {
-        cudaEvent_t ev;
-        WNLQG_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-        WNLQG_CUDA(cudaEventRecord(ev, user));
-        WNLQG_CUDA(cudaStreamWaitEvent(pl->stream, ev, 0));
-        cudaEventDestroy(ev);
-    }
+    return WNLQG_OK;
+}
+
+// Stream a's subsequent work waits for everything queued on stream b so far.
+wnlqg_status stream_after(cudaStream_t a, cudaStream_t b) {
+    cudaEvent_t ev;
+    WNLQG_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    WNLQG_CUDA(cudaEventRecord(ev, b));
+    WNLQG_CUDA(cudaStreamWaitEvent(a, ev, 0));
+    cudaEventDestroy(ev);
+    return WNLQG_OK;
+}
+
+// The mesh sum on the plan's own stream (ordering with other streams is the caller's).
+wnlqg_status enqueue_mesh(wnlqg_plan *pl, const int64_t mesh[3], int64_t k_begin, int64_t k_end, double *out_device) {
+    wnlqg_status st;
+    const int64_t nk = mesh[0] * mesh[1] * mesh[2];
     if ((st = record_event(pl, 0)) != WNLQG_OK) return st;
     pl->launches = 0;
     WNLQG_CUDA(cudaMemsetAsync(pl->d_partials, 0, (size_t)pl->partial_slots * pl->vc * 4 * sizeof(double), pl->stream));
@@ -1327,17 +1335,28 @@ wnlqg_status wnlqg_b200_eval_mesh_device(wnlqg_plan *pl, const int64_t mesh[3], 
     pl->launches += 1;
     WNLQG_CUDA(cudaGetLastError());
     if ((st = record_event(pl, final_ev + 1)) != WNLQG_OK) return st;
-    pl->timing_valid = false;
-    {
-        cudaEvent_t ev;
-        WNLQG_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-        WNLQG_CUDA(cudaEventRecord(ev, pl->stream));
-        WNLQG_CUDA(cudaStreamWaitEvent(user, ev, 0));
-        cudaEventDestroy(ev);
-    }
     pl->timing_valid = true;
     pl->timing_batches = nbatch;
     return WNLQG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+wnlqg_status wnlqg_b200_eval_mesh_device(wnlqg_plan *pl, const int64_t mesh[3], int64_t k_begin, int64_t k_end,
+                                         double *out_device, void *stream) {
+    wnlqg_status st = check_mesh_args(pl, mesh, k_begin, k_end, out_device);
+    if (st != WNLQG_OK) return st;
+    WNLQG_CUDA(cudaSetDevice(pl->model->device));
+    // The caller's stream (NULL = the legacy default stream) and the plan's non-blocking stream
+    // are ordered both ways with events: the work starts after everything queued on the caller's
+    // stream and the caller's stream resumes after the result is written.
+    cudaStream_t user = static_cast<cudaStream_t>(stream);
+    pl->timing_valid = false;
+    if ((st = stream_after(pl->stream, user)) != WNLQG_OK) return st;
+    if ((st = enqueue_mesh(pl, mesh, k_begin, k_end, out_device)) != WNLQG_OK) return st;
+    return stream_after(user, pl->stream);
 }
 
 wnlqg_status wnlqg_b200_eval_points_weighted_device(wnlqg_plan *pl, const double *kpoints_device,
@@ -1397,10 +1416,33 @@ wnlqg_status wnlqg_b200_eval_mesh_many(wnlqg_plan *const *plans, int32_t count, 
         if (i > 0 && plans[i]->model->device != plans[0]->model->device)
             return fail(WNLQG_ERR_INVALID_ARGUMENT, "all plans of one call must live on one device");
     }
-    // Each plan runs on its own stream after the caller's stream and joins back into it, so the
-    // models' kernels overlap on the device.
+    // Every plan's stream forks from the caller's stream before any plan is enqueued and joins back
+    // after all are, so the models' kernels overlap on the device.
     for (int32_t i = 0; i < count; ++i) {
-        wnlqg_status st = wnlqg_b200_eval_mesh_device(plans[i], meshes + 3 * i, k_begin[i], k_end[i], outs_device[i], stream);
+        wnlqg_status st = check_mesh_args(plans[i], meshes + 3 * i, k_begin[i], k_end[i], outs_device[i]);
+        if (st != WNLQG_OK) return st;
+    }
+    if (count == 0) return WNLQG_OK;
+    WNLQG_CUDA(cudaSetDevice(plans[0]->model->device));
+    cudaStream_t user = static_cast<cudaStream_t>(stream);
+    cudaEvent_t fork;
+    WNLQG_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    WNLQG_CUDA(cudaEventRecord(fork, user));
+    for (int32_t i = 0; i < count; ++i) {
+        plans[i]->timing_valid = false;
+        cudaError_t e = cudaStreamWaitEvent(plans[i]->stream, fork, 0);
+        if (e != cudaSuccess) {
+            cudaEventDestroy(fork);
+            return fail(WNLQG_ERR_CUDA, std::string("cudaStreamWaitEvent: ") + cudaGetErrorString(e));
+        }
+    }
+    cudaEventDestroy(fork);
+    for (int32_t i = 0; i < count; ++i) {
+        wnlqg_status st = enqueue_mesh(plans[i], meshes + 3 * i, k_begin[i], k_end[i], outs_device[i]);
+        if (st != WNLQG_OK) return st;
+    }
+    for (int32_t i = 0; i < count; ++i) {
+        wnlqg_status st = stream_after(user, plans[i]->stream);
         if (st != WNLQG_OK) return st;
     }
     return WNLQG_OK;
