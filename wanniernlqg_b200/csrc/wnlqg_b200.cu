@@ -164,6 +164,13 @@ double lattice_det(const double *L) {
            e(0, 2) * (e(1, 0) * e(2, 1) - e(1, 1) * e(2, 0));
 }
 
+// CTAs whose working sets live in global memory: as many as the launch allows while the grid's
+// working sets together stay within ~96 MB of the 126 MB L2 (at least half the SMs stay busy).
+int l2_resident_grid(int grid, int64_t bytes_per_cta, int sm_count) {
+    const int64_t cap = std::max<int64_t>(sm_count / 2, ((int64_t)96 << 20) / std::max<int64_t>(1, bytes_per_cta));
+    return (int)std::max<int64_t>(1, std::min<int64_t>(grid, cap));
+}
+
 int eigh_block_threads(int nw) {
     int np = nw + (nw & 1);
     int blocks = (np / 2) * (np / 2);
@@ -386,6 +393,7 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
         if (e != cudaSuccess) return fail(WNLQG_ERR_CUDA, std::string("occupancy query: ") + cudaGetErrorString(e));
         if (per_sm < 1) return fail(WNLQG_ERR_UNSUPPORTED, "response kernel cannot be resident with its shared memory");
         ps.grid = sm_count * per_sm;
+        if (pass_global) ps.grid = l2_resident_grid(ps.grid, (int64_t)ps.smem, sm_count);
         pl->passes.push_back(ps);
     }
     bool any_global = false;
@@ -465,6 +473,7 @@ wnlqg_status build_shg(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
     if (e != cudaSuccess) return fail(WNLQG_ERR_CUDA, std::string("occupancy query: ") + cudaGetErrorString(e));
     if (per_sm < 1) return fail(WNLQG_ERR_UNSUPPORTED, "second-harmonic kernel cannot be resident with its shared memory");
     pl->shg_grid = sm_count * per_sm;
+    if (shg_global) pl->shg_grid = l2_resident_grid(pl->shg_grid, (int64_t)shg_bytes, sm_count);
     const int64_t stride = ShgSmem::scratch_entries(pl->nw, max_nc);
     for (ShgParams &p : pl->shg) p.scratch_stride = stride;
     e = cudaMalloc(&pl->d_shg_scratch, (size_t)pl->shg_grid * stride * sizeof(double2));
@@ -1143,8 +1152,8 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
         q.nw = nw;
         q.ld = nw + 1;
         q.xw_stride = (int64_t)pl->C * nn;
-        pl->ng_grid = 2 * sm_count;
         q.ws_stride = (NonorthWs::bytes(nw) + 255) & ~(int64_t)255;
+        pl->ng_grid = l2_resident_grid(2 * sm_count, q.ws_stride, sm_count);
         if ((st = alloc((void **)&pl->d_ng_r, (size_t)max_batch * 3 * nn * sizeof(double2))) != WNLQG_OK) return bail(st);
         if ((st = alloc((void **)&pl->d_ng_v, (size_t)max_batch * 3 * nw * sizeof(double))) != WNLQG_OK) return bail(st);
         if ((st = alloc((void **)&pl->d_ng_G, (size_t)max_batch * std::max(1, q.npairs) * nn * sizeof(double2))) != WNLQG_OK)
@@ -1249,8 +1258,8 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
         // CTA eigensolvers keep A, V (and the Cholesky factor) in shared memory when they fit,
         // else in a per-CTA global working set (large nw).
         if (pl->eigh_smem > (size_t)smem_optin) {
-            pl->eigh_grid = 4 * sm_count;
             pl->eigh_scratch_stride = (int64_t)((pl->eigh_smem + 255) & ~(size_t)255);
+            pl->eigh_grid = l2_resident_grid(4 * sm_count, pl->eigh_scratch_stride, sm_count);
             if ((st = alloc((void **)&pl->d_eigh_scratch, (size_t)pl->eigh_grid * pl->eigh_scratch_stride)) != WNLQG_OK)
                 return bail(st);
             pl->eigh_smem = 0;
