@@ -207,6 +207,34 @@ def test_mixed_eigensolver_refined_to_fp64(engine_cls, oracle_mod, name, monkeyp
         assert np.max(np.abs(ov - 1.0)) < 1e-8, (i, np.max(np.abs(ov - 1.0)), np.min(np.diff(eo)))
 
 
+@pytest.mark.parametrize("name", ["nw4", "nw32"])
+def test_fp64_warp_eigensolver_matches_cta_jacobi(engine_cls, name, monkeypatch):
+    """FP64 path up to 32 orbitals: FP32 warp Jacobi as preconditioner, then FP64 sweeps to the
+    CTA Jacobi's stopping rule.  Same spectrum as the FP64 CTA Jacobi (WNLQG_B200_CTA_EIGH=1) to
+    1e-13 of the largest |E|, eigenvectors equal up to phase, and the same mesh response to 1e-12."""
+    model = reference_workload_model(name)
+    task = nw4_task() if name == "nw4" else nw32_task()
+    k = np.random.default_rng(17).random((32, 3))
+    mesh = (6, 6, 6)
+    with engine_cls(model, task) as eng:
+        e_w, u_w = eng.spectrum(k)
+        m_w = eng.integrate_mesh(mesh)
+    monkeypatch.setenv("WNLQG_B200_CTA_EIGH", "1")
+    with engine_cls(model, task) as eng:
+        e_c, u_c = eng.spectrum(k)
+        m_c = eng.integrate_mesh(mesh)
+    assert np.max(np.abs(e_w - e_c)) < 1e-13 * max(1.0, np.abs(e_c).max())
+    for i in range(k.shape[0]):
+        gaps = np.diff(e_c[i])
+        ov = np.abs(np.sum(u_w[i].conj() * u_c[i], axis=0))
+        isolated = np.ones(e_c.shape[1], dtype=bool)
+        isolated[:-1] &= gaps > 1e-6
+        isolated[1:] &= gaps > 1e-6
+        assert np.max(np.abs(ov[isolated] - 1.0)) < 1e-10
+    for g, r in zip(task.split(m_w), task.split(m_c)):
+        assert rel_err(g, r) < 1e-12
+
+
 @pytest.mark.parametrize("name,precision,slices", [("nw4", _abi.PRECISION_FP64, 7), ("nw32", _abi.PRECISION_FP64, 7),
                                                    ("nw4", _abi.PRECISION_MIXED, 4), ("nw32", _abi.PRECISION_MIXED, 4)])
 def test_tensor_core_fourier_eigenvalues_within_slice_bound(engine_cls, oracle_mod, name, precision, slices):
@@ -501,3 +529,21 @@ def test_eval_mesh_many_uneven_models(engine_cls, oracle_mod):
     finally:
         for e in engines:
             e.close()
+
+
+@pytest.mark.parametrize("precision", [_abi.PRECISION_FP64, _abi.PRECISION_MIXED])
+def test_plans_of_different_sizes_share_kernels(engine_cls, oracle_mod, precision):
+    """A smaller plan created after a larger one leaves the larger one usable: kernel attributes
+    (dynamic shared memory limits) are per kernel, not per plan."""
+    big = reference_workload_model("nw32")
+    small = synthetic_orthogonal_model(4, 1, seed=3, full_position=True)
+    task = nw32_task(nom=64, precision=precision)
+    k = np.random.default_rng(21).random((8, 3))
+    with engine_cls(big, task) as eng_big:
+        with engine_cls(small, task) as eng_small:
+            eng_small.point_values(k)
+            got = eng_big.point_values(k)
+    ref = oracle_mod.point_values(big, task, k)
+    tol = RTOL if precision == _abi.PRECISION_FP64 else MIXED_RTOL
+    for g, r in zip(task.split(got), task.split(ref)):
+        assert rel_err(g, r) < tol

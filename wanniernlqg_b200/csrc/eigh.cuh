@@ -145,13 +145,15 @@ WNLQG_D double offdiag_norm(const C *A, int np, int ld, double *red) {
 // Outputs: energies E[b*nw + n] (double) and U[b*nw*nw + i + nw*n] (complex double).
 // gscratch (optional): a per-CTA working set of EighSmem::bytes in global memory, used when the
 // matrices do not fit shared memory (large nw).
-template <typename T>
-__global__ void jacobi_eigh_kernel(const double2 *__restrict__ h_in, int64_t h_stride, int64_t batch, int nw,
+template <typename T, bool GW = false>
+__global__ void __launch_bounds__(256, 4) jacobi_eigh_kernel(const double2 *__restrict__ h_in, int64_t h_stride, int64_t batch, int nw,
                                    double *__restrict__ E_out, double2 *__restrict__ U_out, T tol_scale,
                                    unsigned char *gscratch = nullptr, int64_t gscratch_stride = 0) {
     typedef typename cplx_of<T>::type C;
     extern __shared__ __align__(16) unsigned char smem_dyn[];
-    unsigned char *smraw = gscratch ? gscratch + (int64_t)blockIdx.x * gscratch_stride : smem_dyn;
+    unsigned char *smraw;
+    if constexpr (GW) smraw = gscratch + (int64_t)blockIdx.x * gscratch_stride;
+    else smraw = smem_dyn;
     const int np = nw + (nw & 1);
     const int ld = np + 1;
     const int half = np / 2;
@@ -473,9 +475,13 @@ __global__ void __launch_bounds__(128) jacobi_f32_warp_kernel(const double2 *__r
 }
 
 // Stage 2, warp form: one warp per matrix, FP64 A and W in the warp's shared memory.
-// W = V (I - E/2 + 3E^2/8) with E = V^H V - I (second-order Loewdin), H' = W^H H W, one FP64
-// Jacobi sweep on H' (quadratic convergence: the off-diagonal goes from the FP32 stage's
+// W = V (I - E/2 + 3E^2/8) with E = V^H V - I (second-order Loewdin), H' = W^H H W, then FP64
+// Jacobi sweeps on H' (quadratic convergence: the off-diagonal goes from the FP32 stage's
 // 2^-17 ||H|| to the square of that over the gap), then ascending order and canonical phases.
+// converge = 0 (mixed path): one sweep unless H' is already diagonal to 1e-13 ||H||.
+// converge = 1 (FP64 path): sweeps until the FP64 CTA Jacobi's stopping rule holds (off-diagonal
+// norm <= np 2^-60 ||H||, or a sweep with every |a_pq| <= 2^-60 ||H||), so the FP32 stage only
+// preconditions and the result carries the FP64 solver's accuracy.
 struct WarpRefineSmem {
     static __host__ __device__ size_t per_warp(int nw) {
         const int np = nw + (nw & 1);
@@ -488,7 +494,8 @@ struct WarpRefineSmem {
 
 __global__ void __launch_bounds__(64) eigh_refine_f64_warp_kernel(const double2 *__restrict__ h_in, int64_t h_stride,
                                                                   const float2 *__restrict__ V_in, int64_t batch, int nw,
-                                                                  double *__restrict__ E_out, double2 *__restrict__ U_out) {
+                                                                  double *__restrict__ E_out, double2 *__restrict__ U_out,
+                                                                  int converge) {
     extern __shared__ __align__(16) unsigned char smraw[];
     const int np = nw + (nw & 1);
     const int ld = np + 1;
@@ -545,14 +552,15 @@ __global__ void __launch_bounds__(64) eigh_refine_f64_warp_kernel(const double2 
                 else A[i + ld * i].y = 0.0;
             }
         __syncwarp();
-        {
+        const double tol = fro * 8.673617379884035e-19;
+        for (int sweep = 0; sweep < (converge ? WNLQG_JACOBI_MAX_SWEEPS : 1); ++sweep) {
             double off = 0.0;
             if (lane < np)
                 for (int i = 0; i < np; ++i)
                     if (i != lane) off += A[i + ld * lane].x * A[i + ld * lane].x + A[i + ld * lane].y * A[i + ld * lane].y;
             for (int o = 16; o > 0; o >>= 1) off += __shfl_xor_sync(0xffffffffu, off, o);
-            if (sqrt(off) > fro * 1.0e-13)
-                warp_jacobi_sweep<double>(A, W, np, ld, fro * 8.673617379884035e-19, rot_s, rot_c, rot_p, rot_q, lane);
+            if (sqrt(off) <= (converge ? tol * np : fro * 1.0e-13)) break;
+            if (!warp_jacobi_sweep<double>(A, W, np, ld, tol, rot_s, rot_c, rot_p, rot_q, lane)) break;
         }
         // Ascending order (stable) and canonical phases: lane i handles eigenpair i, then the
         // columns are written row-wise (coalesced).
@@ -597,12 +605,15 @@ struct GenEighSmem {
     }
 };
 
+template <bool GW = false>
 __global__ void generalized_eigh_kernel(const double2 *__restrict__ h_in, const double2 *__restrict__ s_in,
                                         int64_t stride, int64_t batch, int nw, double *__restrict__ E_out,
                                         double2 *__restrict__ U_out, int *__restrict__ status,
                                         unsigned char *gscratch = nullptr, int64_t gscratch_stride = 0) {
     extern __shared__ __align__(16) unsigned char smem_dyn[];
-    unsigned char *smraw = gscratch ? gscratch + (int64_t)blockIdx.x * gscratch_stride : smem_dyn;
+    unsigned char *smraw;
+    if constexpr (GW) smraw = gscratch + (int64_t)blockIdx.x * gscratch_stride;
+    else smraw = smem_dyn;
     const int np = nw + (nw & 1);
     const int ld = np + 1;
     const int half = np / 2;

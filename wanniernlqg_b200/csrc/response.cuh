@@ -248,11 +248,13 @@ WNLQG_D void rotate_to_hamiltonian(const double2 *__restrict__ src, C *T1, C *T2
     __syncthreads();
 }
 
-// diag[n] = (U^H X U)_nn; uses T1, T2.
+// diag[n] = (U^H (X - Y) U)_nn for Wannier-gauge X and optional Y (nullptr: 0); uses T1, T2.
 template <typename C>
-WNLQG_D void rotate_diagonal(const double2 *__restrict__ src, C *T1, C *T2, const C *U, double2 *diag, int nw, int ld) {
+WNLQG_D void rotate_diagonal(const double2 *__restrict__ src, C *T1, C *T2, const C *U, double2 *diag, int nw, int ld,
+                             const double2 *__restrict__ sub = nullptr) {
     const int nn = nw * nw;
-    for (int e = threadIdx.x; e < nn; e += blockDim.x) T1[(e % nw) + ld * (e / nw)] = conv_c<C>(src[e]);
+    for (int e = threadIdx.x; e < nn; e += blockDim.x)
+        T1[(e % nw) + ld * (e / nw)] = conv_c<C>(sub ? csub(src[e], sub[e]) : src[e]);
     __syncthreads();
     mm_xy(T1, U, T2, nw, ld);
     __syncthreads();
@@ -290,10 +292,19 @@ WNLQG_D bool any_within(double te, double half, const RespParams &p) {
 
 #define RS_OMB 4   // largest number of photon energies per thread per pass of the pair loop
 
-// Lorentzian weight numerator / (x^2 + w2): a fast reciprocal on the FP32 path, IEEE division
-// on the FP64 path.
+// Lorentzian weight numerator / (x^2 + w2) with den >= w2 > 0.  FP32 path: the fast hardware
+// quotient.  FP64 path: Newton-Raphson reciprocal iteration r <- r (2 - den r) (quadratic
+// convergence), seeded by the FP32 hardware reciprocal (~2^-22 relative): two steps reach FP64
+// rounding (2^-44, then below 2^-53), a few ulp in all.
 WNLQG_D float lorentz(float num, float den) { return __fdividef(num, den); }
-WNLQG_D double lorentz(double num, double den) { return num / den; }
+WNLQG_D double lorentz(double num, double den) {
+    double r = (double)__fdividef(1.0f, (float)den);
+    double e = fma(-den, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-den, r, 1.0);
+    r = fma(r, e, r);
+    return num * r;
+}
 
 // Frequency contraction of one thread's OMB photon energies over the pair list, for one or two
 // components (TWO).  KIND 0: Gaussian with the sqrt(200) cutoff (transition screen);
@@ -347,11 +358,18 @@ WNLQG_D void contract_dispatch(int pair_mode, int gaussian, const double *ste, c
 // R: storage/arithmetic type of the per-k matrices (double: plain FP64 path; float: mixed path).
 // Energies, inverse energy differences, occupations and every accumulation across pairs of a
 // scalar response and across k-points stay FP64.
-template <typename R>
-__global__ void __launch_bounds__(256) response_kernel(RespParams p) {
+// NG: the per-k geometry comes precomputed (nonorthogonal models); a separate instantiation so the
+// orthogonal kernel carries no code for it.  The FP64 kernel runs one CTA per SM (its shared
+// memory), the FP32 kernel two: the register budgets follow.
+// GW: the per-k working set lives in global memory (p.gscratch); a separate instantiation so that
+// the shared-memory kernel addresses shared memory directly.
+template <typename R, bool NG, bool GW>
+__global__ void __launch_bounds__(256, sizeof(R) == 8 ? 1 : 2) response_kernel(RespParams p) {
     typedef typename cplx_of<R>::type C;
     extern __shared__ __align__(16) unsigned char smem_dyn[];
-    unsigned char *sm = p.gscratch ? p.gscratch + (int64_t)blockIdx.x * p.gscratch_stride : smem_dyn;
+    unsigned char *sm;
+    if constexpr (GW) sm = p.gscratch + (int64_t)blockIdx.x * p.gscratch_stride;
+    else sm = smem_dyn;
     const int nw = p.nw, ld = p.ld, nn = nw * nw;
     const RespSmem L = RespSmem::layout(nw, p.n_slots, p.n_fc, 1, sizeof(C));
     C *sU = reinterpret_cast<C *>(sm + L.U);
@@ -395,7 +413,7 @@ __global__ void __launch_bounds__(256) response_kernel(RespParams p) {
             const double d = sE[i] - sE[j];
             sinv[e] = p.eta_reg == 0.0 ? (d == 0.0 ? 0.0 : 1.0 / d) : reg_inverse(d, p.eta_reg);
         }
-        if (p.ng_r) {
+        if constexpr (NG) {
             // Nonorthogonal model: Berry connection into the A slots, slopes on the dH diagonals,
             // generalized derivatives into the G slots; r_elem then reads r directly (inv = 0).
             for (int e = threadIdx.x; e < nn; e += blockDim.x) sinv[e] = 0.0;
@@ -479,9 +497,12 @@ __global__ void __launch_bounds__(256) response_kernel(RespParams p) {
         for (int s = 0; s < p.n_sc; ++s) {
             const int a = p.sc_a[s], bb = p.sc_b[s];
             if (p.sc_kind[s] == RS_SC_BERRY) {
-                // F_nn = (U' dA_b/dk_a U)_nn - (U' dA_a/dk_b U)_nn - i [A_a, A_b]_nn
-                rotate_diagonal(xw + (int64_t)p.ch_dA[bb * 3 + a] * nn, T1, T2, sU, sFd, nw, ld);
-                rotate_diagonal(xw + (int64_t)p.ch_dA[a * 3 + bb] * nn, T1, T2, sU, sFd + nw, nw, ld);
+                // F_nn = (U' (dA_b/dk_a - dA_a/dk_b) U)_nn - i [A_a, A_b]_nn (one rotation of the
+                // difference; sFd[nw + n] = 0 keeps the two-term form below).
+                rotate_diagonal(xw + (int64_t)p.ch_dA[bb * 3 + a] * nn, T1, T2, sU, sFd, nw, ld,
+                                xw + (int64_t)p.ch_dA[a * 3 + bb] * nn);
+                for (int n = threadIdx.x; n < nw; n += blockDim.x) sFd[nw + n] = make_double2(0.0, 0.0);
+                __syncthreads();
             }
             double local = 0.0;
             for (int e = threadIdx.x; e < nn; e += blockDim.x) {
@@ -518,8 +539,10 @@ __global__ void __launch_bounds__(256) response_kernel(RespParams p) {
         for (int s = 0; s < p.n_mu; ++s) {
             const int a = p.mu_a[s], bb = p.mu_b[s], cc = p.mu_c[s];
             // F_nn^{ab} (Hamiltonian-gauge Wannier curvature diagonal) into sFd[2nw .. 3nw).
-            rotate_diagonal(xw + (int64_t)p.ch_dA[bb * 3 + a] * nn, T1, T2, sU, sFd, nw, ld);
-            rotate_diagonal(xw + (int64_t)p.ch_dA[a * 3 + bb] * nn, T1, T2, sU, sFd + nw, nw, ld);
+            rotate_diagonal(xw + (int64_t)p.ch_dA[bb * 3 + a] * nn, T1, T2, sU, sFd, nw, ld,
+                            xw + (int64_t)p.ch_dA[a * 3 + bb] * nn);
+            for (int n = threadIdx.x; n < nw; n += blockDim.x) sFd[nw + n] = make_double2(0.0, 0.0);
+            __syncthreads();
             const C *Aa = slot(p.slot_A[a]), *Ab = slot(p.slot_A[bb]);
             const C *Ha = slot(p.slot_dH[a]), *Hb = slot(p.slot_dH[bb]);
             for (int n = threadIdx.x; n < nw; n += blockDim.x) {

@@ -181,9 +181,13 @@ WNLQG_D void shg_contract(const ShgParams &p, const double2 *__restrict__ coef, 
     }
 }
 
+// GW: matrices in the per-CTA global working set (large nw); else dynamic shared memory.
+template <bool GW>
 __global__ void __launch_bounds__(256) shg_kernel(ShgParams p) {
     extern __shared__ __align__(16) unsigned char smem_dyn[];
-    unsigned char *sm = p.gscratch ? p.gscratch + (int64_t)blockIdx.x * p.gscratch_stride : smem_dyn;
+    unsigned char *sm;
+    if constexpr (GW) sm = p.gscratch + (int64_t)blockIdx.x * p.gscratch_stride;
+    else sm = smem_dyn;
     const int nw = p.nw, ld = p.ld, nn = nw * nw, nc = p.nc;
     const ShgSmem L = ShgSmem::layout(nw, nc);
     double2 *sU = reinterpret_cast<double2 *>(sm + L.U);

@@ -101,6 +101,7 @@ struct wnlqg_plan {
     int shg_grid = 0;
     double2 *d_shg_scratch = nullptr;
     unsigned char *d_shg_gscratch = nullptr;
+    bool shg_global = false;
     // Tensor-core Fourier for arbitrary k-points: Ozaki slices of the phases (A, per batch) and of
     // the channel tiles (B, built once), tcgen05 kind::i8 GEMM.  tc_slices == 0: FP64 CUDA cores.
     int tc_slices = 0;
@@ -112,7 +113,7 @@ struct wnlqg_plan {
     CUtensorMap tc_mapA, tc_mapB;
     int eigh_threads = 32;
     size_t eigh_smem = 0;
-    bool warp_eigh = false;                   // mixed path, nw <= 32: warp-per-matrix stages
+    bool warp_eigh = false;                   // orthogonal models, nw <= 32: warp-per-matrix stages
     unsigned char *d_eigh_scratch = nullptr;  // per-CTA global working set of the CTA eigensolvers
     int64_t eigh_scratch_stride = 0;
     int eigh_grid = 0;
@@ -183,6 +184,26 @@ int response_threads(int nw) {
     return std::max(32, std::min(256, t));
 }
 
+// Raise a kernel's dynamic shared memory limit to everything the device allows beside the kernel's
+// static shared memory.  The attribute belongs to the kernel, not to a plan: several plans of
+// different sizes share it, so it is never lowered to one plan's need.
+cudaError_t allow_dynamic_smem(const void *fn, int smem_optin) {
+    cudaFuncAttributes a;
+    cudaError_t e = cudaFuncGetAttributes(&a, fn);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin - (int)a.sharedSizeBytes);
+}
+
+// The response kernel instantiation for a precision, a geometry source and a working-set location.
+const void *response_fn(bool mixed, bool nonorth, bool global) {
+    if (mixed) {
+        if (nonorth) return global ? (const void *)response_kernel<float, true, true> : (const void *)response_kernel<float, true, false>;
+        return global ? (const void *)response_kernel<float, false, true> : (const void *)response_kernel<float, false, false>;
+    }
+    if (nonorth) return global ? (const void *)response_kernel<double, true, true> : (const void *)response_kernel<double, true, false>;
+    return global ? (const void *)response_kernel<double, false, true> : (const void *)response_kernel<double, false, false>;
+}
+
 // Build the response passes: group the requested components so that each pass fits the
 // per-pass limits and the shared-memory budget.
 wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
@@ -236,9 +257,9 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
     const bool mixed = t.precision == WNLQG_PRECISION_MIXED;
     const int csize = mixed ? (int)sizeof(float2) : (int)sizeof(double2);
     {
-        cudaError_t e = cudaFuncSetAttribute(response_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_limit);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(response_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_limit);
+        cudaError_t e = cudaSuccess;
+        for (int v = 0; v < 4 && e == cudaSuccess; ++v)
+            e = allow_dynamic_smem(response_fn(v & 1, v & 2, false), (int)smem_limit);
         if (e != cudaSuccess) return fail(WNLQG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
     }
     // Orbital counts whose matrices do not fit shared memory keep each CTA's working set in global
@@ -388,8 +409,8 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
         ps.threads = response_threads(pl->nw);
         int per_sm = 0;
         const size_t launch_smem = pass_global ? 0 : ps.smem;
-        cudaError_t e = mixed ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, response_kernel<float>, ps.threads, launch_smem)
-                              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, response_kernel<double>, ps.threads, launch_smem);
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, response_fn(mixed, pl->nonorth, pass_global),
+                                                                      ps.threads, launch_smem);
         if (e != cudaSuccess) return fail(WNLQG_ERR_CUDA, std::string("occupancy query: ") + cudaGetErrorString(e));
         if (per_sm < 1) return fail(WNLQG_ERR_UNSUPPORTED, "response kernel cannot be resident with its shared memory");
         ps.grid = sm_count * per_sm;
@@ -465,11 +486,12 @@ wnlqg_status build_shg(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
     const size_t shg_bytes = ShgSmem::layout(pl->nw, max_nc).total;
     const bool shg_global = shg_bytes > smem_limit;   // large nw: matrices in a per-CTA global working set
     pl->shg_smem = shg_global ? 0 : shg_bytes;
-    cudaError_t e = cudaFuncSetAttribute(shg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)std::max<size_t>(pl->shg_smem, 48 * 1024));
+    pl->shg_global = shg_global;
+    const void *shg_fn = shg_global ? (const void *)shg_kernel<true> : (const void *)shg_kernel<false>;
+    cudaError_t e = allow_dynamic_smem(shg_fn, (int)smem_limit);
     if (e != cudaSuccess) return fail(WNLQG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, shg_kernel, 256, pl->shg_smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, shg_fn, 256, pl->shg_smem);
     if (e != cudaSuccess) return fail(WNLQG_ERR_CUDA, std::string("occupancy query: ") + cudaGetErrorString(e));
     if (per_sm < 1) return fail(WNLQG_ERR_UNSUPPORTED, "second-harmonic kernel cannot be resident with its shared memory");
     pl->shg_grid = sm_count * per_sm;
@@ -697,9 +719,14 @@ wnlqg_status run_front(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const int64_
     if (st != WNLQG_OK) return st;
     const unsigned eigh_grid = (unsigned)(pl->d_eigh_scratch ? std::min<int64_t>(nb, pl->eigh_grid) : nb);
     if (pl->nonorth) {
-        generalized_eigh_kernel<<<eigh_grid, pl->eigh_threads, pl->eigh_smem, pl->stream>>>(
-            pl->d_xw + (int64_t)pl->ch_H * pl->nn, pl->d_xw + (int64_t)pl->ch_S * pl->nn, N, nb, pl->nw, pl->d_E,
-            pl->d_U, pl->d_status, pl->d_eigh_scratch, pl->eigh_scratch_stride);
+        if (pl->d_eigh_scratch)
+            generalized_eigh_kernel<true><<<eigh_grid, pl->eigh_threads, 0, pl->stream>>>(
+                pl->d_xw + (int64_t)pl->ch_H * pl->nn, pl->d_xw + (int64_t)pl->ch_S * pl->nn, N, nb, pl->nw, pl->d_E,
+                pl->d_U, pl->d_status, pl->d_eigh_scratch, pl->eigh_scratch_stride);
+        else
+            generalized_eigh_kernel<false><<<eigh_grid, pl->eigh_threads, pl->eigh_smem, pl->stream>>>(
+                pl->d_xw + (int64_t)pl->ch_H * pl->nn, pl->d_xw + (int64_t)pl->ch_S * pl->nn, N, nb, pl->nw, pl->d_E,
+                pl->d_U, pl->d_status);
     } else if (pl->warp_eigh) {
         int per_sm = 1;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jacobi_f32_warp_kernel, 128, pl->eigh_smem);
@@ -712,12 +739,17 @@ wnlqg_status run_front(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const int64_
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_r, eigh_refine_f64_warp_kernel, 64, pl->refine_smem);
         const int64_t r_grid = std::min<int64_t>((nb + 1) / 2, (int64_t)std::max(1, per_sm_r) * pl->sm_count);
         eigh_refine_f64_warp_kernel<<<(unsigned)r_grid, 64, pl->refine_smem, pl->stream>>>(
-            pl->d_xw + (int64_t)pl->ch_H * pl->nn, N, pl->d_V32, nb, pl->nw, pl->d_E, pl->d_U);
+            pl->d_xw + (int64_t)pl->ch_H * pl->nn, N, pl->d_V32, nb, pl->nw, pl->d_E, pl->d_U,
+            pl->task.precision == WNLQG_PRECISION_MIXED ? 0 : 1);
         pl->launches += 1;
     } else
-        jacobi_eigh_kernel<double><<<eigh_grid, pl->eigh_threads, pl->eigh_smem, pl->stream>>>(
-            pl->d_xw + (int64_t)pl->ch_H * pl->nn, N, nb, pl->nw, pl->d_E, pl->d_U, 8.673617379884035e-19,
-            pl->d_eigh_scratch, pl->eigh_scratch_stride);
+        if (pl->d_eigh_scratch)
+            jacobi_eigh_kernel<double, true><<<eigh_grid, pl->eigh_threads, 0, pl->stream>>>(
+                pl->d_xw + (int64_t)pl->ch_H * pl->nn, N, nb, pl->nw, pl->d_E, pl->d_U, 8.673617379884035e-19,
+                pl->d_eigh_scratch, pl->eigh_scratch_stride);
+        else
+            jacobi_eigh_kernel<double, false><<<eigh_grid, pl->eigh_threads, pl->eigh_smem, pl->stream>>>(
+                pl->d_xw + (int64_t)pl->ch_H * pl->nn, N, nb, pl->nw, pl->d_E, pl->d_U, 8.673617379884035e-19);
     st = record_event(pl, ev_base + 2);
     if (st != WNLQG_OK) return st;
     pl->launches += staged ? 4 : 3;
@@ -758,10 +790,9 @@ wnlqg_status run_passes(wnlqg_plan *pl, int64_t nb, int mode, double scale, int6
         p.gscratch = ps.global ? pl->d_resp_scratch : nullptr;
         p.gscratch_stride = pl->resp_scratch_stride;
         const size_t launch_smem = ps.global ? 0 : ps.smem;
-        if (pl->task.precision == WNLQG_PRECISION_MIXED)
-            response_kernel<float><<<ps.grid, ps.threads, launch_smem, pl->stream>>>(p);
-        else
-            response_kernel<double><<<ps.grid, ps.threads, launch_smem, pl->stream>>>(p);
+        void *args[] = {&p};
+        WNLQG_CUDA(cudaLaunchKernel(response_fn(pl->task.precision == WNLQG_PRECISION_MIXED, pl->nonorth, ps.global),
+                                    dim3(ps.grid), dim3(ps.threads), args, launch_smem, pl->stream));
         pl->launches += 1;
     }
     for (const ShgParams &tmpl : pl->shg) {
@@ -778,7 +809,8 @@ wnlqg_status run_passes(wnlqg_plan *pl, int64_t nb, int mode, double scale, int6
         p.point_offset = point_offset;
         p.scratch = pl->d_shg_scratch;
         p.gscratch = pl->d_shg_gscratch;
-        shg_kernel<<<pl->shg_grid, 256, pl->shg_smem, pl->stream>>>(p);
+        if (pl->shg_global) shg_kernel<true><<<pl->shg_grid, 256, pl->shg_smem, pl->stream>>>(p);
+        else shg_kernel<false><<<pl->shg_grid, 256, pl->shg_smem, pl->stream>>>(p);
         pl->launches += 1;
     }
     WNLQG_CUDA(cudaGetLastError());
@@ -1224,7 +1256,14 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
     }
 
     pl->eigh_threads = eigh_block_threads(nw);
-    pl->warp_eigh = !pl->nonorth && t.precision == WNLQG_PRECISION_MIXED && nw <= 32;
+    // Up to 32 orbitals (orthogonal models) both precisions use the warp eigensolver: FP32 Jacobi,
+    // then FP64 refinement (one sweep on the mixed path, sweeps to FP64 convergence on the FP64
+    // path).  WNLQG_B200_CTA_EIGH=1 keeps the FP64 CTA Jacobi on the FP64 path.
+    {
+        const char *cta = std::getenv("WNLQG_B200_CTA_EIGH");
+        const bool cta_fp64 = cta && cta[0] == '1' && t.precision != WNLQG_PRECISION_MIXED;
+        pl->warp_eigh = !pl->nonorth && nw <= 32 && !cta_fp64;
+    }
     if (pl->nonorth) {
         pl->eigh_threads = std::max(pl->eigh_threads, ((nw + (nw & 1)) / 2 + 31) / 32 * 32);
         pl->eigh_smem = GenEighSmem::bytes(nw);
@@ -1237,9 +1276,9 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
             unsigned char tab[136][2];
             for (int k2 = 0, w = 0; k2 < 16; ++k2)
                 for (int k1 = 0; k1 <= k2; ++k1, ++w) { tab[w][0] = (unsigned char)k1; tab[w][1] = (unsigned char)k2; }
-            WNLQG_CUDA(cudaMemcpyToSymbol(c_jacobi_blocks, tab, sizeof(tab)));
-            cudaError_t ea = cudaFuncSetAttribute(jacobi_f32_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                  (int)std::max<size_t>(pl->eigh_smem, 48 * 1024));
+            cudaError_t et = cudaMemcpyToSymbol(c_jacobi_blocks, tab, sizeof(tab));
+            if (et != cudaSuccess) return bail(fail(WNLQG_ERR_CUDA, std::string("cudaMemcpyToSymbol: ") + cudaGetErrorString(et)));
+            cudaError_t ea = allow_dynamic_smem((const void *)jacobi_f32_warp_kernel, smem_optin);
             if (ea != cudaSuccess) return bail(fail(WNLQG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(ea)));
         }
         // Both stages need blockDim >= np/2 (pairs) and 8 * blockDim >= np^2 (register-staged products).
@@ -1247,28 +1286,27 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
         pl->refine_threads = std::max(pl->refine_threads, ((np / 2 + 31) / 32) * 32);
         pl->eigh_threads = pl->refine_threads;
         if ((st = alloc((void **)&pl->d_V32, (size_t)max_batch * np * np * sizeof(float2))) != WNLQG_OK) return bail(st);
-        cudaError_t e = cudaFuncSetAttribute(eigh_refine_f64_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)std::max<size_t>(pl->refine_smem, 48 * 1024));
+        cudaError_t e = allow_dynamic_smem((const void *)eigh_refine_f64_warp_kernel, smem_optin);
         if (e != cudaSuccess) return bail(fail(WNLQG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e)));
     } else {
         // FP64 path, and the mixed path above 32 orbitals: FP64 CTA Jacobi.
         pl->eigh_smem = EighSmem::bytes(nw, sizeof(double2));
     }
     if (!pl->warp_eigh) {
-        // CTA eigensolvers keep A, V (and the Cholesky factor) in shared memory when they fit,
-        // else in a per-CTA global working set (large nw).
-        if (pl->eigh_smem > (size_t)smem_optin) {
+        // CTA eigensolvers keep A, V (and the Cholesky factor) in shared memory when they fit
+        // beside the kernel's static shared memory, else in a per-CTA global working set (large nw).
+        const void *cta_fn = pl->nonorth ? (const void *)generalized_eigh_kernel<false> : (const void *)jacobi_eigh_kernel<double, false>;
+        cudaFuncAttributes fa;
+        cudaError_t fe = cudaFuncGetAttributes(&fa, cta_fn);
+        if (fe != cudaSuccess) return bail(fail(WNLQG_ERR_CUDA, std::string("cudaFuncGetAttributes: ") + cudaGetErrorString(fe)));
+        if (pl->eigh_smem + fa.sharedSizeBytes > (size_t)smem_optin) {
             pl->eigh_scratch_stride = (int64_t)((pl->eigh_smem + 255) & ~(size_t)255);
             pl->eigh_grid = l2_resident_grid(4 * sm_count, pl->eigh_scratch_stride, sm_count);
             if ((st = alloc((void **)&pl->d_eigh_scratch, (size_t)pl->eigh_grid * pl->eigh_scratch_stride)) != WNLQG_OK)
                 return bail(st);
             pl->eigh_smem = 0;
         } else {
-            cudaError_t e = pl->nonorth
-                                ? cudaFuncSetAttribute(generalized_eigh_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                       (int)std::max<size_t>(pl->eigh_smem, 48 * 1024))
-                                : cudaFuncSetAttribute(jacobi_eigh_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                       (int)std::max<size_t>(pl->eigh_smem, 48 * 1024));
+            cudaError_t e = allow_dynamic_smem(cta_fn, smem_optin);
             if (e != cudaSuccess) return bail(fail(WNLQG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e)));
         }
     }
