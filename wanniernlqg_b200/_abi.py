@@ -143,6 +143,7 @@ class TaskArrays:
         d = TaskDesc()
         d.num_responses = len(responses)
         self.responses = []
+        self.components = []   # per response: the 0-based Cartesian axes of each component
         for i, (kind, comps) in enumerate(responses):
             comps = list(comps)
             if not 1 <= len(comps) <= MAX_COMPONENTS:
@@ -154,6 +155,8 @@ class TaskArrays:
                 for j in range(4):
                     d.responses[i].components[c][j] = ax[j]
             self.responses.append((int(kind), len(comps)))
+            self.components.append([tuple(["xyz".index(ch) for ch in comp]) if isinstance(comp, str)
+                                    else tuple(int(v) for v in comp) for comp in comps])
         d.fermi_energy = float(fermi_energy)
         d.temperature = float(temperature)
         d.broadening_type = int(broadening_type)
@@ -185,6 +188,23 @@ class TaskArrays:
             else:
                 total += nc
         return total
+
+    def block_offsets(self) -> list:
+        """(offset, length) of each response's block in the concatenated value vector."""
+        out = []
+        off = 0
+        for kind, nc in self.responses:
+            if kind == SECOND_HARMONIC:
+                n = nc * self.photon_energies.size * 14
+            elif kind in FREQUENCY_KINDS:
+                n = nc * self.photon_energies.size
+            elif kind in FERMI_AXIS_KINDS:
+                n = nc * self.fermi_energies.size
+            else:
+                n = nc
+            out.append((off, n))
+            off += n
+        return out
 
     def split(self, values: np.ndarray) -> list:
         """Split a concatenated value vector into one (axis, component) array per response;

@@ -125,6 +125,13 @@ class ResponseEngine:
             out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
         return out
 
+    def integrate_mesh_reduced(self, mesh: Sequence[int], operations, *, orbits=None) -> np.ndarray:
+        """Mesh average of a shift / injection current task evaluated on the symmetry-reduced
+        mesh (representatives weighted by orbit size, then projected onto the group-invariant
+        tensors); see wanniernlqg_b200.symmetry.integrate_mesh_reduced."""
+        from .symmetry import integrate_mesh_reduced
+        return integrate_mesh_reduced(self.mesh_weighted_sum, self.task, mesh, operations, orbits=orbits)
+
     def spectrum(self, kpoints):
         """(energies [n, nw], canonical eigenvectors [n, nw, nw]) at fractional k-points."""
         k = np.ascontiguousarray(np.asarray(kpoints, dtype=np.float64).reshape(-1, 3))
