@@ -43,6 +43,9 @@ WNLQG_HD double2 make_neg(double2 a) { return make_double2(-a.x, -a.y); }
 WNLQG_HD float2 make_neg(float2 a) { return make_float2(-a.x, -a.y); }
 
 // Complex type traits for templated kernels: real type R, complex type C.
+template <typename A, typename B> struct same_type { static constexpr bool value = false; };
+template <typename A> struct same_type<A, A> { static constexpr bool value = true; };
+
 template <typename R> struct cplx_of;
 template <> struct cplx_of<double> { typedef double2 type; };
 template <> struct cplx_of<float> { typedef float2 type; };

@@ -1,0 +1,80 @@
+// dmma.cuh - CTA-wide products of complex FP64 matrices in shared memory on the FP64 tensor
+// cores (DMMA: mma.sync.aligned.m8n8k4.row.col.f64, sm_80 and later, sm_100a included; tcgen05
+// has no FP64 kind).
+//
+// A complex product C = op(X) Y is four real products, Re C = Re A Re B - Im A Im B and
+// Im C = Re A Im B + Im A Re B, each accumulated in FP64 by the tensor core.  Outputs are cut into
+// 8 x 8 tiles; each warp takes two tiles at a time (eight independent accumulator chains) and walks
+// K in steps of 4.  Fragment layout of m8n8k4 (PTX ISA, "Matrix fragments for mma.m8n8k4 with
+// .f64"): A (8 x 4, row) lane t holds A[t / 4][t % 4]; B (4 x 8, col) lane t holds B[t % 4][t / 4];
+// C/D (8 x 8) lane t holds C[t / 4][2 (t % 4) + i], i = 0, 1.  Every operand load is masked to
+// the nw x nw block (zero outside), so nw need not be a multiple of 8 and no access leaves the
+// matrices; stores are masked the same way.  All lanes of a warp execute every mma (the masks act
+// on values, never on control flow).
+#pragma once
+#include "common.cuh"
+
+WNLQG_D void dmma_m8n8k4(double &d0, double &d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+// acc += a * b (complex), a and b one fragment element each.
+WNLQG_D void dmma_cplx(double (&re)[2], double (&im)[2], double2 a, double2 b) {
+    dmma_m8n8k4(re[0], re[1], a.x, b.x);
+    dmma_m8n8k4(re[0], re[1], -a.y, b.y);
+    dmma_m8n8k4(im[0], im[1], a.x, b.y);
+    dmma_m8n8k4(im[0], im[1], a.y, b.x);
+}
+
+// MODE 0: out = X Y;  MODE 1: out = X^H Y;  MODE 2: out = X Y - Y X.
+// X, Y, out: column-major nw x nw, leading dimension ld, in shared memory (or a CTA's global
+// working set); out must not alias X or Y.  All threads of the CTA call it; it ends without a
+// barrier (callers synchronise before reading out).
+template <int MODE>
+WNLQG_D void dmma_product(const double2 *X, const double2 *Y, double2 *out, int nw, int ld) {
+    const int nt = (nw + 7) >> 3;
+    const int ntiles = nt * nt;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int fr = lane >> 2, fk = lane & 3;   // A: row fr, column fk; B: row fk, column fr
+    const double2 zero = make_double2(0.0, 0.0);
+    auto a_elem = [&](const double2 *M, int i, int k) -> double2 {
+        if (i >= nw || k >= nw) return zero;
+        if (MODE == 1) {
+            const double2 v = M[k + ld * i];
+            return make_double2(v.x, -v.y);
+        }
+        return M[i + ld * k];
+    };
+    auto b_elem = [&](const double2 *M, int k, int j) -> double2 {
+        return (k < nw && j < nw) ? M[k + ld * j] : zero;
+    };
+    for (int t0 = 2 * warp; t0 < ntiles; t0 += 2 * nwarps) {
+        const int t1 = t0 + 1 < ntiles ? t0 + 1 : t0;   // a lone last tile is computed twice, stored once
+        const int r0 = 8 * (t0 / nt), c0 = 8 * (t0 % nt);
+        const int r1 = 8 * (t1 / nt), c1 = 8 * (t1 % nt);
+        double re0[2] = {0.0, 0.0}, im0[2] = {0.0, 0.0}, re1[2] = {0.0, 0.0}, im1[2] = {0.0, 0.0};
+        for (int k0 = 0; k0 < nw; k0 += 4) {
+            const int ka = k0 + fk;
+            const double2 a0 = a_elem(X, r0 + fr, ka), b0 = b_elem(Y, ka, c0 + fr);
+            const double2 a1 = a_elem(X, r1 + fr, ka), b1 = b_elem(Y, ka, c1 + fr);
+            dmma_cplx(re0, im0, a0, b0);
+            dmma_cplx(re1, im1, a1, b1);
+            if (MODE == 2) {
+                // - Y X: A = -Y, B = X.
+                const double2 y0 = a_elem(Y, r0 + fr, ka), x0 = b_elem(X, ka, c0 + fr);
+                const double2 y1 = a_elem(Y, r1 + fr, ka), x1 = b_elem(X, ka, c1 + fr);
+                dmma_cplx(re0, im0, make_double2(-y0.x, -y0.y), x0);
+                dmma_cplx(re1, im1, make_double2(-y1.x, -y1.y), x1);
+            }
+        }
+        const int orow = fr, ocol = 2 * fk;
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            if (r0 + orow < nw && c0 + ocol + i < nw) out[(r0 + orow) + ld * (c0 + ocol + i)] = make_double2(re0[i], im0[i]);
+            if (t1 != t0 && r1 + orow < nw && c1 + ocol + i < nw)
+                out[(r1 + orow) + ld * (c1 + ocol + i)] = make_double2(re1[i], im1[i]);
+        }
+    }
+}

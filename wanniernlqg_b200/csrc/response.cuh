@@ -18,6 +18,7 @@
 //   quantum metric (band sum)   quantum_metric_band_sum_component, ConventionalQuantumGeometry.jl:321-355
 #pragma once
 #include "common.cuh"
+#include "dmma.cuh"
 
 #define RS_MAX_FREQ 8
 #define RS_MAX_SCALAR 16
@@ -162,7 +163,8 @@ WNLQG_D double fermi_occ(double e, double mu, double kT) {
 }
 
 // ---- shared-memory matrix products (all threads participate; ld = nw + 1) -------------------
-// Work item w -> row i = w % nw and four columns 4*(w / nw) .. +3: the row operand is read
+// Complex FP64 (double2): FP64 tensor cores (dmma_product).  Complex FP32 (float2): CUDA cores,
+// work item w -> row i = w % nw and four columns 4*(w / nw) .. +3: the row operand is read
 // conflict-free across lanes, the column operand is a broadcast.
 #define RS_JB 4
 
@@ -173,6 +175,10 @@ template <> WNLQG_D float2 conv_c<float2>(double2 v) { return make_float2((float
 
 // out = X * Y
 template <typename C> WNLQG_D void mm_xy(const C *X, const C *Y, C *out, int nw, int ld) {
+    if constexpr (same_type<C, double2>::value) {
+        dmma_product<0>(X, Y, out, nw, ld);
+        return;
+    }
     const int ng = (nw + RS_JB - 1) / RS_JB;
     for (int w = threadIdx.x; w < nw * ng; w += blockDim.x) {
         const int i = w % nw, j0 = (w / nw) * RS_JB;
@@ -193,6 +199,10 @@ template <typename C> WNLQG_D void mm_xy(const C *X, const C *Y, C *out, int nw,
 
 // out = X^H * Y
 template <typename C> WNLQG_D void mm_xhy(const C *X, const C *Y, C *out, int nw, int ld) {
+    if constexpr (same_type<C, double2>::value) {
+        dmma_product<1>(X, Y, out, nw, ld);
+        return;
+    }
     const int ng = (nw + RS_JB - 1) / RS_JB;
     for (int w = threadIdx.x; w < nw * ng; w += blockDim.x) {
         const int i = w % nw, j0 = (w / nw) * RS_JB;
@@ -213,6 +223,10 @@ template <typename C> WNLQG_D void mm_xhy(const C *X, const C *Y, C *out, int nw
 
 // out = X * Y - Y * X
 template <typename C> WNLQG_D void mm_comm(const C *X, const C *Y, C *out, int nw, int ld) {
+    if constexpr (same_type<C, double2>::value) {
+        dmma_product<2>(X, Y, out, nw, ld);
+        return;
+    }
     const int ng = (nw + RS_JB - 1) / RS_JB;
     for (int w = threadIdx.x; w < nw * ng; w += blockDim.x) {
         const int i = w % nw, j0 = (w / nw) * RS_JB;
