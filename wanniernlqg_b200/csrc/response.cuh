@@ -306,54 +306,80 @@ WNLQG_D bool any_within(double te, double half, const RespParams &p) {
 
 #define RS_OMB 4   // largest number of photon energies per thread per pass of the pair loop
 
-// Lorentzian weight numerator / (x^2 + w2) with den >= w2 > 0.  FP32 path: the fast hardware
-// quotient.  FP64 path: Newton-Raphson reciprocal iteration r <- r (2 - den r) (quadratic
-// convergence), seeded by the FP32 hardware reciprocal (~2^-22 relative): two steps reach FP64
-// rounding (2^-44, then below 2^-53), a few ulp in all.
-WNLQG_D float lorentz(float num, float den) { return __fdividef(num, den); }
-WNLQG_D double lorentz(double num, double den) {
-    double r = (double)__fdividef(1.0f, (float)den);
+// Reciprocal of a Lorentzian denominator den >= w2 > 0.  FP32 path: the fast hardware quotient.
+// FP64 path: Newton-Raphson iteration r <- r (2 - den r) (quadratic convergence) seeded by the
+// PTX instruction rcp.approx.ftz.f64 (a hardware approximation), so that no FP64 <-> FP32
+// conversions are needed; three steps take any seed better than 2^-8 relative to FP64 rounding
+// (a few ulp).  The denominators are normal numbers (den >= w2 > 0), so flushing subnormals
+// changes nothing.
+WNLQG_D float lorentz_recip(float den) { return __fdividef(1.0f, den); }
+WNLQG_D double lorentz_recip(double den) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(den));
     double e = fma(-den, r, 1.0);
     r = fma(r, e, r);
     e = fma(-den, r, 1.0);
     r = fma(r, e, r);
-    return num * r;
+    e = fma(-den, r, 1.0);
+    return fma(r, e, r);
+}
+WNLQG_D float lorentz(float num, float den) { return __fdividef(num, den); }
+WNLQG_D double lorentz(double num, double den) { return num * lorentz_recip(den); }
+
+// One pair's contribution to a thread's OMB photon energies.  KIND 0: Gaussian with the
+// sqrt(200) cutoff (transition screen); 1: Lorentzian (fq * width / pi folded once per pair);
+// 2: jerk's windowed delta (Gaussian or Lorentzian by `gaussian`).
+template <typename R, typename C, int KIND, int OMB, bool TWO>
+WNLQG_D void contract_one(double te, R fq, C q0, C q1, const double *om, C (*acc)[2], R gsc, R cut, R invw,
+                          R w2, R lor, R win, int gaussian) {
+    const R fql = fq * lor;
+#pragma unroll
+    for (int j = 0; j < OMB; ++j) {
+        const R x = (R)(te - om[j]);
+        R weight;
+        if (KIND == 0) {
+            if (!(fabs(x) < cut)) continue;
+            const R y = x * invw;
+            weight = fq * (gsc * exp(-y * y));
+        } else if (KIND == 1) {
+            weight = fql * lorentz_recip(x * x + w2);
+        } else {
+            if (win > (R)0 && fabs(x) > win) continue;
+            const R y = x * invw;
+            weight = fq * (gaussian ? gsc * exp(-y * y) : lorentz(lor, x * x + w2));
+        }
+        acc[j][0].x = fma(weight, q0.x, acc[j][0].x);
+        acc[j][0].y = fma(weight, q0.y, acc[j][0].y);
+        if (TWO) {
+            acc[j][1].x = fma(weight, q1.x, acc[j][1].x);
+            acc[j][1].y = fma(weight, q1.y, acc[j][1].y);
+        }
+    }
 }
 
 // Frequency contraction of one thread's OMB photon energies over the pair list, for one or two
-// components (TWO).  KIND 0: Gaussian with the sqrt(200) cutoff (transition screen);
-// 1: Lorentzian; 2: jerk's windowed delta (Gaussian or Lorentzian by `gaussian`).
+// components (TWO).  Pairs are streamed two at a time into separate accumulators (two independent
+// dependency chains per energy), which are added at the end.
 template <typename R, typename C, int KIND, int OMB, bool TWO>
 WNLQG_D void contract_pairs(const double *ste, const double *sfnm, const C *Q0, const C *Q1, int npairs,
                             const double *om, C (*acc)[2], R gsc, R cut, R invw, R w2, R lor, R win, int gaussian) {
-    for (int q = 0; q < npairs; ++q) {
-        const double te = ste[q];
-        const R fq = (R)sfnm[q];
-        const C q0 = Q0[q];
-        const C q1 = TWO ? Q1[q] : q0;
+    C odd[OMB][2];
 #pragma unroll
-        for (int j = 0; j < OMB; ++j) {
-            const R x = (R)(te - om[j]);
-            R delta;
-            if (KIND == 0) {
-                if (!(fabs(x) < cut)) continue;
-                const R y = x * invw;
-                delta = gsc * exp(-y * y);
-            } else if (KIND == 1) {
-                delta = lorentz(lor, x * x + w2);
-            } else {
-                if (win > (R)0 && fabs(x) > win) continue;
-                const R y = x * invw;
-                delta = gaussian ? gsc * exp(-y * y) : lorentz(lor, x * x + w2);
-            }
-            const R weight = fq * delta;
-            acc[j][0].x = fma(weight, q0.x, acc[j][0].x);
-            acc[j][0].y = fma(weight, q0.y, acc[j][0].y);
-            if (TWO) {
-                acc[j][1].x = fma(weight, q1.x, acc[j][1].x);
-                acc[j][1].y = fma(weight, q1.y, acc[j][1].y);
-            }
-        }
+    for (int j = 0; j < OMB; ++j) { odd[j][0] = czero<C>(); odd[j][1] = czero<C>(); }
+    int q = 0;
+    for (; q + 1 < npairs; q += 2) {
+        contract_one<R, C, KIND, OMB, TWO>(ste[q], (R)sfnm[q], Q0[q], TWO ? Q1[q] : Q0[q], om, acc, gsc, cut, invw,
+                                           w2, lor, win, gaussian);
+        contract_one<R, C, KIND, OMB, TWO>(ste[q + 1], (R)sfnm[q + 1], Q0[q + 1], TWO ? Q1[q + 1] : Q0[q + 1], om, odd,
+                                           gsc, cut, invw, w2, lor, win, gaussian);
+    }
+    if (q < npairs)
+        contract_one<R, C, KIND, OMB, TWO>(ste[q], (R)sfnm[q], Q0[q], TWO ? Q1[q] : Q0[q], om, acc, gsc, cut, invw, w2,
+                                           lor, win, gaussian);
+#pragma unroll
+    for (int j = 0; j < OMB; ++j) {
+        acc[j][0] = cadd(acc[j][0], odd[j][0]);
+        acc[j][1] = cadd(acc[j][1], odd[j][1]);
     }
 }
 
