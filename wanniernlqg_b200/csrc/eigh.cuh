@@ -236,23 +236,53 @@ __global__ void __launch_bounds__(256, 4) jacobi_eigh_kernel(const double2 *__re
 }
 
 // ---------------------------------------------------------------------------------------------
-// Mixed-precision eigensolver, one warp per matrix in two kernels:
-//   stage 1 (jacobi_f32_warp_kernel): FP32 parallel Jacobi until the off-diagonal norm is below
+// Mixed-precision eigensolver, one team of TEAM threads per matrix, in two kernels:
+//   stage 1 (jacobi_f32_team_kernel): FP32 parallel Jacobi until the off-diagonal norm is below
 //     2^-17 ||H||, warm-started along runs of consecutive mesh points from the previous point's
 //     eigenvectors (V <- V (3I - V^H V)/2, A <- V^H H V);
-//   stage 2 (eigh_refine_f64_warp_kernel): FP64 Rayleigh-Ritz refinement, W = second-order
-//     Loewdin orthonormalisation of V, H' = W^H H W, one FP64 Jacobi sweep (quadratic
+//   stage 2 (eigh_refine_f64_team_kernel): FP64 Rayleigh-Ritz refinement, W = second-order
+//     Loewdin orthonormalisation of V, H' = W^H H W, FP64 Jacobi sweeps (quadratic
 //     convergence), U = W J, ascending order and canonical phases.
-// A and V sit in the warp's own shared memory, so a round synchronises with __syncwarp only.
-// The Hermitian 2x2 block updates of a round take their (k1 <= k2) pair indices from a fixed
-// table (the order w = k2 (k2 + 1) / 2 + k1 is a prefix for every np <= 32); V <- V J runs one
-// row per lane.
+// A team is one warp (TEAM = 32: several teams per CTA, synchronised with __syncwarp) or one
+// 64-thread CTA (TEAM = 64: two warps share a matrix, synchronised with __syncthreads; each
+// thread then holds half a column in the products and does half of a round's updates, and an
+// SM holds twice the warps for the same shared memory).  A and V sit in the team's own shared
+// memory.  The Hermitian 2x2 block updates of a round take their (k1 <= k2) pair indices from a
+// fixed table (the order w = k2 (k2 + 1) / 2 + k1 is a prefix for every np <= 32); V <- V J
+// runs one row per thread, the pairs of a round split between the warps.
 // ---------------------------------------------------------------------------------------------
 __constant__ unsigned char c_jacobi_blocks[136][2];
 
+template <int TEAM> struct Team {
+    static_assert(TEAM == 32 || TEAM == 64, "a team is one warp or one 64-thread CTA");
+    static constexpr int ROWS = 32 / (TEAM / 32);   // rows of a product column held per thread: 32 or 16
+    static WNLQG_D int rank() { return TEAM == 32 ? (int)(threadIdx.x & 31) : (int)threadIdx.x; }
+    static WNLQG_D void sync() {
+        if constexpr (TEAM == 32) __syncwarp();
+        else __syncthreads();
+    }
+    static WNLQG_D bool any(bool v) {
+        if constexpr (TEAM == 32) return __any_sync(0xffffffffu, v);
+        else return __syncthreads_or(v ? 1 : 0) != 0;
+    }
+    // Sum of one double per thread over the team, the same value in every thread (fixed order).
+    static WNLQG_D double sum(double v, double *red) {
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if constexpr (TEAM == 32) {
+            return v;
+        } else {
+            if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+            __syncthreads();
+            const double t = red[0] + red[1];
+            __syncthreads();
+            return t;
+        }
+    }
+};
+
 struct WarpJacobiSmem {
-    // Per warp: A, V (np x ld complex float), rotation sines, cosines and pair indices.
-    static __host__ __device__ size_t per_warp(int nw) {
+    // Per team: A, V (np x ld complex float), rotation sines, cosines and pair indices.
+    static __host__ __device__ size_t per_team(int nw) {
         const int np = nw + (nw & 1);
         const int ld = np + 1;
         size_t s = 2 * (size_t)np * ld * sizeof(float2) + 16 * (sizeof(float2) + sizeof(float) + 2 * sizeof(int));
@@ -260,20 +290,26 @@ struct WarpJacobiSmem {
     }
 };
 
-// One warp-synchronous parallel-Jacobi sweep (np - 1 rounds); returns true when a rotation was applied.
+// One team-synchronous parallel-Jacobi sweep (np - 1 rounds); returns true (in every thread)
+// when a rotation was applied.
 WNLQG_D float recip_sqrt(float x) { return rsqrtf(x); }
 WNLQG_D double recip_sqrt(double x) { return 1.0 / sqrt(x); }
 
-template <typename T>
-WNLQG_D bool warp_jacobi_sweep(typename cplx_of<T>::type *A, typename cplx_of<T>::type *V, int np, int ld, T tol,
-                               typename cplx_of<T>::type *rot_s, T *rot_c, int *rot_p, int *rot_q, int lane) {
+template <typename T, int TEAM>
+WNLQG_D bool team_jacobi_sweep(typename cplx_of<T>::type *A, typename cplx_of<T>::type *V, int np, int ld, T tol,
+                               typename cplx_of<T>::type *rot_s, T *rot_c, int *rot_p, int *rot_q) {
     typedef typename cplx_of<T>::type C;
+    const int t = Team<TEAM>::rank();
     const int half = np / 2;
     const int nblk = half * (half + 1) / 2;
+    // V <- V J: thread t handles row t % 32 and the pairs [kb, ke) of its warp.
+    const int vrow = t & 31;
+    const int kper = (half + TEAM / 32 - 1) / (TEAM / 32);
+    const int kb = (t >> 5) * kper, ke = min(half, kb + kper);
     bool rotated = false;
     for (int round = 0; round < np - 1; ++round) {
-        if (lane < half) {
-            const int s1 = lane, s2 = np - 1 - lane;
+        if (t < half) {
+            const int s1 = t, s2 = np - 1 - t;
             const int i1 = s1 == 0 ? 0 : ((s1 - 1 + round) % (np - 1)) + 1;
             const int i2 = ((s2 - 1 + round) % (np - 1)) + 1;
             const int p = min(i1, i2), q = max(i1, i2);
@@ -284,20 +320,20 @@ WNLQG_D bool warp_jacobi_sweep(typename cplx_of<T>::type *A, typename cplx_of<T>
             if (g > tol) {
                 const T app = A[p + ld * p].x, aqq = A[q + ld * q].x;
                 const T theta = (aqq - app) / ((T)2 * g);
-                const T t = (theta >= (T)0 ? (T)1 : (T)-1) / (fabs(theta) + sqrt(theta * theta + (T)1));
-                c = recip_sqrt(t * t + (T)1);
-                const T sn = t * c;
+                const T tt = (theta >= (T)0 ? (T)1 : (T)-1) / (fabs(theta) + sqrt(theta * theta + (T)1));
+                c = recip_sqrt(tt * tt + (T)1);
+                const T sn = tt * c;
                 sp.x = sn * (apq.x / g);
                 sp.y = sn * (apq.y / g);
                 rotated = true;
             }
-            rot_c[lane] = c;
-            rot_s[lane] = sp;
-            rot_p[lane] = p;
-            rot_q[lane] = q;
+            rot_c[t] = c;
+            rot_s[t] = sp;
+            rot_p[t] = p;
+            rot_q[t] = q;
         }
-        __syncwarp();
-        for (int w = lane; w < nblk; w += 32) {
+        Team<TEAM>::sync();
+        for (int w = t; w < nblk; w += TEAM) {
             const int k1 = c_jacobi_blocks[w][0], k2 = c_jacobi_blocks[w][1];
             const int p1 = rot_p[k1], q1 = rot_q[k1], p2 = rot_p[k2], q2 = rot_q[k2];
             const T c1 = rot_c[k1], c2 = rot_c[k2];
@@ -328,153 +364,182 @@ WNLQG_D bool warp_jacobi_sweep(typename cplx_of<T>::type *A, typename cplx_of<T>
                 A[p2 + ld * q1] = cconj(o10); A[q2 + ld * q1] = cconj(o11);
             }
         }
-        if (lane < np) {
-            for (int k = 0; k < half; ++k) {
+        if (vrow < np) {
+            for (int k = kb; k < ke; ++k) {
                 const int p = rot_p[k], q = rot_q[k];
                 const T c = rot_c[k];
                 const C sk = rot_s[k], skc = cconj(sk);
-                const C vp = V[lane + ld * p], vq = V[lane + ld * q];
-                V[lane + ld * p] = csub(cscale(vp, c), cmul(vq, skc));
-                V[lane + ld * q] = cadd(cmul(vp, sk), cscale(vq, c));
+                const C vp = V[vrow + ld * p], vq = V[vrow + ld * q];
+                V[vrow + ld * p] = csub(cscale(vp, c), cmul(vq, skc));
+                V[vrow + ld * q] = cadd(cmul(vp, sk), cscale(vq, c));
             }
         }
-        __syncwarp();
+        Team<TEAM>::sync();
     }
-    return __any_sync(0xffffffffu, rotated);
+    return Team<TEAM>::any(rotated);
 }
 
-// out = op(X) * Y[:, lane] for the warp's np x np shared matrices (op = conjugate transpose when
-// xh): the lane's column of the product, returned in registers (static indices only).
-template <typename C>
-WNLQG_D void warp_column_product(const C *X, const C *Y, C (&out)[32], int np, int ld, int lane, bool xh) {
+// out[r] = (op(X) * Y)[r0 + r, col] for the team's np x np shared matrices (op = conjugate
+// transpose when xh), with col = t % 32 and rows r0 = (t / 32) * ROWS .. + ROWS: each thread's
+// part of one column of the product, in registers (static indices only).
+template <int TEAM, typename C>
+WNLQG_D void team_column_product(const C *X, const C *Y, C (&out)[Team<TEAM>::ROWS], int np, int ld, bool xh) {
+    constexpr int ROWS = Team<TEAM>::ROWS;
+    const int t = Team<TEAM>::rank();
+    const int col = t & 31, r0 = (t >> 5) * ROWS;
 #pragma unroll
-    for (int i = 0; i < 32; ++i) out[i] = czero<C>();
-    if (lane >= np) return;
+    for (int i = 0; i < ROWS; ++i) out[i] = czero<C>();
+    if (col >= np) return;
     for (int l = 0; l < np; ++l) {
-        const C y = Y[l + ld * lane];
+        const C y = Y[l + ld * col];
         if (xh) {
 #pragma unroll
-            for (int i = 0; i < 32; ++i)
-                if (i < np) out[i] = cfmaconj(X[l + ld * i], y, out[i]);
+            for (int i = 0; i < ROWS; ++i)
+                if (r0 + i < np) out[i] = cfmaconj(X[l + ld * (r0 + i)], y, out[i]);
         } else {
 #pragma unroll
-            for (int i = 0; i < 32; ++i)
-                if (i < np) out[i] = cfma(X[i + ld * l], y, out[i]);
+            for (int i = 0; i < ROWS; ++i)
+                if (r0 + i < np) out[i] = cfma(X[(r0 + i) + ld * l], y, out[i]);
         }
     }
 }
 
-template <typename C> WNLQG_D void warp_store_column(C *M, const C (&v)[32], int np, int ld, int lane) {
-    if (lane < np) {
+template <int TEAM, typename C>
+WNLQG_D void team_store_column(C *M, const C (&v)[Team<TEAM>::ROWS], int np, int ld) {
+    constexpr int ROWS = Team<TEAM>::ROWS;
+    const int t = Team<TEAM>::rank();
+    const int col = t & 31, r0 = (t >> 5) * ROWS;
+    if (col < np) {
 #pragma unroll
-        for (int i = 0; i < 32; ++i)
-            if (i < np) M[i + ld * lane] = v[i];
+        for (int i = 0; i < ROWS; ++i)
+            if (r0 + i < np) M[(r0 + i) + ld * col] = v[i];
     }
 }
 
 // A <- H(k) from the upper triangle of the stored matrix (lower = conjugate, real diagonal),
-// zero-padded to np; returns the Frobenius norm.
-template <typename C>
-WNLQG_D double warp_load_hermitian(C *A, const double2 *__restrict__ h, int nw, int np, int ld, int lane) {
-    for (int j = 0; j < np; ++j) {
+// zero-padded to np; returns the Frobenius norm (the same value in every thread).
+template <int TEAM, typename C>
+WNLQG_D double team_load_hermitian(C *A, const double2 *__restrict__ h, int nw, int np, int ld, double *red) {
+    const int t = Team<TEAM>::rank();
+    const int row = t & 31, j0 = t >> 5;
+    for (int j = j0; j < np; j += TEAM / 32) {
         double2 v = make_double2(0.0, 0.0);
-        if (lane < nw && j < nw) v = h[lane + (size_t)nw * j];
-        if (lane < np) A[lane + ld * j] = from_c64<C>(v);
+        if (row < nw && j < nw) v = h[row + (size_t)nw * j];
+        if (row < np) A[row + ld * j] = from_c64<C>(v);
     }
-    __syncwarp();
-    if (lane < np)
-        for (int i = lane; i < np; ++i) {
-            if (i > lane) A[i + ld * lane] = cconj(A[lane + ld * i]);
+    Team<TEAM>::sync();
+    if (row < np)
+        for (int i = row + j0; i < np; i += TEAM / 32) {
+            if (i > row) A[i + ld * row] = cconj(A[row + ld * i]);
             else A[i + ld * i].y = 0;
         }
-    __syncwarp();
+    Team<TEAM>::sync();
     double local = 0.0;
-    if (lane < np)
-        for (int i = 0; i < np; ++i) {
-            const C z = A[i + ld * lane];
+    if (row < np)
+        for (int i = j0; i < np; i += TEAM / 32) {
+            const C z = A[i + ld * row];
             local += (double)z.x * z.x + (double)z.y * z.y;
         }
-    for (int o = 16; o > 0; o >>= 1) local += __shfl_xor_sync(0xffffffffu, local, o);
-    return sqrt(local);
+    return sqrt(Team<TEAM>::sum(local, red));
 }
 
-__global__ void __launch_bounds__(128) jacobi_f32_warp_kernel(const double2 *__restrict__ h_in, int64_t h_stride,
+// Squared off-diagonal Frobenius norm of the team's matrix (the same value in every thread).
+template <int TEAM, typename C>
+WNLQG_D double team_offdiag2(const C *A, int np, int ld, double *red) {
+    const int t = Team<TEAM>::rank();
+    const int row = t & 31, j0 = t >> 5;
+    double off = 0.0;
+    if (row < np)
+        for (int i = j0; i < np; i += TEAM / 32)
+            if (i != row) {
+                const C z = A[i + ld * row];
+                off += (double)z.x * z.x + (double)z.y * z.y;
+            }
+    return Team<TEAM>::sum(off, red);
+}
+
+// TEAM = 32: blocks of 128 threads (four teams); TEAM = 64: blocks of 64 threads (one team).
+template <int TEAM>
+__global__ void __launch_bounds__(TEAM == 32 ? 128 : 64, TEAM == 32 ? 4 : 12) jacobi_f32_team_kernel(const double2 *__restrict__ h_in, int64_t h_stride,
                                                               int64_t batch, int nw, float2 *__restrict__ V_out,
                                                               int warm_start) {
     extern __shared__ __align__(16) unsigned char smraw[];
+    constexpr int ROWS = Team<TEAM>::ROWS;
+    __shared__ double red[2];
     const int np = nw + (nw & 1);
     const int ld = np + 1;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    unsigned char *base = smraw + (size_t)warp * WarpJacobiSmem::per_warp(nw);
+    const int team = TEAM == 32 ? (int)(threadIdx.x >> 5) : 0;
+    const int teams = TEAM == 32 ? (int)(blockDim.x >> 5) : 1;
+    unsigned char *base = smraw + (size_t)team * WarpJacobiSmem::per_team(nw);
     float2 *A = reinterpret_cast<float2 *>(base);
     float2 *V = A + (size_t)np * ld;
     float2 *rot_s = V + (size_t)np * ld;
     float *rot_c = reinterpret_cast<float *>(rot_s + 16);
     int *rot_p = reinterpret_cast<int *>(rot_c + 16);
     int *rot_q = rot_p + 16;
-    const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
-    const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
-    const int64_t kb = (batch * gw) / nwarps, ke = (batch * (gw + 1)) / nwarps;
-    float2 col[32];
+    const int t = Team<TEAM>::rank();
+    const int64_t nteams = (int64_t)gridDim.x * teams;
+    const int64_t gt = (int64_t)blockIdx.x * teams + team;
+    const int64_t kb = (batch * gt) / nteams, ke = (batch * (gt + 1)) / nteams;
+    float2 col[ROWS];
     for (int64_t b = kb; b < ke; ++b) {
         const double2 *h = h_in + b * h_stride;
         double fro;
         if (b == kb || !warm_start) {
-            fro = warp_load_hermitian(A, h, nw, np, ld, lane);
-            if (lane < np)
-                for (int i = 0; i < np; ++i) V[i + ld * lane] = make_float2(i == lane ? 1.0f : 0.0f, 0.0f);
-            __syncwarp();
+            fro = team_load_hermitian<TEAM>(A, h, nw, np, ld, red);
+            for (int e = t; e < np * np; e += TEAM) {
+                const int i = e % np, j = e / np;
+                V[i + ld * j] = make_float2(i == j ? 1.0f : 0.0f, 0.0f);
+            }
+            Team<TEAM>::sync();
         } else {
             // Warm start from the previous point's V: V <- V (3I - V^H V)/2 and A <- V^H H V; the
             // second factor of every product is read from shared memory (A serves as scratch).
-            warp_column_product(V, V, col, np, ld, lane, true);                // (V^H V)[:, lane]
+            const int c0 = t & 31, r0 = (t >> 5) * ROWS;
+            team_column_product<TEAM>(V, V, col, np, ld, true);                // (V^H V)[:, c0]
 #pragma unroll
-            for (int i = 0; i < 32; ++i)
-                col[i] = make_float2((i == lane ? 1.5f : 0.0f) - 0.5f * col[i].x, -0.5f * col[i].y);
-            warp_store_column(A, col, np, ld, lane);                            // A <- M
-            __syncwarp();
-            warp_column_product(V, A, col, np, ld, lane, false);                // (V M)[:, lane]
-            __syncwarp();
-            warp_store_column(V, col, np, ld, lane);
-            fro = warp_load_hermitian(A, h, nw, np, ld, lane);                  // A <- H
-            warp_column_product(A, V, col, np, ld, lane, false);                // (H V)[:, lane]
-            __syncwarp();
-            warp_store_column(A, col, np, ld, lane);                            // A <- H V
-            __syncwarp();
-            warp_column_product(V, A, col, np, ld, lane, true);                 // (V^H H V)[:, lane]
-            __syncwarp();
-            warp_store_column(A, col, np, ld, lane);
-            __syncwarp();
-            if (lane < np)
-                for (int i = lane; i < np; ++i) {
-                    if (i > lane) A[i + ld * lane] = cconj(A[lane + ld * i]);
+            for (int i = 0; i < ROWS; ++i)
+                col[i] = make_float2((r0 + i == c0 ? 1.5f : 0.0f) - 0.5f * col[i].x, -0.5f * col[i].y);
+            team_store_column<TEAM>(A, col, np, ld);                           // A <- M
+            Team<TEAM>::sync();
+            team_column_product<TEAM>(V, A, col, np, ld, false);               // (V M)[:, c0]
+            Team<TEAM>::sync();
+            team_store_column<TEAM>(V, col, np, ld);
+            fro = team_load_hermitian<TEAM>(A, h, nw, np, ld, red);            // A <- H
+            team_column_product<TEAM>(A, V, col, np, ld, false);               // (H V)[:, c0]
+            Team<TEAM>::sync();
+            team_store_column<TEAM>(A, col, np, ld);                           // A <- H V
+            Team<TEAM>::sync();
+            team_column_product<TEAM>(V, A, col, np, ld, true);                // (V^H H V)[:, c0]
+            Team<TEAM>::sync();
+            team_store_column<TEAM>(A, col, np, ld);
+            Team<TEAM>::sync();
+            const int row = t & 31;
+            if (row < np)
+                for (int i = row + (t >> 5); i < np; i += TEAM / 32) {
+                    if (i > row) A[i + ld * row] = cconj(A[row + ld * i]);
                     else A[i + ld * i].y = 0.0f;
                 }
-            __syncwarp();
+            Team<TEAM>::sync();
         }
         // The FP64 stage converges quadratically from here: the FP32 stage stops once the
         // off-diagonal norm is below 2^-17 ||H|| (rotating elements above 2^-20 ||H||).
         const float tol32 = (float)(fro * 9.5367431640625e-07);
         for (int sweep = 0; sweep < WNLQG_JACOBI_MAX_SWEEPS; ++sweep) {
-            double off = 0.0;
-            if (lane < np)
-                for (int i = 0; i < np; ++i)
-                    if (i != lane) {
-                        const float2 z = A[i + ld * lane];
-                        off += (double)z.x * z.x + (double)z.y * z.y;
-                    }
-            for (int o = 16; o > 0; o >>= 1) off += __shfl_xor_sync(0xffffffffu, off, o);
+            const double off = team_offdiag2<TEAM>(A, np, ld, red);
             if (sqrt(off) <= fro * 7.62939453125e-06) break;
-            if (!warp_jacobi_sweep<float>(A, V, np, ld, tol32, rot_s, rot_c, rot_p, rot_q, lane)) break;
+            if (!team_jacobi_sweep<float, TEAM>(A, V, np, ld, tol32, rot_s, rot_c, rot_p, rot_q)) break;
         }
         float2 *vo = V_out + b * (int64_t)np * np;
-        if (lane < np)
-            for (int j = 0; j < np; ++j) vo[lane + (int64_t)np * j] = V[lane + ld * j];
-        __syncwarp();
+        for (int e = t; e < np * np; e += TEAM) {
+            const int i = e % np, j = e / np;
+            vo[i + (int64_t)np * j] = V[i + ld * j];
+        }
+        Team<TEAM>::sync();
     }
 }
 
-// Stage 2, warp form: one warp per matrix, FP64 A and W in the warp's shared memory.
+// Stage 2: FP64 A and W in the team's shared memory.
 // W = V (I - E/2 + 3E^2/8) with E = V^H V - I (second-order Loewdin), H' = W^H H W, then FP64
 // Jacobi sweeps on H' (quadratic convergence: the off-diagonal goes from the FP32 stage's
 // 2^-17 ||H|| to the square of that over the gap), then ascending order and canonical phases.
@@ -483,7 +548,7 @@ __global__ void __launch_bounds__(128) jacobi_f32_warp_kernel(const double2 *__r
 // norm <= np 2^-60 ||H||, or a sweep with every |a_pq| <= 2^-60 ||H||), so the FP32 stage only
 // preconditions and the result carries the FP64 solver's accuracy.
 struct WarpRefineSmem {
-    static __host__ __device__ size_t per_warp(int nw) {
+    static __host__ __device__ size_t per_team(int nw) {
         const int np = nw + (nw & 1);
         const int ld = np + 1;
         size_t s = 2 * (size_t)np * ld * sizeof(double2) + 16 * (sizeof(double2) + sizeof(double) + 2 * sizeof(int)) +
@@ -492,15 +557,20 @@ struct WarpRefineSmem {
     }
 };
 
-__global__ void __launch_bounds__(64) eigh_refine_f64_warp_kernel(const double2 *__restrict__ h_in, int64_t h_stride,
+// Blocks of 64 threads: two teams (TEAM = 32) or one (TEAM = 64).
+template <int TEAM>
+__global__ void __launch_bounds__(64, TEAM == 32 ? 1 : 6) eigh_refine_f64_team_kernel(const double2 *__restrict__ h_in, int64_t h_stride,
                                                                   const float2 *__restrict__ V_in, int64_t batch, int nw,
                                                                   double *__restrict__ E_out, double2 *__restrict__ U_out,
                                                                   int converge) {
     extern __shared__ __align__(16) unsigned char smraw[];
+    constexpr int ROWS = Team<TEAM>::ROWS;
+    __shared__ double red[2];
     const int np = nw + (nw & 1);
     const int ld = np + 1;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    unsigned char *base = smraw + (size_t)warp * WarpRefineSmem::per_warp(nw);
+    const int team = TEAM == 32 ? (int)(threadIdx.x >> 5) : 0;
+    const int teams = TEAM == 32 ? (int)(blockDim.x >> 5) : 1;
+    unsigned char *base = smraw + (size_t)team * WarpRefineSmem::per_team(nw);
     double2 *A = reinterpret_cast<double2 *>(base);
     double2 *W = A + (size_t)np * ld;
     double2 *rot_s = W + (size_t)np * ld;
@@ -509,87 +579,90 @@ __global__ void __launch_bounds__(64) eigh_refine_f64_warp_kernel(const double2 
     int *rot_p = reinterpret_cast<int *>(rot_c + 16);
     int *rot_q = rot_p + 16;
     int *rank = rot_q + 16;
-    const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
-    double2 col[32];
-    for (int64_t b = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp; b < batch; b += nwarps) {
+    const int t = Team<TEAM>::rank();
+    const int c0 = t & 31, r0 = (t >> 5) * ROWS;
+    const int64_t nteams = (int64_t)gridDim.x * teams;
+    double2 col[ROWS];
+    for (int64_t b = (int64_t)blockIdx.x * teams + team; b < batch; b += nteams) {
         const float2 *vi = V_in + b * (int64_t)np * np;
-        if (lane < np)
-            for (int j = 0; j < np; ++j) W[lane + ld * j] = to_c64(vi[lane + np * j]);
-        __syncwarp();
+        for (int e = t; e < np * np; e += TEAM) {
+            const int i = e % np, j = e / np;
+            W[i + ld * j] = to_c64(vi[i + np * j]);
+        }
+        Team<TEAM>::sync();
         // E = V^H V - I into A; then M = I - E/2 + 3 E^2 / 8 into A; W <- V M.
-        warp_column_product(W, W, col, np, ld, lane, true);
+        team_column_product<TEAM>(W, W, col, np, ld, true);
 #pragma unroll
-        for (int i = 0; i < 32; ++i)
-            if (i == lane) col[i].x -= 1.0;
-        warp_store_column(A, col, np, ld, lane);
-        __syncwarp();
-        warp_column_product(A, A, col, np, ld, lane, false);                 // (E^2)[:, lane]
+        for (int i = 0; i < ROWS; ++i)
+            if (r0 + i == c0) col[i].x -= 1.0;
+        team_store_column<TEAM>(A, col, np, ld);
+        Team<TEAM>::sync();
+        team_column_product<TEAM>(A, A, col, np, ld, false);                 // (E^2)[:, c0]
 #pragma unroll
-        for (int i = 0; i < 32; ++i) {
-            if (i < np && lane < np) {
-                const double2 e = A[i + ld * lane];
-                col[i] = make_double2((i == lane ? 1.0 : 0.0) - 0.5 * e.x + 0.375 * col[i].x, -0.5 * e.y + 0.375 * col[i].y);
+        for (int i = 0; i < ROWS; ++i) {
+            if (r0 + i < np && c0 < np) {
+                const double2 e = A[(r0 + i) + ld * c0];
+                col[i] = make_double2((r0 + i == c0 ? 1.0 : 0.0) - 0.5 * e.x + 0.375 * col[i].x, -0.5 * e.y + 0.375 * col[i].y);
             }
         }
-        __syncwarp();
-        warp_store_column(A, col, np, ld, lane);
-        __syncwarp();
-        warp_column_product(W, A, col, np, ld, lane, false);                 // (V M)[:, lane]
-        __syncwarp();
-        warp_store_column(W, col, np, ld, lane);
-        const double fro = warp_load_hermitian(A, h_in + b * h_stride, nw, np, ld, lane);   // A <- H
-        warp_column_product(A, W, col, np, ld, lane, false);                 // (H W)[:, lane]
-        __syncwarp();
-        warp_store_column(A, col, np, ld, lane);
-        __syncwarp();
-        warp_column_product(W, A, col, np, ld, lane, true);                  // (W^H H W)[:, lane]
-        __syncwarp();
-        warp_store_column(A, col, np, ld, lane);
-        __syncwarp();
-        if (lane < np)
-            for (int i = lane; i < np; ++i) {
-                if (i > lane) A[i + ld * lane] = cconj(A[lane + ld * i]);
-                else A[i + ld * i].y = 0.0;
-            }
-        __syncwarp();
+        Team<TEAM>::sync();
+        team_store_column<TEAM>(A, col, np, ld);
+        Team<TEAM>::sync();
+        team_column_product<TEAM>(W, A, col, np, ld, false);                 // (V M)[:, c0]
+        Team<TEAM>::sync();
+        team_store_column<TEAM>(W, col, np, ld);
+        const double fro = team_load_hermitian<TEAM>(A, h_in + b * h_stride, nw, np, ld, red);   // A <- H
+        team_column_product<TEAM>(A, W, col, np, ld, false);                 // (H W)[:, c0]
+        Team<TEAM>::sync();
+        team_store_column<TEAM>(A, col, np, ld);
+        Team<TEAM>::sync();
+        team_column_product<TEAM>(W, A, col, np, ld, true);                  // (W^H H W)[:, c0]
+        Team<TEAM>::sync();
+        team_store_column<TEAM>(A, col, np, ld);
+        Team<TEAM>::sync();
+        {
+            const int row = t & 31;
+            if (row < np)
+                for (int i = row + (t >> 5); i < np; i += TEAM / 32) {
+                    if (i > row) A[i + ld * row] = cconj(A[row + ld * i]);
+                    else A[i + ld * i].y = 0.0;
+                }
+        }
+        Team<TEAM>::sync();
         const double tol = fro * 8.673617379884035e-19;
         for (int sweep = 0; sweep < (converge ? WNLQG_JACOBI_MAX_SWEEPS : 1); ++sweep) {
-            double off = 0.0;
-            if (lane < np)
-                for (int i = 0; i < np; ++i)
-                    if (i != lane) off += A[i + ld * lane].x * A[i + ld * lane].x + A[i + ld * lane].y * A[i + ld * lane].y;
-            for (int o = 16; o > 0; o >>= 1) off += __shfl_xor_sync(0xffffffffu, off, o);
+            const double off = team_offdiag2<TEAM>(A, np, ld, red);
             if (sqrt(off) <= (converge ? tol * np : fro * 1.0e-13)) break;
-            if (!warp_jacobi_sweep<double>(A, W, np, ld, tol, rot_s, rot_c, rot_p, rot_q, lane)) break;
+            if (!team_jacobi_sweep<double, TEAM>(A, W, np, ld, tol, rot_s, rot_c, rot_p, rot_q)) break;
         }
-        // Ascending order (stable) and canonical phases: lane i handles eigenpair i, then the
-        // columns are written row-wise (coalesced).
-        if (lane < nw) {
-            const double di = A[lane + ld * lane].x;
+        // Ascending order (stable) and canonical phases: thread i handles eigenpair i, then the
+        // columns are written row-wise (coalesced), the warps taking alternate columns.
+        if (t < nw) {
+            const double di = A[t + ld * t].x;
             int r = 0;
             for (int j = 0; j < nw; ++j) {
                 const double dj = A[j + ld * j].x;
-                r += (dj < di) || (dj == di && j < lane);
+                r += (dj < di) || (dj == di && j < t);
             }
             int pivot = 0;
-            double pm = hypot(W[0 + ld * lane].x, W[0 + ld * lane].y);
+            double pm = hypot(W[0 + ld * t].x, W[0 + ld * t].y);
             for (int rr = 1; rr < nw; ++rr) {
-                const double mg = hypot(W[rr + ld * lane].x, W[rr + ld * lane].y);
+                const double mg = hypot(W[rr + ld * t].x, W[rr + ld * t].y);
                 if (mg > pm) { pm = mg; pivot = rr; }
             }
-            phase[lane] = pm > 0.0 ? make_double2(W[pivot + ld * lane].x / pm, -W[pivot + ld * lane].y / pm)
-                                   : make_double2(1.0, 0.0);
-            rank[lane] = r;
+            phase[t] = pm > 0.0 ? make_double2(W[pivot + ld * t].x / pm, -W[pivot + ld * t].y / pm)
+                                : make_double2(1.0, 0.0);
+            rank[t] = r;
             E_out[b * nw + r] = di;
         }
-        __syncwarp();
+        Team<TEAM>::sync();
         double2 *u = U_out + b * (int64_t)nw * nw;
-        for (int c = 0; c < nw; ++c)
-            if (lane < nw) u[lane + (int64_t)nw * rank[c]] = cmul(W[lane + ld * c], phase[c]);
-        __syncwarp();
+        const int row = t & 31;
+        for (int c = t >> 5; c < nw; c += TEAM / 32)
+            if (row < nw) u[row + (int64_t)nw * rank[c]] = cmul(W[row + ld * c], phase[c]);
+        Team<TEAM>::sync();
     }
 }
-
 // ---------------------------------------------------------------------------------------------
 // Generalised Hermitian eigensolve H C = S C E for nonorthogonal models, FP64
 // (generalized_hermitian_spectrum, DenseSpectra.jl:33-39: eigen(Hermitian(H,:U), Hermitian(S,:U))).
