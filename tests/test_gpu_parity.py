@@ -551,19 +551,20 @@ def test_plans_of_different_sizes_share_kernels(engine_cls, oracle_mod, precisio
 
 @pytest.mark.parametrize("precision", [_abi.PRECISION_FP64, _abi.PRECISION_MIXED])
 def test_eigensolver_team_sizes_agree(engine_cls, oracle_mod, precision, monkeypatch):
-    """Warp-per-matrix and two-warps-per-matrix eigensolver stages give the same spectrum (to
+    """Eigensolver stages with one, two or four warps per matrix give the same spectrum (to
     rounding) and the same mesh responses on the nw = 32 workload."""
     model = reference_workload_model("nw32")
     task = nw32_task(nom=64, precision=precision)
     k = np.random.default_rng(18).random((16, 3))
     res = {}
-    for team in ("32", "64"):
+    for team in ("32", "64", "128"):
         monkeypatch.setenv("WNLQG_B200_EIGH_TEAM", team)
         with engine_cls(model, task) as eng:
             res[team] = (eng.spectrum(k)[0], eng.integrate_mesh((6, 5, 4)))
     e32, m32 = res["32"]
-    e64, m64 = res["64"]
-    assert np.max(np.abs(e32 - e64)) < 1e-12 * np.abs(e32).max()
     tol = 1e-11 if precision == _abi.PRECISION_FP64 else 1e-6
-    for g, r in zip(task.split(m64), task.split(m32)):
-        assert rel_err(g, r) < tol
+    for team in ("64", "128"):
+        e, m = res[team]
+        assert np.max(np.abs(e - e32)) < 1e-12 * np.abs(e32).max()
+        for g, r in zip(task.split(m), task.split(m32)):
+            assert rel_err(g, r) < tol

@@ -244,9 +244,9 @@ __global__ void __launch_bounds__(256, 4) jacobi_eigh_kernel(const double2 *__re
 //     Loewdin orthonormalisation of V, H' = W^H H W, FP64 Jacobi sweeps (quadratic
 //     convergence), U = W J, ascending order and canonical phases.
 // A team is one warp (TEAM = 32: several teams per CTA, synchronised with __syncwarp) or one
-// 64-thread CTA (TEAM = 64: two warps share a matrix, synchronised with __syncthreads; each
-// thread then holds half a column in the products and does half of a round's updates, and an
-// SM holds twice the warps for the same shared memory).  A and V sit in the team's own shared
+// CTA of 64 or 128 threads (two or four warps share a matrix, synchronised with __syncthreads;
+// each thread then holds a half or a quarter of a column in the products and does that share of
+// a round's updates, and an SM holds more warps for the same shared memory).  A and V sit in the team's own shared
 // memory.  The Hermitian 2x2 block updates of a round take their (k1 <= k2) pair indices from a
 // fixed table (the order w = k2 (k2 + 1) / 2 + k1 is a prefix for every np <= 32); V <- V J
 // runs one row per thread, the pairs of a round split between the warps.
@@ -254,8 +254,8 @@ __global__ void __launch_bounds__(256, 4) jacobi_eigh_kernel(const double2 *__re
 __constant__ unsigned char c_jacobi_blocks[136][2];
 
 template <int TEAM> struct Team {
-    static_assert(TEAM == 32 || TEAM == 64, "a team is one warp or one 64-thread CTA");
-    static constexpr int ROWS = 32 / (TEAM / 32);   // rows of a product column held per thread: 32 or 16
+    static_assert(TEAM == 32 || TEAM == 64 || TEAM == 128, "a team is one warp or one CTA of 2 or 4 warps");
+    static constexpr int ROWS = 32 / (TEAM / 32);   // rows of a product column held per thread: 32, 16 or 8
     static WNLQG_D int rank() { return TEAM == 32 ? (int)(threadIdx.x & 31) : (int)threadIdx.x; }
     static WNLQG_D void sync() {
         if constexpr (TEAM == 32) __syncwarp();
@@ -273,7 +273,9 @@ template <int TEAM> struct Team {
         } else {
             if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
             __syncthreads();
-            const double t = red[0] + red[1];
+            double t = red[0];
+#pragma unroll
+            for (int w = 1; w < TEAM / 32; ++w) t += red[w];
             __syncthreads();
             return t;
         }
@@ -458,14 +460,14 @@ WNLQG_D double team_offdiag2(const C *A, int np, int ld, double *red) {
     return Team<TEAM>::sum(off, red);
 }
 
-// TEAM = 32: blocks of 128 threads (four teams); TEAM = 64: blocks of 64 threads (one team).
+// TEAM = 32: blocks of 128 threads (four teams); otherwise blocks of TEAM threads (one team).
 template <int TEAM>
-__global__ void __launch_bounds__(TEAM == 32 ? 128 : 64, TEAM == 32 ? 4 : 12) jacobi_f32_team_kernel(const double2 *__restrict__ h_in, int64_t h_stride,
+__global__ void __launch_bounds__(TEAM == 32 ? 128 : TEAM, TEAM == 32 ? 4 : (TEAM == 64 ? 12 : 8)) jacobi_f32_team_kernel(const double2 *__restrict__ h_in, int64_t h_stride,
                                                               int64_t batch, int nw, float2 *__restrict__ V_out,
                                                               int warm_start) {
     extern __shared__ __align__(16) unsigned char smraw[];
     constexpr int ROWS = Team<TEAM>::ROWS;
-    __shared__ double red[2];
+    __shared__ double red[4];
     const int np = nw + (nw & 1);
     const int ld = np + 1;
     const int team = TEAM == 32 ? (int)(threadIdx.x >> 5) : 0;
@@ -557,15 +559,15 @@ struct WarpRefineSmem {
     }
 };
 
-// Blocks of 64 threads: two teams (TEAM = 32) or one (TEAM = 64).
+// Blocks of 64 threads holding two teams (TEAM = 32), otherwise blocks of TEAM threads (one team).
 template <int TEAM>
-__global__ void __launch_bounds__(64, TEAM == 32 ? 1 : 6) eigh_refine_f64_team_kernel(const double2 *__restrict__ h_in, int64_t h_stride,
+__global__ void __launch_bounds__(TEAM == 128 ? 128 : 64, TEAM == 32 ? 1 : 6) eigh_refine_f64_team_kernel(const double2 *__restrict__ h_in, int64_t h_stride,
                                                                   const float2 *__restrict__ V_in, int64_t batch, int nw,
                                                                   double *__restrict__ E_out, double2 *__restrict__ U_out,
                                                                   int converge) {
     extern __shared__ __align__(16) unsigned char smraw[];
     constexpr int ROWS = Team<TEAM>::ROWS;
-    __shared__ double red[2];
+    __shared__ double red[4];
     const int np = nw + (nw & 1);
     const int ld = np + 1;
     const int team = TEAM == 32 ? (int)(threadIdx.x >> 5) : 0;

@@ -114,7 +114,7 @@ struct wnlqg_plan {
     int eigh_threads = 32;
     size_t eigh_smem = 0;
     bool warp_eigh = false;                   // orthogonal models, nw <= 32: team-per-matrix stages
-    int eigh_team = 32;                       // threads per matrix in those stages: 32 or 64
+    int eigh_team = 32;                       // threads per matrix in those stages: 32, 64 or 128
     unsigned char *d_eigh_scratch = nullptr;  // per-CTA global working set of the CTA eigensolvers
     int64_t eigh_scratch_stride = 0;
     int eigh_grid = 0;
@@ -731,10 +731,13 @@ wnlqg_status run_front(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const int64_
     } else if (pl->warp_eigh) {
         // Stage 1: four one-warp teams per 128-thread block, or one 64-thread team per block.
         // Stage 2: 64-thread blocks holding two one-warp teams or one 64-thread team.
-        const bool t64 = pl->eigh_team == 64;
-        const void *f32_fn = t64 ? (const void *)jacobi_f32_team_kernel<64> : (const void *)jacobi_f32_team_kernel<32>;
-        const void *ref_fn = t64 ? (const void *)eigh_refine_f64_team_kernel<64> : (const void *)eigh_refine_f64_team_kernel<32>;
-        const int f32_threads = t64 ? 64 : 128, f32_teams = t64 ? 1 : 4, ref_teams = t64 ? 1 : 2;
+        const int tm = pl->eigh_team;
+        const void *f32_fn = tm == 128 ? (const void *)jacobi_f32_team_kernel<128>
+                             : tm == 64 ? (const void *)jacobi_f32_team_kernel<64> : (const void *)jacobi_f32_team_kernel<32>;
+        const void *ref_fn = tm == 128 ? (const void *)eigh_refine_f64_team_kernel<128>
+                             : tm == 64 ? (const void *)eigh_refine_f64_team_kernel<64> : (const void *)eigh_refine_f64_team_kernel<32>;
+        const int f32_threads = tm == 32 ? 128 : tm, f32_teams = tm == 32 ? 4 : 1;
+        const int ref_threads = tm == 128 ? 128 : 64, ref_teams = tm == 32 ? 2 : 1;
         int per_sm = 1;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f32_fn, f32_threads, pl->eigh_smem);
         const int64_t f32_grid = std::min<int64_t>((nb + f32_teams - 1) / f32_teams, (int64_t)std::max(1, per_sm) * pl->sm_count);
@@ -750,7 +753,7 @@ wnlqg_status run_front(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const int64_
             WNLQG_CUDA(cudaLaunchKernel(f32_fn, dim3((unsigned)f32_grid), dim3(f32_threads), args, pl->eigh_smem, pl->stream));
         }
         int per_sm_r = 1;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_r, ref_fn, 64, pl->refine_smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_r, ref_fn, ref_threads, pl->refine_smem);
         const int64_t r_grid = std::min<int64_t>((nb + ref_teams - 1) / ref_teams, (int64_t)std::max(1, per_sm_r) * pl->sm_count);
         {
             int64_t stride = N, nb_arg = nb;
@@ -760,7 +763,7 @@ wnlqg_status run_front(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const int64_
             double2 *U = pl->d_U;
             int converge = pl->task.precision == WNLQG_PRECISION_MIXED ? 0 : 1;
             void *args[] = {(void *)&hk, &stride, (void *)&v32, &nb_arg, &nw_arg, &E, &U, &converge};
-            WNLQG_CUDA(cudaLaunchKernel(ref_fn, dim3((unsigned)r_grid), dim3(64), args, pl->refine_smem, pl->stream));
+            WNLQG_CUDA(cudaLaunchKernel(ref_fn, dim3((unsigned)r_grid), dim3(ref_threads), args, pl->refine_smem, pl->stream));
         }
         pl->launches += 1;
     } else
@@ -1290,16 +1293,16 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
         pl->eigh_smem = GenEighSmem::bytes(nw);
     } else if (pl->warp_eigh) {
         const int np = nw + (nw & 1);
-        // Above 16 orbitals two warps share a matrix (64-thread teams); WNLQG_B200_EIGH_TEAM=32 or
-        // 64 overrides the choice.
-        pl->eigh_team = nw > 16 ? 64 : 32;
+        // Above 16 orbitals four warps share a matrix (128-thread teams); WNLQG_B200_EIGH_TEAM=32,
+        // 64 or 128 overrides the choice.
+        pl->eigh_team = nw > 16 ? 128 : 32;
         if (const char *tm = std::getenv("WNLQG_B200_EIGH_TEAM")) {
             if (std::string(tm) == "32") pl->eigh_team = 32;
             else if (std::string(tm) == "64") pl->eigh_team = 64;
+            else if (std::string(tm) == "128") pl->eigh_team = 128;
         }
-        const bool t64 = pl->eigh_team == 64;
-        pl->eigh_smem = (t64 ? 1 : 4) * WarpJacobiSmem::per_team(nw);
-        pl->refine_smem = (t64 ? 1 : 2) * WarpRefineSmem::per_team(nw);
+        pl->eigh_smem = (pl->eigh_team == 32 ? 4 : 1) * WarpJacobiSmem::per_team(nw);
+        pl->refine_smem = (pl->eigh_team == 32 ? 2 : 1) * WarpRefineSmem::per_team(nw);
         {
             // Pair-block table of the warp Jacobi: w = k2 (k2 + 1) / 2 + k1, k1 <= k2 < 16.
             unsigned char tab[136][2];
@@ -1309,6 +1312,7 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
             if (et != cudaSuccess) return bail(fail(WNLQG_ERR_CUDA, std::string("cudaMemcpyToSymbol: ") + cudaGetErrorString(et)));
             cudaError_t ea = allow_dynamic_smem((const void *)jacobi_f32_team_kernel<32>, smem_optin);
             if (ea == cudaSuccess) ea = allow_dynamic_smem((const void *)jacobi_f32_team_kernel<64>, smem_optin);
+            if (ea == cudaSuccess) ea = allow_dynamic_smem((const void *)jacobi_f32_team_kernel<128>, smem_optin);
             if (ea != cudaSuccess) return bail(fail(WNLQG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(ea)));
         }
         // Both stages need blockDim >= np/2 (pairs) and 8 * blockDim >= np^2 (register-staged products).
@@ -1318,6 +1322,7 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
         if ((st = alloc((void **)&pl->d_V32, (size_t)max_batch * np * np * sizeof(float2))) != WNLQG_OK) return bail(st);
         cudaError_t e = allow_dynamic_smem((const void *)eigh_refine_f64_team_kernel<32>, smem_optin);
         if (e == cudaSuccess) e = allow_dynamic_smem((const void *)eigh_refine_f64_team_kernel<64>, smem_optin);
+        if (e == cudaSuccess) e = allow_dynamic_smem((const void *)eigh_refine_f64_team_kernel<128>, smem_optin);
         if (e != cudaSuccess) return bail(fail(WNLQG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e)));
     } else {
         // FP64 path, and the mixed path above 32 orbitals: FP64 CTA Jacobi.
