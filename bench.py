@@ -335,10 +335,12 @@ def main():
     # DRAM bytes per k-point (read + write) of each stage's kernel, from the committed ncu
     # captures of 8192-point launches (profiles/*.md), scaled to the step's batch: the kernels
     # stream their inputs point by point, so traffic grows in proportion to the points.
+    # The eigensolve stage is two kernels (FP32 Jacobi, FP64 refinement): their bytes are summed.
     traffic_per_k = {
-        ("fp64", "response"): (1.080335e9 + 6.255872e6) / 8192,     # response_kernel_fp64_nw32_mesh.md
-        ("fp64", "eigen"): (0.084022e9 + 84.824064e6) / 8192,       # response_kernel_fp64_nw32_mesh.md
-        ("mixed", "response"): (1.084089e9 + 8.529664e6) / 8192,    # mixed_path_kernels_nw32_mesh.md
+        ("fp64", "response"): (1.078567e9 + 5.804032e6) / 8192,     # response_kernel_fp64_nw32_mesh.md
+        ("fp64", "eigen"): (0.134364e9 + 35.584512e6 + 0.201415e9 + 99.751424e6) / 8192,
+        ("mixed", "response"): (1.082575e9 + 10.373376e6) / 8192,   # mixed_path_kernels_nw32_mesh.md
+        ("mixed", "eigen"): (0.134277e9 + 35.303168e6 + 0.201391e9 + 96.798464e6) / 8192,
         ("mixed", "fourier_random"): (436.281088e6 + 1.025739e9) / 8192,  # tc_fourier_kernel_nw32_random_k.md
     }
     prec_key = "fp64" if precision == _abi.PRECISION_FP64 else "mixed"
