@@ -247,11 +247,11 @@ __global__ void __launch_bounds__(256, 4) jacobi_eigh_kernel(const double2 *__re
 // CTA of 64 or 128 threads (two or four warps share a matrix, synchronised with __syncthreads;
 // each thread then holds a half or a quarter of a column in the products and does that share of
 // a round's updates, and an SM holds more warps for the same shared memory).  A and V sit in the team's own shared
-// memory.  The Hermitian 2x2 block updates of a round take their (k1 <= k2) pair indices from a
-// fixed table (the order w = k2 (k2 + 1) / 2 + k1 is a prefix for every np <= 32); V <- V J
+// memory.  The off-diagonal 2x2 block updates of a round take their (k1 < k2) pair indices from a
+// fixed table (the order w = k2 (k2 - 1) / 2 + k1 is a prefix for every np <= 32); V <- V J
 // runs one row per thread, the pairs of a round split between the warps.
 // ---------------------------------------------------------------------------------------------
-__constant__ unsigned char c_jacobi_blocks[136][2];
+__constant__ unsigned char c_jacobi_offdiag[120][2];   // k1 < k2 < 16 in the order w = k2 (k2 - 1) / 2 + k1
 
 template <int TEAM> struct Team {
     static_assert(TEAM == 32 || TEAM == 64 || TEAM == 128, "a team is one warp or one CTA of 2 or 4 warps");
@@ -303,7 +303,7 @@ WNLQG_D bool team_jacobi_sweep(typename cplx_of<T>::type *A, typename cplx_of<T>
     typedef typename cplx_of<T>::type C;
     const int t = Team<TEAM>::rank();
     const int half = np / 2;
-    const int nblk = half * (half + 1) / 2;
+    const int noff = half * (half - 1) / 2;
     // V <- V J: thread t handles row t % 32 and the pairs [kb, ke) of its warp.
     const int vrow = t & 31;
     const int kper = (half + TEAM / 32 - 1) / (TEAM / 32);
@@ -335,8 +335,10 @@ WNLQG_D bool team_jacobi_sweep(typename cplx_of<T>::type *A, typename cplx_of<T>
             rot_q[t] = q;
         }
         Team<TEAM>::sync();
-        for (int w = t; w < nblk; w += TEAM) {
-            const int k1 = c_jacobi_blocks[w][0], k2 = c_jacobi_blocks[w][1];
+        // 2x2 block updates: the off-diagonal blocks (k1 < k2, table order) go to threads 0, 1, ...
+        // and the cheaper diagonal blocks (k1 == k2) to the last threads of the team, so that no
+        // thread takes two off-diagonal blocks before every thread has one.
+        auto block = [&](int k1, int k2) {
             const int p1 = rot_p[k1], q1 = rot_q[k1], p2 = rot_p[k2], q2 = rot_q[k2];
             const T c1 = rot_c[k1], c2 = rot_c[k2];
             const C s1 = rot_s[k1], s2 = rot_s[k2];
@@ -365,7 +367,9 @@ WNLQG_D bool team_jacobi_sweep(typename cplx_of<T>::type *A, typename cplx_of<T>
                 A[p2 + ld * p1] = cconj(o00); A[q2 + ld * p1] = cconj(o01);
                 A[p2 + ld * q1] = cconj(o10); A[q2 + ld * q1] = cconj(o11);
             }
-        }
+        };
+        for (int w = t; w < noff; w += TEAM) block(c_jacobi_offdiag[w][0], c_jacobi_offdiag[w][1]);
+        for (int k = TEAM - 1 - t; k < half; k += TEAM) block(k, k);
         if (vrow < np) {
             for (int k = kb; k < ke; ++k) {
                 const int p = rot_p[k], q = rot_q[k];

@@ -327,12 +327,11 @@ WNLQG_D float lorentz(float num, float den) { return __fdividef(num, den); }
 WNLQG_D double lorentz(double num, double den) { return num * lorentz_recip(den); }
 
 // One pair's contribution to a thread's OMB photon energies.  KIND 0: Gaussian with the
-// sqrt(200) cutoff (transition screen); 1: Lorentzian (fq * width / pi folded once per pair);
+// sqrt(200) cutoff (transition screen); 1: Lorentzian (q0, q1 already carry f_nm width / pi);
 // 2: jerk's windowed delta (Gaussian or Lorentzian by `gaussian`).
 template <typename R, typename C, int KIND, int OMB, bool TWO>
 WNLQG_D void contract_one(double te, R fq, C q0, C q1, const double *om, C (*acc)[2], R gsc, R cut, R invw,
                           R w2, R lor, R win, int gaussian) {
-    const R fql = fq * lor;
 #pragma unroll
     for (int j = 0; j < OMB; ++j) {
         const R x = (R)(te - om[j]);
@@ -342,7 +341,7 @@ WNLQG_D void contract_one(double te, R fq, C q0, C q1, const double *om, C (*acc
             const R y = x * invw;
             weight = fq * (gsc * exp(-y * y));
         } else if (KIND == 1) {
-            weight = fql * lorentz_recip(x * x + w2);
+            weight = lorentz_recip(x * x + w2);
         } else {
             if (win > (R)0 && fabs(x) > win) continue;
             const R y = x * invw;
@@ -775,6 +774,9 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 1 : 2) response_kernel(R
                             const C *Ha = slot(p.slot_dH[a]);
                             q = cmul(cmul(csub(Ha[m + ld * m], Ha[n + ld * n]), rc_nm), rb_mn);
                         }
+                        // Lorentzian kernel (pair mode 0): the pair factor f_nm width / pi is
+                        // folded into Q here, once per pair instead of once per photon energy.
+                        if (p.pair_mode == 0 && !p.gaussian) q = cscale(q, (R)(fnm * p.width / WNLQG_PI));
                         sQ[(size_t)c * nn + before] = q;
                     }
                 }

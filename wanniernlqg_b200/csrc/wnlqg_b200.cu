@@ -1304,11 +1304,11 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
         pl->eigh_smem = (pl->eigh_team == 32 ? 4 : 1) * WarpJacobiSmem::per_team(nw);
         pl->refine_smem = (pl->eigh_team == 32 ? 2 : 1) * WarpRefineSmem::per_team(nw);
         {
-            // Pair-block table of the warp Jacobi: w = k2 (k2 + 1) / 2 + k1, k1 <= k2 < 16.
-            unsigned char tab[136][2];
-            for (int k2 = 0, w = 0; k2 < 16; ++k2)
-                for (int k1 = 0; k1 <= k2; ++k1, ++w) { tab[w][0] = (unsigned char)k1; tab[w][1] = (unsigned char)k2; }
-            cudaError_t et = cudaMemcpyToSymbol(c_jacobi_blocks, tab, sizeof(tab));
+            // Off-diagonal pair blocks of the team Jacobi: w = k2 (k2 - 1) / 2 + k1, k1 < k2 < 16.
+            unsigned char off[120][2];
+            for (int k2 = 1, w = 0; k2 < 16; ++k2)
+                for (int k1 = 0; k1 < k2; ++k1, ++w) { off[w][0] = (unsigned char)k1; off[w][1] = (unsigned char)k2; }
+            cudaError_t et = cudaMemcpyToSymbol(c_jacobi_offdiag, off, sizeof(off));
             if (et != cudaSuccess) return bail(fail(WNLQG_ERR_CUDA, std::string("cudaMemcpyToSymbol: ") + cudaGetErrorString(et)));
             cudaError_t ea = allow_dynamic_smem((const void *)jacobi_f32_team_kernel<32>, smem_optin);
             if (ea == cudaSuccess) ea = allow_dynamic_smem((const void *)jacobi_f32_team_kernel<64>, smem_optin);
