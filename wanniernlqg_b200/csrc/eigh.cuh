@@ -299,7 +299,7 @@ WNLQG_D double recip_sqrt(double x) { return 1.0 / sqrt(x); }
 
 template <typename T, int TEAM>
 WNLQG_D bool team_jacobi_sweep(typename cplx_of<T>::type *A, typename cplx_of<T>::type *V, int np, int ld, T tol,
-                               typename cplx_of<T>::type *rot_s, T *rot_c, int *rot_p, int *rot_q) {
+                               typename cplx_of<T>::type *rot_s, T *rot_c) {
     typedef typename cplx_of<T>::type C;
     const int t = Team<TEAM>::rank();
     const int half = np / 2;
@@ -310,11 +310,23 @@ WNLQG_D bool team_jacobi_sweep(typename cplx_of<T>::type *A, typename cplx_of<T>
     const int kb = (t >> 5) * kper, ke = min(half, kb + kper);
     bool rotated = false;
     for (int round = 0; round < np - 1; ++round) {
+        // Pair k of this round rotates indices (p, q) of slots k and np - 1 - k: slot 0 holds index
+        // 0, slot s >= 1 holds ((s - 1 + round) mod (np - 1)) + 1.  Every thread computes the
+        // indices it needs in registers, so its shared-memory loads wait on nothing else.
+        auto slot_index = [&](int sl) -> int {
+            if (sl == 0) return 0;
+            int v = sl - 1 + round;
+            if (v >= np - 1) v -= np - 1;
+            return v + 1;
+        };
+        auto pair_pq = [&](int k, int &p, int &q) {
+            const int i1 = slot_index(k), i2 = slot_index(np - 1 - k);
+            p = min(i1, i2);
+            q = max(i1, i2);
+        };
         if (t < half) {
-            const int s1 = t, s2 = np - 1 - t;
-            const int i1 = s1 == 0 ? 0 : ((s1 - 1 + round) % (np - 1)) + 1;
-            const int i2 = ((s2 - 1 + round) % (np - 1)) + 1;
-            const int p = min(i1, i2), q = max(i1, i2);
+            int p, q;
+            pair_pq(t, p, q);
             const C apq = A[p + ld * q];
             const T g = hypot(apq.x, apq.y);
             T c = (T)1;
@@ -331,15 +343,15 @@ WNLQG_D bool team_jacobi_sweep(typename cplx_of<T>::type *A, typename cplx_of<T>
             }
             rot_c[t] = c;
             rot_s[t] = sp;
-            rot_p[t] = p;
-            rot_q[t] = q;
         }
         Team<TEAM>::sync();
         // 2x2 block updates: the off-diagonal blocks (k1 < k2, table order) go to threads 0, 1, ...
         // and the cheaper diagonal blocks (k1 == k2) to the last threads of the team, so that no
         // thread takes two off-diagonal blocks before every thread has one.
         auto block = [&](int k1, int k2) {
-            const int p1 = rot_p[k1], q1 = rot_q[k1], p2 = rot_p[k2], q2 = rot_q[k2];
+            int p1, q1, p2, q2;
+            pair_pq(k1, p1, q1);
+            pair_pq(k2, p2, q2);
             const T c1 = rot_c[k1], c2 = rot_c[k2];
             const C s1 = rot_s[k1], s2 = rot_s[k2];
             const C s2c = cconj(s2), s1c = cconj(s1);
@@ -372,7 +384,8 @@ WNLQG_D bool team_jacobi_sweep(typename cplx_of<T>::type *A, typename cplx_of<T>
         for (int k = TEAM - 1 - t; k < half; k += TEAM) block(k, k);
         if (vrow < np) {
             for (int k = kb; k < ke; ++k) {
-                const int p = rot_p[k], q = rot_q[k];
+                int p, q;
+                pair_pq(k, p, q);
                 const T c = rot_c[k];
                 const C sk = rot_s[k], skc = cconj(sk);
                 const C vp = V[vrow + ld * p], vq = V[vrow + ld * q];
@@ -481,8 +494,6 @@ __global__ void __launch_bounds__(TEAM == 32 ? 128 : TEAM, TEAM == 32 ? 4 : (TEA
     float2 *V = A + (size_t)np * ld;
     float2 *rot_s = V + (size_t)np * ld;
     float *rot_c = reinterpret_cast<float *>(rot_s + 16);
-    int *rot_p = reinterpret_cast<int *>(rot_c + 16);
-    int *rot_q = rot_p + 16;
     const int t = Team<TEAM>::rank();
     const int64_t nteams = (int64_t)gridDim.x * teams;
     const int64_t gt = (int64_t)blockIdx.x * teams + team;
@@ -534,7 +545,7 @@ __global__ void __launch_bounds__(TEAM == 32 ? 128 : TEAM, TEAM == 32 ? 4 : (TEA
         for (int sweep = 0; sweep < WNLQG_JACOBI_MAX_SWEEPS; ++sweep) {
             const double off = team_offdiag2<TEAM>(A, np, ld, red);
             if (sqrt(off) <= fro * 7.62939453125e-06) break;
-            if (!team_jacobi_sweep<float, TEAM>(A, V, np, ld, tol32, rot_s, rot_c, rot_p, rot_q)) break;
+            if (!team_jacobi_sweep<float, TEAM>(A, V, np, ld, tol32, rot_s, rot_c)) break;
         }
         float2 *vo = V_out + b * (int64_t)np * np;
         for (int e = t; e < np * np; e += TEAM) {
@@ -582,9 +593,7 @@ __global__ void __launch_bounds__(TEAM == 128 ? 128 : 64, TEAM == 32 ? 1 : 6) ei
     double2 *rot_s = W + (size_t)np * ld;
     double2 *phase = rot_s + 16;
     double *rot_c = reinterpret_cast<double *>(phase + 32);
-    int *rot_p = reinterpret_cast<int *>(rot_c + 16);
-    int *rot_q = rot_p + 16;
-    int *rank = rot_q + 16;
+    int *rank = reinterpret_cast<int *>(rot_c + 16) + 32;
     const int t = Team<TEAM>::rank();
     const int c0 = t & 31, r0 = (t >> 5) * ROWS;
     const int64_t nteams = (int64_t)gridDim.x * teams;
@@ -639,7 +648,7 @@ __global__ void __launch_bounds__(TEAM == 128 ? 128 : 64, TEAM == 32 ? 1 : 6) ei
         for (int sweep = 0; sweep < (converge ? WNLQG_JACOBI_MAX_SWEEPS : 1); ++sweep) {
             const double off = team_offdiag2<TEAM>(A, np, ld, red);
             if (sqrt(off) <= (converge ? tol * np : fro * 1.0e-13)) break;
-            if (!team_jacobi_sweep<double, TEAM>(A, W, np, ld, tol, rot_s, rot_c, rot_p, rot_q)) break;
+            if (!team_jacobi_sweep<double, TEAM>(A, W, np, ld, tol, rot_s, rot_c)) break;
         }
         // Ascending order (stable) and canonical phases: thread i handles eigenpair i, then the
         // columns are written row-wise (coalesced), the warps taking alternate columns.
