@@ -436,7 +436,7 @@ def test_large_nw_mesh_matches_oracle(engine_cls, oracle_mod):
         assert rel_err(g, r) < RTOL
 
 
-@pytest.mark.parametrize("nw", [96])
+@pytest.mark.parametrize("nw", [96, 128])
 def test_large_nw_spectrum_matches_oracle(engine_cls, oracle_mod, nw):
     model = synthetic_orthogonal_model(nw, 1, seed=3)
     task = _abi.TaskArrays([(_abi.QUANTUM_METRIC, ["xx"])])
@@ -568,3 +568,35 @@ def test_eigensolver_team_sizes_agree(engine_cls, oracle_mod, precision, monkeyp
         assert np.max(np.abs(e - e32)) < 1e-12 * np.abs(e32).max()
         for g, r in zip(task.split(m), task.split(m32)):
             assert rel_err(g, r) < tol
+
+
+@pytest.mark.parametrize("nw,precision", [(48, _abi.PRECISION_MIXED), (64, _abi.PRECISION_FP64),
+                                          (96, _abi.PRECISION_FP64), (128, _abi.PRECISION_MIXED)])
+def test_large_nw_mixed_precision_eigensolver_matches_cta_jacobi(engine_cls, nw, precision, monkeypatch):
+    """Above 32 orbitals (the FP64 path from 60 orbitals): FP32 CTA Jacobi + FP64 CTA refinement
+    (shared memory at 48 and 64, a global working set for the FP64 stage at 96 and for both at
+    128) against the FP64 CTA Jacobi
+    (WNLQG_B200_CTA_EIGH=1): spectra to 1e-12 (FP64 path) / 1e-11 (mixed path, one FP64 sweep)
+    of max |E|, FP64 mesh responses to 1e-11.  Both engines take the FP64 CUDA-core Fourier sums,
+    which isolates the eigensolver from the mixed path's 4-slice tensor-core Fourier."""
+    monkeypatch.setenv("WNLQG_B200_DIRECT_FOURIER", "1")
+    model = synthetic_orthogonal_model(nw, 1, seed=nw + 1, full_position=True)
+    task = _abi.TaskArrays([(_abi.SHIFT_CURRENT, ["xyy"]), (_abi.QUANTUM_METRIC, ["xx"])],
+                           broadening_type=_abi.LORENTZIAN, broadening=0.03, photon_energies=np.linspace(0, 3, 16),
+                           precision=precision)
+    ref_task = _abi.TaskArrays([(_abi.SHIFT_CURRENT, ["xyy"]), (_abi.QUANTUM_METRIC, ["xx"])],
+                               broadening_type=_abi.LORENTZIAN, broadening=0.03, photon_energies=np.linspace(0, 3, 16))
+    k = np.random.default_rng(nw).random((6, 3))
+    mesh = (3, 2, 2)
+    with engine_cls(model, task) as eng:
+        e, _ = eng.spectrum(k)
+        m = eng.integrate_mesh(mesh)
+    monkeypatch.setenv("WNLQG_B200_CTA_EIGH", "1")
+    with engine_cls(model, ref_task) as eng:
+        e_ref, _ = eng.spectrum(k)
+        m_ref = eng.integrate_mesh(mesh)
+    etol = 1e-12 if precision == _abi.PRECISION_FP64 else 1e-11
+    assert np.max(np.abs(e - e_ref)) < etol * np.abs(e_ref).max()
+    rtol = 1e-11 if precision == _abi.PRECISION_FP64 else MIXED_RTOL
+    for g, r in zip(task.split(m), ref_task.split(m_ref)):
+        assert rel_err(g, r) < rtol

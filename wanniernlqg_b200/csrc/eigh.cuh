@@ -13,6 +13,7 @@
 // (rows of pair k1, columns of pair k2), and V <- V J likewise.
 #pragma once
 #include "common.cuh"
+#include "dmma.cuh"
 
 #define WNLQG_JACOBI_MAX_SWEEPS 30
 
@@ -678,6 +679,208 @@ __global__ void __launch_bounds__(TEAM == 128 ? 128 : 64, TEAM == 32 ? 1 : 6) ei
         Team<TEAM>::sync();
     }
 }
+// ---------------------------------------------------------------------------------------------
+// Mixed-precision eigensolver above 32 orbitals, one CTA per matrix, in two kernels (the same
+// scheme as the team kernels, for matrices a warp team cannot hold):
+//   stage 1 (jacobi_f32_cta_kernel): FP32 parallel Jacobi until the off-diagonal norm is below
+//     2^-17 ||H|| (rotating elements above 2^-20 ||H||), eigenvectors written unsorted;
+//   stage 2 (eigh_refine_f64_cta_kernel): W = second-order Loewdin orthonormalisation of V
+//     (E = W^H W - I, W <- W (I - E/2 + 3E^2/8)), H' = W^H H W, FP64 Jacobi sweeps (mixed path:
+//     one, unless H' is diagonal to 1e-13 ||H||; FP64 path: until the FP64 CTA Jacobi's stopping
+//     rule holds, np 2^-60 ||H||), U = W J, ascending order and canonical phases.  The products
+//     run on the FP64 tensor cores (dmma_product).
+// GW: the working set lives in global memory (gscratch, one stride per CTA) when it does not fit
+// shared memory.
+// ---------------------------------------------------------------------------------------------
+template <bool GW>
+__global__ void __launch_bounds__(256, 3) jacobi_f32_cta_kernel(const double2 *__restrict__ h_in, int64_t h_stride,
+                                                              int64_t batch, int nw, float2 *__restrict__ V_out,
+                                                              unsigned char *gscratch, int64_t gscratch_stride) {
+    extern __shared__ __align__(16) unsigned char smem_dyn[];
+    unsigned char *smraw;
+    if constexpr (GW) smraw = gscratch + (int64_t)blockIdx.x * gscratch_stride;
+    else smraw = smem_dyn;
+    const int np = nw + (nw & 1);
+    const int ld = np + 1;
+    const int half = np / 2;
+    float2 *A = reinterpret_cast<float2 *>(smraw);
+    float2 *V = A + (size_t)np * ld;
+    float2 *rot_s = V + (size_t)np * ld;
+    double *scratch = reinterpret_cast<double *>(rot_s + half);
+    float *rot_c = reinterpret_cast<float *>(scratch + 2);
+    int *rot_p = reinterpret_cast<int *>(rot_c + half);
+    int *rot_q = rot_p + half;
+    __shared__ double red[48];
+    __shared__ int rot_flag;
+    const int tid = threadIdx.x;
+    for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) {
+        const double2 *h = h_in + b * h_stride;
+        double local = 0.0;
+        for (int e = tid; e < np * np; e += blockDim.x) {
+            const int i = e % np, j = e / np;
+            double2 v = make_double2(0.0, 0.0);
+            if (i < nw && j < nw) {
+                if (i < j) v = h[i + (size_t)nw * j];
+                else if (i > j) v = cconj(h[j + (size_t)nw * i]);
+                else v = make_double2(h[i + (size_t)nw * i].x, 0.0);
+            }
+            local += v.x * v.x + v.y * v.y;
+            A[i + ld * j] = make_float2((float)v.x, (float)v.y);
+            V[i + ld * j] = make_float2(i == j ? 1.0f : 0.0f, 0.0f);
+        }
+        for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xffffffffu, local, o);
+        if ((tid & 31) == 0) red[tid >> 5] = local;
+        __syncthreads();
+        if (tid == 0) {
+            double s = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+            scratch[0] = sqrt(s);
+        }
+        __syncthreads();
+        const double fro = scratch[0];
+        const float tol32 = (float)(fro * 9.5367431640625e-07);
+        for (int sweep = 0; sweep < WNLQG_JACOBI_MAX_SWEEPS; ++sweep) {
+            if (offdiag_norm(A, np, ld, red) <= fro * 7.62939453125e-06) break;
+            if (tid == 0) rot_flag = 0;
+            __syncthreads();
+            jacobi_sweep<float>(A, V, np, ld, tol32, rot_s, rot_c, rot_p, rot_q, &rot_flag);
+            const int any = rot_flag;
+            __syncthreads();
+            if (!any) break;
+        }
+        float2 *vo = V_out + b * (int64_t)np * np;
+        for (int e = tid; e < np * np; e += blockDim.x) {
+            const int i = e % np, j = e / np;
+            vo[i + (int64_t)np * j] = V[i + ld * j];
+        }
+        __syncthreads();
+    }
+}
+
+struct RefineCtaSmem {
+    // A, W, T (np x ld complex double), rotation sines, cosines and pair indices, scratch.
+    static __host__ __device__ size_t bytes(int nw) {
+        const int np = nw + (nw & 1);
+        const int ld = np + 1;
+        const int half = np / 2;
+        size_t s = 3 * (size_t)np * ld * sizeof(double2);
+        s += (size_t)half * (sizeof(double2) + sizeof(double) + 2 * sizeof(int));
+        return (s + 15) & ~(size_t)15;
+    }
+};
+
+template <bool GW>
+__global__ void __launch_bounds__(512, 1) eigh_refine_f64_cta_kernel(const double2 *__restrict__ h_in, int64_t h_stride,
+                                                                   const float2 *__restrict__ V_in, int64_t batch, int nw,
+                                                                   double *__restrict__ E_out, double2 *__restrict__ U_out,
+                                                                   int converge, unsigned char *gscratch,
+                                                                   int64_t gscratch_stride) {
+    extern __shared__ __align__(16) unsigned char smem_dyn[];
+    unsigned char *smraw;
+    if constexpr (GW) smraw = gscratch + (int64_t)blockIdx.x * gscratch_stride;
+    else smraw = smem_dyn;
+    const int np = nw + (nw & 1);
+    const int ld = np + 1;
+    const int half = np / 2;
+    const size_t mat = (size_t)np * ld;
+    double2 *A = reinterpret_cast<double2 *>(smraw);
+    double2 *W = A + mat;
+    double2 *T = W + mat;
+    double2 *rot_s = T + mat;
+    double *rot_c = reinterpret_cast<double *>(rot_s + half);
+    int *rot_p = reinterpret_cast<int *>(rot_c + half);
+    int *rot_q = rot_p + half;
+    __shared__ double red[48];
+    __shared__ int rot_flag;
+    const int tid = threadIdx.x;
+    for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) {
+        double2 *Wc = W, *Tc = T;
+        const float2 *vi = V_in + b * (int64_t)np * np;
+        for (int e = tid; e < np * np; e += blockDim.x) {
+            const int i = e % np, j = e / np;
+            Wc[i + ld * j] = to_c64(vi[i + np * j]);
+        }
+        __syncthreads();
+        dmma_product<1>(Wc, Wc, Tc, np, ld);                 // T = W^H W
+        __syncthreads();
+        for (int i = tid; i < np; i += blockDim.x) Tc[i + ld * i].x -= 1.0;   // E = W^H W - I
+        __syncthreads();
+        dmma_product<0>(Tc, Tc, A, np, ld);                  // A = E^2
+        __syncthreads();
+        for (int e = tid; e < np * np; e += blockDim.x) {    // A = M = I - E/2 + 3 E^2 / 8
+            const int i = e % np, j = e / np, o = i + ld * j;
+            const double2 ev = Tc[o], e2 = A[o];
+            A[o] = make_double2((i == j ? 1.0 : 0.0) - 0.5 * ev.x + 0.375 * e2.x, -0.5 * ev.y + 0.375 * e2.y);
+        }
+        __syncthreads();
+        dmma_product<0>(Wc, A, Tc, np, ld);                  // T = W M
+        __syncthreads();
+        { double2 *x = Wc; Wc = Tc; Tc = x; }                // W <- W M
+        // A <- H (Hermitian from the upper triangle, zero-padded), Frobenius norm.
+        const double2 *h = h_in + b * h_stride;
+        double local = 0.0;
+        for (int e = tid; e < np * np; e += blockDim.x) {
+            const int i = e % np, j = e / np;
+            double2 v = make_double2(0.0, 0.0);
+            if (i < nw && j < nw) {
+                if (i < j) v = h[i + (size_t)nw * j];
+                else if (i > j) v = cconj(h[j + (size_t)nw * i]);
+                else v = make_double2(h[i + (size_t)nw * i].x, 0.0);
+            }
+            local += v.x * v.x + v.y * v.y;
+            A[i + ld * j] = v;
+        }
+        for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xffffffffu, local, o);
+        if ((tid & 31) == 0) red[tid >> 5] = local;
+        __syncthreads();
+        double fro = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) fro += red[w];
+        fro = sqrt(fro);
+        dmma_product<0>(A, Wc, Tc, np, ld);                  // T = H W
+        __syncthreads();
+        dmma_product<1>(Wc, Tc, A, np, ld);                  // A = W^H H W
+        __syncthreads();
+        for (int e = tid; e < np * np; e += blockDim.x) {    // exact Hermitian symmetry
+            const int i = e % np, j = e / np;
+            if (i > j) A[i + ld * j] = cconj(A[j + ld * i]);
+            else if (i == j) A[i + ld * i].y = 0.0;
+        }
+        __syncthreads();
+        const double tol = fro * 8.673617379884035e-19;
+        for (int sweep = 0; sweep < (converge ? WNLQG_JACOBI_MAX_SWEEPS : 1); ++sweep) {
+            const double off = offdiag_norm(A, np, ld, red);
+            if (off <= (converge ? tol * np : fro * 1.0e-13)) break;
+            if (tid == 0) rot_flag = 0;
+            __syncthreads();
+            jacobi_sweep<double>(A, Wc, np, ld, tol, rot_s, rot_c, rot_p, rot_q, &rot_flag);
+            const int any = rot_flag;
+            __syncthreads();
+            if (!any) break;
+        }
+        // Ascending order (stable), then phase canonicalisation per column.
+        for (int i = tid; i < nw; i += blockDim.x) {
+            const double di = A[i + ld * i].x;
+            int rank = 0;
+            for (int j = 0; j < nw; ++j) {
+                const double dj = A[j + ld * j].x;
+                rank += (dj < di) || (dj == di && j < i);
+            }
+            int pivot = 0;
+            double pm = hypot(Wc[0 + ld * i].x, Wc[0 + ld * i].y);
+            for (int r = 1; r < nw; ++r) {
+                const double mg = hypot(Wc[r + ld * i].x, Wc[r + ld * i].y);
+                if (mg > pm) { pm = mg; pivot = r; }
+            }
+            double2 phase = make_double2(1.0, 0.0);
+            if (pm > 0.0) phase = make_double2(Wc[pivot + ld * i].x / pm, -Wc[pivot + ld * i].y / pm);
+            E_out[b * nw + rank] = di;
+            double2 *u = U_out + b * (int64_t)nw * nw + (int64_t)nw * rank;
+            for (int r = 0; r < nw; ++r) u[r] = cmul(Wc[r + ld * i], phase);
+        }
+        __syncthreads();
+    }
+}
+
 // ---------------------------------------------------------------------------------------------
 // Generalised Hermitian eigensolve H C = S C E for nonorthogonal models, FP64
 // (generalized_hermitian_spectrum, DenseSpectra.jl:33-39: eigen(Hermitian(H,:U), Hermitian(S,:U))).

@@ -115,6 +115,9 @@ struct wnlqg_plan {
     size_t eigh_smem = 0;
     bool warp_eigh = false;                   // orthogonal models, nw <= 32: team-per-matrix stages
     int eigh_team = 32;                       // threads per matrix in those stages: 32, 64 or 128
+    bool cta_mixed = false;                   // orthogonal models above 32 orbitals: CTA FP32 + FP64 stages
+    bool cta_gw1 = false, cta_gw2 = false;    // those stages' working sets in global memory
+    int refine_cta_threads = 512;             // FP64 CTA refinement block size
     unsigned char *d_eigh_scratch = nullptr;  // per-CTA global working set of the CTA eigensolvers
     int64_t eigh_scratch_stride = 0;
     int eigh_grid = 0;
@@ -766,6 +769,31 @@ wnlqg_status run_front(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const int64_
             WNLQG_CUDA(cudaLaunchKernel(ref_fn, dim3((unsigned)r_grid), dim3(ref_threads), args, pl->refine_smem, pl->stream));
         }
         pl->launches += 1;
+    } else if (pl->cta_mixed) {
+        const double2 *hk = pl->d_xw + (int64_t)pl->ch_H * pl->nn;
+        const int converge = pl->task.precision == WNLQG_PRECISION_MIXED ? 0 : 1;
+        if (pl->cta_gw1) {
+            jacobi_f32_cta_kernel<true><<<(unsigned)std::min<int64_t>(nb, pl->eigh_grid), 256, 0, pl->stream>>>(
+                hk, N, nb, pl->nw, pl->d_V32, pl->d_eigh_scratch, pl->eigh_scratch_stride);
+        } else {
+            int per_sm = 1;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jacobi_f32_cta_kernel<false>, 256, pl->eigh_smem);
+            const int64_t grid = std::min<int64_t>(nb, (int64_t)std::max(1, per_sm) * pl->sm_count);
+            jacobi_f32_cta_kernel<false><<<(unsigned)grid, 256, pl->eigh_smem, pl->stream>>>(hk, N, nb, pl->nw, pl->d_V32,
+                                                                                            nullptr, 0);
+        }
+        if (pl->cta_gw2) {
+            eigh_refine_f64_cta_kernel<true><<<(unsigned)std::min<int64_t>(nb, pl->eigh_grid), pl->refine_cta_threads, 0, pl->stream>>>(
+                hk, N, pl->d_V32, nb, pl->nw, pl->d_E, pl->d_U, converge, pl->d_eigh_scratch, pl->eigh_scratch_stride);
+        } else {
+            int per_sm = 1;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, eigh_refine_f64_cta_kernel<false>, pl->refine_cta_threads,
+                                                          pl->refine_smem);
+            const int64_t grid = std::min<int64_t>(nb, (int64_t)std::max(1, per_sm) * pl->sm_count);
+            eigh_refine_f64_cta_kernel<false><<<(unsigned)grid, pl->refine_cta_threads, pl->refine_smem, pl->stream>>>(
+                hk, N, pl->d_V32, nb, pl->nw, pl->d_E, pl->d_U, converge, nullptr, 0);
+        }
+        pl->launches += 1;
     } else
         if (pl->d_eigh_scratch)
             jacobi_eigh_kernel<double, true><<<eigh_grid, pl->eigh_threads, 0, pl->stream>>>(
@@ -1287,6 +1315,12 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
         const char *cta = std::getenv("WNLQG_B200_CTA_EIGH");
         const bool cta_fp64 = cta && cta[0] == '1' && t.precision != WNLQG_PRECISION_MIXED;
         pl->warp_eigh = !pl->nonorth && nw <= 32 && !cta_fp64;
+        // Above 32 orbitals the CTA FP32 + FP64 stages; on the FP64 path only once two FP64 CTA
+        // Jacobi working sets no longer fit one SM (there the plain FP64 Jacobi is faster).
+        const bool fp64_cta_pair_fits =
+            2 * (EighSmem::bytes(nw, sizeof(double2)) + 512) <= (size_t)smem_optin;
+        pl->cta_mixed = !pl->nonorth && nw > 32 && !cta_fp64 &&
+                        (t.precision == WNLQG_PRECISION_MIXED || !fp64_cta_pair_fits);
     }
     if (pl->nonorth) {
         pl->eigh_threads = std::max(pl->eigh_threads, ((nw + (nw & 1)) / 2 + 31) / 32 * 32);
@@ -1324,11 +1358,39 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
         if (e == cudaSuccess) e = allow_dynamic_smem((const void *)eigh_refine_f64_team_kernel<64>, smem_optin);
         if (e == cudaSuccess) e = allow_dynamic_smem((const void *)eigh_refine_f64_team_kernel<128>, smem_optin);
         if (e != cudaSuccess) return bail(fail(WNLQG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e)));
+    } else if (pl->cta_mixed) {
+        // Above 32 orbitals: FP32 CTA Jacobi (256 threads) and FP64 CTA refinement (512 threads),
+        // each in shared memory when it fits beside the kernel's static shared memory, else in a
+        // per-CTA global working set (one scratch, one grid, the larger stride).
+        const int np = nw + (nw & 1);
+        pl->eigh_smem = EighSmem::bytes(nw, sizeof(float2));
+        pl->refine_smem = RefineCtaSmem::bytes(nw);
+        cudaFuncAttributes fa1, fa2;
+        cudaError_t fe = cudaFuncGetAttributes(&fa1, (const void *)jacobi_f32_cta_kernel<false>);
+        if (fe == cudaSuccess) fe = cudaFuncGetAttributes(&fa2, (const void *)eigh_refine_f64_cta_kernel<false>);
+        if (fe != cudaSuccess) return bail(fail(WNLQG_ERR_CUDA, std::string("cudaFuncGetAttributes: ") + cudaGetErrorString(fe)));
+        pl->cta_gw1 = pl->eigh_smem + fa1.sharedSizeBytes > (size_t)smem_optin;
+        pl->cta_gw2 = pl->refine_smem + fa2.sharedSizeBytes > (size_t)smem_optin;
+        // 256-thread refinement blocks when two fit an SM (shared memory and registers), else 512.
+        pl->refine_cta_threads =
+            (!pl->cta_gw2 && 2 * (pl->refine_smem + fa2.sharedSizeBytes) <= (size_t)smem_optin) ? 256 : 512;
+        if ((st = alloc((void **)&pl->d_V32, (size_t)max_batch * np * np * sizeof(float2))) != WNLQG_OK) return bail(st);
+        if (pl->cta_gw1 || pl->cta_gw2) {
+            const size_t need = std::max(pl->cta_gw1 ? pl->eigh_smem : 0, pl->cta_gw2 ? pl->refine_smem : 0);
+            pl->eigh_scratch_stride = (int64_t)((need + 255) & ~(size_t)255);
+            pl->eigh_grid = l2_resident_grid(4 * sm_count, pl->eigh_scratch_stride, sm_count);
+            if ((st = alloc((void **)&pl->d_eigh_scratch, (size_t)pl->eigh_grid * pl->eigh_scratch_stride)) != WNLQG_OK)
+                return bail(st);
+        }
+        cudaError_t e = cudaSuccess;
+        if (!pl->cta_gw1) e = allow_dynamic_smem((const void *)jacobi_f32_cta_kernel<false>, smem_optin);
+        if (e == cudaSuccess && !pl->cta_gw2) e = allow_dynamic_smem((const void *)eigh_refine_f64_cta_kernel<false>, smem_optin);
+        if (e != cudaSuccess) return bail(fail(WNLQG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e)));
     } else {
-        // FP64 path, and the mixed path above 32 orbitals: FP64 CTA Jacobi.
+        // FP64 CTA Jacobi (WNLQG_B200_CTA_EIGH=1 on the FP64 path).
         pl->eigh_smem = EighSmem::bytes(nw, sizeof(double2));
     }
-    if (!pl->warp_eigh) {
+    if (!pl->warp_eigh && !pl->cta_mixed) {
         // CTA eigensolvers keep A, V (and the Cholesky factor) in shared memory when they fit
         // beside the kernel's static shared memory, else in a per-CTA global working set (large nw).
         const void *cta_fn = pl->nonorth ? (const void *)generalized_eigh_kernel<false> : (const void *)jacobi_eigh_kernel<double, false>;
