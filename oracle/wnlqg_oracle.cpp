@@ -87,6 +87,7 @@ struct Needs {
     bool A[3] = {false, false, false};
     bool dA[3][3] = {};   // [position][derivative]
     bool F[3][3] = {};
+    bool shg = false;     // second harmonic generation (metric models: the source jets below)
     void need_r(int a) { A[a] = true; dH[a] = true; }
     void need_gder(int p, int d) {   // r^p_{nm;d}
         dA[p][d] = true; ddH[p][d] = true; ddH[d][p] = true;
@@ -103,6 +104,11 @@ struct KData {
     // metric generalized derivatives G[p][d] (position p, derivative d) replace gder.
     bool nonorth = false;
     Mat G[3][3];
+    // Metric SHG inputs (nonorthogonal models with an SHG request): the normalized local source
+    // jets (hamiltonian derivatives, internal connection, their derivatives), the metric energy
+    // Hessians esd[l + n (a + 3 b)] and the isolated-band curvatures iso[l + n (a + 3 b)].
+    Mat srcV[3], srcA[3], srcW[3][3], srcdA[3][3];
+    std::vector<double> esd, iso;
 };
 
 void set_error(const std::string &s) { g_error = s; }
@@ -531,6 +537,111 @@ void nonorth_kpoint(const Model &m, const Needs &need, const double k[3], double
                     G(l, mm) = I1 * dd + bd(l, mm) - I1 * (d.r[q](l, l) - d.r[q](mm, mm)) * d.r[p](l, mm);
                 }
         }
+    if (!need.shg) return;
+    // Metric SHG inputs.
+    Mat rot2h[3][3], rot2s[3][3], rotB[3][3];   // C^H d2H_ab C, C^H d2S_ab C, C^H (dr_ab + i d2S_ab) C
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+            rotate(d, d2h[a][b], rot2h[a][b]);
+            rotate(d, d2s[a][b], rot2s[a][b]);
+            Mat X; X.init(n);
+            for (size_t e = 0; e < nn; ++e) X.v[e] = dr[a][b].v[e] + I1 * d2s[a][b].v[e];
+            rotate(d, X, rotB[a][b]);
+        }
+    // Normalized local source jets (_prepare_nonorthogonal_optical_cutoff!,
+    // NonorthogonalOpticalCutoffVertices.jl:67-186): with k_a = C^H dH_a C, g_a = C^H dS_a C and
+    // raw_a = C^H (r_a + i dS_a) C,
+    //   V_a = k_a - (E_i + E_j) g_a / 2,   A_a = raw_a - i g_a / 2,
+    //   z_ab = -C^H d2S_ab C / 2 + 3 (g_a g_b + g_b g_a) / 8,
+    //   W_ab = C^H d2H_ab C - (g_a k_b + k_b g_a + g_b k_a + k_a g_b) / 2
+    //          + (g_a E g_b + g_b E g_a) / 4 + (E_i + E_j) z_ab,
+    //   dA_ab = C^H (dr_ab + i d2S_ab) C - (g_b raw_a + raw_a g_b) / 2 + i (z_ab - g_b g_a / 4).
+    for (int a = 0; a < 3; ++a) {
+        d.srcV[a] = numer[a];
+        d.srcA[a].init(n);
+        for (size_t e = 0; e < nn; ++e) d.srcA[a].v[e] = conn[a].v[e] - 0.5 * I1 * dsb[a].v[e];
+    }
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+            const Mat &ga = dsb[a], &gb = dsb[b], &ka = dhb[a], &kb = dhb[b];
+            Mat gagb = mul(ga, gb), gbga = mul(gb, ga);
+            Mat z; z.init(n);
+            for (size_t e = 0; e < nn; ++e) z.v[e] = -0.5 * rot2s[a][b].v[e] + 0.375 * (gagb.v[e] + gbga.v[e]);
+            Mat Egb, Ega;
+            Egb.init(n); Ega.init(n);
+            for (int j = 0; j < n; ++j)
+                for (int i = 0; i < n; ++i) { Egb(i, j) = ev[i] * gb(i, j); Ega(i, j) = ev[i] * ga(i, j); }
+            Mat p1 = mul(ga, kb), p2 = mul(kb, ga), p3 = mul(gb, ka), p4 = mul(ka, gb);
+            Mat q1 = mul(ga, Egb), q2 = mul(gb, Ega);
+            Mat &W = d.srcW[a][b];
+            W.init(n);
+            for (int j = 0; j < n; ++j)
+                for (int i = 0; i < n; ++i) {
+                    const size_t e = (size_t)i + (size_t)n * j;
+                    W.v[e] = rot2h[a][b].v[e] - 0.5 * (p1.v[e] + p2.v[e] + p3.v[e] + p4.v[e]) +
+                             0.25 * (q1.v[e] + q2.v[e]) + (ev[i] + ev[j]) * z.v[e];
+                }
+            Mat r1 = mul(gb, conn[a]), r2 = mul(conn[a], gb);
+            Mat &dA = d.srcdA[a][b];
+            dA.init(n);
+            for (size_t e = 0; e < nn; ++e)
+                dA.v[e] = rotB[a][b].v[e] - 0.5 * (r1.v[e] + r2.v[e]) + I1 * (z.v[e] - 0.25 * gbga.v[e]);
+        }
+    // Metric energy Hessians (_nonorthogonal_geometry, NonorthogonalMatrixElements.jl:660-727):
+    // with hd = D_b^H dh_a + dh_a D_b + C^H d2H_ab C and sd likewise from ds,
+    // esd[l, a, b] = Re(hd_ll - E_l sd_ll - v_l^b ds_ll^a).
+    d.esd.assign((size_t)n * 9, 0.0);
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+            const Mat &Db = d.D[b];
+            for (int l = 0; l < n; ++l) {
+                cd hd = rot2h[a][b](l, l), sd = rot2s[a][b](l, l);
+                for (int q = 0; q < n; ++q) {
+                    hd += std::conj(Db(q, l)) * dhb[a](q, l) + dhb[a](l, q) * Db(q, l);
+                    sd += std::conj(Db(q, l)) * dsb[a](q, l) + dsb[a](l, q) * Db(q, l);
+                }
+                d.esd[l + (size_t)n * (a + 3 * b)] =
+                    (hd - ev[l] * sd - ed[l + (size_t)n * b] * dsb[a](l, l)).real();
+            }
+        }
+    // Isolated-band curvature (isolated_band_curvature, NonorthogonalMatrixElements.jl:1141-1185)
+    // with the band-frame ambient metric curvature (_nonorthogonal_ambient_curvature, :819-878):
+    // using S^-1 = C C^H, its diagonal is
+    //   (B_b;a - g_a B_b - B_a;b + g_b B_a - i (B_a B_b - B_b B_a))_nn,
+    // B_a = C^H (r_a + i dS_a) C and B_a;b = C^H (dr_ab + i d2S_ab) C.
+    auto bare_inv = [](double x) { return std::fabs(x) < 1.0e-7 ? 0.0 : 1.0 / x; };
+    d.iso.assign((size_t)n * 9, 0.0);
+    for (int l = 0; l < n; ++l) {
+        cd row[3][128], col[3][128];
+        for (int mm = 0; mm < n; ++mm) {
+            if (mm == l) continue;
+            const double inv = bare_inv(ev[mm] - ev[l]), rinv = bare_inv(ev[l] - ev[mm]);
+            const double avg = 0.5 * (ev[l] + ev[mm]);
+            for (int a = 0; a < 3; ++a) {
+                const cd fw = conn[a](l, mm), rv = conn[a](mm, l);
+                const cd mf = -I1 * (fw - std::conj(rv)), mr = -I1 * (rv - std::conj(fw));
+                const cd ff = 0.5 * (fw + std::conj(rv)), fr = 0.5 * (rv + std::conj(fw));
+                const cd nf = dhb[a](l, mm) - avg * mf, nr = dhb[a](mm, l) - avg * mr;
+                row[a][mm] = inv == 0.0 ? ff : ff + I1 * nf * inv;
+                col[a][mm] = rinv == 0.0 ? fr : fr + I1 * nr * rinv;
+            }
+        }
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) {
+                if (a == b) continue;
+                cd band = rotB[b][a](l, l) - rotB[a][b](l, l);
+                for (int q = 0; q < n; ++q) {
+                    band += -dsb[a](l, q) * conn[b](q, l) + dsb[b](l, q) * conn[a](q, l) -
+                            I1 * (conn[a](l, q) * conn[b](q, l) - conn[b](l, q) * conn[a](q, l));
+                }
+                double value = band.real();
+                for (int mm = 0; mm < n; ++mm) {
+                    if (mm == l) continue;
+                    value -= 2.0 * (row[a][mm] * col[b][mm]).imag();
+                }
+                d.iso[l + (size_t)n * (a + 3 * b)] = value;
+            }
+    }
 }
 
 // conventional_generalized_position_derivative_element (ConventionalShiftCurrent.jl:191-229):
@@ -687,6 +798,7 @@ bool build_task(const wnlqg_task_desc *t, Task &task) {
                 if (q.kind == WNLQG_BERRY_DIPOLE) task.need.dH[cc] = true;
                 break;
             case WNLQG_SECOND_HARMONIC:
+                task.need.shg = true;
                 for (int x = 0; x < 3; ++x) {
                     task.need.dH[x] = true; task.need.A[x] = true;
                     for (int y = 0; y < 3; ++y) { task.need.dA[x][y] = true; task.need.ddH[x][y] = true; }
@@ -828,6 +940,12 @@ double shg_occupation(double e, double mu, double T) {
 struct ShgParams {
     double mu, T, width, low_width, eta, degeneracy;
     bool gaussian, eta_correction;
+    // Metric (nonorthogonal) models: the vertices take the geometry width vertex_eta, r_eta is
+    // the metric Berry connection, and the Hessians and isolated-band curvatures are the metric
+    // ones (SecondHarmonicKernels.jl:47-68, NonorthogonalMatrixElements.jl:1088-1139).
+    double vertex_eta = -1.0;                 // < 0: the energy-sum width eta
+    const cd *rdip = nullptr;                  // [n*n*3]
+    const double *hess = nullptr, *curv = nullptr;   // [n*9], index l + n (a + 3 b)
 };
 
 void shg_response(int n, const double *E, const cd *V, const cd *A, const cd *dA, const cd *W, int64_t nom,
@@ -852,9 +970,9 @@ void shg_response(int n, const double *E, const cd *V, const cd *A, const cd *dA
                 size_t e = i + n * (j + (size_t)n * a);
                 double inv = bare_inverse(E[j] - E[i]);
                 D0[e] = inv == 0.0 ? cd(0.0, 0.0) : V[e] * inv;
-                Dr[e] = V[e] * regularized_inverse(E[j] - E[i], p.eta);
+                Dr[e] = V[e] * regularized_inverse(E[j] - E[i], p.vertex_eta >= 0.0 ? p.vertex_eta : p.eta);
                 r0[e] = A[e] + I1 * D0[e];
-                re[e] = A[e] + I1 * Dr[e];
+                re[e] = p.rdip ? p.rdip[e] : A[e] + I1 * Dr[e];
             }
     auto d0 = [&](int i, int j, int a) { return D0[i + n * (j + n * a)]; };
     auto dr = [&](int i, int j, int a) { return Dr[i + n * (j + n * a)]; };
@@ -952,7 +1070,10 @@ void shg_response(int n, const double *E, const cd *V, const cd *A, const cd *dA
         // _second_harmonic_bcd_enabled: a singleton of the adjacent-gap partition.
         const bool isolated = (i == 0 || E[i] - E[i - 1] > p.degeneracy) && (i == n - 1 || E[i + 1] - E[i] > p.degeneracy);
         double curv[3][3] = {};
-        if (isolated)
+        if (isolated && p.curv)
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) curv[a][b] = a == b ? 0.0 : p.curv[i + n * (a + 3 * b)];
+        else if (isolated)
             for (int a = 0; a < 3; ++a)
                 for (int b = 0; b < 3; ++b) {
                     if (a == b) continue;
@@ -965,9 +1086,13 @@ void shg_response(int n, const double *E, const cd *V, const cd *A, const cd *dA
         for (int c = 0; c < nc; ++c) {
             const int a = comps[c][0], b = comps[c][1], cc = comps[c][2];
             double hess = w4(i, i, b, cc).real();
-            for (int q = 0; q < n; ++q) {
-                if (q == i) continue;
-                hess += 2.0 * (v3(i, q, b) * v3(q, i, cc)).real() * shg_principal(E[i] - E[q], p.eta);
+            if (p.hess) {
+                hess = p.hess[i + n * (b + 3 * cc)];
+            } else {
+                for (int q = 0; q < n; ++q) {
+                    if (q == i) continue;
+                    hess += 2.0 * (v3(i, q, b) * v3(q, i, cc)).real() * shg_principal(E[i] - E[q], p.eta);
+                }
             }
             const double va = v3(i, i, a).real(), vb = v3(i, i, b).real(), vc = v3(i, i, cc).real();
             const double semi = sd * va * vb * vc + fd * va * hess;
@@ -1138,14 +1263,22 @@ void point_values(const Model &m, const Task &task, const double k[3], cd *out) 
             o += nmu * nc;
         } else if (q.kind == WNLQG_SECOND_HARMONIC) {
             const size_t nn = (size_t)n * n;
-            std::vector<cd> V(nn * 3), A(nn * 3), dA(nn * 9), W(nn * 9);
+            std::vector<cd> V(nn * 3), A(nn * 3), dA(nn * 9), W(nn * 9), R;
             for (int a = 0; a < 3; ++a) {
-                for (size_t e = 0; e < nn; ++e) { V[e + nn * a] = d.dH[a].v[e]; A[e + nn * a] = d.Aint[a].v[e]; }
-                for (int b = 0; b < 3; ++b)
+                const Mat &va = d.nonorth ? d.srcV[a] : d.dH[a], &aa = d.nonorth ? d.srcA[a] : d.Aint[a];
+                for (size_t e = 0; e < nn; ++e) { V[e + nn * a] = va.v[e]; A[e + nn * a] = aa.v[e]; }
+                for (int b = 0; b < 3; ++b) {
+                    const Mat &dab = d.nonorth ? d.srcdA[a][b] : d.dA[a][b], &wab = d.nonorth ? d.srcW[a][b] : d.ddH[a][b];
                     for (size_t e = 0; e < nn; ++e) {
-                        dA[e + nn * (a + 3 * b)] = d.dA[a][b].v[e];
-                        W[e + nn * (a + 3 * b)] = d.ddH[a][b].v[e];
+                        dA[e + nn * (a + 3 * b)] = dab.v[e];
+                        W[e + nn * (a + 3 * b)] = wab.v[e];
                     }
+                }
+            }
+            if (d.nonorth) {
+                R.resize(nn * 3);
+                for (int a = 0; a < 3; ++a)
+                    for (size_t e = 0; e < nn; ++e) R[e + nn * a] = d.r[a].v[e];
             }
             ShgParams p;
             p.mu = t.fermi_energy; p.T = t.temperature; p.width = t.broadening;
@@ -1154,6 +1287,12 @@ void point_values(const Model &m, const Task &task, const double k[3], cd *out) 
             p.degeneracy = t.degeneracy_threshold;
             p.gaussian = t.broadening_type == WNLQG_GAUSSIAN;
             p.eta_correction = t.shg_eta_correction != 0;
+            if (d.nonorth) {
+                p.vertex_eta = t.denominator_regularization;
+                p.rdip = R.data();
+                p.hess = d.esd.data();
+                p.curv = d.iso.data();
+            }
             shg_response(n, d.E.data(), V.data(), A.data(), dA.data(), W.data(), nom, t.photon_energies, nc,
                          q.components, p, o);
             o += nom * nc * 14;
@@ -1218,11 +1357,22 @@ int64_t oracle_value_count(const wnlqg_task_desc *t) {
 // Per-point values: k[3*n] -> out[n*value_count] complex (interleaved).
 bool nonorth_kinds_ok(const Model &m, const wnlqg_task_desc *t) {
     if (!m.has_overlap) return true;
-    for (int r = 0; r < t->num_responses; ++r)
-        if (t->responses[r].kind != WNLQG_SHIFT_CURRENT && t->responses[r].kind != WNLQG_INJECTION_CURRENT) {
-            set_error("nonorthogonal models: shift and injection current only");
+    for (int r = 0; r < t->num_responses; ++r) {
+        const int kind = t->responses[r].kind;
+        if (kind == WNLQG_SECOND_HARMONIC) {
+            // Metric SHG preconditions (NonorthogonalMatrixElements.jl:1088-1110).
+            if (t->shg_eta_correction) { set_error("NONORTHOGONAL_SHG_ETA_CORRECTION_UNSUPPORTED"); return false; }
+            if (!(std::isfinite(t->denominator_regularization) && t->denominator_regularization > 0)) {
+                set_error("NONORTHOGONAL_SHG_POSITIVE_GEOMETRY_REQUIRED");
+                return false;
+            }
+            continue;
+        }
+        if (kind != WNLQG_SHIFT_CURRENT && kind != WNLQG_INJECTION_CURRENT) {
+            set_error("nonorthogonal models: shift current, injection current and second harmonic generation only");
             return false;
         }
+    }
     return true;
 }
 

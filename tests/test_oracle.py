@@ -271,3 +271,41 @@ def test_nonorthogonal_currents_equal_orthogonal(oracle_mod, eta, transform):
     a = oracle_mod.point_values(model, task, k)
     b = oracle_mod.point_values(other, task, k)
     assert np.max(np.abs(a - b)) <= 1e-10 * np.max(np.abs(a))
+
+
+@pytest.mark.parametrize("transform", ["identity", "constant"])
+@pytest.mark.parametrize("temperature", [0.0, 300.0])
+def test_metric_second_harmonic_equals_orthogonal(oracle_mod, transform, temperature):
+    """Metric SHG (normalized source jets of NonorthogonalOpticalCutoffVertices.jl:67-186, metric
+    Berry connection as r_eta, metric energy Hessians and isolated-band curvature,
+    SecondHarmonicKernels.jl:47-68) gives the orthogonal SHG tables when the overlap is the
+    identity and is invariant under a constant non-unitary basis change, all seven terms
+    (one-band terms at T > 0) and both quantities.  The geometry width is the SHG width here
+    (intermediate regularization 0 selects the denominator regularization)."""
+    model = synthetic_orthogonal_model(6, 1, seed=4, full_position=True)
+    rng = np.random.default_rng(9)
+    M = None if transform == "identity" else np.eye(6) + 0.2 * (rng.standard_normal((6, 6)) + 1j * rng.standard_normal((6, 6)))
+    other = _overlap_copy(model, M)
+    task = _abi.TaskArrays([(_abi.SECOND_HARMONIC, ["xxx", "xyy", "yzx", "zxz"])], broadening_type=_abi.LORENTZIAN,
+                           broadening=0.03, photon_energies=np.linspace(0.1, 2.0, 7), denominator_regularization=0.01,
+                           shg_intermediate_regularization=0.0, shg_eta_correction=False, temperature=temperature,
+                           fermi_energy=0.1)
+    k = np.random.default_rng(3).random((5, 3))
+    a = oracle_mod.point_values(model, task, k)
+    b = oracle_mod.point_values(other, task, k)
+    assert np.max(np.abs(a)) > 0
+    assert np.max(np.abs(a - b)) <= 1e-10 * np.max(np.abs(a))
+
+
+def test_metric_second_harmonic_preconditions(oracle_mod):
+    """Metric SHG needs a positive geometry width and no eta correction
+    (NonorthogonalMatrixElements.jl:1088-1110)."""
+    other = _overlap_copy(synthetic_orthogonal_model(4, 1, seed=1, full_position=True))
+    k = np.zeros((1, 3))
+    kw = dict(broadening=0.03, photon_energies=[0.5], shg_intermediate_regularization=0.01)
+    with pytest.raises(RuntimeError, match="ETA_CORRECTION_UNSUPPORTED"):
+        oracle_mod.point_values(other, _abi.TaskArrays([(_abi.SECOND_HARMONIC, ["xxx"])], denominator_regularization=0.01,
+                                                       shg_eta_correction=True, **kw), k)
+    with pytest.raises(RuntimeError, match="POSITIVE_GEOMETRY_REQUIRED"):
+        oracle_mod.point_values(other, _abi.TaskArrays([(_abi.SECOND_HARMONIC, ["xxx"])], denominator_regularization=0.0,
+                                                       shg_eta_correction=False, **kw), k)
