@@ -141,3 +141,92 @@ def test_shg_large_nw_matches_oracle(engine_cls, oracle_mod):
         got = task.split(eng.point_values(k))[0]
     ref = task.split(oracle_mod.point_values(model, task, k))[0]
     assert block_err(got, ref) < RTOL
+
+
+# ---- metric (nonorthogonal) SHG --------------------------------------------------------------
+
+def _overlap_model(model, M):
+    """The same model in a nonorthogonal basis: S = M^H M at R = 0, H' = M^H H M, A' = M^H A M."""
+    import copy
+    nw, nr = model.num_orbitals, model.num_r_vectors
+    out = copy.deepcopy(model)
+    home = int(np.where(np.all(model.r_vectors == 0, axis=0))[0][0])
+    S = np.zeros((nw, nw, nr), dtype=np.complex128, order="F")
+    S[:, :, home] = M.conj().T @ M
+    out.overlap_r = S
+    out.hamiltonian_r = np.asfortranarray(np.einsum("ji,jkr,kl->ilr", M.conj(), model.hamiltonian_r, M))
+    out.position_r = np.asfortranarray(np.einsum("ji,jkar,kl->ilar", M.conj(), model.position_r, M))
+    return out
+
+
+def metric_task(*, T=300.0, mu=0.1, components=COMPONENTS, omegas=(0.1, 0.6, 1.4)):
+    return _abi.TaskArrays([(_abi.SECOND_HARMONIC, components)], broadening_type=_abi.LORENTZIAN, broadening=0.03,
+                           photon_energies=omegas, fermi_energy=mu, temperature=T, degeneracy_threshold=0.002,
+                           shg_low_frequency_broadening=0.025, shg_intermediate_regularization=0.0,
+                           denominator_regularization=0.01, shg_eta_correction=False)
+
+
+@pytest.mark.parametrize("T", [0.0, 300.0])
+def test_metric_shg_matches_oracle(engine_cls, oracle_mod, T):
+    """Nonorthogonal model (constant non-unitary basis change of an orthogonal one): GPU metric SHG
+    (metric_shg_kernel + shg_kernel) against the oracle term by term, and equal to the orthogonal
+    model's SHG (basis invariance)."""
+    from wanniernlqg_b200.model import synthetic_orthogonal_model
+    base = synthetic_orthogonal_model(6, 1, seed=4, full_position=True)
+    rng = np.random.default_rng(9)
+    model = _overlap_model(base, np.eye(6) + 0.2 * (rng.standard_normal((6, 6)) + 1j * rng.standard_normal((6, 6))))
+    task = metric_task(T=T)
+    k = np.random.default_rng(5).random((6, 3))
+    with engine_cls(model, task) as eng:
+        got = eng.point_values(k)
+    with engine_cls(base, task) as eng:
+        orth = eng.point_values(k)
+    ref = oracle_mod.point_values(model, task, k)
+    g, r, o = task.split(got)[0], task.split(ref)[0], task.split(orth)[0]
+    assert block_err(g, r) < RTOL
+    assert block_err(g, o) < 1e-9
+
+
+def test_metric_shg_identity_overlap_mesh(engine_cls, oracle_mod):
+    """Identity overlap: the metric path's mesh integral equals the orthogonal path's and the oracle."""
+    from wanniernlqg_b200.model import synthetic_orthogonal_model
+    base = synthetic_orthogonal_model(5, 1, seed=6, full_position=True)
+    model = _overlap_model(base, np.eye(5))
+    task = metric_task(components=[(0, 0, 0), (1, 2, 2), (2, 0, 1)])
+    mesh = (4, 3, 3)
+    with engine_cls(model, task, max_batch=13) as eng:
+        got = eng.integrate_mesh(mesh)
+    with engine_cls(base, task) as eng:
+        orth = eng.integrate_mesh(mesh)
+    ref = oracle_mod.integrate_mesh(model, task, mesh)
+    assert block_err(task.split(got)[0], task.split(ref)[0]) < RTOL
+    assert block_err(task.split(got)[0], task.split(orth)[0]) < 1e-9
+
+
+def test_metric_shg_preconditions(engine_cls):
+    from wanniernlqg_b200._lib import EngineError
+    from wanniernlqg_b200.model import synthetic_orthogonal_model
+    model = _overlap_model(synthetic_orthogonal_model(4, 1, seed=1, full_position=True), np.eye(4))
+    bad_corr = _abi.TaskArrays([(_abi.SECOND_HARMONIC, [(0, 0, 0)])], broadening=0.03, photon_energies=[0.5],
+                               denominator_regularization=0.01, shg_intermediate_regularization=0.01,
+                               shg_eta_correction=True)
+    bad_eta = _abi.TaskArrays([(_abi.SECOND_HARMONIC, [(0, 0, 0)])], broadening=0.03, photon_energies=[0.5],
+                              denominator_regularization=0.0, shg_intermediate_regularization=0.01,
+                              shg_eta_correction=False)
+    for task, msg in ((bad_corr, "ETA_CORRECTION_UNSUPPORTED"), (bad_eta, "POSITIVE_GEOMETRY_REQUIRED")):
+        with pytest.raises(EngineError) as ei:
+            engine_cls(model, task)
+        assert ei.value.status == 1 and msg in str(ei.value)
+
+
+def test_metric_shg_nw64_matches_oracle(engine_cls, oracle_mod):
+    """64 orbitals with a k-dependent overlap S(R) (the SHG chi^xxx shape of the nonorthogonal
+    workload): metric inputs and the SHG kernel's global working set against the oracle."""
+    from wanniernlqg_b200.model import synthetic_nonorthogonal_model
+    model = synthetic_nonorthogonal_model(64, 1, seed=7, full_position=True)
+    task = metric_task(components=[(0, 0, 0), (1, 0, 1)], omegas=(0.4, 1.2), T=300.0, mu=0.0)
+    k = np.random.default_rng(8).random((2, 3))
+    with engine_cls(model, task) as eng:
+        got = eng.point_values(k)
+    ref = oracle_mod.point_values(model, task, k)
+    assert block_err(task.split(got)[0], task.split(ref)[0]) < RTOL

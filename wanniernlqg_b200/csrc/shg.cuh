@@ -57,6 +57,14 @@ struct ShgParams {
     int64_t scratch_stride;      // double2 entries per CTA
     unsigned char *gscratch;     // per-CTA matrix working set in global memory (large nw); nullptr: shared
     int64_t gscratch_stride;
+    // Metric (nonorthogonal) models: V, A, d2H, dA come as the normalized source jets of
+    // metric_shg_kernel (m_src, [27][nn] per point), the vertices take the geometry width
+    // vertex_eta, r_eta is the metric Berry connection, and the one-band Hessians and
+    // isolated-band curvatures are the metric ones (m_diag, [18][nw] per point).
+    int metric;
+    double vertex_eta;
+    const double2 *m_src;
+    const double *m_diag;
 };
 
 struct ShgSmem {
@@ -217,7 +225,12 @@ __global__ void __launch_bounds__(256) shg_kernel(ShgParams p) {
     // r0 = A + i D0 with D0_ij = dH_ij I0(E_j - E_i); r_eta with the regularised inverse.
     auto d0 = [&](int a, int i, int j) { return cscale(V(a, i, j), I0[i + nw * j]); };
     auto dip = [&](int a, int i, int j) { return cadd(A(a, i, j), cmuli(d0(a, i, j))); };
-    auto rdip = [&](int a, int i, int j) { return cadd(A(a, i, j), cmuli(cscale(V(a, i, j), Rg[i + nw * j]))); };
+    const double2 *msrc = nullptr;
+    const double *mdiag = nullptr;
+    auto rdip = [&](int a, int i, int j) {
+        if (p.metric) return msrc[(int64_t)(24 + a) * nn + i + nw * j];
+        return cadd(A(a, i, j), cmuli(cscale(V(a, i, j), Rg[i + nw * j])));
+    };
     auto gel = [&](int a, int b, int i, int j) { return G[(int64_t)(a + 3 * b) * nn + i + nw * j]; };
     const double eta = p.eta;
 
@@ -226,6 +239,10 @@ __global__ void __launch_bounds__(256) shg_kernel(ShgParams p) {
     for (int64_t b = kb; b < ke; ++b) {
         const double2 *xw = p.xw + b * p.xw_stride;
         const double wk = p.weights ? p.weights[b] * p.scale : p.scale;
+        if (p.metric) {
+            msrc = p.m_src + b * 27 * (int64_t)nn;
+            mdiag = p.m_diag + b * 18 * (int64_t)nw;
+        }
         for (int e = threadIdx.x; e < nn; e += blockDim.x) sU[(e % nw) + ld * (e / nw)] = p.U[b * nn + e];
         for (int i = threadIdx.x; i < nw; i += blockDim.x) {
             const double e = p.E[b * nw + i];
@@ -236,19 +253,37 @@ __global__ void __launch_bounds__(256) shg_kernel(ShgParams p) {
         for (int e = threadIdx.x; e < nn; e += blockDim.x) {
             const int i = e % nw, j = e / nw;
             I0[e] = shg_bare_inverse(sE[j] - sE[i]);
-            Rg[e] = reg_inverse(sE[j] - sE[i], eta);
+            Rg[e] = reg_inverse(sE[j] - sE[i], p.metric ? p.vertex_eta : eta);
             Wt[e] = shg_weight(sE[i] - sE[j], eta);
         }
-        for (int a = 0; a < 3; ++a) {
-            rotate_to_hamiltonian(xw + (int64_t)p.ch_dH[a] * nn, T1, T2, sU, sV + matsz * a, nw, ld);
-            rotate_to_hamiltonian(xw + (int64_t)p.ch_A[a] * nn, T1, T2, sU, sA + matsz * a, nw, ld);
+        if (p.metric) {
+            for (int e = threadIdx.x; e < 3 * nn; e += blockDim.x) {
+                const int a = e / nn, r = e % nn, o = (r % nw) + ld * (r / nw);
+                sV[matsz * a + o] = msrc[(int64_t)a * nn + r];
+                sA[matsz * a + o] = msrc[(int64_t)(3 + a) * nn + r];
+            }
+            __syncthreads();
+        } else {
+            for (int a = 0; a < 3; ++a) {
+                rotate_to_hamiltonian(xw + (int64_t)p.ch_dH[a] * nn, T1, T2, sU, sV + matsz * a, nw, ld);
+                rotate_to_hamiltonian(xw + (int64_t)p.ch_A[a] * nn, T1, T2, sU, sA + matsz * a, nw, ld);
+            }
         }
 
         // Stage 2: G^{ab} (optical_position_vertices!, OpticalPositionDerivatives.jl:36-89).
         for (int ab = 0; ab < 9; ++ab) {
             const int a = ab % 3, bb = ab / 3;
-            rotate_to_hamiltonian(xw + (int64_t)p.ch_ddH[a * 3 + bb] * nn, T1, T2, sU, X, nw, ld);
-            rotate_to_hamiltonian(xw + (int64_t)p.ch_dA[a * 3 + bb] * nn, T1, T2, sU, T1, nw, ld);
+            if (p.metric) {
+                for (int e = threadIdx.x; e < nn; e += blockDim.x) {
+                    const int o = (e % nw) + ld * (e / nw);
+                    X[o] = msrc[(int64_t)(6 + a * 3 + bb) * nn + e];
+                    T1[o] = msrc[(int64_t)(15 + a * 3 + bb) * nn + e];
+                }
+                __syncthreads();
+            } else {
+                rotate_to_hamiltonian(xw + (int64_t)p.ch_ddH[a * 3 + bb] * nn, T1, T2, sU, X, nw, ld);
+                rotate_to_hamiltonian(xw + (int64_t)p.ch_dA[a * 3 + bb] * nn, T1, T2, sU, T1, nw, ld);
+            }
             for (int n = threadIdx.x; n < nw; n += blockDim.x) {
                 ddHd[ab * nw + n] = X[n + ld * n];
                 dAd[ab * nw + n] = T1[n + ld * n];
@@ -414,7 +449,9 @@ __global__ void __launch_bounds__(256) shg_kernel(ShgParams p) {
                 double value = 0.0;
                 const bool isolated = (n == 0 || sE[n] - sE[n - 1] > p.degeneracy) &&
                                       (n == nw - 1 || sE[n + 1] - sE[n] > p.degeneracy);
-                if (a != bb && isolated && fabs(sE[n] - p.mu) <= 5.0 * kt) {
+                if (a != bb && isolated && fabs(sE[n] - p.mu) <= 5.0 * kt && p.metric) {
+                    value = mdiag[(9 + a * 3 + bb) * nw + n];
+                } else if (a != bb && isolated && fabs(sE[n] - p.mu) <= 5.0 * kt) {
                     double2 v = csub(dAd[(bb + 3 * a) * nw + n], dAd[(a + 3 * bb) * nw + n]);
                     for (int l = 0; l < nw; ++l) {
                         const double2 t = csub(cadd(csub(cmul(A(bb, n, l), d0(a, l, n)), cmul(d0(a, n, l), A(bb, l, n))),
@@ -438,9 +475,14 @@ __global__ void __launch_bounds__(256) shg_kernel(ShgParams p) {
                     const double sd = -offset / (kt * kt) * fd;
                     const bool isolated = (n == 0 || sE[n] - sE[n - 1] > p.degeneracy) &&
                                           (n == nw - 1 || sE[n + 1] - sE[n] > p.degeneracy);
-                    double hess = ddHd[(bb + 3 * cc) * nw + n].x;
-                    for (int l = 0; l < nw; ++l)
-                        if (l != n) hess += 2.0 * cmul(V(bb, n, l), V(cc, l, n)).x * shg_principal(sE[n] - sE[l], eta);
+                    double hess;
+                    if (p.metric) {
+                        hess = mdiag[(bb * 3 + cc) * nw + n];
+                    } else {
+                        hess = ddHd[(bb + 3 * cc) * nw + n].x;
+                        for (int l = 0; l < nw; ++l)
+                            if (l != n) hess += 2.0 * cmul(V(bb, n, l), V(cc, l, n)).x * shg_principal(sE[n] - sE[l], eta);
+                    }
                     const double va = V(a, n, n).x, vb = V(bb, n, n).x, vc = V(cc, n, n).x;
                     semi += sd * va * vb * vc + fd * va * hess;
                     if (isolated) bcd += fd * (vb * curv[n * 9 + a + 3 * cc] + vc * curv[n * 9 + a + 3 * bb]);

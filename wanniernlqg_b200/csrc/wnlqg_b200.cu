@@ -130,6 +130,13 @@ struct wnlqg_plan {
     double2 *d_ng_r = nullptr, *d_ng_G = nullptr;
     double *d_ng_v = nullptr;
     unsigned char *d_ng_ws = nullptr;
+    // Second harmonic generation of nonorthogonal models: metric inputs per batch point.
+    bool metric_shg = false;
+    MetricShgParams mshg;
+    int mshg_grid = 0;
+    double2 *d_mshg_src = nullptr;
+    double *d_mshg_diag = nullptr;
+    unsigned char *d_mshg_ws = nullptr;
     int refine_threads = 32;
     int sm_count = 148;
     size_t refine_smem = 0;
@@ -150,7 +157,7 @@ int find_channel(const std::vector<Channel> &chs, int op, int p, int d) {
 }
 
 int add_channel(std::vector<Channel> &chs, int op, int p, int d) {
-    if (op == CH_DDH && p > d) std::swap(p, d);
+    if ((op == CH_DDH || op == CH_DDS) && p > d) std::swap(p, d);   // symmetric second derivatives
     int idx = find_channel(chs, op, p, d);
     if (idx >= 0) return idx;
     chs.push_back(Channel{op, p, d});
@@ -811,7 +818,7 @@ wnlqg_status run_front(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const int64_
 
 wnlqg_status run_passes(wnlqg_plan *pl, int64_t nb, int mode, double scale, int64_t point_offset,
                         const double *weights = nullptr) {
-    if (pl->nonorth) {
+    if (pl->nonorth && !pl->passes.empty()) {
         NonorthParams q = pl->ng;
         q.batch = nb;
         q.xw = pl->d_xw;
@@ -847,9 +854,24 @@ wnlqg_status run_passes(wnlqg_plan *pl, int64_t nb, int mode, double scale, int6
                                     dim3(ps.grid), dim3(ps.threads), args, launch_smem, pl->stream));
         pl->launches += 1;
     }
+    if (pl->metric_shg && !pl->shg.empty()) {
+        MetricShgParams q = pl->mshg;
+        q.batch = nb;
+        q.xw = pl->d_xw;
+        q.E = pl->d_E;
+        q.U = pl->d_U;
+        metric_shg_kernel<<<(unsigned)std::min<int64_t>(nb, pl->mshg_grid), 256, 0, pl->stream>>>(q);
+        pl->launches += 1;
+    }
     for (const ShgParams &tmpl : pl->shg) {
         ShgParams p = tmpl;
         p.batch = nb;
+        if (pl->metric_shg) {
+            p.metric = 1;
+            p.vertex_eta = pl->task.denominator_regularization;
+            p.m_src = pl->d_mshg_src;
+            p.m_diag = pl->d_mshg_diag;
+        }
         p.xw = pl->d_xw;
         p.E = pl->d_E;
         p.U = pl->d_U;
@@ -973,7 +995,7 @@ wnlqg_status wnlqg_b200_plan_destroy(wnlqg_plan *pl) {
                       (void *)pl->d_shg_scratch, (void *)pl->d_tcA, (void *)pl->d_tcB, (void *)pl->d_tc_colscale,
                       (void *)pl->d_tc_err, (void *)pl->d_shg_gscratch, (void *)pl->d_eigh_scratch,
                       (void *)pl->d_resp_scratch, (void *)pl->d_ng_r, (void *)pl->d_ng_v, (void *)pl->d_ng_G,
-                      (void *)pl->d_ng_ws})
+                      (void *)pl->d_ng_ws, (void *)pl->d_mshg_src, (void *)pl->d_mshg_diag, (void *)pl->d_mshg_ws})
         if (ptr) cudaFree(ptr);
     for (cudaEvent_t ev : pl->events) cudaEventDestroy(ev);
     if (pl->stream) cudaStreamDestroy(pl->stream);
@@ -1034,9 +1056,19 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
             for (int i = 0; i < 4; ++i)
                 if (x[i] < 0 || x[i] > 2) return bail(fail(WNLQG_ERR_INVALID_ARGUMENT, "component axis out of range"));
             int a = x[0], b = x[1], cc = x[2];
-            if (model->has_overlap && q.kind != WNLQG_SHIFT_CURRENT && q.kind != WNLQG_INJECTION_CURRENT)
+            if (model->has_overlap && q.kind != WNLQG_SHIFT_CURRENT && q.kind != WNLQG_INJECTION_CURRENT &&
+                q.kind != WNLQG_SECOND_HARMONIC)
                 return bail(fail(WNLQG_ERR_UNSUPPORTED,
-                                 "nonorthogonal models: shift and injection current are built; other responses are not"));
+                                 "nonorthogonal models: shift current, injection current and second harmonic generation "
+                                 "are built; other responses are not"));
+            if (model->has_overlap && q.kind == WNLQG_SECOND_HARMONIC) {
+                // Metric SHG preconditions (NonorthogonalMatrixElements.jl:1088-1110).
+                if (t.shg_eta_correction)
+                    return bail(fail(WNLQG_ERR_INVALID_ARGUMENT, "NONORTHOGONAL_SHG_ETA_CORRECTION_UNSUPPORTED"));
+                if (!(std::isfinite(t.denominator_regularization) && t.denominator_regularization > 0))
+                    return bail(fail(WNLQG_ERR_INVALID_ARGUMENT, "NONORTHOGONAL_SHG_POSITIVE_GEOMETRY_REQUIRED"));
+                pl->metric_shg = true;
+            }
             switch (q.kind) {
             case WNLQG_SHIFT_CURRENT: {
                 need_r(a); need_r(b); need_r(cc);
@@ -1150,6 +1182,22 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
             }
             q.eta = t.denominator_regularization;
         }
+        if (pl->metric_shg) {
+            // Metric SHG: dH, dS, r on every axis and d2H, d2S, dr for every (axis, derivative).
+            MetricShgParams &ms = pl->mshg;
+            std::memset(&ms, 0, sizeof(ms));
+            for (int a = 0; a < 3; ++a) {
+                ms.ch_dH[a] = add_channel(ch, CH_DH, a, 0);
+                ms.ch_dS[a] = add_channel(ch, CH_DS, a, 0);
+                ms.ch_A[a] = add_channel(ch, CH_A, a, 0);
+                for (int bb = 0; bb < 3; ++bb) {
+                    ms.ch_ddH[a * 3 + bb] = add_channel(ch, CH_DDH, a, bb);
+                    ms.ch_ddS[a * 3 + bb] = add_channel(ch, CH_DDS, a, bb);
+                    ms.ch_dA[a * 3 + bb] = add_channel(ch, CH_DA, a, bb);
+                }
+            }
+            ms.eta = t.denominator_regularization;
+        }
     }
     pl->C = (int)ch.size();
 
@@ -1206,6 +1254,7 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
 
     if (max_batch <= 0) {
         int64_t per_k = (int64_t)pl->C * nn * 16 + (int64_t)nr * 16 + nn * 16 + nw * 8 + vc * 16;
+        if (pl->metric_shg) per_k += MetricShgWs::src_entries(nw) * 16 + MetricShgWs::diag_entries(nw) * 8;
         // About 4 GiB of batch workspace (HBM is 180 GB): long runs of neighbouring k-points per
         // CTA for the warm-started eigensolver and few batches per call.
         max_batch = std::max<int64_t>(256, std::min<int64_t>(1 << 20, ((int64_t)1 << 32) / per_k));
@@ -1247,6 +1296,22 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
         q.v_out = pl->d_ng_v;
         q.g_out = pl->d_ng_G;
         q.ws = pl->d_ng_ws;
+    }
+    if (pl->metric_shg) {
+        MetricShgParams &ms = pl->mshg;
+        ms.nw = nw;
+        ms.ld = nw + 1;
+        ms.xw_stride = (int64_t)pl->C * nn;
+        ms.ws_stride = (MetricShgWs::bytes(nw) + 255) & ~(int64_t)255;
+        pl->mshg_grid = l2_resident_grid(2 * sm_count, ms.ws_stride, sm_count);
+        if ((st = alloc((void **)&pl->d_mshg_src, (size_t)max_batch * MetricShgWs::src_entries(nw) * sizeof(double2))) != WNLQG_OK)
+            return bail(st);
+        if ((st = alloc((void **)&pl->d_mshg_diag, (size_t)max_batch * MetricShgWs::diag_entries(nw) * sizeof(double))) != WNLQG_OK)
+            return bail(st);
+        if ((st = alloc((void **)&pl->d_mshg_ws, (size_t)pl->mshg_grid * ms.ws_stride)) != WNLQG_OK) return bail(st);
+        ms.src = pl->d_mshg_src;
+        ms.diag = pl->d_mshg_diag;
+        ms.ws = pl->d_mshg_ws;
     }
     if ((st = alloc((void **)&pl->d_points, (size_t)max_batch * vc * sizeof(double2))) != WNLQG_OK) return bail(st);
     if ((st = alloc((void **)&pl->d_out, (size_t)vc * sizeof(double2))) != WNLQG_OK) return bail(st);

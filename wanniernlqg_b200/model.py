@@ -226,13 +226,13 @@ def synthetic_orthogonal_model(nw: int, rmax: int, seed: int = 0, *, full_positi
 
 
 def synthetic_nonorthogonal_model(nw: int, rmax: int, seed: int = 0, *, overlap_scale: float = 0.05,
-                                  min_overlap_eig: float = 0.5) -> TightBindingModel:
+                                  min_overlap_eig: float = 0.5, full_position: bool = False) -> TightBindingModel:
     """Orthogonal generator plus S(R) = delta_R0 I + overlap_scale*exp(-|R|)*CN, Hermitian-paired.
 
     The off-identity part is rescaled so that min over k of eig S(k) >= ``min_overlap_eig``
     (a bound from sum_R ||X(R)||_2, which bounds every ||X(k)||_2).
     """
-    base = synthetic_orthogonal_model(nw, rmax, seed)
+    base = synthetic_orthogonal_model(nw, rmax, seed, full_position=full_position)
     rng = np.random.default_rng(seed + 7919)
     rvecs = base.r_vectors
     x = _paired_gaussian(rng, nw, rvecs, lambda n: overlap_scale * np.exp(-n), zero_diag_value=np.zeros(nw))
