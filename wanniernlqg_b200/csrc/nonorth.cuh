@@ -216,6 +216,7 @@ __global__ void __launch_bounds__(256) metric_shg_kernel(MetricShgParams p) {
     __shared__ double sE[128];
     __shared__ double sv[3 * 128];
     __shared__ double2 rbd[9 * 128];
+    __shared__ double hdiag[9 * 128];   // diagonal of C^H d2H_ab C (symmetric in a, b)
     const double eta = p.eta;
     auto fgap = [&](double g) { return eta == 0.0 ? 1.0 / g : g / (g * g + eta * eta); };
     auto at = [&](double2 *M, int a) { return M + a * mat; };
@@ -252,12 +253,16 @@ __global__ void __launch_bounds__(256) metric_shg_kernel(MetricShgParams p) {
             const int a = ab / 3, bb = ab % 3;
             const double2 *ga = at(Gm, a), *gb = at(Gm, bb), *ka = at(K, a), *kbm = at(K, bb);
             const double2 *ra = at(Rw, a), *Db = at(D, bb);
-            ng_rotate(xw + (int64_t)p.ch_ddH[ab] * nn, nullptr, T1, T2, U, R2H, nw, ld);
+            // W_ab = W_ba (d2H, d2S and z are symmetric): for a > b only dA and the diagonals are new.
+            const bool wnew = a <= bb;
+            if (wnew) ng_rotate(xw + (int64_t)p.ch_ddH[ab] * nn, nullptr, T1, T2, U, R2H, nw, ld);
             ng_rotate(xw + (int64_t)p.ch_ddS[ab] * nn, nullptr, T1, T2, U, R2S, nw, ld);
             ng_rotate(xw + (int64_t)p.ch_dA[ab] * nn, xw + (int64_t)p.ch_ddS[ab] * nn, T1, T2, U, RB, nw, ld);
             // Energy Hessian diagonal and the B_a;b diagonal (before W and dA overwrite R2H, RB).
             for (int l = threadIdx.x; l < nw; l += blockDim.x) {
-                double2 hd = R2H[l + ld * l], sd = R2S[l + ld * l];
+                if (wnew) hdiag[ab * 128 + l] = R2H[l + ld * l].x;
+                double2 hd = make_double2(wnew ? R2H[l + ld * l].x : hdiag[(bb * 3 + a) * 128 + l], 0.0);
+                double2 sd = R2S[l + ld * l];
                 for (int q = 0; q < nw; ++q) {
                     const double2 dql = Db[q + ld * l];
                     hd = cfma(ka[l + ld * q], dql, cfmaconj(dql, ka[q + ld * l], hd));
@@ -275,13 +280,13 @@ __global__ void __launch_bounds__(256) metric_shg_kernel(MetricShgParams p) {
                 const double2 z = cadd(cscale(R2S[o], -0.5), cscale(cadd(P[o], Q[o]), 0.375));
                 Z[o] = z;
                 // W starts as C^H d2H C + (E_l + E_m) z; dA as C^H (dr + i d2S) C + i (z - g_b g_a / 4).
-                R2H[o] = cadd(R2H[o], cscale(z, sE[l] + sE[m]));
+                if (wnew) R2H[o] = cadd(R2H[o], cscale(z, sE[l] + sE[m]));
                 RB[o] = cadd(RB[o], cmuli(csub(z, cscale(Q[o], 0.25))));
             }
             __syncthreads();
             // W -= (g_a k_b + k_b g_a + g_b k_a + k_a g_b) / 2.
             const double2 *pairs[4][2] = {{ga, kbm}, {kbm, ga}, {gb, ka}, {ka, gb}};
-            for (int t = 0; t < 4; ++t) {
+            for (int t = 0; t < (wnew ? 4 : 0); ++t) {
                 mm_xy(pairs[t][0], pairs[t][1], P, nw, ld);
                 __syncthreads();
                 for (int e = threadIdx.x; e < nn; e += blockDim.x) {
@@ -291,7 +296,7 @@ __global__ void __launch_bounds__(256) metric_shg_kernel(MetricShgParams p) {
                 __syncthreads();
             }
             // W += (g_a (E g_b) + g_b (E g_a)) / 4.
-            for (int t = 0; t < 2; ++t) {
+            for (int t = 0; t < (wnew ? 2 : 0); ++t) {
                 const double2 *left = t == 0 ? ga : gb, *right = t == 0 ? gb : ga;
                 for (int e = threadIdx.x; e < nn; e += blockDim.x) {
                     const int l = e % nw, o = l + ld * (e / nw);
@@ -312,7 +317,7 @@ __global__ void __launch_bounds__(256) metric_shg_kernel(MetricShgParams p) {
             __syncthreads();
             for (int e = threadIdx.x; e < nn; e += blockDim.x) {
                 const int o = (e % nw) + ld * (e / nw);
-                src[(int64_t)(6 + ab) * nn + e] = R2H[o];
+                src[(int64_t)(6 + ab) * nn + e] = wnew ? R2H[o] : src[(int64_t)(6 + bb * 3 + a) * nn + e];
                 src[(int64_t)(15 + ab) * nn + e] = csub(RB[o], cscale(cadd(P[o], Q[o]), 0.5));
             }
             __syncthreads();

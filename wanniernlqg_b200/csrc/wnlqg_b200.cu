@@ -1303,7 +1303,7 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
         ms.ld = nw + 1;
         ms.xw_stride = (int64_t)pl->C * nn;
         ms.ws_stride = (MetricShgWs::bytes(nw) + 255) & ~(int64_t)255;
-        pl->mshg_grid = l2_resident_grid(2 * sm_count, ms.ws_stride, sm_count);
+        pl->mshg_grid = sm_count;   // one CTA per SM: its products reuse the working set from L1 / L2
         if ((st = alloc((void **)&pl->d_mshg_src, (size_t)max_batch * MetricShgWs::src_entries(nw) * sizeof(double2))) != WNLQG_OK)
             return bail(st);
         if ((st = alloc((void **)&pl->d_mshg_diag, (size_t)max_batch * MetricShgWs::diag_entries(nw) * sizeof(double))) != WNLQG_OK)
