@@ -600,3 +600,25 @@ def test_large_nw_mixed_precision_eigensolver_matches_cta_jacobi(engine_cls, nw,
     rtol = 1e-11 if precision == _abi.PRECISION_FP64 else MIXED_RTOL
     for g, r in zip(task.split(m), ref_task.split(m_ref)):
         assert rel_err(g, r) < rtol
+
+
+@pytest.mark.parametrize("nw", [1, 2, 3, 5])
+@pytest.mark.parametrize("precision", [_abi.PRECISION_FP64, _abi.PRECISION_MIXED])
+def test_small_orbital_counts_match_oracle(engine_cls, oracle_mod, nw, precision):
+    """One to five orbitals (odd counts padded to an even Jacobi size, single-band models with
+    no transitions): point values and the spectrum against the oracle."""
+    model = synthetic_orthogonal_model(nw, 1, seed=30 + nw, full_position=True)
+    task = _abi.TaskArrays([(_abi.SHIFT_CURRENT, ["xyy"]), (_abi.QUANTUM_METRIC, ["xx"]), (_abi.BERRY_CURVATURE, ["xy"])],
+                           broadening_type=_abi.LORENTZIAN, broadening=0.05, photon_energies=np.linspace(0, 3, 12),
+                           precision=precision)
+    k = np.random.default_rng(nw).random((5, 3))
+    with engine_cls(model, task) as eng:
+        got = eng.point_values(k)
+        e, _ = eng.spectrum(k)
+    ref = oracle_mod.point_values(model, task, k)
+    tol = RTOL if precision == _abi.PRECISION_FP64 else MIXED_RTOL
+    for g, r in zip(task.split(got), task.split(ref)):
+        assert rel_err(g, r) < tol
+    for i in range(k.shape[0]):
+        eo, _, _ = oracle_mod.kpoint_spectrum(model, k[i])
+        assert np.max(np.abs(e[i] - eo)) < 1e-6 * max(1.0, np.abs(eo).max())
