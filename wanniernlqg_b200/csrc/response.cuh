@@ -309,7 +309,8 @@ WNLQG_D bool any_within(double te, double half, const RespParams &p) {
 // Reciprocal of a Lorentzian denominator den >= w2 > 0.  FP32 path: the fast hardware quotient.
 // FP64 path: Newton-Raphson iteration r <- r (2 - den r) (quadratic convergence) seeded by the
 // PTX instruction rcp.approx.ftz.f64 (a hardware approximation), so that no FP64 <-> FP32
-// conversions are needed; three steps take any seed better than 2^-8 relative to FP64 rounding
+// conversions are needed.  The seed's relative error measured on B200 is at most 2^-19.96 (4M
+// denominators from 1e-10 to 1e4); two steps take any seed better than 2^-14 to FP64 rounding
 // (a few ulp).  The denominators are normal numbers (den >= w2 > 0), so flushing subnormals
 // changes nothing.
 WNLQG_D float lorentz_recip(float den) { return __fdividef(1.0f, den); }
@@ -317,8 +318,6 @@ WNLQG_D double lorentz_recip(double den) {
     double r;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(den));
     double e = fma(-den, r, 1.0);
-    r = fma(r, e, r);
-    e = fma(-den, r, 1.0);
     r = fma(r, e, r);
     e = fma(-den, r, 1.0);
     return fma(r, e, r);
