@@ -337,10 +337,10 @@ def main():
     # stream their inputs point by point, so traffic grows in proportion to the points.
     # The eigensolve stage is two kernels (FP32 Jacobi, FP64 refinement): their bytes are summed.
     traffic_per_k = {
-        ("fp64", "response"): (1.078567e9 + 5.804032e6) / 8192,     # response_kernel_fp64_nw32_mesh.md
-        ("fp64", "eigen"): (0.134364e9 + 35.584512e6 + 0.201415e9 + 99.751424e6) / 8192,
-        ("mixed", "response"): (1.082575e9 + 10.373376e6) / 8192,   # mixed_path_kernels_nw32_mesh.md
-        ("mixed", "eigen"): (0.134277e9 + 35.303168e6 + 0.201391e9 + 96.798464e6) / 8192,
+        ("fp64", "response"): (1.078604e9 + 4.801024e6) / 8192,     # response_kernel_fp64_nw32_mesh.md
+        ("fp64", "eigen"): (0.134277e9 + 35.683584e6 + 0.201497e9 + 97.044736e6) / 8192,
+        ("mixed", "response"): (1.082281e9 + 9.649408e6) / 8192,    # mixed_path_kernels_nw32_mesh.md
+        ("mixed", "eigen"): (0.134329e9 + 35.740160e6 + 0.201393e9 + 98.023680e6) / 8192,
         ("mixed", "fourier_random"): (436.281088e6 + 1.025739e9) / 8192,  # tc_fourier_kernel_nw32_random_k.md
     }
     prec_key = "fp64" if precision == _abi.PRECISION_FP64 else "mixed"
