@@ -115,6 +115,14 @@ typedef struct wnlqg_task_desc {
     int32_t band_window_size;               /* shift/injection pairs: bands around mu, widened to complete
                                                degeneracy groups (select_band_window, CalculationUtils.jl:71-90,
                                                TransitionScreening.jl:201-233); -1 = all bands */
+    /* Explicit interband selection (cfg.band_selection = (conduction, valence),
+       validate_interband_band_selection, CalculationUtils.jl:501-522; gate in _fill_transition_screen!,
+       TransitionScreening.jl:32-94): with use_band_selection = 1 a shift / injection pair (n, m) is kept
+       only if bit n of valence_bands and bit m of conduction_bands are set (0-based band indices, bit i
+       of word i / 32); both groups nonempty, disjoint and below num_orbitals; band_window_size must be -1. */
+    int32_t use_band_selection;
+    uint32_t valence_bands[4];
+    uint32_t conduction_bands[4];
 } wnlqg_task_desc;
 
 typedef struct wnlqg_model wnlqg_model;   /* device-resident model */

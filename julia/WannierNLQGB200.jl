@@ -51,6 +51,9 @@ struct TaskDesc
     shg_intermediate_regularization::Float64   # cfg.shg_intermediate_regularization (0: denominator_regularization)
     shg_eta_correction::Int32                  # cfg.shg_eta_correction
     band_window_size::Int32                    # cfg.band_window_size (-1: all bands)
+    use_band_selection::Int32                  # 1: cfg.band_selection = (conduction, valence) is set
+    valence_bands::NTuple{4, UInt32}           # bit (n - 1) for valence band n
+    conduction_bands::NTuple{4, UInt32}        # bit (m - 1) for conduction band m
 end
 
 function check(status)

@@ -731,7 +731,11 @@ void fill_screen(const std::vector<double> &E, const std::vector<double> &f,
             double od = f[a] - f[b];
             s.fnm[a + (size_t)n * b] = od;
             double te = E[b] - E[a];
-            bool occ = std::fabs(od) > 1.0e-10 && a >= wlo && a < whi && b >= wlo && b < whi;
+            // Explicit interband selection (_fill_transition_screen!, TransitionScreening.jl:57-61):
+            // source (valence) band a, target (conduction) band b.
+            const bool selected = !t.use_band_selection || (((t.valence_bands[a >> 5] >> (a & 31)) & 1u) &&
+                                                            ((t.conduction_bands[b >> 5] >> (b & 31)) & 1u));
+            bool occ = selected && std::fabs(od) > 1.0e-10 && a >= wlo && a < whi && b >= wlo && b < whi;
             bool pair_active = occ && !gaussian;
             if (occ && !gaussian && thr <= 0) s.active = true;
             for (int64_t w = 0; w < nom; ++w) {
@@ -762,6 +766,18 @@ struct Task {
 bool build_task(const wnlqg_task_desc *t, Task &task) {
     task.desc = *t;
     if (t->num_photon_energies < 0 || t->num_fermi_energies < 0) { set_error("negative axis length"); return false; }
+    if (t->use_band_selection) {
+        // validate_interband_band_selection (CalculationUtils.jl:501-522).
+        bool any_v = false, any_c = false, overlap = false;
+        for (int w = 0; w < 4; ++w) {
+            any_v |= t->valence_bands[w] != 0;
+            any_c |= t->conduction_bands[w] != 0;
+            overlap |= (t->valence_bands[w] & t->conduction_bands[w]) != 0;
+        }
+        if (!any_v || !any_c) { set_error("band_selection groups must be nonempty and inside the orbitals"); return false; }
+        if (overlap) { set_error("band_selection groups must not overlap"); return false; }
+        if (t->band_window_size != -1) { set_error("band_selection together with a band window is not built"); return false; }
+    }
     task.omegas.assign(t->photon_energies, t->photon_energies + t->num_photon_energies);
     if (t->num_fermi_energies > 0) task.mus.assign(t->fermi_energies, t->fermi_energies + t->num_fermi_energies);
     task.desc.photon_energies = task.omegas.data();

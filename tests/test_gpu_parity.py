@@ -622,3 +622,33 @@ def test_small_orbital_counts_match_oracle(engine_cls, oracle_mod, nw, precision
     for i in range(k.shape[0]):
         eo, _, _ = oracle_mod.kpoint_spectrum(model, k[i])
         assert np.max(np.abs(e[i] - eo)) < 1e-6 * max(1.0, np.abs(eo).max())
+
+
+@pytest.mark.parametrize("precision", [_abi.PRECISION_FP64, _abi.PRECISION_MIXED])
+def test_band_selection_matches_oracle(engine_cls, oracle_mod, precision):
+    """Explicit interband selection (conduction, valence groups, 1-based): point values and a mesh
+    against the oracle (transition threshold on, applied per selection as in the reference), and
+    the plan-time checks of the groups."""
+    from wanniernlqg_b200._lib import EngineError
+    model = reference_workload_model("nw32")
+    sel = ([17, 18, 19, 20, 22], [10, 12, 13, 14, 15, 16])
+    task = nw32_task(nom=48, precision=precision, band_selection=sel)
+    k = np.random.default_rng(19).random((8, 3))
+    mesh = (4, 3, 3)
+    with engine_cls(model, task) as eng:
+        got = eng.point_values(k)
+        got_mesh = eng.integrate_mesh(mesh)
+    ref = oracle_mod.point_values(model, task, k)
+    ref_mesh = oracle_mod.integrate_mesh(model, task, mesh)
+    tol = RTOL if precision == _abi.PRECISION_FP64 else MIXED_RTOL
+    for g, r in zip(task.split(got), task.split(ref)):
+        assert rel_err(g, r) < tol
+    for g, r in zip(task.split(got_mesh), task.split(ref_mesh)):
+        assert rel_err(g, r) < tol
+    for bad, status in ((([1, 2], [2, 3]), 1), (([40], [1]), 1)):
+        with pytest.raises(EngineError) as ei:
+            engine_cls(model, nw32_task(nom=8, band_selection=bad))
+        assert ei.value.status == status
+    with pytest.raises(EngineError) as ei:
+        engine_cls(model, nw32_task(nom=8, band_selection=([3], [1]), band_window_size=4))
+    assert ei.value.status == 6

@@ -309,3 +309,33 @@ def test_metric_second_harmonic_preconditions(oracle_mod):
     with pytest.raises(RuntimeError, match="POSITIVE_GEOMETRY_REQUIRED"):
         oracle_mod.point_values(other, _abi.TaskArrays([(_abi.SECOND_HARMONIC, ["xxx"])], denominator_regularization=0.0,
                                                        shg_eta_correction=False, **kw), k)
+
+
+def test_band_selection_partitions_add_up(oracle_mod):
+    """Explicit interband selection (valence n, conduction m): the shift and injection currents of
+    all valence x conduction group combinations of a band partition add up to the unselected
+    result.  The transition threshold is off (transition_window_factor = 0): with it, a point
+    counts only when a selected pair lies near a photon energy, which the reference applies per
+    selection, so blocks of a partition may drop Lorentzian tails that the full run keeps."""
+    model = synthetic_orthogonal_model(6, 1, seed=8, full_position=True)
+    kw = dict(broadening_type=_abi.LORENTZIAN, broadening=0.05, photon_energies=np.linspace(0, 3, 10),
+              transition_window_factor=0.0)
+    resp = [(_abi.SHIFT_CURRENT, ["xyy", "zxz"]), (_abi.INJECTION_CURRENT, ["xyy"])]
+    k = np.random.default_rng(2).random((4, 3))
+    full = oracle_mod.point_values(model, _abi.TaskArrays(resp, **kw), k)
+    groups = [[1, 2], [3, 4], [5, 6]]
+    total = np.zeros_like(full)
+    for v in groups:
+        for c in groups:
+            if v == c:
+                continue
+            total += oracle_mod.point_values(model, _abi.TaskArrays(resp, band_selection=(c, v), **kw), k)
+    # pairs inside one group: each group once as its own halves
+    for g in groups:
+        total += oracle_mod.point_values(model, _abi.TaskArrays(resp, band_selection=([g[1]], [g[0]]), **kw), k)
+        total += oracle_mod.point_values(model, _abi.TaskArrays(resp, band_selection=([g[0]], [g[1]]), **kw), k)
+    assert np.max(np.abs(total - full)) <= 1e-12 * np.max(np.abs(full))
+    with pytest.raises(RuntimeError, match="overlap"):
+        oracle_mod.point_values(model, _abi.TaskArrays(resp, band_selection=([1, 2], [2, 3]), **kw), k)
+    with pytest.raises(RuntimeError, match="band window"):
+        oracle_mod.point_values(model, _abi.TaskArrays(resp, band_selection=([1], [2]), band_window_size=2, **kw), k)

@@ -83,6 +83,9 @@ class TaskDesc(ctypes.Structure):
         ("shg_intermediate_regularization", ctypes.c_double),
         ("shg_eta_correction", ctypes.c_int32),
         ("band_window_size", ctypes.c_int32),
+        ("use_band_selection", ctypes.c_int32),
+        ("valence_bands", ctypes.c_uint32 * 4),
+        ("conduction_bands", ctypes.c_uint32 * 4),
     ]
 
 
@@ -135,7 +138,8 @@ class TaskArrays:
                  denominator_regularization=0.001, degeneracy_threshold=2.0e-3,
                  photon_energies=(0.10,), fermi_energies=(), precision=PRECISION_FP64,
                  fermi_surface_broadening=0.0, shg_low_frequency_broadening=0.025,
-                 shg_intermediate_regularization=0.0, shg_eta_correction=True, band_window_size=-1):
+                 shg_intermediate_regularization=0.0, shg_eta_correction=True, band_window_size=-1,
+                 band_selection=None):
         if not 1 <= len(responses) <= MAX_RESPONSES:
             raise ValueError("between 1 and 8 responses are supported per task")
         self.photon_energies = np.ascontiguousarray(np.asarray(photon_energies, dtype=np.float64))
@@ -174,6 +178,21 @@ class TaskArrays:
         d.shg_intermediate_regularization = float(shg_intermediate_regularization)
         d.shg_eta_correction = 1 if shg_eta_correction else 0
         d.band_window_size = int(band_window_size)
+        # band_selection = (conduction bands, valence bands), 1-based as in the reference's
+        # cfg.band_selection; pairs (n, m) with n valence and m conduction are kept.
+        if band_selection is not None:
+            conduction, valence = band_selection
+            d.use_band_selection = 1
+            for field, bands in (("conduction_bands", conduction), ("valence_bands", valence)):
+                words = [0, 0, 0, 0]
+                for band in bands:
+                    i = int(band) - 1
+                    if not 0 <= i < 128:
+                        raise ValueError(f"band {band} outside 1..128")
+                    words[i // 32] |= 1 << (i % 32)
+                arr = getattr(d, field)
+                for w in range(4):
+                    arr[w] = words[w]
         self.desc = d
 
     def value_count(self) -> int:

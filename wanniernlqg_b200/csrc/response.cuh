@@ -89,6 +89,8 @@ struct RespParams {
     int64_t gscratch_stride;
     // Shift/injection band window (-1: all bands) and the response degeneracy threshold.
     int band_window;
+    int use_sel;                         // explicit interband selection (valence n, conduction m)
+    unsigned vsel[4], csel[4];
     double degeneracy_threshold;
     // Nonorthogonal models: per-k geometry precomputed by nonorth_geometry_kernel (Berry
     // connection r [batch][3][nn], Hellmann-Feynman slopes v [batch][3][nw], generalized
@@ -738,7 +740,9 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 1 : 2) response_kernel(R
                     n = e % nw; m = e / nw;
                     fnm = sf[n] - sf[m];
                     te = sE[m] - sE[n];
-                    if (fabs(fnm) > 1.0e-10 && n >= wlo && n < whi && m >= wlo && m < whi) {
+                    const bool selected = !p.use_sel || (((p.vsel[n >> 5] >> (n & 31)) & 1u) &&
+                                                         ((p.csel[m >> 5] >> (m & 31)) & 1u));
+                    if (selected && fabs(fnm) > 1.0e-10 && n >= wlo && n < whi && m >= wlo && m < whi) {
                         if (p.gaussian) {
                             keep = any_within(te, p.cutoff, p);
                             if (keep) ired[1] = 1;

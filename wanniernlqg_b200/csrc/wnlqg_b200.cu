@@ -412,6 +412,8 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
         p.om_hi = sorted.empty() ? 0.0 : sorted.back();
         p.eta_reg = t.denominator_regularization;
         p.band_window = t.band_window_size;
+        p.use_sel = t.use_band_selection ? 1 : 0;
+        for (int w = 0; w < 4; ++w) { p.vsel[w] = t.valence_bands[w]; p.csel[w] = t.conduction_bands[w]; }
         p.degeneracy_threshold = t.degeneracy_threshold;
         p.vc = pl->vc;
         p.xw_stride = (int64_t)pl->C * pl->nn;
@@ -1026,6 +1028,23 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
         return fail(WNLQG_ERR_INVALID_ARGUMENT, "unknown precision");
     if (t.band_window_size < -1 || t.band_window_size == 0)
         return fail(WNLQG_ERR_INVALID_ARGUMENT, "band_window_size must be -1 or positive");
+    if (t.use_band_selection) {
+        // validate_interband_band_selection (CalculationUtils.jl:501-522): two nonempty, disjoint
+        // groups inside the orbitals.
+        bool any_v = false, any_c = false, overlap = false, outside = false;
+        for (int w = 0; w < 4; ++w) {
+            any_v |= t.valence_bands[w] != 0;
+            any_c |= t.conduction_bands[w] != 0;
+            overlap |= (t.valence_bands[w] & t.conduction_bands[w]) != 0;
+            for (int bit = 0; bit < 32; ++bit)
+                if (32 * w + bit >= model->nw && (((t.valence_bands[w] | t.conduction_bands[w]) >> bit) & 1u)) outside = true;
+        }
+        if (!any_v || !any_c || outside)
+            return fail(WNLQG_ERR_INVALID_ARGUMENT, "band_selection groups must be nonempty and inside the orbitals");
+        if (overlap) return fail(WNLQG_ERR_INVALID_ARGUMENT, "band_selection groups must not overlap");
+        if (t.band_window_size != -1)
+            return fail(WNLQG_ERR_UNSUPPORTED, "band_selection together with a band window is not built");
+    }
     WNLQG_CUDA(cudaSetDevice(model->device));
 
     wnlqg_plan *pl = new wnlqg_plan();
