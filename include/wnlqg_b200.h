@@ -123,6 +123,11 @@ typedef struct wnlqg_task_desc {
     int32_t use_band_selection;
     uint32_t valence_bands[4];
     uint32_t conduction_bands[4];
+    /* Wannier-center convention (WannierCenterConventionTransforms.jl:1-130): 0 = Convention II
+       (reference default), 1 = Convention I: centres tau = Re diag A(R = 0), derivative factors
+       R + tau_j - tau_i, home-cell connection A - tau, and the similarity D(k) = diag(exp(2 pi i
+       k.tau_frac)); orthogonal models only. */
+    int32_t wannier_center_convention;
 } wnlqg_task_desc;
 
 typedef struct wnlqg_model wnlqg_model;   /* device-resident model */

@@ -54,6 +54,7 @@ struct TaskDesc
     use_band_selection::Int32                  # 1: cfg.band_selection = (conduction, valence) is set
     valence_bands::NTuple{4, UInt32}           # bit (n - 1) for valence band n
     conduction_bands::NTuple{4, UInt32}        # bit (m - 1) for conduction band m
+    wannier_center_convention::Int32           # 0: CONVENTION_II, 1: CONVENTION_I
 end
 
 function check(status)

@@ -40,7 +40,7 @@ def lib():
                                           ctypes.c_int64, ctypes.c_int, dp]
         L.oracle_integrate_mesh.argtypes = [ctypes.POINTER(_abi.ModelDesc), ctypes.POINTER(_abi.TaskDesc), ip,
                                             ctypes.c_int64, ctypes.c_int64, ctypes.c_int, dp]
-        L.oracle_kpoint_spectrum.argtypes = [ctypes.POINTER(_abi.ModelDesc), dp, dp, dp, dp]
+        L.oracle_kpoint_spectrum.argtypes = [ctypes.POINTER(_abi.ModelDesc), dp, ctypes.c_int, dp, dp, dp]
         L.oracle_hermitian_eigen.argtypes = [ctypes.c_int64, dp, dp, dp]
         L.oracle_generalized_eigen.argtypes = [ctypes.c_int64, dp, dp, dp, dp]
         L.oracle_generalized_eigen.restype = ctypes.c_int
@@ -94,15 +94,17 @@ def integrate_mesh(model: TightBindingModel, task: _abi.TaskArrays, mesh, k_begi
     return out
 
 
-def kpoint_spectrum(model: TightBindingModel, k):
-    """(energies[nw], canonical U[nw, nw], Hamiltonian-gauge dH[nw, nw, 3]) at one k."""
+def kpoint_spectrum(model: TightBindingModel, k, convention: str = "II"):
+    """(energies[nw], canonical U[nw, nw], Hamiltonian-gauge dH[nw, nw, 3]) at one k, in the
+    given Wannier-center convention ("II" or "I")."""
     nw = model.num_orbitals
     m = _abi.ModelArrays(model)
     kk = np.ascontiguousarray(np.asarray(k, dtype=np.float64))
     e = np.zeros(nw)
     u = np.zeros((nw, nw), dtype=np.complex128, order="F")
     dh = np.zeros((nw, nw, 3), dtype=np.complex128, order="F")
-    _check(lib().oracle_kpoint_spectrum(ctypes.byref(m.desc), _dp(kk), _dp(e), _dp(u), _dp(dh)))
+    _check(lib().oracle_kpoint_spectrum(ctypes.byref(m.desc), _dp(kk), 1 if convention == "I" else 0, _dp(e), _dp(u),
+                                        _dp(dh)))
     return e, u, dh
 
 

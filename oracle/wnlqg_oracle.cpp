@@ -77,6 +77,10 @@ struct Model {
     std::vector<cd> S;            // [nw*nw*NR] overlap (nonorthogonal models)
     bool has_position = false;
     bool has_overlap = false;
+    // Convention I centres (_initialize_wannier_center_scratch!, WannierCenterConventionTransforms.jl:15-56).
+    int home = -1;
+    std::string centers_error;           // empty: centres valid
+    std::vector<double> tau_cart, tau_frac;   // [3 * nw], index a * nw + i
 };
 
 // Which Cartesian channels a task needs (the reference's MatrixElementPlan direction
@@ -88,6 +92,7 @@ struct Needs {
     bool dA[3][3] = {};   // [position][derivative]
     bool F[3][3] = {};
     bool shg = false;     // second harmonic generation (metric models: the source jets below)
+    int convention = 0;   // 0: Convention II, 1: Convention I
     void need_r(int a) { A[a] = true; dH[a] = true; }
     void need_gder(int p, int d) {   // r^p_{nm;d}
         dA[p][d] = true; ddH[p][d] = true; ddH[d][p] = true;
@@ -308,6 +313,7 @@ void compute_kpoint(const Model &m, const Needs &need, const double k[3], double
         double phase = (double)r[0] * k[0] + (double)r[1] * k[1] + (double)r[2] * k[2];
         f[ir] = std::polar(1.0, 2.0 * PI * phase) / (double)m.deg[ir];
     }
+    const bool conv1 = need.convention == 1;
     Mat Hw; Hw.init(n);
     Mat dHw[3], ddHw[3][3], Aw[3], dAw[3][3];
     bool needAw[3];
@@ -328,6 +334,14 @@ void compute_kpoint(const Model &m, const Needs &need, const double k[3], double
         }
     }
     // Direct sums in R order (HamiltonianMatrixElements.jl:42-58, 428-460; PositionMatrixElements.jl:294-332).
+    // Convention I: per-element displacement R + tau_j - tau_i (_convention_displacement_component,
+    // WannierCenterConventionTransforms.jl:85-96) and the centred home-cell connection A - tau
+    // (_convention_position_value, :99-113).
+    auto disp = [&](const double rc[3], int a, size_t e) {
+        if (!conv1) return rc[a];
+        const int i = (int)(e % n), j = (int)(e / n);
+        return rc[a] + m.tau_cart[a * n + j] - m.tau_cart[a * n + i];
+    };
     for (int ir = 0; ir < m.nr; ++ir) {
         double rc[3];
         r_cartesian(m, ir, rc);
@@ -339,21 +353,43 @@ void compute_kpoint(const Model &m, const Needs &need, const double k[3], double
         }
         for (int a = 0; a < 3; ++a) {
             if (need.dH[a]) {
-                for (size_t e = 0; e < nn; ++e) dHw[a].v[e] += fr * (I1 * rc[a] * h[e]);
+                for (size_t e = 0; e < nn; ++e) dHw[a].v[e] += fr * (I1 * disp(rc, a, e) * h[e]);
             }
             for (int b = 0; b < 3; ++b)
                 if (need.ddH[a][b])
-                    for (size_t e = 0; e < nn; ++e) ddHw[a][b].v[e] += fr * (-rc[a] * rc[b] * h[e]);
+                    for (size_t e = 0; e < nn; ++e) ddHw[a][b].v[e] += fr * (-disp(rc, a, e) * disp(rc, b, e) * h[e]);
         }
         if (m.has_position) {
             for (int a = 0; a < 3; ++a) {
                 const cd *pa = &m.A[nn * (a + 3 * (size_t)ir)];
+                auto pos = [&](size_t e) {
+                    cd v = pa[e];
+                    if (conv1 && ir == m.home && e % n == e / n) v -= m.tau_cart[a * n + (int)(e % n)];
+                    return v;
+                };
                 if (needAw[a])
-                    for (size_t e = 0; e < nn; ++e) Aw[a].v[e] += fr * pa[e];
+                    for (size_t e = 0; e < nn; ++e) Aw[a].v[e] += fr * pos(e);
                 for (int b = 0; b < 3; ++b)
                     if (needdAw[a][b])
-                        for (size_t e = 0; e < nn; ++e) dAw[a][b].v[e] += fr * (I1 * rc[b] * pa[e]);
+                        for (size_t e = 0; e < nn; ++e) dAw[a][b].v[e] += fr * (I1 * disp(rc, b, e) * pos(e));
             }
+        }
+    }
+    if (conv1) {
+        // D(k)^H X D(k), D = diag(exp(2 pi i k.tau_frac)) (_apply_wannier_center_similarity!, :68-81).
+        std::vector<cd> phi(n);
+        for (int i = 0; i < n; ++i)
+            phi[i] = std::polar(1.0, 2.0 * PI * (k[0] * m.tau_frac[i] + k[1] * m.tau_frac[n + i] + k[2] * m.tau_frac[2 * n + i]));
+        auto sim = [&](Mat &X) {
+            if (X.n != n) return;
+            for (int j = 0; j < n; ++j)
+                for (int i = 0; i < n; ++i) X(i, j) *= std::conj(phi[i]) * phi[j];
+        };
+        sim(Hw);
+        for (int a = 0; a < 3; ++a) {
+            sim(dHw[a]);
+            sim(Aw[a]);
+            for (int b = 0; b < 3; ++b) { sim(ddHw[a][b]); sim(dAw[a][b]); }
         }
     }
     std::vector<double> ev;
@@ -766,6 +802,11 @@ struct Task {
 bool build_task(const wnlqg_task_desc *t, Task &task) {
     task.desc = *t;
     if (t->num_photon_energies < 0 || t->num_fermi_energies < 0) { set_error("negative axis length"); return false; }
+    if (t->wannier_center_convention != 0 && t->wannier_center_convention != 1) {
+        set_error("wannier_center_convention must be 0 (II) or 1 (I)");
+        return false;
+    }
+    task.need.convention = t->wannier_center_convention;
     if (t->use_band_selection) {
         // validate_interband_band_selection (CalculationUtils.jl:501-522).
         bool any_v = false, any_c = false, overlap = false;
@@ -1355,6 +1396,43 @@ bool build_model(const wnlqg_model_desc *desc, Model &m) {
     }
     for (auto &z : m.H) if (!std::isfinite(z.real()) || !std::isfinite(z.imag())) { set_error("hamiltonian_r contains non-finite values"); return false; }
     for (int64_t g : m.deg) if (g <= 0) { set_error("r_degeneracies must be positive"); return false; }
+    // Convention I centres: tau = Re diag A(R = 0) and its fractional coordinates.
+    int homes = 0;
+    for (int r = 0; r < m.nr; ++r)
+        if (m.rvec[3 * (size_t)r] == 0 && m.rvec[3 * (size_t)r + 1] == 0 && m.rvec[3 * (size_t)r + 2] == 0) { m.home = r; ++homes; }
+    m.tau_cart.assign(3 * (size_t)m.nw, 0.0);
+    m.tau_frac.assign(3 * (size_t)m.nw, 0.0);
+    if (homes != 1) {
+        m.centers_error = homes == 0 ? "Convention_I requires one R=(0,0,0) position block in the TB model."
+                                     : "TB model contains more than one R=(0,0,0) block.";
+    } else {
+        for (int i = 0; i < m.nw && m.centers_error.empty(); ++i)
+            for (int a = 0; a < 3; ++a) {
+                const cd v = m.has_position ? m.A[nn * (a + 3 * (size_t)m.home) + i + (size_t)m.nw * i] : cd(0.0, 0.0);
+                if (!std::isfinite(v.real()) || !std::isfinite(v.imag())) { m.centers_error = "Convention_I Wannier center is non-finite"; break; }
+                if (std::fabs(v.imag()) > 1.0e-10) { m.centers_error = "Convention_I Wannier center has an imaginary part"; break; }
+                m.tau_cart[a * m.nw + i] = v.real();
+            }
+        // tau_cart[j] = sum_r tau_frac[r] * lattice[r + 3 j]: Gaussian elimination with pivoting.
+        for (int i = 0; i < m.nw; ++i) {
+            double M[3][4];
+            for (int j = 0; j < 3; ++j) {
+                for (int r = 0; r < 3; ++r) M[j][r] = m.lattice[r + 3 * j];
+                M[j][3] = m.tau_cart[j * m.nw + i];
+            }
+            for (int c = 0; c < 3; ++c) {
+                int piv = c;
+                for (int r = c + 1; r < 3; ++r) if (std::fabs(M[r][c]) > std::fabs(M[piv][c])) piv = r;
+                for (int q = 0; q < 4; ++q) std::swap(M[c][q], M[piv][q]);
+                for (int r = 0; r < 3; ++r) {
+                    if (r == c || M[c][c] == 0.0) continue;
+                    const double fct = M[r][c] / M[c][c];
+                    for (int q = 0; q < 4; ++q) M[r][q] -= fct * M[c][q];
+                }
+            }
+            for (int c = 0; c < 3; ++c) m.tau_frac[c * m.nw + i] = M[c][3] / M[c][c];
+        }
+    }
     return true;
 }
 
@@ -1372,6 +1450,10 @@ int64_t oracle_value_count(const wnlqg_task_desc *t) {
 
 // Per-point values: k[3*n] -> out[n*value_count] complex (interleaved).
 bool nonorth_kinds_ok(const Model &m, const wnlqg_task_desc *t) {
+    if (t->wannier_center_convention == 1) {
+        if (m.has_overlap) { set_error("Convention I with an overlap is not built"); return false; }
+        if (!m.centers_error.empty()) { set_error(m.centers_error); return false; }
+    }
     if (!m.has_overlap) return true;
     for (int r = 0; r < t->num_responses; ++r) {
         const int kind = t->responses[r].kind;
@@ -1451,10 +1533,14 @@ int oracle_integrate_mesh(const wnlqg_model_desc *md, const wnlqg_task_desc *td,
 
 // Band data at one k for tests: energies[nw], U[nw*nw] (canonical, column-major complex),
 // and the Hamiltonian-gauge velocity matrices dH[a] (complex [nw,nw,3]).
-int oracle_kpoint_spectrum(const wnlqg_model_desc *md, const double k[3], double *energies,
+int oracle_kpoint_spectrum(const wnlqg_model_desc *md, const double k[3], int convention, double *energies,
                            double *eigenvectors, double *dh) {
     Model m;
     if (!build_model(md, m)) return WNLQG_ERR_INVALID_ARGUMENT;
+    if (convention == 1 && (m.has_overlap || !m.centers_error.empty())) {
+        set_error(m.has_overlap ? "Convention I with an overlap is not built" : m.centers_error);
+        return WNLQG_ERR_INVALID_ARGUMENT;
+    }
     if (m.has_overlap) {
         // Nonorthogonal spectrum: H(k), S(k) by the direct sums, then the generalised eigensolve.
         const size_t nn = (size_t)m.nw * m.nw;
@@ -1476,6 +1562,7 @@ int oracle_kpoint_spectrum(const wnlqg_model_desc *md, const double k[3], double
     }
     Needs need;
     for (int a = 0; a < 3; ++a) need.dH[a] = true;
+    need.convention = convention;
     KData d;
     compute_kpoint(m, need, k, 0.001, d);
     size_t nn = (size_t)m.nw * m.nw;

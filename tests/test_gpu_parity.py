@@ -652,3 +652,43 @@ def test_band_selection_matches_oracle(engine_cls, oracle_mod, precision):
     with pytest.raises(EngineError) as ei:
         engine_cls(model, nw32_task(nom=8, band_selection=([3], [1]), band_window_size=4))
     assert ei.value.status == 6
+
+
+def test_convention_one_matches_oracle(engine_cls, oracle_mod):
+    """Wannier-center Convention I (centred connection, R + tau_j - tau_i displacement tiles; the
+    D(k) similarity cancels in the band frame and is applied to the returned eigenvectors):
+    point values, a mesh and canonical eigenvectors against the oracle on a non-cubic lattice;
+    models without an R = 0 block and models with an overlap are rejected."""
+    import copy
+    from wanniernlqg_b200._lib import EngineError
+    from wanniernlqg_b200.model import synthetic_nonorthogonal_model
+    model = copy.deepcopy(synthetic_orthogonal_model(6, 1, seed=14, full_position=True))
+    model.lattice = np.asfortranarray(np.array([[3.1, 0.0, 0.0], [0.9, 2.7, 0.0], [0.4, 0.6, 3.5]]))
+    resp = [(_abi.SHIFT_CURRENT, ["xyy", "zxz"]), (_abi.INJECTION_CURRENT, ["xyy"]),
+            (_abi.BERRY_CURVATURE, ["xy"]), (_abi.QUANTUM_METRIC, ["xz"]), (_abi.SECOND_HARMONIC, [(0, 1, 1)])]
+    task = _abi.TaskArrays(resp, broadening_type=_abi.LORENTZIAN, broadening=0.05, photon_energies=np.linspace(0.1, 2.5, 8),
+                           wannier_center_convention="I", shg_intermediate_regularization=0.04)
+    k = np.random.default_rng(21).random((6, 3))
+    mesh = (4, 3, 3)
+    with engine_cls(model, task) as eng:
+        got = eng.point_values(k)
+        got_mesh = eng.integrate_mesh(mesh)
+        _, u = eng.spectrum(k)
+    ref = oracle_mod.point_values(model, task, k)
+    ref_mesh = oracle_mod.integrate_mesh(model, task, mesh)
+    for g, r in zip(task.split(got), task.split(ref)):
+        assert rel_err(g, r) < RTOL
+    for g, r in zip(task.split(got_mesh), task.split(ref_mesh)):
+        assert rel_err(g, r) < RTOL
+    for i in range(k.shape[0]):
+        _, uo, _ = oracle_mod.kpoint_spectrum(model, k[i], "I")
+        assert np.max(np.abs(u[i] - uo)) < 1e-9
+    shifted = copy.deepcopy(model)
+    shifted.r_vectors = np.asfortranarray(shifted.r_vectors + np.array([[5], [0], [0]]))
+    with pytest.raises(EngineError) as ei:
+        engine_cls(shifted, task)
+    assert ei.value.status == 1
+    with pytest.raises(EngineError) as ei:
+        engine_cls(synthetic_nonorthogonal_model(4, 1, seed=2),
+                   _abi.TaskArrays([(_abi.SHIFT_CURRENT, ["xyy"])], wannier_center_convention="I"))
+    assert ei.value.status == 6

@@ -339,3 +339,62 @@ def test_band_selection_partitions_add_up(oracle_mod):
         oracle_mod.point_values(model, _abi.TaskArrays(resp, band_selection=([1, 2], [2, 3]), **kw), k)
     with pytest.raises(RuntimeError, match="band window"):
         oracle_mod.point_values(model, _abi.TaskArrays(resp, band_selection=([1], [2]), band_window_size=2, **kw), k)
+
+
+def _lattice_model(full_position, seed=12, nw=5):
+    """A synthetic model on a non-cubic lattice (so that fractional and Cartesian centres differ)."""
+    import copy
+    model = copy.deepcopy(synthetic_orthogonal_model(nw, 1, seed=seed, full_position=full_position))
+    model.lattice = np.asfortranarray(np.array([[3.1, 0.0, 0.0], [0.9, 2.7, 0.0], [0.4, 0.6, 3.5]]))
+    return model
+
+
+def test_convention_one_is_a_gauge_transform_of_convention_two(oracle_mod):
+    """Convention I (centred connection, R + tau_j - tau_i displacements, D(k) similarity,
+    WannierCenterConventionTransforms.jl) is a k-dependent diagonal gauge transform of Convention
+    II: with the complete position operator and bare inverses (eta = 0) the shift and injection
+    currents, Berry curvature and quantum metric agree; the eigenvalues agree and each Convention I
+    eigenvector is D(k)^H times the Convention II one up to its canonical phase."""
+    model = _lattice_model(True)
+    resp = [(_abi.SHIFT_CURRENT, ["xyy", "zxz"]), (_abi.INJECTION_CURRENT, ["xyy"]),
+            (_abi.BERRY_CURVATURE, ["xy", "yz"]), (_abi.QUANTUM_METRIC, ["xx", "xz"])]
+    kw = dict(broadening_type=_abi.LORENTZIAN, broadening=0.05, photon_energies=np.linspace(0, 3, 10),
+              denominator_regularization=0.0)
+    k = np.random.default_rng(3).random((4, 3))
+    two = oracle_mod.point_values(model, _abi.TaskArrays(resp, **kw), k)
+    one = oracle_mod.point_values(model, _abi.TaskArrays(resp, wannier_center_convention="I", **kw), k)
+    for a, b in zip(_abi.TaskArrays(resp, **kw).split(two), _abi.TaskArrays(resp, **kw).split(one)):
+        assert np.max(np.abs(a - b)) <= 1e-9 * np.max(np.abs(a))
+    tau = np.real(np.array([np.diag(model.position_r[:, :, x, 13]) for x in range(3)]))   # R = 0 is index 13 of the cube
+    assert np.all(model.r_vectors[:, 13] == 0)
+    frac = np.linalg.solve(model.lattice.T, tau)          # tau_cart[j] = sum_r frac_r lattice[r, j]
+    for kp in k:
+        e2, u2, _ = oracle_mod.kpoint_spectrum(model, kp, "II")
+        e1, u1, _ = oracle_mod.kpoint_spectrum(model, kp, "I")
+        assert np.max(np.abs(e1 - e2)) < 1e-12
+        d = np.exp(2j * np.pi * (kp @ frac))
+        ov = np.abs(np.sum(u1.conj() * (d.conj()[:, None] * u2), axis=0))
+        assert np.max(np.abs(ov - 1.0)) < 1e-10
+        piv = np.argmax(np.abs(u1), axis=0)
+        assert np.all(np.abs(u1[piv, np.arange(u1.shape[1])].imag) < 1e-12)
+
+
+def test_convention_one_with_diagonal_positions_and_home_cell_check(oracle_mod):
+    """With only the centres on the home-cell diagonal (tight-binding positions) Convention I is
+    still a gauge transform of Convention II: the centre terms of r = A + i D cancel exactly with
+    bare inverses (eta = 0) and up to the regularization with eta > 0.  A model without an R = 0
+    block is rejected under Convention I."""
+    import copy
+    model = _lattice_model(False)
+    resp = [(_abi.SHIFT_CURRENT, ["xyy"]), (_abi.INJECTION_CURRENT, ["zxz"])]
+    kw = dict(broadening_type=_abi.LORENTZIAN, broadening=0.05, photon_energies=np.linspace(0.5, 2.5, 6))
+    k = np.random.default_rng(4).random((3, 3))
+    for eta, tol in ((0.0, 1e-9), (0.001, 1e-5)):
+        two = oracle_mod.point_values(model, _abi.TaskArrays(resp, denominator_regularization=eta, **kw), k)
+        one = oracle_mod.point_values(model, _abi.TaskArrays(resp, denominator_regularization=eta,
+                                                             wannier_center_convention="I", **kw), k)
+        assert np.max(np.abs(one - two)) <= tol * np.max(np.abs(two))
+    shifted = copy.deepcopy(model)
+    shifted.r_vectors = np.asfortranarray(shifted.r_vectors + np.array([[5], [0], [0]]))
+    with pytest.raises(RuntimeError, match="R=\\(0,0,0\\)"):
+        oracle_mod.point_values(shifted, _abi.TaskArrays(resp, wannier_center_convention="I", **kw), k)

@@ -86,6 +86,7 @@ class TaskDesc(ctypes.Structure):
         ("use_band_selection", ctypes.c_int32),
         ("valence_bands", ctypes.c_uint32 * 4),
         ("conduction_bands", ctypes.c_uint32 * 4),
+        ("wannier_center_convention", ctypes.c_int32),
     ]
 
 
@@ -139,7 +140,7 @@ class TaskArrays:
                  photon_energies=(0.10,), fermi_energies=(), precision=PRECISION_FP64,
                  fermi_surface_broadening=0.0, shg_low_frequency_broadening=0.025,
                  shg_intermediate_regularization=0.0, shg_eta_correction=True, band_window_size=-1,
-                 band_selection=None):
+                 band_selection=None, wannier_center_convention="II"):
         if not 1 <= len(responses) <= MAX_RESPONSES:
             raise ValueError("between 1 and 8 responses are supported per task")
         self.photon_energies = np.ascontiguousarray(np.asarray(photon_energies, dtype=np.float64))
@@ -178,6 +179,9 @@ class TaskArrays:
         d.shg_intermediate_regularization = float(shg_intermediate_regularization)
         d.shg_eta_correction = 1 if shg_eta_correction else 0
         d.band_window_size = int(band_window_size)
+        if wannier_center_convention not in ("I", "II"):
+            raise ValueError("wannier_center_convention must be 'I' or 'II'")
+        d.wannier_center_convention = 1 if wannier_center_convention == "I" else 0
         # band_selection = (conduction bands, valence bands), 1-based as in the reference's
         # cfg.band_selection; pairs (n, m) with n valence and m conduction are kept.
         if band_selection is not None:

@@ -115,6 +115,9 @@ struct wnlqg_plan {
     size_t eigh_smem = 0;
     bool warp_eigh = false;                   // orthogonal models, nw <= 32: team-per-matrix stages
     int eigh_team = 32;                       // threads per matrix in those stages: 32, 64 or 128
+    // Convention I: Cartesian and fractional Wannier centres (tau[a * nw + i]).
+    bool conv1 = false;
+    std::vector<double> tau_cart, tau_frac;
     bool cta_mixed = false;                   // orthogonal models above 32 orbitals: CTA FP32 + FP64 stages
     bool cta_gw1 = false, cta_gw2 = false;    // those stages' working sets in global memory
     int refine_cta_threads = 512;             // FP64 CTA refinement block size
@@ -1028,6 +1031,10 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
         return fail(WNLQG_ERR_INVALID_ARGUMENT, "unknown precision");
     if (t.band_window_size < -1 || t.band_window_size == 0)
         return fail(WNLQG_ERR_INVALID_ARGUMENT, "band_window_size must be -1 or positive");
+    if (t.wannier_center_convention != 0 && t.wannier_center_convention != 1)
+        return fail(WNLQG_ERR_INVALID_ARGUMENT, "wannier_center_convention must be 0 (II) or 1 (I)");
+    if (t.wannier_center_convention == 1 && model->has_overlap)
+        return fail(WNLQG_ERR_UNSUPPORTED, "Convention I with an overlap is not built");
     if (t.use_band_selection) {
         // validate_interband_band_selection (CalculationUtils.jl:501-522): two nonempty, disjoint
         // groups inside the orbitals.
@@ -1220,6 +1227,54 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
     }
     pl->C = (int)ch.size();
 
+    // Convention I centres (_initialize_wannier_center_scratch!, WannierCenterConventionTransforms.jl:15-56):
+    // tau = Re diag A(R = 0), fractional coordinates from the lattice rows.
+    int home = -1;
+    if (t.wannier_center_convention == 1) {
+        for (int r = 0; r < pl->nr; ++r) {
+            const int64_t *rv = &model->rvec[3 * (size_t)r];
+            if (rv[0] == 0 && rv[1] == 0 && rv[2] == 0) {
+                if (home >= 0) return bail(fail(WNLQG_ERR_INVALID_ARGUMENT, "TB model contains more than one R=(0,0,0) block."));
+                home = r;
+            }
+        }
+        if (home < 0)
+            return bail(fail(WNLQG_ERR_INVALID_ARGUMENT, "Convention_I requires one R=(0,0,0) position block in the TB model."));
+        const int nwc = pl->nw;
+        pl->tau_cart.assign(3 * (size_t)nwc, 0.0);
+        pl->tau_frac.assign(3 * (size_t)nwc, 0.0);
+        if (model->has_position)
+            for (int i = 0; i < nwc; ++i)
+                for (int a = 0; a < 3; ++a) {
+                    const double2 v = model->A[((size_t)home * 3 + a) * pl->nn + i + (size_t)nwc * i];
+                    if (!std::isfinite(v.x) || !std::isfinite(v.y))
+                        return bail(fail(WNLQG_ERR_NONFINITE, "Convention_I Wannier center is non-finite"));
+                    if (std::fabs(v.y) > 1.0e-10)
+                        return bail(fail(WNLQG_ERR_INVALID_ARGUMENT, "Convention_I Wannier center has an imaginary part"));
+                    pl->tau_cart[a * nwc + i] = v.x;
+                }
+        // tau_cart[j] = sum_i tau_frac_i lattice[i + 3 j]: solve the 3 x 3 system (Cramer).
+        const double *L = model->lattice;
+        auto M = [&](int i, int j) { return L[i + 3 * j]; };   // row i = lattice vector i
+        const double det = M(0, 0) * (M(1, 1) * M(2, 2) - M(2, 1) * M(1, 2)) - M(1, 0) * (M(0, 1) * M(2, 2) - M(2, 1) * M(0, 2)) +
+                           M(2, 0) * (M(0, 1) * M(1, 2) - M(1, 1) * M(0, 2));
+        if (!(std::fabs(det) > 0)) return bail(fail(WNLQG_ERR_INVALID_ARGUMENT, "singular lattice"));
+        for (int i = 0; i < nwc; ++i) {
+            const double b[3] = {pl->tau_cart[i], pl->tau_cart[nwc + i], pl->tau_cart[2 * nwc + i]};
+            // Unknown x with sum_r x_r M(r, j) = b_j: columns of the system matrix are M(r, :).
+            auto solve_col = [&](int c) {
+                double A3[3][3];
+                for (int j = 0; j < 3; ++j)
+                    for (int r = 0; r < 3; ++r) A3[j][r] = r == c ? b[j] : M(r, j);
+                return (A3[0][0] * (A3[1][1] * A3[2][2] - A3[1][2] * A3[2][1]) -
+                        A3[0][1] * (A3[1][0] * A3[2][2] - A3[1][2] * A3[2][0]) +
+                        A3[0][2] * (A3[1][0] * A3[2][1] - A3[1][1] * A3[2][0])) / det;
+            };
+            for (int c = 0; c < 3; ++c) pl->tau_frac[c * nwc + i] = solve_col(c);
+        }
+        pl->conv1 = true;
+    }
+
     // Real-space tiles T[R][c][i + nw j] (prepare_hamiltonian_real_space!,
     // HamiltonianMatrixElements.jl:92-177; prepare_position_real_space!, PositionMatrixElements.jl:8-84;
     // Convention II displacements).
@@ -1238,15 +1293,27 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
             for (int64_t e = 0; e < nn; ++e) {
                 double2 h = model->H[(size_t)r * nn + e];
                 double2 v = make_double2(0.0, 0.0);
+                // Convention I: displacement R + tau_j - tau_i (_convention_displacement_component,
+                // WannierCenterConventionTransforms.jl:85-96) and the centred home-cell connection
+                // A - tau (_convention_position_value, :99-113).
+                const int ei = (int)(e % nw), ej = (int)(e / nw);
+                double dsp[3] = {rc[0], rc[1], rc[2]};
+                if (pl->conv1)
+                    for (int x = 0; x < 3; ++x) dsp[x] += pl->tau_cart[x * nw + ej] - pl->tau_cart[x * nw + ei];
+                auto position = [&](int p) {
+                    double2 a = model->A[((size_t)r * 3 + p) * nn + e];
+                    if (pl->conv1 && r == home && ei == ej) a.x -= pl->tau_cart[p * nw + ei];
+                    return a;
+                };
                 switch (cc.op) {
                 case CH_H: v = h; break;
-                case CH_DH: v = cmuli(cscale(h, rc[cc.p])); break;
-                case CH_DDH: v = cscale(h, -rc[cc.p] * rc[cc.d]); break;
+                case CH_DH: v = cmuli(cscale(h, dsp[cc.p])); break;
+                case CH_DDH: v = cscale(h, -dsp[cc.p] * dsp[cc.d]); break;
                 case CH_A:
-                    if (model->has_position) v = model->A[((size_t)r * 3 + cc.p) * nn + e];
+                    if (model->has_position) v = position(cc.p);
                     break;
                 case CH_DA:
-                    if (model->has_position) v = cmuli(cscale(model->A[((size_t)r * 3 + cc.p) * nn + e], rc[cc.d]));
+                    if (model->has_position) v = cmuli(cscale(position(cc.p), dsp[cc.d]));
                     break;
                 case CH_S:
                     v = model->S[(size_t)r * nn + e];
@@ -1817,6 +1884,35 @@ wnlqg_status wnlqg_b200_eval_spectrum(wnlqg_plan *pl, const double *kpoints, int
     if (pl->nonorth)
         for (int v : stat)
             if (v) return fail(WNLQG_ERR_INVALID_ARGUMENT, "effective S(k) is not positive definite");
+    if (pl->conv1 && eigenvectors) {
+        // Convention I eigenvectors: D(k)^H U, D = diag(exp(2 pi i k.tau_frac)) (the similarity of
+        // _apply_wannier_center_similarity!), then the canonical phase rule again
+        // (canonicalize_eigenvectors!, HamiltonianMatrixElements.jl:6-25); energies are unchanged.
+        const int nw = pl->nw;
+        std::vector<double2> ph(nw);
+        for (int64_t s = 0; s < n; ++s) {
+            const double *k = kpoints + 3 * s;
+            for (int i = 0; i < nw; ++i) {
+                const double x = 2.0 * WNLQG_PI * (k[0] * pl->tau_frac[i] + k[1] * pl->tau_frac[nw + i] + k[2] * pl->tau_frac[2 * nw + i]);
+                ph[i] = make_double2(std::cos(x), -std::sin(x));   // conj(phi_i)
+            }
+            double2 *u = reinterpret_cast<double2 *>(eigenvectors) + s * pl->nn;
+            for (int c = 0; c < nw; ++c) {
+                double2 *col = u + (size_t)nw * c;
+                int pivot = 0;
+                double pm = -1.0;
+                for (int i = 0; i < nw; ++i) {
+                    col[i] = cmul(ph[i], col[i]);
+                    const double mg = std::hypot(col[i].x, col[i].y);
+                    if (mg > pm) { pm = mg; pivot = i; }
+                }
+                if (pm > 0.0) {
+                    const double2 q = make_double2(col[pivot].x / pm, -col[pivot].y / pm);
+                    for (int i = 0; i < nw; ++i) col[i] = cmul(col[i], q);
+                }
+            }
+        }
+    }
     return WNLQG_OK;
 }
 
