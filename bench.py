@@ -192,6 +192,8 @@ def main():
                     help="skip the batched uneven-models measurement (one GPU only)")
     ap.add_argument("--no-time-to-tolerance", action="store_true",
                     help="skip the time-to-1e-4 convergence study of sigma^xyy (one GPU only)")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the built-in eigensolver team and contraction tile rules")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -225,6 +227,10 @@ def main():
     def block(step):
         b = ((step * world + rank) * batch) % nk
         return b, min(nk, b + batch)
+
+    # The autotuner picks the eigensolver team and the contraction tile on the first step's block
+    # (untimed; every rank tunes its own plan).
+    tuning = None if args.no_autotune else engine.autotune(MESH, *block(0))
 
     random_mode = args.sampling == "random"
     if random_mode:
@@ -369,7 +375,8 @@ def main():
         "config": {"workload": WORKLOAD_RANDOM if random_mode else WORKLOAD, "k_per_step_per_gpu": batch,
                    "mesh": None if random_mode else list(MESH), "sampling": args.sampling,
                    "precision": args.precision, "l2": "inputs larger than L2 (per-step workspace >> 126 MB)",
-                   "parallelism": f"k-blocks x{world}"},
+                   "parallelism": f"k-blocks x{world}",
+                   "autotune": tuning},
         "roofline": roofline,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": int(idx.nbytes + w.nbytes),
                 "d2h_bytes_per_step": int(16 * vc)},
@@ -430,10 +437,10 @@ def batched_uneven(device: int, mesh: int = 16) -> dict:
     nw in {6, 8, 12, 16, 24, 32}, every second one Kramers-doubled (H (x) I_2 + i 1e-3 eV M (x)
     sigma_z, so nw up to 64), intrinsic AHC sigma^xy and Berry-curvature dipole D^xzz at
     mu in {-0.5, 0, 0.5} eV and T = 50 K, each on its own mesh^3 mesh.  Timed (CUDA events on the
-    caller's stream) as one concurrent wnlqg_b200_eval_mesh_many call and as the same models one
-    call after another."""
+    caller's stream) as one concurrent wnlqg_b200_eval_mesh_many call, as the same models one
+    call after another, and as that concurrent call captured once in a CUDA graph and replayed."""
     import torch
-    from wanniernlqg_b200.engine import ResponseEngine, integrate_meshes_many
+    from wanniernlqg_b200.engine import CapturedGraph, ResponseEngine, integrate_meshes_many
     from wanniernlqg_b200.model import kramers_doubled_model, synthetic_orthogonal_model
 
     task = _abi.TaskArrays([(_abi.INTRINSIC_AHC, ["xy"]), (_abi.BERRY_DIPOLE, ["xzz"])],
@@ -471,6 +478,13 @@ def batched_uneven(device: int, mesh: int = 16) -> dict:
 
         t_conc = timed(concurrent)
         t_seq = timed(sequential)
+        # The same call captured once as a CUDA graph and replayed.
+        graph = CapturedGraph.mesh_many(engines, meshes, ranges, ptrs)
+        try:
+            t_graph = timed(lambda: graph.launch(stream.cuda_stream))
+            graph_kernels = graph.kernel_count
+        finally:
+            graph.close()
     finally:
         for e in engines:
             e.close()
@@ -478,6 +492,7 @@ def batched_uneven(device: int, mesh: int = 16) -> dict:
     return {"models": len(models), "orbitals": [m.num_orbitals for m in models], "mesh": mesh,
             "responses": "AHC xy + Berry dipole xzz at 3 Fermi energies, T = 50 K",
             "concurrent_ms": t_conc, "sequential_ms": t_seq, "speedup": t_seq / t_conc,
+            "graph_ms": t_graph, "graph_kernels": graph_kernels,
             "kpoints_per_s": total / (t_conc / 1e3)}
 
 

@@ -269,6 +269,50 @@ WNLQG_API wnlqg_status wnlqg_b200_plan_last_timing(const wnlqg_plan *plan, doubl
 /* Number of kernel launches issued by the last eval_mesh* call. */
 WNLQG_API int64_t wnlqg_b200_plan_last_launch_count(const wnlqg_plan *plan);
 
+/* ---- CUDA graphs (no reference counterpart: the reference's worker loop calls its evaluator
+ * point by point; here one captured graph replaces a whole call) ------------------------------
+ * A graph holds the complete Fourier -> eigensolve -> response -> reduce chain of one call with
+ * its arguments fixed: wnlqg_b200_eval_mesh_many's work for several plans (models of different
+ * orbital counts on their own streams, forked from and joined to the launch stream), or
+ * wnlqg_b200_eval_points_weighted_device's work for one plan on fixed device buffers (the caller
+ * rewrites the k-points and weights between launches; cells of an uneven adaptive refinement are
+ * padded to the captured count with weight-0 points).  Capture runs the call once directly, then
+ * records it.  While a graph exists its plans cannot be destroyed or autotuned, and buffers a
+ * later direct call outgrows are retired, not freed.  Launches are asynchronous on `stream`;
+ * after synchronising, wnlqg_b200_graph_status reports a bounded device wait that gave up. */
+typedef struct wnlqg_graph wnlqg_graph;
+WNLQG_API wnlqg_status wnlqg_b200_graph_capture_mesh_many(wnlqg_plan *const *plans, int32_t count,
+                                                const int64_t *meshes, const int64_t *k_begin,
+                                                const int64_t *k_end, double *const *outs_device,
+                                                wnlqg_graph **out_graph);
+WNLQG_API wnlqg_status wnlqg_b200_graph_capture_points_weighted(wnlqg_plan *plan, const double *kpoints_device,
+                                                      const double *weights_device, int64_t n,
+                                                      double *out_device, wnlqg_graph **out_graph);
+WNLQG_API wnlqg_status wnlqg_b200_graph_launch(wnlqg_graph *graph, void *stream);
+WNLQG_API wnlqg_status wnlqg_b200_graph_status(wnlqg_graph *graph);
+/* Kernels one launch of the graph runs. */
+WNLQG_API int64_t wnlqg_b200_graph_kernel_count(const wnlqg_graph *graph);
+WNLQG_API wnlqg_status wnlqg_b200_graph_destroy(wnlqg_graph *graph);
+
+/* ---- Autotuner (no reference counterpart) -------------------------------------------------
+ * Measures, on the mesh block [k_begin, k_end) of `mesh`, every eigensolver team size (32, 64 and
+ * 128 threads per matrix; orthogonal models up to 32 orbitals) and every contraction tile (1, 2
+ * and 4 photon energies per thread; frequency-resolved responses), keeps the fastest of each in
+ * the plan and remembers it for the process (key: device, orbitals, precision, geometry, photon
+ * energies, value count), so later plans with the same key take it without measuring.  Every
+ * candidate is a configuration the library runs anyway; the tile choice leaves results bitwise
+ * unchanged.  Times are CUDA-event milliseconds of the second of two runs; -1 = not a
+ * candidate; 0 in a choice = not tunable for this plan. */
+typedef struct wnlqg_autotune_report {
+    int32_t eigh_team;             /* chosen threads per matrix (32, 64, 128), 0 = fixed variant */
+    int32_t energies_per_thread;   /* chosen contraction tile (1, 2, 4), 0 = no energy axis */
+    double eigh_ms[3];             /* eigensolve time with 32, 64, 128 threads per matrix */
+    double response_ms[3];         /* response time with 1, 2, 4 energies per thread */
+    int32_t from_cache;            /* 1 when the choice came from the process cache */
+} wnlqg_autotune_report;
+WNLQG_API wnlqg_status wnlqg_b200_plan_autotune(wnlqg_plan *plan, const int64_t mesh[3], int64_t k_begin,
+                                      int64_t k_end, wnlqg_autotune_report *report);
+
 #ifdef __cplusplus
 }
 #endif

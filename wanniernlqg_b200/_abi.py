@@ -62,6 +62,17 @@ class ResponseRequest(ctypes.Structure):
     ]
 
 
+class AutotuneReport(ctypes.Structure):
+    """wnlqg_autotune_report."""
+    _fields_ = [
+        ("eigh_team", ctypes.c_int32),
+        ("energies_per_thread", ctypes.c_int32),
+        ("eigh_ms", ctypes.c_double * 3),
+        ("response_ms", ctypes.c_double * 3),
+        ("from_cache", ctypes.c_int32),
+    ]
+
+
 class TaskDesc(ctypes.Structure):
     _fields_ = [
         ("num_responses", ctypes.c_int32),

@@ -23,6 +23,9 @@ EXPORTED_SYMBOLS = (
     "wnlqg_b200_spectrum_noalloc",
     "wnlqg_b200_mlp_param_count", "wnlqg_b200_mlp_create", "wnlqg_b200_mlp_destroy", "wnlqg_b200_mlp_get_params",
     "wnlqg_b200_mlp_set_params", "wnlqg_b200_mlp_forward", "wnlqg_b200_mlp_loss_grad", "wnlqg_b200_mlp_train",
+    "wnlqg_b200_graph_capture_mesh_many", "wnlqg_b200_graph_capture_points_weighted", "wnlqg_b200_graph_launch",
+    "wnlqg_b200_graph_status", "wnlqg_b200_graph_kernel_count", "wnlqg_b200_graph_destroy",
+    "wnlqg_b200_plan_autotune",
 )
 
 _lib = None
@@ -86,6 +89,20 @@ def load():
         getattr(L, name).restype = ctypes.c_int
     L.wnlqg_b200_plan_last_launch_count.restype = ctypes.c_int64
     L.wnlqg_b200_plan_last_launch_count.argtypes = [vp]
+    L.wnlqg_b200_graph_capture_mesh_many.argtypes = [ctypes.POINTER(vp), ctypes.c_int32, ip, ip, ip,
+                                                     ctypes.POINTER(vp), ctypes.POINTER(vp)]
+    L.wnlqg_b200_graph_capture_points_weighted.argtypes = [vp, vp, vp, ctypes.c_int64, vp, ctypes.POINTER(vp)]
+    L.wnlqg_b200_graph_launch.argtypes = [vp, vp]
+    L.wnlqg_b200_graph_status.argtypes = [vp]
+    L.wnlqg_b200_graph_kernel_count.restype = ctypes.c_int64
+    L.wnlqg_b200_graph_kernel_count.argtypes = [vp]
+    L.wnlqg_b200_graph_destroy.argtypes = [vp]
+    L.wnlqg_b200_plan_autotune.argtypes = [vp, ip, ctypes.c_int64, ctypes.c_int64,
+                                           ctypes.POINTER(_abi.AutotuneReport)]
+    for name in ("wnlqg_b200_graph_capture_mesh_many", "wnlqg_b200_graph_capture_points_weighted",
+                 "wnlqg_b200_graph_launch", "wnlqg_b200_graph_status", "wnlqg_b200_graph_destroy",
+                 "wnlqg_b200_plan_autotune"):
+        getattr(L, name).restype = ctypes.c_int
     for name in ("wnlqg_b200_last_error", "wnlqg_b200_model_create", "wnlqg_b200_model_destroy",
                  "wnlqg_b200_plan_create", "wnlqg_b200_plan_destroy", "wnlqg_b200_eval_mesh",
                  "wnlqg_b200_eval_mesh_device", "wnlqg_b200_eval_mesh_many", "wnlqg_b200_eval_points",

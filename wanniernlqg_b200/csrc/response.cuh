@@ -32,6 +32,7 @@ enum { RS_MU_AHC = 1, RS_MU_DIPOLE = 2 };
 
 struct RespParams {
     int nw, ld;
+    int omb_force;              // photon energies per thread in the contraction: 1, 2, 4; 0 = sized to the axis
     int64_t batch;
     int64_t xw_stride;          // complex entries per k in xw
     const double2 *xw;          // Wannier-gauge channels [batch][C][nw][nw]
@@ -799,7 +800,9 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 1 : 2) response_kernel(R
             const R w2 = (R)(p.width * p.width), lor = (R)(p.width / WNLQG_PI);
             const R gsc = (R)p.gscale, cut = (R)p.cutoff, invw = (R)(1.0 / p.width);
             const R win = (R)(p.thr > 0.0 ? p.thr : 0.0);
-            const int omb = p.nom <= (int)blockDim.x ? 1 : (p.nom <= 2 * (int)blockDim.x ? 2 : RS_OMB);
+            const int omb = p.omb_force == 1 || p.omb_force == 2 || p.omb_force == RS_OMB
+                                ? p.omb_force
+                                : (p.nom <= (int)blockDim.x ? 1 : (p.nom <= 2 * (int)blockDim.x ? 2 : RS_OMB));
             for (int w0 = 0; w0 < p.nom; w0 += omb * blockDim.x) {
                 if (w0 + (int)threadIdx.x >= p.nom) continue;
                 double om[RS_OMB];

@@ -13,6 +13,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <limits>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -149,6 +151,11 @@ struct wnlqg_plan {
     size_t timing_batches = 0;
     int64_t launches = 0;
     bool timing_valid = false;
+    // CUDA graphs that captured this plan's launches: while any exists, buffers that a later call
+    // outgrows are retired (kept until the plan is destroyed) instead of freed, and the plan
+    // cannot be destroyed.
+    int graph_refs = 0;
+    std::vector<void *> retired;
 };
 
 namespace {
@@ -698,14 +705,16 @@ wnlqg_status run_front(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const int64_
         const int64_t n3t = i3_last - i3_first + 1;
         const size_t needY = (size_t)n3t * pl->P12 * N, needZ = (size_t)nlines * pl->P1 * N;
         if (needY > pl->stageY_elems) {
-            if (pl->d_stageY) WNLQG_CUDA(cudaFree(pl->d_stageY));
+            if (pl->d_stageY && pl->graph_refs > 0) pl->retired.push_back(pl->d_stageY);
+            else if (pl->d_stageY) WNLQG_CUDA(cudaFree(pl->d_stageY));
             pl->d_stageY = nullptr;
             pl->stageY_elems = 0;
             WNLQG_CUDA(cudaMalloc(&pl->d_stageY, needY * sizeof(double2)));
             pl->stageY_elems = needY;
         }
         if (needZ > pl->stageZ_elems) {
-            if (pl->d_stageZ) WNLQG_CUDA(cudaFree(pl->d_stageZ));
+            if (pl->d_stageZ && pl->graph_refs > 0) pl->retired.push_back(pl->d_stageZ);
+            else if (pl->d_stageZ) WNLQG_CUDA(cudaFree(pl->d_stageZ));
             pl->d_stageZ = nullptr;
             pl->stageZ_elems = 0;
             WNLQG_CUDA(cudaMalloc(&pl->d_stageZ, needZ * sizeof(double2)));
@@ -991,7 +1000,10 @@ wnlqg_status wnlqg_b200_model_destroy(wnlqg_model *model) {
 
 wnlqg_status wnlqg_b200_plan_destroy(wnlqg_plan *pl) {
     if (!pl) return WNLQG_OK;
+    if (pl->graph_refs > 0)
+        return fail(WNLQG_ERR_INVALID_ARGUMENT, "plan is captured in a CUDA graph: destroy the graph first");
     cudaSetDevice(pl->model->device);
+    for (void *ptr : pl->retired) cudaFree(ptr);
     if (pl->stream) cudaStreamSynchronize(pl->stream);
     for (void *ptr : {(void *)pl->d_tiles, (void *)pl->d_phase, (void *)pl->d_xw, (void *)pl->d_U, (void *)pl->d_out,
                       (void *)pl->d_points, (void *)pl->d_E, (void *)pl->d_kpts, (void *)pl->d_omegas,
@@ -1636,6 +1648,103 @@ wnlqg_status enqueue_mesh(wnlqg_plan *pl, const int64_t mesh[3], int64_t k_begin
     return WNLQG_OK;
 }
 
+// Events that order streams: destroyed at once in direct calls, kept alive until the end of a
+// stream capture (the capture records their dependencies).
+struct EventKeeper {
+    std::vector<cudaEvent_t> *keep = nullptr;
+    void done(cudaEvent_t ev) {
+        if (keep) keep->push_back(ev);
+        else cudaEventDestroy(ev);
+    }
+};
+
+wnlqg_status order_after(cudaStream_t a, cudaStream_t b, EventKeeper &ek) {
+    cudaEvent_t ev;
+    WNLQG_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    cudaError_t e = cudaEventRecord(ev, b);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(a, ev, 0);
+    ek.done(ev);
+    if (e != cudaSuccess) return fail(WNLQG_ERR_CUDA, std::string("stream ordering: ") + cudaGetErrorString(e));
+    return WNLQG_OK;
+}
+
+// Several plans' mesh sums forked from `origin` and joined back into it.
+wnlqg_status enqueue_many(wnlqg_plan *const *plans, int32_t count, const int64_t *meshes, const int64_t *k_begin,
+                          const int64_t *k_end, double *const *outs_device, cudaStream_t origin, EventKeeper &ek) {
+    cudaEvent_t fork;
+    WNLQG_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    cudaError_t e = cudaEventRecord(fork, origin);
+    for (int32_t i = 0; i < count && e == cudaSuccess; ++i) {
+        plans[i]->timing_valid = false;
+        e = cudaStreamWaitEvent(plans[i]->stream, fork, 0);
+    }
+    ek.done(fork);
+    if (e != cudaSuccess) return fail(WNLQG_ERR_CUDA, std::string("stream fork: ") + cudaGetErrorString(e));
+    for (int32_t i = 0; i < count; ++i) {
+        wnlqg_status st = enqueue_mesh(plans[i], meshes + 3 * i, k_begin[i], k_end[i], outs_device[i]);
+        if (st != WNLQG_OK) return st;
+    }
+    for (int32_t i = 0; i < count; ++i) {
+        wnlqg_status st = order_after(origin, plans[i]->stream, ek);
+        if (st != WNLQG_OK) return st;
+    }
+    return WNLQG_OK;
+}
+
+// Weighted point sum on the plan's stream: out = sum_i w_i value(k_i), k-points and weights on
+// the device.
+wnlqg_status enqueue_points_weighted(wnlqg_plan *pl, const double *kpoints_device, const double *weights_device,
+                                     int64_t n, double *out_device) {
+    wnlqg_status st;
+    if ((st = record_event(pl, 0)) != WNLQG_OK) return st;
+    pl->launches = 0;
+    WNLQG_CUDA(cudaMemsetAsync(pl->d_partials, 0, (size_t)pl->partial_slots * pl->vc * 4 * sizeof(double), pl->stream));
+    size_t nbatch = 0;
+    for (int64_t s = 0; s < n; s += pl->max_batch, ++nbatch) {
+        const int64_t nb = std::min(pl->max_batch, n - s);
+        const size_t base = 1 + 3 * nbatch;
+        if ((st = record_event(pl, base)) != WNLQG_OK) return st;
+        if ((st = run_front(pl, nb, 0, nullptr, kpoints_device + 3 * s, base)) != WNLQG_OK) return st;
+        if ((st = run_passes(pl, nb, 0, 1.0, 0, weights_device + s)) != WNLQG_OK) return st;
+    }
+    const size_t final_ev = 1 + 3 * nbatch;
+    if ((st = record_event(pl, final_ev)) != WNLQG_OK) return st;
+    reduce_partials_kernel<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((pl->vc + 255) / 256, 1024)), 256, 0,
+                             pl->stream>>>(pl->d_partials, pl->partial_slots, pl->vc, reinterpret_cast<double2 *>(out_device));
+    pl->launches += 1;
+    WNLQG_CUDA(cudaGetLastError());
+    if ((st = record_event(pl, final_ev + 1)) != WNLQG_OK) return st;
+    pl->timing_valid = true;
+    pl->timing_batches = nbatch;
+    return WNLQG_OK;
+}
+
+wnlqg_status check_points_args(wnlqg_plan *pl, const double *kpoints_device, const double *weights_device, int64_t n,
+                               const double *out_device) {
+    wnlqg_status st = check_plan(pl);
+    if (st != WNLQG_OK) return st;
+    if (n < 0 || (n > 0 && (!kpoints_device || !weights_device)) || !out_device)
+        return fail(WNLQG_ERR_INVALID_ARGUMENT, "invalid points");
+    return WNLQG_OK;
+}
+
+wnlqg_status check_many_args(wnlqg_plan *const *plans, int32_t count, const int64_t *meshes, const int64_t *k_begin,
+                             const int64_t *k_end, double *const *outs_device) {
+    if (count < 0 || (count > 0 && (!plans || !meshes || !k_begin || !k_end || !outs_device)))
+        return fail(WNLQG_ERR_INVALID_ARGUMENT, "invalid plan list");
+    for (int32_t i = 0; i < count; ++i) {
+        wnlqg_status st = check_plan(plans[i]);
+        if (st != WNLQG_OK) return st;
+        if (i > 0 && plans[i]->model->device != plans[0]->model->device)
+            return fail(WNLQG_ERR_INVALID_ARGUMENT, "all plans of one call must live on one device");
+    }
+    for (int32_t i = 0; i < count; ++i) {
+        wnlqg_status st = check_mesh_args(plans[i], meshes + 3 * i, k_begin[i], k_end[i], outs_device[i]);
+        if (st != WNLQG_OK) return st;
+    }
+    return WNLQG_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1658,90 +1767,27 @@ wnlqg_status wnlqg_b200_eval_mesh_device(wnlqg_plan *pl, const int64_t mesh[3], 
 wnlqg_status wnlqg_b200_eval_points_weighted_device(wnlqg_plan *pl, const double *kpoints_device,
                                                     const double *weights_device, int64_t n, double *out_device,
                                                     void *stream) {
-    wnlqg_status st = check_plan(pl);
+    wnlqg_status st = check_points_args(pl, kpoints_device, weights_device, n, out_device);
     if (st != WNLQG_OK) return st;
-    if (n < 0 || (n > 0 && (!kpoints_device || !weights_device)) || !out_device)
-        return fail(WNLQG_ERR_INVALID_ARGUMENT, "invalid points");
     WNLQG_CUDA(cudaSetDevice(pl->model->device));
     cudaStream_t user = static_cast<cudaStream_t>(stream);
-    {
-        cudaEvent_t ev;
-        WNLQG_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-        WNLQG_CUDA(cudaEventRecord(ev, user));
-        WNLQG_CUDA(cudaStreamWaitEvent(pl->stream, ev, 0));
-        cudaEventDestroy(ev);
-    }
-    if ((st = record_event(pl, 0)) != WNLQG_OK) return st;
-    pl->launches = 0;
-    WNLQG_CUDA(cudaMemsetAsync(pl->d_partials, 0, (size_t)pl->partial_slots * pl->vc * 4 * sizeof(double), pl->stream));
-    size_t nbatch = 0;
-    for (int64_t s = 0; s < n; s += pl->max_batch, ++nbatch) {
-        const int64_t nb = std::min(pl->max_batch, n - s);
-        const size_t base = 1 + 3 * nbatch;
-        if ((st = record_event(pl, base)) != WNLQG_OK) return st;
-        if ((st = run_front(pl, nb, 0, nullptr, kpoints_device + 3 * s, base)) != WNLQG_OK) return st;
-        if ((st = run_passes(pl, nb, 0, 1.0, 0, weights_device + s)) != WNLQG_OK) return st;
-    }
-    const size_t final_ev = 1 + 3 * nbatch;
-    if ((st = record_event(pl, final_ev)) != WNLQG_OK) return st;
-    reduce_partials_kernel<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((pl->vc + 255) / 256, 1024)), 256, 0,
-                             pl->stream>>>(pl->d_partials, pl->partial_slots, pl->vc, reinterpret_cast<double2 *>(out_device));
-    pl->launches += 1;
-    WNLQG_CUDA(cudaGetLastError());
-    if ((st = record_event(pl, final_ev + 1)) != WNLQG_OK) return st;
-    {
-        cudaEvent_t ev;
-        WNLQG_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-        WNLQG_CUDA(cudaEventRecord(ev, pl->stream));
-        WNLQG_CUDA(cudaStreamWaitEvent(user, ev, 0));
-        cudaEventDestroy(ev);
-    }
-    pl->timing_valid = true;
-    pl->timing_batches = nbatch;
-    return WNLQG_OK;
+    EventKeeper ek;
+    if ((st = order_after(pl->stream, user, ek)) != WNLQG_OK) return st;
+    if ((st = enqueue_points_weighted(pl, kpoints_device, weights_device, n, out_device)) != WNLQG_OK) return st;
+    return order_after(user, pl->stream, ek);
 }
 
 wnlqg_status wnlqg_b200_eval_mesh_many(wnlqg_plan *const *plans, int32_t count, const int64_t *meshes,
                                        const int64_t *k_begin, const int64_t *k_end, double *const *outs_device,
                                        void *stream) {
-    if (count < 0 || (count > 0 && (!plans || !meshes || !k_begin || !k_end || !outs_device)))
-        return fail(WNLQG_ERR_INVALID_ARGUMENT, "invalid plan list");
-    for (int32_t i = 0; i < count; ++i) {
-        wnlqg_status st = check_plan(plans[i]);
-        if (st != WNLQG_OK) return st;
-        if (i > 0 && plans[i]->model->device != plans[0]->model->device)
-            return fail(WNLQG_ERR_INVALID_ARGUMENT, "all plans of one call must live on one device");
-    }
-    // Every plan's stream forks from the caller's stream before any plan is enqueued and joins back
-    // after all are, so the models' kernels overlap on the device.
-    for (int32_t i = 0; i < count; ++i) {
-        wnlqg_status st = check_mesh_args(plans[i], meshes + 3 * i, k_begin[i], k_end[i], outs_device[i]);
-        if (st != WNLQG_OK) return st;
-    }
+    wnlqg_status st = check_many_args(plans, count, meshes, k_begin, k_end, outs_device);
+    if (st != WNLQG_OK) return st;
     if (count == 0) return WNLQG_OK;
     WNLQG_CUDA(cudaSetDevice(plans[0]->model->device));
-    cudaStream_t user = static_cast<cudaStream_t>(stream);
-    cudaEvent_t fork;
-    WNLQG_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
-    WNLQG_CUDA(cudaEventRecord(fork, user));
-    for (int32_t i = 0; i < count; ++i) {
-        plans[i]->timing_valid = false;
-        cudaError_t e = cudaStreamWaitEvent(plans[i]->stream, fork, 0);
-        if (e != cudaSuccess) {
-            cudaEventDestroy(fork);
-            return fail(WNLQG_ERR_CUDA, std::string("cudaStreamWaitEvent: ") + cudaGetErrorString(e));
-        }
-    }
-    cudaEventDestroy(fork);
-    for (int32_t i = 0; i < count; ++i) {
-        wnlqg_status st = enqueue_mesh(plans[i], meshes + 3 * i, k_begin[i], k_end[i], outs_device[i]);
-        if (st != WNLQG_OK) return st;
-    }
-    for (int32_t i = 0; i < count; ++i) {
-        wnlqg_status st = stream_after(user, plans[i]->stream);
-        if (st != WNLQG_OK) return st;
-    }
-    return WNLQG_OK;
+    // Every plan's stream forks from the caller's stream before any plan is enqueued and joins back
+    // after all are, so the models' kernels overlap on the device.
+    EventKeeper ek;
+    return enqueue_many(plans, count, meshes, k_begin, k_end, outs_device, static_cast<cudaStream_t>(stream), ek);
 }
 
 wnlqg_status wnlqg_b200_eval_mesh(wnlqg_plan *pl, const int64_t mesh[3], int64_t k_begin, int64_t k_end, double *out) {
@@ -1948,6 +1994,265 @@ wnlqg_status wnlqg_b200_plan_last_timing(const wnlqg_plan *pl_const, double *fou
 int64_t wnlqg_b200_plan_last_launch_count(const wnlqg_plan *plan) { return plan ? plan->launches : -1; }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// CUDA graphs: the whole interpolate -> eigensolve -> integrand -> reduce chain of one call (one
+// plan, or several plans on their own streams forked from one origin), captured once and replayed
+// with one cudaGraphLaunch.  The graph bakes in the call's arguments and the plans' buffers.
+// ---------------------------------------------------------------------------------------------
+struct wnlqg_graph {
+    std::vector<wnlqg_plan *> plans;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t origin = nullptr;
+    int device = 0;
+    int64_t kernels = 0;
+};
+
+namespace {
+
+void graph_release(wnlqg_graph *g) {
+    if (!g) return;
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    if (g->origin) cudaStreamDestroy(g->origin);
+    for (wnlqg_plan *pl : g->plans) pl->graph_refs -= 1;
+    delete g;
+}
+
+// Runs `body(origin, keeper)` once directly (so that every lazily sized buffer exists), then under
+// stream capture of a private origin stream, and instantiates the captured graph.
+template <typename Body>
+wnlqg_status capture_graph(const std::vector<wnlqg_plan *> &plans, Body body, wnlqg_graph **out) {
+    if (!out) return fail(WNLQG_ERR_INVALID_ARGUMENT, "NULL graph handle");
+    *out = nullptr;
+    wnlqg_graph *g = new wnlqg_graph();
+    g->device = plans[0]->model->device;
+    WNLQG_CUDA(cudaSetDevice(g->device));
+    cudaError_t e = cudaStreamCreateWithFlags(&g->origin, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete g;
+        return fail(WNLQG_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
+    }
+    // Plans join the graph's reference count first: buffers a later call outgrows are retired.
+    g->plans = plans;
+    for (wnlqg_plan *pl : plans) pl->graph_refs += 1;
+    {
+        EventKeeper direct;
+        wnlqg_status st = body(g->origin, direct);
+        if (st == WNLQG_OK && (e = cudaStreamSynchronize(g->origin)) != cudaSuccess)
+            st = fail(WNLQG_ERR_CUDA, std::string("graph warm-up: ") + cudaGetErrorString(e));
+        if (st != WNLQG_OK) {
+            graph_release(g);
+            return st;
+        }
+    }
+    std::vector<cudaEvent_t> kept;
+    EventKeeper keeper;
+    keeper.keep = &kept;
+    e = cudaStreamBeginCapture(g->origin, cudaStreamCaptureModeRelaxed);
+    if (e != cudaSuccess) {
+        graph_release(g);
+        return fail(WNLQG_ERR_CUDA, std::string("cudaStreamBeginCapture: ") + cudaGetErrorString(e));
+    }
+    wnlqg_status st = body(g->origin, keeper);
+    cudaGraph_t graph = nullptr;
+    e = cudaStreamEndCapture(g->origin, &graph);
+    for (cudaEvent_t ev : kept) cudaEventDestroy(ev);
+    for (wnlqg_plan *pl : plans) pl->timing_valid = false;   // the captured event records time nothing
+    if (st == WNLQG_OK && e != cudaSuccess)
+        st = fail(WNLQG_ERR_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e));
+    if (st != WNLQG_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        graph_release(g);
+        return st;
+    }
+    g->graph = graph;
+    e = cudaGraphInstantiate(&g->exec, g->graph, 0);
+    if (e != cudaSuccess) {
+        graph_release(g);
+        return fail(WNLQG_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    }
+    for (wnlqg_plan *pl : plans) g->kernels += pl->launches;
+    *out = g;
+    return WNLQG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+wnlqg_status wnlqg_b200_graph_capture_mesh_many(wnlqg_plan *const *plans, int32_t count, const int64_t *meshes,
+                                                const int64_t *k_begin, const int64_t *k_end,
+                                                double *const *outs_device, wnlqg_graph **out_graph) {
+    wnlqg_status st = check_many_args(plans, count, meshes, k_begin, k_end, outs_device);
+    if (st != WNLQG_OK) return st;
+    if (count == 0) return fail(WNLQG_ERR_INVALID_ARGUMENT, "a graph needs at least one plan");
+    std::vector<wnlqg_plan *> list(plans, plans + count);
+    for (size_t i = 0; i < list.size(); ++i)
+        for (size_t j = 0; j < i; ++j)
+            if (list[i] == list[j]) return fail(WNLQG_ERR_INVALID_ARGUMENT, "a plan appears twice in one graph");
+    std::vector<int64_t> m(meshes, meshes + 3 * (size_t)count), kb(k_begin, k_begin + count), ke(k_end, k_end + count);
+    std::vector<double *> outs(outs_device, outs_device + count);
+    return capture_graph(list, [&](cudaStream_t origin, EventKeeper &ek) {
+        return enqueue_many(list.data(), count, m.data(), kb.data(), ke.data(), outs.data(), origin, ek);
+    }, out_graph);
+}
+
+wnlqg_status wnlqg_b200_graph_capture_points_weighted(wnlqg_plan *plan, const double *kpoints_device,
+                                                      const double *weights_device, int64_t n, double *out_device,
+                                                      wnlqg_graph **out_graph) {
+    wnlqg_status st = check_points_args(plan, kpoints_device, weights_device, n, out_device);
+    if (st != WNLQG_OK) return st;
+    std::vector<wnlqg_plan *> list{plan};
+    return capture_graph(list, [&](cudaStream_t origin, EventKeeper &ek) {
+        wnlqg_status s2 = order_after(plan->stream, origin, ek);
+        if (s2 == WNLQG_OK) s2 = enqueue_points_weighted(plan, kpoints_device, weights_device, n, out_device);
+        if (s2 == WNLQG_OK) s2 = order_after(origin, plan->stream, ek);
+        return s2;
+    }, out_graph);
+}
+
+wnlqg_status wnlqg_b200_graph_launch(wnlqg_graph *graph, void *stream) {
+    if (!graph || !graph->exec) return fail(WNLQG_ERR_INVALID_ARGUMENT, "invalid graph");
+    WNLQG_CUDA(cudaSetDevice(graph->device));
+    WNLQG_CUDA(cudaGraphLaunch(graph->exec, static_cast<cudaStream_t>(stream)));
+    return WNLQG_OK;
+}
+
+wnlqg_status wnlqg_b200_graph_status(wnlqg_graph *graph) {
+    if (!graph) return fail(WNLQG_ERR_INVALID_ARGUMENT, "invalid graph");
+    WNLQG_CUDA(cudaSetDevice(graph->device));
+    for (wnlqg_plan *pl : graph->plans) {
+        if (!pl->d_tc_err) continue;
+        int h = 0;
+        WNLQG_CUDA(cudaMemcpy(&h, pl->d_tc_err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (h) {
+            cudaMemset(pl->d_tc_err, 0, sizeof(int));
+            return fail(WNLQG_ERR_DEVICE_TIMEOUT, "tensor-core Fourier: a bounded device wait gave up");
+        }
+    }
+    return WNLQG_OK;
+}
+
+int64_t wnlqg_b200_graph_kernel_count(const wnlqg_graph *graph) { return graph ? graph->kernels : -1; }
+
+wnlqg_status wnlqg_b200_graph_destroy(wnlqg_graph *graph) {
+    if (!graph) return WNLQG_OK;
+    cudaSetDevice(graph->device);
+    cudaDeviceSynchronize();
+    graph_release(graph);
+    return WNLQG_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// Autotuner: per orbital count, the eigensolver team (threads per matrix of the FP32 Jacobi and
+// FP64 refinement stages, orthogonal models up to 32 orbitals) and the contraction tile (photon
+// energies per thread) measured on the caller's own mesh block; the fastest of each is kept in
+// the plan and remembered for the process (device, orbitals, precision, geometry, energies,
+// values).  Every candidate is a configuration the library runs anyway.
+// ---------------------------------------------------------------------------------------------
+namespace {
+
+struct TuneChoice { int team; int omb; wnlqg_autotune_report report; };
+std::map<std::tuple<int, int, int, int, int64_t, int64_t>, TuneChoice> g_tune_cache;
+std::mutex g_tune_mutex;
+
+void apply_team(wnlqg_plan *pl, int team) {
+    pl->eigh_team = team;
+    pl->eigh_smem = (team == 32 ? 4 : 1) * WarpJacobiSmem::per_team(pl->nw);
+    pl->refine_smem = (team == 32 ? 2 : 1) * WarpRefineSmem::per_team(pl->nw);
+}
+
+void apply_omb(wnlqg_plan *pl, int omb) {
+    for (Pass &ps : pl->passes) ps.params.omb_force = omb;
+}
+
+// Two timed mesh sums (the first warms caches); the second's eigensolve and response times.
+wnlqg_status tune_measure(wnlqg_plan *pl, const int64_t mesh[3], int64_t kb, int64_t ke, double *eig, double *resp) {
+    *eig = *resp = std::numeric_limits<double>::infinity();
+    for (int rep = 0; rep < 2; ++rep) {
+        wnlqg_status st = enqueue_mesh(pl, mesh, kb, ke, reinterpret_cast<double *>(pl->d_out));
+        if (st != WNLQG_OK) return st;
+        double f = 0, e = 0, r = 0, t = 0;
+        if ((st = wnlqg_b200_plan_last_timing(pl, &f, &e, &r, &t)) != WNLQG_OK) return st;
+        if (rep == 1) {
+            *eig = e;
+            *resp = r;
+        }
+    }
+    return WNLQG_OK;
+}
+
+}  // namespace
+
+extern "C" wnlqg_status wnlqg_b200_plan_autotune(wnlqg_plan *pl, const int64_t mesh[3], int64_t k_begin,
+                                                 int64_t k_end, wnlqg_autotune_report *report) {
+    wnlqg_status st = check_mesh_args(pl, mesh, k_begin, k_end, reinterpret_cast<const double *>(pl ? pl->d_out : nullptr));
+    if (st != WNLQG_OK) return st;
+    if (pl->graph_refs > 0)
+        return fail(WNLQG_ERR_INVALID_ARGUMENT, "plan is captured in a CUDA graph: tune it before capturing");
+    WNLQG_CUDA(cudaSetDevice(pl->model->device));
+    const auto key = std::make_tuple(pl->model->device, pl->nw, (int)pl->task.precision, pl->nonorth ? 1 : 0,
+                                     (int64_t)pl->task.num_photon_energies, pl->vc);
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            if (pl->warp_eigh && it->second.team) apply_team(pl, it->second.team);
+            apply_omb(pl, it->second.omb);
+            if (report) {
+                *report = it->second.report;
+                report->from_cache = 1;
+            }
+            return WNLQG_OK;
+        }
+    }
+    wnlqg_autotune_report rep;
+    std::memset(&rep, 0, sizeof(rep));
+    for (int i = 0; i < 3; ++i) rep.eigh_ms[i] = rep.response_ms[i] = -1.0;
+    const int teams[3] = {32, 64, 128}, ombs[3] = {1, 2, 4};
+    if (pl->warp_eigh) {
+        const int start = pl->eigh_team;
+        int best = start;
+        double best_ms = std::numeric_limits<double>::infinity(), r = 0;
+        for (int i = 0; i < 3; ++i) {
+            apply_team(pl, teams[i]);
+            if ((st = tune_measure(pl, mesh, k_begin, k_end, &rep.eigh_ms[i], &r)) != WNLQG_OK) {
+                apply_team(pl, start);
+                return st;
+            }
+            if (rep.eigh_ms[i] < best_ms) { best_ms = rep.eigh_ms[i]; best = teams[i]; }
+        }
+        apply_team(pl, best);
+        rep.eigh_team = best;
+    }
+    bool freq = false;
+    for (const Pass &ps : pl->passes) freq |= ps.params.n_fc > 0 && ps.params.nom > 0;
+    if (freq) {
+        int best = 0;
+        double best_ms = std::numeric_limits<double>::infinity(), e = 0;
+        for (int i = 0; i < 3; ++i) {
+            apply_omb(pl, ombs[i]);
+            if ((st = tune_measure(pl, mesh, k_begin, k_end, &e, &rep.response_ms[i])) != WNLQG_OK) {
+                apply_omb(pl, 0);
+                return st;
+            }
+            if (rep.response_ms[i] < best_ms) { best_ms = rep.response_ms[i]; best = ombs[i]; }
+        }
+        apply_omb(pl, best);
+        rep.energies_per_thread = best;
+    }
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        g_tune_cache[key] = TuneChoice{rep.eigh_team, rep.energies_per_thread, rep};
+    }
+    if (report) *report = rep;
+    return WNLQG_OK;
+}
 
 // ---------------------------------------------------------------------------------------------
 // Allocation-free spectrum entry point.

@@ -40,7 +40,8 @@ class ResponseEngine:
     # -- lifetime ------------------------------------------------------------------------
     def close(self) -> None:
         if self._plan:
-            self._L.wnlqg_b200_plan_destroy(self._plan)
+            # Refused while a CUDA graph holds the plan: the model then stays alive too.
+            _lib.check(self._L.wnlqg_b200_plan_destroy(self._plan))
             self._plan = ctypes.c_void_p()
         if self._model:
             self._L.wnlqg_b200_model_destroy(self._model)
@@ -153,6 +154,21 @@ class ResponseEngine:
     def last_launch_count(self) -> int:
         return int(self._L.wnlqg_b200_plan_last_launch_count(self._plan))
 
+    def autotune(self, mesh: Sequence[int], k_begin: int = 0, k_end: Optional[int] = None) -> dict:
+        """Pick the eigensolver team size and the contraction tile by timing them on a block of
+        ``mesh`` (wnlqg_b200_plan_autotune); the choice stays in this plan and in the process
+        cache.  Returns the report as a dict."""
+        mesh_a = np.ascontiguousarray(np.asarray(mesh, dtype=np.int64))
+        if k_end is None:
+            k_end = int(np.prod(mesh_a))
+        rep = _abi.AutotuneReport()
+        _lib.check(self._L.wnlqg_b200_plan_autotune(self._plan, mesh_a.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                                                    int(k_begin), int(k_end), ctypes.byref(rep)))
+        return {"eigh_team": rep.eigh_team, "energies_per_thread": rep.energies_per_thread,
+                "eigh_ms": {t: rep.eigh_ms[i] for i, t in enumerate((32, 64, 128)) if rep.eigh_ms[i] >= 0},
+                "response_ms": {t: rep.response_ms[i] for i, t in enumerate((1, 2, 4)) if rep.response_ms[i] >= 0},
+                "from_cache": bool(rep.from_cache)}
+
 
 def integrate_meshes_many(engines, meshes, ranges, outs_device, stream_ptr: int = 0) -> None:
     """Mesh sums of several engines (models) in one asynchronous call (wnlqg_b200_eval_mesh_many):
@@ -169,3 +185,64 @@ def integrate_meshes_many(engines, meshes, ranges, outs_device, stream_ptr: int 
     ip = ctypes.POINTER(ctypes.c_int64)
     _lib.check(L.wnlqg_b200_eval_mesh_many(plans, n, mesh_a.ctypes.data_as(ip), kb.ctypes.data_as(ip),
                                            ke.ctypes.data_as(ip), outs, vp(stream_ptr)))
+
+
+class CapturedGraph:
+    """One CUDA graph holding a whole call (wnlqg_b200_graph_*): build it with
+    :meth:`mesh_many` or :meth:`points_weighted`, replay it with :meth:`launch`.  The engines it
+    captured must outlive it; close it before closing them."""
+
+    def __init__(self, handle, engines):
+        self._L = _lib.load()
+        self._g = handle
+        self._engines = list(engines)
+
+    @classmethod
+    def mesh_many(cls, engines, meshes, ranges, outs_device) -> "CapturedGraph":
+        """The work of :func:`integrate_meshes_many` with these arguments."""
+        n = len(engines)
+        L = _lib.load()
+        vp = ctypes.c_void_p
+        plans = (vp * n)(*[e._plan for e in engines])
+        mesh_a = np.ascontiguousarray(np.asarray(meshes, dtype=np.int64).reshape(n, 3))
+        kb = np.ascontiguousarray(np.array([r[0] for r in ranges], dtype=np.int64))
+        ke = np.ascontiguousarray(np.array([r[1] for r in ranges], dtype=np.int64))
+        outs = (vp * n)(*[vp(o) for o in outs_device])
+        ip = ctypes.POINTER(ctypes.c_int64)
+        g = vp()
+        _lib.check(L.wnlqg_b200_graph_capture_mesh_many(plans, n, mesh_a.ctypes.data_as(ip), kb.ctypes.data_as(ip),
+                                                        ke.ctypes.data_as(ip), outs, ctypes.byref(g)))
+        return cls(g, engines)
+
+    @classmethod
+    def points_weighted(cls, engine, kpoints_ptr: int, weights_ptr: int, n: int,
+                        out_device_ptr: int) -> "CapturedGraph":
+        """The work of :meth:`ResponseEngine.weighted_sum_device` on these device buffers."""
+        L = _lib.load()
+        g = ctypes.c_void_p()
+        _lib.check(L.wnlqg_b200_graph_capture_points_weighted(
+            engine._plan, ctypes.c_void_p(kpoints_ptr), ctypes.c_void_p(weights_ptr), int(n),
+            ctypes.c_void_p(out_device_ptr), ctypes.byref(g)))
+        return cls(g, [engine])
+
+    @property
+    def kernel_count(self) -> int:
+        return int(self._L.wnlqg_b200_graph_kernel_count(self._g))
+
+    def launch(self, stream_ptr: int = 0) -> None:
+        _lib.check(self._L.wnlqg_b200_graph_launch(self._g, ctypes.c_void_p(stream_ptr)))
+
+    def status(self) -> None:
+        """After synchronising: raises when a bounded device wait of the last launch gave up."""
+        _lib.check(self._L.wnlqg_b200_graph_status(self._g))
+
+    def close(self) -> None:
+        if self._g:
+            _lib.check(self._L.wnlqg_b200_graph_destroy(self._g))
+            self._g = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
