@@ -393,6 +393,7 @@ def main():
         line["time_to_tolerance"] = time_to_tolerance(model, local_rank)
     if rank == 0 and world == 1 and not args.no_batched:
         line["batched_uneven"] = batched_uneven(local_rank)
+        line["graph_small_calls"] = graph_small_calls(local_rank)
     if dist:
         dist.destroy_process_group()
     if rank == 0:
@@ -494,6 +495,49 @@ def batched_uneven(device: int, mesh: int = 16) -> dict:
             "concurrent_ms": t_conc, "sequential_ms": t_seq, "speedup": t_seq / t_conc,
             "graph_ms": t_graph, "graph_kernels": graph_kernels,
             "kpoints_per_s": total / (t_conc / 1e3)}
+
+
+def graph_small_calls(device: int, n: int = 512, calls: int = 100) -> dict:
+    """Launch-bound calls, as an adaptive controller makes them: weighted sums over n arbitrary
+    k-points of the 4-orbital workload model (shift + injection current xyy at 128 energies), the
+    points and weights already on the device, enqueued back to back on one stream and timed with
+    CUDA events per call: the direct call against the same call captured once as a CUDA graph."""
+    import torch
+    from wanniernlqg_b200.engine import CapturedGraph, ResponseEngine
+
+    task = _abi.TaskArrays([(_abi.SHIFT_CURRENT, ["xyy"]), (_abi.INJECTION_CURRENT, ["xyy"])],
+                           broadening_type=_abi.LORENTZIAN, broadening=0.02,
+                           photon_energies=np.linspace(0, 3, 128))
+    with ResponseEngine(reference_workload_model("nw4"), task, device=device, max_batch=n) as eng:
+        gen = torch.Generator(device="cuda")
+        gen.manual_seed(77)
+        k = torch.rand((n, 3), dtype=torch.float64, device="cuda", generator=gen)
+        w = torch.full((n,), 1.0 / n, dtype=torch.float64, device="cuda")
+        out = torch.zeros(2 * eng.value_count, dtype=torch.float64, device="cuda")
+        stream = torch.cuda.current_stream()
+
+        def per_call(fn):
+            for _ in range(5):
+                fn()
+            torch.cuda.synchronize()
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            for _ in range(calls):
+                fn()
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            return ev0.elapsed_time(ev1) / calls
+
+        t_direct = per_call(lambda: eng.weighted_sum_device(k.data_ptr(), w.data_ptr(), n, out.data_ptr(),
+                                                            stream.cuda_stream))
+        ref = out.clone()
+        with CapturedGraph.points_weighted(eng, k.data_ptr(), w.data_ptr(), n, out.data_ptr()) as graph:
+            t_graph = per_call(lambda: graph.launch(stream.cuda_stream))
+            kernels = graph.kernel_count
+        same = bool(torch.equal(ref, out))
+    return {"orbitals": 4, "points_per_call": n, "calls": calls, "kernels_per_call": kernels,
+            "direct_ms_per_call": t_direct, "graph_ms_per_call": t_graph, "speedup": t_direct / t_graph,
+            "bitwise_equal": same}
 
 
 def fourier_channels(task) -> int:

@@ -102,6 +102,39 @@ function eval_points!(out::Matrix{ComplexF64}, plan, kpoints::Matrix{Float64})
     return out
 end
 
+"""wnlqg_autotune_report: the chosen eigensolver team and contraction tile, with the timings."""
+struct AutotuneReport
+    eigh_team::Int32
+    energies_per_thread::Int32
+    eigh_ms::NTuple{3, Float64}
+    response_ms::NTuple{3, Float64}
+    from_cache::Int32
+end
+
+"""Pick the eigensolver team and contraction tile by timing them on mesh indices [first, last)."""
+function autotune!(plan, mesh::NTuple{3, Int}, first::Integer, last::Integer)
+    m = Int64[mesh...]
+    rep = Ref{AutotuneReport}()
+    check(ccall((:wnlqg_b200_plan_autotune, LIB), Cint, (Ptr{Cvoid}, Ptr{Int64}, Int64, Int64, Ref{AutotuneReport}),
+                plan, m, Int64(first), Int64(last), rep))
+    return rep[]
+end
+
+"""Capture one weighted-points call on fixed device buffers (CuPtr addresses) as a CUDA graph;
+refill the buffers and call graph_launch for each batch of adaptive nodes."""
+function graph_capture_points(plan, kpoints_dev::Ptr{Float64}, weights_dev::Ptr{Float64}, n::Integer,
+                              out_dev::Ptr{ComplexF64})
+    g = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((:wnlqg_b200_graph_capture_points_weighted, LIB), Cint,
+                (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Int64, Ptr{ComplexF64}, Ref{Ptr{Cvoid}}),
+                plan, kpoints_dev, weights_dev, Int64(n), out_dev, g))
+    return g[]
+end
+
+graph_launch(g, stream::Ptr{Cvoid} = C_NULL) =
+    check(ccall((:wnlqg_b200_graph_launch, LIB), Cint, (Ptr{Cvoid}, Ptr{Cvoid}), g, stream))
+graph_destroy(g) = ccall((:wnlqg_b200_graph_destroy, LIB), Cint, (Ptr{Cvoid},), g)
+
 plan_destroy(plan) = ccall((:wnlqg_b200_plan_destroy, LIB), Cint, (Ptr{Cvoid},), plan)
 model_destroy(h) = ccall((:wnlqg_b200_model_destroy, LIB), Cint, (Ptr{Cvoid},), h)
 
