@@ -83,6 +83,7 @@ struct RespParams {
     double *partials;           // [gridDim][vc][4]: (sum re, sum im, comp re, comp im)
     double2 *out_points;        // [batch][vc]
     int64_t point_offset;       // global index of batch entry 0 (mode 1)
+    const int *out_perm;        // mode 1: batch entry b is written to row out_perm[b]; nullptr: row b
     int n_slots;
     // Per-CTA working set in global memory (L1/L2-resident) when it exceeds shared memory
     // (large nw); nullptr: dynamic shared memory.
@@ -570,7 +571,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 1 : 2) response_kernel(R
                     double *acc = p.partials + ((int64_t)blockIdx.x * p.vc + p.sc_out[s]) * 4;
                     neumaier_add(acc[0], acc[2], total * wk);
                 } else {
-                    p.out_points[(p.point_offset + b) * p.vc + p.sc_out[s]] = make_double2(total * p.scale, 0.0);
+                    p.out_points[(p.point_offset + (p.out_perm ? (int64_t)p.out_perm[b] : (int64_t)b)) * p.vc + p.sc_out[s]] = make_double2(total * p.scale, 0.0);
                 }
             }
         }
@@ -625,7 +626,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 1 : 2) response_kernel(R
                             double *a4 = p.partials + ((int64_t)blockIdx.x * p.vc + idx) * 4;
                             neumaier_add(a4[0], a4[2], value * wk);
                         } else {
-                            p.out_points[(p.point_offset + b) * p.vc + idx] = make_double2(value * p.scale, 0.0);
+                            p.out_points[(p.point_offset + (p.out_perm ? (int64_t)p.out_perm[b] : (int64_t)b)) * p.vc + idx] = make_double2(value * p.scale, 0.0);
                         }
                     }
                 }
@@ -689,7 +690,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 1 : 2) response_kernel(R
                                 double *a4 = p.partials + ((int64_t)blockIdx.x * p.vc + idx) * 4;
                                 neumaier_add(a4[0], a4[2], total * wk);
                             } else {
-                                p.out_points[(p.point_offset + b) * p.vc + idx] = make_double2(total * p.scale, 0.0);
+                                p.out_points[(p.point_offset + (p.out_perm ? (int64_t)p.out_perm[b] : (int64_t)b)) * p.vc + idx] = make_double2(total * p.scale, 0.0);
                             }
                         }
                     }
@@ -848,7 +849,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 1 : 2) response_kernel(R
                                     neumaier_add(a4[1], a4[3], v.y * wk);
                                 }
                             } else {
-                                p.out_points[(p.point_offset + b) * p.vc + idx] = cscale(v, p.scale);
+                                p.out_points[(p.point_offset + (p.out_perm ? (int64_t)p.out_perm[b] : (int64_t)b)) * p.vc + idx] = cscale(v, p.scale);
                             }
                         }
                     }

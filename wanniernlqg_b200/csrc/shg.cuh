@@ -53,6 +53,7 @@ struct ShgParams {
     double *partials;
     double2 *out_points;
     int64_t point_offset;
+    const int *out_perm;         // mode 1: batch entry b is written to row out_perm[b]; nullptr: row b
     double2 *scratch;            // per CTA: G[9][nn] | coef[nn][nc][7] | pinfo[nn] (fo, inv, diff, 0)
     int64_t scratch_stride;      // double2 entries per CTA
     unsigned char *gscratch;     // per-CTA matrix working set in global memory (large nw); nullptr: shared
@@ -144,7 +145,7 @@ WNLQG_D void shg_emit(const ShgParams &p, int64_t b, int64_t idx, double2 v, dou
         neumaier_add(a4[0], a4[2], v.x * wk);
         neumaier_add(a4[1], a4[3], v.y * wk);
     } else {
-        p.out_points[(p.point_offset + b) * p.vc + idx] = cscale(v, p.scale);
+        p.out_points[(p.point_offset + (p.out_perm ? (int64_t)p.out_perm[b] : b)) * p.vc + idx] = cscale(v, p.scale);
     }
 }
 

@@ -26,6 +26,8 @@
 #include "shg.cuh"
 #include "tc_fourier.cuh"
 #include "nonorth.cuh"
+#include "order.cuh"
+#include <cub/device/device_radix_sort.cuh>
 
 namespace {
 
@@ -146,6 +148,15 @@ struct wnlqg_plan {
     int sm_count = 148;
     size_t refine_smem = 0;
     float2 *d_V32 = nullptr;
+    // Morton ordering of arbitrary k-point batches (team eigensolver plans): keys and indices
+    // (two halves each, radix-sort input and output), the ordered k-points and weights, and the
+    // sort's temporary storage.
+    bool order_points = false;
+    uint32_t *d_okeys = nullptr;
+    int *d_operm = nullptr;
+    double *d_ok = nullptr, *d_ow = nullptr;
+    void *d_osort_tmp = nullptr;
+    size_t osort_bytes = 0;
     cudaStream_t stream = nullptr;
     std::vector<cudaEvent_t> events;
     size_t timing_batches = 0;
@@ -691,7 +702,7 @@ wnlqg_status setup_tc_fourier(wnlqg_plan *pl, const std::vector<double2> &tiles)
 
 // One batch: phases, Fourier GEMM, eigensolve.  kpts_device == nullptr selects mesh mode.
 wnlqg_status run_front(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const int64_t *mesh, const double *kpts_device,
-                       size_t ev_base, const int64_t *kidx_device = nullptr) {
+                       size_t ev_base, const int64_t *kidx_device = nullptr, bool ordered = false) {
     const int nr = pl->nr;
     int64_t N = (int64_t)pl->C * pl->nn;
     const bool staged = mesh != nullptr && kpts_device == nullptr && kidx_device == nullptr && pl->P1 <= STAGED_MAX_P1 &&
@@ -766,7 +777,8 @@ wnlqg_status run_front(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const int64_
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f32_fn, f32_threads, pl->eigh_smem);
         const int64_t f32_grid = std::min<int64_t>((nb + f32_teams - 1) / f32_teams, (int64_t)std::max(1, per_sm) * pl->sm_count);
         // Consecutive mesh points are neighbours: warm-start the Jacobi iteration along the run.
-        int warm = (mesh != nullptr && kpts_device == nullptr && kidx_device == nullptr) ? 1 : 0;
+        // Arbitrary points in Morton order (ordered) are neighbours along the run as well.
+        int warm = ((mesh != nullptr && kpts_device == nullptr && kidx_device == nullptr) || ordered) ? 1 : 0;
         const double2 *hk = pl->d_xw + (int64_t)pl->ch_H * pl->nn;
         {
             int64_t nb_arg = nb;
@@ -831,7 +843,7 @@ wnlqg_status run_front(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const int64_
 }
 
 wnlqg_status run_passes(wnlqg_plan *pl, int64_t nb, int mode, double scale, int64_t point_offset,
-                        const double *weights = nullptr) {
+                        const double *weights = nullptr, const int *out_perm = nullptr) {
     if (pl->nonorth && !pl->passes.empty()) {
         NonorthParams q = pl->ng;
         q.batch = nb;
@@ -860,6 +872,7 @@ wnlqg_status run_passes(wnlqg_plan *pl, int64_t nb, int mode, double scale, int6
         p.partials = pl->d_partials;
         p.out_points = pl->d_points;
         p.point_offset = point_offset;
+        p.out_perm = out_perm;
         p.gscratch = ps.global ? pl->d_resp_scratch : nullptr;
         p.gscratch_stride = pl->resp_scratch_stride;
         const size_t launch_smem = ps.global ? 0 : ps.smem;
@@ -895,6 +908,7 @@ wnlqg_status run_passes(wnlqg_plan *pl, int64_t nb, int mode, double scale, int6
         p.partials = pl->d_partials;
         p.out_points = pl->d_points;
         p.point_offset = point_offset;
+        p.out_perm = out_perm;
         p.scratch = pl->d_shg_scratch;
         p.gscratch = pl->d_shg_gscratch;
         if (pl->shg_global) shg_kernel<true><<<pl->shg_grid, 256, pl->shg_smem, pl->stream>>>(p);
@@ -1012,7 +1026,8 @@ wnlqg_status wnlqg_b200_plan_destroy(wnlqg_plan *pl) {
                       (void *)pl->d_shg_scratch, (void *)pl->d_tcA, (void *)pl->d_tcB, (void *)pl->d_tc_colscale,
                       (void *)pl->d_tc_err, (void *)pl->d_shg_gscratch, (void *)pl->d_eigh_scratch,
                       (void *)pl->d_resp_scratch, (void *)pl->d_ng_r, (void *)pl->d_ng_v, (void *)pl->d_ng_G,
-                      (void *)pl->d_ng_ws, (void *)pl->d_mshg_src, (void *)pl->d_mshg_diag, (void *)pl->d_mshg_ws})
+                      (void *)pl->d_ng_ws, (void *)pl->d_mshg_src, (void *)pl->d_mshg_diag, (void *)pl->d_mshg_ws,
+                      (void *)pl->d_okeys, (void *)pl->d_operm, (void *)pl->d_ok, (void *)pl->d_ow, pl->d_osort_tmp})
         if (ptr) cudaFree(ptr);
     for (cudaEvent_t ev : pl->events) cudaEventDestroy(ev);
     if (pl->stream) cudaStreamDestroy(pl->stream);
@@ -1517,6 +1532,22 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
         pl->refine_threads = std::max(pl->refine_threads, ((np / 2 + 31) / 32) * 32);
         pl->eigh_threads = pl->refine_threads;
         if ((st = alloc((void **)&pl->d_V32, (size_t)max_batch * np * np * sizeof(float2))) != WNLQG_OK) return bail(st);
+        // Arbitrary k-point batches are put in Morton order so that the FP32 stage can warm-start
+        // along them (WNLQG_B200_POINT_ORDER=0 keeps the caller's order and cold starts).
+        const char *ord = std::getenv("WNLQG_B200_POINT_ORDER");
+        if (!(ord && ord[0] == '0') && max_batch < ((int64_t)1 << 31)) {
+            size_t tmp = 0;
+            cudaError_t ce = cub::DeviceRadixSort::SortPairs(nullptr, tmp, (const uint32_t *)nullptr, (uint32_t *)nullptr,
+                                                             (const int *)nullptr, (int *)nullptr, (int)max_batch, 0, 30);
+            if (ce != cudaSuccess) return bail(fail(WNLQG_ERR_CUDA, std::string("radix sort sizing: ") + cudaGetErrorString(ce)));
+            if ((st = alloc((void **)&pl->d_okeys, 2 * (size_t)max_batch * sizeof(uint32_t))) != WNLQG_OK) return bail(st);
+            if ((st = alloc((void **)&pl->d_operm, 2 * (size_t)max_batch * sizeof(int))) != WNLQG_OK) return bail(st);
+            if ((st = alloc((void **)&pl->d_ok, (size_t)max_batch * 3 * sizeof(double))) != WNLQG_OK) return bail(st);
+            if ((st = alloc((void **)&pl->d_ow, (size_t)max_batch * sizeof(double))) != WNLQG_OK) return bail(st);
+            if ((st = alloc(&pl->d_osort_tmp, tmp)) != WNLQG_OK) return bail(st);
+            pl->osort_bytes = std::max<size_t>(tmp, 16);
+            pl->order_points = true;
+        }
         cudaError_t e = allow_dynamic_smem((const void *)eigh_refine_f64_team_kernel<32>, smem_optin);
         if (e == cudaSuccess) e = allow_dynamic_smem((const void *)eigh_refine_f64_team_kernel<64>, smem_optin);
         if (e == cudaSuccess) e = allow_dynamic_smem((const void *)eigh_refine_f64_team_kernel<128>, smem_optin);
@@ -1597,6 +1628,23 @@ int64_t wnlqg_b200_plan_value_count(const wnlqg_plan *plan) { return plan ? plan
 }  // extern "C"
 
 namespace {
+
+// Morton order of nb device k-points (and weights, when given): afterwards pl->d_ok (and d_ow)
+// hold them in that order and pl->d_operm + max_batch the original row of each ordered entry.
+wnlqg_status order_batch(wnlqg_plan *pl, const double *k, const double *w, int64_t nb) {
+    if (nb <= 0) return WNLQG_OK;
+    uint32_t *keys_in = pl->d_okeys, *keys_out = pl->d_okeys + pl->max_batch;
+    int *idx_in = pl->d_operm, *idx_out = pl->d_operm + pl->max_batch;
+    const unsigned blocks = (unsigned)((nb + 255) / 256);
+    morton_keys_kernel<<<blocks, 256, 0, pl->stream>>>(k, nb, keys_in, idx_in);
+    size_t tmp = pl->osort_bytes;
+    WNLQG_CUDA(cub::DeviceRadixSort::SortPairs(pl->d_osort_tmp, tmp, keys_in, keys_out, idx_in, idx_out, (int)nb, 0, 30,
+                                               pl->stream));
+    gather_points_kernel<<<blocks, 256, 0, pl->stream>>>(k, w, idx_out, nb, pl->d_ok, pl->d_ow);
+    pl->launches += 2;
+    WNLQG_CUDA(cudaGetLastError());
+    return WNLQG_OK;
+}
 
 wnlqg_status check_mesh_args(wnlqg_plan *pl, const int64_t mesh[3], int64_t k_begin, int64_t k_end, const double *out) {
     wnlqg_status st = check_plan(pl);
@@ -1704,8 +1752,15 @@ wnlqg_status enqueue_points_weighted(wnlqg_plan *pl, const double *kpoints_devic
         const int64_t nb = std::min(pl->max_batch, n - s);
         const size_t base = 1 + 3 * nbatch;
         if ((st = record_event(pl, base)) != WNLQG_OK) return st;
-        if ((st = run_front(pl, nb, 0, nullptr, kpoints_device + 3 * s, base)) != WNLQG_OK) return st;
-        if ((st = run_passes(pl, nb, 0, 1.0, 0, weights_device + s)) != WNLQG_OK) return st;
+        const double *kb = kpoints_device + 3 * s, *wb = weights_device + s;
+        const bool ord = pl->order_points && nb > 1;
+        if (ord) {
+            if ((st = order_batch(pl, kb, wb, nb)) != WNLQG_OK) return st;
+            kb = pl->d_ok;
+            wb = pl->d_ow;
+        }
+        if ((st = run_front(pl, nb, 0, nullptr, kb, base, nullptr, ord)) != WNLQG_OK) return st;
+        if ((st = run_passes(pl, nb, 0, 1.0, 0, wb)) != WNLQG_OK) return st;
     }
     const size_t final_ev = 1 + 3 * nbatch;
     if ((st = record_event(pl, final_ev)) != WNLQG_OK) return st;
@@ -1815,8 +1870,11 @@ wnlqg_status wnlqg_b200_eval_points(wnlqg_plan *pl, const double *kpoints, int64
         int64_t nb = std::min(pl->max_batch, n - s);
         WNLQG_CUDA(cudaMemcpyAsync(pl->d_kpts, kpoints + 3 * s, (size_t)nb * 3 * sizeof(double), cudaMemcpyHostToDevice,
                                    pl->stream));
-        if ((st = run_front(pl, nb, 0, nullptr, pl->d_kpts, 1)) != WNLQG_OK) return st;
-        if ((st = run_passes(pl, nb, 1, 1.0, 0)) != WNLQG_OK) return st;
+        const bool ord = pl->order_points && nb > 1;
+        if (ord && (st = order_batch(pl, pl->d_kpts, nullptr, nb)) != WNLQG_OK) return st;
+        if ((st = run_front(pl, nb, 0, nullptr, ord ? pl->d_ok : pl->d_kpts, 1, nullptr, ord)) != WNLQG_OK) return st;
+        if ((st = run_passes(pl, nb, 1, 1.0, 0, nullptr, ord ? pl->d_operm + pl->max_batch : nullptr)) != WNLQG_OK)
+            return st;
         WNLQG_CUDA(cudaMemcpyAsync(out + 2 * s * pl->vc, pl->d_points, (size_t)nb * pl->vc * sizeof(double2),
                                    cudaMemcpyDeviceToHost, pl->stream));
     }
@@ -1844,8 +1902,10 @@ wnlqg_status wnlqg_b200_eval_points_weighted(wnlqg_plan *pl, const double *kpoin
                                    pl->stream));
         WNLQG_CUDA(cudaMemcpyAsync(pl->d_weights, weights + s, (size_t)nb * sizeof(double), cudaMemcpyHostToDevice,
                                    pl->stream));
-        if ((st = run_front(pl, nb, 0, nullptr, pl->d_kpts, 1)) != WNLQG_OK) return st;
-        if ((st = run_passes(pl, nb, 0, 1.0, 0, pl->d_weights)) != WNLQG_OK) return st;
+        const bool ord = pl->order_points && nb > 1;
+        if (ord && (st = order_batch(pl, pl->d_kpts, pl->d_weights, nb)) != WNLQG_OK) return st;
+        if ((st = run_front(pl, nb, 0, nullptr, ord ? pl->d_ok : pl->d_kpts, 1, nullptr, ord)) != WNLQG_OK) return st;
+        if ((st = run_passes(pl, nb, 0, 1.0, 0, ord ? pl->d_ow : pl->d_weights)) != WNLQG_OK) return st;
     }
     reduce_partials_kernel<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((pl->vc + 255) / 256, 1024)), 256, 0,
                              pl->stream>>>(pl->d_partials, pl->partial_slots, pl->vc, pl->d_out);
