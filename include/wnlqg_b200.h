@@ -296,8 +296,10 @@ WNLQG_API wnlqg_status wnlqg_b200_graph_destroy(wnlqg_graph *graph);
 
 /* ---- Autotuner (no reference counterpart) -------------------------------------------------
  * Measures, on the mesh block [k_begin, k_end) of `mesh`, every eigensolver team size (32, 64 and
- * 128 threads per matrix; orthogonal models up to 32 orbitals) and every contraction tile (1, 2
- * and 4 photon energies per thread; frequency-resolved responses), keeps the fastest of each in
+ * 128 threads per matrix; orthogonal models up to 32 orbitals), the FP32 eigensolver stage's
+ * start (warm from the previous point along mesh runs and ordered batches, or cold from the
+ * identity; orthogonal models on the team or CTA mixed-precision stages) and every contraction
+ * tile (1, 2 and 4 photon energies per thread; frequency-resolved responses), keeps the fastest of each in
  * the plan and remembers it for the process (key: device, orbitals, precision, geometry, photon
  * energies, value count), so later plans with the same key take it without measuring.  Every
  * candidate is a configuration the library runs anyway; the tile choice leaves results bitwise
@@ -309,6 +311,8 @@ typedef struct wnlqg_autotune_report {
     double eigh_ms[3];             /* eigensolve time with 32, 64, 128 threads per matrix */
     double response_ms[3];         /* response time with 1, 2, 4 energies per thread */
     int32_t from_cache;            /* 1 when the choice came from the process cache */
+    int32_t warm_start;            /* chosen FP32 start: 1 warm, 0 cold, -1 = not tunable */
+    double start_ms[2];            /* eigensolve time with a cold and a warm start */
 } wnlqg_autotune_report;
 WNLQG_API wnlqg_status wnlqg_b200_plan_autotune(wnlqg_plan *plan, const int64_t mesh[3], int64_t k_begin,
                                       int64_t k_end, wnlqg_autotune_report *report);

@@ -109,6 +109,8 @@ struct AutotuneReport
     eigh_ms::NTuple{3, Float64}
     response_ms::NTuple{3, Float64}
     from_cache::Int32
+    warm_start::Int32
+    start_ms::NTuple{2, Float64}
 end
 
 """Pick the eigensolver team and contraction tile by timing them on mesh indices [first, last)."""

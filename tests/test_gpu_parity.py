@@ -720,3 +720,32 @@ def test_morton_ordered_points_match_caller_order(engine_cls, oracle_mod, precis
     ref = oracle_mod.point_values(model, task, k[pick])
     for g, r in zip(task.split(vals[pick]), task.split(ref)):
         assert rel_err(g, r) < (RTOL if precision == _abi.PRECISION_FP64 else 1e-4)
+
+
+@pytest.mark.parametrize("nw,precision", [(48, _abi.PRECISION_MIXED), (64, _abi.PRECISION_FP64)])
+def test_large_nw_warm_started_ranges_match_cta_jacobi(engine_cls, nw, precision, monkeypatch):
+    """Above 32 orbitals each FP32 CTA takes a contiguous range of points and warm-starts along
+    it (mesh runs, Morton-ordered point batches): a 2048-point mesh block and a 3000-point
+    weighted sum agree with the FP64 CTA Jacobi (WNLQG_B200_CTA_EIGH=1) to 1e-11 (FP64 path) or
+    the mixed path's bound."""
+    monkeypatch.setenv("WNLQG_B200_DIRECT_FOURIER", "1")
+    model = synthetic_orthogonal_model(nw, 1, seed=nw + 5, full_position=True)
+    kw = dict(broadening_type=_abi.LORENTZIAN, broadening=0.03, photon_energies=np.linspace(0, 3, 16))
+    task = _abi.TaskArrays([(_abi.SHIFT_CURRENT, ["xyy"]), (_abi.QUANTUM_METRIC, ["xx"])], precision=precision, **kw)
+    ref_task = _abi.TaskArrays([(_abi.SHIFT_CURRENT, ["xyy"]), (_abi.QUANTUM_METRIC, ["xx"])], **kw)
+    rng = np.random.default_rng(nw + 9)
+    k = rng.random((3000, 3))
+    w = rng.random(3000) / 3000
+    mesh = (16, 16, 16)
+    with engine_cls(model, task) as eng:
+        m = eng.integrate_mesh(mesh, 1024, 3072)
+        s = eng.weighted_sum(k, w)
+    monkeypatch.setenv("WNLQG_B200_CTA_EIGH", "1")
+    with engine_cls(model, ref_task) as eng:
+        m_ref = eng.integrate_mesh(mesh, 1024, 3072)
+        s_ref = eng.weighted_sum(k, w)
+    rtol = 1e-11 if precision == _abi.PRECISION_FP64 else MIXED_RTOL
+    for g, r in zip(task.split(m), task.split(m_ref)):
+        assert rel_err(g, r) < rtol
+    for g, r in zip(task.split(s), task.split(s_ref)):
+        assert rel_err(g, r) < rtol

@@ -70,6 +70,8 @@ class AutotuneReport(ctypes.Structure):
         ("eigh_ms", ctypes.c_double * 3),
         ("response_ms", ctypes.c_double * 3),
         ("from_cache", ctypes.c_int32),
+        ("warm_start", ctypes.c_int32),
+        ("start_ms", ctypes.c_double * 2),
     ]
 
 

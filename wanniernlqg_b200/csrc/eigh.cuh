@@ -683,7 +683,9 @@ __global__ void __launch_bounds__(TEAM == 128 ? 128 : 64, TEAM == 32 ? 1 : 6) ei
 // Mixed-precision eigensolver above 32 orbitals, one CTA per matrix, in two kernels (the same
 // scheme as the team kernels, for matrices a warp team cannot hold):
 //   stage 1 (jacobi_f32_cta_kernel): FP32 parallel Jacobi until the off-diagonal norm is below
-//     2^-17 ||H|| (rotating elements above 2^-20 ||H||), eigenvectors written unsorted;
+//     2^-17 ||H|| (rotating elements above 2^-20 ||H||), eigenvectors written unsorted; each CTA
+//     takes a contiguous range of points and, along mesh runs and Morton-ordered point batches,
+//     warm-starts each point from the previous one's eigenvectors;
 //   stage 2 (eigh_refine_f64_cta_kernel): W = second-order Loewdin orthonormalisation of V
 //     (E = W^H W - I, W <- W (I - E/2 + 3E^2/8)), H' = W^H H W, FP64 Jacobi sweeps (mixed path:
 //     one, unless H' is diagonal to 1e-13 ||H||; FP64 path: until the FP64 CTA Jacobi's stopping
@@ -692,10 +694,29 @@ __global__ void __launch_bounds__(TEAM == 128 ? 128 : 64, TEAM == 32 ? 1 : 6) ei
 // GW: the working set lives in global memory (gscratch, one stride per CTA) when it does not fit
 // shared memory.
 // ---------------------------------------------------------------------------------------------
+// out = op(X) Y for np x np FP32 complex matrices with leading dimensions ldx, ldy, ldo (either
+// input may live in global memory), op = conjugate transpose when xh; the CTA's threads take
+// out's elements in turn, rows fastest.
+WNLQG_D void cta_product_f32(const float2 *X, int ldx, const float2 *Y, int ldy, float2 *out, int ldo, int np, bool xh) {
+    for (int e = threadIdx.x; e < np * np; e += blockDim.x) {
+        const int i = e % np, j = e / np;
+        float2 acc = make_float2(0.0f, 0.0f);
+        if (xh)
+            for (int l = 0; l < np; ++l) acc = cfmaconj(X[l + ldx * i], Y[l + ldy * j], acc);
+        else
+            for (int l = 0; l < np; ++l) acc = cfma(X[i + ldx * l], Y[l + ldy * j], acc);
+        out[i + ldo * j] = acc;
+    }
+}
+
+// Each CTA takes a contiguous range of the batch.  warm_start: every point after the first of the
+// range starts from the previous point's eigenvectors Vp (already in V_out; this point's V_out
+// slot serves as the scratch W): W = Vp (3I - Vp^H Vp)/2, A = W^H H W, V = W.
 template <bool GW>
 __global__ void __launch_bounds__(256, 3) jacobi_f32_cta_kernel(const double2 *__restrict__ h_in, int64_t h_stride,
-                                                              int64_t batch, int nw, float2 *__restrict__ V_out,
-                                                              unsigned char *gscratch, int64_t gscratch_stride) {
+                                                              int64_t batch, int nw, float2 *V_out,
+                                                              unsigned char *gscratch, int64_t gscratch_stride,
+                                                              int warm_start) {
     extern __shared__ __align__(16) unsigned char smem_dyn[];
     unsigned char *smraw;
     if constexpr (GW) smraw = gscratch + (int64_t)blockIdx.x * gscratch_stride;
@@ -713,8 +734,24 @@ __global__ void __launch_bounds__(256, 3) jacobi_f32_cta_kernel(const double2 *_
     __shared__ double red[48];
     __shared__ int rot_flag;
     const int tid = threadIdx.x;
-    for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) {
+    const int64_t nn = (int64_t)np * np;
+    const int64_t kb = (batch * (int64_t)blockIdx.x) / gridDim.x, ke = (batch * ((int64_t)blockIdx.x + 1)) / gridDim.x;
+    for (int64_t b = kb; b < ke; ++b) {
         const double2 *h = h_in + b * h_stride;
+        const bool warm = warm_start && b > kb;
+        float2 *Wg = V_out + b * nn;
+        const float2 *Vp = warm ? V_out + (b - 1) * nn : nullptr;
+        if (warm) {
+            cta_product_f32(Vp, np, Vp, np, V, ld, np, true);                  // V <- Vp^H Vp
+            __syncthreads();
+            for (int e = tid; e < np * np; e += blockDim.x) {                   // V <- M = (3I - V)/2
+                const int i = e % np, j = e / np;
+                const float2 m = V[i + ld * j];
+                V[i + ld * j] = make_float2((i == j ? 1.5f : 0.0f) - 0.5f * m.x, -0.5f * m.y);
+            }
+            __syncthreads();
+            cta_product_f32(Vp, np, V, ld, Wg, np, np, false);                 // W <- Vp M (global)
+        }
         double local = 0.0;
         for (int e = tid; e < np * np; e += blockDim.x) {
             const int i = e % np, j = e / np;
@@ -726,7 +763,7 @@ __global__ void __launch_bounds__(256, 3) jacobi_f32_cta_kernel(const double2 *_
             }
             local += v.x * v.x + v.y * v.y;
             A[i + ld * j] = make_float2((float)v.x, (float)v.y);
-            V[i + ld * j] = make_float2(i == j ? 1.0f : 0.0f, 0.0f);
+            if (!warm) V[i + ld * j] = make_float2(i == j ? 1.0f : 0.0f, 0.0f);
         }
         for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xffffffffu, local, o);
         if ((tid & 31) == 0) red[tid >> 5] = local;
@@ -737,6 +774,19 @@ __global__ void __launch_bounds__(256, 3) jacobi_f32_cta_kernel(const double2 *_
             scratch[0] = sqrt(s);
         }
         __syncthreads();
+        if (warm) {
+            cta_product_f32(A, ld, Wg, np, V, ld, np, false);                  // V <- H W
+            __syncthreads();
+            cta_product_f32(Wg, np, V, ld, A, ld, np, true);                   // A <- W^H H W
+            __syncthreads();
+            for (int e = tid; e < np * np; e += blockDim.x) {                   // V <- W; A Hermitian
+                const int i = e % np, j = e / np;
+                V[i + ld * j] = Wg[i + (int64_t)np * j];
+                if (i > j) A[i + ld * j] = cconj(A[j + ld * i]);
+                else if (i == j) A[i + ld * i].y = 0.0f;
+            }
+            __syncthreads();
+        }
         const double fro = scratch[0];
         const float tol32 = (float)(fro * 9.5367431640625e-07);
         for (int sweep = 0; sweep < WNLQG_JACOBI_MAX_SWEEPS; ++sweep) {
@@ -748,10 +798,9 @@ __global__ void __launch_bounds__(256, 3) jacobi_f32_cta_kernel(const double2 *_
             __syncthreads();
             if (!any) break;
         }
-        float2 *vo = V_out + b * (int64_t)np * np;
         for (int e = tid; e < np * np; e += blockDim.x) {
             const int i = e % np, j = e / np;
-            vo[i + (int64_t)np * j] = V[i + ld * j];
+            Wg[i + (int64_t)np * j] = V[i + ld * j];
         }
         __syncthreads();
     }

@@ -152,6 +152,9 @@ struct wnlqg_plan {
     // (two halves each, radix-sort input and output), the ordered k-points and weights, and the
     // sort's temporary storage.
     bool order_points = false;
+    // FP32 eigensolver stages warm-start along mesh runs and ordered batches (1) or always start
+    // from the identity (0): WNLQG_B200_WARM_START at plan creation, then the autotuner.
+    int warm_mode = 1;
     uint32_t *d_okeys = nullptr;
     int *d_operm = nullptr;
     double *d_ok = nullptr, *d_ow = nullptr;
@@ -778,7 +781,7 @@ wnlqg_status run_front(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const int64_
         const int64_t f32_grid = std::min<int64_t>((nb + f32_teams - 1) / f32_teams, (int64_t)std::max(1, per_sm) * pl->sm_count);
         // Consecutive mesh points are neighbours: warm-start the Jacobi iteration along the run.
         // Arbitrary points in Morton order (ordered) are neighbours along the run as well.
-        int warm = ((mesh != nullptr && kpts_device == nullptr && kidx_device == nullptr) || ordered) ? 1 : 0;
+        int warm = pl->warm_mode && ((mesh != nullptr && kpts_device == nullptr && kidx_device == nullptr) || ordered) ? 1 : 0;
         const double2 *hk = pl->d_xw + (int64_t)pl->ch_H * pl->nn;
         {
             int64_t nb_arg = nb;
@@ -805,15 +808,18 @@ wnlqg_status run_front(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const int64_
     } else if (pl->cta_mixed) {
         const double2 *hk = pl->d_xw + (int64_t)pl->ch_H * pl->nn;
         const int converge = pl->task.precision == WNLQG_PRECISION_MIXED ? 0 : 1;
+        // Mesh runs and Morton-ordered point batches warm-start along each CTA's range.
+        const int warm =
+            pl->warm_mode && ((mesh != nullptr && kpts_device == nullptr && kidx_device == nullptr) || ordered) ? 1 : 0;
         if (pl->cta_gw1) {
             jacobi_f32_cta_kernel<true><<<(unsigned)std::min<int64_t>(nb, pl->eigh_grid), 256, 0, pl->stream>>>(
-                hk, N, nb, pl->nw, pl->d_V32, pl->d_eigh_scratch, pl->eigh_scratch_stride);
+                hk, N, nb, pl->nw, pl->d_V32, pl->d_eigh_scratch, pl->eigh_scratch_stride, warm);
         } else {
             int per_sm = 1;
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jacobi_f32_cta_kernel<false>, 256, pl->eigh_smem);
             const int64_t grid = std::min<int64_t>(nb, (int64_t)std::max(1, per_sm) * pl->sm_count);
             jacobi_f32_cta_kernel<false><<<(unsigned)grid, 256, pl->eigh_smem, pl->stream>>>(hk, N, nb, pl->nw, pl->d_V32,
-                                                                                            nullptr, 0);
+                                                                                            nullptr, 0, warm);
         }
         if (pl->cta_gw2) {
             eigh_refine_f64_cta_kernel<true><<<(unsigned)std::min<int64_t>(nb, pl->eigh_grid), pl->refine_cta_threads, 0, pl->stream>>>(
@@ -1485,6 +1491,29 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
         pl->groups.q1_r1 = base;
     }
 
+    // Arbitrary k-point batches are put in Morton order so that the FP32 eigensolver stage can
+    // warm-start along them (WNLQG_B200_POINT_ORDER=0 keeps the caller's order and cold starts).
+    {
+        const char *wm = std::getenv("WNLQG_B200_WARM_START");
+        pl->warm_mode = (wm && wm[0] == '0') ? 0 : 1;
+    }
+    auto alloc_ordering = [&]() -> wnlqg_status {
+        const char *ord = std::getenv("WNLQG_B200_POINT_ORDER");
+        if ((ord && ord[0] == '0') || max_batch >= ((int64_t)1 << 31)) return WNLQG_OK;
+        size_t tmp = 0;
+        cudaError_t ce = cub::DeviceRadixSort::SortPairs(nullptr, tmp, (const uint32_t *)nullptr, (uint32_t *)nullptr,
+                                                         (const int *)nullptr, (int *)nullptr, (int)max_batch, 0, 30);
+        if (ce != cudaSuccess) return fail(WNLQG_ERR_CUDA, std::string("radix sort sizing: ") + cudaGetErrorString(ce));
+        wnlqg_status s2;
+        if ((s2 = alloc((void **)&pl->d_okeys, 2 * (size_t)max_batch * sizeof(uint32_t))) != WNLQG_OK) return s2;
+        if ((s2 = alloc((void **)&pl->d_operm, 2 * (size_t)max_batch * sizeof(int))) != WNLQG_OK) return s2;
+        if ((s2 = alloc((void **)&pl->d_ok, (size_t)max_batch * 3 * sizeof(double))) != WNLQG_OK) return s2;
+        if ((s2 = alloc((void **)&pl->d_ow, (size_t)max_batch * sizeof(double))) != WNLQG_OK) return s2;
+        if ((s2 = alloc(&pl->d_osort_tmp, tmp)) != WNLQG_OK) return s2;
+        pl->osort_bytes = std::max<size_t>(tmp, 16);
+        pl->order_points = true;
+        return WNLQG_OK;
+    };
     pl->eigh_threads = eigh_block_threads(nw);
     // Up to 32 orbitals (orthogonal models) both precisions use the warp eigensolver: FP32 Jacobi,
     // then FP64 refinement (one sweep on the mixed path, sweeps to FP64 convergence on the FP64
@@ -1532,22 +1561,7 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
         pl->refine_threads = std::max(pl->refine_threads, ((np / 2 + 31) / 32) * 32);
         pl->eigh_threads = pl->refine_threads;
         if ((st = alloc((void **)&pl->d_V32, (size_t)max_batch * np * np * sizeof(float2))) != WNLQG_OK) return bail(st);
-        // Arbitrary k-point batches are put in Morton order so that the FP32 stage can warm-start
-        // along them (WNLQG_B200_POINT_ORDER=0 keeps the caller's order and cold starts).
-        const char *ord = std::getenv("WNLQG_B200_POINT_ORDER");
-        if (!(ord && ord[0] == '0') && max_batch < ((int64_t)1 << 31)) {
-            size_t tmp = 0;
-            cudaError_t ce = cub::DeviceRadixSort::SortPairs(nullptr, tmp, (const uint32_t *)nullptr, (uint32_t *)nullptr,
-                                                             (const int *)nullptr, (int *)nullptr, (int)max_batch, 0, 30);
-            if (ce != cudaSuccess) return bail(fail(WNLQG_ERR_CUDA, std::string("radix sort sizing: ") + cudaGetErrorString(ce)));
-            if ((st = alloc((void **)&pl->d_okeys, 2 * (size_t)max_batch * sizeof(uint32_t))) != WNLQG_OK) return bail(st);
-            if ((st = alloc((void **)&pl->d_operm, 2 * (size_t)max_batch * sizeof(int))) != WNLQG_OK) return bail(st);
-            if ((st = alloc((void **)&pl->d_ok, (size_t)max_batch * 3 * sizeof(double))) != WNLQG_OK) return bail(st);
-            if ((st = alloc((void **)&pl->d_ow, (size_t)max_batch * sizeof(double))) != WNLQG_OK) return bail(st);
-            if ((st = alloc(&pl->d_osort_tmp, tmp)) != WNLQG_OK) return bail(st);
-            pl->osort_bytes = std::max<size_t>(tmp, 16);
-            pl->order_points = true;
-        }
+        if ((st = alloc_ordering()) != WNLQG_OK) return bail(st);
         cudaError_t e = allow_dynamic_smem((const void *)eigh_refine_f64_team_kernel<32>, smem_optin);
         if (e == cudaSuccess) e = allow_dynamic_smem((const void *)eigh_refine_f64_team_kernel<64>, smem_optin);
         if (e == cudaSuccess) e = allow_dynamic_smem((const void *)eigh_refine_f64_team_kernel<128>, smem_optin);
@@ -1569,6 +1583,7 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
         pl->refine_cta_threads =
             (!pl->cta_gw2 && 2 * (pl->refine_smem + fa2.sharedSizeBytes) <= (size_t)smem_optin) ? 256 : 512;
         if ((st = alloc((void **)&pl->d_V32, (size_t)max_batch * np * np * sizeof(float2))) != WNLQG_OK) return bail(st);
+        if ((st = alloc_ordering()) != WNLQG_OK) return bail(st);
         if (pl->cta_gw1 || pl->cta_gw2) {
             const size_t need = std::max(pl->cta_gw1 ? pl->eigh_smem : 0, pl->cta_gw2 ? pl->refine_smem : 0);
             pl->eigh_scratch_stride = (int64_t)((need + 255) & ~(size_t)255);
@@ -2217,7 +2232,7 @@ wnlqg_status wnlqg_b200_graph_destroy(wnlqg_graph *graph) {
 // ---------------------------------------------------------------------------------------------
 namespace {
 
-struct TuneChoice { int team; int omb; wnlqg_autotune_report report; };
+struct TuneChoice { int team; int omb; int warm; wnlqg_autotune_report report; };
 std::map<std::tuple<int, int, int, int, int64_t, int64_t>, TuneChoice> g_tune_cache;
 std::mutex g_tune_mutex;
 
@@ -2263,6 +2278,7 @@ extern "C" wnlqg_status wnlqg_b200_plan_autotune(wnlqg_plan *pl, const int64_t m
         auto it = g_tune_cache.find(key);
         if (it != g_tune_cache.end()) {
             if (pl->warp_eigh && it->second.team) apply_team(pl, it->second.team);
+            if (it->second.warm >= 0) pl->warm_mode = it->second.warm;
             apply_omb(pl, it->second.omb);
             if (report) {
                 *report = it->second.report;
@@ -2274,6 +2290,8 @@ extern "C" wnlqg_status wnlqg_b200_plan_autotune(wnlqg_plan *pl, const int64_t m
     wnlqg_autotune_report rep;
     std::memset(&rep, 0, sizeof(rep));
     for (int i = 0; i < 3; ++i) rep.eigh_ms[i] = rep.response_ms[i] = -1.0;
+    rep.warm_start = -1;
+    rep.start_ms[0] = rep.start_ms[1] = -1.0;
     const int teams[3] = {32, 64, 128}, ombs[3] = {1, 2, 4};
     if (pl->warp_eigh) {
         const int start = pl->eigh_team;
@@ -2289,6 +2307,19 @@ extern "C" wnlqg_status wnlqg_b200_plan_autotune(wnlqg_plan *pl, const int64_t m
         }
         apply_team(pl, best);
         rep.eigh_team = best;
+    }
+    if (pl->warp_eigh || pl->cta_mixed) {
+        const int start = pl->warm_mode;
+        double r = 0;
+        for (int w = 0; w < 2; ++w) {
+            pl->warm_mode = w;
+            if ((st = tune_measure(pl, mesh, k_begin, k_end, &rep.start_ms[w], &r)) != WNLQG_OK) {
+                pl->warm_mode = start;
+                return st;
+            }
+        }
+        pl->warm_mode = rep.start_ms[1] <= rep.start_ms[0] ? 1 : 0;
+        rep.warm_start = pl->warm_mode;
     }
     bool freq = false;
     for (const Pass &ps : pl->passes) freq |= ps.params.n_fc > 0 && ps.params.nom > 0;
@@ -2308,7 +2339,7 @@ extern "C" wnlqg_status wnlqg_b200_plan_autotune(wnlqg_plan *pl, const int64_t m
     }
     {
         std::lock_guard<std::mutex> lock(g_tune_mutex);
-        g_tune_cache[key] = TuneChoice{rep.eigh_team, rep.energies_per_thread, rep};
+        g_tune_cache[key] = TuneChoice{rep.eigh_team, rep.energies_per_thread, rep.warm_start, rep};
     }
     if (report) *report = rep;
     return WNLQG_OK;

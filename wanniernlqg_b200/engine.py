@@ -167,6 +167,8 @@ class ResponseEngine:
         return {"eigh_team": rep.eigh_team, "energies_per_thread": rep.energies_per_thread,
                 "eigh_ms": {t: rep.eigh_ms[i] for i, t in enumerate((32, 64, 128)) if rep.eigh_ms[i] >= 0},
                 "response_ms": {t: rep.response_ms[i] for i, t in enumerate((1, 2, 4)) if rep.response_ms[i] >= 0},
+                "warm_start": rep.warm_start,
+                "start_ms": ({"cold": rep.start_ms[0], "warm": rep.start_ms[1]} if rep.warm_start >= 0 else {}),
                 "from_cache": bool(rep.from_cache)}
 
 
