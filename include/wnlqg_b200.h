@@ -298,8 +298,10 @@ WNLQG_API wnlqg_status wnlqg_b200_graph_destroy(wnlqg_graph *graph);
  * Measures, on the mesh block [k_begin, k_end) of `mesh`, every eigensolver team size (32, 64 and
  * 128 threads per matrix; orthogonal models up to 32 orbitals), the FP32 eigensolver stage's
  * start (warm from the previous point along mesh runs and ordered batches, or cold from the
- * identity; orthogonal models on the team or CTA mixed-precision stages) and every contraction
- * tile (1, 2 and 4 photon energies per thread; frequency-resolved responses), keeps the fastest of each in
+ * identity; orthogonal models on the team or CTA mixed-precision stages), every contraction
+ * tile (1, 2 and 4 photon energies per thread; frequency-resolved responses) and the FP64
+ * response CTA width (256 or 512 threads; orthogonal models whose per-point working set fits
+ * shared memory), keeps the fastest of each in
  * the plan and remembers it for the process (key: device, orbitals, precision, geometry, photon
  * energies, value count), so later plans with the same key take it without measuring.  Every
  * candidate is a configuration the library runs anyway; the tile choice leaves results bitwise
@@ -313,6 +315,8 @@ typedef struct wnlqg_autotune_report {
     int32_t from_cache;            /* 1 when the choice came from the process cache */
     int32_t warm_start;            /* chosen FP32 start: 1 warm, 0 cold, -1 = not tunable */
     double start_ms[2];            /* eigensolve time with a cold and a warm start */
+    int32_t response_threads;      /* chosen FP64 response CTA width (256, 512), -1 = not tunable */
+    double width_ms[2];            /* response time with 256 and 512 threads per CTA */
 } wnlqg_autotune_report;
 WNLQG_API wnlqg_status wnlqg_b200_plan_autotune(wnlqg_plan *plan, const int64_t mesh[3], int64_t k_begin,
                                       int64_t k_end, wnlqg_autotune_report *report);

@@ -111,6 +111,8 @@ struct AutotuneReport
     from_cache::Int32
     warm_start::Int32
     start_ms::NTuple{2, Float64}
+    response_threads::Int32
+    width_ms::NTuple{2, Float64}
 end
 
 """Pick the eigensolver team and contraction tile by timing them on mesh indices [first, last)."""

@@ -113,6 +113,10 @@ def test_autotune_keeps_results(torch_and_engine, nw, precision):
         assert sorted(rep["eigh_ms"]) == [32, 64, 128] and sorted(rep["response_ms"]) == [1, 2, 4]
         assert all(v > 0 for v in list(rep["eigh_ms"].values()) + list(rep["response_ms"].values()))
         assert rep["warm_start"] in (0, 1) and set(rep["start_ms"]) == {"cold", "warm"}
+        if nw == 32 and precision == _abi.PRECISION_FP64:
+            assert rep["response_threads"] in (256, 512) and set(rep["width_ms"]) == {256, 512}
+        else:
+            assert rep["response_threads"] == -1
         after = e.integrate_mesh(mesh, 0, 8192)
         tol = 1e-11 if precision == _abi.PRECISION_FP64 else 1e-6
         for a, b in zip(task.split(after), task.split(before)):
@@ -122,3 +126,4 @@ def test_autotune_keeps_results(torch_and_engine, nw, precision):
         assert again["from_cache"] and again["eigh_team"] == rep["eigh_team"]
         assert again["energies_per_thread"] == rep["energies_per_thread"]
         assert again["warm_start"] == rep["warm_start"]
+        assert again["response_threads"] == rep["response_threads"]

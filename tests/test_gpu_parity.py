@@ -749,3 +749,23 @@ def test_large_nw_warm_started_ranges_match_cta_jacobi(engine_cls, nw, precision
         assert rel_err(g, r) < rtol
     for g, r in zip(task.split(s), task.split(s_ref)):
         assert rel_err(g, r) < rtol
+
+
+def test_wide_fp64_response_matches(engine_cls, oracle_mod, monkeypatch):
+    """The 512-thread FP64 response kernel (WNLQG_B200_RESPONSE_WIDE=1) gives the 256-thread
+    kernel's mesh sums to 1e-12 (only the order of the per-point block sums changes) and the
+    oracle's point values."""
+    model = reference_workload_model("nw32")
+    task = nw32_task(nom=512)
+    k = np.random.default_rng(61).random((12, 3))
+    with engine_cls(model, task) as eng:
+        base = eng.integrate_mesh((8, 8, 8))
+    monkeypatch.setenv("WNLQG_B200_RESPONSE_WIDE", "1")
+    with engine_cls(model, task) as eng:
+        wide = eng.integrate_mesh((8, 8, 8))
+        pts = eng.point_values(k)
+    for g, r in zip(task.split(wide), task.split(base)):
+        assert rel_err(g, r) < 1e-12
+    ref = oracle_mod.point_values(model, task, k)
+    for g, r in zip(task.split(pts), task.split(ref)):
+        assert rel_err(g, r) < RTOL

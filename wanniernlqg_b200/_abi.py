@@ -72,6 +72,8 @@ class AutotuneReport(ctypes.Structure):
         ("from_cache", ctypes.c_int32),
         ("warm_start", ctypes.c_int32),
         ("start_ms", ctypes.c_double * 2),
+        ("response_threads", ctypes.c_int32),
+        ("width_ms", ctypes.c_double * 2),
     ]
 
 

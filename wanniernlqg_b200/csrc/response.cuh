@@ -405,8 +405,10 @@ WNLQG_D void contract_dispatch(int pair_mode, int gaussian, const double *ste, c
 // memory), the FP32 kernel two: the register budgets follow.
 // GW: the per-k working set lives in global memory (p.gscratch); a separate instantiation so that
 // the shared-memory kernel addresses shared memory directly.
-template <typename R, bool NG, bool GW>
-__global__ void __launch_bounds__(256, sizeof(R) == 8 ? 1 : 2) response_kernel(RespParams p) {
+// WIDE: 512 threads per CTA (16 warps to hide the FP64 latencies of the one CTA an SM holds) at
+// 128 registers per thread instead of 256 threads at up to 255; the autotuner picks the width.
+template <typename R, bool NG, bool GW, bool WIDE = false>
+__global__ void __launch_bounds__(WIDE ? 512 : 256, WIDE ? 1 : (sizeof(R) == 8 ? 1 : 2)) response_kernel(RespParams p) {
     typedef typename cplx_of<R>::type C;
     extern __shared__ __align__(16) unsigned char smem_dyn[];
     unsigned char *sm;

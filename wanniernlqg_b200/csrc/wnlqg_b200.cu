@@ -72,6 +72,7 @@ struct Pass {
     size_t smem = 0;
     int threads = 0;
     int grid = 0;
+    int grid_wide = 0;   // grid of the 512-thread variant (FP64 orthogonal shared-memory passes), 0 = none
 };
 
 struct wnlqg_plan {
@@ -155,6 +156,9 @@ struct wnlqg_plan {
     // FP32 eigensolver stages warm-start along mesh runs and ordered batches (1) or always start
     // from the identity (0): WNLQG_B200_WARM_START at plan creation, then the autotuner.
     int warm_mode = 1;
+    // FP64 response passes on the 512-thread variant (WNLQG_B200_RESPONSE_WIDE at plan creation,
+    // then the autotuner).
+    bool resp_wide = false;
     uint32_t *d_okeys = nullptr;
     int *d_operm = nullptr;
     double *d_ok = nullptr, *d_ow = nullptr;
@@ -229,6 +233,9 @@ cudaError_t allow_dynamic_smem(const void *fn, int smem_optin) {
     return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin - (int)a.sharedSizeBytes);
 }
 
+// The 512-thread FP64 response kernel (orthogonal models, working set in shared memory).
+const void *response_wide_fn() { return (const void *)response_kernel<double, false, false, true>; }
+
 // The response kernel instantiation for a precision, a geometry source and a working-set location.
 const void *response_fn(bool mixed, bool nonorth, bool global) {
     if (mixed) {
@@ -295,6 +302,7 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
         cudaError_t e = cudaSuccess;
         for (int v = 0; v < 4 && e == cudaSuccess; ++v)
             e = allow_dynamic_smem(response_fn(v & 1, v & 2, false), (int)smem_limit);
+        if (e == cudaSuccess) e = allow_dynamic_smem(response_wide_fn(), (int)smem_limit);
         if (e != cudaSuccess) return fail(WNLQG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
     }
     // Orbital counts whose matrices do not fit shared memory keep each CTA's working set in global
@@ -452,6 +460,12 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
         if (per_sm < 1) return fail(WNLQG_ERR_UNSUPPORTED, "response kernel cannot be resident with its shared memory");
         ps.grid = sm_count * per_sm;
         if (pass_global) ps.grid = l2_resident_grid(ps.grid, (int64_t)ps.smem, sm_count);
+        if (!mixed && !pl->nonorth && !pass_global && ps.threads == 256) {
+            int per_sm_w = 0;
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_w, response_wide_fn(), 512, ps.smem);
+            if (e != cudaSuccess) return fail(WNLQG_ERR_CUDA, std::string("occupancy query: ") + cudaGetErrorString(e));
+            ps.grid_wide = per_sm_w >= 1 ? sm_count * per_sm_w : 0;
+        }
         pl->passes.push_back(ps);
     }
     bool any_global = false;
@@ -883,8 +897,11 @@ wnlqg_status run_passes(wnlqg_plan *pl, int64_t nb, int mode, double scale, int6
         p.gscratch_stride = pl->resp_scratch_stride;
         const size_t launch_smem = ps.global ? 0 : ps.smem;
         void *args[] = {&p};
-        WNLQG_CUDA(cudaLaunchKernel(response_fn(pl->task.precision == WNLQG_PRECISION_MIXED, pl->nonorth, ps.global),
-                                    dim3(ps.grid), dim3(ps.threads), args, launch_smem, pl->stream));
+        if (pl->resp_wide && ps.grid_wide > 0)
+            WNLQG_CUDA(cudaLaunchKernel(response_wide_fn(), dim3(ps.grid_wide), dim3(512), args, launch_smem, pl->stream));
+        else
+            WNLQG_CUDA(cudaLaunchKernel(response_fn(pl->task.precision == WNLQG_PRECISION_MIXED, pl->nonorth, ps.global),
+                                        dim3(ps.grid), dim3(ps.threads), args, launch_smem, pl->stream));
         pl->launches += 1;
     }
     if (pl->metric_shg && !pl->shg.empty()) {
@@ -1496,6 +1513,8 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
     {
         const char *wm = std::getenv("WNLQG_B200_WARM_START");
         pl->warm_mode = (wm && wm[0] == '0') ? 0 : 1;
+        const char *rw = std::getenv("WNLQG_B200_RESPONSE_WIDE");
+        pl->resp_wide = rw && rw[0] == '1';
     }
     auto alloc_ordering = [&]() -> wnlqg_status {
         const char *ord = std::getenv("WNLQG_B200_POINT_ORDER");
@@ -1630,7 +1649,7 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
     }
     if ((st = build_passes(pl, sm_count, (size_t)smem_optin)) != WNLQG_OK) return bail(st);
     if ((st = build_shg(pl, sm_count, (size_t)smem_optin)) != WNLQG_OK) return bail(st);
-    for (const Pass &ps : pl->passes) pl->partial_slots = std::max(pl->partial_slots, ps.grid);
+    for (const Pass &ps : pl->passes) pl->partial_slots = std::max(pl->partial_slots, std::max(ps.grid, ps.grid_wide));
     pl->partial_slots = std::max(pl->partial_slots, pl->shg_grid);
     if ((st = alloc((void **)&pl->d_partials, (size_t)pl->partial_slots * vc * 4 * sizeof(double))) != WNLQG_OK)
         return bail(st);
@@ -2232,7 +2251,7 @@ wnlqg_status wnlqg_b200_graph_destroy(wnlqg_graph *graph) {
 // ---------------------------------------------------------------------------------------------
 namespace {
 
-struct TuneChoice { int team; int omb; int warm; wnlqg_autotune_report report; };
+struct TuneChoice { int team; int omb; int warm; int wide; wnlqg_autotune_report report; };
 std::map<std::tuple<int, int, int, int, int64_t, int64_t>, TuneChoice> g_tune_cache;
 std::mutex g_tune_mutex;
 
@@ -2279,6 +2298,7 @@ extern "C" wnlqg_status wnlqg_b200_plan_autotune(wnlqg_plan *pl, const int64_t m
         if (it != g_tune_cache.end()) {
             if (pl->warp_eigh && it->second.team) apply_team(pl, it->second.team);
             if (it->second.warm >= 0) pl->warm_mode = it->second.warm;
+            if (it->second.wide >= 0) pl->resp_wide = it->second.wide == 1;
             apply_omb(pl, it->second.omb);
             if (report) {
                 *report = it->second.report;
@@ -2292,6 +2312,8 @@ extern "C" wnlqg_status wnlqg_b200_plan_autotune(wnlqg_plan *pl, const int64_t m
     for (int i = 0; i < 3; ++i) rep.eigh_ms[i] = rep.response_ms[i] = -1.0;
     rep.warm_start = -1;
     rep.start_ms[0] = rep.start_ms[1] = -1.0;
+    rep.response_threads = -1;
+    rep.width_ms[0] = rep.width_ms[1] = -1.0;
     const int teams[3] = {32, 64, 128}, ombs[3] = {1, 2, 4};
     if (pl->warp_eigh) {
         const int start = pl->eigh_team;
@@ -2337,9 +2359,25 @@ extern "C" wnlqg_status wnlqg_b200_plan_autotune(wnlqg_plan *pl, const int64_t m
         apply_omb(pl, best);
         rep.energies_per_thread = best;
     }
+    bool widen = false;
+    for (const Pass &ps : pl->passes) widen |= ps.grid_wide > 0;
+    if (widen) {
+        const bool start = pl->resp_wide;
+        double e = 0;
+        for (int w = 0; w < 2; ++w) {
+            pl->resp_wide = w == 1;
+            if ((st = tune_measure(pl, mesh, k_begin, k_end, &e, &rep.width_ms[w])) != WNLQG_OK) {
+                pl->resp_wide = start;
+                return st;
+            }
+        }
+        pl->resp_wide = rep.width_ms[1] < rep.width_ms[0];
+        rep.response_threads = pl->resp_wide ? 512 : 256;
+    }
     {
         std::lock_guard<std::mutex> lock(g_tune_mutex);
-        g_tune_cache[key] = TuneChoice{rep.eigh_team, rep.energies_per_thread, rep.warm_start, rep};
+        g_tune_cache[key] = TuneChoice{rep.eigh_team, rep.energies_per_thread, rep.warm_start,
+                                       rep.response_threads < 0 ? -1 : (rep.response_threads == 512 ? 1 : 0), rep};
     }
     if (report) *report = rep;
     return WNLQG_OK;

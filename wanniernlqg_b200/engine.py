@@ -169,6 +169,8 @@ class ResponseEngine:
                 "response_ms": {t: rep.response_ms[i] for i, t in enumerate((1, 2, 4)) if rep.response_ms[i] >= 0},
                 "warm_start": rep.warm_start,
                 "start_ms": ({"cold": rep.start_ms[0], "warm": rep.start_ms[1]} if rep.warm_start >= 0 else {}),
+                "response_threads": rep.response_threads,
+                "width_ms": ({256: rep.width_ms[0], 512: rep.width_ms[1]} if rep.response_threads > 0 else {}),
                 "from_cache": bool(rep.from_cache)}
 
 
