@@ -769,3 +769,56 @@ def test_wide_fp64_response_matches(engine_cls, oracle_mod, monkeypatch):
     ref = oracle_mod.point_values(model, task, k)
     for g, r in zip(task.split(pts), task.split(ref)):
         assert rel_err(g, r) < RTOL
+
+
+@pytest.mark.parametrize("nw", [7, 40, 64])
+def test_nonorthogonal_mixed_path_cholesky_reduction(engine_cls, oracle_mod, nw, monkeypatch):
+    """Nonorthogonal models on the mixed path: FP64 Cholesky reduction C = L^-1 H L^-H, the
+    orthogonal mixed-precision stages on C (team stages at 7 orbitals, CTA stages at 40 and 64),
+    U = L^-H V.  Eigenvalues to 1e-11 of max |E| against the oracle's generalised solve,
+    U^H S(k) U = I to 1e-11, eigenvectors of well-separated bands S-parallel to the oracle's to
+    1e-8; currents at points and on a
+    warm-started mesh block against the FP64 generalised path to the mixed bound; a
+    non-positive-definite S(k) is reported on this path too.  The FP64 CUDA-core Fourier sums
+    (WNLQG_B200_DIRECT_FOURIER=1) isolate the eigensolver from the mixed path's 4-slice
+    tensor-core Fourier."""
+    from wanniernlqg_b200._lib import EngineError
+    monkeypatch.setenv("WNLQG_B200_DIRECT_FOURIER", "1")
+    model = _nonorth_full_position(nw, 11)
+    task = _currents_task(_abi.PRECISION_MIXED)
+    ref_task = _currents_task(_abi.PRECISION_FP64)
+    k = np.random.default_rng(nw + 3).random((6, 3))
+    with engine_cls(model, task) as eng:
+        e, c = eng.spectrum(k)
+        pts = eng.point_values(k[:3])
+        mesh = eng.integrate_mesh((12, 10, 8), 100, 700)
+    with engine_cls(model, ref_task) as eng:
+        mesh_ref = eng.integrate_mesh((12, 10, 8), 100, 700)
+    for i in range(k.shape[0]):
+        eo, co, _ = oracle_mod.kpoint_spectrum(model, k[i])
+        assert np.max(np.abs(e[i] - eo)) < 1e-11 * max(1.0, np.abs(eo).max())
+        ph = np.exp(2j * np.pi * (model.r_vectors.T @ k[i])) / model.r_degeneracies
+        sk = np.einsum("ijr,r->ij", model.overlap_r, ph)
+        gram = c[i].conj().T @ sk @ c[i]
+        assert np.max(np.abs(gram - np.eye(nw))) < 1e-11
+        # Bands 0.05 eV from their neighbours: the one FP64 sweep leaves their vectors S-parallel
+        # to the oracle's to second order.
+        gaps = np.diff(eo)
+        isolated = np.ones(nw, dtype=bool)
+        isolated[:-1] &= gaps > 0.05
+        isolated[1:] &= gaps > 0.05
+        ov = np.abs(np.sum(c[i].conj() * (sk @ co), axis=0))
+        if isolated.any():
+            assert np.max(np.abs(ov - 1.0)[isolated]) < 1e-8
+    ref = oracle_mod.point_values(model, ref_task, k[:3])
+    for g, r in zip(task.split(pts), task.split(ref)):
+        assert rel_err(g, r) < MIXED_RTOL
+    for g, r in zip(task.split(mesh), task.split(mesh_ref)):
+        assert rel_err(g, r) < MIXED_RTOL
+    bad = _nonorth_full_position(nw, 11)
+    home = int(np.where(np.all(bad.r_vectors == 0, axis=0))[0][0])
+    bad.overlap_r[:, :, home] -= 2.0 * np.eye(nw)
+    with engine_cls(bad, task) as eng:
+        with pytest.raises(EngineError) as ei:
+            eng.spectrum(np.array([[0.1, 0.2, 0.3]]))
+        assert ei.value.status == 1

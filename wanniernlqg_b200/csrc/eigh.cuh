@@ -945,6 +945,67 @@ struct GenEighSmem {
     }
 };
 
+// S = L L^H (lower Cholesky factor in Lm) and A = L^-1 H L^-H (Hermitian, full) for one padded
+// np x np matrix, CTA-wide; V is scratch.  Sets *bad when a pivot of S is not positive.
+WNLQG_D void gen_cholesky_reduce(const double2 *__restrict__ h, const double2 *__restrict__ sk, int nw, int np,
+                                 int ld, double2 *A, double2 *V, double2 *Lm, int *bad) {
+    const int tid = threadIdx.x;
+    if (tid == 0) *bad = 0;
+    for (int e = tid; e < np * np; e += blockDim.x) {
+        const int i = e % np, j = e / np;
+        double2 hv = make_double2(0.0, 0.0), sv = make_double2(i == j ? 1.0 : 0.0, 0.0);
+        if (i < nw && j < nw) {
+            if (i < j) { hv = h[i + (size_t)nw * j]; sv = sk[i + (size_t)nw * j]; }
+            else if (i > j) { hv = cconj(h[j + (size_t)nw * i]); sv = cconj(sk[j + (size_t)nw * i]); }
+            else { hv = make_double2(h[i + (size_t)nw * i].x, 0.0); sv = make_double2(sk[i + (size_t)nw * i].x, 0.0); }
+        }
+        A[i + ld * j] = hv;
+        Lm[i + ld * j] = sv;
+    }
+    __syncthreads();
+    // Right-looking Cholesky in place (lower triangle of Lm).
+    for (int j = 0; j < np; ++j) {
+        if (tid == 0) {
+            const double d = Lm[j + ld * j].x;
+            if (!(d > 0.0)) *bad = 1;
+            Lm[j + ld * j] = make_double2(d > 0.0 ? sqrt(d) : 1.0, 0.0);
+        }
+        __syncthreads();
+        const double ljj = Lm[j + ld * j].x;
+        for (int i = j + 1 + tid; i < np; i += blockDim.x) Lm[i + ld * j] = cscale(Lm[i + ld * j], 1.0 / ljj);
+        __syncthreads();
+        for (int e = tid; e < np * np; e += blockDim.x) {
+            const int r = e % np, c = e / np;
+            if (c > j && r >= c) Lm[r + ld * c] = csub(Lm[r + ld * c], cmul(Lm[r + ld * j], cconj(Lm[c + ld * j])));
+        }
+        __syncthreads();
+    }
+    // X = L^-1 H (forward substitution, one thread per column), stored in V.
+    for (int c = tid; c < np; c += blockDim.x)
+        for (int r = 0; r < np; ++r) {
+            double2 acc = A[r + ld * c];
+            for (int k = 0; k < r; ++k) acc = csub(acc, cmul(Lm[r + ld * k], V[k + ld * c]));
+            V[r + ld * c] = cscale(acc, 1.0 / Lm[r + ld * r].x);
+        }
+    __syncthreads();
+    // Ht = X L^-H = (L^-1 X^H)^H: solve L Y = X^H column by column (column c of X^H is row c
+    // of X, conjugated); Ht[c][r] = conj(Y[r][c]).
+    for (int c = tid; c < np; c += blockDim.x)
+        for (int r = 0; r < np; ++r) {
+            double2 acc = cconj(V[c + ld * r]);
+            for (int k = 0; k < r; ++k) acc = csub(acc, cmul(Lm[r + ld * k], cconj(A[c + ld * k])));
+            A[c + ld * r] = cconj(cscale(acc, 1.0 / Lm[r + ld * r].x));
+        }
+    __syncthreads();
+    // Hermitian part from the upper triangle.
+    for (int e = tid; e < np * np; e += blockDim.x) {
+        const int i = e % np, j = e / np;
+        if (i > j) A[i + ld * j] = cconj(A[j + ld * i]);
+        if (i == j) A[i + ld * i].y = 0.0;
+    }
+    __syncthreads();
+}
+
 template <bool GW = false>
 __global__ void generalized_eigh_kernel(const double2 *__restrict__ h_in, const double2 *__restrict__ s_in,
                                         int64_t stride, int64_t batch, int nw, double *__restrict__ E_out,
@@ -970,64 +1031,11 @@ __global__ void generalized_eigh_kernel(const double2 *__restrict__ h_in, const 
     for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) {
         const double2 *h = h_in + b * stride;
         const double2 *sk = s_in + b * stride;
-        if (tid == 0) bad = 0;
-        for (int e = tid; e < np * np; e += blockDim.x) {
-            const int i = e % np, j = e / np;
-            double2 hv = make_double2(0.0, 0.0), sv = make_double2(i == j ? 1.0 : 0.0, 0.0);
-            if (i < nw && j < nw) {
-                if (i < j) { hv = h[i + (size_t)nw * j]; sv = sk[i + (size_t)nw * j]; }
-                else if (i > j) { hv = cconj(h[j + (size_t)nw * i]); sv = cconj(sk[j + (size_t)nw * i]); }
-                else { hv = make_double2(h[i + (size_t)nw * i].x, 0.0); sv = make_double2(sk[i + (size_t)nw * i].x, 0.0); }
-            }
-            A[i + ld * j] = hv;
-            Lm[i + ld * j] = sv;
-            V[i + ld * j] = make_double2(i == j ? 1.0 : 0.0, 0.0);
-        }
-        __syncthreads();
-        // Right-looking Cholesky in place (lower triangle of Lm).
-        for (int j = 0; j < np; ++j) {
-            if (tid == 0) {
-                const double d = Lm[j + ld * j].x;
-                if (!(d > 0.0)) bad = 1;
-                Lm[j + ld * j] = make_double2(d > 0.0 ? sqrt(d) : 1.0, 0.0);
-            }
-            __syncthreads();
-            const double ljj = Lm[j + ld * j].x;
-            for (int i = j + 1 + tid; i < np; i += blockDim.x) Lm[i + ld * j] = cscale(Lm[i + ld * j], 1.0 / ljj);
-            __syncthreads();
-            for (int e = tid; e < np * np; e += blockDim.x) {
-                const int r = e % np, c = e / np;
-                if (c > j && r >= c) Lm[r + ld * c] = csub(Lm[r + ld * c], cmul(Lm[r + ld * j], cconj(Lm[c + ld * j])));
-            }
-            __syncthreads();
-        }
-        // X = L^-1 H (forward substitution, one thread per column), stored in V.
-        for (int c = tid; c < np; c += blockDim.x)
-            for (int r = 0; r < np; ++r) {
-                double2 acc = A[r + ld * c];
-                for (int k = 0; k < r; ++k) acc = csub(acc, cmul(Lm[r + ld * k], V[k + ld * c]));
-                V[r + ld * c] = cscale(acc, 1.0 / Lm[r + ld * r].x);
-            }
-        __syncthreads();
-        // Ht = X L^-H = (L^-1 X^H)^H: solve L Y = X^H column by column (column c of X^H is row c
-        // of X, conjugated); Ht[c][r] = conj(Y[r][c]).
-        for (int c = tid; c < np; c += blockDim.x)
-            for (int r = 0; r < np; ++r) {
-                double2 acc = cconj(V[c + ld * r]);
-                for (int k = 0; k < r; ++k) acc = csub(acc, cmul(Lm[r + ld * k], cconj(A[c + ld * k])));
-                A[c + ld * r] = cconj(cscale(acc, 1.0 / Lm[r + ld * r].x));
-            }
-        __syncthreads();
-        // Hermitian part from the upper triangle; identity for the eigenvector accumulation.
+        gen_cholesky_reduce(h, sk, nw, np, ld, A, V, Lm, &bad);
+        // Identity for the eigenvector accumulation.
         for (int e = tid; e < np * np; e += blockDim.x) {
             const int i = e % np, j = e / np;
             V[i + ld * j] = make_double2(i == j ? 1.0 : 0.0, 0.0);
-        }
-        __syncthreads();
-        for (int e = tid; e < np * np; e += blockDim.x) {
-            const int i = e % np, j = e / np;
-            if (i > j) A[i + ld * j] = cconj(A[j + ld * i]);
-            if (i == j) A[i + ld * i].y = 0.0;
         }
         __syncthreads();
         double local = 0.0;
@@ -1083,5 +1091,81 @@ __global__ void generalized_eigh_kernel(const double2 *__restrict__ h_in, const 
         }
         if (tid == 0 && status) status[b] = bad;
         __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Mixed-precision generalised eigensolve (nonorthogonal models on the mixed path): the FP64
+// Cholesky S = L L^H and reduction C = L^-1 H L^-H (cholesky_reduce_kernel, the same arithmetic
+// as generalized_eigh_kernel), the orthogonal mixed-precision stages on C (FP32 Jacobi, FP64
+// refinement, ascending order and canonical phases of C's eigenvectors V), then U = L^-H V and
+// the canonical phase rule on U (gen_back_substitute_kernel), so U^H S U = I.
+// ---------------------------------------------------------------------------------------------
+struct GenReduceSmem {
+    static __host__ __device__ size_t bytes(int nw) {
+        const int np = nw + (nw & 1);
+        return 3 * (size_t)np * (np + 1) * sizeof(double2);
+    }
+};
+
+template <bool GW>
+__global__ void __launch_bounds__(256) cholesky_reduce_kernel(const double2 *__restrict__ h_in,
+                                                              const double2 *__restrict__ s_in, int64_t stride,
+                                                              int64_t batch, int nw, double2 *__restrict__ C_out,
+                                                              double2 *__restrict__ L_out, int *__restrict__ status,
+                                                              unsigned char *gscratch, int64_t gscratch_stride) {
+    extern __shared__ __align__(16) unsigned char smem_dyn[];
+    unsigned char *smraw;
+    if constexpr (GW) smraw = gscratch + (int64_t)blockIdx.x * gscratch_stride;
+    else smraw = smem_dyn;
+    const int np = nw + (nw & 1);
+    const int ld = np + 1;
+    double2 *A = reinterpret_cast<double2 *>(smraw);
+    double2 *V = A + (size_t)np * ld;
+    double2 *Lm = V + (size_t)np * ld;
+    __shared__ int bad;
+    const int64_t nn = (int64_t)nw * nw;
+    for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) {
+        gen_cholesky_reduce(h_in + b * stride, s_in + b * stride, nw, np, ld, A, V, Lm, &bad);
+        double2 *c = C_out + b * nn;
+        double2 *l = L_out + b * nn;
+        for (int e = threadIdx.x; e < nw * nw; e += blockDim.x) {
+            const int i = e % nw, j = e / nw;
+            c[e] = A[i + ld * j];
+            l[e] = i >= j ? Lm[i + ld * j] : make_double2(0.0, 0.0);
+        }
+        if (threadIdx.x == 0) status[b] = bad;
+        __syncthreads();
+    }
+}
+
+// U <- L^-H U for each point's nw x nw eigenvector matrix (columns), L lower; then each column
+// is rotated so that its largest-modulus entry is real and positive (first such entry on ties).
+// One thread per column; L is read from global memory (every thread of a warp reads the same
+// element at once).
+__global__ void __launch_bounds__(128) gen_back_substitute_kernel(const double2 *__restrict__ L_in, double2 *U,
+                                                                  int64_t batch, int nw) {
+    const int64_t nn = (int64_t)nw * nw;
+    for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) {
+        const double2 *L = L_in + b * nn;
+        double2 *u = U + b * nn;
+        for (int c = threadIdx.x; c < nw; c += blockDim.x) {
+            double2 *col = u + (int64_t)nw * c;
+            for (int r = nw - 1; r >= 0; --r) {
+                double2 acc = col[r];
+                for (int k = r + 1; k < nw; ++k) acc = csub(acc, cmul(cconj(L[k + (int64_t)nw * r]), col[k]));
+                col[r] = cscale(acc, 1.0 / L[r + (int64_t)nw * r].x);
+            }
+            int pivot = 0;
+            double pm = hypot(col[0].x, col[0].y);
+            for (int r = 1; r < nw; ++r) {
+                const double mg = hypot(col[r].x, col[r].y);
+                if (mg > pm) { pm = mg; pivot = r; }
+            }
+            if (pm > 0.0) {
+                const double2 ph = make_double2(col[pivot].x / pm, -col[pivot].y / pm);
+                for (int r = 0; r < nw; ++r) col[r] = cmul(col[r], ph);
+            }
+        }
     }
 }

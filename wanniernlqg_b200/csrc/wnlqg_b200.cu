@@ -159,6 +159,15 @@ struct wnlqg_plan {
     // FP64 response passes on the 512-thread variant (WNLQG_B200_RESPONSE_WIDE at plan creation,
     // then the autotuner).
     bool resp_wide = false;
+    // Nonorthogonal models on the mixed path: FP64 Cholesky reduction C = L^-1 H L^-H (d_gC, with
+    // L in d_gL), the orthogonal mixed-precision stages on C, back-substitution U = L^-H V.
+    bool gen_mixed = false;
+    double2 *d_gC = nullptr, *d_gL = nullptr;
+    size_t gred_smem = 0;
+    bool gred_gw = false;
+    unsigned char *d_gred_scratch = nullptr;
+    int64_t gred_stride = 0;
+    int gred_grid = 0;
     uint32_t *d_okeys = nullptr;
     int *d_operm = nullptr;
     double *d_ok = nullptr, *d_ow = nullptr;
@@ -718,6 +727,77 @@ wnlqg_status setup_tc_fourier(wnlqg_plan *pl, const std::vector<double2> &tiles)
 }
 
 // One batch: phases, Fourier GEMM, eigensolve.  kpts_device == nullptr selects mesh mode.
+// The orthogonal eigensolver stages on Hermitian matrices hk + b * stride_in (nw x nw, upper
+// triangle read): the team stages up to 32 orbitals, the CTA mixed-precision stages above;
+// eigenvalues into d_E, canonical eigenvectors into d_U.  warm_in: warm-start along the batch.
+wnlqg_status run_orth_eigen(wnlqg_plan *pl, const double2 *hk, int64_t stride_in, int64_t nb, int warm_in) {
+    if (pl->warp_eigh) {
+        // Stage 1: four one-warp teams per 128-thread block, or one 64-thread team per block.
+        // Stage 2: 64-thread blocks holding two one-warp teams or one 64-thread team.
+        const int tm = pl->eigh_team;
+        const void *f32_fn = tm == 128 ? (const void *)jacobi_f32_team_kernel<128>
+                             : tm == 64 ? (const void *)jacobi_f32_team_kernel<64> : (const void *)jacobi_f32_team_kernel<32>;
+        const void *ref_fn = tm == 128 ? (const void *)eigh_refine_f64_team_kernel<128>
+                             : tm == 64 ? (const void *)eigh_refine_f64_team_kernel<64> : (const void *)eigh_refine_f64_team_kernel<32>;
+        const int f32_threads = tm == 32 ? 128 : tm, f32_teams = tm == 32 ? 4 : 1;
+        const int ref_threads = tm == 128 ? 128 : 64, ref_teams = tm == 32 ? 2 : 1;
+        int per_sm = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f32_fn, f32_threads, pl->eigh_smem);
+        const int64_t f32_grid = std::min<int64_t>((nb + f32_teams - 1) / f32_teams, (int64_t)std::max(1, per_sm) * pl->sm_count);
+        int warm = warm_in;
+        {
+            int64_t nb_arg = nb;
+            int nw_arg = pl->nw;
+            float2 *v32 = pl->d_V32;
+            int64_t stride = stride_in;
+            void *args[] = {(void *)&hk, &stride, &nb_arg, &nw_arg, &v32, &warm};
+            WNLQG_CUDA(cudaLaunchKernel(f32_fn, dim3((unsigned)f32_grid), dim3(f32_threads), args, pl->eigh_smem, pl->stream));
+        }
+        int per_sm_r = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_r, ref_fn, ref_threads, pl->refine_smem);
+        const int64_t r_grid = std::min<int64_t>((nb + ref_teams - 1) / ref_teams, (int64_t)std::max(1, per_sm_r) * pl->sm_count);
+        {
+            int64_t stride = stride_in, nb_arg = nb;
+            int nw_arg = pl->nw;
+            const float2 *v32 = pl->d_V32;
+            double *E = pl->d_E;
+            double2 *U = pl->d_U;
+            int converge = pl->task.precision == WNLQG_PRECISION_MIXED ? 0 : 1;
+            void *args[] = {(void *)&hk, &stride, (void *)&v32, &nb_arg, &nw_arg, &E, &U, &converge};
+            WNLQG_CUDA(cudaLaunchKernel(ref_fn, dim3((unsigned)r_grid), dim3(ref_threads), args, pl->refine_smem, pl->stream));
+        }
+        pl->launches += 1;
+    } else if (pl->cta_mixed) {
+        const int converge = pl->task.precision == WNLQG_PRECISION_MIXED ? 0 : 1;
+        const int warm = warm_in;
+        const int64_t N = stride_in;
+        if (pl->cta_gw1) {
+            jacobi_f32_cta_kernel<true><<<(unsigned)std::min<int64_t>(nb, pl->eigh_grid), 256, 0, pl->stream>>>(
+                hk, N, nb, pl->nw, pl->d_V32, pl->d_eigh_scratch, pl->eigh_scratch_stride, warm);
+        } else {
+            int per_sm = 1;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jacobi_f32_cta_kernel<false>, 256, pl->eigh_smem);
+            const int64_t grid = std::min<int64_t>(nb, (int64_t)std::max(1, per_sm) * pl->sm_count);
+            jacobi_f32_cta_kernel<false><<<(unsigned)grid, 256, pl->eigh_smem, pl->stream>>>(hk, N, nb, pl->nw, pl->d_V32,
+                                                                                            nullptr, 0, warm);
+        }
+        if (pl->cta_gw2) {
+            eigh_refine_f64_cta_kernel<true><<<(unsigned)std::min<int64_t>(nb, pl->eigh_grid), pl->refine_cta_threads, 0, pl->stream>>>(
+                hk, N, pl->d_V32, nb, pl->nw, pl->d_E, pl->d_U, converge, pl->d_eigh_scratch, pl->eigh_scratch_stride);
+        } else {
+            int per_sm = 1;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, eigh_refine_f64_cta_kernel<false>, pl->refine_cta_threads,
+                                                          pl->refine_smem);
+            const int64_t grid = std::min<int64_t>(nb, (int64_t)std::max(1, per_sm) * pl->sm_count);
+            eigh_refine_f64_cta_kernel<false><<<(unsigned)grid, pl->refine_cta_threads, pl->refine_smem, pl->stream>>>(
+                hk, N, pl->d_V32, nb, pl->nw, pl->d_E, pl->d_U, converge, nullptr, 0);
+        }
+        pl->launches += 1;
+    }
+    WNLQG_CUDA(cudaGetLastError());
+    return WNLQG_OK;
+}
+
 wnlqg_status run_front(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const int64_t *mesh, const double *kpts_device,
                        size_t ev_base, const int64_t *kidx_device = nullptr, bool ordered = false) {
     const int nr = pl->nr;
@@ -771,7 +851,26 @@ wnlqg_status run_front(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const int64_
     wnlqg_status st = record_event(pl, ev_base + 1);
     if (st != WNLQG_OK) return st;
     const unsigned eigh_grid = (unsigned)(pl->d_eigh_scratch ? std::min<int64_t>(nb, pl->eigh_grid) : nb);
-    if (pl->nonorth) {
+    if (pl->nonorth && pl->gen_mixed) {
+        // FP64 Cholesky reduction, the orthogonal mixed-precision stages on C, U = L^-H V.
+        const double2 *hk = pl->d_xw + (int64_t)pl->ch_H * pl->nn, *sk = pl->d_xw + (int64_t)pl->ch_S * pl->nn;
+        if (pl->gred_gw) {
+            cholesky_reduce_kernel<true><<<(unsigned)std::min<int64_t>(nb, pl->gred_grid), 256, 0, pl->stream>>>(
+                hk, sk, N, nb, pl->nw, pl->d_gC, pl->d_gL, pl->d_status, pl->d_gred_scratch, pl->gred_stride);
+        } else {
+            int per_sm = 1;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cholesky_reduce_kernel<false>, 256, pl->gred_smem);
+            const int64_t grid = std::min<int64_t>(nb, (int64_t)std::max(1, per_sm) * pl->sm_count);
+            cholesky_reduce_kernel<false><<<(unsigned)grid, 256, pl->gred_smem, pl->stream>>>(
+                hk, sk, N, nb, pl->nw, pl->d_gC, pl->d_gL, pl->d_status, nullptr, 0);
+        }
+        const bool contiguous = mesh != nullptr && kpts_device == nullptr && kidx_device == nullptr;
+        const int warm = pl->warm_mode && (contiguous || ordered) ? 1 : 0;
+        if ((st = run_orth_eigen(pl, pl->d_gC, pl->nn, nb, warm)) != WNLQG_OK) return st;
+        gen_back_substitute_kernel<<<(unsigned)std::min<int64_t>(nb, (int64_t)pl->sm_count * 16), 128, 0, pl->stream>>>(
+            pl->d_gL, pl->d_U, nb, pl->nw);
+        pl->launches += 2;
+    } else if (pl->nonorth) {
         if (pl->d_eigh_scratch)
             generalized_eigh_kernel<true><<<eigh_grid, pl->eigh_threads, 0, pl->stream>>>(
                 pl->d_xw + (int64_t)pl->ch_H * pl->nn, pl->d_xw + (int64_t)pl->ch_S * pl->nn, N, nb, pl->nw, pl->d_E,
@@ -780,73 +879,11 @@ wnlqg_status run_front(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const int64_
             generalized_eigh_kernel<false><<<eigh_grid, pl->eigh_threads, pl->eigh_smem, pl->stream>>>(
                 pl->d_xw + (int64_t)pl->ch_H * pl->nn, pl->d_xw + (int64_t)pl->ch_S * pl->nn, N, nb, pl->nw, pl->d_E,
                 pl->d_U, pl->d_status);
-    } else if (pl->warp_eigh) {
-        // Stage 1: four one-warp teams per 128-thread block, or one 64-thread team per block.
-        // Stage 2: 64-thread blocks holding two one-warp teams or one 64-thread team.
-        const int tm = pl->eigh_team;
-        const void *f32_fn = tm == 128 ? (const void *)jacobi_f32_team_kernel<128>
-                             : tm == 64 ? (const void *)jacobi_f32_team_kernel<64> : (const void *)jacobi_f32_team_kernel<32>;
-        const void *ref_fn = tm == 128 ? (const void *)eigh_refine_f64_team_kernel<128>
-                             : tm == 64 ? (const void *)eigh_refine_f64_team_kernel<64> : (const void *)eigh_refine_f64_team_kernel<32>;
-        const int f32_threads = tm == 32 ? 128 : tm, f32_teams = tm == 32 ? 4 : 1;
-        const int ref_threads = tm == 128 ? 128 : 64, ref_teams = tm == 32 ? 2 : 1;
-        int per_sm = 1;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f32_fn, f32_threads, pl->eigh_smem);
-        const int64_t f32_grid = std::min<int64_t>((nb + f32_teams - 1) / f32_teams, (int64_t)std::max(1, per_sm) * pl->sm_count);
-        // Consecutive mesh points are neighbours: warm-start the Jacobi iteration along the run.
-        // Arbitrary points in Morton order (ordered) are neighbours along the run as well.
-        int warm = pl->warm_mode && ((mesh != nullptr && kpts_device == nullptr && kidx_device == nullptr) || ordered) ? 1 : 0;
-        const double2 *hk = pl->d_xw + (int64_t)pl->ch_H * pl->nn;
-        {
-            int64_t nb_arg = nb;
-            int nw_arg = pl->nw;
-            float2 *v32 = pl->d_V32;
-            int64_t stride = N;
-            void *args[] = {(void *)&hk, &stride, &nb_arg, &nw_arg, &v32, &warm};
-            WNLQG_CUDA(cudaLaunchKernel(f32_fn, dim3((unsigned)f32_grid), dim3(f32_threads), args, pl->eigh_smem, pl->stream));
-        }
-        int per_sm_r = 1;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_r, ref_fn, ref_threads, pl->refine_smem);
-        const int64_t r_grid = std::min<int64_t>((nb + ref_teams - 1) / ref_teams, (int64_t)std::max(1, per_sm_r) * pl->sm_count);
-        {
-            int64_t stride = N, nb_arg = nb;
-            int nw_arg = pl->nw;
-            const float2 *v32 = pl->d_V32;
-            double *E = pl->d_E;
-            double2 *U = pl->d_U;
-            int converge = pl->task.precision == WNLQG_PRECISION_MIXED ? 0 : 1;
-            void *args[] = {(void *)&hk, &stride, (void *)&v32, &nb_arg, &nw_arg, &E, &U, &converge};
-            WNLQG_CUDA(cudaLaunchKernel(ref_fn, dim3((unsigned)r_grid), dim3(ref_threads), args, pl->refine_smem, pl->stream));
-        }
-        pl->launches += 1;
-    } else if (pl->cta_mixed) {
-        const double2 *hk = pl->d_xw + (int64_t)pl->ch_H * pl->nn;
-        const int converge = pl->task.precision == WNLQG_PRECISION_MIXED ? 0 : 1;
-        // Mesh runs and Morton-ordered point batches warm-start along each CTA's range.
-        const int warm =
-            pl->warm_mode && ((mesh != nullptr && kpts_device == nullptr && kidx_device == nullptr) || ordered) ? 1 : 0;
-        if (pl->cta_gw1) {
-            jacobi_f32_cta_kernel<true><<<(unsigned)std::min<int64_t>(nb, pl->eigh_grid), 256, 0, pl->stream>>>(
-                hk, N, nb, pl->nw, pl->d_V32, pl->d_eigh_scratch, pl->eigh_scratch_stride, warm);
-        } else {
-            int per_sm = 1;
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jacobi_f32_cta_kernel<false>, 256, pl->eigh_smem);
-            const int64_t grid = std::min<int64_t>(nb, (int64_t)std::max(1, per_sm) * pl->sm_count);
-            jacobi_f32_cta_kernel<false><<<(unsigned)grid, 256, pl->eigh_smem, pl->stream>>>(hk, N, nb, pl->nw, pl->d_V32,
-                                                                                            nullptr, 0, warm);
-        }
-        if (pl->cta_gw2) {
-            eigh_refine_f64_cta_kernel<true><<<(unsigned)std::min<int64_t>(nb, pl->eigh_grid), pl->refine_cta_threads, 0, pl->stream>>>(
-                hk, N, pl->d_V32, nb, pl->nw, pl->d_E, pl->d_U, converge, pl->d_eigh_scratch, pl->eigh_scratch_stride);
-        } else {
-            int per_sm = 1;
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, eigh_refine_f64_cta_kernel<false>, pl->refine_cta_threads,
-                                                          pl->refine_smem);
-            const int64_t grid = std::min<int64_t>(nb, (int64_t)std::max(1, per_sm) * pl->sm_count);
-            eigh_refine_f64_cta_kernel<false><<<(unsigned)grid, pl->refine_cta_threads, pl->refine_smem, pl->stream>>>(
-                hk, N, pl->d_V32, nb, pl->nw, pl->d_E, pl->d_U, converge, nullptr, 0);
-        }
-        pl->launches += 1;
+    } else if (pl->warp_eigh || pl->cta_mixed) {
+        const bool contiguous = mesh != nullptr && kpts_device == nullptr && kidx_device == nullptr;
+        // Mesh runs and Morton-ordered point batches warm-start the FP32 stage along the run.
+        const int warm = pl->warm_mode && (contiguous || ordered) ? 1 : 0;
+        if ((st = run_orth_eigen(pl, pl->d_xw + (int64_t)pl->ch_H * pl->nn, N, nb, warm)) != WNLQG_OK) return st;
     } else
         if (pl->d_eigh_scratch)
             jacobi_eigh_kernel<double, true><<<eigh_grid, pl->eigh_threads, 0, pl->stream>>>(
@@ -1050,7 +1087,8 @@ wnlqg_status wnlqg_b200_plan_destroy(wnlqg_plan *pl) {
                       (void *)pl->d_tc_err, (void *)pl->d_shg_gscratch, (void *)pl->d_eigh_scratch,
                       (void *)pl->d_resp_scratch, (void *)pl->d_ng_r, (void *)pl->d_ng_v, (void *)pl->d_ng_G,
                       (void *)pl->d_ng_ws, (void *)pl->d_mshg_src, (void *)pl->d_mshg_diag, (void *)pl->d_mshg_ws,
-                      (void *)pl->d_okeys, (void *)pl->d_operm, (void *)pl->d_ok, (void *)pl->d_ow, pl->d_osort_tmp})
+                      (void *)pl->d_okeys, (void *)pl->d_operm, (void *)pl->d_ok, (void *)pl->d_ow, pl->d_osort_tmp,
+                      (void *)pl->d_gC, (void *)pl->d_gL, (void *)pl->d_gred_scratch})
         if (ptr) cudaFree(ptr);
     for (cudaEvent_t ev : pl->events) cudaEventDestroy(ev);
     if (pl->stream) cudaStreamDestroy(pl->stream);
@@ -1391,6 +1429,7 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
     if (max_batch <= 0) {
         int64_t per_k = (int64_t)pl->C * nn * 16 + (int64_t)nr * 16 + nn * 16 + nw * 8 + vc * 16;
         if (pl->metric_shg) per_k += MetricShgWs::src_entries(nw) * 16 + MetricShgWs::diag_entries(nw) * 8;
+        if (pl->nonorth && t.precision == WNLQG_PRECISION_MIXED) per_k += 2 * nn * 16 + nn * 8;
         // About 4 GiB of batch workspace (HBM is 180 GB): long runs of neighbouring k-points per
         // CTA for the warm-started eigensolver and few batches per call.
         max_batch = std::max<int64_t>(256, std::min<int64_t>(1 << 20, ((int64_t)1 << 32) / per_k));
@@ -1540,15 +1579,21 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
     {
         const char *cta = std::getenv("WNLQG_B200_CTA_EIGH");
         const bool cta_fp64 = cta && cta[0] == '1' && t.precision != WNLQG_PRECISION_MIXED;
-        pl->warp_eigh = !pl->nonorth && nw <= 32 && !cta_fp64;
+        // Nonorthogonal models on the mixed path reduce to C = L^-1 H L^-H in FP64 and then take
+        // the orthogonal mixed-precision stages (WNLQG_B200_GEN_MIXED=0 keeps the FP64 generalised
+        // Jacobi).
+        const char *gm = std::getenv("WNLQG_B200_GEN_MIXED");
+        pl->gen_mixed = pl->nonorth && t.precision == WNLQG_PRECISION_MIXED && !(gm && gm[0] == '0');
+        const bool orth_stages = !pl->nonorth || pl->gen_mixed;
+        pl->warp_eigh = orth_stages && nw <= 32 && !cta_fp64;
         // Above 32 orbitals the CTA FP32 + FP64 stages; on the FP64 path only once two FP64 CTA
         // Jacobi working sets no longer fit one SM (there the plain FP64 Jacobi is faster).
         const bool fp64_cta_pair_fits =
             2 * (EighSmem::bytes(nw, sizeof(double2)) + 512) <= (size_t)smem_optin;
-        pl->cta_mixed = !pl->nonorth && nw > 32 && !cta_fp64 &&
+        pl->cta_mixed = orth_stages && nw > 32 && !cta_fp64 &&
                         (t.precision == WNLQG_PRECISION_MIXED || !fp64_cta_pair_fits);
     }
-    if (pl->nonorth) {
+    if (pl->nonorth && !pl->gen_mixed) {
         pl->eigh_threads = std::max(pl->eigh_threads, ((nw + (nw & 1)) / 2 + 31) / 32 * 32);
         pl->eigh_smem = GenEighSmem::bytes(nw);
     } else if (pl->warp_eigh) {
@@ -1633,6 +1678,24 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
             pl->eigh_smem = 0;
         } else {
             cudaError_t e = allow_dynamic_smem(cta_fn, smem_optin);
+            if (e != cudaSuccess) return bail(fail(WNLQG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e)));
+        }
+    }
+    if (pl->gen_mixed) {
+        if ((st = alloc((void **)&pl->d_gC, (size_t)max_batch * nn * sizeof(double2))) != WNLQG_OK) return bail(st);
+        if ((st = alloc((void **)&pl->d_gL, (size_t)max_batch * nn * sizeof(double2))) != WNLQG_OK) return bail(st);
+        pl->gred_smem = GenReduceSmem::bytes(nw);
+        cudaFuncAttributes fa;
+        cudaError_t fe = cudaFuncGetAttributes(&fa, (const void *)cholesky_reduce_kernel<false>);
+        if (fe != cudaSuccess) return bail(fail(WNLQG_ERR_CUDA, std::string("cudaFuncGetAttributes: ") + cudaGetErrorString(fe)));
+        if (pl->gred_smem + fa.sharedSizeBytes > (size_t)smem_optin) {
+            pl->gred_gw = true;
+            pl->gred_stride = (int64_t)((pl->gred_smem + 255) & ~(size_t)255);
+            pl->gred_grid = l2_resident_grid(4 * sm_count, pl->gred_stride, sm_count);
+            if ((st = alloc((void **)&pl->d_gred_scratch, (size_t)pl->gred_grid * pl->gred_stride)) != WNLQG_OK)
+                return bail(st);
+        } else {
+            cudaError_t e = allow_dynamic_smem((const void *)cholesky_reduce_kernel<false>, smem_optin);
             if (e != cudaSuccess) return bail(fail(WNLQG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e)));
         }
     }
