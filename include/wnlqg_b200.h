@@ -299,9 +299,11 @@ WNLQG_API wnlqg_status wnlqg_b200_graph_destroy(wnlqg_graph *graph);
  * 128 threads per matrix; orthogonal models up to 32 orbitals), the FP32 eigensolver stage's
  * start (warm from the previous point along mesh runs and ordered batches, or cold from the
  * identity; orthogonal models on the team or CTA mixed-precision stages), every contraction
- * tile (1, 2 and 4 photon energies per thread; frequency-resolved responses) and the FP64
+ * tile (1, 2 and 4 photon energies per thread; frequency-resolved responses), the FP64
  * response CTA width (256 or 512 threads; orthogonal models whose per-point working set fits
- * shared memory), keeps the fastest of each in
+ * shared memory) and the grids of the second-harmonic kernels whose working sets live in global
+ * memory (metric inputs: 1, 2, 4 CTAs per SM; second harmonic: the L2-resident grid, 1, 2 CTAs
+ * per SM), keeps the fastest of each in
  * the plan and remembers it for the process (key: device, orbitals, precision, geometry, photon
  * energies, value count), so later plans with the same key take it without measuring.  Every
  * candidate is a configuration the library runs anyway; the tile choice leaves results bitwise
@@ -317,6 +319,10 @@ typedef struct wnlqg_autotune_report {
     double start_ms[2];            /* eigensolve time with a cold and a warm start */
     int32_t response_threads;      /* chosen FP64 response CTA width (256, 512), -1 = not tunable */
     double width_ms[2];            /* response time with 256 and 512 threads per CTA */
+    int32_t metric_shg_grid;       /* chosen CTAs of the metric SHG input kernel, -1 = none */
+    double metric_shg_grid_ms[3];  /* response time with 1, 2 and 4 CTAs per SM */
+    int32_t shg_grid;              /* chosen CTAs of the SHG kernel's global working-set variant, -1 = none */
+    double shg_grid_ms[3];         /* response time with the L2-resident grid, 1 and 2 CTAs per SM */
 } wnlqg_autotune_report;
 WNLQG_API wnlqg_status wnlqg_b200_plan_autotune(wnlqg_plan *plan, const int64_t mesh[3], int64_t k_begin,
                                       int64_t k_end, wnlqg_autotune_report *report);

@@ -113,6 +113,10 @@ struct AutotuneReport
     start_ms::NTuple{2, Float64}
     response_threads::Int32
     width_ms::NTuple{2, Float64}
+    metric_shg_grid::Int32
+    metric_shg_grid_ms::NTuple{3, Float64}
+    shg_grid::Int32
+    shg_grid_ms::NTuple{3, Float64}
 end
 
 """Pick the eigensolver team and contraction tile by timing them on mesh indices [first, last)."""

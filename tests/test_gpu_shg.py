@@ -230,3 +230,24 @@ def test_metric_shg_nw64_matches_oracle(engine_cls, oracle_mod):
         got = eng.point_values(k)
     ref = oracle_mod.point_values(model, task, k)
     assert block_err(task.split(got)[0], task.split(ref)[0]) < RTOL
+
+
+def test_metric_shg_autotuned_grids_keep_results(engine_cls, oracle_mod):
+    """The autotuner's grid choices for the metric input kernel (1, 2, 4 CTAs per SM) and the SHG
+    kernel's global working set (the L2-resident grid, 1, 2 CTAs per SM) change no result: mesh
+    sums before and after tuning agree to 1e-12, and the tuned point values match the oracle."""
+    from wanniernlqg_b200.model import synthetic_nonorthogonal_model
+    model = synthetic_nonorthogonal_model(64, 1, seed=9, full_position=True)
+    task = metric_task(components=[(0, 0, 0)], omegas=(0.4, 1.2), T=0.0, mu=0.0)
+    mesh = (8, 8, 8)
+    with engine_cls(model, task, max_batch=256) as eng:
+        before = eng.integrate_mesh(mesh, 0, 256)
+        rep = eng.autotune(mesh, 0, 256)
+        after = eng.integrate_mesh(mesh, 0, 256)
+        k = np.random.default_rng(10).random((2, 3))
+        got = eng.point_values(k)
+    assert rep["metric_shg_grid"] > 0 and len(rep["metric_shg_grid_ms"]) == 3
+    assert rep["shg_grid"] > 0 and len(rep["shg_grid_ms"]) == 3
+    assert np.max(np.abs(after - before)) <= 1e-12 * np.max(np.abs(before))
+    ref = oracle_mod.point_values(model, task, k)
+    assert block_err(task.split(got)[0], task.split(ref)[0]) < RTOL

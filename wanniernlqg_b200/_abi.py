@@ -74,6 +74,10 @@ class AutotuneReport(ctypes.Structure):
         ("start_ms", ctypes.c_double * 2),
         ("response_threads", ctypes.c_int32),
         ("width_ms", ctypes.c_double * 2),
+        ("metric_shg_grid", ctypes.c_int32),
+        ("metric_shg_grid_ms", ctypes.c_double * 3),
+        ("shg_grid", ctypes.c_int32),
+        ("shg_grid_ms", ctypes.c_double * 3),
     ]
 
 

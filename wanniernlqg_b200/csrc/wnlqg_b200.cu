@@ -104,6 +104,8 @@ struct wnlqg_plan {
     std::vector<ShgParams> shg;
     size_t shg_smem = 0;
     int shg_grid = 0;
+    int shg_grid_alloc = 0;   // CTAs the scratch is allocated for (the largest grid a launch may take)
+    int shg_grid_l2 = 0;      // global working set: the grid whose sets stay L2-resident
     double2 *d_shg_scratch = nullptr;
     unsigned char *d_shg_gscratch = nullptr;
     bool shg_global = false;
@@ -142,6 +144,7 @@ struct wnlqg_plan {
     bool metric_shg = false;
     MetricShgParams mshg;
     int mshg_grid = 0;
+    int mshg_grid_alloc = 0;
     double2 *d_mshg_src = nullptr;
     double *d_mshg_diag = nullptr;
     unsigned char *d_mshg_ws = nullptr;
@@ -555,17 +558,25 @@ wnlqg_status build_shg(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
     if (e != cudaSuccess) return fail(WNLQG_ERR_CUDA, std::string("occupancy query: ") + cudaGetErrorString(e));
     if (per_sm < 1) return fail(WNLQG_ERR_UNSUPPORTED, "second-harmonic kernel cannot be resident with its shared memory");
     pl->shg_grid = sm_count * per_sm;
-    if (shg_global) pl->shg_grid = l2_resident_grid(pl->shg_grid, (int64_t)shg_bytes, sm_count);
+    // A global working set is allocated for up to two CTAs per SM; one CTA per SM is the default
+    // (measured at 64 orbitals: the L2-resident half grid is slower), the autotuner may change it.
+    pl->shg_grid_alloc = shg_global ? std::max(pl->shg_grid, 2 * sm_count) : pl->shg_grid;
+    if (shg_global) {
+        pl->shg_grid_l2 = l2_resident_grid(pl->shg_grid, (int64_t)shg_bytes, sm_count);
+        pl->shg_grid = sm_count;
+    }
+    if (const char *g = std::getenv("WNLQG_B200_SHG_GRID"))
+        pl->shg_grid = std::max(1, std::min(pl->shg_grid_alloc, std::atoi(g)));
     const int64_t stride = ShgSmem::scratch_entries(pl->nw, max_nc);
     for (ShgParams &p : pl->shg) p.scratch_stride = stride;
-    e = cudaMalloc(&pl->d_shg_scratch, (size_t)pl->shg_grid * stride * sizeof(double2));
+    e = cudaMalloc(&pl->d_shg_scratch, (size_t)pl->shg_grid_alloc * stride * sizeof(double2));
     if (e != cudaSuccess) {
         cudaGetLastError();
         return fail(WNLQG_ERR_OUT_OF_MEMORY, "cudaMalloc of the second-harmonic scratch failed");
     }
     if (shg_global) {
         const int64_t gstride = (int64_t)((shg_bytes + 255) & ~(size_t)255);
-        e = cudaMalloc(&pl->d_shg_gscratch, (size_t)pl->shg_grid * gstride);
+        e = cudaMalloc(&pl->d_shg_gscratch, (size_t)pl->shg_grid_alloc * gstride);
         if (e != cudaSuccess) {
             cudaGetLastError();
             return fail(WNLQG_ERR_OUT_OF_MEMORY, "cudaMalloc of the second-harmonic working set failed");
@@ -1478,12 +1489,17 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
         ms.ld = nw + 1;
         ms.xw_stride = (int64_t)pl->C * nn;
         ms.ws_stride = (MetricShgWs::bytes(nw) + 255) & ~(int64_t)255;
-        pl->mshg_grid = sm_count;   // one CTA per SM: its products reuse the working set from L1 / L2
+        // Metric inputs: up to four CTAs per SM over the per-CTA global working sets; two by default
+        // (measured at 64 orbitals), the autotuner may change it.
+        pl->mshg_grid_alloc = 4 * sm_count;
+        pl->mshg_grid = 2 * sm_count;
+        if (const char *g = std::getenv("WNLQG_B200_MSHG_GRID"))
+            pl->mshg_grid = std::max(1, std::min(pl->mshg_grid_alloc, std::atoi(g)));
         if ((st = alloc((void **)&pl->d_mshg_src, (size_t)max_batch * MetricShgWs::src_entries(nw) * sizeof(double2))) != WNLQG_OK)
             return bail(st);
         if ((st = alloc((void **)&pl->d_mshg_diag, (size_t)max_batch * MetricShgWs::diag_entries(nw) * sizeof(double))) != WNLQG_OK)
             return bail(st);
-        if ((st = alloc((void **)&pl->d_mshg_ws, (size_t)pl->mshg_grid * ms.ws_stride)) != WNLQG_OK) return bail(st);
+        if ((st = alloc((void **)&pl->d_mshg_ws, (size_t)pl->mshg_grid_alloc * ms.ws_stride)) != WNLQG_OK) return bail(st);
         ms.src = pl->d_mshg_src;
         ms.diag = pl->d_mshg_diag;
         ms.ws = pl->d_mshg_ws;
@@ -1713,7 +1729,7 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
     if ((st = build_passes(pl, sm_count, (size_t)smem_optin)) != WNLQG_OK) return bail(st);
     if ((st = build_shg(pl, sm_count, (size_t)smem_optin)) != WNLQG_OK) return bail(st);
     for (const Pass &ps : pl->passes) pl->partial_slots = std::max(pl->partial_slots, std::max(ps.grid, ps.grid_wide));
-    pl->partial_slots = std::max(pl->partial_slots, pl->shg_grid);
+    pl->partial_slots = std::max(pl->partial_slots, pl->shg_grid_alloc);
     if ((st = alloc((void **)&pl->d_partials, (size_t)pl->partial_slots * vc * 4 * sizeof(double))) != WNLQG_OK)
         return bail(st);
     *out_plan = pl;
@@ -2314,7 +2330,7 @@ wnlqg_status wnlqg_b200_graph_destroy(wnlqg_graph *graph) {
 // ---------------------------------------------------------------------------------------------
 namespace {
 
-struct TuneChoice { int team; int omb; int warm; int wide; wnlqg_autotune_report report; };
+struct TuneChoice { int team; int omb; int warm; int wide; int mshg_grid; int shg_grid; wnlqg_autotune_report report; };
 std::map<std::tuple<int, int, int, int, int64_t, int64_t>, TuneChoice> g_tune_cache;
 std::mutex g_tune_mutex;
 
@@ -2362,6 +2378,8 @@ extern "C" wnlqg_status wnlqg_b200_plan_autotune(wnlqg_plan *pl, const int64_t m
             if (pl->warp_eigh && it->second.team) apply_team(pl, it->second.team);
             if (it->second.warm >= 0) pl->warm_mode = it->second.warm;
             if (it->second.wide >= 0) pl->resp_wide = it->second.wide == 1;
+            if (it->second.mshg_grid > 0) pl->mshg_grid = it->second.mshg_grid;
+            if (it->second.shg_grid > 0) pl->shg_grid = it->second.shg_grid;
             apply_omb(pl, it->second.omb);
             if (report) {
                 *report = it->second.report;
@@ -2377,6 +2395,8 @@ extern "C" wnlqg_status wnlqg_b200_plan_autotune(wnlqg_plan *pl, const int64_t m
     rep.start_ms[0] = rep.start_ms[1] = -1.0;
     rep.response_threads = -1;
     rep.width_ms[0] = rep.width_ms[1] = -1.0;
+    rep.metric_shg_grid = rep.shg_grid = -1;
+    for (int i = 0; i < 3; ++i) rep.metric_shg_grid_ms[i] = rep.shg_grid_ms[i] = -1.0;
     const int teams[3] = {32, 64, 128}, ombs[3] = {1, 2, 4};
     if (pl->warp_eigh) {
         const int start = pl->eigh_team;
@@ -2437,10 +2457,39 @@ extern "C" wnlqg_status wnlqg_b200_plan_autotune(wnlqg_plan *pl, const int64_t m
         pl->resp_wide = rep.width_ms[1] < rep.width_ms[0];
         rep.response_threads = pl->resp_wide ? 512 : 256;
     }
+    if (pl->metric_shg && !pl->shg.empty()) {
+        const int start = pl->mshg_grid;
+        const int cand[3] = {pl->sm_count, 2 * pl->sm_count, 4 * pl->sm_count};
+        double best = std::numeric_limits<double>::infinity(), e = 0;
+        for (int i = 0; i < 3; ++i) {
+            pl->mshg_grid = std::min(cand[i], pl->mshg_grid_alloc);
+            if ((st = tune_measure(pl, mesh, k_begin, k_end, &e, &rep.metric_shg_grid_ms[i])) != WNLQG_OK) {
+                pl->mshg_grid = start;
+                return st;
+            }
+            if (rep.metric_shg_grid_ms[i] < best) { best = rep.metric_shg_grid_ms[i]; rep.metric_shg_grid = pl->mshg_grid; }
+        }
+        pl->mshg_grid = rep.metric_shg_grid;
+    }
+    if (pl->shg_global && !pl->shg.empty()) {
+        const int start = pl->shg_grid;
+        const int cand[3] = {pl->shg_grid_l2, pl->sm_count, 2 * pl->sm_count};
+        double best = std::numeric_limits<double>::infinity(), e = 0;
+        for (int i = 0; i < 3; ++i) {
+            pl->shg_grid = std::max(1, std::min(cand[i], pl->shg_grid_alloc));
+            if ((st = tune_measure(pl, mesh, k_begin, k_end, &e, &rep.shg_grid_ms[i])) != WNLQG_OK) {
+                pl->shg_grid = start;
+                return st;
+            }
+            if (rep.shg_grid_ms[i] < best) { best = rep.shg_grid_ms[i]; rep.shg_grid = pl->shg_grid; }
+        }
+        pl->shg_grid = rep.shg_grid;
+    }
     {
         std::lock_guard<std::mutex> lock(g_tune_mutex);
         g_tune_cache[key] = TuneChoice{rep.eigh_team, rep.energies_per_thread, rep.warm_start,
-                                       rep.response_threads < 0 ? -1 : (rep.response_threads == 512 ? 1 : 0), rep};
+                                       rep.response_threads < 0 ? -1 : (rep.response_threads == 512 ? 1 : 0),
+                                       rep.metric_shg_grid, rep.shg_grid, rep};
     }
     if (report) *report = rep;
     return WNLQG_OK;

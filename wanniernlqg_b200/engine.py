@@ -171,6 +171,10 @@ class ResponseEngine:
                 "start_ms": ({"cold": rep.start_ms[0], "warm": rep.start_ms[1]} if rep.warm_start >= 0 else {}),
                 "response_threads": rep.response_threads,
                 "width_ms": ({256: rep.width_ms[0], 512: rep.width_ms[1]} if rep.response_threads > 0 else {}),
+                "metric_shg_grid": rep.metric_shg_grid,
+                "metric_shg_grid_ms": list(rep.metric_shg_grid_ms) if rep.metric_shg_grid > 0 else [],
+                "shg_grid": rep.shg_grid,
+                "shg_grid_ms": list(rep.shg_grid_ms) if rep.shg_grid > 0 else [],
                 "from_cache": bool(rep.from_cache)}
 
 
