@@ -303,7 +303,8 @@ WNLQG_API wnlqg_status wnlqg_b200_graph_destroy(wnlqg_graph *graph);
  * response CTA width (256 or 512 threads; orthogonal models whose per-point working set fits
  * shared memory) and the grids of the second-harmonic kernels whose working sets live in global
  * memory (metric inputs: 1, 2, 4 CTAs per SM; second harmonic: the L2-resident grid, 1, 2 CTAs
- * per SM), keeps the fastest of each in
+ * per SM), and likewise the grids of response passes and eigensolver stages whose per-CTA working
+ * sets live in global memory (large orbital counts), keeps the fastest of each in
  * the plan and remembers it for the process (key: device, orbitals, precision, geometry, photon
  * energies, value count), so later plans with the same key take it without measuring.  Every
  * candidate is a configuration the library runs anyway; the tile choice leaves results bitwise
@@ -323,6 +324,11 @@ typedef struct wnlqg_autotune_report {
     double metric_shg_grid_ms[3];  /* response time with 1, 2 and 4 CTAs per SM */
     int32_t shg_grid;              /* chosen CTAs of the SHG kernel's global working-set variant, -1 = none */
     double shg_grid_ms[3];         /* response time with the L2-resident grid, 1 and 2 CTAs per SM */
+    int32_t response_grid;         /* chosen grid of response passes with global working sets
+                                      (0 = each pass's L2-resident grid), -1 = none */
+    double response_grid_ms[3];    /* response time with the L2-resident grids, 1 and 2 CTAs per SM */
+    int32_t eigh_grid;             /* chosen grid of eigensolver stages with global working sets, -1 = none */
+    double eigh_grid_ms[3];        /* eigensolve time with the L2-resident grid, 1 and 2 CTAs per SM */
 } wnlqg_autotune_report;
 WNLQG_API wnlqg_status wnlqg_b200_plan_autotune(wnlqg_plan *plan, const int64_t mesh[3], int64_t k_begin,
                                       int64_t k_end, wnlqg_autotune_report *report);

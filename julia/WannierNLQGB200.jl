@@ -117,6 +117,10 @@ struct AutotuneReport
     metric_shg_grid_ms::NTuple{3, Float64}
     shg_grid::Int32
     shg_grid_ms::NTuple{3, Float64}
+    response_grid::Int32
+    response_grid_ms::NTuple{3, Float64}
+    eigh_grid::Int32
+    eigh_grid_ms::NTuple{3, Float64}
 end
 
 """Pick the eigensolver team and contraction tile by timing them on mesh indices [first, last)."""

@@ -78,6 +78,10 @@ class AutotuneReport(ctypes.Structure):
         ("metric_shg_grid_ms", ctypes.c_double * 3),
         ("shg_grid", ctypes.c_int32),
         ("shg_grid_ms", ctypes.c_double * 3),
+        ("response_grid", ctypes.c_int32),
+        ("response_grid_ms", ctypes.c_double * 3),
+        ("eigh_grid", ctypes.c_int32),
+        ("eigh_grid_ms", ctypes.c_double * 3),
     ]
 
 

@@ -131,11 +131,15 @@ struct wnlqg_plan {
     unsigned char *d_eigh_scratch = nullptr;  // per-CTA global working set of the CTA eigensolvers
     int64_t eigh_scratch_stride = 0;
     int eigh_grid = 0;
+    int eigh_grid_alloc = 0;                  // CTAs the eigensolver working sets are allocated for
+    int eigh_grid_l2 = 0;                     // the grid whose working sets stay L2-resident
     unsigned char *d_resp_scratch = nullptr;  // per-CTA global working set of the response passes
+    int resp_gw_grid = 0;                     // grid of the global working-set passes; 0 = each pass's own
     int64_t resp_scratch_stride = 0;
     // Nonorthogonal responses: metric geometry per batch (Berry connection, slopes, G pairs).
     NonorthParams ng;
     int ng_grid = 0;
+    int ng_grid_alloc = 0;
     int ng_gidx[9];
     double2 *d_ng_r = nullptr, *d_ng_G = nullptr;
     double *d_ng_v = nullptr;
@@ -482,12 +486,15 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
     }
     bool any_global = false;
     for (const Pass &ps : pl->passes) any_global |= ps.global;
+    // Global working-set passes default to two CTAs per SM (measured at 96 and 128 orbitals: 1.8-2.9x
+    // faster than the L2-resident grids); the autotuner may pick another grid.
+    if (any_global) pl->resp_gw_grid = 2 * sm_count;
     if (any_global) {
         int64_t grid = 0;
         size_t bytes = 0;
         for (const Pass &ps : pl->passes) {
             if (!ps.global) continue;
-            grid = std::max<int64_t>(grid, ps.grid);
+            grid = std::max<int64_t>(grid, std::max(ps.grid, 2 * sm_count));   // up to two CTAs per SM
             bytes = std::max(bytes, ps.smem);
         }
         pl->resp_scratch_stride = (int64_t)((bytes + 255) & ~(size_t)255);
@@ -949,7 +956,8 @@ wnlqg_status run_passes(wnlqg_plan *pl, int64_t nb, int mode, double scale, int6
             WNLQG_CUDA(cudaLaunchKernel(response_wide_fn(), dim3(ps.grid_wide), dim3(512), args, launch_smem, pl->stream));
         else
             WNLQG_CUDA(cudaLaunchKernel(response_fn(pl->task.precision == WNLQG_PRECISION_MIXED, pl->nonorth, ps.global),
-                                        dim3(ps.grid), dim3(ps.threads), args, launch_smem, pl->stream));
+                                        dim3(ps.global && pl->resp_gw_grid > 0 ? pl->resp_gw_grid : ps.grid),
+                                        dim3(ps.threads), args, launch_smem, pl->stream));
         pl->launches += 1;
     }
     if (pl->metric_shg && !pl->shg.empty()) {
@@ -1472,12 +1480,18 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
         q.ld = nw + 1;
         q.xw_stride = (int64_t)pl->C * nn;
         q.ws_stride = (NonorthWs::bytes(nw) + 255) & ~(int64_t)255;
-        pl->ng_grid = l2_resident_grid(2 * sm_count, q.ws_stride, sm_count);
+        // Two CTAs per SM over the per-CTA global working sets (measured at 64 orbitals: the
+        // L2-resident grid takes twice as long).
+        pl->ng_grid_alloc = 2 * sm_count;
+        pl->ng_grid = 2 * sm_count;
+        if (const char *g = std::getenv("WNLQG_B200_NG_GRID"))
+            pl->ng_grid = std::max(1, std::min(pl->ng_grid_alloc, std::atoi(g)));
         if ((st = alloc((void **)&pl->d_ng_r, (size_t)max_batch * 3 * nn * sizeof(double2))) != WNLQG_OK) return bail(st);
         if ((st = alloc((void **)&pl->d_ng_v, (size_t)max_batch * 3 * nw * sizeof(double))) != WNLQG_OK) return bail(st);
         if ((st = alloc((void **)&pl->d_ng_G, (size_t)max_batch * std::max(1, q.npairs) * nn * sizeof(double2))) != WNLQG_OK)
             return bail(st);
-        if ((st = alloc((void **)&pl->d_ng_ws, (size_t)pl->ng_grid * q.ws_stride)) != WNLQG_OK) return bail(st);
+        if ((st = alloc((void **)&pl->d_ng_ws, (size_t)std::max(pl->ng_grid, pl->ng_grid_alloc) * q.ws_stride)) != WNLQG_OK)
+            return bail(st);
         q.r_out = pl->d_ng_r;
         q.v_out = pl->d_ng_v;
         q.g_out = pl->d_ng_G;
@@ -1668,7 +1682,10 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
             const size_t need = std::max(pl->cta_gw1 ? pl->eigh_smem : 0, pl->cta_gw2 ? pl->refine_smem : 0);
             pl->eigh_scratch_stride = (int64_t)((need + 255) & ~(size_t)255);
             pl->eigh_grid = l2_resident_grid(4 * sm_count, pl->eigh_scratch_stride, sm_count);
-            if ((st = alloc((void **)&pl->d_eigh_scratch, (size_t)pl->eigh_grid * pl->eigh_scratch_stride)) != WNLQG_OK)
+            pl->eigh_grid_l2 = pl->eigh_grid;
+            pl->eigh_grid_alloc = std::max(pl->eigh_grid, 2 * sm_count);
+            pl->eigh_grid = 2 * sm_count;   // measured faster than the L2-resident grid; tunable
+            if ((st = alloc((void **)&pl->d_eigh_scratch, (size_t)pl->eigh_grid_alloc * pl->eigh_scratch_stride)) != WNLQG_OK)
                 return bail(st);
         }
         cudaError_t e = cudaSuccess;
@@ -1689,7 +1706,10 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
         if (pl->eigh_smem + fa.sharedSizeBytes > (size_t)smem_optin) {
             pl->eigh_scratch_stride = (int64_t)((pl->eigh_smem + 255) & ~(size_t)255);
             pl->eigh_grid = l2_resident_grid(4 * sm_count, pl->eigh_scratch_stride, sm_count);
-            if ((st = alloc((void **)&pl->d_eigh_scratch, (size_t)pl->eigh_grid * pl->eigh_scratch_stride)) != WNLQG_OK)
+            pl->eigh_grid_l2 = pl->eigh_grid;
+            pl->eigh_grid_alloc = std::max(pl->eigh_grid, 2 * sm_count);
+            pl->eigh_grid = 2 * sm_count;   // measured faster than the L2-resident grid; tunable
+            if ((st = alloc((void **)&pl->d_eigh_scratch, (size_t)pl->eigh_grid_alloc * pl->eigh_scratch_stride)) != WNLQG_OK)
                 return bail(st);
             pl->eigh_smem = 0;
         } else {
@@ -1728,7 +1748,9 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
     }
     if ((st = build_passes(pl, sm_count, (size_t)smem_optin)) != WNLQG_OK) return bail(st);
     if ((st = build_shg(pl, sm_count, (size_t)smem_optin)) != WNLQG_OK) return bail(st);
-    for (const Pass &ps : pl->passes) pl->partial_slots = std::max(pl->partial_slots, std::max(ps.grid, ps.grid_wide));
+    for (const Pass &ps : pl->passes)
+        pl->partial_slots = std::max(pl->partial_slots, std::max(ps.global ? std::max(ps.grid, 2 * sm_count) : ps.grid,
+                                                                   ps.grid_wide));
     pl->partial_slots = std::max(pl->partial_slots, pl->shg_grid_alloc);
     if ((st = alloc((void **)&pl->d_partials, (size_t)pl->partial_slots * vc * 4 * sizeof(double))) != WNLQG_OK)
         return bail(st);
@@ -2330,7 +2352,10 @@ wnlqg_status wnlqg_b200_graph_destroy(wnlqg_graph *graph) {
 // ---------------------------------------------------------------------------------------------
 namespace {
 
-struct TuneChoice { int team; int omb; int warm; int wide; int mshg_grid; int shg_grid; wnlqg_autotune_report report; };
+struct TuneChoice {
+    int team, omb, warm, wide, mshg_grid, shg_grid, resp_grid, eigh_grid;
+    wnlqg_autotune_report report;
+};
 std::map<std::tuple<int, int, int, int, int64_t, int64_t>, TuneChoice> g_tune_cache;
 std::mutex g_tune_mutex;
 
@@ -2380,6 +2405,8 @@ extern "C" wnlqg_status wnlqg_b200_plan_autotune(wnlqg_plan *pl, const int64_t m
             if (it->second.wide >= 0) pl->resp_wide = it->second.wide == 1;
             if (it->second.mshg_grid > 0) pl->mshg_grid = it->second.mshg_grid;
             if (it->second.shg_grid > 0) pl->shg_grid = it->second.shg_grid;
+            if (it->second.resp_grid >= 0) pl->resp_gw_grid = it->second.resp_grid;
+            if (it->second.eigh_grid > 0) pl->eigh_grid = it->second.eigh_grid;
             apply_omb(pl, it->second.omb);
             if (report) {
                 *report = it->second.report;
@@ -2397,6 +2424,23 @@ extern "C" wnlqg_status wnlqg_b200_plan_autotune(wnlqg_plan *pl, const int64_t m
     rep.width_ms[0] = rep.width_ms[1] = -1.0;
     rep.metric_shg_grid = rep.shg_grid = -1;
     for (int i = 0; i < 3; ++i) rep.metric_shg_grid_ms[i] = rep.shg_grid_ms[i] = -1.0;
+    rep.response_grid = rep.eigh_grid = -1;
+    for (int i = 0; i < 3; ++i) rep.response_grid_ms[i] = rep.eigh_grid_ms[i] = -1.0;
+    if (pl->d_eigh_scratch && pl->eigh_grid_alloc > 0) {
+        // Eigensolver stages with per-CTA global working sets: the L2-resident grid, 1 or 2 CTAs per SM.
+        const int start = pl->eigh_grid;
+        const int cand[3] = {pl->eigh_grid_l2, pl->sm_count, 2 * pl->sm_count};
+        double best = std::numeric_limits<double>::infinity(), r = 0;
+        for (int i = 0; i < 3; ++i) {
+            pl->eigh_grid = std::max(1, std::min(cand[i], pl->eigh_grid_alloc));
+            if ((st = tune_measure(pl, mesh, k_begin, k_end, &rep.eigh_grid_ms[i], &r)) != WNLQG_OK) {
+                pl->eigh_grid = start;
+                return st;
+            }
+            if (rep.eigh_grid_ms[i] < best) { best = rep.eigh_grid_ms[i]; rep.eigh_grid = pl->eigh_grid; }
+        }
+        pl->eigh_grid = rep.eigh_grid;
+    }
     const int teams[3] = {32, 64, 128}, ombs[3] = {1, 2, 4};
     if (pl->warp_eigh) {
         const int start = pl->eigh_team;
@@ -2457,6 +2501,22 @@ extern "C" wnlqg_status wnlqg_b200_plan_autotune(wnlqg_plan *pl, const int64_t m
         pl->resp_wide = rep.width_ms[1] < rep.width_ms[0];
         rep.response_threads = pl->resp_wide ? 512 : 256;
     }
+    bool gw_pass = false;
+    for (const Pass &ps : pl->passes) gw_pass |= ps.global;
+    if (gw_pass) {
+        // Response passes with per-CTA global working sets: their L2-resident grids, 1 or 2 CTAs per SM.
+        const int cand[3] = {0, pl->sm_count, 2 * pl->sm_count};
+        double best = std::numeric_limits<double>::infinity(), e = 0;
+        for (int i = 0; i < 3; ++i) {
+            pl->resp_gw_grid = cand[i];
+            if ((st = tune_measure(pl, mesh, k_begin, k_end, &e, &rep.response_grid_ms[i])) != WNLQG_OK) {
+                pl->resp_gw_grid = 0;
+                return st;
+            }
+            if (rep.response_grid_ms[i] < best) { best = rep.response_grid_ms[i]; rep.response_grid = cand[i]; }
+        }
+        pl->resp_gw_grid = rep.response_grid;
+    }
     if (pl->metric_shg && !pl->shg.empty()) {
         const int start = pl->mshg_grid;
         const int cand[3] = {pl->sm_count, 2 * pl->sm_count, 4 * pl->sm_count};
@@ -2489,7 +2549,7 @@ extern "C" wnlqg_status wnlqg_b200_plan_autotune(wnlqg_plan *pl, const int64_t m
         std::lock_guard<std::mutex> lock(g_tune_mutex);
         g_tune_cache[key] = TuneChoice{rep.eigh_team, rep.energies_per_thread, rep.warm_start,
                                        rep.response_threads < 0 ? -1 : (rep.response_threads == 512 ? 1 : 0),
-                                       rep.metric_shg_grid, rep.shg_grid, rep};
+                                       rep.metric_shg_grid, rep.shg_grid, rep.response_grid, rep.eigh_grid, rep};
     }
     if (report) *report = rep;
     return WNLQG_OK;

@@ -175,6 +175,10 @@ class ResponseEngine:
                 "metric_shg_grid_ms": list(rep.metric_shg_grid_ms) if rep.metric_shg_grid > 0 else [],
                 "shg_grid": rep.shg_grid,
                 "shg_grid_ms": list(rep.shg_grid_ms) if rep.shg_grid > 0 else [],
+                "response_grid": rep.response_grid,
+                "response_grid_ms": list(rep.response_grid_ms) if rep.response_grid >= 0 else [],
+                "eigh_grid": rep.eigh_grid,
+                "eigh_grid_ms": list(rep.eigh_grid_ms) if rep.eigh_grid > 0 else [],
                 "from_cache": bool(rep.from_cache)}
 
 
