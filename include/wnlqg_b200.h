@@ -56,7 +56,10 @@ typedef enum wnlqg_response_kind {
     WNLQG_INTRINSIC_AHC = 5,      /* sigma^{ab} Fermi sea over the mu axis, IntrinsicHallOccupations.jl */
     WNLQG_BERRY_DIPOLE = 6,       /* D^{abc} Fermi surface over the mu axis, BerryMultipoleMoments.jl */
     WNLQG_SECOND_HARMONIC = 7,    /* seven-term chi/sigma^{abc}(omega; 2 omega), SecondHarmonicKernels.jl */
-    WNLQG_JERK_CURRENT = 8        /* ordered jerk (abcd)(omega), ConventionalJerkCurrent.jl */
+    WNLQG_JERK_CURRENT = 8,       /* ordered jerk (abcd)(omega), ConventionalJerkCurrent.jl */
+    WNLQG_LINEAR_TRANSPORT_BERRY = 9 /* Berry-curvature channel of the dc linear transport conductivity
+                                        over the mu axis (any temperature), S m^2 per k-point before BZ
+                                        weights and cell volume: LinearTransportKernels.jl:100-163 */
 } wnlqg_response_kind;
 
 typedef enum wnlqg_broadening {
@@ -128,6 +131,20 @@ typedef struct wnlqg_task_desc {
        R + tau_j - tau_i, home-cell connection A - tau, and the similarity D(k) = diag(exp(2 pi i
        k.tau_frac)); orthogonal models only. */
     int32_t wannier_center_convention;
+    /* Spectral gap tolerance in eV (EffectiveTaskConfig.spectral_gap_tolerance, Config.jl:104, reference
+       default 1e-10).  With denominator_regularization = 0 the exact geometry of shift / injection
+       current, Berry curvature, quantum metric and Berry dipole requires every pair of bands at a
+       k-point to be split by more than this (geometry_isolated_spectrum_minimum_gap,
+       OrthogonalBandDerivatives.jl:66-82, called at PositionMatrixElements.jl:447-452); the linear
+       transport Berry channel groups levels closer than 32 eps into blocks and rejects distinct
+       levels split by no more than this (spectral_subspace_blocks, SubspacePositionMatrixElements.jl:5-22).
+       The Berry dipole always requires pairs split by more than degeneracy_threshold
+       (BerryMultipoleGeometry.jl:81, BerryMultipoleDriver.jl:162).  A point that fails makes the call
+       return WNLQG_ERR_INVALID_ARGUMENT with the reference's message. */
+    double spectral_gap_tolerance;
+    /* Interband rate gamma_inter in eV of WNLQG_LINEAR_TRANSPORT_BERRY (the reference's gamma_inter_ev,
+       Config.jl:101; 0 = the clean limit). */
+    double linear_transport_gamma_inter;
 } wnlqg_task_desc;
 
 typedef struct wnlqg_model wnlqg_model;   /* device-resident model */
@@ -236,7 +253,12 @@ WNLQG_API wnlqg_status wnlqg_b200_eval_spectrum(wnlqg_plan *plan, const double *
  * WNLQG_ERR_INVALID_ARGUMENT); nw <= 32.  The first call on a device looks up the scratch
  * address (cudaGetSymbolAddress); make that first call before any stream capture.  All calls
  * share the one scratch array: calls whose GPU work overlaps (other streams, other threads)
- * race on it.  Asynchronous on `stream` (NULL = legacy default stream); allocates nothing. */
+ * race on it.  Asynchronous on `stream` (NULL = legacy default stream).  The call itself
+ * allocates nothing, but the 8 MiB array (with the library's device code) is reserved on each
+ * device when the CUDA runtime loads this library's module there; under lazy module loading
+ * (CUDA_MODULE_LOADING=LAZY, the CUDA 12 default) that happens inside the first call on the
+ * device.  A caller with a fixed device budget should therefore make one warm-up call per device
+ * at initialisation, before it sizes its pool and before any stream capture. */
 WNLQG_API wnlqg_status wnlqg_b200_spectrum_noalloc(int64_t num_orbitals, int64_t num_r_vectors,
                                          const double *hamiltonian_r, const int64_t *r_vectors,
                                          const int64_t *r_degeneracies, const double *kpoints,
@@ -268,6 +290,14 @@ WNLQG_API wnlqg_status wnlqg_b200_plan_last_timing(const wnlqg_plan *plan, doubl
 
 /* Number of kernel launches issued by the last eval_mesh* call. */
 WNLQG_API int64_t wnlqg_b200_plan_last_launch_count(const wnlqg_plan *plan);
+
+/* Device-side errors of the asynchronous entry points (*_device, eval_mesh_many): call after
+ * synchronising the stream they ran on.  Reports, and clears, a bounded device wait that gave up
+ * (WNLQG_ERR_DEVICE_TIMEOUT) and a k-point whose spectrum fails the task's isolation contract
+ * (WNLQG_ERR_INVALID_ARGUMENT, the reference's GEOMETRY_SINGLE_BAND_SPECTRUM_NOT_ISOLATED /
+ * SPECTRAL_CROSS_BLOCK_GAP_UNRESOLVED message; see spectral_gap_tolerance).  The synchronous entry
+ * points run the same checks themselves. */
+WNLQG_API wnlqg_status wnlqg_b200_plan_status(wnlqg_plan *plan);
 
 /* ---- CUDA graphs (no reference counterpart: the reference's worker loop calls its evaluator
  * point by point; here one captured graph replaces a whole call) ------------------------------
@@ -308,7 +338,8 @@ WNLQG_API wnlqg_status wnlqg_b200_graph_destroy(wnlqg_graph *graph);
  * the plan and remembers it for the process (key: device, orbitals, precision, geometry, photon
  * energies, value count), so later plans with the same key take it without measuring.  Every
  * candidate is a configuration the library runs anyway; the tile choice leaves results bitwise
- * unchanged.  Times are CUDA-event milliseconds of the second of two runs; -1 = not a
+ * unchanged, while the grid choices decide how points are split among CTAs, and so the order of
+ * the partial sums, and may change results in the last bits.  Times are CUDA-event milliseconds of the second of two runs; -1 = not a
  * candidate; 0 in a choice = not tunable for this plan. */
 typedef struct wnlqg_autotune_report {
     int32_t eigh_team;             /* chosen threads per matrix (32, 64, 128), 0 = fixed variant */

@@ -13,6 +13,7 @@ const INTRINSIC_AHC = Int32(5)
 const BERRY_DIPOLE = Int32(6)
 const SECOND_HARMONIC = Int32(7)
 const JERK_CURRENT = Int32(8)
+const LINEAR_TRANSPORT_BERRY = Int32(9)
 
 struct ModelDesc
     num_orbitals::Int64
@@ -55,6 +56,8 @@ struct TaskDesc
     valence_bands::NTuple{4, UInt32}           # bit (n - 1) for valence band n
     conduction_bands::NTuple{4, UInt32}        # bit (m - 1) for conduction band m
     wannier_center_convention::Int32           # 0: CONVENTION_II, 1: CONVENTION_I
+    spectral_gap_tolerance::Float64            # cfg.spectral_gap_tolerance (reference default 1e-10)
+    linear_transport_gamma_inter::Float64      # cfg.gamma_inter_ev of the linear transport Berry channel
 end
 
 function check(status)
@@ -142,6 +145,10 @@ function graph_capture_points(plan, kpoints_dev::Ptr{Float64}, weights_dev::Ptr{
                 plan, kpoints_dev, weights_dev, Int64(n), out_dev, g))
     return g[]
 end
+
+"""After synchronising the stream of an asynchronous call: pending device-side errors (a bounded
+wait that gave up; a k-point failing the spectral isolation contract, thrown as ArgumentError)."""
+plan_status(plan) = check(ccall((:wnlqg_b200_plan_status, LIB), Cint, (Ptr{Cvoid},), plan))
 
 graph_launch(g, stream::Ptr{Cvoid} = C_NULL) =
     check(ccall((:wnlqg_b200_graph_launch, LIB), Cint, (Ptr{Cvoid}, Ptr{Cvoid}), g, stream))

@@ -48,12 +48,15 @@ def lib():
                                           ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                           ctypes.c_double, ctypes.c_int64, ctypes.POINTER(ctypes.c_int32), dp]
         L.oracle_kpoint_data.argtypes = [ctypes.POINTER(_abi.ModelDesc), dp, dp, dp, dp, dp, dp]
+        L.oracle_kpoint_geometry.argtypes = [ctypes.POINTER(_abi.ModelDesc), dp, ctypes.c_double, dp, dp, dp, dp,
+                                             dp]
         L.oracle_shg_algebra.argtypes = [ctypes.c_int64, dp, dp, dp, dp, dp, ctypes.c_int64, dp, ctypes.c_int64,
                                          ctypes.POINTER(ctypes.c_int32), ctypes.c_double, ctypes.c_double,
                                          ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                          ctypes.c_int, ctypes.c_double, dp]
         for name in ("oracle_point_values", "oracle_integrate_mesh", "oracle_kpoint_spectrum",
-                     "oracle_hermitian_eigen", "oracle_jerk_algebra", "oracle_kpoint_data", "oracle_shg_algebra"):
+                     "oracle_hermitian_eigen", "oracle_jerk_algebra", "oracle_kpoint_data", "oracle_shg_algebra",
+                     "oracle_kpoint_geometry"):
             getattr(L, name).restype = ctypes.c_int
         _lib = L
     return _lib
@@ -159,6 +162,23 @@ def kpoint_data(model: TightBindingModel, k):
     ddh = np.zeros((nw, nw, 3, 3), dtype=np.complex128, order="F")
     _check(lib().oracle_kpoint_data(ctypes.byref(m.desc), _dp(kk), _dp(e), _dp(dh), _dp(a), _dp(da), _dp(ddh)))
     return e, dh, a, da, ddh
+
+
+def kpoint_geometry(model: TightBindingModel, k, eta: float = 0.0):
+    """Hamiltonian-gauge geometry at one k (canonical gauge): energies[nw], U[nw, nw],
+    r[nw, nw, 3] (A + i D), gder[nw, nw, a, b] = r^a_{nm;b} and F[nw, nw, a, b], at denominator
+    regularization ``eta`` (0: bare inverses)."""
+    nw = model.num_orbitals
+    m = _abi.ModelArrays(model)
+    kk = np.ascontiguousarray(np.asarray(k, dtype=np.float64))
+    e = np.zeros(nw)
+    u = np.zeros((nw, nw), dtype=np.complex128, order="F")
+    r = np.zeros((nw, nw, 3), dtype=np.complex128, order="F")
+    g = np.zeros((nw, nw, 3, 3), dtype=np.complex128, order="F")
+    f = np.zeros((nw, nw, 3, 3), dtype=np.complex128, order="F")
+    _check(lib().oracle_kpoint_geometry(ctypes.byref(m.desc), _dp(kk), float(eta), _dp(e), _dp(u), _dp(r), _dp(g),
+                                        _dp(f)))
+    return e, u, r, g, f
 
 
 def shg_algebra(energies, V, A, dA, W, omegas, components, *, mu=0.0, T=0.0, broadening=0.025,

@@ -797,7 +797,68 @@ struct Task {
     std::vector<double> omegas, mus;
     Needs need;
     int64_t value_count = 0;
+    // Spectral isolation contract: -1 none, 0 every pair split by more than iso_tol
+    // (geometry_isolated_spectrum_minimum_gap), 1 spectral blocks (spectral_subspace_blocks).
+    int iso_mode = -1;
+    double iso_tol = 0.0;
 };
+
+// geometry_isolated_spectrum_minimum_gap (MatrixElements/Interpolated/OrthogonalBandDerivatives.jl:66-82):
+// every pair (l < m, loop over m then l) must be split by more than the tolerance.
+std::string isolated_spectrum_error(const std::vector<double> &E, double tol) {
+    for (double e : E)
+        if (!std::isfinite(e)) return "empty/nonfinite geometry spectrum";
+    char buf[200];
+    for (size_t m = 0; m < E.size(); ++m)
+        for (size_t l = 0; l < m; ++l) {
+            const double gap = std::fabs(E[m] - E[l]);
+            if (!(gap > tol)) {
+                std::snprintf(buf, sizeof(buf),
+                              "GEOMETRY_SINGLE_BAND_SPECTRUM_NOT_ISOLATED: bands=(%d,%d), gap_ev=%.17g, threshold_ev=%.17g",
+                              (int)l + 1, (int)m + 1, gap, tol);
+                return buf;
+            }
+        }
+    return "";
+}
+
+// spectral_subspace_blocks (MatrixElements/Interpolated/SubspacePositionMatrixElements.jl:5-22):
+// levels within 32 eps max(1, max|E|) of a block's first level join it; a new block must be split
+// from the previous level by more than the tolerance.  Returns the 0-based first index of each
+// block followed by E.size(), or sets err.
+std::vector<int> spectral_blocks(const std::vector<double> &E, double tol, std::string &err) {
+    std::vector<int> starts;
+    for (double e : E)
+        if (!std::isfinite(e)) { err = "Invalid spectrum"; return starts; }
+    double emax = 0.0;
+    for (double e : E) emax = std::max(emax, std::fabs(e));
+    const double exact = 32.0 * 2.220446049250313e-16 * std::max(1.0, emax);
+    int start = 0;
+    starts.push_back(0);
+    for (int n = 1; n < (int)E.size(); ++n) {
+        if (E[n] - E[start] > exact) {
+            const double adjacent = E[n] - E[n - 1];
+            if (!(adjacent > tol)) {
+                char buf[120];
+                std::snprintf(buf, sizeof(buf), "SPECTRAL_CROSS_BLOCK_GAP_UNRESOLVED: gap=%.17g eV", adjacent);
+                err = buf;
+                return starts;
+            }
+            starts.push_back(n);
+            start = n;
+        }
+    }
+    starts.push_back((int)E.size());
+    return starts;
+}
+
+// response_occupation (Responses/Shared/ResponseOccupations.jl:8-14).
+double response_occupation(double e, double mu, double T) {
+    if (T == 0.0) return e < mu ? 1.0 : (e > mu ? 0.0 : 0.5);
+    const double x = (e - mu) / (RESPONSE_KB_EV * T);
+    const double z = std::exp(-std::fabs(x));
+    return x >= 0 ? z / (1 + z) : 1 / (1 + z);
+}
 
 bool build_task(const wnlqg_task_desc *t, Task &task) {
     task.desc = *t;
@@ -825,6 +886,10 @@ bool build_task(const wnlqg_task_desc *t, Task &task) {
     task.desc.fermi_energies = task.mus.data();
     if (!(t->broadening > 0) || !std::isfinite(t->broadening)) { set_error("broadening must be finite and positive"); return false; }
     if (!(t->denominator_regularization >= 0)) { set_error("denominator_regularization must be >= 0"); return false; }
+    if (!(std::isfinite(t->spectral_gap_tolerance) && t->spectral_gap_tolerance >= 0)) {
+        set_error("invalid spectral isolation threshold");
+        return false;
+    }
     if (t->num_responses < 1 || t->num_responses > WNLQG_MAX_RESPONSES) { set_error("num_responses out of range"); return false; }
     int64_t count = 0;
     for (int r = 0; r < t->num_responses; ++r) {
@@ -851,6 +916,7 @@ bool build_task(const wnlqg_task_desc *t, Task &task) {
                 break;
             case WNLQG_INTRINSIC_AHC:
             case WNLQG_BERRY_DIPOLE:
+            case WNLQG_LINEAR_TRANSPORT_BERRY:
                 task.need.F[a][b] = true; task.need.need_r(a); task.need.need_r(b);
                 if (q.kind == WNLQG_BERRY_DIPOLE) task.need.dH[cc] = true;
                 break;
@@ -887,7 +953,20 @@ bool build_task(const wnlqg_task_desc *t, Task &task) {
             }
             count += q.num_components * t->num_photon_energies * 14;
         }
-        else if (q.kind == WNLQG_INTRINSIC_AHC || q.kind == WNLQG_BERRY_DIPOLE) {
+        else if (q.kind == WNLQG_INTRINSIC_AHC || q.kind == WNLQG_BERRY_DIPOLE || q.kind == WNLQG_LINEAR_TRANSPORT_BERRY) {
+            // intrinsic_hall_fermi_sea (IntrinsicHallOccupations.jl:15-16) is zero-temperature only.
+            if (q.kind == WNLQG_INTRINSIC_AHC && t->temperature != 0.0) {
+                set_error("INTRINSIC_HALL_REQUIRES_ZERO_TEMPERATURE"); return false;
+            }
+            if (q.kind == WNLQG_LINEAR_TRANSPORT_BERRY) {
+                // spectral_response_geometry(data) (SpectralResponseGeometry.jl:61-66).
+                if (!(std::isfinite(t->denominator_regularization) && t->denominator_regularization > 0)) {
+                    set_error("spectral position regularization must be finite and positive"); return false;
+                }
+                if (!(std::isfinite(t->linear_transport_gamma_inter) && t->linear_transport_gamma_inter >= 0)) {
+                    set_error("gamma_inter_ev must be finite and nonnegative"); return false;
+                }
+            }
             if (t->num_fermi_energies < 1) { set_error("a Fermi-energy axis is required"); return false; }
             if (q.kind == WNLQG_BERRY_DIPOLE && t->temperature == 0.0 && !(t->fermi_surface_broadening > 0)) {
                 set_error("T=0 requires positive eta_fs_ev"); return false;
@@ -897,6 +976,29 @@ bool build_task(const wnlqg_task_desc *t, Task &task) {
             count += q.num_components;
     }
     task.value_count = count;
+    // Isolation contract (BerryMultipoleGeometry.jl:81 with degeneracy_threshold; the eta = 0 gauge
+    // correction, PositionMatrixElements.jl:447-452, with spectral_gap_tolerance; the linear
+    // transport Berry channel's spectral blocks with spectral_gap_tolerance).
+    bool dipole = false, exact = false, blocks = false;
+    for (int r = 0; r < t->num_responses; ++r) {
+        const int kind = t->responses[r].kind;
+        dipole |= kind == WNLQG_BERRY_DIPOLE;
+        exact |= t->denominator_regularization == 0.0 &&
+                 (kind == WNLQG_SHIFT_CURRENT || kind == WNLQG_INJECTION_CURRENT || kind == WNLQG_BERRY_CURVATURE ||
+                  kind == WNLQG_QUANTUM_METRIC || kind == WNLQG_BERRY_DIPOLE);
+        blocks |= kind == WNLQG_LINEAR_TRANSPORT_BERRY;
+    }
+    if (dipole && !(std::isfinite(t->degeneracy_threshold) && t->degeneracy_threshold >= 0)) {
+        set_error("invalid spectral isolation threshold");
+        return false;
+    }
+    if (dipole || exact) {
+        task.iso_mode = 0;
+        task.iso_tol = std::max(dipole ? t->degeneracy_threshold : 0.0, exact ? t->spectral_gap_tolerance : 0.0);
+    } else if (blocks) {
+        task.iso_mode = 1;
+        task.iso_tol = t->spectral_gap_tolerance;
+    }
     return true;
 }
 
@@ -1168,11 +1270,19 @@ void shg_response(int n, const double *E, const cd *V, const cd *A, const cd *dA
 
 // One k-point's concatenated response values (point_value!, IntegralDriver.jl:596-...), with
 // num_kpoints = 1 in every prefactor (the 1/Nk scale is applied by the lane consumer).
-void point_values(const Model &m, const Task &task, const double k[3], cd *out) {
+std::string point_values(const Model &m, const Task &task, const double k[3], cd *out) {
     const wnlqg_task_desc &t = task.desc;
     KData d;
     compute_kpoint(m, task.need, k, t.denominator_regularization, d);
     int n = d.nw;
+    if (task.iso_mode == 0) {
+        std::string err = isolated_spectrum_error(d.E, task.iso_tol);
+        if (!err.empty()) return err;
+    } else if (task.iso_mode == 1) {
+        std::string err;
+        spectral_blocks(d.E, task.iso_tol, err);
+        if (!err.empty()) return err;
+    }
     std::vector<double> f;
     fermi(d.E, t.fermi_energy, t.temperature, f);
     Screen s;
@@ -1260,6 +1370,41 @@ void point_values(const Model &m, const Task &task, const double k[3], cd *out) 
                 o[c] = cd(value, 0.0);
             }
             o += nc;
+        } else if (q.kind == WNLQG_LINEAR_TRANSPORT_BERRY) {
+            // Berry-curvature channel of _linear_transport_response (LinearTransportKernels.jl:100-163,
+            // kernel from linear_transport_kernel, :4-62, conventional_spectral_pair,
+            // SpectralResponseGeometry.jl:79-85): summands 1 (contact) and 4 (interband imaginary
+            // part), each accumulated in the reference's order, then added.
+            const int64_t nmu = t.num_fermi_energies;
+            const double factor = ELEMENTARY_CHARGE_C * ELEMENTARY_CHARGE_C / REDUCED_PLANCK_CONSTANT_J_S * 1e-20;
+            const double gamma = t.linear_transport_gamma_inter;
+            std::string berr;
+            const std::vector<int> starts = spectral_blocks(d.E, t.spectral_gap_tolerance, berr);
+            if (!berr.empty()) return berr;
+            const int nblocks = (int)starts.size() - 1;
+            for (int c = 0; c < nc; ++c) {
+                const int a = q.components[c][0], b = q.components[c][1];
+                for (int64_t im = 0; im < nmu; ++im) {
+                    const double mu = t.fermi_energies[im];
+                    double contact = 0.0, interband = 0.0;
+                    for (int nn = 0; nn < n; ++nn)
+                        contact -= factor * response_occupation(d.E[nn], mu, t.temperature) * d.F[a][b](nn, nn).real();
+                    for (int i = 0; i < nblocks; ++i)
+                        for (int j = i + 1; j < nblocks; ++j) {
+                            const double el = d.E[starts[i]], er = d.E[starts[j]];
+                            const double gap = er - el;
+                            cd qv(0.0, 0.0);
+                            for (int mm = starts[j]; mm < starts[j + 1]; ++mm)
+                                for (int nn = starts[i]; nn < starts[i + 1]; ++nn)
+                                    qv += d.r[a](nn, mm) * d.r[b](mm, nn);
+                            const double occ = response_occupation(el, mu, t.temperature) -
+                                               response_occupation(er, mu, t.temperature);
+                            interband += 2 * factor * occ * gap * gap / (gap * gap + gamma * gamma) * qv.imag();
+                        }
+                    o[im + nmu * c] = cd(contact + interband, 0.0);
+                }
+            }
+            o += nmu * nc;
         } else if (q.kind == WNLQG_INTRINSIC_AHC || q.kind == WNLQG_BERRY_DIPOLE) {
             const int64_t nmu = t.num_fermi_energies;
             for (int c = 0; c < nc; ++c) {
@@ -1283,18 +1428,6 @@ void point_values(const Model &m, const Task &task, const double k[3], cd *out) 
                                 value -= (left - right).imag();
                             }
                         }
-                    } else if (q.kind == WNLQG_INTRINSIC_AHC) {
-                        // Finite temperature: occupation-weighted Berry curvature (the Fermi-sea
-                        // form of berry_curvature_occupied_sum_component, ConventionalQuantumGeometry.jl:188-215).
-                        std::vector<double> fm;
-                        fermi(d.E, mu, t.temperature, fm);
-                        cd v(0.0, 0.0);
-                        for (int nn = 0; nn < n; ++nn) {
-                            v += fm[nn] * d.F[a][b](nn, nn);
-                            for (int mm = 0; mm < n; ++mm)
-                                if (mm != nn) v += (fm[nn] - fm[mm]) * I1 * d.r[a](nn, mm) * d.r[b](mm, nn);
-                        }
-                        value = v.real();
                     } else {
                         // D[mu,a,b,c] = sum_n (-f'(E_n)) Omega_n^{ab} dE_n/dk_c.
                         for (int nn = 0; nn < n; ++nn) {
@@ -1371,6 +1504,7 @@ void point_values(const Model &m, const Task &task, const double k[3], cd *out) 
             o += nom * nc;
         }
     }
+    return "";
 }
 
 bool build_model(const wnlqg_model_desc *desc, Model &m) {
@@ -1438,6 +1572,21 @@ bool build_model(const wnlqg_model_desc *desc, Model &m) {
 
 }  // namespace
 
+// The failing point with the smallest row among parallel workers; reported like the GPU engine's
+// message (the reference's text followed by the k-point row).
+struct FirstError {
+    int64_t row = -1;
+    std::string msg;
+    void record(int64_t r, const std::string &m) {
+#pragma omp critical(oracle_first_error)
+        if (row < 0 || r < row) { row = r; msg = m; }
+    }
+    int report() const {
+        set_error(msg + " (k-point row " + std::to_string(row) + ")");
+        return WNLQG_ERR_INVALID_ARGUMENT;
+    }
+};
+
 extern "C" {
 
 const char *oracle_last_error(void) { return g_error.c_str(); }
@@ -1481,12 +1630,15 @@ int oracle_point_values(const wnlqg_model_desc *md, const wnlqg_task_desc *td, c
     if (!nonorth_kinds_ok(m, td)) return WNLQG_ERR_UNSUPPORTED;
     int64_t vc = task.value_count;
     if (threads <= 0) threads = omp_get_max_threads();
+    FirstError first;
 #pragma omp parallel for schedule(dynamic, 1) num_threads(threads)
     for (int64_t i = 0; i < n; ++i) {
         std::vector<cd> vals((size_t)vc);
-        point_values(m, task, &k[3 * i], vals.data());
+        std::string err = point_values(m, task, &k[3 * i], vals.data());
+        if (!err.empty()) first.record(i, err);
         for (int64_t e = 0; e < vc; ++e) { out[2 * (i * vc + e)] = vals[e].real(); out[2 * (i * vc + e) + 1] = vals[e].imag(); }
     }
+    if (first.row >= 0) return first.report();
     return WNLQG_OK;
 }
 
@@ -1506,6 +1658,7 @@ int oracle_integrate_mesh(const wnlqg_model_desc *md, const wnlqg_task_desc *td,
     std::vector<std::vector<cd>> lane_sum((size_t)lanes, std::vector<cd>((size_t)vc, cd(0.0, 0.0)));
     if (threads <= 0) threads = omp_get_max_threads();
     const double scale = 1.0 / (double)nk;
+    FirstError failed;
 #pragma omp parallel for schedule(dynamic, 1) num_threads(threads)
     for (int64_t L = 0; L < lanes; ++L) {
         int64_t first = (L * nk) / lanes;          // 0-based inclusive
@@ -1518,10 +1671,12 @@ int oracle_integrate_mesh(const wnlqg_model_desc *md, const wnlqg_task_desc *td,
             k[0] = (double)(idx % mesh[0]) / (double)mesh[0];
             k[1] = (double)((idx / mesh[0]) % mesh[1]) / (double)mesh[1];
             k[2] = (double)(idx / (mesh[0] * mesh[1])) / (double)mesh[2];
-            point_values(m, task, k, vals.data());
+            std::string err = point_values(m, task, k, vals.data());
+            if (!err.empty()) { failed.record(idx, err); break; }
             for (int64_t e = 0; e < vc; ++e) lane_sum[L][e] += scale * vals[e];
         }
     }
+    if (failed.row >= 0) return failed.report();
     for (int64_t e = 0; e < vc; ++e) {
         cd acc(0.0, 0.0);
         for (int64_t L = 0; L < lanes; ++L) acc += lane_sum[L][e];
@@ -1639,6 +1794,43 @@ int oracle_kpoint_data(const wnlqg_model_desc *md, const double k[3], double *en
         put(dh, nn * x, d.dH[x], nn);
         put(a, nn * x, d.Aint[x], nn);
         for (int y = 0; y < 3; ++y) { put(da, nn * (x + 3 * y), d.dA[x][y], nn); put(ddh, nn * (x + 3 * y), d.ddH[x][y], nn); }
+    }
+    return WNLQG_OK;
+}
+
+// Hamiltonian-gauge geometry at one k for the parity pins: energies[nw], canonical U[nw,nw],
+// r[nw,nw,3] (Berry connection A + i D) and the generalized derivatives gder[nw,nw,3,3] with
+// element (n, m, a, b) = r^a_{nm;b} (conventional_generalized_position_derivative_element,
+// ConventionalShiftCurrent.jl:191-229) and F[nw,nw,3,3] (Wannier curvature, (a, b) order), all at
+// the given denominator regularization (0 = bare inverses).
+int oracle_kpoint_geometry(const wnlqg_model_desc *md, const double k[3], double eta, double *energies, double *u,
+                           double *r, double *gd, double *f) {
+    Model m;
+    if (!build_model(md, m)) return WNLQG_ERR_INVALID_ARGUMENT;
+    if (m.has_overlap) { set_error("orthogonal models only"); return WNLQG_ERR_UNSUPPORTED; }
+    Needs need;
+    for (int x = 0; x < 3; ++x)
+        for (int y = 0; y < 3; ++y) { need.need_gder(x, y); need.F[x][y] = true; }
+    KData d;
+    compute_kpoint(m, need, k, eta, d);
+    const size_t nn = (size_t)m.nw * m.nw;
+    auto put = [](double *dst, size_t off, const Mat &x, size_t nn_) {
+        for (size_t e = 0; e < nn_; ++e) { dst[2 * (off + e)] = x.v[e].real(); dst[2 * (off + e) + 1] = x.v[e].imag(); }
+    };
+    for (int i = 0; i < m.nw; ++i) energies[i] = d.E[i];
+    put(u, 0, d.U, nn);
+    for (int a = 0; a < 3; ++a) {
+        put(r, nn * a, d.r[a], nn);
+        for (int b = 0; b < 3; ++b) {
+            put(f, nn * (a + 3 * b), d.F[a][b], nn);
+            for (int n = 0; n < m.nw; ++n)
+                for (int mm = 0; mm < m.nw; ++mm) {
+                    const cd g = gder(d, n, mm, a, b);
+                    const size_t e = nn * (a + 3 * b) + n + (size_t)m.nw * mm;
+                    gd[2 * e] = g.real();
+                    gd[2 * e + 1] = g.imag();
+                }
+        }
     }
     return WNLQG_OK;
 }

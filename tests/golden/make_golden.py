@@ -1,6 +1,6 @@
 """Copy the reference's own golden vectors for this path into tests/golden/.
 
-Run in a container that mounts the WannierNLQG reference at /root/reference.  The files are
+Usage: python make_golden.py <path of the WannierNLQG source tree>.  The files are
 data fixtures of the reference's test suite (not source):
   test/fixtures/third_order/jerk_input.dat, jerk_reference.dat   (third_order_unit.jl:210-253)
   examples/fixtures/synthetic_runtime/synthetic_tb.dat            (4-orbital _tb.dat fixture)
@@ -10,7 +10,9 @@ import os
 import shutil
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: make_golden.py <WannierNLQG source tree>")
+REF = sys.argv[1]
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 FILES = {

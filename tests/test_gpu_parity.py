@@ -278,10 +278,15 @@ def test_mesh_weighted_sum_contiguous_and_scattered(engine_cls, oracle_mod):
 @pytest.mark.parametrize("precision", [_abi.PRECISION_FP64, _abi.PRECISION_MIXED])
 @pytest.mark.parametrize("temperature", [0.0, 50.0])
 def test_ahc_and_berry_dipole_match_oracle(engine_cls, oracle_mod, precision, temperature):
+    """Fermi-axis responses: the intrinsic AHC at T = 0 (the only temperature the reference's AHC
+    accepts), the linear transport Berry channel at T > 0 (with an interband rate), and the Berry
+    dipole at a degeneracy threshold below every gap of the sampled spectra."""
     model = synthetic_orthogonal_model(8, 1, 6, full_position=True)
-    task = _abi.TaskArrays([(_abi.INTRINSIC_AHC, ["xy", "zx"]), (_abi.BERRY_DIPOLE, ["xyz", "xzx", "yzy"])],
+    hall = _abi.INTRINSIC_AHC if temperature == 0.0 else _abi.LINEAR_TRANSPORT_BERRY
+    task = _abi.TaskArrays([(hall, ["xy", "zx"]), (_abi.BERRY_DIPOLE, ["xyz", "xzx", "yzy"])],
                            fermi_energies=[-0.5, 0.0, 0.5], temperature=temperature,
-                           fermi_surface_broadening=0.05, precision=precision)
+                           fermi_surface_broadening=0.05, precision=precision, degeneracy_threshold=1e-8,
+                           linear_transport_gamma_inter=0.0 if temperature == 0.0 else 0.01)
     tol = RTOL if precision == _abi.PRECISION_FP64 else MIXED_RTOL
     k = np.random.default_rng(17).random((12, 3))
     with engine_cls(model, task) as eng:
@@ -501,9 +506,11 @@ def test_kslice_map_on_gpu_matches_oracle(engine_cls, oracle_mod):
     assert rel_err(got, ref) < RTOL
 
 
-def test_eval_mesh_many_uneven_models(engine_cls, oracle_mod):
+@pytest.mark.parametrize("precision", [_abi.PRECISION_FP64, _abi.PRECISION_MIXED])
+def test_eval_mesh_many_uneven_models(engine_cls, oracle_mod, precision):
     """Models of different orbital counts (half Kramers-doubled with an O(1e-3 eV) splitting) in
-    one concurrent call: each result equals the model's own evaluation and the oracle."""
+    one concurrent call: each result equals the model's own evaluation and the oracle, on both
+    precision paths (the mixed path's FP64 refinement resolves the near-degenerate pairs)."""
     import torch
     from wanniernlqg_b200.engine import integrate_meshes_many
     from wanniernlqg_b200.model import kramers_doubled_model
@@ -511,8 +518,13 @@ def test_eval_mesh_many_uneven_models(engine_cls, oracle_mod):
     for i, nw in enumerate([6, 8, 12, 16]):
         base = synthetic_orthogonal_model(nw, 1, seed=20 + i, full_position=True)
         models.append(kramers_doubled_model(base, 1e-3, seed=i) if i % 2 else base)
-    task = _abi.TaskArrays([(_abi.INTRINSIC_AHC, ["xy"]), (_abi.BERRY_DIPOLE, ["xzz"])],
-                           fermi_energies=[-0.5, 0.0, 0.5], temperature=50.0)
+    # Finite-temperature Hall response as the reference computes it (the linear transport Berry
+    # channel); the Berry dipole at a threshold that counts the O(1e-3 eV) Kramers splittings as
+    # isolated (the reference's default 2e-3 eV would refuse these models).
+    task = _abi.TaskArrays([(_abi.LINEAR_TRANSPORT_BERRY, ["xy"]), (_abi.BERRY_DIPOLE, ["xzz"])],
+                           fermi_energies=[-0.5, 0.0, 0.5], temperature=50.0, degeneracy_threshold=1e-9,
+                           precision=precision)
+    tol = RTOL if precision == _abi.PRECISION_FP64 else MIXED_RTOL
     engines = [engine_cls(m, task) for m in models]
     try:
         meshes = [(6, 5, 4), (4, 4, 4), (5, 3, 3), (3, 3, 4)]
@@ -525,7 +537,8 @@ def test_eval_mesh_many_uneven_models(engine_cls, oracle_mod):
             single = e.integrate_mesh(ms)
             assert np.array_equal(got, single)
             ref = oracle_mod.integrate_mesh(m, task, ms)
-            assert rel_err(got, ref) < RTOL
+            for g, r in zip(task.split(got), task.split(ref)):
+                assert rel_err(g, r) < tol
     finally:
         for e in engines:
             e.close()

@@ -163,17 +163,6 @@ def test_thread_count_does_not_change_mesh_result(oracle_mod):
     assert np.array_equal(a, b)
 
 
-def test_generalized_derivative_finite_difference(oracle_mod):
-    """With bare denominators the shift-current bracket is gauge covariant: compare the oracle's
-    shift current at b=c against the shift-vector form built from finite differences of r."""
-    model = synthetic_orthogonal_model(4, 1, 3, full_position=True)
-    k0 = np.array([0.13, 0.29, 0.41])
-    task = _abi.TaskArrays([(_abi.SHIFT_CURRENT, ["xyy"])], broadening_type=_abi.LORENTZIAN, broadening=0.05,
-                           photon_energies=[1.0], denominator_regularization=0.0)
-    val = oracle_mod.point_values(model, task, k0)[0, 0]
-    assert np.isfinite(val)
-
-
 def test_ahc_zero_temperature_matches_occupied_curvature(oracle_mod):
     """T=0 intrinsic AHC (bare occupied/empty links) equals the occupied-sum Berry curvature up to
     the eta^2/gap^2 difference between bare and regularised links."""

@@ -26,6 +26,7 @@ INTRINSIC_AHC = 5
 BERRY_DIPOLE = 6
 SECOND_HARMONIC = 7
 JERK_CURRENT = 8
+LINEAR_TRANSPORT_BERRY = 9
 
 GAUSSIAN = 0
 LORENTZIAN = 1
@@ -38,7 +39,7 @@ MAX_COMPONENTS = 81
 
 # Kinds whose values carry the photon-energy axis.
 FREQUENCY_KINDS = (SHIFT_CURRENT, INJECTION_CURRENT, JERK_CURRENT)
-FERMI_AXIS_KINDS = (INTRINSIC_AHC, BERRY_DIPOLE)
+FERMI_AXIS_KINDS = (INTRINSIC_AHC, BERRY_DIPOLE, LINEAR_TRANSPORT_BERRY)
 
 
 class ModelDesc(ctypes.Structure):
@@ -110,6 +111,8 @@ class TaskDesc(ctypes.Structure):
         ("valence_bands", ctypes.c_uint32 * 4),
         ("conduction_bands", ctypes.c_uint32 * 4),
         ("wannier_center_convention", ctypes.c_int32),
+        ("spectral_gap_tolerance", ctypes.c_double),
+        ("linear_transport_gamma_inter", ctypes.c_double),
     ]
 
 
@@ -163,7 +166,8 @@ class TaskArrays:
                  photon_energies=(0.10,), fermi_energies=(), precision=PRECISION_FP64,
                  fermi_surface_broadening=0.0, shg_low_frequency_broadening=0.025,
                  shg_intermediate_regularization=0.0, shg_eta_correction=True, band_window_size=-1,
-                 band_selection=None, wannier_center_convention="II"):
+                 band_selection=None, wannier_center_convention="II", spectral_gap_tolerance=1e-10,
+                 linear_transport_gamma_inter=0.0):
         if not 1 <= len(responses) <= MAX_RESPONSES:
             raise ValueError("between 1 and 8 responses are supported per task")
         self.photon_energies = np.ascontiguousarray(np.asarray(photon_energies, dtype=np.float64))
@@ -205,6 +209,8 @@ class TaskArrays:
         if wannier_center_convention not in ("I", "II"):
             raise ValueError("wannier_center_convention must be 'I' or 'II'")
         d.wannier_center_convention = 1 if wannier_center_convention == "I" else 0
+        d.spectral_gap_tolerance = float(spectral_gap_tolerance)
+        d.linear_transport_gamma_inter = float(linear_transport_gamma_inter)
         # band_selection = (conduction bands, valence bands), 1-based as in the reference's
         # cfg.band_selection; pairs (n, m) with n valence and m conduction are kept.
         if band_selection is not None:

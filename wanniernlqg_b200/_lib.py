@@ -25,7 +25,7 @@ EXPORTED_SYMBOLS = (
     "wnlqg_b200_mlp_set_params", "wnlqg_b200_mlp_forward", "wnlqg_b200_mlp_loss_grad", "wnlqg_b200_mlp_train",
     "wnlqg_b200_graph_capture_mesh_many", "wnlqg_b200_graph_capture_points_weighted", "wnlqg_b200_graph_launch",
     "wnlqg_b200_graph_status", "wnlqg_b200_graph_kernel_count", "wnlqg_b200_graph_destroy",
-    "wnlqg_b200_plan_autotune",
+    "wnlqg_b200_plan_autotune", "wnlqg_b200_plan_status",
 )
 
 _lib = None
@@ -89,6 +89,8 @@ def load():
         getattr(L, name).restype = ctypes.c_int
     L.wnlqg_b200_plan_last_launch_count.restype = ctypes.c_int64
     L.wnlqg_b200_plan_last_launch_count.argtypes = [vp]
+    L.wnlqg_b200_plan_status.argtypes = [vp]
+    L.wnlqg_b200_plan_status.restype = ctypes.c_int
     L.wnlqg_b200_graph_capture_mesh_many.argtypes = [ctypes.POINTER(vp), ctypes.c_int32, ip, ip, ip,
                                                      ctypes.POINTER(vp), ctypes.POINTER(vp)]
     L.wnlqg_b200_graph_capture_points_weighted.argtypes = [vp, vp, vp, ctypes.c_int64, vp, ctypes.POINTER(vp)]

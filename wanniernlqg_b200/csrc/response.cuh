@@ -26,7 +26,7 @@
 
 enum { RS_FC_SHIFT = 1, RS_FC_INJECTION = 2, RS_FC_JERK = 3 };
 enum { RS_SC_BERRY = 1, RS_SC_METRIC = 2 };
-enum { RS_MU_AHC = 1, RS_MU_DIPOLE = 2 };
+enum { RS_MU_AHC = 1, RS_MU_DIPOLE = 2, RS_MU_LT = 3 };
 #define RS_MAX_HESS 9
 #define RS_MU_CHUNK 8
 
@@ -63,6 +63,7 @@ struct RespParams {
     int nmu;
     const double *mus;
     double temperature, fs_width;
+    double lt_gamma, lt_factor;   // linear transport Berry channel: interband rate (eV), e^2/hbar 1e-20
     // Scalar components (Berry curvature, quantum metric).
     int n_sc;
     int sc_kind[RS_MAX_SCALAR], sc_a[RS_MAX_SCALAR], sc_b[RS_MAX_SCALAR];
@@ -158,6 +159,15 @@ WNLQG_D double reg_inverse(double d, double eta) {
     double sc = fmax(fabs(d), eta);
     double sd = d / sc, sw = eta / sc;
     return (sd / (sd * sd + sw * sw)) / sc;
+}
+
+// response_occupation (Responses/Shared/ResponseOccupations.jl:8-14): strict step with one half
+// at equality at T = 0, the stable logistic form above.
+WNLQG_D double response_occ(double e, double mu, double T) {
+    if (T == 0.0) return e < mu ? 1.0 : (e > mu ? 0.0 : 0.5);
+    const double x = (e - mu) / (8.617333262145e-5 * T);
+    const double z = exp(-fabs(x));
+    return x >= 0.0 ? z / (1.0 + z) : 1.0 / (1.0 + z);
 }
 
 WNLQG_D double fermi_occ(double e, double mu, double kT) {
@@ -646,10 +656,36 @@ __global__ void __launch_bounds__(WIDE ? 512 : 256, WIDE ? 1 : (sizeof(R) == 8 ?
                             for (int n = 0; n < nw; ++n) nocc[j] += sE[n] <= mu ? 1 : 0;
                         }
                     }
+                    double exact = 0.0;   // spectral blocks: levels within 32 eps max(1, max|E|)
+                    if (p.mu_kind[s] == RS_MU_LT) {
+                        for (int n = 0; n < nw; ++n) exact = fmax(exact, fabs(sE[n]));
+                        exact = 32.0 * 2.220446049250313e-16 * fmax(1.0, exact);
+                    }
                     for (int e = threadIdx.x; e < nn; e += blockDim.x) {
                         const int l = e % nw, m = e / nw;
-                        if (p.temperature == 0.0) {
-                            // Matrix curvature with bare occupied/empty links
+                        if (p.mu_kind[s] == RS_MU_LT) {
+                            // Berry channel of _linear_transport_response (LinearTransportKernels.jl:
+                            // 100-163): contact -f(E_l) Re F_ll and, over ordered pairs of distinct
+                            // spectral blocks, (f_l - f_m) gap^2/(gap^2 + gamma^2) Im(r^a_lm r^b_ml)
+                            // (both orders give the reference's 2 Im q of each unordered pair); the
+                            // common factor -e^2/hbar 1e-20 is applied to the sum.
+                            const double gap = sE[m] - sE[l];
+                            const bool joined = l != m && fabs(gap) <= exact;
+                            const double rate = gap * gap / (gap * gap + p.lt_gamma * p.lt_gamma);
+                            const double2 t = (l == m || joined)
+                                                  ? make_double2(0.0, 0.0)
+                                                  : cmuli(to_c64(cmul(r_elem(a, l, m), r_elem(bb, m, l))));
+#pragma unroll
+                            for (int j = 0; j < RS_MU_CHUNK; ++j) {
+                                if (m0 + j >= p.nmu) continue;
+                                const double mu = p.mus[m0 + j];
+                                const double fl = response_occ(sE[l], mu, p.temperature);
+                                if (l == m) loc[j] += fl * sFd[2 * nw + l].x;
+                                else if (!joined) loc[j] += (fl - response_occ(sE[m], mu, p.temperature)) * rate * t.x;
+                            }
+                        } else {
+                            // Zero temperature (the only AHC temperature, checked at plan creation):
+                            // matrix curvature with bare occupied/empty links
                             // (IntrinsicHallCurvature.jl:2-29, IntrinsicHallGeometry.jl:117-136).
                             double pair = 0.0;
                             if (l != m) {
@@ -670,22 +706,11 @@ __global__ void __launch_bounds__(WIDE ? 512 : 256, WIDE ? 1 : (sizeof(R) == 8 ?
                                 if (l == m) { if (l < nocc[j]) loc[j] += sFd[2 * nw + l].x; }
                                 else if (l < nocc[j] && m >= nocc[j]) loc[j] += pair;
                             }
-                        } else {
-                            // Finite temperature: occupation-weighted Berry curvature.
-                            const double2 t = l == m ? make_double2(0.0, 0.0)
-                                                     : cmuli(to_c64(cmul(r_elem(a, l, m), r_elem(bb, m, l))));
-#pragma unroll
-                            for (int j = 0; j < RS_MU_CHUNK; ++j) {
-                                if (m0 + j >= p.nmu) continue;
-                                const double mu = p.mus[m0 + j];
-                                const double fl = fermi_occ(sE[l], mu, p.kT);
-                                if (l == m) loc[j] += fl * sFd[2 * nw + l].x;
-                                else loc[j] += (fl - fermi_occ(sE[m], mu, p.kT)) * t.x;
-                            }
                         }
                     }
+                    const double mu_scale = p.mu_kind[s] == RS_MU_LT ? -p.lt_factor : 1.0;
                     for (int j = 0; j < RS_MU_CHUNK && m0 + j < p.nmu; ++j) {
-                        const double total = block_sum(loc[j], red);
+                        const double total = mu_scale * block_sum(loc[j], red);
                         if (threadIdx.x == 0) {
                             const int64_t idx = p.mu_out[s] + m0 + j;
                             if (p.mode == 0) {

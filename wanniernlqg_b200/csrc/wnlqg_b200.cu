@@ -27,6 +27,7 @@
 #include "tc_fourier.cuh"
 #include "nonorth.cuh"
 #include "order.cuh"
+#include "isolation.cuh"
 #include <cub/device/device_radix_sort.cuh>
 
 namespace {
@@ -83,6 +84,12 @@ struct wnlqg_plan {
     int ch_H = 0, ch_S = -1;
     bool nonorth = false;
     int *d_status = nullptr;
+    // Spectral isolation contract (isolation.cuh): -1 = none, else ISO_ALL_PAIRS or
+    // ISO_SPECTRAL_BLOCKS with tolerance iso_tol; the first failing row and its record.
+    int iso_mode = -1;
+    double iso_tol = 0.0;
+    unsigned long long *d_iso_key = nullptr;
+    IsoRecord *d_iso_rec = nullptr;
     int ch_dH[3], ch_A[3], ch_ddH[9], ch_dA[9];
     int nw = 0, nr = 0, C = 0;
     int64_t nn = 0, vc = 0, max_batch = 0;
@@ -135,6 +142,7 @@ struct wnlqg_plan {
     int eigh_grid_l2 = 0;                     // the grid whose working sets stay L2-resident
     unsigned char *d_resp_scratch = nullptr;  // per-CTA global working set of the response passes
     int resp_gw_grid = 0;                     // grid of the global working-set passes; 0 = each pass's own
+    int resp_gw_grid_alloc = 0;               // CTAs the response working sets are allocated for
     int64_t resp_scratch_stride = 0;
     // Nonorthogonal responses: metric geometry per batch (Berry connection, slopes, G pairs).
     NonorthParams ng;
@@ -279,7 +287,8 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
             const int32_t *x = q.components[c];
             if (q.kind == WNLQG_SHIFT_CURRENT || q.kind == WNLQG_INJECTION_CURRENT || q.kind == WNLQG_JERK_CURRENT) {
                 items.push_back({q.kind, x[0], x[1], x[2], x[3], off + (int64_t)c * t.num_photon_energies});
-            } else if (q.kind == WNLQG_INTRINSIC_AHC || q.kind == WNLQG_BERRY_DIPOLE) {
+            } else if (q.kind == WNLQG_INTRINSIC_AHC || q.kind == WNLQG_BERRY_DIPOLE ||
+                       q.kind == WNLQG_LINEAR_TRANSPORT_BERRY) {
                 items.push_back({q.kind, x[0], x[1], x[2], 0, off + (int64_t)c * t.num_fermi_energies});
             } else {
                 items.push_back({q.kind, x[0], x[1], 0, 0, off + c});
@@ -287,7 +296,7 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
         }
         if (q.kind == WNLQG_SHIFT_CURRENT || q.kind == WNLQG_INJECTION_CURRENT || q.kind == WNLQG_JERK_CURRENT)
             off += (int64_t)q.num_components * t.num_photon_energies;
-        else if (q.kind == WNLQG_INTRINSIC_AHC || q.kind == WNLQG_BERRY_DIPOLE)
+        else if (q.kind == WNLQG_INTRINSIC_AHC || q.kind == WNLQG_BERRY_DIPOLE || q.kind == WNLQG_LINEAR_TRANSPORT_BERRY)
             off += (int64_t)q.num_components * t.num_fermi_energies;
         else
             off += q.num_components;
@@ -365,7 +374,8 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
             auto need_r = [&](int a) { tH[a] = true; tA[a] = true; };
             const bool freq = it.kind == WNLQG_SHIFT_CURRENT || it.kind == WNLQG_INJECTION_CURRENT ||
                               it.kind == WNLQG_JERK_CURRENT;
-            const bool muaxis = it.kind == WNLQG_INTRINSIC_AHC || it.kind == WNLQG_BERRY_DIPOLE;
+            const bool muaxis = it.kind == WNLQG_INTRINSIC_AHC || it.kind == WNLQG_BERRY_DIPOLE ||
+                                it.kind == WNLQG_LINEAR_TRANSPORT_BERRY;
             const int mode = it.kind == WNLQG_JERK_CURRENT ? 1 : 0;
             if (freq && p.n_fc > 0 && p.pair_mode != mode) break;   // one pair family per pass
             if (it.kind == WNLQG_SHIFT_CURRENT) {
@@ -424,7 +434,8 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
                 p.pair_mode = 1;
             } else if (muaxis) {
                 int m = p.n_mu++;
-                p.mu_kind[m] = it.kind == WNLQG_INTRINSIC_AHC ? RS_MU_AHC : RS_MU_DIPOLE;
+                p.mu_kind[m] = it.kind == WNLQG_INTRINSIC_AHC ? RS_MU_AHC
+                               : it.kind == WNLQG_BERRY_DIPOLE ? RS_MU_DIPOLE : RS_MU_LT;
                 p.mu_a[m] = it.a; p.mu_b[m] = it.b; p.mu_c[m] = it.c; p.mu_out[m] = it.out;
             } else {
                 int s = p.n_sc++;
@@ -446,6 +457,9 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
         p.mus = pl->d_mus;
         p.temperature = t.temperature;
         p.fs_width = t.fermi_surface_broadening;
+        p.lt_gamma = t.linear_transport_gamma_inter;
+        // factor = e^2 / hbar * 1e-20 of _linear_transport_response (LinearTransportKernels.jl:116).
+        p.lt_factor = WNLQG_ELEMENTARY_CHARGE_C * WNLQG_ELEMENTARY_CHARGE_C / WNLQG_HBAR_J_S * 1e-20;
         p.nom = (int)t.num_photon_energies;
         p.omegas = pl->d_omegas;
         p.mu = t.fermi_energy;
@@ -498,6 +512,7 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
             bytes = std::max(bytes, ps.smem);
         }
         pl->resp_scratch_stride = (int64_t)((bytes + 255) & ~(size_t)255);
+        pl->resp_gw_grid_alloc = (int)grid;
         cudaError_t e = cudaMalloc(&pl->d_resp_scratch, (size_t)grid * pl->resp_scratch_stride);
         if (e != cudaSuccess) {
             cudaGetLastError();
@@ -652,6 +667,46 @@ wnlqg_status tc_check(wnlqg_plan *pl) {
         return fail(WNLQG_ERR_DEVICE_TIMEOUT, "tensor-core Fourier: a bounded device wait gave up");
     }
     return WNLQG_OK;
+}
+
+// The isolation contract on one batch's energies (after the eigensolve): rows are row_base + the
+// batch entry, or row_base + perm[entry] for Morton-ordered batches.
+wnlqg_status run_isolation(wnlqg_plan *pl, int64_t nb, int64_t row_base, const int *perm) {
+    if (pl->iso_mode < 0 || nb <= 0) return WNLQG_OK;
+    isolation_check_kernel<<<(unsigned)((nb + 127) / 128), 128, 0, pl->stream>>>(pl->d_E, nb, pl->nw, pl->iso_tol,
+                                                                               pl->iso_mode, row_base, perm,
+                                                                               pl->d_iso_key);
+    isolation_record_kernel<<<1, 1, 0, pl->stream>>>(pl->d_E, nb, pl->nw, pl->iso_tol, pl->iso_mode, row_base,
+                                                      pl->d_iso_key, pl->d_iso_rec);
+    pl->launches += 2;
+    WNLQG_CUDA(cudaGetLastError());
+    return WNLQG_OK;
+}
+
+// Reports (and clears) an isolation failure after a synchronised call, with the reference's
+// message (geometry_isolated_spectrum_minimum_gap, OrthogonalBandDerivatives.jl:66-82;
+// spectral_subspace_blocks, SubspacePositionMatrixElements.jl:5-22; bands 1-based).
+wnlqg_status iso_check(wnlqg_plan *pl) {
+    if (pl->iso_mode < 0 || !pl->d_iso_key) return WNLQG_OK;
+    unsigned long long key = ISO_NONE;
+    WNLQG_CUDA(cudaMemcpy(&key, pl->d_iso_key, sizeof(key), cudaMemcpyDeviceToHost));
+    if (key == ISO_NONE) return WNLQG_OK;
+    IsoRecord rec;
+    WNLQG_CUDA(cudaMemcpy(&rec, pl->d_iso_rec, sizeof(rec), cudaMemcpyDeviceToHost));
+    WNLQG_CUDA(cudaMemset(pl->d_iso_key, 0xFF, sizeof(unsigned long long)));
+    char buf[256];
+    const long long row = (long long)(key >> ISO_LOCAL_BITS);
+    if (!std::isfinite(rec.gap))
+        std::snprintf(buf, sizeof(buf), "empty/nonfinite geometry spectrum (k-point row %lld)", row);
+    else if (pl->iso_mode == ISO_ALL_PAIRS)
+        std::snprintf(buf, sizeof(buf),
+                      "GEOMETRY_SINGLE_BAND_SPECTRUM_NOT_ISOLATED: bands=(%d,%d), gap_ev=%.17g, threshold_ev=%.17g "
+                      "(k-point row %lld)",
+                      rec.l + 1, rec.m + 1, rec.gap, pl->iso_tol, row);
+    else
+        std::snprintf(buf, sizeof(buf), "SPECTRAL_CROSS_BLOCK_GAP_UNRESOLVED: gap=%.17g eV (k-point row %lld)", rec.gap,
+                      row);
+    return fail(WNLQG_ERR_INVALID_ARGUMENT, buf);
 }
 
 typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
@@ -1107,7 +1162,8 @@ wnlqg_status wnlqg_b200_plan_destroy(wnlqg_plan *pl) {
                       (void *)pl->d_resp_scratch, (void *)pl->d_ng_r, (void *)pl->d_ng_v, (void *)pl->d_ng_G,
                       (void *)pl->d_ng_ws, (void *)pl->d_mshg_src, (void *)pl->d_mshg_diag, (void *)pl->d_mshg_ws,
                       (void *)pl->d_okeys, (void *)pl->d_operm, (void *)pl->d_ok, (void *)pl->d_ow, pl->d_osort_tmp,
-                      (void *)pl->d_gC, (void *)pl->d_gL, (void *)pl->d_gred_scratch})
+                      (void *)pl->d_gC, (void *)pl->d_gL, (void *)pl->d_gred_scratch, (void *)pl->d_iso_key,
+                      (void *)pl->d_iso_rec})
         if (ptr) cudaFree(ptr);
     for (cudaEvent_t ev : pl->events) cudaEventDestroy(ev);
     if (pl->stream) cudaStreamDestroy(pl->stream);
@@ -1142,6 +1198,8 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
         return fail(WNLQG_ERR_INVALID_ARGUMENT, "wannier_center_convention must be 0 (II) or 1 (I)");
     if (t.wannier_center_convention == 1 && model->has_overlap)
         return fail(WNLQG_ERR_UNSUPPORTED, "Convention I with an overlap is not built");
+    if (!(std::isfinite(t.spectral_gap_tolerance) && t.spectral_gap_tolerance >= 0))
+        return fail(WNLQG_ERR_INVALID_ARGUMENT, "invalid spectral isolation threshold");
     if (t.use_band_selection) {
         // validate_interband_band_selection (CalculationUtils.jl:501-522): two nonempty, disjoint
         // groups inside the orbitals.
@@ -1228,6 +1286,7 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
                 break;
             case WNLQG_INTRINSIC_AHC:
             case WNLQG_BERRY_DIPOLE:
+            case WNLQG_LINEAR_TRANSPORT_BERRY:
                 need_r(a); need_r(b);
                 pl->ch_dA[b * 3 + a] = add_channel(ch, CH_DA, b, a);
                 pl->ch_dA[a * 3 + b] = add_channel(ch, CH_DA, a, b);
@@ -1276,7 +1335,21 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
             if (!(std::isfinite(t.degeneracy_threshold) && t.degeneracy_threshold >= 0))
                 return bail(fail(WNLQG_ERR_INVALID_ARGUMENT, "SHG degeneracy_threshold must be finite and nonnegative in eV"));
             vc += (int64_t)q.num_components * t.num_photon_energies * 14;
-        } else if (q.kind == WNLQG_INTRINSIC_AHC || q.kind == WNLQG_BERRY_DIPOLE) {
+        } else if (q.kind == WNLQG_INTRINSIC_AHC || q.kind == WNLQG_BERRY_DIPOLE ||
+                   q.kind == WNLQG_LINEAR_TRANSPORT_BERRY) {
+            // intrinsic_hall_fermi_sea is zero-temperature only (IntrinsicHallOccupations.jl:15-16);
+            // the finite-temperature Berry channel is the linear transport kind.
+            if (q.kind == WNLQG_INTRINSIC_AHC && t.temperature != 0.0)
+                return bail(fail(WNLQG_ERR_INVALID_ARGUMENT, "INTRINSIC_HALL_REQUIRES_ZERO_TEMPERATURE"));
+            if (q.kind == WNLQG_LINEAR_TRANSPORT_BERRY) {
+                // spectral_response_geometry(data) (SpectralResponseGeometry.jl:61-66) and the
+                // interband rate of _linear_transport_response (LinearTransportKernels.jl:100-163).
+                if (!(std::isfinite(t.denominator_regularization) && t.denominator_regularization > 0))
+                    return bail(fail(WNLQG_ERR_INVALID_ARGUMENT,
+                                     "spectral position regularization must be finite and positive"));
+                if (!(std::isfinite(t.linear_transport_gamma_inter) && t.linear_transport_gamma_inter >= 0))
+                    return bail(fail(WNLQG_ERR_INVALID_ARGUMENT, "gamma_inter_ev must be finite and nonnegative"));
+            }
             if (t.num_fermi_energies < 1 || !t.fermi_energies)
                 return bail(fail(WNLQG_ERR_INVALID_ARGUMENT, "finite nonempty Fermi energy axis required"));
             if (!finite_array(t.fermi_energies, (size_t)t.num_fermi_energies))
@@ -1474,6 +1547,37 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
     if ((st = alloc((void **)&pl->d_weights, (size_t)max_batch * sizeof(double))) != WNLQG_OK) return bail(st);
     if ((st = alloc((void **)&pl->d_kidx, (size_t)max_batch * sizeof(int64_t))) != WNLQG_OK) return bail(st);
     if ((st = alloc((void **)&pl->d_status, (size_t)max_batch * sizeof(int))) != WNLQG_OK) return bail(st);
+    {
+        // Isolation contract: the Berry dipole needs every pair split by more than
+        // degeneracy_threshold (BerryMultipoleGeometry.jl:81); eta = 0 geometry by more than
+        // spectral_gap_tolerance (PositionMatrixElements.jl:447-452); the linear transport Berry
+        // channel resolves its spectral blocks with spectral_gap_tolerance.
+        bool dipole = false, exact = false, blocks = false;
+        for (int r = 0; r < t.num_responses; ++r) {
+            const int kind = t.responses[r].kind;
+            dipole |= kind == WNLQG_BERRY_DIPOLE;
+            exact |= t.denominator_regularization == 0.0 &&
+                     (kind == WNLQG_SHIFT_CURRENT || kind == WNLQG_INJECTION_CURRENT || kind == WNLQG_BERRY_CURVATURE ||
+                      kind == WNLQG_QUANTUM_METRIC || kind == WNLQG_BERRY_DIPOLE);
+            blocks |= kind == WNLQG_LINEAR_TRANSPORT_BERRY;
+        }
+        if (dipole && !(std::isfinite(t.degeneracy_threshold) && t.degeneracy_threshold >= 0))
+            return bail(fail(WNLQG_ERR_INVALID_ARGUMENT, "invalid spectral isolation threshold"));
+        if (dipole || exact) {
+            pl->iso_mode = ISO_ALL_PAIRS;
+            pl->iso_tol = std::max(dipole ? t.degeneracy_threshold : 0.0, exact ? t.spectral_gap_tolerance : 0.0);
+        } else if (blocks) {
+            pl->iso_mode = ISO_SPECTRAL_BLOCKS;
+            pl->iso_tol = t.spectral_gap_tolerance;
+        }
+        if (pl->iso_mode >= 0) {
+            if (max_batch > ((int64_t)1 << ISO_LOCAL_BITS))
+                return bail(fail(WNLQG_ERR_UNSUPPORTED, "max_batch above 2^24 with a spectral isolation check"));
+            if ((st = alloc((void **)&pl->d_iso_key, sizeof(unsigned long long))) != WNLQG_OK) return bail(st);
+            if ((st = alloc((void **)&pl->d_iso_rec, sizeof(IsoRecord))) != WNLQG_OK) return bail(st);
+            WNLQG_CUDA(cudaMemset(pl->d_iso_key, 0xFF, sizeof(unsigned long long)));
+        }
+    }
     if (pl->nonorth && vc > 0) {
         NonorthParams &q = pl->ng;
         q.nw = nw;
@@ -1815,6 +1919,7 @@ wnlqg_status enqueue_mesh(wnlqg_plan *pl, const int64_t mesh[3], int64_t k_begin
         size_t base = 1 + 3 * nbatch;
         if ((st = record_event(pl, base)) != WNLQG_OK) return st;
         if ((st = run_front(pl, nb, s, mesh, nullptr, base)) != WNLQG_OK) return st;
+        if ((st = run_isolation(pl, nb, s, nullptr)) != WNLQG_OK) return st;
         if ((st = run_passes(pl, nb, 0, scale, 0)) != WNLQG_OK) return st;
     }
     // Events: [0] start, per batch b: [1+3b] batch start, [2+3b] after Fourier, [3+3b] after eigh,
@@ -1895,6 +2000,7 @@ wnlqg_status enqueue_points_weighted(wnlqg_plan *pl, const double *kpoints_devic
             wb = pl->d_ow;
         }
         if ((st = run_front(pl, nb, 0, nullptr, kb, base, nullptr, ord)) != WNLQG_OK) return st;
+        if ((st = run_isolation(pl, nb, s, ord ? pl->d_operm + pl->max_batch : nullptr)) != WNLQG_OK) return st;
         if ((st = run_passes(pl, nb, 0, 1.0, 0, wb)) != WNLQG_OK) return st;
     }
     const size_t final_ev = 1 + 3 * nbatch;
@@ -1989,6 +2095,7 @@ wnlqg_status wnlqg_b200_eval_mesh(wnlqg_plan *pl, const int64_t mesh[3], int64_t
     WNLQG_CUDA(cudaMemcpyAsync(out, pl->d_out, (size_t)pl->vc * sizeof(double2), cudaMemcpyDeviceToHost, pl->stream));
     WNLQG_CUDA(cudaStreamSynchronize(pl->stream));
     if ((st = tc_check(pl)) != WNLQG_OK) return st;
+    if ((st = iso_check(pl)) != WNLQG_OK) return st;
     for (int64_t v = 0; v < 2 * pl->vc; ++v)
         if (!std::isfinite(out[v])) return fail(WNLQG_ERR_NONFINITE, "response contains non-finite values");
     return WNLQG_OK;
@@ -2008,6 +2115,7 @@ wnlqg_status wnlqg_b200_eval_points(wnlqg_plan *pl, const double *kpoints, int64
         const bool ord = pl->order_points && nb > 1;
         if (ord && (st = order_batch(pl, pl->d_kpts, nullptr, nb)) != WNLQG_OK) return st;
         if ((st = run_front(pl, nb, 0, nullptr, ord ? pl->d_ok : pl->d_kpts, 1, nullptr, ord)) != WNLQG_OK) return st;
+        if ((st = run_isolation(pl, nb, s, ord ? pl->d_operm + pl->max_batch : nullptr)) != WNLQG_OK) return st;
         if ((st = run_passes(pl, nb, 1, 1.0, 0, nullptr, ord ? pl->d_operm + pl->max_batch : nullptr)) != WNLQG_OK)
             return st;
         WNLQG_CUDA(cudaMemcpyAsync(out + 2 * s * pl->vc, pl->d_points, (size_t)nb * pl->vc * sizeof(double2),
@@ -2016,6 +2124,7 @@ wnlqg_status wnlqg_b200_eval_points(wnlqg_plan *pl, const double *kpoints, int64
     WNLQG_CUDA(cudaStreamSynchronize(pl->stream));
     pl->timing_valid = false;
     if ((st = tc_check(pl)) != WNLQG_OK) return st;
+    if ((st = iso_check(pl)) != WNLQG_OK) return st;
     for (int64_t v = 0; v < 2 * n * pl->vc; ++v)
         if (!std::isfinite(out[v])) return fail(WNLQG_ERR_NONFINITE, "response contains non-finite values");
     return WNLQG_OK;
@@ -2040,6 +2149,7 @@ wnlqg_status wnlqg_b200_eval_points_weighted(wnlqg_plan *pl, const double *kpoin
         const bool ord = pl->order_points && nb > 1;
         if (ord && (st = order_batch(pl, pl->d_kpts, pl->d_weights, nb)) != WNLQG_OK) return st;
         if ((st = run_front(pl, nb, 0, nullptr, ord ? pl->d_ok : pl->d_kpts, 1, nullptr, ord)) != WNLQG_OK) return st;
+        if ((st = run_isolation(pl, nb, s, ord ? pl->d_operm + pl->max_batch : nullptr)) != WNLQG_OK) return st;
         if ((st = run_passes(pl, nb, 0, 1.0, 0, ord ? pl->d_ow : pl->d_weights)) != WNLQG_OK) return st;
     }
     reduce_partials_kernel<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((pl->vc + 255) / 256, 1024)), 256, 0,
@@ -2050,6 +2160,7 @@ wnlqg_status wnlqg_b200_eval_points_weighted(wnlqg_plan *pl, const double *kpoin
     WNLQG_CUDA(cudaStreamSynchronize(pl->stream));
     pl->timing_valid = false;
     if ((st = tc_check(pl)) != WNLQG_OK) return st;
+    if ((st = iso_check(pl)) != WNLQG_OK) return st;
     for (int64_t v = 0; v < 2 * pl->vc; ++v)
         if (!std::isfinite(out[v])) return fail(WNLQG_ERR_NONFINITE, "response contains non-finite values");
     return WNLQG_OK;
@@ -2082,6 +2193,7 @@ wnlqg_status wnlqg_b200_eval_mesh_weighted(wnlqg_plan *pl, const int64_t mesh[3]
                                        pl->stream));
             if ((st = run_front(pl, nb, 0, mesh, nullptr, 1, pl->d_kidx)) != WNLQG_OK) return st;
         }
+        if ((st = run_isolation(pl, nb, s, nullptr)) != WNLQG_OK) return st;
         if ((st = run_passes(pl, nb, 0, 1.0, 0, pl->d_weights)) != WNLQG_OK) return st;
     }
     reduce_partials_kernel<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((pl->vc + 255) / 256, 1024)), 256, 0,
@@ -2092,6 +2204,7 @@ wnlqg_status wnlqg_b200_eval_mesh_weighted(wnlqg_plan *pl, const int64_t mesh[3]
     WNLQG_CUDA(cudaStreamSynchronize(pl->stream));
     pl->timing_valid = false;
     if ((st = tc_check(pl)) != WNLQG_OK) return st;
+    if ((st = iso_check(pl)) != WNLQG_OK) return st;
     for (int64_t v = 0; v < 2 * pl->vc; ++v)
         if (!std::isfinite(out[v])) return fail(WNLQG_ERR_NONFINITE, "response contains non-finite values");
     return WNLQG_OK;
@@ -2187,6 +2300,15 @@ wnlqg_status wnlqg_b200_plan_last_timing(const wnlqg_plan *pl_const, double *fou
 }
 
 int64_t wnlqg_b200_plan_last_launch_count(const wnlqg_plan *plan) { return plan ? plan->launches : -1; }
+
+wnlqg_status wnlqg_b200_plan_status(wnlqg_plan *pl) {
+    wnlqg_status st = check_plan(pl);
+    if (st != WNLQG_OK) return st;
+    WNLQG_CUDA(cudaSetDevice(pl->model->device));
+    pl->tc_used = true;   // read the flag even if the last direct call did not use the tensor cores
+    if ((st = tc_check(pl)) != WNLQG_OK) return st;
+    return iso_check(pl);
+}
 
 }  // extern "C"
 
@@ -2328,6 +2450,10 @@ wnlqg_status wnlqg_b200_graph_status(wnlqg_graph *graph) {
             return fail(WNLQG_ERR_DEVICE_TIMEOUT, "tensor-core Fourier: a bounded device wait gave up");
         }
     }
+    for (wnlqg_plan *pl : graph->plans) {
+        wnlqg_status st = iso_check(pl);
+        if (st != WNLQG_OK) return st;
+    }
     return WNLQG_OK;
 }
 
@@ -2403,10 +2529,17 @@ extern "C" wnlqg_status wnlqg_b200_plan_autotune(wnlqg_plan *pl, const int64_t m
             if (pl->warp_eigh && it->second.team) apply_team(pl, it->second.team);
             if (it->second.warm >= 0) pl->warm_mode = it->second.warm;
             if (it->second.wide >= 0) pl->resp_wide = it->second.wide == 1;
-            if (it->second.mshg_grid > 0) pl->mshg_grid = it->second.mshg_grid;
-            if (it->second.shg_grid > 0) pl->shg_grid = it->second.shg_grid;
-            if (it->second.resp_grid >= 0) pl->resp_gw_grid = it->second.resp_grid;
-            if (it->second.eigh_grid > 0) pl->eigh_grid = it->second.eigh_grid;
+            // Grids are clamped to what this plan's working sets and partial slots were sized for:
+            // the cache key leaves out the solver choices (environment switches at plan creation)
+            // that decide those sizes.
+            if (it->second.mshg_grid > 0 && pl->d_mshg_ws)
+                pl->mshg_grid = std::min(it->second.mshg_grid, pl->mshg_grid_alloc);
+            if (it->second.shg_grid > 0 && pl->shg_grid_alloc > 0)
+                pl->shg_grid = std::min(it->second.shg_grid, pl->shg_grid_alloc);
+            if (it->second.resp_grid >= 0 && pl->d_resp_scratch)
+                pl->resp_gw_grid = std::min(it->second.resp_grid, pl->resp_gw_grid_alloc);
+            if (it->second.eigh_grid > 0 && pl->d_eigh_scratch)
+                pl->eigh_grid = std::min(it->second.eigh_grid, pl->eigh_grid_alloc);
             apply_omb(pl, it->second.omb);
             if (report) {
                 *report = it->second.report;
@@ -2605,12 +2738,15 @@ extern "C" wnlqg_status wnlqg_b200_spectrum_noalloc(int64_t num_orbitals, int64_
     const int nw = (int)num_orbitals, nr = (int)num_r_vectors;
     const int64_t nn = (int64_t)nw * nw;
     // Scratch: phase table [n][NR] then H(k) [n][nw*nw], complex double, 256-byte aligned parts.
+    // The point count is bounded by a division first, so no product below can wrap around.
+    const size_t per_point = (size_t)(nr + nn) * sizeof(double2);
+    const size_t max_points = (WNLQG_NOALLOC_SCRATCH_BYTES - 256) / per_point;
+    const std::string too_many = "spectrum_noalloc: n*(NR + nw^2)*16 bytes exceeds the 8 MiB scratch; pass fewer points "
+                                 "per call (at most " + std::to_string(max_points) + ")";
+    if ((uint64_t)n > (uint64_t)max_points) return fail(WNLQG_ERR_INVALID_ARGUMENT, too_many);
     const size_t phase_bytes = (((size_t)n * nr * sizeof(double2)) + 255) & ~(size_t)255;
     const size_t hk_bytes = (size_t)n * nn * sizeof(double2);
-    if (phase_bytes + hk_bytes > WNLQG_NOALLOC_SCRATCH_BYTES)
-        return fail(WNLQG_ERR_INVALID_ARGUMENT,
-                    "spectrum_noalloc: n*(NR + nw^2)*16 bytes exceeds the 8 MiB scratch; pass fewer points per call (at most " +
-                        std::to_string(WNLQG_NOALLOC_SCRATCH_BYTES / ((size_t)(nr + nn) * sizeof(double2) + 256)) + ")");
+    if (phase_bytes + hk_bytes > WNLQG_NOALLOC_SCRATCH_BYTES) return fail(WNLQG_ERR_INVALID_ARGUMENT, too_many);
     int device = 0;
     WNLQG_CUDA(cudaGetDevice(&device));
     void *scratch = nullptr;

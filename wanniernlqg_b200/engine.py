@@ -154,6 +154,12 @@ class ResponseEngine:
     def last_launch_count(self) -> int:
         return int(self._L.wnlqg_b200_plan_last_launch_count(self._plan))
 
+    def status(self) -> None:
+        """After synchronising the stream of an asynchronous call (``*_device``, the many-plan
+        call): raises on a bounded device wait that gave up or on a k-point that failed the task's
+        spectral isolation contract (wnlqg_b200_plan_status)."""
+        _lib.check(self._L.wnlqg_b200_plan_status(self._plan))
+
     def autotune(self, mesh: Sequence[int], k_begin: int = 0, k_end: Optional[int] = None) -> dict:
         """Pick the eigensolver team size and the contraction tile by timing them on a block of
         ``mesh`` (wnlqg_b200_plan_autotune); the choice stays in this plan and in the process
