@@ -339,7 +339,9 @@ WNLQG_API wnlqg_status wnlqg_b200_graph_destroy(wnlqg_graph *graph);
  * energies, value count), so later plans with the same key take it without measuring.  Every
  * candidate is a configuration the library runs anyway; the tile choice leaves results bitwise
  * unchanged, while the grid choices decide how points are split among CTAs, and so the order of
- * the partial sums, and may change results in the last bits.  Times are CUDA-event milliseconds of the second of two runs; -1 = not a
+ * the partial sums: on the FP64 path they may change results in the last bits; on the mixed path
+ * they also change which neighbour each point's FP32 eigensolve warm-starts from, so results
+ * change within the mixed path's accuracy (about 1e-6 relative).  Times are CUDA-event milliseconds of the second of two runs; -1 = not a
  * candidate; 0 in a choice = not tunable for this plan. */
 typedef struct wnlqg_autotune_report {
     int32_t eigh_team;             /* chosen threads per matrix (32, 64, 128), 0 = fixed variant */

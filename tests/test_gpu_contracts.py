@@ -72,7 +72,8 @@ def test_berry_dipole_isolation_error_matches_oracle(engine_cls, oracle_mod, pre
         assert gexc.value.status == 1
         got = _parsed(str(gexc.value))
         assert got[:2] == ref[:2] and got[3] == ref[3] and got[4] == ref[4]
-        assert got[2] == pytest.approx(ref[2], rel=1e-9)
+        # Mixed-path energies come out of one FP64 refinement sweep: the gap agrees to ~1e-8.
+        assert got[2] == pytest.approx(ref[2], rel=1e-9 if precision == _abi.PRECISION_FP64 else 1e-6)
         with pytest.raises(EngineError):
             eng.weighted_sum(k, np.ones(len(k)))
         with pytest.raises(EngineError, match="NOT_ISOLATED"):
@@ -157,8 +158,8 @@ def test_qwz_chern_number_on_device(engine_cls, precision):
 def test_large_orbital_autotuned_grids_keep_results(engine_cls, oracle_mod, precision):
     """nw = 96 (per-CTA global working sets for the response passes and the CTA eigensolver
     stages): the autotuner's grid choices change how points are split among CTAs, and so the
-    summation order, but not the results beyond the last bits; tuned point values match the
-    oracle."""
+    summation order (FP64: last bits) and, on the mixed path, the FP32 eigensolver's warm-start
+    chains (results within the mixed accuracy); tuned point values match the oracle."""
     model = synthetic_orthogonal_model(96, 1, seed=41, full_position=True)
     task = _abi.TaskArrays([(_abi.SHIFT_CURRENT, ["xyy"]), (_abi.BERRY_CURVATURE, ["xy"]),
                             (_abi.QUANTUM_METRIC, ["xx"])], broadening_type=_abi.LORENTZIAN, broadening=0.02,
@@ -172,9 +173,10 @@ def test_large_orbital_autotuned_grids_keep_results(engine_cls, oracle_mod, prec
         got = eng.point_values(k)
     assert rep["response_grid"] != -1 and len(rep["response_grid_ms"]) == 3
     assert rep["eigh_grid"] != -1 and len(rep["eigh_grid_ms"]) == 3
-    for g, r in zip(task.split(after), task.split(before)):
-        assert rel_err(g, r) <= 1e-12
+    # FP64: only the summation order changes; mixed: the FP32 warm-start chains change too.
     tol = RTOL if precision == _abi.PRECISION_FP64 else MIXED_RTOL
+    for g, r in zip(task.split(after), task.split(before)):
+        assert rel_err(g, r) <= (1e-12 if precision == _abi.PRECISION_FP64 else 1e-5)
     ref = oracle_mod.point_values(model, task, k)
     for g, r in zip(task.split(got), task.split(ref)):
         assert rel_err(g, r) < tol
