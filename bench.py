@@ -194,6 +194,8 @@ def main():
                     help="skip the time-to-1e-4 convergence study of sigma^xyy (one GPU only)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the built-in eigensolver team and contraction tile rules")
+    ap.add_argument("--adaptive-study", action="store_true",
+                    help="add the learned adaptive refinement study (one GPU; a few minutes)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -304,7 +306,9 @@ def main():
     C = fourier_channels(task)
     # Algorithmic work per k-point (counts of the algorithms executed):
     #   staged Fourier (mesh): 8*P1*C*nw^2 flop (P1 = 9 distinct r1 on the |R_i|<=4 cube) and
-    #     C*nw^2*16 B written + read once (FP64 Wannier-gauge channels);
+    #     C*nw^2*16 B written (the FP64 Wannier-gauge channels) plus the line stage's reads,
+    #     P1*C*nw^2*16 B per line of n1 = 256 points (the channels' later read belongs to the
+    #     response kernel);
     #   tensor-core Fourier (random): S(S+1)/2 int8 slice products of 2*Kpad*Npad ops each
     #     (Kpad = 2*NR rounded up to 64, Npad = 2*C*nw^2 rounded up to the tile width);
     #   eigensolve: 30*nw^3 flop (LAPACK-class modelling count for a Hermitian eigensolve);
@@ -312,7 +316,7 @@ def main():
     p1 = 9
     flop = {"fourier": 8.0 * p1 * C * nw * nw, "eigen": 30.0 * nw ** 3,
             "response": 18 * 8.0 * nw ** 3 + 4.0 * nw * nw * 512}
-    hbm = {"fourier": 2.0 * C * nw * nw * 16, "eigen": nw * nw * 16 * 2.0 + nw * 8,
+    hbm = {"fourier": C * nw * nw * 16 * (1.0 + p1 / MESH[0]), "eigen": nw * nw * 16 * 2.0 + nw * 8,
            "response": (C - 1) * nw * nw * 16 + nw * nw * 16}
     sm_peak = {"fp64": 37.0, "mixed": 74.0}["fp64" if precision == _abi.PRECISION_FP64 else "mixed"]
     sm_src = "nominal B200 CUDA-core peak (FP64 37 / FP32 74 TFLOP/s; not in the measured peaks file)"
@@ -391,6 +395,8 @@ def main():
     engine.close()
     if rank == 0 and world == 1 and not args.no_time_to_tolerance:
         line["time_to_tolerance"] = time_to_tolerance(model, local_rank)
+    if rank == 0 and world == 1 and args.adaptive_study:
+        line["learned_adaptive"] = learned_time_to_tolerance(local_rank)
     if rank == 0 and world == 1 and not args.no_batched:
         line["batched_uneven"] = batched_uneven(local_rank)
         line["graph_small_calls"] = graph_small_calls(local_rank)
@@ -449,33 +455,135 @@ def time_to_tolerance(model, device: int, rtol: float = 1e-4, blocks: int = 4, b
             "speedup_mixed_vs_fp64": t64 / tmx}
 
 
-def batched_uneven(device: int, mesh: int = 16) -> dict:
-    """Several models of uneven orbital counts through one call: 12 seeded models with
-    nw in {6, 8, 12, 16, 24, 32}, every second one Kramers-doubled (H (x) I_2 + i 1e-3 eV M (x)
-    sigma_z, so nw up to 64), the Berry-curvature channel of the linear transport conductivity
-    sigma^xy and the Berry-curvature dipole D^xzz at
-    mu in {-0.5, 0, 0.5} eV and T = 50 K, each on its own mesh^3 mesh.  Timed (CUDA events on the
-    caller's stream) as one concurrent wnlqg_b200_eval_mesh_many call, as the same models one
-    call after another, and as that concurrent call captured once in a CUDA graph and replayed."""
+def adaptive_study(model, make_task_fn, device: int, *, omegas, support, n0: int, rtol: float, max_level: int,
+                   max_leaves: int = 4_000_000, max_evaluations: int = 60_000_000, seed: int = 3) -> dict:
+    """Time to tolerance of one response with the cell-adaptive integrator: the plain FP64 path
+    (every leaf checked, FP64 kernels) against the mixed + batched + learned path (mixed-precision
+    kernels, each round's uneven cells in one batched device call, the GPU-trained MLP choosing
+    which leaves to check, with the support guard).  Both run to `rtol` or to the leaf / evaluation
+    budget; times are wall clock of the whole adaptive run (device calls, host bookkeeping, feature
+    spectra and network training).  The plain run's value judges the learned run's."""
+    from wanniernlqg_b200.adaptive import MlpProposer, integrate_cells
+    from wanniernlqg_b200.engine import ResponseEngine
+
+    warm = np.random.default_rng(0).random((4096, 3))
+    kw = dict(n0=n0, rtol=rtol, max_level=max_level, max_leaves=max_leaves, max_evaluations=max_evaluations)
+    with ResponseEngine(model, make_task_fn(_abi.PRECISION_FP64), device=device) as eng:
+        eng.point_values(warm)
+        plain = integrate_cells(eng.point_values, **kw)
+    with ResponseEngine(model, make_task_fn(_abi.PRECISION_MIXED), device=device) as eng:
+        eng.point_values(warm)
+        eng.spectrum(warm, vectors=False)
+        prop = MlpProposer(0.0, omegas, lambda k: eng.spectrum(k, vectors=False), device=device, seed=seed,
+                           lattice=model.lattice, support=support)
+        try:
+            learned = integrate_cells(eng.point_values, proposer=prop, seed=seed, **kw)
+            spectra = prop.spectrum_evaluations
+        finally:
+            prop.close()
+
+    def summary(r):
+        scale = float(np.max(np.abs(r.value)))
+        return {"seconds": r.seconds, "evaluations": int(r.evaluations), "leaves": int(r.leaves),
+                "checked_cells": int(r.checked_cells), "rounds": int(r.rounds), "converged": bool(r.converged),
+                "error_estimate_rel": float(r.error_estimate / scale) if scale > 0 else None}
+
+    out = {"n0": n0, "max_level": max_level, "rtol": rtol, "max_leaves": max_leaves,
+           "plain_fp64": summary(plain), "mixed_batched_learned": summary(learned)}
+    out["mixed_batched_learned"].update({"fallback_rounds": int(learned.fallbacks), "feature_spectra": int(spectra),
+                                         "value_vs_plain_rel": float(np.max(np.abs(learned.value - plain.value)) /
+                                                                     np.max(np.abs(plain.value)))})
+    out["speedup"] = plain.seconds / learned.seconds
+    return out
+
+
+def learned_time_to_tolerance(device: int) -> dict:
+    """The learned adaptive refinement workload at its stated parameters and the nw = 32 shift
+    current on a low photon window (both opt-in: `--adaptive-study`).
+
+    * Band-crossing model: nw = 16 (|R_i| <= 2) with its onsite energies shifted so that a Weyl
+      crossing of bands 8/9 sits at mu = 0; injection current eta^xyz and eta^xyy at 20 photon
+      energies in [0.005, 0.1] eV, width 0.005 eV with the reference's default (Gaussian)
+      broadening, T = 0; cells from 48^3, up to 8 levels, rtol 1e-4.
+    * nw = 32 workload model: sigma^xyy at 32 photon energies in [0.01, 0.25] eV, Gaussian 0.01 eV,
+      mu = 0; cells from 24^3, up to 6 levels, rtol 1e-4."""
+    from wanniernlqg_b200.model import crossing_model
+
+    res = {}
+    om4 = np.linspace(0.005, 0.1, 20)
+    eta4 = 0.005
+    crossing = crossing_model(16, 2, 0)
+    for comp in ("xyz", "xyy"):
+        res[f"injection_{comp}_nw16_crossing"] = adaptive_study(
+            crossing, lambda prec, comp=comp: _abi.TaskArrays(
+                [(_abi.INJECTION_CURRENT, [comp])], broadening_type=_abi.GAUSSIAN, broadening=eta4,
+                photon_energies=om4, fermi_energy=0.0, precision=prec),
+            device, omegas=om4, support=(om4.min() - np.sqrt(200.0) * eta4, om4.max() + np.sqrt(200.0) * eta4),
+            n0=48, rtol=1e-4, max_level=8)
+    res["crossing"] = {"bands": [int(b) + 1 for b in crossing.crossing["bands"]], "gap_ev": crossing.crossing["gap_ev"]}
+    om2 = np.linspace(0.01, 0.25, 32)
+    res["shift_xyy_nw32_low_window"] = adaptive_study(
+        reference_workload_model("nw32"),
+        lambda prec: _abi.TaskArrays([(_abi.SHIFT_CURRENT, ["xyy"])], broadening_type=_abi.GAUSSIAN, broadening=0.01,
+                                     photon_energies=om2, fermi_energy=0.0, precision=prec),
+        device, omegas=om2, support=(om2.min() - np.sqrt(200.0) * 0.01, om2.max() + np.sqrt(200.0) * 0.01),
+        n0=24, rtol=1e-4, max_level=6)
+    return res
+
+
+def cfg3_models(seed: int = 2024):
+    """The batched uneven workload's 24 seeded models: orbital counts drawn from {6, 8, 12, 16,
+    24, 32, 48, 64, 96}, R cubes |R_i| <= 2, 3 or 4, every second model Kramers-doubled (a model
+    of half the drawn count, doubled as H (x) I_2 + i 1e-3 eV M (x) sigma_z), each with its own mesh
+    from {64, 96, 128, 160, 192}^3."""
+    from wanniernlqg_b200.model import kramers_doubled_model, synthetic_orthogonal_model
+    rng = np.random.default_rng(seed)
+    choices = [6, 8, 12, 16, 24, 32, 48, 64, 96]
+    out = []
+    for i in range(24):
+        nw = int(rng.choice(choices))
+        cube = int(rng.integers(2, 5))
+        mesh = int(rng.choice([64, 96, 128, 160, 192]))
+        doubled = i % 2 == 1
+        base = synthetic_orthogonal_model(nw // 2 if doubled else nw, cube, seed=300 + i, full_position=True)
+        model = kramers_doubled_model(base, 1e-3, seed=i) if doubled else base
+        out.append((model, (mesh, mesh, mesh), doubled, cube))
+    return out
+
+
+def batched_uneven(device: int, points_per_model: int = 65536) -> dict:
+    """The batched uneven workload: the 24 models of cfg3_models, the Berry-curvature channel of
+    the linear transport conductivity sigma^xy (the reference's finite-temperature Hall response;
+    its intrinsic AHC is zero-temperature only) and the Berry-curvature dipole D^xz (Omega^xy with
+    the x velocity, component xyx) at mu in {-0.5, 0, 0.5} eV and T = 50 K.  The dipole threshold
+    is 1e-9 eV, so that the 1e-3 eV Kramers splittings count as isolated (the reference's 2e-3 eV
+    default refuses those models).  Every plan is autotuned on its own first block (choices cached
+    per orbital count); each model then sums the first `points_per_model` points of its own mesh
+    (a lane range).  Timed with CUDA events on the caller's stream: one concurrent
+    wnlqg_b200_eval_mesh_many call, the models one call after another, and the concurrent call
+    captured once as a CUDA graph and replayed."""
     import torch
     from wanniernlqg_b200.engine import CapturedGraph, ResponseEngine, integrate_meshes_many
-    from wanniernlqg_b200.model import kramers_doubled_model, synthetic_orthogonal_model
 
-    # The finite-temperature Hall response as the reference defines it (the linear transport Berry
-    # channel; its intrinsic AHC is zero-temperature only) and the Berry dipole at a degeneracy
-    # threshold that counts the O(1e-3 eV) Kramers splittings as isolated.
-    task = _abi.TaskArrays([(_abi.LINEAR_TRANSPORT_BERRY, ["xy"]), (_abi.BERRY_DIPOLE, ["xzz"])],
+    task = _abi.TaskArrays([(_abi.LINEAR_TRANSPORT_BERRY, ["xy"]), (_abi.BERRY_DIPOLE, ["xyx"])],
                            fermi_energies=[-0.5, 0.0, 0.5], temperature=50.0, degeneracy_threshold=1e-9)
-    models = []
-    for i, nw in enumerate([6, 8, 12, 16, 24, 32] * 2):
-        base = synthetic_orthogonal_model(nw, 2 if nw <= 16 else 1, seed=100 + i, full_position=True)
-        models.append(kramers_doubled_model(base, 1e-3, seed=i) if i % 2 else base)
-    nk = mesh ** 3
-    engines = [ResponseEngine(m, task, device=device, max_batch=nk) for m in models]
+    spec = cfg3_models()
+    engines = []
     try:
+        tuning = {}
+        for model, mesh, _, _ in spec:
+            # Small models hold one whole sample per batch; large ones take the library's ~4 GiB
+            # batch workspace (a 65536-point batch at 96 orbitals would need ~70 GB).
+            eng = ResponseEngine(model, task, device=device,
+                                 max_batch=points_per_model if model.num_orbitals <= 48 else 0)
+            engines.append(eng)
+            rep = eng.autotune(mesh, 0, min(points_per_model, 16384))
+            tuning.setdefault(model.num_orbitals, {"eigh_team": rep["eigh_team"], "eigh_grid": rep["eigh_grid"],
+                                                   "response_grid": rep["response_grid"],
+                                                   "warm_start": rep["warm_start"]})
         outs = [torch.zeros(2 * e.value_count, dtype=torch.float64, device="cuda") for e in engines]
-        meshes = [(mesh, mesh, mesh)] * len(engines)
-        ranges = [(0, nk)] * len(engines)
+        meshes = [m for _, m, _, _ in spec]
+        ranges = [(0, min(points_per_model, int(np.prod(m)))) for m in meshes]
         stream = torch.cuda.current_stream()
         ptrs = [o.data_ptr() for o in outs]
 
@@ -483,8 +591,8 @@ def batched_uneven(device: int, mesh: int = 16) -> dict:
             integrate_meshes_many(engines, meshes, ranges, ptrs, stream.cuda_stream)
 
         def sequential():
-            for e, o in zip(engines, outs):
-                e.integrate_mesh_device(meshes[0], 0, nk, o.data_ptr(), stream.cuda_stream)
+            for e, m, r, o in zip(engines, meshes, ranges, outs):
+                e.integrate_mesh_device(m, r[0], r[1], o.data_ptr(), stream.cuda_stream)
                 torch.cuda.synchronize()
 
         def timed(fn):
@@ -498,22 +606,27 @@ def batched_uneven(device: int, mesh: int = 16) -> dict:
             return ev0.elapsed_time(ev1)
 
         t_conc = timed(concurrent)
+        for e in engines:
+            e.status()
         t_seq = timed(sequential)
-        # The same call captured once as a CUDA graph and replayed.
         graph = CapturedGraph.mesh_many(engines, meshes, ranges, ptrs)
         try:
             t_graph = timed(lambda: graph.launch(stream.cuda_stream))
+            graph.status()
             graph_kernels = graph.kernel_count
         finally:
             graph.close()
     finally:
         for e in engines:
             e.close()
-    total = nk * len(models)
-    return {"models": len(models), "orbitals": [m.num_orbitals for m in models], "mesh": mesh,
-            "responses": "linear transport Berry channel xy + Berry dipole xzz at 3 Fermi energies, T = 50 K",
+    total = sum(r[1] - r[0] for r in ranges)
+    return {"models": len(spec), "orbitals": [m.num_orbitals for m, _, _, _ in spec],
+            "kramers_doubled": [bool(d) for _, _, d, _ in spec], "r_cube": [c for _, _, _, c in spec],
+            "meshes": [m[0] for m in meshes], "points_per_model": points_per_model,
+            "responses": "linear transport Berry channel xy + Berry dipole xyx (D^xz) at 3 Fermi energies, T = 50 K",
+            "autotune_per_orbitals": {str(k): v for k, v in sorted(tuning.items())},
             "concurrent_ms": t_conc, "sequential_ms": t_seq, "speedup": t_seq / t_conc,
-            "graph_ms": t_graph, "graph_kernels": graph_kernels,
+            "graph_ms": t_graph, "graph_kernels": graph_kernels, "kpoints_per_s_graph": total / (t_graph / 1e3),
             "kpoints_per_s": total / (t_conc / 1e3)}
 
 

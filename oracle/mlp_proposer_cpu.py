@@ -14,6 +14,9 @@ class NumpyMlpProposer(MlpProposer):
         om = np.asarray(omegas, dtype=np.float64)
         self.om_lo, self.om_hi = float(om.min()), float(om.max())
         self.spectrum_fn = spectrum_fn
+        self.kscale = 2.0 * np.pi * np.ones(3)
+        self.support = None
+        self.must_check = None
         self.train_steps = train_steps
         self.lr = learning_rate
         self.X, self.E = [], []

@@ -15,8 +15,9 @@ Scheme (this engine's own; the reference's adaptive integrator is the HCubature 
 * Stop when sum(errors) <= rtol * ||I||.
 
 The plain method checks every leaf.  The learned method (``MlpProposer``) predicts log10 of each
-unchecked leaf's error from cheap features (cell centre, size, parent error, the centre value
-and the distance of the centre's spectrum to the Fermi level and to the photon window) and
+unchecked leaf's error from cheap features (cell centre and size, the local minimum transition
+energy across the Fermi level and that pair's |v_nm| from the spectrum, the parent's error and
+the centre value) and
 checks only the leaves predicted above the threshold plus a random audit sample.  The audit
 estimates the error mass the network missed (audited under-prediction divided by the audit
 fraction); if that mass exceeds the tolerance budget, the round falls back to the plain method
@@ -59,7 +60,7 @@ class MlpProposer:
     """Feature builder plus the GPU MLP (wnlqg_b200_mlp_*) trained online on checked cells."""
 
     def __init__(self, fermi_energy: float, omegas, spectrum_fn: Callable, *, device: int = 0, seed: int = 1,
-                 train_steps: int = 200, learning_rate: float = 3e-3):
+                 train_steps: int = 200, learning_rate: float = 3e-3, lattice=None, support=None):
         self.L = _lib.load()
         self.m = ctypes.c_void_p()
         _lib.check(self.L.wnlqg_b200_mlp_create(device, seed, ctypes.byref(self.m)))
@@ -67,6 +68,14 @@ class MlpProposer:
         om = np.asarray(omegas, dtype=np.float64)
         self.om_lo, self.om_hi = (float(om.min()), float(om.max())) if om.size else (0.0, 0.0)
         self.spectrum_fn = spectrum_fn
+        # Transition energies (eV) where the integrand can be nonzero (for interband responses at
+        # T = 0: the photon window widened by the broadening's support; (-inf, inf) for Lorentzian
+        # tails).  None: no guard, for integrands that are not band resonances.
+        self.support = support
+        self.must_check = None
+        # Cartesian length (Angstrom^-1) of a unit fractional step along each axis: 2 pi |b_a|.
+        lat = np.eye(3) if lattice is None else np.asarray(lattice, dtype=np.float64)
+        self.kscale = 2.0 * np.pi * np.linalg.norm(np.linalg.inv(lat), axis=0)
         self.train_steps = train_steps
         self.lr = learning_rate
         self.X = []
@@ -85,22 +94,47 @@ class MlpProposer:
             pass
 
     def features(self, centers, sizes, parent_err, coarse_norm) -> np.ndarray:
-        e, _ = self.spectrum_fn(centers)
-        self.spectrum_evaluations += centers.shape[0]
-        dmu = np.min(np.abs(e - self.mu), axis=1)
-        occ = e <= self.mu
-        # Smallest distance of an occupied -> empty transition energy to the photon window.
-        emax_occ = np.where(occ, e, -np.inf).max(axis=1)
-        emin_emp = np.where(~occ, e, np.inf).min(axis=1)
-        gap = emin_emp - emax_occ
-        dwin = np.where(gap < self.om_lo, self.om_lo - gap, np.where(gap > self.om_hi, gap - self.om_hi, 0.0))
+        """Eight inputs per cell: its centre (sin 2 pi c per axis), its size, the local minimum
+        transition energy across mu (the smallest E_m - E_n with n occupied and m empty at the
+        centre), |v_nm| of that pair (|grad (E_m - E_n)| by a forward difference of the spectrum,
+        eV Angstrom), and the method's own signals: the parent's error and the centre value."""
+        n = centers.shape[0]
+        h = 1e-4
+        pts = np.concatenate([centers] + [centers + h * np.eye(3)[a] for a in range(3)]) % 1.0
+        e, _ = self.spectrum_fn(pts)
+        self.spectrum_evaluations += pts.shape[0]
+        e0 = e[:n]
+        occ = e0 <= self.mu
+        # Smallest occupied -> empty transition energy and its band pair.
+        n_top = np.where(occ, np.arange(e0.shape[1])[None, :], -1).max(axis=1)
+        m_bot = np.where(~occ, np.arange(e0.shape[1])[None, :], e0.shape[1]).min(axis=1)
+        ok = (n_top >= 0) & (m_bot < e0.shape[1])
+        nt, mb = np.clip(n_top, 0, e0.shape[1] - 1), np.clip(m_bot, 0, e0.shape[1] - 1)
+        rows = np.arange(n)
+        gap = np.where(ok, e0[rows, mb] - e0[rows, nt], 10.0)
+        grad = np.zeros((n, 3))
+        for a in range(3):
+            ea = e[(a + 1) * n:(a + 2) * n]
+            grad[:, a] = (ea[rows, mb] - ea[rows, nt] - gap) / (h * self.kscale[a])
+        vnm = np.where(ok, np.linalg.norm(grad, axis=1), 0.0)
+        # Support guard (not learned): a cell whose smallest transition energy can reach the
+        # support anywhere inside it (gap - |v_nm| times the Cartesian half diagonal) must be checked,
+        # whatever the network predicts, so that a resonance no training sample has hit is never
+        # skipped.  Cells without a pair across mu carry no interband weight.
+        if self.support is None:
+            self.must_check = None
+        else:
+            half_diag = 0.5 * np.sqrt(np.sum((np.asarray(sizes)[:, None] * self.kscale[None, :]) ** 2, axis=1))
+            lo = gap - vnm * half_diag
+            hi = gap + vnm * half_diag
+            self.must_check = ok & (hi >= self.support[0]) & (lo <= self.support[1])
         f = np.stack([
             np.sin(2 * np.pi * centers[:, 0]), np.sin(2 * np.pi * centers[:, 1]), np.sin(2 * np.pi * centers[:, 2]),
             np.log2(sizes) / 8.0,
+            np.log10(np.maximum(gap, 1e-6)),
+            np.log10(np.maximum(vnm, 1e-6)),
             np.log10(np.maximum(parent_err, 1e-30)) / 10.0,
             np.log10(np.maximum(coarse_norm, 1e-30)) / 10.0,
-            np.log10(np.maximum(dmu, 1e-6)),
-            np.log10(np.maximum(dwin, 1e-6)),
         ], axis=1)
         return np.ascontiguousarray(f, dtype=np.float32)
 
@@ -135,11 +169,14 @@ class MlpProposer:
 def integrate_cells(point_values: Callable, *, n0: int = 16, rtol: float = 1e-4, max_level: int = 8,
                     max_evaluations: int = 50_000_000, proposer: Optional[MlpProposer] = None,
                     warmup_fraction: float = 0.15, audit_fraction: float = 0.05,
-                    safety: float = 4.0, seed: int = 0, component=None) -> AdaptiveResult:
+                    safety: float = 4.0, seed: int = 0, component=None,
+                    max_leaves: int = 2_000_000, max_rounds: int = 1_000_000) -> AdaptiveResult:
     """Integrate the domain average of point_values(k[n,3]) -> [n, V] over [0,1)^3.
 
     `component` (index array) restricts the error norm to those value entries (for example the
-    sigma^xyy(omega) block); the integral covers all entries."""
+    sigma^xyy(omega) block); the integral covers all entries.  Every leaf keeps its coarse, fine
+    and 8 octant values (10 V complex numbers), so `max_leaves` bounds the host memory: a round
+    that would exceed it ends the run unconverged, like the evaluation budget."""
     t0 = time.perf_counter()
     rng = np.random.default_rng(seed)
     g = (np.arange(n0) + 0.5) / n0
@@ -198,10 +235,14 @@ def integrate_cells(point_values: Callable, *, n0: int = 16, rtol: float = 1e-4,
             pred[todo] = p * vol[todo] / vol[todo].max()
             value_now = np.where(checked[:, None], fine, coarse).sum(axis=0)
             budget = rtol * _norm(value_now[sel]) / safety
-            rest = todo[~checked[todo]]
+            guard = proposer.must_check
+            rest_mask = ~checked[todo]
+            rest = todo[rest_mask]
             order = np.argsort(-pred[rest], kind="stable")
             csum = np.cumsum(pred[rest][order][::-1])[::-1]
             must = order[csum > budget * 0.5]
+            if guard is not None:
+                must = np.union1d(must, np.where(guard[rest_mask])[0])
             audit = rng.random(rest.size) < audit_fraction
             pick = np.zeros(rest.size, dtype=bool)
             pick[must] = True
@@ -209,9 +250,9 @@ def integrate_cells(point_values: Callable, *, n0: int = 16, rtol: float = 1e-4,
             chosen = rest[pick]
             check(chosen)
             checked_total += chosen.size
-            proposer.observe(proposer.features(centers[chosen], 2 * half[chosen], parent_err[chosen],
-                                               np.max(np.abs(coarse[chosen][:, sel]), axis=1) / vol[chosen]),
-                             err[chosen])
+            where = np.full(centers.shape[0], -1, dtype=np.int64)
+            where[todo] = np.arange(todo.size)
+            proposer.observe(feats[where[chosen]], err[chosen])
             aud = rest[audit & ~np.isin(np.arange(rest.size), must)]
             if aud.size:
                 # The audit estimates the error mass the network missed among the unchecked leaves
@@ -232,12 +273,15 @@ def integrate_cells(point_values: Callable, *, n0: int = 16, rtol: float = 1e-4,
             return AdaptiveResult(value, total_err, evaluations, centers.shape[0], checked_total, rounds, True,
                                   time.perf_counter() - t0, fallbacks)
         splittable = np.where(checked & (level < max_level))[0]
-        if splittable.size == 0 or evaluations >= max_evaluations:
+        if splittable.size == 0 or evaluations >= max_evaluations or rounds >= max_rounds:
             return AdaptiveResult(value, total_err, evaluations, centers.shape[0], checked_total, rounds, False,
                                   time.perf_counter() - t0, fallbacks)
         order = splittable[np.argsort(-est[splittable], kind="stable")]
         keep_err = total_err - np.cumsum(est[order])
         nsplit = int(np.searchsorted(-keep_err, -0.5 * rtol * inorm)) + 1
+        if centers.shape[0] + 7 * min(nsplit, order.size) > max_leaves:
+            return AdaptiveResult(value, total_err, evaluations, centers.shape[0], checked_total, rounds, False,
+                                  time.perf_counter() - t0, fallbacks)
         split = order[:min(nsplit, order.size)]
         # Children: octant centres of each split cell, coarse values from the parent's octants.
         ch_c = (centers[split, None, :] + OCTANTS[None, :, :] * half[split, None, None]).reshape(-1, 3)

@@ -133,17 +133,18 @@ class ResponseEngine:
         from .symmetry import integrate_mesh_reduced
         return integrate_mesh_reduced(self.mesh_weighted_sum, self.task, mesh, operations, orbits=orbits)
 
-    def spectrum(self, kpoints):
-        """(energies [n, nw], canonical eigenvectors [n, nw, nw]) at fractional k-points."""
+    def spectrum(self, kpoints, vectors: bool = True):
+        """(energies [n, nw], canonical eigenvectors [n, nw, nw] or None when ``vectors`` is
+        false) at fractional k-points."""
         k = np.ascontiguousarray(np.asarray(kpoints, dtype=np.float64).reshape(-1, 3))
         nw = self.model.num_orbitals
         e = np.zeros((k.shape[0], nw))
         # Column-major per k: store as [n, col, row] and transpose.
-        u = np.zeros((k.shape[0], nw, nw), dtype=np.complex128)
-        _lib.check(self._L.wnlqg_b200_eval_spectrum(self._plan, k.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
-                                                    k.shape[0], e.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
-                                                    u.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
-        return e, np.ascontiguousarray(u.transpose(0, 2, 1))
+        u = np.zeros((k.shape[0], nw, nw), dtype=np.complex128) if vectors else None
+        dp = ctypes.POINTER(ctypes.c_double)
+        _lib.check(self._L.wnlqg_b200_eval_spectrum(self._plan, k.ctypes.data_as(dp), k.shape[0], e.ctypes.data_as(dp),
+                                                    u.ctypes.data_as(dp) if vectors else None))
+        return e, (np.ascontiguousarray(u.transpose(0, 2, 1)) if vectors else None)
 
     def last_timing(self):
         """Device milliseconds (fourier, eigen, response, total) of the last mesh evaluation."""

@@ -269,12 +269,57 @@ def kramers_doubled_model(model: TightBindingModel, lam: float = 1e-3, seed: int
     return TightBindingModel(model.lattice.copy(), model.r_vectors.copy(), model.r_degeneracies.copy(), ham, pos)
 
 
+def crossing_model(nw: int = 16, rmax: int = 2, seed: int = 0, *, grid: int = 20) -> TightBindingModel:
+    """The synthetic model with its onsite energies shifted so that two bands cross at the Fermi
+    level mu = 0: the adjacent pair (n, n+1) around the middle of the spectrum whose direct gap
+    min_k (E_{n+1} - E_n) is smallest on a grid^3 mesh is located, the minimum refined by a
+    Nelder-Mead search in k, and every home-cell diagonal energy shifted by the midpoint of the two
+    bands there (a uniform shift: the spectrum moves rigidly).  The pair's energies at the
+    crossing are then within the minimum gap (a Weyl point in 3D without symmetry: usually below
+    1e-3 eV) of mu = 0."""
+    from scipy.optimize import minimize
+
+    base = synthetic_orthogonal_model(nw, rmax, seed, full_position=True)
+    rv = base.r_vectors.astype(np.float64)
+
+    def energies(kfrac):
+        ph = np.exp(2j * np.pi * (rv.T @ np.asarray(kfrac))) / base.r_degeneracies
+        return np.linalg.eigvalsh(np.einsum("ijr,r->ij", base.hamiltonian_r, ph))
+
+    g = (np.arange(grid) + 0.5) / grid
+    kz, ky, kx = np.meshgrid(g, g, g, indexing="ij")
+    ks = np.stack([kx.ravel(), ky.ravel(), kz.ravel()], axis=1)
+    ph = np.exp(2j * np.pi * (ks @ rv)) / base.r_degeneracies
+    hk = np.einsum("ijr,kr->kij", base.hamiltonian_r, ph)
+    ev = np.linalg.eigvalsh(hk)
+    mids = range(nw // 2 - 2, nw // 2 + 1)
+    best = None
+    for n in mids:
+        gap = ev[:, n + 1] - ev[:, n]
+        i = int(np.argmin(gap))
+        res = minimize(lambda k: float(np.diff(energies(k % 1.0))[n]), ks[i], method="Nelder-Mead",
+                       options={"xatol": 1e-10, "fatol": 1e-12, "maxiter": 4000})
+        if best is None or res.fun < best[0]:
+            best = (float(res.fun), n, res.x % 1.0)
+    gap, n, kstar = best
+    e = energies(kstar)
+    shift = 0.5 * (e[n] + e[n + 1])
+    ham = base.hamiltonian_r.copy(order="F")
+    home = int(np.where(np.all(base.r_vectors == 0, axis=0))[0][0])
+    ham[np.arange(nw), np.arange(nw), home] -= shift
+    model = TightBindingModel(base.lattice.copy(), base.r_vectors.copy(), base.r_degeneracies.copy(), ham,
+                              base.position_r.copy(order="F"))
+    model.crossing = {"bands": (n, n + 1), "k": kstar, "gap_ev": gap}
+    return model
+
+
 def reference_workload_model(name: str) -> TightBindingModel:
     """Models of the reference workloads, by the short name used in tests and the bench.
 
     ``nw4``: nw=4, |R_i|<=2 (125 R), diagonal position operator (CPU-runnable case).
     ``nw32``: nw=32, |R_i|<=4 (729 R), full off-diagonal A(R).
-    ``nw16_crossing``: nw=16, |R_i|<=2 with a home-cell shift that puts a band crossing near 0 eV.
+    ``nw16_crossing``: nw=16, |R_i|<=2, onsite energies shifted so that two bands cross at 0 eV
+    (:func:`crossing_model`).
     ``nw64_nonorth``: nw=64, |R_i|<=3 (343 R), with S(R).
     """
     if name == "nw4":
@@ -282,7 +327,7 @@ def reference_workload_model(name: str) -> TightBindingModel:
     if name == "nw32":
         return synthetic_orthogonal_model(32, 4, 0, full_position=True)
     if name == "nw16_crossing":
-        return synthetic_orthogonal_model(16, 2, 0, full_position=True)
+        return crossing_model(16, 2, 0)
     if name == "nw64_nonorth":
         return synthetic_nonorthogonal_model(64, 3, 0)
     raise KeyError(name)
