@@ -276,6 +276,13 @@ def main():
         elapsed_ms = float(t.item())
         dist.barrier()
     value = world * batch * args.steps / (elapsed_ms / 1e3)
+    # The data path's one exchange, outside the timed region: the ranks' lane tensors (here each
+    # rank's last block sum, value_count complex values) combined by one NCCL all-reduce, then read
+    # back on rank 0; every rank's block is different, so the combined sum checks the exchange.
+    combined = out.clone()
+    if dist:
+        dist.all_reduce(combined)
+    lane_sum = combined.cpu().numpy().view(np.complex128)
 
     # End to end through the public host API: the step's mesh indices and weights in pinned
     # host memory (H2D), the weighted mesh sum, and the result read back (D2H); synchronous,
@@ -386,6 +393,8 @@ def main():
                 "d2h_bytes_per_step": int(16 * vc)},
         "clocks": clocks,
         "gpu_launches": launches,
+        "lane_exchange": {"ranks": world, "collective": "all_reduce (NCCL)" if dist else "none (one rank)",
+                          "values": int(vc), "max_abs": float(np.max(np.abs(lane_sum)))},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -456,7 +465,7 @@ def time_to_tolerance(model, device: int, rtol: float = 1e-4, blocks: int = 4, b
 
 
 def adaptive_study(model, make_task_fn, device: int, *, omegas, support, n0: int, rtol: float, max_level: int,
-                   max_leaves: int = 4_000_000, max_evaluations: int = 60_000_000, seed: int = 3) -> dict:
+                   max_leaves: int = 1_500_000, max_evaluations: int = 30_000_000, seed: int = 3) -> dict:
     """Time to tolerance of one response with the cell-adaptive integrator: the plain FP64 path
     (every leaf checked, FP64 kernels) against the mixed + batched + learned path (mixed-precision
     kernels, each round's uneven cells in one batched device call, the GPU-trained MLP choosing

@@ -203,10 +203,14 @@ def integrate_cells(point_values: Callable, *, n0: int = 16, rtol: float = 1e-4,
         nonlocal evaluations
         if idx.size == 0:
             return
-        pts = (centers[idx, None, :] + OCTANTS[None, :, :] * half[idx, None, None]).reshape(-1, 3)
-        vals = point_values(pts % 1.0).reshape(idx.size, 8, nv)
-        evaluations += pts.shape[0]
-        octv[idx] = vals
+        # In chunks of at most 131072 cells (about 1M points), so that one device call's host
+        # arrays stay small.
+        for c0 in range(0, idx.size, 131072):
+            sub = idx[c0:c0 + 131072]
+            pts = (centers[sub, None, :] + OCTANTS[None, :, :] * half[sub, None, None]).reshape(-1, 3)
+            octv[sub] = point_values(pts % 1.0).reshape(sub.size, 8, nv)
+            evaluations += pts.shape[0]
+        vals = octv[idx]
         fine[idx] = vals.mean(axis=1) * vol[idx, None]
         # Midpoint rules converge as h^2: the fine value's error is |fine - coarse| / 3.
         err[idx] = np.max(np.abs((fine[idx] - coarse[idx])[:, sel]), axis=1) / 3.0
