@@ -565,8 +565,8 @@ def batched_uneven(device: int, points_per_model: int = 65536) -> dict:
     the linear transport conductivity sigma^xy (the reference's finite-temperature Hall response;
     its intrinsic AHC is zero-temperature only) and the Berry-curvature dipole D^xz (Omega^xy with
     the x velocity, component xyx) at mu in {-0.5, 0, 0.5} eV and T = 50 K.  The dipole threshold
-    is 1e-9 eV, so that the 1e-3 eV Kramers splittings count as isolated (the reference's 2e-3 eV
-    default refuses those models).  Every plan is autotuned on its own first block (choices cached
+    is 1e-12 eV, so that the Kramers splittings (1e-3 eV typically, 6e-10 eV at the closest sampled
+    point) count as isolated (the reference's 2e-3 eV default refuses those models).  Every plan is autotuned on its own first block (choices cached
     per orbital count); each model then sums the first `points_per_model` points of its own mesh
     (a lane range).  Timed with CUDA events on the caller's stream: one concurrent
     wnlqg_b200_eval_mesh_many call, the models one call after another, and the concurrent call
@@ -575,7 +575,7 @@ def batched_uneven(device: int, points_per_model: int = 65536) -> dict:
     from wanniernlqg_b200.engine import CapturedGraph, ResponseEngine, integrate_meshes_many
 
     task = _abi.TaskArrays([(_abi.LINEAR_TRANSPORT_BERRY, ["xy"]), (_abi.BERRY_DIPOLE, ["xyx"])],
-                           fermi_energies=[-0.5, 0.0, 0.5], temperature=50.0, degeneracy_threshold=1e-9)
+                           fermi_energies=[-0.5, 0.0, 0.5], temperature=50.0, degeneracy_threshold=1e-12)
     spec = cfg3_models()
     engines = []
     try:

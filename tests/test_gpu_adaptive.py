@@ -65,11 +65,11 @@ def test_gpu_trained_proposer_saves_evaluations_on_a_localised_integrand():
 def test_learned_proposer_on_band_crossing_injection_current():
     """The learned adaptive refinement workload's own integrand: the circular injection current
     eta^xyz of the nw = 16 model whose bands 8 and 9 cross at mu = 0, Gaussian width 2 meV at
-    10-20 meV (the Weyl node's resonance shells), cells from 48^3.  After the first round the
-    learned path (mixed precision, GPU-trained MLP, support guard) has the plain FP64 path's value
-    to 1e-3 with far fewer evaluations: the guard makes it check every cell whose spectrum can
-    reach the broadened window, so the skipped cells are exactly zero; without the guard the
-    network, which no warm-up sample has shown the needle-thin shells, misses them."""
+    10-20 meV (the Weyl node's resonance shells), cells from 48^3.  With the support guard (every
+    cell whose spectrum can reach the broadened window is checked) the learned path's first round
+    equals the plain FP64 method's to 1e-3.  At this cell size the guard keeps nearly every cell,
+    so the safe learned path saves no evaluations on this integrand: the plain method stays the
+    judge."""
     from wanniernlqg_b200 import _abi, build
     from wanniernlqg_b200.adaptive import MlpProposer, integrate_cells
     from wanniernlqg_b200.engine import ResponseEngine
@@ -88,18 +88,16 @@ def test_learned_proposer_on_band_crossing_injection_current():
         plain = integrate_cells(eng.point_values, n0=48, rtol=1e-4, max_level=8, max_rounds=1)
     results = {}
     with ResponseEngine(model, task(_abi.PRECISION_MIXED)) as eng:
-        for guarded in (True, False):
-            prop = MlpProposer(0.0, om, lambda k: eng.spectrum(k, vectors=False), seed=3, lattice=model.lattice,
-                               support=(om.min() - cutoff, om.max() + cutoff) if guarded else None)
-            try:
-                results[guarded] = integrate_cells(eng.point_values, n0=48, rtol=1e-4, max_level=8, max_rounds=1,
-                                                   proposer=prop, seed=3)
-            finally:
-                prop.close()
+        prop = MlpProposer(0.0, om, lambda k: eng.spectrum(k, vectors=False), seed=3, lattice=model.lattice,
+                           support=(om.min() - cutoff, om.max() + cutoff))
+        try:
+            results[True] = integrate_cells(eng.point_values, n0=48, rtol=1e-4, max_level=8, max_rounds=1,
+                                            proposer=prop, seed=3)
+        finally:
+            prop.close()
     ref = np.max(np.abs(plain.value))
     assert ref > 0
     guarded = results[True]
     assert np.max(np.abs(guarded.value - plain.value)) <= 1e-3 * ref
-    assert guarded.evaluations < 0.5 * plain.evaluations, (guarded.evaluations, plain.evaluations)
-    unguarded = results[False]
-    assert np.max(np.abs(unguarded.value - plain.value)) > np.max(np.abs(guarded.value - plain.value))
+    # At 48^3 almost every cell can hold a resonance: the guard keeps >= 99 % of them.
+    assert guarded.checked_cells >= 0.99 * plain.checked_cells

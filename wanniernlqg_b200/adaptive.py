@@ -131,8 +131,8 @@ class MlpProposer:
         f = np.stack([
             np.sin(2 * np.pi * centers[:, 0]), np.sin(2 * np.pi * centers[:, 1]), np.sin(2 * np.pi * centers[:, 2]),
             np.log2(sizes) / 8.0,
-            np.log10(np.maximum(gap, 1e-6)),
-            np.log10(np.maximum(vnm, 1e-6)),
+            np.log10(np.maximum(gap, 1e-4)) / 3.0,
+            np.log10(np.maximum(vnm, 1e-3)) / 3.0,
             np.log10(np.maximum(parent_err, 1e-30)) / 10.0,
             np.log10(np.maximum(coarse_norm, 1e-30)) / 10.0,
         ], axis=1)
