@@ -78,3 +78,71 @@ WNLQG_D void dmma_product(const double2 *X, const double2 *Y, double2 *out, int 
         }
     }
 }
+
+// Two independent products in one pass: out0 = op(X0, Y0) and out1 = op(X1, Y1) (MODE 0: X Y,
+// MODE 1: X^H Y, MODE 2: X Y - Y X, where X must have leading dimension ld).  Each warp takes the same tile pair of both products, so it keeps four
+// accumulator tiles (eight independent DMMA chains) in flight instead of two.  X0 and X1 have
+// their own leading dimensions (a Wannier-gauge channel can be read straight from global memory,
+// ldx = nw); Y and out use ld.  out0 and out1 must not alias any operand.  No closing barrier.
+template <int MODE>
+WNLQG_D void dmma_product_pair(const double2 *X0, int ldx0, const double2 *Y0, double2 *out0, const double2 *X1,
+                               int ldx1, const double2 *Y1, double2 *out1, int nw, int ld) {
+    const int nt = (nw + 7) >> 3;
+    const int ntiles = nt * nt;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int fr = lane >> 2, fk = lane & 3;
+    const double2 zero = make_double2(0.0, 0.0);
+    auto a_elem = [&](const double2 *M, int ldm, int i, int k) -> double2 {
+        if (i >= nw || k >= nw) return zero;
+        if (MODE == 1) {
+            const double2 v = M[k + ldm * i];
+            return make_double2(v.x, -v.y);
+        }
+        return M[i + ldm * k];
+    };
+    auto b_elem = [&](const double2 *M, int k, int j) -> double2 {
+        return (k < nw && j < nw) ? M[k + ld * j] : zero;
+    };
+    for (int t0 = 2 * warp; t0 < ntiles; t0 += 2 * nwarps) {
+        const int t1 = t0 + 1 < ntiles ? t0 + 1 : t0;
+        const int r0 = 8 * (t0 / nt), c0 = 8 * (t0 % nt);
+        const int r1 = 8 * (t1 / nt), c1 = 8 * (t1 % nt);
+        double re[4][2], im[4][2];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) { re[q][0] = re[q][1] = 0.0; im[q][0] = im[q][1] = 0.0; }
+        for (int k0 = 0; k0 < nw; k0 += 4) {
+            const int ka = k0 + fk;
+            const double2 a0 = a_elem(X0, ldx0, r0 + fr, ka), b0 = b_elem(Y0, ka, c0 + fr);
+            const double2 a1 = a_elem(X0, ldx0, r1 + fr, ka), b1 = b_elem(Y0, ka, c1 + fr);
+            const double2 a2 = a_elem(X1, ldx1, r0 + fr, ka), b2 = b_elem(Y1, ka, c0 + fr);
+            const double2 a3 = a_elem(X1, ldx1, r1 + fr, ka), b3 = b_elem(Y1, ka, c1 + fr);
+            dmma_cplx(re[0], im[0], a0, b0);
+            dmma_cplx(re[1], im[1], a1, b1);
+            dmma_cplx(re[2], im[2], a2, b2);
+            dmma_cplx(re[3], im[3], a3, b3);
+            if (MODE == 2) {
+                // - Y X: A = -Y, B = X (X stored with leading dimension ld).
+                const double2 y0 = a_elem(Y0, ld, r0 + fr, ka), x0 = b_elem(X0, ka, c0 + fr);
+                const double2 y1 = a_elem(Y0, ld, r1 + fr, ka), x1 = b_elem(X0, ka, c1 + fr);
+                const double2 y2 = a_elem(Y1, ld, r0 + fr, ka), x2 = b_elem(X1, ka, c0 + fr);
+                const double2 y3 = a_elem(Y1, ld, r1 + fr, ka), x3 = b_elem(X1, ka, c1 + fr);
+                dmma_cplx(re[0], im[0], make_double2(-y0.x, -y0.y), x0);
+                dmma_cplx(re[1], im[1], make_double2(-y1.x, -y1.y), x1);
+                dmma_cplx(re[2], im[2], make_double2(-y2.x, -y2.y), x2);
+                dmma_cplx(re[3], im[3], make_double2(-y3.x, -y3.y), x3);
+            }
+        }
+        const int orow = fr, ocol = 2 * fk;
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            if (r0 + orow < nw && c0 + ocol + i < nw) {
+                out0[(r0 + orow) + ld * (c0 + ocol + i)] = make_double2(re[0][i], im[0][i]);
+                out1[(r0 + orow) + ld * (c0 + ocol + i)] = make_double2(re[2][i], im[2][i]);
+            }
+            if (t1 != t0 && r1 + orow < nw && c1 + ocol + i < nw) {
+                out0[(r1 + orow) + ld * (c1 + ocol + i)] = make_double2(re[1][i], im[1][i]);
+                out1[(r1 + orow) + ld * (c1 + ocol + i)] = make_double2(re[3][i], im[3][i]);
+            }
+        }
+    }
+}

@@ -276,6 +276,24 @@ WNLQG_D void rotate_to_hamiltonian(const double2 *__restrict__ src, C *T1, C *T2
     __syncthreads();
 }
 
+// dst0 = U^H X0 U and dst1 = U^H X1 U for two Wannier-gauge channels in global memory.  FP64: two
+// paired DMMA passes (X read straight from global memory into the fragments, four accumulator
+// tiles per warp; two barriers for both channels); dst0 and dst1 must not alias T1, T2 or U.
+// FP32: two single rotations.
+template <typename C>
+WNLQG_D void rotate_two_to_hamiltonian(const double2 *__restrict__ src0, const double2 *__restrict__ src1, C *T1,
+                                       C *T2, const C *U, C *dst0, C *dst1, int nw, int ld) {
+    if constexpr (same_type<C, double2>::value) {
+        dmma_product_pair<0>(src0, nw, U, T1, src1, nw, U, T2, nw, ld);
+        __syncthreads();
+        dmma_product_pair<1>(U, ld, T1, dst0, U, ld, T2, dst1, nw, ld);
+        __syncthreads();
+    } else {
+        rotate_to_hamiltonian(src0, T1, T2, U, dst0, nw, ld);
+        rotate_to_hamiltonian(src1, T1, T2, U, dst1, nw, ld);
+    }
+}
+
 // diag[n] = (U^H (X - Y) U)_nn for Wannier-gauge X and optional Y (nullptr: 0); uses T1, T2.
 template <typename C>
 WNLQG_D void rotate_diagonal(const double2 *__restrict__ src, C *T1, C *T2, const C *U, double2 *diag, int nw, int ld,
@@ -493,10 +511,19 @@ __global__ void __launch_bounds__(WIDE ? 512 : 256, WIDE ? 1 : (sizeof(R) == 8 ?
             }
             __syncthreads();
         } else {
-            for (int a = 0; a < 3; ++a)
-                if (p.slot_dH[a] >= 0) rotate_to_hamiltonian(xw + (int64_t)p.ch_dH[a] * nn, T1, T2, sU, slot(p.slot_dH[a]), nw, ld);
-            for (int a = 0; a < 3; ++a)
-                if (p.slot_A[a] >= 0) rotate_to_hamiltonian(xw + (int64_t)p.ch_A[a] * nn, T1, T2, sU, slot(p.slot_A[a]), nw, ld);
+            // The velocity and connection channels, two rotations per paired pass.
+            {
+                const double2 *src[6];
+                C *dst[6];
+                int nrot = 0;
+                for (int a = 0; a < 3; ++a)
+                    if (p.slot_dH[a] >= 0) { src[nrot] = xw + (int64_t)p.ch_dH[a] * nn; dst[nrot++] = slot(p.slot_dH[a]); }
+                for (int a = 0; a < 3; ++a)
+                    if (p.slot_A[a] >= 0) { src[nrot] = xw + (int64_t)p.ch_A[a] * nn; dst[nrot++] = slot(p.slot_A[a]); }
+                int r = 0;
+                for (; r + 1 < nrot; r += 2) rotate_two_to_hamiltonian(src[r], src[r + 1], T1, T2, sU, dst[r], dst[r + 1], nw, ld);
+                if (r < nrot) rotate_to_hamiltonian(src[r], T1, T2, sU, dst[r], nw, ld);
+            }
             // Gauge corrections D_d = -dH_d .* inv for the derivative axes of the generalised derivatives.
             for (int a = 0; a < 3; ++a)
                 if (p.slot_D[a] >= 0) {
@@ -513,15 +540,24 @@ __global__ void __launch_bounds__(WIDE ? 512 : 256, WIDE ? 1 : (sizeof(R) == 8 ?
             // l != n,m sums written as commutators (exact: D_nn = 0):
             //   sum_AD + AD_bit = [A_p, D_d]_nm + (A_d,nn - A_d,mm) D_p,nm
             //   sum_HD + DV_bit = [dH_p, D_d]_nm + (dH_d,nn - dH_d,mm) D_p,nm
+            // The pair-data region (transition energies, occupations, pair kernels: at least
+            // 32 nw^2 bytes) is unused until the pairs are built, so it holds the rotated ddH.
+            C *Hpd = reinterpret_cast<C *>(sm + L.te);
             for (int g = 0; g < p.n_g; ++g) {
                 const int pp = p.g_p[g], dd = p.g_d[g];
                 C *G = slot(p.g_slot[g]);
-                rotate_to_hamiltonian(xw + (int64_t)p.ch_dA[pp * 3 + dd] * nn, T1, T2, sU, G, nw, ld);
-                rotate_to_hamiltonian(xw + (int64_t)p.ch_ddH[pp * 3 + dd] * nn, T1, T2, sU, T1, nw, ld);
+                rotate_two_to_hamiltonian(xw + (int64_t)p.ch_dA[pp * 3 + dd] * nn, xw + (int64_t)p.ch_ddH[pp * 3 + dd] * nn,
+                                          T1, T2, sU, G, Hpd, nw, ld);
                 const C *Ap = slot(p.slot_A[pp]), *Ad = slot(p.slot_A[dd]);
                 const C *Hp = slot(p.slot_dH[pp]), *Hd = slot(p.slot_dH[dd]);
                 const C *Dd = slot(p.slot_D[dd]);
-                mm_comm(Ap, Dd, T2, nw, ld);
+                // T1 = [A_p, D_d], T2 = [dH_p, D_d] in one pass.
+                if constexpr (same_type<C, double2>::value) {
+                    dmma_product_pair<2>(Ap, ld, Dd, T1, Hp, ld, Dd, T2, nw, ld);
+                } else {
+                    mm_comm(Ap, Dd, T1, nw, ld);
+                    mm_comm(Hp, Dd, T2, nw, ld);
+                }
                 __syncthreads();
                 for (int e = threadIdx.x; e < nn; e += blockDim.x) {
                     const int n = e % nw, m = e / nw;
@@ -529,19 +565,11 @@ __global__ void __launch_bounds__(WIDE ? 512 : 256, WIDE ? 1 : (sizeof(R) == 8 ?
                     const C Dp = cscale(Hp[o], (R)(-sinv[e]));
                     const C dAd = csub(Ad[n + ld * n], Ad[m + ld * m]);
                     const C dHd = csub(Hd[n + ld * n], Hd[m + ld * m]);
-                    // G <- dA + (A_d,nn - A_d,mm)(D_p - i A_p) + [A_p, D_d]
-                    G[o] = cadd(cadd(G[o], cmul(dAd, csub(Dp, cmuli(Ap[o])))), T2[o]);
-                    // T1 <- ddH + (dH_d,nn - dH_d,mm) D_p
-                    T1[o] = cadd(T1[o], cmul(dHd, Dp));
-                }
-                __syncthreads();
-                mm_comm(Hp, Dd, T2, nw, ld);
-                __syncthreads();
-                for (int e = threadIdx.x; e < nn; e += blockDim.x) {
-                    const int n = e % nw, m = e / nw;
-                    const int o = n + ld * m;
-                    const C h = cadd(T1[o], T2[o]);
-                    G[o] = cadd(G[o], cmuli(cscale(h, (R)(-sinv[e]))));
+                    // G = dA + (A_d,nn - A_d,mm)(D_p - i A_p) + [A_p, D_d]
+                    //     + i (ddH + (dH_d,nn - dH_d,mm) D_p + [dH_p, D_d]) (-inv)
+                    const C h = cadd(cadd(Hpd[o], cmul(dHd, Dp)), T2[o]);
+                    G[o] = cadd(cadd(cadd(G[o], cmul(dAd, csub(Dp, cmuli(Ap[o])))), T1[o]),
+                                cmuli(cscale(h, (R)(-sinv[e]))));
                 }
                 __syncthreads();
             }
