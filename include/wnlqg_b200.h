@@ -57,9 +57,14 @@ typedef enum wnlqg_response_kind {
     WNLQG_BERRY_DIPOLE = 6,       /* D^{abc} Fermi surface over the mu axis, BerryMultipoleMoments.jl */
     WNLQG_SECOND_HARMONIC = 7,    /* seven-term chi/sigma^{abc}(omega; 2 omega), SecondHarmonicKernels.jl */
     WNLQG_JERK_CURRENT = 8,       /* ordered jerk (abcd)(omega), ConventionalJerkCurrent.jl */
-    WNLQG_LINEAR_TRANSPORT_BERRY = 9 /* Berry-curvature channel of the dc linear transport conductivity
+    WNLQG_LINEAR_TRANSPORT_BERRY = 9, /* Berry-curvature channel of the dc linear transport conductivity
                                         over the mu axis (any temperature), S m^2 per k-point before BZ
                                         weights and cell volume: LinearTransportKernels.jl:100-163 */
+    WNLQG_BERRY_DIPOLE_SEA = 10   /* D^{abc} Fermi sea over the mu axis: sum_n f(E_n) d_c Omega_n^{ab}
+                                     with the reference's default finite-difference geometry (central
+                                     difference of the band curvature at k +- h e_c, h =
+                                     finite_difference_step); BerryMultipoleGeometry.jl:67-161,
+                                     QuantumGeometryDerivatives.jl:193-228, BerryMultipoleDC.jl:56-62 */
 } wnlqg_response_kind;
 
 typedef enum wnlqg_broadening {
@@ -145,6 +150,11 @@ typedef struct wnlqg_task_desc {
     /* Interband rate gamma_inter in eV of WNLQG_LINEAR_TRANSPORT_BERRY (the reference's gamma_inter_ev,
        Config.jl:101; 0 = the clean limit). */
     double linear_transport_gamma_inter;
+    /* Cartesian step h in 1/Angstrom of WNLQG_BERRY_DIPOLE_SEA (the reference's finite_difference_step,
+       Config.jl:153, default 1e-4); the shifted points are k +- h e_c in fractional coordinates
+       (finite_difference_step_matrix, Core/Coordinates.jl:33-44).  Their spectra must pass the same
+       isolation check as the centre (degeneracy_threshold), reported on the centre's row. */
+    double finite_difference_step;
 } wnlqg_task_desc;
 
 typedef struct wnlqg_model wnlqg_model;   /* device-resident model */

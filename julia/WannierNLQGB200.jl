@@ -14,6 +14,7 @@ const BERRY_DIPOLE = Int32(6)
 const SECOND_HARMONIC = Int32(7)
 const JERK_CURRENT = Int32(8)
 const LINEAR_TRANSPORT_BERRY = Int32(9)
+const BERRY_DIPOLE_SEA = Int32(10)            # Fermi-sea D^{abc}, finite-difference geometry
 
 struct ModelDesc
     num_orbitals::Int64
@@ -58,6 +59,7 @@ struct TaskDesc
     wannier_center_convention::Int32           # 0: CONVENTION_II, 1: CONVENTION_I
     spectral_gap_tolerance::Float64            # cfg.spectral_gap_tolerance (reference default 1e-10)
     linear_transport_gamma_inter::Float64      # cfg.gamma_inter_ev of the linear transport Berry channel
+    finite_difference_step::Float64            # cfg.finite_difference_step (1/Angstrom, reference default 1e-4)
 end
 
 function check(status)

@@ -917,6 +917,7 @@ bool build_task(const wnlqg_task_desc *t, Task &task) {
             case WNLQG_INTRINSIC_AHC:
             case WNLQG_BERRY_DIPOLE:
             case WNLQG_LINEAR_TRANSPORT_BERRY:
+            case WNLQG_BERRY_DIPOLE_SEA:
                 task.need.F[a][b] = true; task.need.need_r(a); task.need.need_r(b);
                 if (q.kind == WNLQG_BERRY_DIPOLE) task.need.dH[cc] = true;
                 break;
@@ -953,7 +954,8 @@ bool build_task(const wnlqg_task_desc *t, Task &task) {
             }
             count += q.num_components * t->num_photon_energies * 14;
         }
-        else if (q.kind == WNLQG_INTRINSIC_AHC || q.kind == WNLQG_BERRY_DIPOLE || q.kind == WNLQG_LINEAR_TRANSPORT_BERRY) {
+        else if (q.kind == WNLQG_INTRINSIC_AHC || q.kind == WNLQG_BERRY_DIPOLE || q.kind == WNLQG_LINEAR_TRANSPORT_BERRY ||
+                 q.kind == WNLQG_BERRY_DIPOLE_SEA) {
             // intrinsic_hall_fermi_sea (IntrinsicHallOccupations.jl:15-16) is zero-temperature only.
             if (q.kind == WNLQG_INTRINSIC_AHC && t->temperature != 0.0) {
                 set_error("INTRINSIC_HALL_REQUIRES_ZERO_TEMPERATURE"); return false;
@@ -968,6 +970,9 @@ bool build_task(const wnlqg_task_desc *t, Task &task) {
                 }
             }
             if (t->num_fermi_energies < 1) { set_error("a Fermi-energy axis is required"); return false; }
+            if (q.kind == WNLQG_BERRY_DIPOLE_SEA && !(std::isfinite(t->finite_difference_step) && t->finite_difference_step > 0)) {
+                set_error("finite_difference_step must be finite and positive"); return false;
+            }
             if (q.kind == WNLQG_BERRY_DIPOLE && t->temperature == 0.0 && !(t->fermi_surface_broadening > 0)) {
                 set_error("T=0 requires positive eta_fs_ev"); return false;
             }
@@ -982,10 +987,10 @@ bool build_task(const wnlqg_task_desc *t, Task &task) {
     bool dipole = false, exact = false, blocks = false;
     for (int r = 0; r < t->num_responses; ++r) {
         const int kind = t->responses[r].kind;
-        dipole |= kind == WNLQG_BERRY_DIPOLE;
+        dipole |= kind == WNLQG_BERRY_DIPOLE || kind == WNLQG_BERRY_DIPOLE_SEA;
         exact |= t->denominator_regularization == 0.0 &&
                  (kind == WNLQG_SHIFT_CURRENT || kind == WNLQG_INJECTION_CURRENT || kind == WNLQG_BERRY_CURVATURE ||
-                  kind == WNLQG_QUANTUM_METRIC || kind == WNLQG_BERRY_DIPOLE);
+                  kind == WNLQG_QUANTUM_METRIC || kind == WNLQG_BERRY_DIPOLE || kind == WNLQG_BERRY_DIPOLE_SEA);
         blocks |= kind == WNLQG_LINEAR_TRANSPORT_BERRY;
     }
     if (dipole && !(std::isfinite(t->degeneracy_threshold) && t->degeneracy_threshold >= 0)) {
@@ -1402,6 +1407,60 @@ std::string point_values(const Model &m, const Task &task, const double k[3], cd
                             interband += 2 * factor * occ * gap * gap / (gap * gap + gamma * gamma) * qv.imag();
                         }
                     o[im + nmu * c] = cd(contact + interband, 0.0);
+                }
+            }
+            o += nmu * nc;
+        } else if (q.kind == WNLQG_BERRY_DIPOLE_SEA) {
+            // Fermi-sea dipole on the finite-difference geometry (prepare_berry_multipole_geometry!,
+            // BerryMultipoleGeometry.jl:67-161): per band n the central difference of the band
+            // curvature (berry_curvature_group_sum_component with the group {n},
+            // ConventionalQuantumGeometry.jl:530-557) at k +- delta_c, where delta_c is the
+            // fractional image lattice * (h e_c) / 2pi of the Cartesian step (finite_difference_step_matrix,
+            // Core/Coordinates.jl:15-44; berry_curvature_dipole_component!,
+            // QuantumGeometryDerivatives.jl:193-228).  Every shifted spectrum passes the centre's
+            // isolation check (isolation_threshold_ev = gap_tolerance, BerryMultipoleGeometry.jl:38-39).
+            // D[mu,a,b,c] = sum_n f(E_n; mu, T) d_c Omega_n^{ab} (berry_dipole_moments!,
+            // BerryMultipoleMoments.jl:7-47, with berry_multipole_sea_weight, BerryMultipoleDC.jl:56-62).
+            const int64_t nmu = t.num_fermi_energies;
+            const double h = t.finite_difference_step;
+            KData shifted[3][2];
+            bool have[3] = {false, false, false};
+            for (int c = 0; c < nc; ++c) {
+                const int cc = q.components[c][2];
+                if (have[cc]) continue;
+                have[cc] = true;
+                for (int sgn = 0; sgn < 2; ++sgn) {
+                    double ks[3];
+                    for (int i = 0; i < 3; ++i)
+                        ks[i] = k[i] + (sgn == 0 ? 1.0 : -1.0) * (m.lattice[i + 3 * cc] * h / (2.0 * PI));
+                    compute_kpoint(m, task.need, ks, t.denominator_regularization, shifted[cc][sgn]);
+                    if (task.iso_mode == 0) {
+                        std::string err = isolated_spectrum_error(shifted[cc][sgn].E, task.iso_tol);
+                        if (!err.empty()) return err;
+                    }
+                }
+            }
+            auto band_curvature = [&](const KData &s, int a, int b, int nu) {
+                double value = s.F[a][b](nu, nu).real();
+                for (int mm = 0; mm < n; ++mm) {
+                    if (mm == nu) continue;
+                    const cd qab = s.r[a](nu, mm) * s.r[b](mm, nu);
+                    const cd qba = s.r[b](nu, mm) * s.r[a](mm, nu);
+                    value += -(qab - qba).imag();
+                }
+                return value;
+            };
+            for (int c = 0; c < nc; ++c) {
+                const int a = q.components[c][0], b = q.components[c][1], cc = q.components[c][2];
+                std::vector<double> dO(n);
+                for (int nu = 0; nu < n; ++nu)
+                    dO[nu] = (band_curvature(shifted[cc][0], a, b, nu) - band_curvature(shifted[cc][1], a, b, nu)) /
+                             (2.0 * h);
+                for (int64_t im = 0; im < nmu; ++im) {
+                    double value = 0.0;
+                    for (int nu = 0; nu < n; ++nu)
+                        value += response_occupation(d.E[nu], t.fermi_energies[im], t.temperature) * dO[nu];
+                    o[im + nmu * c] = cd(value, 0.0);
                 }
             }
             o += nmu * nc;

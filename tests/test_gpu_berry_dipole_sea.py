@@ -1,0 +1,151 @@
+"""GPU parity of the Fermi-sea Berry-curvature dipole on the finite-difference geometry
+(BerryMultipoleGeometry.jl:67-161, QuantumGeometryDerivatives.jl:193-228): every entry point
+against the FP64 oracle, the integration-by-parts identity with the Fermi-surface form on the
+device, and the isolation check of the shifted spectra.
+
+The central difference divides the band-curvature difference by 2h = 2e-4 1/Angstrom, so rounding
+of the curvature (FP64: ~1e-13 relative) reaches the dipole amplified ~5000x: the FP64 bar is
+1e-8 of the largest value.  The mixed path carries its 4-slice Fourier and FP32 curvature error
+through the same amplification (measured below 2e-3 relative); its bar is 1e-2.
+"""
+import os
+import re
+import sys
+
+import numpy as np
+import pytest
+
+from wanniernlqg_b200 import _abi
+from wanniernlqg_b200.model import synthetic_orthogonal_model
+
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+from test_berry_dipole_sea import LATTICE, asymmetric_two_band_model, sea_task  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+RTOL = 1e-8
+MIXED_RTOL = 1e-2
+COMPS = ["xyz", "xzx", "yzy", "xyx", "zxx", "xyy"]
+
+
+@pytest.fixture(scope="module")
+def engine_cls():
+    from wanniernlqg_b200 import build
+    build.build()
+    from wanniernlqg_b200.engine import ResponseEngine
+    return ResponseEngine
+
+
+def rel_err(got, ref):
+    scale = np.max(np.abs(ref))
+    return np.max(np.abs(got - ref)) / (scale if scale > 0 else 1.0)
+
+
+def _models():
+    return {"two_band": asymmetric_two_band_model(),
+            "nw8_position": synthetic_orthogonal_model(8, 1, 5, full_position=True),
+            "nw32": synthetic_orthogonal_model(32, 1, 7)}
+
+
+@pytest.mark.parametrize("precision", [_abi.PRECISION_FP64, _abi.PRECISION_MIXED])
+@pytest.mark.parametrize("name", ["two_band", "nw8_position", "nw32"])
+def test_sea_dipole_points_match_oracle(engine_cls, oracle_mod, name, precision):
+    model = _models()[name]
+    k = np.random.default_rng(3).random((96, 3))
+    e = oracle_mod.kpoint_spectrum(model, k[0])[0]
+    mus = [float(np.median(e)), float(e.min()) - 1.0, float(e.max()) + 1.0]
+    task = sea_task(COMPS, mus, temperature=300.0, degeneracy_threshold=1e-7, denominator_regularization=1e-3,
+                    precision=precision)
+    ref = oracle_mod.point_values(model, task, k)
+    with engine_cls(model, task) as eng:
+        got = eng.point_values(k)
+    assert np.abs(got.imag).max() == 0.0
+    assert rel_err(got, ref) < (RTOL if precision == _abi.PRECISION_FP64 else MIXED_RTOL)
+
+
+@pytest.mark.parametrize("precision", [_abi.PRECISION_FP64, _abi.PRECISION_MIXED])
+def test_sea_dipole_mesh_and_weighted_sums_match_oracle(engine_cls, oracle_mod, precision):
+    """Mesh integral (staged centre Fourier, arbitrary-k stencil), a mesh index list and a weighted
+    point sum of the same points, together with the Fermi-surface dipole and the AHC in one task
+    (value offsets of mixed kinds)."""
+    model = synthetic_orthogonal_model(8, 1, 5, full_position=True)
+    mesh = (6, 5, 4)
+    mus = [-0.3, 0.0, 0.4]
+    task = _abi.TaskArrays([(_abi.INTRINSIC_AHC, ["xy"]), (_abi.BERRY_DIPOLE_SEA, COMPS),
+                            (_abi.BERRY_DIPOLE, ["xyz", "yzx"])], fermi_energies=mus, temperature=0.0,
+                           fermi_surface_broadening=0.05, degeneracy_threshold=1e-7, finite_difference_step=1e-4,
+                           precision=precision)
+    ref = oracle_mod.integrate_mesh(model, task, mesh)
+    n = int(np.prod(mesh))
+    idx = np.arange(n)
+    kp = np.stack([(idx % mesh[0]) / mesh[0], (idx // mesh[0]) % mesh[1] / mesh[1], idx // (mesh[0] * mesh[1]) / mesh[2]],
+                  axis=1)
+    tol = RTOL if precision == _abi.PRECISION_FP64 else MIXED_RTOL
+    with engine_cls(model, task) as eng:
+        got = eng.integrate_mesh(mesh)
+        assert rel_err(got, ref) < tol
+        perm = np.random.default_rng(1).permutation(n)
+        listed = eng.mesh_weighted_sum(mesh, perm, np.full(n, 1.0 / n))
+        assert rel_err(listed, ref) < tol
+        weighted = eng.weighted_sum(kp, np.full(n, 1.0 / n))
+        assert rel_err(weighted, ref) < tol
+
+
+def test_sea_dipole_equals_fermi_surface_form_on_device(engine_cls):
+    """Integration by parts over the zone, both forms on the GPU at T = 3000 K on a 48^3 mesh of
+    the gapped two-band model without inversion (the oracle's 32^3 agreement is 1e-7)."""
+    model = asymmetric_two_band_model()
+    mus = [-3.5, 3.0, 4.5]
+    sea = sea_task(COMPS, mus, temperature=3000.0)
+    fs = _abi.TaskArrays([(_abi.BERRY_DIPOLE, COMPS)], fermi_energies=mus, temperature=3000.0,
+                         degeneracy_threshold=1e-3, denominator_regularization=0.0)
+    with engine_cls(model, sea) as eng:
+        a = eng.integrate_mesh((48, 48, 48)).real
+    with engine_cls(model, fs) as eng:
+        b = eng.integrate_mesh((48, 48, 48)).real
+    assert np.abs(a - b).max() <= 1e-7 * np.abs(b).max()
+
+
+@pytest.mark.parametrize("precision", [_abi.PRECISION_FP64, _abi.PRECISION_MIXED])
+def test_sea_dipole_shifted_isolation_matches_oracle(engine_cls, oracle_mod, precision):
+    """The centre passes and a shifted spectrum fails: the engine reports the oracle's row, pair,
+    gap (the shifted spectrum's) and threshold; a centre failure in the same batch on an earlier
+    row takes precedence."""
+    from wanniernlqg_b200._lib import EngineError
+    model = asymmetric_two_band_model()
+    h = 1e-2
+    k = np.array([0.13, 0.31, 0.77])
+    delta = LATTICE[:, 0] * h / (2 * np.pi)
+    e0 = oracle_mod.kpoint_spectrum(model, k)[0]
+    gs = [np.diff(oracle_mod.kpoint_spectrum(model, k + s * delta)[0])[0] for s in (1, -1)]
+    failing = min(gs)
+    thr = 0.5 * (failing + min(e0[1] - e0[0], max(gs)))
+    rng = np.random.default_rng(9)
+    pts = rng.random((200, 3))
+    gaps = np.array([np.diff(oracle_mod.kpoint_spectrum(model, p)[0])[0] for p in pts])
+    pts = pts[gaps > thr + 0.05][:20]          # rows that pass at the centre and (by margin) shifted
+    pts[7] = k                                  # row 7 fails at k + delta only
+    task = sea_task(["yzx"], [0.0], h, degeneracy_threshold=thr, precision=precision)
+    with pytest.raises(RuntimeError) as oexc:
+        oracle_mod.point_values(model, task, pts)
+    pat = re.compile(r"bands=\(1,2\), gap_ev=(\S+), threshold_ev=(\S+) \(k-point row (\d+)\)")
+    ref = pat.search(str(oexc.value))
+    assert ref and int(ref.group(3)) == 7
+    with engine_cls(model, task) as eng:
+        with pytest.raises(EngineError) as gexc:
+            eng.point_values(pts)
+        got = pat.search(str(gexc.value))
+        assert got, str(gexc.value)
+        assert int(got.group(3)) == 7 and float(got.group(2)) == thr
+        assert float(got.group(1)) == pytest.approx(failing, rel=1e-9 if precision == _abi.PRECISION_FP64 else 1e-5)
+        # A centre failure on row 3 (a spectrum with a gap below the threshold) wins.
+        low = np.random.default_rng(2).random((400, 3))
+        lg = np.array([np.diff(oracle_mod.kpoint_spectrum(model, p)[0])[0] for p in low])
+        assert np.any(lg < thr - 0.05)
+        pts2 = pts.copy()
+        pts2[3] = low[np.argmax(lg < thr - 0.05)]
+        with pytest.raises(EngineError) as gexc2:
+            eng.point_values(pts2)
+        got2 = pat.search(str(gexc2.value))
+        c2 = np.diff(oracle_mod.kpoint_spectrum(model, pts2[3])[0])[0]
+        assert int(got2.group(3)) == 3
+        assert float(got2.group(1)) == pytest.approx(c2, rel=1e-9 if precision == _abi.PRECISION_FP64 else 1e-5)

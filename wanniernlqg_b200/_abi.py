@@ -27,6 +27,7 @@ BERRY_DIPOLE = 6
 SECOND_HARMONIC = 7
 JERK_CURRENT = 8
 LINEAR_TRANSPORT_BERRY = 9
+BERRY_DIPOLE_SEA = 10
 
 GAUSSIAN = 0
 LORENTZIAN = 1
@@ -39,7 +40,7 @@ MAX_COMPONENTS = 81
 
 # Kinds whose values carry the photon-energy axis.
 FREQUENCY_KINDS = (SHIFT_CURRENT, INJECTION_CURRENT, JERK_CURRENT)
-FERMI_AXIS_KINDS = (INTRINSIC_AHC, BERRY_DIPOLE, LINEAR_TRANSPORT_BERRY)
+FERMI_AXIS_KINDS = (INTRINSIC_AHC, BERRY_DIPOLE, LINEAR_TRANSPORT_BERRY, BERRY_DIPOLE_SEA)
 
 
 class ModelDesc(ctypes.Structure):
@@ -113,6 +114,7 @@ class TaskDesc(ctypes.Structure):
         ("wannier_center_convention", ctypes.c_int32),
         ("spectral_gap_tolerance", ctypes.c_double),
         ("linear_transport_gamma_inter", ctypes.c_double),
+        ("finite_difference_step", ctypes.c_double),
     ]
 
 
@@ -167,7 +169,7 @@ class TaskArrays:
                  fermi_surface_broadening=0.0, shg_low_frequency_broadening=0.025,
                  shg_intermediate_regularization=0.0, shg_eta_correction=True, band_window_size=-1,
                  band_selection=None, wannier_center_convention="II", spectral_gap_tolerance=1e-10,
-                 linear_transport_gamma_inter=0.0):
+                 linear_transport_gamma_inter=0.0, finite_difference_step=1e-4):
         if not 1 <= len(responses) <= MAX_RESPONSES:
             raise ValueError("between 1 and 8 responses are supported per task")
         self.photon_energies = np.ascontiguousarray(np.asarray(photon_energies, dtype=np.float64))
@@ -211,6 +213,7 @@ class TaskArrays:
         d.wannier_center_convention = 1 if wannier_center_convention == "I" else 0
         d.spectral_gap_tolerance = float(spectral_gap_tolerance)
         d.linear_transport_gamma_inter = float(linear_transport_gamma_inter)
+        d.finite_difference_step = float(finite_difference_step)
         # band_selection = (conduction bands, valence bands), 1-based as in the reference's
         # cfg.band_selection; pairs (n, m) with n valence and m conduction are kept.
         if band_selection is not None:

@@ -12,7 +12,10 @@
 // Energies come out of the eigensolvers in ascending order, so the smallest pair gap is the
 // smallest adjacent gap.  A failing point records (row << 24 | batch entry) with atomicMin, so
 // the smallest caller row wins; a one-thread kernel then stores, for that row, the first failing
-// pair in the reference's loop order (m ascending, then l ascending) and its gap.
+// pair in the reference's loop order (m ascending, then l ascending) and its gap.  One row can be
+// checked on several spectra (the centre and the shifted points of a finite-difference stencil):
+// each check carries a priority in the reference's order (0 = the centre) and the record keeps
+// the failing spectrum of the smallest priority.
 #pragma once
 
 #include <math_constants.h>
@@ -28,7 +31,8 @@ enum { ISO_ALL_PAIRS = 0, ISO_SPECTRAL_BLOCKS = 1 };
 struct IsoRecord {
     int l, m;       // 0-based bands of the first failing pair
     double gap;     // their energy difference (eV)
-    int64_t row;    // caller row (mesh index or point index) of the failing k-point
+    int64_t row;    // caller row (mesh index or point index) of the failing k-point; -1 = none
+    int prio;       // priority of the spectrum that failed (0 = the centre)
 };
 
 // First failing pair of one sorted spectrum in the reference's loop order; false when none fails.
@@ -84,20 +88,22 @@ __global__ void isolation_check_kernel(const double *__restrict__ E, int64_t nb,
 // so the record of an earlier batch is never overwritten by a later one).
 __global__ void isolation_record_kernel(const double *__restrict__ E, int64_t nb, int nw, double tol, int mode,
                                         int64_t row_base, const unsigned long long *__restrict__ key,
-                                        IsoRecord *__restrict__ rec) {
+                                        IsoRecord *__restrict__ rec, int prio) {
     const unsigned long long k = *key;
     if (k == ISO_NONE) return;
     const int64_t row = (int64_t)(k >> ISO_LOCAL_BITS);
     const int64_t i = (int64_t)(k & ((1ull << ISO_LOCAL_BITS) - 1));
     if (row < row_base || i >= nb) return;
+    if (rec->row == row && rec->prio <= prio) return;   // an earlier spectrum of this row failed
     const double *e = E + i * nw;
     int l = -1, m = -1;
     double gap = 0.0;
     bool nonfinite = false;
     for (int j = 0; j < nw; ++j) nonfinite |= !isfinite(e[j]);
-    if (!nonfinite) iso_first_failure(e, nw, tol, mode, l, m, gap);
+    if (!nonfinite && !iso_first_failure(e, nw, tol, mode, l, m, gap)) return;   // this spectrum passes
     rec->l = l;
     rec->m = m;
     rec->gap = nonfinite ? CUDART_NAN : gap;
     rec->row = row;
+    rec->prio = prio;
 }

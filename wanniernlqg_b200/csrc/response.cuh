@@ -26,7 +26,7 @@
 
 enum { RS_FC_SHIFT = 1, RS_FC_INJECTION = 2, RS_FC_JERK = 3 };
 enum { RS_SC_BERRY = 1, RS_SC_METRIC = 2 };
-enum { RS_MU_AHC = 1, RS_MU_DIPOLE = 2, RS_MU_LT = 3 };
+enum { RS_MU_AHC = 1, RS_MU_DIPOLE = 2, RS_MU_LT = 3, RS_MU_BANDCURV = 4 };
 #define RS_MAX_HESS 9
 #define RS_MU_CHUNK 8
 
@@ -64,6 +64,10 @@ struct RespParams {
     const double *mus;
     double temperature, fs_width;
     double lt_gamma, lt_factor;   // linear transport Berry channel: interband rate (eV), e^2/hbar 1e-20
+    // Band curvature items (RS_MU_BANDCURV, the shifted points of the finite-difference Fermi-sea
+    // dipole): Omega_n^{ab} of batch entry b goes to curv_out[b * curv_stride + mu_out * nw + n].
+    double *curv_out;
+    int64_t curv_stride;
     // Scalar components (Berry curvature, quantum metric).
     int n_sc;
     int sc_kind[RS_MAX_SCALAR], sc_a[RS_MAX_SCALAR], sc_b[RS_MAX_SCALAR];
@@ -634,7 +638,20 @@ __global__ void __launch_bounds__(WIDE ? 512 : 256, WIDE ? 1 : (sizeof(R) == 8 ?
                 sFd[2 * nw + n] = csub(csub(sFd[n], sFd[nw + n]), cmuli(comm));
             }
             __syncthreads();
-            if (p.mu_kind[s] == RS_MU_DIPOLE) {
+            if (p.mu_kind[s] == RS_MU_BANDCURV) {
+                // berry_curvature_group_sum_component with the group {n} (ConventionalQuantumGeometry.jl:
+                // 530-557): Re F_nn + sum_{m != n} -Im(r^a_nm r^b_mn - r^b_nm r^a_mn).
+                double *dst = p.curv_out + b * p.curv_stride + p.mu_out[s] * nw;
+                for (int n = threadIdx.x; n < nw; n += blockDim.x) {
+                    double om = 0.0;
+                    for (int m = 0; m < nw; ++m)
+                        if (m != n)
+                            om -= to_c64(csub(cmul(r_elem(a, n, m), r_elem(bb, m, n)),
+                                              cmul(r_elem(bb, n, m), r_elem(a, m, n)))).y;
+                    dst[n] = sFd[2 * nw + n].x + om;
+                }
+                __syncthreads();
+            } else if (p.mu_kind[s] == RS_MU_DIPOLE) {
                 // Band Berry curvature Omega_n = -2 sum_m Im(r^a_nm r^b_mn) + Re F_nn
                 // (berry_curvature_component, ConventionalQuantumGeometry.jl:166-180) into sFd[3nw..).
                 for (int n = threadIdx.x; n < nw; n += blockDim.x) {

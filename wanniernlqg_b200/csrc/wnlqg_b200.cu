@@ -28,6 +28,7 @@
 #include "nonorth.cuh"
 #include "order.cuh"
 #include "isolation.cuh"
+#include "fdsea.cuh"
 #include <cub/device/device_radix_sort.cuh>
 
 namespace {
@@ -74,6 +75,7 @@ struct Pass {
     int threads = 0;
     int grid = 0;
     int grid_wide = 0;   // grid of the 512-thread variant (FP64 orthogonal shared-memory passes), 0 = none
+    bool fd = false;     // band-curvature pass of the finite-difference stencil (shifted points only)
 };
 
 struct wnlqg_plan {
@@ -90,6 +92,15 @@ struct wnlqg_plan {
     double iso_tol = 0.0;
     unsigned long long *d_iso_key = nullptr;
     IsoRecord *d_iso_rec = nullptr;
+    // Fermi-sea Berry dipole on the finite-difference geometry (fdsea.cuh): the derivative axes in
+    // order of first use, their fractional steps, the (a, b) curvature pairs, the combine items,
+    // and per batch the shifted k-points and band curvatures [entry][2 nd][npair][nw].
+    int fd_nd = 0, fd_npair = 0;
+    int fd_axis[3] = {0, 0, 0};
+    int fd_pair[9][2];
+    double fd_delta[3][3];
+    double *d_fd_k = nullptr, *d_fd_curv = nullptr;
+    SeaParams sea;
     int ch_dH[3], ch_A[3], ch_ddH[9], ch_dA[9];
     int nw = 0, nr = 0, C = 0;
     int64_t nn = 0, vc = 0, max_batch = 0;
@@ -275,12 +286,18 @@ const void *response_fn(bool mixed, bool nonorth, bool global) {
 wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
     const wnlqg_task_desc &t = pl->task;
     struct Item { int kind; int a, b, c, d; int64_t out; };
+    // Band-curvature items of the finite-difference stencil: their own passes (shifted points only).
+    const int ITEM_BANDCURV = -1;
     std::vector<Item> items;
     int64_t off = 0;
     for (int r = 0; r < t.num_responses; ++r) {
         const wnlqg_response_request &q = t.responses[r];
         if (q.kind == WNLQG_SECOND_HARMONIC) {   // its own kernel (build_shg)
             off += (int64_t)q.num_components * t.num_photon_energies * 14;
+            continue;
+        }
+        if (q.kind == WNLQG_BERRY_DIPOLE_SEA) {   // sea_dipole_kernel (items set at plan creation)
+            off += (int64_t)q.num_components * t.num_fermi_energies;
             continue;
         }
         for (int c = 0; c < q.num_components; ++c) {
@@ -301,6 +318,7 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
         else
             off += q.num_components;
     }
+    for (int pr = 0; pr < pl->fd_npair; ++pr) items.push_back({ITEM_BANDCURV, pl->fd_pair[pr][0], pl->fd_pair[pr][1], 0, 0, pr});
     const double vol = lattice_det(pl->model->lattice);
     const double e3 = WNLQG_ELEMENTARY_CHARGE_C * WNLQG_ELEMENTARY_CHARGE_C * WNLQG_ELEMENTARY_CHARGE_C;
     const double P_sc = WNLQG_HBAR_EV_S * WNLQG_PI * (-e3) / (2.0 * WNLQG_HBAR_J_S * WNLQG_HBAR_J_S * vol);
@@ -363,8 +381,10 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
         };
         size_t start = i;
         bool pass_global = global_mode;   // a pass whose first component alone exceeds shared memory
+        const bool pass_fd = items[start].kind == ITEM_BANDCURV;
         while (i < items.size()) {
             const Item &it = items[i];
+            if ((it.kind == ITEM_BANDCURV) != pass_fd) break;   // stencil passes hold only curvature items
             // Tentatively add the item and check limits.
             bool tH[3], tA[3], tD[3];
             std::copy(needH, needH + 3, tH);
@@ -375,7 +395,7 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
             const bool freq = it.kind == WNLQG_SHIFT_CURRENT || it.kind == WNLQG_INJECTION_CURRENT ||
                               it.kind == WNLQG_JERK_CURRENT;
             const bool muaxis = it.kind == WNLQG_INTRINSIC_AHC || it.kind == WNLQG_BERRY_DIPOLE ||
-                                it.kind == WNLQG_LINEAR_TRANSPORT_BERRY;
+                                it.kind == WNLQG_LINEAR_TRANSPORT_BERRY || it.kind == ITEM_BANDCURV;
             const int mode = it.kind == WNLQG_JERK_CURRENT ? 1 : 0;
             if (freq && p.n_fc > 0 && p.pair_mode != mode) break;   // one pair family per pass
             if (it.kind == WNLQG_SHIFT_CURRENT) {
@@ -435,7 +455,8 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
             } else if (muaxis) {
                 int m = p.n_mu++;
                 p.mu_kind[m] = it.kind == WNLQG_INTRINSIC_AHC ? RS_MU_AHC
-                               : it.kind == WNLQG_BERRY_DIPOLE ? RS_MU_DIPOLE : RS_MU_LT;
+                               : it.kind == WNLQG_BERRY_DIPOLE ? RS_MU_DIPOLE
+                               : it.kind == ITEM_BANDCURV ? RS_MU_BANDCURV : RS_MU_LT;
                 p.mu_a[m] = it.a; p.mu_b[m] = it.b; p.mu_c[m] = it.c; p.mu_out[m] = it.out;
             } else {
                 int s = p.n_sc++;
@@ -479,8 +500,10 @@ wnlqg_status build_passes(wnlqg_plan *pl, int sm_count, size_t smem_limit) {
         p.degeneracy_threshold = t.degeneracy_threshold;
         p.vc = pl->vc;
         p.xw_stride = (int64_t)pl->C * pl->nn;
+        p.curv_stride = (int64_t)2 * pl->fd_nd * pl->fd_npair * pl->nw;
         ps.smem = RespSmem::layout(pl->nw, p.n_slots, p.n_fc, 1, csize).total;
         ps.global = pass_global;
+        ps.fd = pass_fd;
         ps.threads = response_threads(pl->nw);
         int per_sm = 0;
         const size_t launch_smem = pass_global ? 0 : ps.smem;
@@ -671,13 +694,13 @@ wnlqg_status tc_check(wnlqg_plan *pl) {
 
 // The isolation contract on one batch's energies (after the eigensolve): rows are row_base + the
 // batch entry, or row_base + perm[entry] for Morton-ordered batches.
-wnlqg_status run_isolation(wnlqg_plan *pl, int64_t nb, int64_t row_base, const int *perm) {
+wnlqg_status run_isolation(wnlqg_plan *pl, int64_t nb, int64_t row_base, const int *perm, int prio = 0) {
     if (pl->iso_mode < 0 || nb <= 0) return WNLQG_OK;
     isolation_check_kernel<<<(unsigned)((nb + 127) / 128), 128, 0, pl->stream>>>(pl->d_E, nb, pl->nw, pl->iso_tol,
                                                                                pl->iso_mode, row_base, perm,
                                                                                pl->d_iso_key);
     isolation_record_kernel<<<1, 1, 0, pl->stream>>>(pl->d_E, nb, pl->nw, pl->iso_tol, pl->iso_mode, row_base,
-                                                      pl->d_iso_key, pl->d_iso_rec);
+                                                      pl->d_iso_key, pl->d_iso_rec, prio);
     pl->launches += 2;
     WNLQG_CUDA(cudaGetLastError());
     return WNLQG_OK;
@@ -694,6 +717,7 @@ wnlqg_status iso_check(wnlqg_plan *pl) {
     IsoRecord rec;
     WNLQG_CUDA(cudaMemcpy(&rec, pl->d_iso_rec, sizeof(rec), cudaMemcpyDeviceToHost));
     WNLQG_CUDA(cudaMemset(pl->d_iso_key, 0xFF, sizeof(unsigned long long)));
+    WNLQG_CUDA(cudaMemset(pl->d_iso_rec, 0xFF, sizeof(IsoRecord)));
     char buf[256];
     const long long row = (long long)(key >> ISO_LOCAL_BITS);
     if (!std::isfinite(rec.gap))
@@ -972,6 +996,43 @@ wnlqg_status run_front(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const int64_
     return WNLQG_OK;
 }
 
+// One response-kernel pass over the current batch (curv_out: the stencil slot of band-curvature passes).
+wnlqg_status launch_pass(wnlqg_plan *pl, const Pass &ps, int64_t nb, int mode, double scale, int64_t point_offset,
+                         const double *weights, const int *out_perm, double *curv_out) {
+    RespParams p = ps.params;
+    if (pl->nonorth) {
+        p.ng_r = pl->d_ng_r;
+        p.ng_v = pl->d_ng_v;
+        p.ng_G = pl->d_ng_G;
+        p.ng_pairs = pl->ng.npairs;
+        for (int g = 0; g < p.n_g; ++g) p.g_ng[g] = pl->ng_gidx[p.g_p[g] * 3 + p.g_d[g]];
+    }
+    p.batch = nb;
+    p.xw = pl->d_xw;
+    p.E = pl->d_E;
+    p.U = pl->d_U;
+    p.mode = mode;
+    p.scale = scale;
+    p.weights = weights;
+    p.partials = pl->d_partials;
+    p.out_points = pl->d_points;
+    p.point_offset = point_offset;
+    p.out_perm = out_perm;
+    p.curv_out = curv_out;
+    p.gscratch = ps.global ? pl->d_resp_scratch : nullptr;
+    p.gscratch_stride = pl->resp_scratch_stride;
+    const size_t launch_smem = ps.global ? 0 : ps.smem;
+    void *args[] = {&p};
+    if (pl->resp_wide && ps.grid_wide > 0)
+        WNLQG_CUDA(cudaLaunchKernel(response_wide_fn(), dim3(ps.grid_wide), dim3(512), args, launch_smem, pl->stream));
+    else
+        WNLQG_CUDA(cudaLaunchKernel(response_fn(pl->task.precision == WNLQG_PRECISION_MIXED, pl->nonorth, ps.global),
+                                    dim3(ps.global && pl->resp_gw_grid > 0 ? pl->resp_gw_grid : ps.grid),
+                                    dim3(ps.threads), args, launch_smem, pl->stream));
+    pl->launches += 1;
+    return WNLQG_OK;
+}
+
 wnlqg_status run_passes(wnlqg_plan *pl, int64_t nb, int mode, double scale, int64_t point_offset,
                         const double *weights = nullptr, const int *out_perm = nullptr) {
     if (pl->nonorth && !pl->passes.empty()) {
@@ -983,36 +1044,26 @@ wnlqg_status run_passes(wnlqg_plan *pl, int64_t nb, int mode, double scale, int6
         nonorth_geometry_kernel<<<(unsigned)std::min<int64_t>(nb, pl->ng_grid), 256, 0, pl->stream>>>(q);
         pl->launches += 1;
     }
-    for (Pass &ps : pl->passes) {
-        RespParams p = ps.params;
-        if (pl->nonorth) {
-            p.ng_r = pl->d_ng_r;
-            p.ng_v = pl->d_ng_v;
-            p.ng_G = pl->d_ng_G;
-            p.ng_pairs = pl->ng.npairs;
-            for (int g = 0; g < p.n_g; ++g) p.g_ng[g] = pl->ng_gidx[p.g_p[g] * 3 + p.g_d[g]];
-        }
-        p.batch = nb;
-        p.xw = pl->d_xw;
-        p.E = pl->d_E;
-        p.U = pl->d_U;
-        p.mode = mode;
-        p.scale = scale;
-        p.weights = weights;
-        p.partials = pl->d_partials;
-        p.out_points = pl->d_points;
-        p.point_offset = point_offset;
-        p.out_perm = out_perm;
-        p.gscratch = ps.global ? pl->d_resp_scratch : nullptr;
-        p.gscratch_stride = pl->resp_scratch_stride;
-        const size_t launch_smem = ps.global ? 0 : ps.smem;
-        void *args[] = {&p};
-        if (pl->resp_wide && ps.grid_wide > 0)
-            WNLQG_CUDA(cudaLaunchKernel(response_wide_fn(), dim3(ps.grid_wide), dim3(512), args, launch_smem, pl->stream));
-        else
-            WNLQG_CUDA(cudaLaunchKernel(response_fn(pl->task.precision == WNLQG_PRECISION_MIXED, pl->nonorth, ps.global),
-                                        dim3(ps.global && pl->resp_gw_grid > 0 ? pl->resp_gw_grid : ps.grid),
-                                        dim3(ps.threads), args, launch_smem, pl->stream));
+    for (const Pass &ps : pl->passes) {
+        if (ps.fd) continue;
+        wnlqg_status st = launch_pass(pl, ps, nb, mode, scale, point_offset, weights, out_perm, nullptr);
+        if (st != WNLQG_OK) return st;
+    }
+    if (pl->fd_nd > 0 && nb > 0) {
+        // Fermi-sea dipole: centre occupations times the stencil's curvature differences.
+        SeaParams q = pl->sea;
+        q.batch = nb;
+        q.E = pl->d_E;
+        q.mus = pl->d_mus;
+        q.scale = scale;
+        q.weights = weights;
+        q.mode = mode;
+        q.partials = pl->d_partials;
+        q.out_points = pl->d_points;
+        q.point_offset = point_offset;
+        q.out_perm = out_perm;
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(nb, std::min(pl->sm_count, pl->partial_slots)));
+        sea_dipole_kernel<<<grid, 128, 0, pl->stream>>>(q);
         pl->launches += 1;
     }
     if (pl->metric_shg && !pl->shg.empty()) {
@@ -1049,6 +1100,38 @@ wnlqg_status run_passes(wnlqg_plan *pl, int64_t nb, int mode, double scale, int6
         else shg_kernel<false><<<pl->shg_grid, 256, pl->shg_smem, pl->stream>>>(p);
         pl->launches += 1;
     }
+    WNLQG_CUDA(cudaGetLastError());
+    return WNLQG_OK;
+}
+
+// The finite-difference stencil of the Fermi-sea Berry dipole for one batch (its k-points from
+// the same source as the centre's front): for each derivative axis j and sign, the shifted points
+// k +- delta_j go through the arbitrary-k front, the isolation contract (priority 1 + 2 j + sign,
+// after the centre's 0, the reference's order) and the band-curvature passes into stencil slot
+// 2 j + sign.  Runs before the centre's front, which then leaves the centre's energies in place.
+wnlqg_status run_fd_stencil(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const int64_t *mesh, const double *kpts_device,
+                            const int64_t *kidx_device, bool ordered, size_t ev_base, int64_t row_base, const int *perm) {
+    if (pl->fd_nd == 0 || nb <= 0) return WNLQG_OK;
+    // Shifted runs follow the centre's order: mesh runs and ordered batches warm-start the eigensolver.
+    const bool run = ordered || (mesh != nullptr && kpts_device == nullptr && kidx_device == nullptr);
+    const int64_t slot = (int64_t)pl->fd_npair * pl->nw;
+    for (int j = 0; j < pl->fd_nd; ++j)
+        for (int sgn = 0; sgn < 2; ++sgn) {
+            const double s = sgn == 0 ? 1.0 : -1.0;
+            const double *dl = pl->fd_delta[j];
+            fd_shift_kernel<<<(unsigned)((nb + 255) / 256), 256, 0, pl->stream>>>(
+                kpts_device, kidx_device, k_begin, mesh ? mesh[0] : 1, mesh ? mesh[1] : 1, mesh ? mesh[2] : 1, nb,
+                s * dl[0], s * dl[1], s * dl[2], pl->d_fd_k);
+            pl->launches += 1;
+            wnlqg_status st = run_front(pl, nb, 0, nullptr, pl->d_fd_k, ev_base, nullptr, run);
+            if (st != WNLQG_OK) return st;
+            if ((st = run_isolation(pl, nb, row_base, perm, 1 + 2 * j + sgn)) != WNLQG_OK) return st;
+            for (const Pass &ps : pl->passes) {
+                if (!ps.fd) continue;
+                if ((st = launch_pass(pl, ps, nb, 1, 1.0, 0, nullptr, nullptr, pl->d_fd_curv + (2 * j + sgn) * slot)) != WNLQG_OK)
+                    return st;
+            }
+        }
     WNLQG_CUDA(cudaGetLastError());
     return WNLQG_OK;
 }
@@ -1163,7 +1246,7 @@ wnlqg_status wnlqg_b200_plan_destroy(wnlqg_plan *pl) {
                       (void *)pl->d_ng_ws, (void *)pl->d_mshg_src, (void *)pl->d_mshg_diag, (void *)pl->d_mshg_ws,
                       (void *)pl->d_okeys, (void *)pl->d_operm, (void *)pl->d_ok, (void *)pl->d_ow, pl->d_osort_tmp,
                       (void *)pl->d_gC, (void *)pl->d_gL, (void *)pl->d_gred_scratch, (void *)pl->d_iso_key,
-                      (void *)pl->d_iso_rec})
+                      (void *)pl->d_iso_rec, (void *)pl->d_fd_k, (void *)pl->d_fd_curv})
         if (ptr) cudaFree(ptr);
     for (cudaEvent_t ev : pl->events) cudaEventDestroy(ev);
     if (pl->stream) cudaStreamDestroy(pl->stream);
@@ -1229,6 +1312,7 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
     pl->nw = model->nw;
     pl->nr = model->nr;
     pl->nn = (int64_t)pl->nw * pl->nw;
+    std::memset(&pl->sea, 0, sizeof(pl->sea));
     auto bail = [&](wnlqg_status st) { wnlqg_b200_plan_destroy(pl); return st; };
 
     // Channels required by the requested components.
@@ -1287,6 +1371,7 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
             case WNLQG_INTRINSIC_AHC:
             case WNLQG_BERRY_DIPOLE:
             case WNLQG_LINEAR_TRANSPORT_BERRY:
+            case WNLQG_BERRY_DIPOLE_SEA:
                 need_r(a); need_r(b);
                 pl->ch_dA[b * 3 + a] = add_channel(ch, CH_DA, b, a);
                 pl->ch_dA[a * 3 + b] = add_channel(ch, CH_DA, a, b);
@@ -1336,7 +1421,7 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
                 return bail(fail(WNLQG_ERR_INVALID_ARGUMENT, "SHG degeneracy_threshold must be finite and nonnegative in eV"));
             vc += (int64_t)q.num_components * t.num_photon_energies * 14;
         } else if (q.kind == WNLQG_INTRINSIC_AHC || q.kind == WNLQG_BERRY_DIPOLE ||
-                   q.kind == WNLQG_LINEAR_TRANSPORT_BERRY) {
+                   q.kind == WNLQG_LINEAR_TRANSPORT_BERRY || q.kind == WNLQG_BERRY_DIPOLE_SEA) {
             // intrinsic_hall_fermi_sea is zero-temperature only (IntrinsicHallOccupations.jl:15-16);
             // the finite-temperature Berry channel is the linear transport kind.
             if (q.kind == WNLQG_INTRINSIC_AHC && t.temperature != 0.0)
@@ -1356,6 +1441,29 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
                 return bail(fail(WNLQG_ERR_INVALID_ARGUMENT, "finite nonempty Fermi energy axis required"));
             if (q.kind == WNLQG_BERRY_DIPOLE && t.temperature == 0.0 && !(t.fermi_surface_broadening > 0))
                 return bail(fail(WNLQG_ERR_INVALID_ARGUMENT, "T=0 requires positive eta_fs_ev"));
+            if (q.kind == WNLQG_BERRY_DIPOLE_SEA) {
+                if (!(std::isfinite(t.finite_difference_step) && t.finite_difference_step > 0))
+                    return bail(fail(WNLQG_ERR_INVALID_ARGUMENT, "finite_difference_step must be finite and positive"));
+                // Derivative axes in order of first use and the distinct (a, b) curvature pairs.
+                for (int c = 0; c < q.num_components; ++c) {
+                    const int32_t *x = q.components[c];
+                    int j = 0, pr = 0;
+                    while (j < pl->fd_nd && pl->fd_axis[j] != x[2]) ++j;
+                    if (j == pl->fd_nd) pl->fd_axis[pl->fd_nd++] = x[2];
+                    while (pr < pl->fd_npair && !(pl->fd_pair[pr][0] == x[0] && pl->fd_pair[pr][1] == x[1])) ++pr;
+                    if (pr == pl->fd_npair) {
+                        pl->fd_pair[pr][0] = x[0];
+                        pl->fd_pair[pr][1] = x[1];
+                        ++pl->fd_npair;
+                    }
+                    if (pl->sea.n_items >= SEA_MAX_ITEMS)
+                        return bail(fail(WNLQG_ERR_UNSUPPORTED, "more than 96 Fermi-sea dipole components in one task"));
+                    const int it = pl->sea.n_items++;
+                    pl->sea.item_dir[it] = j;
+                    pl->sea.item_pair[it] = pr;
+                    pl->sea.item_out[it] = vc + (int64_t)c * t.num_fermi_energies;
+                }
+            }
             vc += (int64_t)q.num_components * t.num_fermi_energies;
         } else {
             vc += q.num_components;
@@ -1522,6 +1630,7 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
         int64_t per_k = (int64_t)pl->C * nn * 16 + (int64_t)nr * 16 + nn * 16 + nw * 8 + vc * 16;
         if (pl->metric_shg) per_k += MetricShgWs::src_entries(nw) * 16 + MetricShgWs::diag_entries(nw) * 8;
         if (pl->nonorth && t.precision == WNLQG_PRECISION_MIXED) per_k += 2 * nn * 16 + nn * 8;
+        per_k += (int64_t)2 * pl->fd_nd * pl->fd_npair * nw * 8 + (pl->fd_nd > 0 ? 24 : 0);
         // About 4 GiB of batch workspace (HBM is 180 GB): long runs of neighbouring k-points per
         // CTA for the warm-started eigensolver and few batches per call.
         max_batch = std::max<int64_t>(256, std::min<int64_t>(1 << 20, ((int64_t)1 << 32) / per_k));
@@ -1547,6 +1656,26 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
     if ((st = alloc((void **)&pl->d_weights, (size_t)max_batch * sizeof(double))) != WNLQG_OK) return bail(st);
     if ((st = alloc((void **)&pl->d_kidx, (size_t)max_batch * sizeof(int64_t))) != WNLQG_OK) return bail(st);
     if ((st = alloc((void **)&pl->d_status, (size_t)max_batch * sizeof(int))) != WNLQG_OK) return bail(st);
+    if (pl->fd_nd > 0) {
+        // Fractional image lattice * (h e_c) / 2 pi of each Cartesian step (finite_difference_step_matrix,
+        // Core/Coordinates.jl:33-44; lattice element (i, c) at i + 3 c).
+        for (int j = 0; j < pl->fd_nd; ++j)
+            for (int i = 0; i < 3; ++i)
+                pl->fd_delta[j][i] = model->lattice[i + 3 * pl->fd_axis[j]] * t.finite_difference_step / (2.0 * WNLQG_PI);
+        if ((st = alloc((void **)&pl->d_fd_k, (size_t)max_batch * 3 * sizeof(double))) != WNLQG_OK) return bail(st);
+        if ((st = alloc((void **)&pl->d_fd_curv, (size_t)max_batch * 2 * pl->fd_nd * pl->fd_npair * nw * sizeof(double))) !=
+            WNLQG_OK)
+            return bail(st);
+        SeaParams &q = pl->sea;
+        q.nw = nw;
+        q.curv = pl->d_fd_curv;
+        q.nd = pl->fd_nd;
+        q.npair = pl->fd_npair;
+        q.nmu = (int)t.num_fermi_energies;
+        q.temperature = t.temperature;
+        q.two_h = 2.0 * t.finite_difference_step;
+        q.vc = vc;
+    }
     {
         // Isolation contract: the Berry dipole needs every pair split by more than
         // degeneracy_threshold (BerryMultipoleGeometry.jl:81); eta = 0 geometry by more than
@@ -1555,10 +1684,10 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
         bool dipole = false, exact = false, blocks = false;
         for (int r = 0; r < t.num_responses; ++r) {
             const int kind = t.responses[r].kind;
-            dipole |= kind == WNLQG_BERRY_DIPOLE;
+            dipole |= kind == WNLQG_BERRY_DIPOLE || kind == WNLQG_BERRY_DIPOLE_SEA;
             exact |= t.denominator_regularization == 0.0 &&
                      (kind == WNLQG_SHIFT_CURRENT || kind == WNLQG_INJECTION_CURRENT || kind == WNLQG_BERRY_CURVATURE ||
-                      kind == WNLQG_QUANTUM_METRIC || kind == WNLQG_BERRY_DIPOLE);
+                      kind == WNLQG_QUANTUM_METRIC || kind == WNLQG_BERRY_DIPOLE || kind == WNLQG_BERRY_DIPOLE_SEA);
             blocks |= kind == WNLQG_LINEAR_TRANSPORT_BERRY;
         }
         if (dipole && !(std::isfinite(t.degeneracy_threshold) && t.degeneracy_threshold >= 0))
@@ -1576,6 +1705,7 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
             if ((st = alloc((void **)&pl->d_iso_key, sizeof(unsigned long long))) != WNLQG_OK) return bail(st);
             if ((st = alloc((void **)&pl->d_iso_rec, sizeof(IsoRecord))) != WNLQG_OK) return bail(st);
             WNLQG_CUDA(cudaMemset(pl->d_iso_key, 0xFF, sizeof(unsigned long long)));
+            WNLQG_CUDA(cudaMemset(pl->d_iso_rec, 0xFF, sizeof(IsoRecord)));   // row -1: no record
         }
     }
     if (pl->nonorth && vc > 0) {
@@ -1918,6 +2048,7 @@ wnlqg_status enqueue_mesh(wnlqg_plan *pl, const int64_t mesh[3], int64_t k_begin
         int64_t nb = std::min(pl->max_batch, k_end - s);
         size_t base = 1 + 3 * nbatch;
         if ((st = record_event(pl, base)) != WNLQG_OK) return st;
+        if ((st = run_fd_stencil(pl, nb, s, mesh, nullptr, nullptr, false, base, s, nullptr)) != WNLQG_OK) return st;
         if ((st = run_front(pl, nb, s, mesh, nullptr, base)) != WNLQG_OK) return st;
         if ((st = run_isolation(pl, nb, s, nullptr)) != WNLQG_OK) return st;
         if ((st = run_passes(pl, nb, 0, scale, 0)) != WNLQG_OK) return st;
@@ -1999,8 +2130,10 @@ wnlqg_status enqueue_points_weighted(wnlqg_plan *pl, const double *kpoints_devic
             kb = pl->d_ok;
             wb = pl->d_ow;
         }
+        const int *perm = ord ? pl->d_operm + pl->max_batch : nullptr;
+        if ((st = run_fd_stencil(pl, nb, 0, nullptr, kb, nullptr, ord, base, s, perm)) != WNLQG_OK) return st;
         if ((st = run_front(pl, nb, 0, nullptr, kb, base, nullptr, ord)) != WNLQG_OK) return st;
-        if ((st = run_isolation(pl, nb, s, ord ? pl->d_operm + pl->max_batch : nullptr)) != WNLQG_OK) return st;
+        if ((st = run_isolation(pl, nb, s, perm)) != WNLQG_OK) return st;
         if ((st = run_passes(pl, nb, 0, 1.0, 0, wb)) != WNLQG_OK) return st;
     }
     const size_t final_ev = 1 + 3 * nbatch;
@@ -2114,8 +2247,11 @@ wnlqg_status wnlqg_b200_eval_points(wnlqg_plan *pl, const double *kpoints, int64
                                    pl->stream));
         const bool ord = pl->order_points && nb > 1;
         if (ord && (st = order_batch(pl, pl->d_kpts, nullptr, nb)) != WNLQG_OK) return st;
+        const int *perm = ord ? pl->d_operm + pl->max_batch : nullptr;
+        if ((st = run_fd_stencil(pl, nb, 0, nullptr, ord ? pl->d_ok : pl->d_kpts, nullptr, ord, 1, s, perm)) != WNLQG_OK)
+            return st;
         if ((st = run_front(pl, nb, 0, nullptr, ord ? pl->d_ok : pl->d_kpts, 1, nullptr, ord)) != WNLQG_OK) return st;
-        if ((st = run_isolation(pl, nb, s, ord ? pl->d_operm + pl->max_batch : nullptr)) != WNLQG_OK) return st;
+        if ((st = run_isolation(pl, nb, s, perm)) != WNLQG_OK) return st;
         if ((st = run_passes(pl, nb, 1, 1.0, 0, nullptr, ord ? pl->d_operm + pl->max_batch : nullptr)) != WNLQG_OK)
             return st;
         WNLQG_CUDA(cudaMemcpyAsync(out + 2 * s * pl->vc, pl->d_points, (size_t)nb * pl->vc * sizeof(double2),
@@ -2148,8 +2284,11 @@ wnlqg_status wnlqg_b200_eval_points_weighted(wnlqg_plan *pl, const double *kpoin
                                    pl->stream));
         const bool ord = pl->order_points && nb > 1;
         if (ord && (st = order_batch(pl, pl->d_kpts, pl->d_weights, nb)) != WNLQG_OK) return st;
+        const int *perm = ord ? pl->d_operm + pl->max_batch : nullptr;
+        if ((st = run_fd_stencil(pl, nb, 0, nullptr, ord ? pl->d_ok : pl->d_kpts, nullptr, ord, 1, s, perm)) != WNLQG_OK)
+            return st;
         if ((st = run_front(pl, nb, 0, nullptr, ord ? pl->d_ok : pl->d_kpts, 1, nullptr, ord)) != WNLQG_OK) return st;
-        if ((st = run_isolation(pl, nb, s, ord ? pl->d_operm + pl->max_batch : nullptr)) != WNLQG_OK) return st;
+        if ((st = run_isolation(pl, nb, s, perm)) != WNLQG_OK) return st;
         if ((st = run_passes(pl, nb, 0, 1.0, 0, ord ? pl->d_ow : pl->d_weights)) != WNLQG_OK) return st;
     }
     reduce_partials_kernel<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((pl->vc + 255) / 256, 1024)), 256, 0,
@@ -2187,10 +2326,12 @@ wnlqg_status wnlqg_b200_eval_mesh_weighted(wnlqg_plan *pl, const int64_t mesh[3]
                                    pl->stream));
         if (contiguous) {
             // A run of consecutive mesh indices takes the staged mesh contraction.
+            if ((st = run_fd_stencil(pl, nb, indices[s], mesh, nullptr, nullptr, false, 1, s, nullptr)) != WNLQG_OK) return st;
             if ((st = run_front(pl, nb, indices[s], mesh, nullptr, 1)) != WNLQG_OK) return st;
         } else {
             WNLQG_CUDA(cudaMemcpyAsync(pl->d_kidx, indices + s, (size_t)nb * sizeof(int64_t), cudaMemcpyHostToDevice,
                                        pl->stream));
+            if ((st = run_fd_stencil(pl, nb, 0, mesh, nullptr, pl->d_kidx, false, 1, s, nullptr)) != WNLQG_OK) return st;
             if ((st = run_front(pl, nb, 0, mesh, nullptr, 1, pl->d_kidx)) != WNLQG_OK) return st;
         }
         if ((st = run_isolation(pl, nb, s, nullptr)) != WNLQG_OK) return st;
