@@ -63,3 +63,93 @@ def test_two_rank_gloo_sharding_is_bitwise_identical(tmp_path, oracle_mod):
     single = oracle_mod.integrate_mesh(model, _task(), mesh, threads=1)
     assert np.array_equal(r0, r1)
     assert np.array_equal(r0, single)
+
+
+# ---- adaptive integration over ranks (integrate_response_mpi, ResponseIntegration.jl:200-387) ----
+
+def _adaptive_setup():
+    from wanniernlqg_b200 import integration
+    model = reference_workload_model("nw4")
+    task = _abi.TaskArrays([(_abi.BERRY_CURVATURE, ["xy"]), (_abi.QUANTUM_METRIC, ["xx"])])
+    domain = integration.IntegrationDomain((0.0, 0.0, 0.0), (1.0, 1.0, 1.0))
+    algorithm = integration.HAdaptiveCubature(atol=0.0, rtol=2e-3, max_evaluations=1500)
+    return model, task, domain, algorithm
+
+
+def _adaptive_worker(rank, world, port, mode, out_path):
+    import pickle
+    import torch.distributed as dist
+    from oracle import oracle
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    model, task, domain, algorithm = _adaptive_setup()
+    evaluated = []
+
+    def evaluator(nodes):
+        evaluated.append(len(nodes))
+        if mode == "fail" and rank == 1 and np.any(nodes[:, 0] > 0.6):
+            raise ValueError("planted failure")
+        return oracle.point_values(model, task, nodes, threads=1)
+
+    if mode == "contract" and rank == 1:
+        from wanniernlqg_b200 import integration
+        algorithm = integration.HAdaptiveCubature(atol=0.0, rtol=1e-3, max_evaluations=1500)
+    try:
+        res = parallel.distributed_integrate_response(evaluator, domain, algorithm, batched=(mode == "batched"))
+        outcome = {"value": res.value, "evaluations": res.evaluations, "estimate": res.embedded_estimate,
+                   "local_nodes": int(sum(evaluated))}
+    except Exception as exc:   # noqa: BLE001 - recorded for the test
+        outcome = {"error": f"{type(exc).__name__}: {exc}", "local_nodes": int(sum(evaluated))}
+    with open(out_path + f".{rank}.pkl", "wb") as fh:
+        pickle.dump(outcome, fh)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def _run_adaptive(tmp_path, world, mode):
+    import pickle
+    import torch.multiprocessing as mp
+    out = str(tmp_path / f"adaptive_{mode}_{world}")
+    mp.start_processes(_adaptive_worker, args=(world, _free_port(), mode, out), nprocs=world, start_method="spawn",
+                       join=True)
+    res = []
+    for r in range(world):
+        with open(out + f".{r}.pkl", "rb") as fh:
+            res.append(pickle.load(fh))
+    return res
+
+
+@pytest.mark.parametrize("world,mode", [(2, "serial"), (3, "serial"), (2, "batched")])
+def test_adaptive_over_ranks_is_bitwise_the_single_rank_run(tmp_path, oracle_mod, world, mode):
+    """Rank 0's controller sees the one-rank values in the one-rank order: value, estimate and
+    evaluation count are identical to the single-process run, on every rank, and the rule nodes
+    are shared out round-robin (every rank evaluates about 1/world of them)."""
+    from wanniernlqg_b200 import integration
+    model, task, domain, algorithm = _adaptive_setup()
+    ev = lambda nodes: oracle_mod.point_values(model, task, nodes, threads=1)   # noqa: E731
+    if mode == "batched":
+        single = integration.integrate_response_batched(ev, domain, algorithm)
+    else:
+        single = integration.integrate_response(None, domain, algorithm, batch_evaluator=ev)
+    res = _run_adaptive(tmp_path, world, mode)
+    for r in res:
+        assert "error" not in r, r
+        assert np.array_equal(r["value"], single.value)
+        assert r["evaluations"] == single.evaluations and r["estimate"] == single.embedded_estimate
+    shares = [r["local_nodes"] for r in res]
+    assert sum(shares) == single.evaluations
+    assert max(shares) - min(shares) <= len(res) * 40   # one rule (33 nodes) of imbalance per packet at most
+
+
+def test_adaptive_over_ranks_reports_evaluator_failure_everywhere(tmp_path, oracle_mod):
+    res = _run_adaptive(tmp_path, 2, "fail")
+    for r in res:
+        assert "error" in r and "rank 1: ValueError: planted failure" in r["error"], r
+
+
+def test_adaptive_over_ranks_refuses_different_contracts(tmp_path, oracle_mod):
+    res = _run_adaptive(tmp_path, 2, "contract")
+    for r in res:
+        assert "error" in r and "different global contracts" in r["error"], r
+        assert r["local_nodes"] == 0
