@@ -149,3 +149,21 @@ def test_sea_dipole_shifted_isolation_matches_oracle(engine_cls, oracle_mod, pre
         c2 = np.diff(oracle_mod.kpoint_spectrum(model, pts2[3])[0])[0]
         assert int(got2.group(3)) == 3
         assert float(got2.group(1)) == pytest.approx(c2, rel=1e-9 if precision == _abi.PRECISION_FP64 else 1e-5)
+
+
+@pytest.mark.parametrize("precision", [_abi.PRECISION_FP64, _abi.PRECISION_MIXED])
+def test_dirac_dipole_known_answer_on_device(engine_cls, precision):
+    """The reference's tilted-Dirac Fermi-surface dipole (test/berry_multipole_dirac_unit.jl) through
+    the engine's weighted point sum: within the oracle's 2e-6 of the ellipse answer on both meshes
+    (the reference's own bar is 2e-4), the error against the width-free answer shrinking."""
+    from test_dirac_dipole_known_answer import (CASES, MU, angular_dipole, dipole_task, dirac_lattice_model,
+                                                gaussian_reference, region_points)
+    model = dirac_lattice_model()
+    errors = []
+    for mesh, width in CASES:
+        k, w = region_points(mesh)
+        with engine_cls(model, dipole_task(width, precision=precision)) as eng:
+            got = float(eng.weighted_sum(k, np.full(len(k), w))[0].real)
+        assert got == pytest.approx(gaussian_reference(width), rel=2e-6 if precision == _abi.PRECISION_FP64 else 1e-4)
+        errors.append(abs(got - angular_dipole(MU)))
+    assert errors[1] < 0.4 * errors[0]
