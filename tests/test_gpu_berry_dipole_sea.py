@@ -5,8 +5,9 @@ device, and the isolation check of the shifted spectra.
 
 The central difference divides the band-curvature difference by 2h = 2e-4 1/Angstrom, so rounding
 of the curvature (FP64: ~1e-13 relative) reaches the dipole amplified ~5000x: the FP64 bar is
-1e-8 of the largest value.  The mixed path carries its 4-slice Fourier and FP32 curvature error
-through the same amplification (measured below 2e-3 relative); its bar is 1e-2.
+1e-8 of the largest value (measured 2.5e-11 to 2.2e-10 on the three point sets).  The mixed path
+carries its 4-slice Fourier and FP32 curvature error through the same amplification (measured
+2.6e-4 to 2.1e-3); its bar is 1e-2.
 """
 import os
 import re
