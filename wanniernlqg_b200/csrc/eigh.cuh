@@ -746,8 +746,9 @@ __global__ void __launch_bounds__(TEAM == 128 ? 128 : 64, TEAM == 32 ? 1 : 6) ei
 //   stage 2 (eigh_refine_f64_cta_kernel): W = second-order Loewdin orthonormalisation of V
 //     (E = W^H W - I, W <- W (I - E/2 + 3E^2/8)), H' = W^H H W, FP64 Jacobi sweeps (mixed path:
 //     one, unless H' is diagonal to 1e-13 ||H||; FP64 path: until the FP64 CTA Jacobi's stopping
-//     rule holds, np 2^-60 ||H||), U = W J, ascending order and canonical phases.  The products
-//     run on the FP64 tensor cores (dmma_product).
+//     rule holds, np 2^-60 ||H||, from the second sweep on replaced by the first-order completion
+//     when its bound holds), U = W J, ascending order and canonical phases.  The products run on
+//     the FP64 tensor cores (dmma_product).
 // GW: the working set lives in global memory (gscratch, one stride per CTA) when it does not fit
 // shared memory.
 // ---------------------------------------------------------------------------------------------
@@ -875,6 +876,51 @@ struct RefineCtaSmem {
     }
 };
 
+// The CTA form of team_first_order_completion (the same bound and algebra, the product on the
+// FP64 tensor cores): on success W <- W (I + E) (Wc and Tc swap roles) and A's diagonal holds the
+// second-order eigenvalues.  dnew: np doubles of shared scratch.
+WNLQG_D bool cta_first_order_completion(double2 *A, double2 *&Wc, double2 *&Tc, int np, int ld, double *dnew) {
+    const int tid = threadIdx.x;
+    const double tau = 1.4901161193847656e-08;   // 2^-26
+    int bad = 0;
+    for (int e = tid; e < np * np; e += blockDim.x) {
+        const int i = e % np, j = e / np;
+        const double2 a = A[i + ld * j];
+        if (i == j || (a.x == 0.0 && a.y == 0.0)) continue;
+        if (!(hypot(a.x, a.y) <= tau * fabs(A[j + ld * j].x - A[i + ld * i].x))) bad = 1;
+    }
+    if (__syncthreads_or(bad)) return false;
+    for (int j = tid; j < np; j += blockDim.x) {
+        const double dj = A[j + ld * j].x;
+        double s = 0.0;
+        for (int i = 0; i < np; ++i) {
+            const double2 a = A[i + ld * j];
+            if (i == j || (a.x == 0.0 && a.y == 0.0)) continue;
+            s += (a.x * a.x + a.y * a.y) / (dj - A[i + ld * i].x);
+        }
+        dnew[j] = dj + s;
+    }
+    __syncthreads();
+    for (int e = tid; e < np * np; e += blockDim.x) {
+        const int i = e % np, j = e / np;
+        const double2 a = A[i + ld * j];
+        if (i == j || (a.x == 0.0 && a.y == 0.0)) continue;
+        const double g = A[j + ld * j].x - A[i + ld * i].x;
+        A[i + ld * j] = make_double2(a.x / g, a.y / g);
+    }
+    __syncthreads();
+    for (int i = tid; i < np; i += blockDim.x) A[i + ld * i] = make_double2(1.0, 0.0);
+    __syncthreads();
+    dmma_product<0>(Wc, A, Tc, np, ld);                      // T = W (I + E)
+    __syncthreads();
+    double2 *x = Wc;
+    Wc = Tc;
+    Tc = x;
+    for (int i = tid; i < np; i += blockDim.x) A[i + ld * i] = make_double2(dnew[i], 0.0);
+    __syncthreads();
+    return true;
+}
+
 template <bool GW>
 __global__ void __launch_bounds__(512, 1) eigh_refine_f64_cta_kernel(const double2 *__restrict__ h_in, int64_t h_stride,
                                                                    const float2 *__restrict__ V_in, int64_t batch, int nw,
@@ -956,6 +1002,8 @@ __global__ void __launch_bounds__(512, 1) eigh_refine_f64_cta_kernel(const doubl
         for (int sweep = 0; sweep < (converge ? WNLQG_JACOBI_MAX_SWEEPS : 1); ++sweep) {
             const double off = offdiag_norm(A, np, ld, red);
             if (off <= (converge ? tol * np : fro * 1.0e-13)) break;
+            if (converge && sweep > 0 && cta_first_order_completion(A, Wc, Tc, np, ld, reinterpret_cast<double *>(rot_s)))
+                break;
             if (tid == 0) rot_flag = 0;
             __syncthreads();
             jacobi_sweep<double>(A, Wc, np, ld, tol, rot_s, rot_c, rot_p, rot_q, &rot_flag);
