@@ -155,6 +155,12 @@ typedef struct wnlqg_task_desc {
        (finite_difference_step_matrix, Core/Coordinates.jl:33-44).  Their spectra must pass the same
        isolation check as the centre (degeneracy_threshold), reported on the centre's row. */
     double finite_difference_step;
+    /* Geometry backend of WNLQG_BERRY_DIPOLE_SEA (the reference's derivative_backend, Config.jl:113):
+       0 = finite differences (the default; finite_difference_step), 1 = analytic, the six-partition
+       contraction of the band derivatives at the centre only (orthogonal_bcd_partition_matrices!,
+       Responses/QuantumGeometry/OrthogonalGeometryDerivatives.jl:24-102, with the band derivatives of
+       MatrixElements/Interpolated/OrthogonalBandDerivatives.jl:123-245). */
+    int32_t derivative_backend;
 } wnlqg_task_desc;
 
 typedef struct wnlqg_model wnlqg_model;   /* device-resident model */

@@ -60,6 +60,7 @@ struct TaskDesc
     spectral_gap_tolerance::Float64            # cfg.spectral_gap_tolerance (reference default 1e-10)
     linear_transport_gamma_inter::Float64      # cfg.gamma_inter_ev of the linear transport Berry channel
     finite_difference_step::Float64            # cfg.finite_difference_step (1/Angstrom, reference default 1e-4)
+    derivative_backend::Int32                  # cfg.derivative_backend: 0 :finite_difference, 1 :analytic
 end
 
 function check(status)

@@ -90,6 +90,7 @@ struct Needs {
     bool ddH[3][3] = {};
     bool A[3] = {false, false, false};
     bool dA[3][3] = {};   // [position][derivative]
+    bool ddA[3][3][3] = {};   // [position][derivative][derivative]: d_c d_g A_p
     bool F[3][3] = {};
     bool shg = false;     // second harmonic generation (metric models: the source jets below)
     int convention = 0;   // 0: Convention II, 1: Convention I
@@ -105,6 +106,7 @@ struct KData {
     std::vector<double> E;
     Mat U, Uadj;
     Mat dH[3], ddH[3][3], Aint[3], dA[3][3], F[3][3], inv, D[3], r[3];
+    Mat ddA[3][3][3];   // U' (d_c d_g A_p) U where requested
     // Nonorthogonal models: r = Berry connection, dH diagonal = Hellmann-Feynman slopes and the
     // metric generalized derivatives G[p][d] (position p, derivative d) replace gder.
     bool nonorth = false;
@@ -325,6 +327,11 @@ void compute_kpoint(const Model &m, const Needs &need, const double k[3], double
     for (int a = 0; a < 3; ++a)
         for (int b = 0; b < 3; ++b)
             needdAw[a][b] = need.dA[a][b] || need.F[a][b] || need.F[b][a];
+    Mat ddAw[3][3][3];
+    for (int p = 0; p < 3; ++p)
+        for (int c = 0; c < 3; ++c)
+            for (int g = 0; g < 3; ++g)
+                if (need.ddA[p][c][g]) ddAw[p][c][g].init(n);
     for (int a = 0; a < 3; ++a) {
         if (need.dH[a]) dHw[a].init(n);
         if (needAw[a]) Aw[a].init(n);
@@ -372,6 +379,11 @@ void compute_kpoint(const Model &m, const Needs &need, const double k[3], double
                 for (int b = 0; b < 3; ++b)
                     if (needdAw[a][b])
                         for (size_t e = 0; e < nn; ++e) dAw[a][b].v[e] += fr * (I1 * disp(rc, b, e) * pos(e));
+                for (int c = 0; c < 3; ++c)
+                    for (int g = 0; g < 3; ++g)
+                        if (need.ddA[a][c][g])
+                            for (size_t e = 0; e < nn; ++e)
+                                ddAw[a][c][g].v[e] += fr * (-disp(rc, c, e) * disp(rc, g, e) * pos(e));
             }
         }
     }
@@ -389,7 +401,11 @@ void compute_kpoint(const Model &m, const Needs &need, const double k[3], double
         for (int a = 0; a < 3; ++a) {
             sim(dHw[a]);
             sim(Aw[a]);
-            for (int b = 0; b < 3; ++b) { sim(ddHw[a][b]); sim(dAw[a][b]); }
+            for (int b = 0; b < 3; ++b) {
+                sim(ddHw[a][b]);
+                sim(dAw[a][b]);
+                for (int g = 0; g < 3; ++g) sim(ddAw[a][b][g]);
+            }
         }
     }
     std::vector<double> ev;
@@ -405,6 +421,8 @@ void compute_kpoint(const Model &m, const Needs &need, const double k[3], double
         for (int b = 0; b < 3; ++b) {
             if (need.ddH[a][b]) rotate(d, ddHw[a][b], d.ddH[a][b]);
             if (need.dA[a][b]) rotate(d, dAw[a][b], d.dA[a][b]);
+            for (int g = 0; g < 3; ++g)
+                if (need.ddA[a][b][g]) rotate(d, ddAw[a][b][g], d.ddA[a][b][g]);
         }
     }
     // Wannier curvature F_ab = dA_b/dk_a - dA_a/dk_b - i[A_a, A_b], then U'FU
@@ -919,6 +937,17 @@ bool build_task(const wnlqg_task_desc *t, Task &task) {
             case WNLQG_LINEAR_TRANSPORT_BERRY:
             case WNLQG_BERRY_DIPOLE_SEA:
                 task.need.F[a][b] = true; task.need.need_r(a); task.need.need_r(b);
+                if (q.kind == WNLQG_BERRY_DIPOLE_SEA && t->derivative_backend == 1) {
+                    // Jets of orthogonal_bcd_partition_matrices! (OrthogonalGeometryDerivatives.jl:24-102)
+                    // and of the band derivatives D_a, D_c, D_ac, D_bc (OrthogonalBandDerivatives.jl:123-245).
+                    task.need.need_r(cc);
+                    task.need.ddH[a][cc] = task.need.ddH[cc][a] = true;
+                    task.need.ddH[b][cc] = task.need.ddH[cc][b] = true;
+                    task.need.dA[a][cc] = task.need.dA[b][cc] = true;
+                    task.need.dA[b][a] = task.need.dA[a][b] = true;
+                    task.need.dA[cc][a] = task.need.dA[cc][b] = true;
+                    task.need.ddA[b][a][cc] = task.need.ddA[a][b][cc] = true;
+                }
                 if (q.kind == WNLQG_BERRY_DIPOLE) task.need.dH[cc] = true;
                 break;
             case WNLQG_SECOND_HARMONIC:
@@ -970,7 +999,11 @@ bool build_task(const wnlqg_task_desc *t, Task &task) {
                 }
             }
             if (t->num_fermi_energies < 1) { set_error("a Fermi-energy axis is required"); return false; }
-            if (q.kind == WNLQG_BERRY_DIPOLE_SEA && !(std::isfinite(t->finite_difference_step) && t->finite_difference_step > 0)) {
+            if (q.kind == WNLQG_BERRY_DIPOLE_SEA && t->derivative_backend != 0 && t->derivative_backend != 1) {
+                set_error("derivative_backend must be 0 (finite difference) or 1 (analytic)"); return false;
+            }
+            if (q.kind == WNLQG_BERRY_DIPOLE_SEA && t->derivative_backend == 0 &&
+                !(std::isfinite(t->finite_difference_step) && t->finite_difference_step > 0)) {
                 set_error("finite_difference_step must be finite and positive"); return false;
             }
             if (q.kind == WNLQG_BERRY_DIPOLE && t->temperature == 0.0 && !(t->fermi_surface_broadening > 0)) {
@@ -1273,6 +1306,136 @@ void shg_response(int n, const double *E, const cd *V, const cd *A, const cd *dA
     }
 }
 
+// ---- analytic local Berry-curvature dipole (derivative_backend = :analytic) ----------------------
+
+Mat mat_mul(const Mat &X, const Mat &Y) {
+    const int n = X.n;
+    Mat out;
+    out.init(n);
+    for (int j = 0; j < n; ++j)
+        for (int l = 0; l < n; ++l) {
+            const cd y = Y(l, j);
+            for (int i = 0; i < n; ++i) out(i, j) += X(i, l) * y;
+        }
+    return out;
+}
+
+// D_a = U' d_a U (orthogonal_band_first_derivative!, MatrixElements/Interpolated/
+// OrthogonalBandDerivatives.jl:123-141): dH_nm / (E_m - E_n) off the diagonal, i A_nn on it.
+Mat band_first_derivative(const KData &d, int a) {
+    const int n = d.nw;
+    Mat D;
+    D.init(n);
+    for (int m = 0; m < n; ++m)
+        for (int i = 0; i < n; ++i)
+            D(i, m) = i == m ? I1 * d.Aint[a](i, i) : d.dH[a](i, m) * (1.0 / (d.E[m] - d.E[i]));
+    return D;
+}
+
+// D_ag = U' d_a d_g U (orthogonal_band_second_derivative!, OrthogonalBandDerivatives.jl:183-245).
+Mat band_second_derivative(const KData &d, const Mat &Da, const Mat &Dg, int a, int g) {
+    const int n = d.nw;
+    Mat T = mat_mul(d.dH[a], Dg), S = mat_mul(d.dH[g], Da);
+    for (size_t e = 0; e < T.v.size(); ++e) T.v[e] += S.v[e];
+    const Mat &Aa = d.Aint[a], &Ag = d.Aint[g];
+    const Mat &dAag = d.dA[a][g], &dAga = d.dA[g][a];   // d_g A_a and d_a A_g
+    Mat out;
+    out.init(n);
+    for (int m = 0; m < n; ++m)
+        for (int i = 0; i < n; ++i) {
+            if (i != m) {
+                const double delta = d.E[m] - d.E[i];
+                cd num = d.ddH[a][g](i, m) + T(i, m);
+                num -= d.dH[a](m, m).real() * Dg(i, m) + d.dH[g](m, m).real() * Da(i, m);
+                out(i, m) = num * (1.0 / delta);
+            } else {
+                cd cag(0.0, 0.0), cga(0.0, 0.0), dd(0.0, 0.0);
+                for (int l = 0; l < n; ++l) {
+                    cag += Dg(i, l) * Aa(l, i);
+                    cag -= Aa(i, l) * Dg(l, i);
+                    cga += Da(i, l) * Ag(l, i);
+                    cga -= Ag(i, l) * Da(l, i);
+                }
+                for (int l = 0; l < n; ++l) {
+                    dd += Dg(i, l) * Da(l, i);
+                    dd += Da(i, l) * Dg(l, i);
+                }
+                const double jet = 0.5 * (dAag(i, i) - cag + dAga(i, i) - cga).real();
+                out(i, i) = cd(0.5 * dd.real(), jet);
+            }
+        }
+    return out;
+}
+
+// Per band the total of the six partitions of orthogonal_bcd_partition_matrices! (omega derivative,
+// second derivative, first derivative, omega transport, mixed products, pure D) at their diagonal
+// (orthogonal_geometry_partition_diagonal), Responses/QuantumGeometry/OrthogonalGeometryDerivatives.jl:
+// 24-113, for the component (alpha, beta, gamma): d_gamma Omega_n^{alpha beta}.
+std::vector<double> analytic_local_dipole(const KData &d, int al, int be, int ga) {
+    const int n = d.nw;
+    const Mat &Aa = d.Aint[al], &Ab = d.Aint[be];
+    const Mat &Aag = d.dA[al][ga], &Abg = d.dA[be][ga];
+    Mat Om, Omg;
+    Om.init(n);
+    Omg.init(n);
+    for (size_t e = 0; e < Om.v.size(); ++e) {
+        Om.v[e] = d.dA[be][al].v[e] - d.dA[al][be].v[e];
+        Omg.v[e] = d.ddA[be][al][ga].v[e] - d.ddA[al][be][ga].v[e];
+    }
+    const Mat Da = band_first_derivative(d, al), Db = band_first_derivative(d, be), Dg = band_first_derivative(d, ga);
+    const Mat Dag = band_second_derivative(d, Da, Dg, al, ga), Dbg = band_second_derivative(d, Db, Dg, be, ga);
+    auto M = mat_mul;
+    std::vector<Mat> parts;
+    parts.push_back(Omg);   // omega_derivative
+    {
+        std::vector<std::pair<double, Mat>> t = {
+            {-1, M(M(Dg, Db), Aa)}, {1, M(Dbg, Aa)}, {-1, M(M(Db, Dg), Aa)}, {-1, M(Aag, Db)},
+            {1, M(M(Dg, Da), Ab)}, {-1, M(Dag, Ab)}, {1, M(M(Da, Dg), Ab)}, {1, M(Abg, Da)}};
+        Mat s;
+        s.init(n);
+        for (auto &x : t)
+            for (size_t e = 0; e < s.v.size(); ++e) s.v[e] += x.first * x.second.v[e];
+        parts.push_back(s);   // second_derivative
+    }
+    {
+        Mat s;
+        s.init(n);
+        const Mat t1 = M(Db, Aag), t2 = M(Aa, Dbg), t3 = M(Da, Abg), t4 = M(Ab, Dag);
+        for (size_t e = 0; e < s.v.size(); ++e) s.v[e] = t1.v[e] - t2.v[e] - t3.v[e] + t4.v[e];
+        parts.push_back(s);   // first_derivative
+    }
+    {
+        Mat s;
+        s.init(n);
+        const Mat t1 = M(Dg, Om), t2 = M(Om, Dg);
+        for (size_t e = 0; e < s.v.size(); ++e) s.v[e] = -t1.v[e] + t2.v[e];
+        parts.push_back(s);   // omega_transport
+    }
+    {
+        Mat s;
+        s.init(n);
+        const Mat t1 = M(M(Dg, Aa), Db), t2 = M(M(Dg, Ab), Da), t3 = M(M(Db, Aa), Dg), t4 = M(M(Da, Ab), Dg);
+        for (size_t e = 0; e < s.v.size(); ++e) s.v[e] = t1.v[e] - t2.v[e] + t3.v[e] - t4.v[e];
+        parts.push_back(s);   // mixed_products
+    }
+    {
+        Mat s;
+        s.init(n);
+        const Mat t1 = M(Da, Dbg), t2 = M(Dag, Db), t3 = M(M(Dg, Da), Db), t4 = M(M(Da, Dg), Db), t5 = M(Db, Dag),
+                  t6 = M(Dbg, Da), t7 = M(M(Dg, Db), Da), t8 = M(M(Db, Dg), Da);
+        for (size_t e = 0; e < s.v.size(); ++e)
+            s.v[e] = I1 * (-t1.v[e] - t2.v[e] + t3.v[e] + t4.v[e] + t5.v[e] + t6.v[e] - t7.v[e] - t8.v[e]);
+        parts.push_back(s);   // pure_D
+    }
+    std::vector<double> out(n);
+    for (int i = 0; i < n; ++i) {
+        double total = 0.0;
+        for (const Mat &p : parts) total += p(i, i).real();
+        out[i] = total;
+    }
+    return out;
+}
+
 // One k-point's concatenated response values (point_value!, IntegralDriver.jl:596-...), with
 // num_kpoints = 1 in every prefactor (the 1/Nk scale is applied by the lane consumer).
 std::string point_values(const Model &m, const Task &task, const double k[3], cd *out) {
@@ -1422,6 +1585,22 @@ std::string point_values(const Model &m, const Task &task, const double k[3], cd
             // D[mu,a,b,c] = sum_n f(E_n; mu, T) d_c Omega_n^{ab} (berry_dipole_moments!,
             // BerryMultipoleMoments.jl:7-47, with berry_multipole_sea_weight, BerryMultipoleDC.jl:56-62).
             const int64_t nmu = t.num_fermi_energies;
+            if (t.derivative_backend == 1) {
+                for (int c = 0; c < nc; ++c) {
+                    const int a = q.components[c][0], b = q.components[c][1], cc = q.components[c][2];
+                    const std::vector<double> ld = analytic_local_dipole(d, a, b, cc);
+                    for (double v : ld)
+                        if (!std::isfinite(v)) return "nonfinite consumed BCD/BCQ geometry";
+                    for (int64_t im = 0; im < nmu; ++im) {
+                        double value = 0.0;
+                        for (int nu = 0; nu < n; ++nu)
+                            value += response_occupation(d.E[nu], t.fermi_energies[im], t.temperature) * ld[nu];
+                        o[im + nmu * c] = cd(value, 0.0);
+                    }
+                }
+                o += nmu * nc;
+                continue;
+            }
             const double h = t.finite_difference_step;
             KData shifted[3][2];
             bool have[3] = {false, false, false};

@@ -38,14 +38,15 @@ def test_struct_sizes_match_c():
 #include <stddef.h>
 #include "wnlqg_b200.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(wnlqg_model_desc), sizeof(wnlqg_response_request),
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(wnlqg_model_desc), sizeof(wnlqg_response_request),
          sizeof(wnlqg_task_desc), offsetof(wnlqg_task_desc, fermi_energy), offsetof(wnlqg_task_desc, precision),
          offsetof(wnlqg_task_desc, fermi_surface_broadening), offsetof(wnlqg_task_desc, wannier_center_convention),
          sizeof(wnlqg_autotune_report), offsetof(wnlqg_autotune_report, response_ms),
          offsetof(wnlqg_autotune_report, warm_start), offsetof(wnlqg_autotune_report, start_ms),
          offsetof(wnlqg_autotune_report, width_ms), offsetof(wnlqg_autotune_report, shg_grid_ms),
          offsetof(wnlqg_autotune_report, eigh_grid_ms), offsetof(wnlqg_task_desc, spectral_gap_tolerance),
-         offsetof(wnlqg_task_desc, linear_transport_gamma_inter), offsetof(wnlqg_task_desc, finite_difference_step));
+         offsetof(wnlqg_task_desc, linear_transport_gamma_inter), offsetof(wnlqg_task_desc, finite_difference_step),
+         offsetof(wnlqg_task_desc, derivative_backend));
   return 0;
 }
 '''
@@ -62,5 +63,6 @@ int main(void) {
            _abi.AutotuneReport.warm_start.offset, _abi.AutotuneReport.start_ms.offset,
            _abi.AutotuneReport.width_ms.offset, _abi.AutotuneReport.shg_grid_ms.offset,
            _abi.AutotuneReport.eigh_grid_ms.offset, _abi.TaskDesc.spectral_gap_tolerance.offset,
-           _abi.TaskDesc.linear_transport_gamma_inter.offset, _abi.TaskDesc.finite_difference_step.offset]
+           _abi.TaskDesc.linear_transport_gamma_inter.offset, _abi.TaskDesc.finite_difference_step.offset,
+           _abi.TaskDesc.derivative_backend.offset]
     assert [int(x) for x in out] == got

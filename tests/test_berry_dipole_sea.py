@@ -174,3 +174,75 @@ def test_sea_dipole_argument_errors(oracle_mod):
         oracle_mod.point_values(model, sea_task(["xyz"], []), k)
     task = sea_task(["xyz", "yzx"], [0.0, 1.0, 2.0])
     assert oracle_mod.point_values(model, task, k).shape == (1, 6)
+
+
+# ---- the analytic geometry backend (derivative_backend = :analytic) ---------------------------
+
+def test_analytic_sea_dipole_is_the_limit_of_the_finite_differences(oracle_mod):
+    """The six-partition contraction of the band derivatives (OrthogonalGeometryDerivatives.jl:
+    24-113) against the central differences of the band curvature: the gap closes as h^2 (a factor
+    4 per halving of h), so both restatements compute d_c Omega_n (a model with a full position
+    operator, Convention II)."""
+    from wanniernlqg_b200.model import synthetic_orthogonal_model
+    model = synthetic_orthogonal_model(6, 1, 3, full_position=True)
+    k = np.random.default_rng(5).random((6, 3))
+    e = oracle_mod.kpoint_spectrum(model, k[0])[0]
+    comps = ["xyz", "xzx", "yzy", "xyx", "zxy", "yxx", "xxy", "zzx"]
+    kw = dict(fermi_energies=[float(np.median(e)), 50.0], temperature=300.0, degeneracy_threshold=1e-6,
+              denominator_regularization=0.0)
+    an = oracle_mod.point_values(model, _abi.TaskArrays([(_abi.BERRY_DIPOLE_SEA, comps)], derivative_backend="analytic",
+                                                        **kw), k)
+    errs = []
+    for h in (4e-4, 2e-4, 1e-4):
+        fd = oracle_mod.point_values(model, _abi.TaskArrays([(_abi.BERRY_DIPOLE_SEA, comps)], finite_difference_step=h,
+                                                            **kw), k)
+        errs.append(np.abs(an - fd).max() / np.abs(an).max())
+    assert errs[-1] < 5e-7
+    for e0, e1 in zip(errs, errs[1:]):
+        assert 3.5 < e0 / e1 < 4.5, errs
+    # mu above every band: sum_n Omega_n^{ab} = Tr F^{ab} = d_a Tr A_b - d_b Tr A_a (the pair terms
+    # cancel, the commutator is traceless), so the moment is d_c of that: a direct Fourier sum of the
+    # traces of the position blocks.
+    rc = model.lattice.T @ model.r_vectors            # Cartesian R, [3, NR]
+    tr = np.einsum("iiar->ar", model.position_r)       # Tr A_R,a, [3, NR]
+    for kk, vals in zip(k, an.reshape(len(k), len(comps), 2)[:, :, 1]):
+        ph = np.exp(2j * np.pi * (model.r_vectors.T @ kk)) / model.r_degeneracies
+        for comp, v in zip(comps, vals):
+            a, b, c = ["xyz".index(x) for x in comp]
+            ref = np.sum(ph * (-rc[a] * rc[c] * tr[b] + rc[b] * rc[c] * tr[a])).real
+            assert v.real == pytest.approx(ref, rel=1e-9, abs=1e-11 * np.abs(an).max())
+
+
+@pytest.mark.parametrize("kfrac", [(0.11, 0.23, 0.37), (0.41, 0.07, 0.83)])
+def test_analytic_sea_dipole_two_band_closed_form(oracle_mod, kfrac):
+    """mu between the bands: d_c Omega_- of the closed form, differentiated by an eighth-order
+    stencil, on the non-cubic lattice."""
+    mass = 1.3
+    model = scaled_two_band_model(mass)
+    s = np.diag(LATTICE)
+    kf = np.array(kfrac)
+    comps = ["xyz", "xzx", "yzy", "xyx", "zxy", "yxx"]
+    task = _abi.TaskArrays([(_abi.BERRY_DIPOLE_SEA, comps)], fermi_energies=[0.0], degeneracy_threshold=1e-3,
+                           denominator_regularization=0.0, derivative_backend="analytic")
+    got = oracle_mod.point_values(model, task, kf[None])[0].real
+    fd8 = ((1, 4 / 5), (2, -1 / 5), (3, 4 / 105), (4, -1 / 280))
+    for i, comp in enumerate(comps):
+        a, b, c = ["xyz".index(x) for x in comp]
+        theta = 2 * np.pi * kf
+        d = 0.0
+        for j, w in fd8:
+            tp, tm = theta.copy(), theta.copy()
+            tp[c] += j * 1e-3
+            tm[c] -= j * 1e-3
+            d += w * (lower_band_curvature(tp, mass, a, b) - lower_band_curvature(tm, mass, a, b)) / 1e-3
+        assert got[i] == pytest.approx(s[a] * s[b] * s[c] * d, rel=1e-9, abs=1e-12)
+
+
+def test_derivative_backend_must_be_known(oracle_mod):
+    model = asymmetric_two_band_model()
+    task = _abi.TaskArrays([(_abi.BERRY_DIPOLE_SEA, ["xyz"])], fermi_energies=[0.0])
+    task.desc.derivative_backend = 2
+    with pytest.raises(RuntimeError, match="derivative_backend must be 0"):
+        oracle_mod.point_values(model, task, np.array([[0.1, 0.2, 0.3]]))
+    with pytest.raises(ValueError):
+        _abi.TaskArrays([(_abi.BERRY_DIPOLE_SEA, ["xyz"])], fermi_energies=[0.0], derivative_backend="spectral")

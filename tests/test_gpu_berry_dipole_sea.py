@@ -168,3 +168,57 @@ def test_dirac_dipole_known_answer_on_device(engine_cls, precision):
         assert got == pytest.approx(gaussian_reference(width), rel=2e-6 if precision == _abi.PRECISION_FP64 else 1e-4)
         errors.append(abs(got - angular_dipole(MU)))
     assert errors[1] < 0.4 * errors[0]
+
+
+ANALYTIC_RTOL = 1e-9
+ANALYTIC_MIXED_RTOL = 1e-3
+
+
+@pytest.mark.parametrize("precision", [_abi.PRECISION_FP64, _abi.PRECISION_MIXED])
+@pytest.mark.parametrize("name", ["two_band", "nw8_position", "nw32"])
+def test_analytic_sea_dipole_points_match_oracle(engine_cls, oracle_mod, name, precision):
+    """The analytic geometry (bcd_analytic_kernel, FP64 on both paths; the mixed path's centre
+    spectrum carries its own precision) against the oracle's six-partition restatement."""
+    model = _models()[name]
+    k = np.random.default_rng(4).random((64, 3))
+    e = oracle_mod.kpoint_spectrum(model, k[0])[0]
+    mus = [float(np.median(e)), float(e.min()) - 1.0, float(e.max()) + 1.0]
+    task = sea_task(COMPS, mus, temperature=300.0, degeneracy_threshold=1e-7, denominator_regularization=1e-3,
+                    precision=precision, derivative_backend="analytic")
+    ref = oracle_mod.point_values(model, task, k)
+    with engine_cls(model, task) as eng:
+        got = eng.point_values(k)
+    assert np.abs(got.imag).max() == 0.0
+    assert rel_err(got, ref) < (ANALYTIC_RTOL if precision == _abi.PRECISION_FP64 else ANALYTIC_MIXED_RTOL)
+
+
+def test_analytic_sea_dipole_sums_match_oracle_and_finite_differences(engine_cls, oracle_mod):
+    """Mesh integral, mesh index list and weighted point sum of the analytic backend in a task with
+    the AHC and the Fermi-surface dipole, against the oracle; and the device's two backends agree
+    to the central difference's O(h^2).  Bare denominators: the finite-difference backend
+    differentiates the regularized curvature (the reference's compute_kpoint! with
+    denominator_regularization), the analytic one the bare band derivatives, which differ by
+    O(eta^2 / gap^2) (1e-4 at the default 1e-3 eV on this model)."""
+    model = synthetic_orthogonal_model(8, 1, 5, full_position=True)
+    mesh = (6, 5, 4)
+    n = int(np.prod(mesh))
+    mus = [-0.3, 0.0, 0.4]
+
+    def task(backend):
+        return _abi.TaskArrays([(_abi.INTRINSIC_AHC, ["xy"]), (_abi.BERRY_DIPOLE_SEA, COMPS),
+                                (_abi.BERRY_DIPOLE, ["xyz", "yzx"])], fermi_energies=mus, temperature=0.0,
+                               fermi_surface_broadening=0.05, degeneracy_threshold=1e-7, finite_difference_step=1e-4,
+                               denominator_regularization=0.0, derivative_backend=backend)
+    ref = oracle_mod.integrate_mesh(model, task("analytic"), mesh)
+    idx = np.arange(n)
+    kp = np.stack([(idx % mesh[0]) / mesh[0], (idx // mesh[0]) % mesh[1] / mesh[1], idx // (mesh[0] * mesh[1]) / mesh[2]],
+                  axis=1)
+    with engine_cls(model, task("analytic")) as eng:
+        got = eng.integrate_mesh(mesh)
+        assert rel_err(got, ref) < ANALYTIC_RTOL
+        perm = np.random.default_rng(1).permutation(n)
+        assert rel_err(eng.mesh_weighted_sum(mesh, perm, np.full(n, 1.0 / n)), ref) < ANALYTIC_RTOL
+        assert rel_err(eng.weighted_sum(kp, np.full(n, 1.0 / n)), ref) < ANALYTIC_RTOL
+    with engine_cls(model, task("finite_difference")) as eng:
+        fd = eng.integrate_mesh(mesh)
+    assert rel_err(fd, got) < 1e-6

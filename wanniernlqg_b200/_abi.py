@@ -115,6 +115,7 @@ class TaskDesc(ctypes.Structure):
         ("spectral_gap_tolerance", ctypes.c_double),
         ("linear_transport_gamma_inter", ctypes.c_double),
         ("finite_difference_step", ctypes.c_double),
+        ("derivative_backend", ctypes.c_int32),
     ]
 
 
@@ -169,7 +170,8 @@ class TaskArrays:
                  fermi_surface_broadening=0.0, shg_low_frequency_broadening=0.025,
                  shg_intermediate_regularization=0.0, shg_eta_correction=True, band_window_size=-1,
                  band_selection=None, wannier_center_convention="II", spectral_gap_tolerance=1e-10,
-                 linear_transport_gamma_inter=0.0, finite_difference_step=1e-4):
+                 linear_transport_gamma_inter=0.0, finite_difference_step=1e-4,
+                 derivative_backend="finite_difference"):
         if not 1 <= len(responses) <= MAX_RESPONSES:
             raise ValueError("between 1 and 8 responses are supported per task")
         self.photon_energies = np.ascontiguousarray(np.asarray(photon_energies, dtype=np.float64))
@@ -214,6 +216,9 @@ class TaskArrays:
         d.spectral_gap_tolerance = float(spectral_gap_tolerance)
         d.linear_transport_gamma_inter = float(linear_transport_gamma_inter)
         d.finite_difference_step = float(finite_difference_step)
+        if derivative_backend not in ("finite_difference", "analytic"):
+            raise ValueError("derivative_backend must be 'finite_difference' or 'analytic'")
+        d.derivative_backend = 1 if derivative_backend == "analytic" else 0
         # band_selection = (conduction bands, valence bands), 1-based as in the reference's
         # cfg.band_selection; pairs (n, m) with n valence and m conduction are kept.
         if band_selection is not None:

@@ -29,6 +29,7 @@
 #include "order.cuh"
 #include "isolation.cuh"
 #include "fdsea.cuh"
+#include "bcd_analytic.cuh"
 #include <cub/device/device_radix_sort.cuh>
 
 namespace {
@@ -48,7 +49,8 @@ wnlqg_status fail(wnlqg_status st, const std::string &msg) {
                         std::string(#call) + ": " + cudaGetErrorString(err_));                            \
     } while (0)
 
-enum ChannelOp { CH_H = 0, CH_DH = 1, CH_DDH = 2, CH_A = 3, CH_DA = 4, CH_S = 5, CH_DS = 6, CH_DDS = 7 };
+// CH_DDA: d_c d_g A_p with d = 3 min(c, g) + max(c, g).
+enum ChannelOp { CH_H = 0, CH_DH = 1, CH_DDH = 2, CH_A = 3, CH_DA = 4, CH_S = 5, CH_DS = 6, CH_DDS = 7, CH_DDA = 8 };
 
 struct Channel {
     int op;
@@ -101,6 +103,11 @@ struct wnlqg_plan {
     double fd_delta[3][3];
     double *d_fd_k = nullptr, *d_fd_curv = nullptr;
     SeaParams sea;
+    // Fermi-sea Berry dipole on the analytic geometry (bcd_analytic.cuh): items, channels, grid and
+    // the per-CTA global working sets.
+    BcdaParams bcda;
+    int bcda_grid = 0;
+    unsigned char *d_bcda_scratch = nullptr;
     int ch_dH[3], ch_A[3], ch_ddH[9], ch_dA[9];
     int nw = 0, nr = 0, C = 0;
     int64_t nn = 0, vc = 0, max_batch = 0;
@@ -1066,6 +1073,24 @@ wnlqg_status run_passes(wnlqg_plan *pl, int64_t nb, int mode, double scale, int6
         sea_dipole_kernel<<<grid, 128, 0, pl->stream>>>(q);
         pl->launches += 1;
     }
+    if (pl->bcda.n_items > 0 && nb > 0) {
+        // Fermi-sea dipole, analytic geometry: the local dipole of every band from the centre.
+        BcdaParams q = pl->bcda;
+        q.batch = nb;
+        q.xw = pl->d_xw;
+        q.E = pl->d_E;
+        q.U = pl->d_U;
+        q.mus = pl->d_mus;
+        q.scale = scale;
+        q.weights = weights;
+        q.mode = mode;
+        q.partials = pl->d_partials;
+        q.out_points = pl->d_points;
+        q.point_offset = point_offset;
+        q.out_perm = out_perm;
+        bcd_analytic_kernel<<<(unsigned)pl->bcda_grid, 256, 0, pl->stream>>>(q);
+        pl->launches += 1;
+    }
     if (pl->metric_shg && !pl->shg.empty()) {
         MetricShgParams q = pl->mshg;
         q.batch = nb;
@@ -1246,7 +1271,7 @@ wnlqg_status wnlqg_b200_plan_destroy(wnlqg_plan *pl) {
                       (void *)pl->d_ng_ws, (void *)pl->d_mshg_src, (void *)pl->d_mshg_diag, (void *)pl->d_mshg_ws,
                       (void *)pl->d_okeys, (void *)pl->d_operm, (void *)pl->d_ok, (void *)pl->d_ow, pl->d_osort_tmp,
                       (void *)pl->d_gC, (void *)pl->d_gL, (void *)pl->d_gred_scratch, (void *)pl->d_iso_key,
-                      (void *)pl->d_iso_rec, (void *)pl->d_fd_k, (void *)pl->d_fd_curv})
+                      (void *)pl->d_iso_rec, (void *)pl->d_fd_k, (void *)pl->d_fd_curv, (void *)pl->d_bcda_scratch})
         if (ptr) cudaFree(ptr);
     for (cudaEvent_t ev : pl->events) cudaEventDestroy(ev);
     if (pl->stream) cudaStreamDestroy(pl->stream);
@@ -1313,6 +1338,7 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
     pl->nr = model->nr;
     pl->nn = (int64_t)pl->nw * pl->nw;
     std::memset(&pl->sea, 0, sizeof(pl->sea));
+    std::memset(&pl->bcda, 0, sizeof(pl->bcda));
     auto bail = [&](wnlqg_status st) { wnlqg_b200_plan_destroy(pl); return st; };
 
     // Channels required by the requested components.
@@ -1376,6 +1402,19 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
                 pl->ch_dA[b * 3 + a] = add_channel(ch, CH_DA, b, a);
                 pl->ch_dA[a * 3 + b] = add_channel(ch, CH_DA, a, b);
                 if (q.kind == WNLQG_BERRY_DIPOLE) pl->ch_dH[cc] = add_channel(ch, CH_DH, cc, 0);
+                if (q.kind == WNLQG_BERRY_DIPOLE_SEA && t.derivative_backend == 1) {
+                    // Jets of orthogonal_bcd_partition_matrices! and of the band derivatives D_a, D_c,
+                    // D_ac, D_bc (OrthogonalGeometryDerivatives.jl:24-102, OrthogonalBandDerivatives.jl:123-245).
+                    need_r(cc);
+                    for (int x : {a, b}) {
+                        const int hidx = add_channel(ch, CH_DDH, x, cc);
+                        pl->ch_ddH[x * 3 + cc] = pl->ch_ddH[cc * 3 + x] = hidx;
+                        pl->ch_dA[x * 3 + cc] = add_channel(ch, CH_DA, x, cc);
+                        pl->ch_dA[cc * 3 + x] = add_channel(ch, CH_DA, cc, x);
+                    }
+                    add_channel(ch, CH_DDA, b, std::min(a, cc) * 3 + std::max(a, cc));
+                    add_channel(ch, CH_DDA, a, std::min(b, cc) * 3 + std::max(b, cc));
+                }
                 break;
             case WNLQG_SECOND_HARMONIC:
                 // Every Cartesian channel: the nine cutoff derivatives G^{ab} and both one-band terms.
@@ -1441,7 +1480,19 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
                 return bail(fail(WNLQG_ERR_INVALID_ARGUMENT, "finite nonempty Fermi energy axis required"));
             if (q.kind == WNLQG_BERRY_DIPOLE && t.temperature == 0.0 && !(t.fermi_surface_broadening > 0))
                 return bail(fail(WNLQG_ERR_INVALID_ARGUMENT, "T=0 requires positive eta_fs_ev"));
-            if (q.kind == WNLQG_BERRY_DIPOLE_SEA) {
+            if (q.kind == WNLQG_BERRY_DIPOLE_SEA && t.derivative_backend != 0 && t.derivative_backend != 1)
+                return bail(fail(WNLQG_ERR_INVALID_ARGUMENT, "derivative_backend must be 0 (finite difference) or 1 (analytic)"));
+            if (q.kind == WNLQG_BERRY_DIPOLE_SEA && t.derivative_backend == 1) {
+                for (int c = 0; c < q.num_components; ++c) {
+                    if (pl->bcda.n_items >= BCDA_MAX_ITEMS)
+                        return bail(fail(WNLQG_ERR_UNSUPPORTED, "more than 32 analytic Fermi-sea dipole components in one task"));
+                    const int it = pl->bcda.n_items++;
+                    pl->bcda.item_a[it] = q.components[c][0];
+                    pl->bcda.item_b[it] = q.components[c][1];
+                    pl->bcda.item_c[it] = q.components[c][2];
+                    pl->bcda.item_out[it] = vc + (int64_t)c * t.num_fermi_energies;
+                }
+            } else if (q.kind == WNLQG_BERRY_DIPOLE_SEA) {
                 if (!(std::isfinite(t.finite_difference_step) && t.finite_difference_step > 0))
                     return bail(fail(WNLQG_ERR_INVALID_ARGUMENT, "finite_difference_step must be finite and positive"));
                 // Derivative axes in order of first use and the distinct (a, b) curvature pairs.
@@ -1612,6 +1663,9 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
                 case CH_DDS:
                     v = cscale(model->S[(size_t)r * nn + e], -rc[cc.p] * rc[cc.d]);
                     break;
+                case CH_DDA:
+                    if (model->has_position) v = cscale(position(cc.p), -dsp[cc.d / 3] * dsp[cc.d % 3]);
+                    break;
                 }
                 dst[e] = v;
             }
@@ -1656,6 +1710,29 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
     if ((st = alloc((void **)&pl->d_weights, (size_t)max_batch * sizeof(double))) != WNLQG_OK) return bail(st);
     if ((st = alloc((void **)&pl->d_kidx, (size_t)max_batch * sizeof(int64_t))) != WNLQG_OK) return bail(st);
     if ((st = alloc((void **)&pl->d_status, (size_t)max_batch * sizeof(int))) != WNLQG_OK) return bail(st);
+    if (pl->bcda.n_items > 0) {
+        // Analytic Fermi-sea dipole: channel indices, two CTAs per SM, BCDA_SLOTS matrices per CTA.
+        BcdaParams &q = pl->bcda;
+        q.nw = nw;
+        q.ld = nw + 1;
+        q.xw_stride = (int64_t)pl->C * nn;
+        for (int x = 0; x < 3; ++x) {
+            q.ch_dH[x] = find_channel(ch, CH_DH, x, 0);
+            q.ch_A[x] = find_channel(ch, CH_A, x, 0);
+            for (int y = 0; y < 3; ++y) {
+                q.ch_ddH[x * 3 + y] = find_channel(ch, CH_DDH, std::min(x, y), std::max(x, y));
+                q.ch_dA[x * 3 + y] = find_channel(ch, CH_DA, x, y);
+                for (int z = 0; z < 3; ++z) q.ch_ddA[x * 9 + y * 3 + z] = find_channel(ch, CH_DDA, x, std::min(y, z) * 3 + std::max(y, z));
+            }
+        }
+        q.nmu = (int)t.num_fermi_energies;
+        q.temperature = t.temperature;
+        q.vc = vc;
+        q.gscratch_stride = (int64_t)(((size_t)BCDA_SLOTS * nw * (nw + 1) * sizeof(double2) + 255) & ~(size_t)255);
+        pl->bcda_grid = 2 * sm_count;
+        if ((st = alloc((void **)&pl->d_bcda_scratch, (size_t)pl->bcda_grid * q.gscratch_stride)) != WNLQG_OK) return bail(st);
+        q.gscratch = pl->d_bcda_scratch;
+    }
     if (pl->fd_nd > 0) {
         // Fractional image lattice * (h e_c) / 2 pi of each Cartesian step (finite_difference_step_matrix,
         // Core/Coordinates.jl:33-44; lattice element (i, c) at i + 3 c).
@@ -1986,6 +2063,7 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
         pl->partial_slots = std::max(pl->partial_slots, std::max(ps.global ? std::max(ps.grid, 2 * sm_count) : ps.grid,
                                                                    ps.grid_wide));
     pl->partial_slots = std::max(pl->partial_slots, pl->shg_grid_alloc);
+    pl->partial_slots = std::max(pl->partial_slots, pl->bcda_grid);
     if ((st = alloc((void **)&pl->d_partials, (size_t)pl->partial_slots * vc * 4 * sizeof(double))) != WNLQG_OK)
         return bail(st);
     *out_plan = pl;
