@@ -103,6 +103,10 @@ struct wnlqg_plan {
     double fd_delta[3][3];
     double *d_fd_k = nullptr, *d_fd_curv = nullptr;
     SeaParams sea;
+    // Mesh batches evaluate the shifted points k +- delta_j as the same mesh with tiles multiplied by
+    // exp(+-2 pi i delta_j . R): 2 nd tile sets [set][NR][C][nw^2] for the staged contraction (exact,
+    // like the centre's), when they fit the budget; else the stencil takes the arbitrary-k front.
+    double2 *d_fd_tiles = nullptr;
     // Fermi-sea Berry dipole on the analytic geometry (bcd_analytic.cuh): items, channels, grid and
     // the per-CTA global working sets.
     BcdaParams bcda;
@@ -903,7 +907,8 @@ wnlqg_status run_orth_eigen(wnlqg_plan *pl, const double2 *hk, int64_t stride_in
 }
 
 wnlqg_status run_front(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const int64_t *mesh, const double *kpts_device,
-                       size_t ev_base, const int64_t *kidx_device = nullptr, bool ordered = false) {
+                       size_t ev_base, const int64_t *kidx_device = nullptr, bool ordered = false,
+                       const double2 *staged_tiles = nullptr) {
     const int nr = pl->nr;
     int64_t N = (int64_t)pl->C * pl->nn;
     const bool staged = mesh != nullptr && kpts_device == nullptr && kidx_device == nullptr && pl->P1 <= STAGED_MAX_P1 &&
@@ -934,7 +939,7 @@ wnlqg_status run_front(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const int64_
         }
         const unsigned cb = (unsigned)((N + 255) / 256);
         staged_r3_kernel<<<dim3(cb, pl->P12, (unsigned)n3t), 256, 0, pl->stream>>>(
-            pl->d_tiles, N, pl->groups, pl->model->d_rvec, pl->model->d_deg, i3_first, n3, pl->d_stageY);
+            staged_tiles ? staged_tiles : pl->d_tiles, N, pl->groups, pl->model->d_rvec, pl->model->d_deg, i3_first, n3, pl->d_stageY);
         staged_r2_kernel<<<dim3(cb, pl->P1, (unsigned)nlines), 256, 0, pl->stream>>>(pl->d_stageY, N, pl->groups,
                                                                                        line_first, n2, i3_first,
                                                                                        pl->d_stageZ);
@@ -1140,15 +1145,24 @@ wnlqg_status run_fd_stencil(wnlqg_plan *pl, int64_t nb, int64_t k_begin, const i
     // Shifted runs follow the centre's order: mesh runs and ordered batches warm-start the eigensolver.
     const bool run = ordered || (mesh != nullptr && kpts_device == nullptr && kidx_device == nullptr);
     const int64_t slot = (int64_t)pl->fd_npair * pl->nw;
+    // A run of mesh points shifted by +-delta is the same run with the shifted tile sets.
+    const bool staged = pl->d_fd_tiles && mesh != nullptr && kpts_device == nullptr && kidx_device == nullptr &&
+                        mesh[0] >= pl->P1;
+    const size_t per = (size_t)pl->nr * pl->C * pl->nn;
     for (int j = 0; j < pl->fd_nd; ++j)
         for (int sgn = 0; sgn < 2; ++sgn) {
-            const double s = sgn == 0 ? 1.0 : -1.0;
-            const double *dl = pl->fd_delta[j];
-            fd_shift_kernel<<<(unsigned)((nb + 255) / 256), 256, 0, pl->stream>>>(
-                kpts_device, kidx_device, k_begin, mesh ? mesh[0] : 1, mesh ? mesh[1] : 1, mesh ? mesh[2] : 1, nb,
-                s * dl[0], s * dl[1], s * dl[2], pl->d_fd_k);
-            pl->launches += 1;
-            wnlqg_status st = run_front(pl, nb, 0, nullptr, pl->d_fd_k, ev_base, nullptr, run);
+            wnlqg_status st;
+            if (staged) {
+                st = run_front(pl, nb, k_begin, mesh, nullptr, ev_base, nullptr, false, pl->d_fd_tiles + (2 * j + sgn) * per);
+            } else {
+                const double s = sgn == 0 ? 1.0 : -1.0;
+                const double *dl = pl->fd_delta[j];
+                fd_shift_kernel<<<(unsigned)((nb + 255) / 256), 256, 0, pl->stream>>>(
+                    kpts_device, kidx_device, k_begin, mesh ? mesh[0] : 1, mesh ? mesh[1] : 1, mesh ? mesh[2] : 1, nb,
+                    s * dl[0], s * dl[1], s * dl[2], pl->d_fd_k);
+                pl->launches += 1;
+                st = run_front(pl, nb, 0, nullptr, pl->d_fd_k, ev_base, nullptr, run);
+            }
             if (st != WNLQG_OK) return st;
             if ((st = run_isolation(pl, nb, row_base, perm, 1 + 2 * j + sgn)) != WNLQG_OK) return st;
             for (const Pass &ps : pl->passes) {
@@ -1271,7 +1285,8 @@ wnlqg_status wnlqg_b200_plan_destroy(wnlqg_plan *pl) {
                       (void *)pl->d_ng_ws, (void *)pl->d_mshg_src, (void *)pl->d_mshg_diag, (void *)pl->d_mshg_ws,
                       (void *)pl->d_okeys, (void *)pl->d_operm, (void *)pl->d_ok, (void *)pl->d_ow, pl->d_osort_tmp,
                       (void *)pl->d_gC, (void *)pl->d_gL, (void *)pl->d_gred_scratch, (void *)pl->d_iso_key,
-                      (void *)pl->d_iso_rec, (void *)pl->d_fd_k, (void *)pl->d_fd_curv, (void *)pl->d_bcda_scratch})
+                      (void *)pl->d_iso_rec, (void *)pl->d_fd_k, (void *)pl->d_fd_curv, (void *)pl->d_bcda_scratch,
+                      (void *)pl->d_fd_tiles})
         if (ptr) cudaFree(ptr);
     for (cudaEvent_t ev : pl->events) cudaEventDestroy(ev);
     if (pl->stream) cudaStreamDestroy(pl->stream);
@@ -1886,6 +1901,28 @@ wnlqg_status wnlqg_b200_plan_create(wnlqg_model *model, const wnlqg_task_desc *t
         pl->groups.q1_start = base; base += P1 + 1;
         pl->groups.q1_q12 = base; base += P12;
         pl->groups.q1_r1 = base;
+    }
+    if (pl->fd_nd > 0 && pl->P1 <= STAGED_MAX_P1 &&
+        2 * (size_t)pl->fd_nd * tiles.size() * sizeof(double2) <= ((size_t)4 << 30)) {
+        // Shifted tile sets of the finite-difference stencil on meshes: T_R exp(2 pi i s delta_j . R).
+        const size_t per = tiles.size();
+        if ((st = alloc((void **)&pl->d_fd_tiles, 2 * (size_t)pl->fd_nd * per * sizeof(double2))) != WNLQG_OK) return bail(st);
+        std::vector<double2> shifted(per);
+        const size_t per_r = (size_t)pl->C * nn;
+        for (int j = 0; j < pl->fd_nd; ++j)
+            for (int sgn = 0; sgn < 2; ++sgn) {
+                const double s = sgn == 0 ? 1.0 : -1.0;
+                for (int r = 0; r < nr; ++r) {
+                    const int64_t *rv = &model->rvec[3 * (size_t)r];
+                    const double phase = 2.0 * WNLQG_PI * s *
+                                         (pl->fd_delta[j][0] * (double)rv[0] + pl->fd_delta[j][1] * (double)rv[1] +
+                                          pl->fd_delta[j][2] * (double)rv[2]);
+                    const double2 f = make_double2(std::cos(phase), std::sin(phase));
+                    for (size_t e = 0; e < per_r; ++e) shifted[r * per_r + e] = cmul(tiles[r * per_r + e], f);
+                }
+                WNLQG_CUDA(cudaMemcpy(pl->d_fd_tiles + (size_t)(2 * j + sgn) * per, shifted.data(), per * sizeof(double2),
+                                      cudaMemcpyHostToDevice));
+            }
     }
 
     // Arbitrary k-point batches are put in Morton order so that the FP32 eigensolver stage can
