@@ -199,16 +199,20 @@ __global__ void __launch_bounds__(256) staged_r1_kernel(const double2 *__restric
     const int64_t l_first = (k_begin + b0) / n1mesh - line_first;
     const int64_t l_last = (k_begin + b0 + bend - 1) / n1mesh - line_first;
     if (l_first == l_last) {
-        double2 z[STAGED_MAX_P1];
+        // One line: each Z element is loaded once and feeds the CTA's STAGED_BT outputs, which stay
+        // in registers (static indices), so nothing goes through local memory.
         const double2 *zl = Z + (l_first * P1) * N + col;
-#pragma unroll 4
-        for (int q1 = 0; q1 < P1; ++q1) z[q1] = zl[(int64_t)q1 * N];
-        for (int bb = 0; bb < bend; ++bb) {
-            double2 acc = make_double2(0.0, 0.0);
-#pragma unroll 4
-            for (int q1 = 0; q1 < P1; ++q1) acc = cfma(ph[bb][q1], z[q1], acc);
-            X[(b0 + bb) * N + col] = acc;
+        double2 acc[STAGED_BT];
+#pragma unroll
+        for (int bb = 0; bb < STAGED_BT; ++bb) acc[bb] = make_double2(0.0, 0.0);
+        for (int q1 = 0; q1 < P1; ++q1) {
+            const double2 z = zl[(int64_t)q1 * N];
+#pragma unroll
+            for (int bb = 0; bb < STAGED_BT; ++bb) acc[bb] = cfma(ph[bb][q1], z, acc[bb]);
         }
+#pragma unroll
+        for (int bb = 0; bb < STAGED_BT; ++bb)
+            if (bb < bend) X[(b0 + bb) * N + col] = acc[bb];
     } else {
         for (int bb = 0; bb < bend; ++bb) {
             const int64_t l = (k_begin + b0 + bb) / n1mesh - line_first;
