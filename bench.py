@@ -361,8 +361,8 @@ def main():
     traffic_per_k = {
         ("fp64", "response"): (1.079503e9 + 4.992e6) / 8192,
         ("fp64", "eigen"): (0.135450e9 + 35.735e6 + 0.201901e9 + 97.160e6) / 8192,
-        ("fp64", "fourier"): (41.633e6 + 1.363982e9) / 8192,
-        ("mixed", "fourier"): (41.633e6 + 1.363982e9) / 8192,
+        ("fp64", "fourier"): (37.772e6 + 1.014368e9) / 8192,
+        ("mixed", "fourier"): (37.772e6 + 1.014368e9) / 8192,
         ("mixed", "response"): (1.082281e9 + 9.649408e6) / 8192,
         ("mixed", "eigen"): (0.134329e9 + 35.740160e6 + 0.201393e9 + 98.023680e6) / 8192,
         ("mixed", "fourier_random"): (436.281088e6 + 1.025739e9) / 8192,
