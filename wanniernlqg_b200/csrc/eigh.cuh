@@ -560,17 +560,20 @@ __global__ void __launch_bounds__(TEAM == 32 ? 128 : TEAM, TEAM == 32 ? 4 : (TEA
 }
 
 // First-order completion of the FP64 refinement.  After one FP64 sweep the off-diagonal of A is
-// quadratically small; when every |a_ij| <= 2^-26 |d_i - d_j|, the eigenvectors of A are
+// quadratically small; when every |a_ij| <= tau |d_i - d_j| (tau = 2^-26), the eigenvectors of A are
 // e_j + sum_{i != j} e_i a_ij / (d_j - d_i) and its eigenvalues d_j + sum_{i != j} |a_ij|^2 / (d_j - d_i)
-// up to terms in products of two such ratios (<= 2^-52: first-order perturbation theory), so
-// W (I + E) with E_ij = a_ij / (d_j - d_i) (anti-Hermitian, hence unitary to the same order) reaches
-// what a further sweep would, for one product instead of np - 1 rotation rounds.  Returns false,
-// with A and W untouched, when some pair is too close for that bound (the caller then sweeps).
-// dnew: np doubles of the team's scratch.
+// up to terms in products of two such ratios (<= tau^2 = 2^-52: first-order perturbation theory),
+// so W (I + E) with E_ij = a_ij / (d_j - d_i) (anti-Hermitian, hence unitary to the same order)
+// reaches what a further sweep would, for one product instead of np - 1 rotation rounds.  The
+// mixed path, whose response arithmetic is FP32, takes tau = 2^-13 straight after the FP32 stage
+// (eigenvector error <= 2^-26, below that arithmetic) in place of its one FP64 sweep; there E is
+// no longer negligible against FP64 rounding, so the rotation is I + E + E^2 / 2 = ((I + E)^2 + I) / 2,
+// whose deviation from unitarity is |E|^4 / 4 instead of |E|^2.  Returns false, with A and W
+// untouched, when some pair is too close for the bound (the caller then sweeps).  dnew: np
+// doubles of the team's scratch.
 template <int TEAM>
-WNLQG_D bool team_first_order_completion(double2 *A, double2 *W, int np, int ld, double *dnew) {
+WNLQG_D bool team_first_order_completion(double2 *A, double2 *W, int np, int ld, double *dnew, double tau) {
     const int t = Team<TEAM>::rank();
-    const double tau = 1.4901161193847656e-08;   // 2^-26
     bool bad = false;
     for (int e = t; e < np * np; e += TEAM) {
         const int i = e % np, j = e / np;
@@ -602,7 +605,18 @@ WNLQG_D bool team_first_order_completion(double2 *A, double2 *W, int np, int ld,
     if (t < np) A[t + ld * t] = make_double2(1.0, 0.0);
     Team<TEAM>::sync();
     double2 col[Team<TEAM>::ROWS];
-    team_column_product<TEAM>(W, A, col, np, ld, false);                    // (W (I + E))[:, c0]
+    if (tau > 1.4901161193847656e-08) {
+        constexpr int ROWS = Team<TEAM>::ROWS;
+        const int c0 = t & 31, r0 = (t >> 5) * ROWS;
+        team_column_product<TEAM>(A, A, col, np, ld, false);                // ((I + E)^2)[:, c0]
+        Team<TEAM>::sync();
+#pragma unroll
+        for (int i = 0; i < ROWS; ++i)
+            col[i] = make_double2(0.5 * (col[i].x + (r0 + i == c0 ? 1.0 : 0.0)), 0.5 * col[i].y);
+        team_store_column<TEAM>(A, col, np, ld);                            // A <- I + E + E^2 / 2
+        Team<TEAM>::sync();
+    }
+    team_column_product<TEAM>(W, A, col, np, ld, false);                    // (W A)[:, c0]
     Team<TEAM>::sync();
     team_store_column<TEAM>(W, col, np, ld);
     if (t < np) A[t + ld * t] = make_double2(dnew[t], 0.0);
@@ -614,7 +628,8 @@ WNLQG_D bool team_first_order_completion(double2 *A, double2 *W, int np, int ld,
 // W = V (I - E/2 + 3E^2/8) with E = V^H V - I (second-order Loewdin), H' = W^H H W, then FP64
 // Jacobi sweeps on H' (quadratic convergence: the off-diagonal goes from the FP32 stage's
 // 2^-17 ||H|| to the square of that over the gap), then ascending order and canonical phases.
-// converge = 0 (mixed path): one sweep unless H' is already diagonal to 1e-13 ||H||.
+// converge = 0 (mixed path): one sweep unless H' is already diagonal to 1e-13 ||H||, or the
+// first-order completion with tau = 2^-13 in its place.
 // converge = 1 (FP64 path): sweeps until the FP64 CTA Jacobi's stopping rule holds (off-diagonal
 // norm <= np 2^-60 ||H||, or a sweep with every |a_pq| <= 2^-60 ||H||), so the FP32 stage only
 // preconditions and the result carries the FP64 solver's accuracy; from the second sweep on, a
@@ -704,7 +719,9 @@ __global__ void __launch_bounds__(TEAM == 128 ? 128 : 64, TEAM == 32 ? 1 : 6) ei
         for (int sweep = 0; sweep < (converge ? WNLQG_JACOBI_MAX_SWEEPS : 1); ++sweep) {
             const double off = team_offdiag2<TEAM>(A, np, ld, red);
             if (sqrt(off) <= (converge ? tol * np : fro * 1.0e-13)) break;
-            if (converge && sweep > 0 && team_first_order_completion<TEAM>(A, W, np, ld, reinterpret_cast<double *>(phase)))
+            if ((converge ? sweep > 0 : sweep == 0) &&
+                team_first_order_completion<TEAM>(A, W, np, ld, reinterpret_cast<double *>(phase),
+                                                  converge ? 1.4901161193847656e-08 : 1.220703125e-04))
                 break;
             if (!team_jacobi_sweep<double, TEAM>(A, W, np, ld, tol, rot_s, rot_c)) break;
         }
@@ -879,9 +896,9 @@ struct RefineCtaSmem {
 // The CTA form of team_first_order_completion (the same bound and algebra, the product on the
 // FP64 tensor cores): on success W <- W (I + E) (Wc and Tc swap roles) and A's diagonal holds the
 // second-order eigenvalues.  dnew: np doubles of shared scratch.
-WNLQG_D bool cta_first_order_completion(double2 *A, double2 *&Wc, double2 *&Tc, int np, int ld, double *dnew) {
+WNLQG_D bool cta_first_order_completion(double2 *A, double2 *&Wc, double2 *&Tc, int np, int ld, double *dnew,
+                                        double tau) {
     const int tid = threadIdx.x;
-    const double tau = 1.4901161193847656e-08;   // 2^-26
     int bad = 0;
     for (int e = tid; e < np * np; e += blockDim.x) {
         const int i = e % np, j = e / np;
@@ -911,7 +928,17 @@ WNLQG_D bool cta_first_order_completion(double2 *A, double2 *&Wc, double2 *&Tc, 
     __syncthreads();
     for (int i = tid; i < np; i += blockDim.x) A[i + ld * i] = make_double2(1.0, 0.0);
     __syncthreads();
-    dmma_product<0>(Wc, A, Tc, np, ld);                      // T = W (I + E)
+    if (tau > 1.4901161193847656e-08) {                      // A <- ((I + E)^2 + I) / 2
+        dmma_product<0>(A, A, Tc, np, ld);
+        __syncthreads();
+        for (int e = tid; e < np * np; e += blockDim.x) {
+            const int i = e % np, j = e / np;
+            const double2 v = Tc[i + ld * j];
+            A[i + ld * j] = make_double2(0.5 * (v.x + (i == j ? 1.0 : 0.0)), 0.5 * v.y);
+        }
+        __syncthreads();
+    }
+    dmma_product<0>(Wc, A, Tc, np, ld);                      // T = W A
     __syncthreads();
     double2 *x = Wc;
     Wc = Tc;
@@ -1002,7 +1029,9 @@ __global__ void __launch_bounds__(512, 1) eigh_refine_f64_cta_kernel(const doubl
         for (int sweep = 0; sweep < (converge ? WNLQG_JACOBI_MAX_SWEEPS : 1); ++sweep) {
             const double off = offdiag_norm(A, np, ld, red);
             if (off <= (converge ? tol * np : fro * 1.0e-13)) break;
-            if (converge && sweep > 0 && cta_first_order_completion(A, Wc, Tc, np, ld, reinterpret_cast<double *>(rot_s)))
+            if ((converge ? sweep > 0 : sweep == 0) &&
+                cta_first_order_completion(A, Wc, Tc, np, ld, reinterpret_cast<double *>(rot_s),
+                                           converge ? 1.4901161193847656e-08 : 1.220703125e-04))
                 break;
             if (tid == 0) rot_flag = 0;
             __syncthreads();
