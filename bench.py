@@ -330,8 +330,23 @@ def main():
             "response": 18 * 8.0 * nw ** 3 + 4.0 * nw * nw * 512}
     hbm = {"fourier": C * nw * nw * 16 * (1.0 + p1 / MESH[0]), "eigen": nw * nw * 16 * 2.0 + nw * 8,
            "response": (C - 1) * nw * nw * 16 + nw * nw * 16}
-    sm_peak = {"fp64": 37.0, "mixed": 74.0}["fp64" if precision == _abi.PRECISION_FP64 else "mixed"]
-    sm_src = "nominal B200 CUDA-core peak (FP64 37 / FP32 74 TFLOP/s; not in the measured peaks file)"
+    # SM-bound stages: measured on this device after the timed region (FP64 DMMA, FP64 FMA, FP32 FMA
+    # probes of wnlqg_b200_measure_peaks); the nominal figures only if the probe fails.
+    try:
+        from wanniernlqg_b200 import _lib
+        sm_measured = _lib.measure_peaks(torch.cuda.current_device())
+    except Exception:   # noqa: BLE001 - the roofline then names its nominal source
+        sm_measured = None
+    if sm_measured is not None and precision == _abi.PRECISION_FP64:
+        sm_peak = max(sm_measured["fp64_dmma_tflops"], sm_measured["fp64_fma_tflops"])
+        sm_src = ("measured in this run: FP64 DMMA %.1f, FP64 FMA %.1f TFLOP/s (the larger)"
+                  % (sm_measured["fp64_dmma_tflops"], sm_measured["fp64_fma_tflops"]))
+    elif sm_measured is not None:
+        sm_peak = sm_measured["fp32_fma_tflops"]
+        sm_src = "measured in this run: FP32 FMA %.1f TFLOP/s" % sm_measured["fp32_fma_tflops"]
+    else:
+        sm_peak = {"fp64": 37.0, "mixed": 74.0}["fp64" if precision == _abi.PRECISION_FP64 else "mixed"]
+        sm_src = "nominal B200 CUDA-core peak (FP64 37 / FP32 74 TFLOP/s; the probe failed)"
     slices = 7 if precision == _abi.PRECISION_FP64 else 4
     tile_n = 64 if slices == 7 else 128
     kpad = -(-2 * nr // 64) * 64
@@ -382,6 +397,7 @@ def main():
         "stages": per_stage,
         "algorithmic_per_k": {"flop": flop, "hbm_bytes": hbm, "tensor_int8_ops": tc_ops if random_mode else None},
         "launches_per_step": launches // max(1, args.steps),
+        "sm_peaks_measured_tflops": sm_measured,
     })
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,

@@ -382,6 +382,15 @@ typedef struct wnlqg_autotune_report {
 WNLQG_API wnlqg_status wnlqg_b200_plan_autotune(wnlqg_plan *plan, const int64_t mesh[3], int64_t k_begin,
                                       int64_t k_end, wnlqg_autotune_report *report);
 
+/* ---- Measured arithmetic peaks (no reference counterpart: the roofline denominators of the
+ * engine's SM-bound stages) ---------------------------------------------------------------------
+ * Dense throughput of the device in TFLOP/s, each from one timed launch of independent dependency
+ * chains on every SM (about 20 ms each): FP64 tensor-core mma.sync.m8n8k4 (DMMA, the engine's FP64
+ * products), FP64 FMA and FP32 FMA on the CUDA cores.  A pure compute probe: no memory traffic,
+ * no waits. */
+WNLQG_API wnlqg_status wnlqg_b200_measure_peaks(int32_t device, double *fp64_dmma_tflops, double *fp64_fma_tflops,
+                                                double *fp32_fma_tflops);
+
 #ifdef __cplusplus
 }
 #endif

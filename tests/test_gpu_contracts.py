@@ -180,3 +180,15 @@ def test_large_orbital_autotuned_grids_keep_results(engine_cls, oracle_mod, prec
     ref = oracle_mod.point_values(model, task, k)
     for g, r in zip(task.split(got), task.split(ref)):
         assert rel_err(g, r) < tol
+
+
+def test_measured_peaks_are_plausible(engine_cls):
+    """The roofline denominators of the SM-bound stages: positive, FP32 FMA above FP64 FMA, and
+    within an order of magnitude of the B200's nominal dense figures (FP64 ~37-40, FP32 ~74-80
+    TFLOP/s)."""
+    from wanniernlqg_b200 import _lib
+    p = _lib.measure_peaks(0)
+    assert 4.0 < p["fp64_dmma_tflops"] < 400.0
+    assert 4.0 < p["fp64_fma_tflops"] < 400.0
+    assert 8.0 < p["fp32_fma_tflops"] < 800.0
+    assert p["fp32_fma_tflops"] > p["fp64_fma_tflops"]

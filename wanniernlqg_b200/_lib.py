@@ -25,7 +25,7 @@ EXPORTED_SYMBOLS = (
     "wnlqg_b200_mlp_set_params", "wnlqg_b200_mlp_forward", "wnlqg_b200_mlp_loss_grad", "wnlqg_b200_mlp_train",
     "wnlqg_b200_graph_capture_mesh_many", "wnlqg_b200_graph_capture_points_weighted", "wnlqg_b200_graph_launch",
     "wnlqg_b200_graph_status", "wnlqg_b200_graph_kernel_count", "wnlqg_b200_graph_destroy",
-    "wnlqg_b200_plan_autotune", "wnlqg_b200_plan_status",
+    "wnlqg_b200_plan_autotune", "wnlqg_b200_plan_status", "wnlqg_b200_measure_peaks",
 )
 
 _lib = None
@@ -91,6 +91,8 @@ def load():
     L.wnlqg_b200_plan_last_launch_count.argtypes = [vp]
     L.wnlqg_b200_plan_status.argtypes = [vp]
     L.wnlqg_b200_plan_status.restype = ctypes.c_int
+    L.wnlqg_b200_measure_peaks.argtypes = [ctypes.c_int32, dp, dp, dp]
+    L.wnlqg_b200_measure_peaks.restype = ctypes.c_int
     L.wnlqg_b200_graph_capture_mesh_many.argtypes = [ctypes.POINTER(vp), ctypes.c_int32, ip, ip, ip,
                                                      ctypes.POINTER(vp), ctypes.POINTER(vp)]
     L.wnlqg_b200_graph_capture_points_weighted.argtypes = [vp, vp, vp, ctypes.c_int64, vp, ctypes.POINTER(vp)]
@@ -125,3 +127,13 @@ def last_error() -> str:
 def check(status: int) -> None:
     if status != _abi.WNLQG_OK:
         raise EngineError(status, last_error())
+
+
+def measure_peaks(device: int = 0) -> dict:
+    """Measured dense throughput of `device` in TFLOP/s: FP64 DMMA, FP64 FMA and FP32 FMA
+    (wnlqg_b200_measure_peaks, about 20 ms of compute)."""
+    L = load()
+    vals = [ctypes.c_double(0.0) for _ in range(3)]
+    st = L.wnlqg_b200_measure_peaks(int(device), *[ctypes.byref(v) for v in vals])
+    check(st)
+    return {"fp64_dmma_tflops": vals[0].value, "fp64_fma_tflops": vals[1].value, "fp32_fma_tflops": vals[2].value}

@@ -3210,3 +3210,80 @@ extern "C" wnlqg_status wnlqg_b200_mlp_train(wnlqg_mlp *m, const float *x, const
     WNLQG_CUDA(cudaStreamSynchronize(m->stream));
     return WNLQG_OK;
 }
+
+// ---- measured arithmetic peaks ----------------------------------------------------------------
+namespace {
+
+// Each warp keeps 8 independent DMMA accumulator pairs; every iteration issues one m8n8k4 per
+// pair (512 FLOP per warp each).  The operands drift with the accumulators so nothing is hoisted.
+__global__ void __launch_bounds__(256) peak_dmma_kernel(int iters, double *out) {
+    double acc[8][2];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) { acc[q][0] = 1e-3 * q; acc[q][1] = 2e-3 * q; }
+    double a = 1.0 + 1e-9 * threadIdx.x, b = 1.0 - 1e-9 * blockIdx.x;
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) dmma_m8n8k4(acc[q][0], acc[q][1], a, b);
+        a = a * 0.999999999 + 1e-12;
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) s += acc[q][0] + acc[q][1];
+    if (s == 123.456) out[0] = s;   // keeps the chains live; never true for these inputs
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) peak_fma_kernel(int iters, T *out) {
+    T acc[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) acc[q] = (T)(1e-3 * (q + threadIdx.x));
+    const T a = (T)(1.0 - 1e-7 * blockIdx.x), b = (T)1e-7;
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) acc[q] = fma(acc[q], a, b);
+    }
+    T s = 0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) s += acc[q];
+    if (s == (T)123.456) out[0] = s;
+}
+
+}  // namespace
+
+extern "C" wnlqg_status wnlqg_b200_measure_peaks(int32_t device, double *fp64_dmma_tflops, double *fp64_fma_tflops,
+                                                 double *fp32_fma_tflops) {
+    if (!fp64_dmma_tflops || !fp64_fma_tflops || !fp32_fma_tflops) return fail(WNLQG_ERR_INVALID_ARGUMENT, "NULL argument");
+    WNLQG_CUDA(cudaSetDevice(device));
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    double *scratch = nullptr;
+    WNLQG_CUDA(cudaMalloc(&scratch, 64));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const int blocks = sms * 8, threads = 256;
+    auto time_ms = [&](auto launch) {
+        launch();   // warm-up
+        cudaEventRecord(e0);
+        launch();
+        cudaEventRecord(e1);
+        cudaEventSynchronize(e1);
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        return (double)ms;
+    };
+    const int it_dmma = 4096, it_fma = 16384;
+    const double t_dmma = time_ms([&] { peak_dmma_kernel<<<blocks, threads>>>(it_dmma, scratch); });
+    const double t_f64 = time_ms([&] { peak_fma_kernel<double><<<blocks, threads>>>(it_fma, scratch); });
+    const double t_f32 = time_ms([&] { peak_fma_kernel<float><<<blocks, threads>>>(it_fma, reinterpret_cast<float *>(scratch)); });
+    cudaError_t err = cudaGetLastError();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(scratch);
+    if (err != cudaSuccess) return fail(WNLQG_ERR_CUDA, std::string("peak probe: ") + cudaGetErrorString(err));
+    const double warps = (double)blocks * threads / 32.0, thr = (double)blocks * threads;
+    *fp64_dmma_tflops = warps * it_dmma * 8.0 * 512.0 / (t_dmma * 1e-3) / 1e12;
+    *fp64_fma_tflops = thr * it_fma * 8.0 * 2.0 / (t_f64 * 1e-3) / 1e12;
+    *fp32_fma_tflops = thr * it_fma * 8.0 * 2.0 / (t_f32 * 1e-3) / 1e12;
+    return WNLQG_OK;
+}
