@@ -156,8 +156,6 @@ def test_graph_of_the_berry_dipole_stencils_replays_the_direct_call(torch_and_en
             graph.status()
             for d, g in zip(direct, graphed):
                 assert torch.equal(d, g)
-        # The two backends agree to the central difference's O(h^2) (default eta: the finite
-        # differences see the regularized curvature, a 1e-4 effect on this model).
         a = direct[0].cpu().numpy().view(np.complex128)
         b = direct[1].cpu().numpy().view(np.complex128)
         assert np.all(np.isfinite(a)) and np.all(np.isfinite(b))
