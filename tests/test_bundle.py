@@ -70,7 +70,8 @@ def test_reference_legacy_bundles_are_rejected():
         path = os.path.join(REFERENCE, rel)
         for reader in (bundle.read_real_space_operator_bundle_manifest,
                        bundle.read_real_space_operator_bundle,
-                       bundle.read_operator_bundle_payload):
+                       bundle.read_operator_bundle_payload,
+                       lambda p: bundle.validate_packed_paired_tb(p, __file__)):
             with pytest.raises(ValueError, match="MODEL_SCHEMA_UNSUPPORTED"):
                 reader(path)
 
@@ -124,6 +125,19 @@ def test_reference_bundle_round_trips_through_the_writer(tmp_path):
 
 def _model():
     return synthetic_orthogonal_model(6, 1, seed=11, full_position=True)
+
+
+def test_paired_tb_validation_has_no_source_in_the_current_format(tmp_path):
+    """validate_packed_paired_tb: a current-format bundle carries no paired _tb.dat source."""
+    from wanniernlqg_b200.model import write_wannier_tb
+    model = _model()
+    path = bundle.write_model_operator_bundle(str(tmp_path / "m.h5"), model, mp_grid=(4, 4, 4))
+    tb = str(tmp_path / "m_tb.dat")
+    write_wannier_tb(model, tb)
+    with pytest.raises(ValueError, match="MissingPairedTBSource"):
+        bundle.validate_packed_paired_tb(path, tb)
+    with pytest.raises(ValueError, match="does not exist"):
+        bundle.validate_packed_paired_tb(str(tmp_path / "absent.h5"), tb)
 
 
 def test_model_round_trip(tmp_path):

@@ -336,6 +336,19 @@ def read_real_space_operator_bundle_manifest(filename: str, receipt_path=None
         return _manifest_from_handle(os.path.realpath(os.path.abspath(filename)), h)
 
 
+def validate_packed_paired_tb(bundle_path: str, filename: str, receipt_path=None) -> None:
+    """``validate_packed_paired_tb`` (IO/RealSpaceOperatorBundles.jl:709-720,
+    WannierNLQGOperatorBundleExt.jl:4190-4218): the byte-for-byte check of a ``_tb.dat`` against
+    the copy a bundle carries.  The current model format (3.0) stores no paired source (its
+    manifest's ``paired_tb_source_bytes`` is nothing), so after the schema gate and the manifest
+    rules the call reports ``MissingPairedTBSource``, as the reference's does; older formats
+    stop at the schema gate (``MODEL_SCHEMA_UNSUPPORTED``)."""
+    read_real_space_operator_bundle_manifest(bundle_path, receipt_path)
+    if not os.path.isfile(filename):
+        raise ValueError("paired _tb.dat source does not exist: %s" % filename)
+    raise ValueError("MissingPairedTBSource")
+
+
 def read_operator_bundle_payload(filename: str, receipt_path=None):
     """The validated manifest and the whole complex128 payload (a host copy)."""
     with _open(filename, receipt_path) as h:
