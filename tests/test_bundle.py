@@ -136,7 +136,9 @@ def test_paired_tb_validation_has_no_source_in_the_current_format(tmp_path):
     write_wannier_tb(model, tb)
     with pytest.raises(ValueError, match="MissingPairedTBSource"):
         bundle.validate_packed_paired_tb(path, tb)
-    with pytest.raises(ValueError, match="does not exist"):
+    with pytest.raises(ValueError, match="MissingPairedTBSource"):
+        bundle.validate_packed_paired_tb(path, str(tmp_path / "absent_tb.dat"))
+    with pytest.raises(ValueError, match="operator bundle does not exist"):
         bundle.validate_packed_paired_tb(str(tmp_path / "absent.h5"), tb)
 
 

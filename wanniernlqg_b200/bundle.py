@@ -344,8 +344,7 @@ def validate_packed_paired_tb(bundle_path: str, filename: str, receipt_path=None
     rules the call reports ``MissingPairedTBSource``, as the reference's does; older formats
     stop at the schema gate (``MODEL_SCHEMA_UNSUPPORTED``)."""
     read_real_space_operator_bundle_manifest(bundle_path, receipt_path)
-    if not os.path.isfile(filename):
-        raise ValueError("paired _tb.dat source does not exist: %s" % filename)
+    # The reference reports the missing source before it opens `filename`.
     raise ValueError("MissingPairedTBSource")
 
 
