@@ -246,3 +246,22 @@ def test_derivative_backend_must_be_known(oracle_mod):
         oracle_mod.point_values(model, task, np.array([[0.1, 0.2, 0.3]]))
     with pytest.raises(ValueError):
         _abi.TaskArrays([(_abi.BERRY_DIPOLE_SEA, ["xyz"])], fermi_energies=[0.0], derivative_backend="spectral")
+
+
+def test_sea_dipole_is_the_same_in_both_wannier_center_conventions(oracle_mod):
+    """Convention I changes the Bloch basis by a k-dependent diagonal phase and the home-cell
+    connection by the centres (WannierCenterConventionTransforms.jl:55-113); the band curvature and
+    its derivative are physical, so both backends give Convention II's moment (analytic to
+    rounding, the finite differences to their rounding amplified by 1/2h)."""
+    from wanniernlqg_b200.model import synthetic_orthogonal_model
+    model = synthetic_orthogonal_model(6, 1, 3, full_position=True)
+    k = np.random.default_rng(5).random((6, 3))
+    comps = ["xyz", "xzx", "yzy", "xyx"]
+    for backend, tol in (("analytic", 1e-13), ("finite_difference", 1e-10)):
+        vals = []
+        for conv in ("II", "I"):
+            task = _abi.TaskArrays([(_abi.BERRY_DIPOLE_SEA, comps)], fermi_energies=[0.0, 50.0], temperature=300.0,
+                                   degeneracy_threshold=1e-6, denominator_regularization=0.0,
+                                   wannier_center_convention=conv, derivative_backend=backend)
+            vals.append(oracle_mod.point_values(model, task, k))
+        assert np.abs(vals[0] - vals[1]).max() <= tol * np.abs(vals[0]).max()

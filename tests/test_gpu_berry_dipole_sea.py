@@ -222,3 +222,20 @@ def test_analytic_sea_dipole_sums_match_oracle_and_finite_differences(engine_cls
     with engine_cls(model, task("finite_difference")) as eng:
         fd = eng.integrate_mesh(mesh)
     assert rel_err(fd, got) < 1e-6
+
+
+@pytest.mark.parametrize("backend", ["finite_difference", "analytic"])
+def test_sea_dipole_convention_one_matches_oracle(engine_cls, oracle_mod, backend):
+    """Convention I (centre displacements in every derivative channel, including the second
+    derivatives of A) against the oracle, on points and on a mesh."""
+    model = synthetic_orthogonal_model(8, 1, 5, full_position=True)
+    task = _abi.TaskArrays([(_abi.BERRY_DIPOLE_SEA, COMPS)], fermi_energies=[-0.2, 0.3], temperature=300.0,
+                           degeneracy_threshold=1e-7, denominator_regularization=0.0, wannier_center_convention="I",
+                           derivative_backend=backend)
+    k = np.random.default_rng(8).random((48, 3))
+    ref = oracle_mod.point_values(model, task, k)
+    ref_mesh = oracle_mod.integrate_mesh(model, task, (6, 5, 4))
+    tol = RTOL if backend == "finite_difference" else ANALYTIC_RTOL
+    with engine_cls(model, task) as eng:
+        assert rel_err(eng.point_values(k), ref) < tol
+        assert rel_err(eng.integrate_mesh((6, 5, 4)), ref_mesh) < tol
