@@ -25,7 +25,7 @@
 
 #define BCDA_MAX_ITEMS 32
 #define BCDA_MAX_NW 128
-#define BCDA_SLOTS 20
+#define BCDA_SLOTS 19
 
 struct BcdaParams {
     int nw, ld;
@@ -66,7 +66,7 @@ __global__ void __launch_bounds__(256) bcd_analytic_kernel(BcdaParams p) {
     double2 *Aa = slots + 8 * mat, *Ab = slots + 9 * mat, *Ac = slots + 10 * mat;
     double2 *Aac = slots + 11 * mat, *Abc = slots + 12 * mat, *Om = slots + 13 * mat;
     double2 *Da = slots + 14 * mat, *Db = slots + 15 * mat, *Dc = slots + 16 * mat;
-    double2 *Dac = slots + 17 * mat, *Dbc = slots + 18 * mat, *P = slots + 19 * mat;
+    double2 *Dac = slots + 17 * mat, *Dbc = slots + 18 * mat;
     __shared__ double sE[BCDA_MAX_NW], sTot[BCDA_MAX_NW];
     __shared__ double sdEa[BCDA_MAX_NW], sdEb[BCDA_MAX_NW], sdEc[BCDA_MAX_NW];
     __shared__ double2 sAca[BCDA_MAX_NW], sAcb[BCDA_MAX_NW], sOmc[BCDA_MAX_NW];
@@ -95,6 +95,14 @@ __global__ void __launch_bounds__(256) bcd_analytic_kernel(BcdaParams p) {
         dmma_product<1>(U, T1, dst, nw, ld);
         __syncthreads();
     };
+    // dst0 = U^H X0 U and dst1 = U^H X1 U in two paired DMMA passes, the channels read straight
+    // from the Wannier-gauge input (leading dimension nw).
+    auto rotate2 = [&](const double2 *xw, int c0, int c1, double2 *dst0, double2 *dst1) {
+        dmma_product_pair<0>(xw + (int64_t)c0 * nn, nw, U, T1, xw + (int64_t)c1 * nn, nw, U, T2, nw, ld);
+        __syncthreads();
+        dmma_product_pair<1>(U, ld, T1, dst0, U, ld, T2, dst1, nw, ld);
+        __syncthreads();
+    };
     // diag[n] = (U^H (X0 - X1) U)_nn
     auto rotate_diag = [&](const double2 *xw, int c0, int c1, double2 *diag) {
         load(xw, c0, c1);
@@ -117,8 +125,7 @@ __global__ void __launch_bounds__(256) bcd_analytic_kernel(BcdaParams p) {
     // D_xc = U^H d_x d_c U (orthogonal_band_second_derivative! with alpha = x, beta = c).
     auto second = [&](const double2 *dHx, const double2 *ddHxc, const double2 *Ax, const double2 *Dx,
                       const double *dEx, const double2 *Axc, const double2 *Acx_diag, double2 *out) {
-        dmma_product<0>(dHx, Dc, T1, nw, ld);
-        dmma_product<0>(dHc, Dx, T2, nw, ld);
+        dmma_product_pair<0>(dHx, ld, Dc, T1, dHc, ld, Dx, T2, nw, ld);
         __syncthreads();
         for (int e = tid; e < nn; e += blockDim.x) {
             const int i = e % nw, m = e / nw;
@@ -151,16 +158,11 @@ __global__ void __launch_bounds__(256) bcd_analytic_kernel(BcdaParams p) {
         for (int it = 0; it < p.n_items; ++it) {
             const int a = p.item_a[it], bb = p.item_b[it], c = p.item_c[it];
             auto sym = [](int x, int y) { return x <= y ? x * 3 + y : y * 3 + x; };
-            rotate(xw, p.ch_dH[a], -1, dHa);
-            rotate(xw, p.ch_dH[bb], -1, dHb);
-            rotate(xw, p.ch_dH[c], -1, dHc);
-            rotate(xw, p.ch_ddH[sym(a, c)], -1, ddHac);
-            rotate(xw, p.ch_ddH[sym(bb, c)], -1, ddHbc);
-            rotate(xw, p.ch_A[a], -1, Aa);
-            rotate(xw, p.ch_A[bb], -1, Ab);
-            rotate(xw, p.ch_A[c], -1, Ac);
-            rotate(xw, p.ch_dA[a * 3 + c], -1, Aac);                         // d_c A_a
-            rotate(xw, p.ch_dA[bb * 3 + c], -1, Abc);                        // d_c A_b
+            rotate2(xw, p.ch_dH[a], p.ch_dH[bb], dHa, dHb);
+            rotate2(xw, p.ch_dH[c], p.ch_ddH[sym(a, c)], dHc, ddHac);
+            rotate2(xw, p.ch_ddH[sym(bb, c)], p.ch_A[a], ddHbc, Aa);
+            rotate2(xw, p.ch_A[bb], p.ch_A[c], Ab, Ac);
+            rotate2(xw, p.ch_dA[a * 3 + c], p.ch_dA[bb * 3 + c], Aac, Abc);  // d_c A_a, d_c A_b
             rotate(xw, p.ch_dA[bb * 3 + a], p.ch_dA[a * 3 + bb], Om);         // d_a A_b - d_b A_a
             rotate_diag(xw, p.ch_dA[c * 3 + a], -1, sAca);                   // d_a A_c
             rotate_diag(xw, p.ch_dA[c * 3 + bb], -1, sAcb);                  // d_b A_c
@@ -186,23 +188,28 @@ __global__ void __launch_bounds__(256) bcd_analytic_kernel(BcdaParams p) {
                 sTot[n] = t;
             }
             __syncthreads();
-            // Triples through one full product each.
+            // Triples through one full product each, two products per paired DMMA pass (into T1, T2).
             const double2 *L[8] = {Dc, Db, Dc, Da, Dc, Dc, Db, Da};
             const double2 *R[8] = {Db, Dc, Da, Dc, Aa, Ab, Aa, Ab};
-            for (int q = 0; q < 8; ++q) {
-                dmma_product<0>(L[q], R[q], P, nw, ld);
+            #pragma unroll
+            for (int q = 0; q < 8; q += 2) {
+                dmma_product_pair<0>(L[q], ld, R[q], T1, L[q + 1], ld, R[q + 1], T2, nw, ld);
                 __syncthreads();
                 for (int n = tid; n < nw; n += blockDim.x) {
-                    double t = 0.0;
+                    double t;
                     switch (q) {
-                    case 0: t = -diag2(P, Aa, n).x + diag2(P, Da, n).y; break;   // Dc Db: second, pure D
-                    case 1: t = -diag2(P, Aa, n).x + diag2(P, Da, n).y; break;   // Db Dc
-                    case 2: t = diag2(P, Ab, n).x - diag2(P, Db, n).y; break;    // Dc Da
-                    case 3: t = diag2(P, Ab, n).x - diag2(P, Db, n).y; break;    // Da Dc
-                    case 4: t = diag2(P, Db, n).x; break;                        // Dc Aa: mixed
-                    case 5: t = -diag2(P, Da, n).x; break;                       // Dc Ab
-                    case 6: t = diag2(P, Dc, n).x; break;                        // Db Aa
-                    default: t = -diag2(P, Dc, n).x; break;                      // Da Ab
+                    case 0:   // Dc Db, Db Dc: second, pure D
+                        t = -diag2(T1, Aa, n).x + diag2(T1, Da, n).y - diag2(T2, Aa, n).x + diag2(T2, Da, n).y;
+                        break;
+                    case 2:   // Dc Da, Da Dc
+                        t = diag2(T1, Ab, n).x - diag2(T1, Db, n).y + diag2(T2, Ab, n).x - diag2(T2, Db, n).y;
+                        break;
+                    case 4:   // Dc Aa, Dc Ab: mixed
+                        t = diag2(T1, Db, n).x - diag2(T2, Da, n).x;
+                        break;
+                    default:  // Db Aa, Da Ab
+                        t = diag2(T1, Dc, n).x - diag2(T2, Dc, n).x;
+                        break;
                     }
                     sTot[n] += t;
                 }
