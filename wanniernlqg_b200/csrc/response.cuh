@@ -298,6 +298,30 @@ WNLQG_D void rotate_two_to_hamiltonian(const double2 *__restrict__ src0, const d
     }
 }
 
+// Per-band sums out(n, sum_l term(n, l)) for n < nw, by groups of g threads per band (g the largest
+// power of two up to 32 with g nw <= blockDim.x): each thread of a group sums the terms l = part,
+// part + g, ... in order, then a fixed shuffle butterfly adds the group's partials, so the order of
+// the additions is fixed and the result reproducible.  A band's group is g consecutive lanes of one
+// warp.  All threads of the CTA call it (every lane takes every shuffle); no closing barrier.
+template <typename F, typename S>
+WNLQG_D void band_sums(int nw, F term, S out) {
+    int g = 32;
+    while (g > 1 && g * nw > (int)blockDim.x) g >>= 1;
+    const int part = threadIdx.x & (g - 1);
+    const int per = (int)blockDim.x / g;
+    for (int n0 = 0; n0 < nw; n0 += per) {
+        const int n = n0 + (int)threadIdx.x / g;
+        double2 acc = make_double2(0.0, 0.0);
+        if (n < nw)
+            for (int l = part; l < nw; l += g) acc = cadd(acc, term(n, l));
+        for (int o = g >> 1; o > 0; o >>= 1) {
+            acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
+            acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
+        }
+        if (part == 0 && n < nw) out(n, acc);
+    }
+}
+
 // diag[n] = (U^H (X - Y) U)_nn for Wannier-gauge X and optional Y (nullptr: 0); uses T1, T2.
 template <typename C>
 WNLQG_D void rotate_diagonal(const double2 *__restrict__ src, C *T1, C *T2, const C *U, double2 *diag, int nw, int ld,
@@ -308,11 +332,9 @@ WNLQG_D void rotate_diagonal(const double2 *__restrict__ src, C *T1, C *T2, cons
     __syncthreads();
     mm_xy(T1, U, T2, nw, ld);
     __syncthreads();
-    for (int n = threadIdx.x; n < nw; n += blockDim.x) {
-        double2 acc = make_double2(0.0, 0.0);
-        for (int l = 0; l < nw; ++l) acc = cfmaconj(to_c64(U[l + ld * n]), to_c64(T2[l + ld * n]), acc);
-        diag[n] = acc;
-    }
+    band_sums(
+        nw, [&](int n, int l) { return cfmaconj(to_c64(U[l + ld * n]), to_c64(T2[l + ld * n]), make_double2(0.0, 0.0)); },
+        [&](int n, double2 v) { diag[n] = v; });
     __syncthreads();
 }
 
@@ -585,7 +607,14 @@ __global__ void __launch_bounds__(WIDE ? 512 : 256, WIDE ? 1 : (sizeof(R) == 8 ?
                 // difference; sFd[nw + n] = 0 keeps the two-term form below).
                 rotate_diagonal(xw + (int64_t)p.ch_dA[bb * 3 + a] * nn, T1, T2, sU, sFd, nw, ld,
                                 xw + (int64_t)p.ch_dA[a * 3 + bb] * nn);
-                for (int n = threadIdx.x; n < nw; n += blockDim.x) sFd[nw + n] = make_double2(0.0, 0.0);
+                // sFd[nw + n] = i [A_a, A_b]_nn.
+                const C *Aa = slot(p.slot_A[a]), *Ab = slot(p.slot_A[bb]);
+                band_sums(
+                    nw,
+                    [&](int n, int l) {
+                        return to_c64(csub(cmul(Aa[n + ld * l], Ab[l + ld * n]), cmul(Ab[n + ld * l], Aa[l + ld * n])));
+                    },
+                    [&](int n, double2 v) { sFd[nw + n] = cmuli(v); });
                 __syncthreads();
             }
             double local = 0.0;
@@ -593,11 +622,7 @@ __global__ void __launch_bounds__(WIDE ? 512 : 256, WIDE ? 1 : (sizeof(R) == 8 ?
                 const int n = e % nw, m = e / nw;
                 if (p.sc_kind[s] == RS_SC_BERRY) {
                     if (n == m) {
-                        double2 comm = make_double2(0.0, 0.0);
-                        const C *Aa = slot(p.slot_A[a]), *Ab = slot(p.slot_A[bb]);
-                        for (int l = 0; l < nw; ++l)
-                            comm = cadd(comm, to_c64(csub(cmul(Aa[n + ld * l], Ab[l + ld * n]), cmul(Ab[n + ld * l], Aa[l + ld * n]))));
-                        const double2 fnn = csub(csub(sFd[n], sFd[nw + n]), cmuli(comm));
+                        const double2 fnn = csub(sFd[n], sFd[nw + n]);
                         local += sf[n] * fnn.x;
                     } else {
                         const double2 t = cmuli(to_c64(cmul(r_elem(a, n, m), r_elem(bb, m, n))));
@@ -629,35 +654,36 @@ __global__ void __launch_bounds__(WIDE ? 512 : 256, WIDE ? 1 : (sizeof(R) == 8 ?
             __syncthreads();
             const C *Aa = slot(p.slot_A[a]), *Ab = slot(p.slot_A[bb]);
             const C *Ha = slot(p.slot_dH[a]), *Hb = slot(p.slot_dH[bb]);
-            for (int n = threadIdx.x; n < nw; n += blockDim.x) {
-                double2 comm = make_double2(0.0, 0.0);
-                for (int l = 0; l < nw; ++l)
-                    comm = cadd(comm, to_c64(csub(cmul(Aa[n + ld * l], Ab[l + ld * n]), cmul(Ab[n + ld * l], Aa[l + ld * n]))));
-                sFd[2 * nw + n] = csub(csub(sFd[n], sFd[nw + n]), cmuli(comm));
-            }
+            band_sums(
+                nw,
+                [&](int n, int l) {
+                    return to_c64(csub(cmul(Aa[n + ld * l], Ab[l + ld * n]), cmul(Ab[n + ld * l], Aa[l + ld * n])));
+                },
+                [&](int n, double2 comm) { sFd[2 * nw + n] = csub(csub(sFd[n], sFd[nw + n]), cmuli(comm)); });
             __syncthreads();
             if (p.mu_kind[s] == RS_MU_BANDCURV) {
                 // berry_curvature_group_sum_component with the group {n} (ConventionalQuantumGeometry.jl:
                 // 530-557): Re F_nn + sum_{m != n} -Im(r^a_nm r^b_mn - r^b_nm r^a_mn).
                 double *dst = p.curv_out + b * p.curv_stride + p.mu_out[s] * nw;
-                for (int n = threadIdx.x; n < nw; n += blockDim.x) {
-                    double om = 0.0;
-                    for (int m = 0; m < nw; ++m)
-                        if (m != n)
-                            om -= to_c64(csub(cmul(r_elem(a, n, m), r_elem(bb, m, n)),
-                                              cmul(r_elem(bb, n, m), r_elem(a, m, n)))).y;
-                    dst[n] = sFd[2 * nw + n].x + om;
-                }
+                band_sums(
+                    nw,
+                    [&](int n, int m) {
+                        if (m == n) return make_double2(0.0, 0.0);
+                        return make_double2(-to_c64(csub(cmul(r_elem(a, n, m), r_elem(bb, m, n)),
+                                                         cmul(r_elem(bb, n, m), r_elem(a, m, n)))).y, 0.0);
+                    },
+                    [&](int n, double2 om) { dst[n] = sFd[2 * nw + n].x + om.x; });
                 __syncthreads();
             } else if (p.mu_kind[s] == RS_MU_DIPOLE) {
                 // Band Berry curvature Omega_n = -2 sum_m Im(r^a_nm r^b_mn) + Re F_nn
                 // (berry_curvature_component, ConventionalQuantumGeometry.jl:166-180) into sFd[3nw..).
-                for (int n = threadIdx.x; n < nw; n += blockDim.x) {
-                    double om = 0.0;
-                    for (int m = 0; m < nw; ++m)
-                        if (m != n) om += -to_c64(cmul(r_elem(a, n, m), r_elem(bb, m, n))).y;
-                    sFd[3 * nw + n] = make_double2(2.0 * om + sFd[2 * nw + n].x, 0.0);
-                }
+                band_sums(
+                    nw,
+                    [&](int n, int m) {
+                        if (m == n) return make_double2(0.0, 0.0);
+                        return make_double2(-to_c64(cmul(r_elem(a, n, m), r_elem(bb, m, n))).y, 0.0);
+                    },
+                    [&](int n, double2 om) { sFd[3 * nw + n] = make_double2(2.0 * om.x + sFd[2 * nw + n].x, 0.0); });
                 __syncthreads();
                 if (threadIdx.x == 0) {
                     const C *Hc = slot(p.slot_dH[cc]);
@@ -774,12 +800,13 @@ __global__ void __launch_bounds__(WIDE ? 512 : 256, WIDE ? 1 : (sizeof(R) == 8 ?
             const int a = p.hess_a[h], dd = p.hess_d[h];
             rotate_diagonal(xw + (int64_t)p.ch_ddH[a * 3 + dd] * nn, T1, T2, sU, sFd, nw, ld);
             const C *Ha = slot(p.slot_dH[a]), *Hd = slot(p.slot_dH[dd]);
-            for (int n = threadIdx.x; n < nw; n += blockDim.x) {
-                double v = sFd[n].x;
-                for (int l = 0; l < nw; ++l)
-                    if (l != n) v += 2.0 * to_c64(cmul(Ha[n + ld * l], Hd[l + ld * n])).x * sinv[n + nw * l];
-                sHess[h * nw + n] = v;
-            }
+            band_sums(
+                nw,
+                [&](int n, int l) {
+                    if (l == n) return make_double2(0.0, 0.0);
+                    return make_double2(2.0 * to_c64(cmul(Ha[n + ld * l], Hd[l + ld * n])).x * sinv[n + nw * l], 0.0);
+                },
+                [&](int n, double2 v) { sHess[h * nw + n] = sFd[n].x + v.x; });
             __syncthreads();
         }
 
