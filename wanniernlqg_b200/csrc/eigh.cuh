@@ -331,18 +331,36 @@ WNLQG_D bool team_jacobi_sweep(typename cplx_of<T>::type *A, typename cplx_of<T>
             int p, q;
             pair_pq(t, p, q);
             const C apq = A[p + ld * q];
-            const T g = hypot(apq.x, apq.y);
             T c = (T)1;
             C sp = czero<C>();
-            if (g > tol) {
-                const T app = A[p + ld * p].x, aqq = A[q + ld * q].x;
-                const T theta = (aqq - app) / ((T)2 * g);
-                const T tt = (theta >= (T)0 ? (T)1 : (T)-1) / (fabs(theta) + sqrt(theta * theta + (T)1));
-                c = recip_sqrt(tt * tt + (T)1);
-                const T sn = tt * c;
-                sp.x = sn * (apq.x / g);
-                sp.y = sn * (apq.y / g);
-                rotated = true;
+            if constexpr (sizeof(T) == 4) {
+                // FP32 preconditioner: the rotation from one reciprocal square root of |a_pq|^2
+                // (no divisions; the FP64 stage absorbs the few-ulp differences).  |a_pq| >= tol
+                // >= 2^-20 ||H|| keeps the squares far from the FP32 range limits.
+                const T g2 = apq.x * apq.x + apq.y * apq.y;
+                if (g2 > tol * tol) {
+                    const T ginv = rsqrtf(g2);
+                    const T app = A[p + ld * p].x, aqq = A[q + ld * q].x;
+                    const T theta = (aqq - app) * ((T)0.5 * ginv);
+                    const T tt = copysignf(__frcp_rn(fabsf(theta) + sqrtf(theta * theta + (T)1)), theta);
+                    c = rsqrtf(tt * tt + (T)1);
+                    const T sg = tt * c * ginv;
+                    sp.x = sg * apq.x;
+                    sp.y = sg * apq.y;
+                    rotated = true;
+                }
+            } else {
+                const T g = hypot(apq.x, apq.y);
+                if (g > tol) {
+                    const T app = A[p + ld * p].x, aqq = A[q + ld * q].x;
+                    const T theta = (aqq - app) / ((T)2 * g);
+                    const T tt = (theta >= (T)0 ? (T)1 : (T)-1) / (fabs(theta) + sqrt(theta * theta + (T)1));
+                    c = recip_sqrt(tt * tt + (T)1);
+                    const T sn = tt * c;
+                    sp.x = sn * (apq.x / g);
+                    sp.y = sn * (apq.y / g);
+                    rotated = true;
+                }
             }
             rot_c[t] = c;
             rot_s[t] = sp;
