@@ -267,12 +267,42 @@ template <typename C> WNLQG_D void mm_comm(const C *X, const C *Y, C *out, int n
     }
 }
 
+// dst0 = X0 - Y0 (and dst1 = X1 when X1 is given) for column-major nw x nw matrices in global
+// memory (Y0 optional), into shared matrices of leading dimension ld.  Each thread issues all the
+// loads of four elements per matrix before its first store, so that the global-memory latency is
+// paid once per four elements instead of once per element.  No closing barrier.
+template <typename C>
+WNLQG_D void stage_from_global(const double2 *__restrict__ X0, C *dst0, int nw, int ld,
+                               const double2 *__restrict__ Y0 = nullptr, const double2 *__restrict__ X1 = nullptr,
+                               C *dst1 = nullptr) {
+    constexpr int B = 4;
+    const int nn = nw * nw;
+    const double2 zero = make_double2(0.0, 0.0);
+    for (int e0 = threadIdx.x; e0 < nn; e0 += B * blockDim.x) {
+        double2 v0[B], v1[B];
+#pragma unroll
+        for (int j = 0; j < B; ++j) {
+            const int e = e0 + j * blockDim.x;
+            v0[j] = e < nn ? (Y0 ? csub(X0[e], Y0[e]) : X0[e]) : zero;
+            v1[j] = (X1 && e < nn) ? X1[e] : zero;
+        }
+#pragma unroll
+        for (int j = 0; j < B; ++j) {
+            const int e = e0 + j * blockDim.x;
+            if (e < nn) {
+                const int o = (e % nw) + ld * (e / nw);
+                dst0[o] = conv_c<C>(v0[j]);
+                if (X1) dst1[o] = conv_c<C>(v1[j]);
+            }
+        }
+    }
+}
+
 // dst = U^H X U for a Wannier-gauge matrix X in global memory (FP64, column-major nw x nw).
 // dst may alias T1.
 template <typename C>
 WNLQG_D void rotate_to_hamiltonian(const double2 *__restrict__ src, C *T1, C *T2, const C *U, C *dst, int nw, int ld) {
-    const int nn = nw * nw;
-    for (int e = threadIdx.x; e < nn; e += blockDim.x) T1[(e % nw) + ld * (e / nw)] = conv_c<C>(src[e]);
+    stage_from_global(src, T1, nw, ld);
     __syncthreads();
     mm_xy(T1, U, T2, nw, ld);
     __syncthreads();
@@ -280,15 +310,17 @@ WNLQG_D void rotate_to_hamiltonian(const double2 *__restrict__ src, C *T1, C *T2
     __syncthreads();
 }
 
-// dst0 = U^H X0 U and dst1 = U^H X1 U for two Wannier-gauge channels in global memory.  FP64: two
-// paired DMMA passes (X read straight from global memory into the fragments, four accumulator
-// tiles per warp; two barriers for both channels); dst0 and dst1 must not alias T1, T2 or U.
-// FP32: two single rotations.
+// dst0 = U^H X0 U and dst1 = U^H X1 U for two Wannier-gauge channels in global memory.  FP64: the
+// channels are staged in dst0 and dst1 (eight loads in flight per thread), then two paired DMMA
+// passes (four accumulator tiles per warp; three barriers for both channels); dst0 and dst1 must
+// not alias T1, T2 or U.  FP32: two single rotations.
 template <typename C>
 WNLQG_D void rotate_two_to_hamiltonian(const double2 *__restrict__ src0, const double2 *__restrict__ src1, C *T1,
                                        C *T2, const C *U, C *dst0, C *dst1, int nw, int ld) {
     if constexpr (same_type<C, double2>::value) {
-        dmma_product_pair<0>(src0, nw, U, T1, src1, nw, U, T2, nw, ld);
+        stage_from_global(src0, dst0, nw, ld, (const double2 *)nullptr, src1, dst1);
+        __syncthreads();
+        dmma_product_pair<0>(dst0, ld, U, T1, dst1, ld, U, T2, nw, ld);
         __syncthreads();
         dmma_product_pair<1>(U, ld, T1, dst0, U, ld, T2, dst1, nw, ld);
         __syncthreads();
@@ -326,9 +358,7 @@ WNLQG_D void band_sums(int nw, F term, S out) {
 template <typename C>
 WNLQG_D void rotate_diagonal(const double2 *__restrict__ src, C *T1, C *T2, const C *U, double2 *diag, int nw, int ld,
                              const double2 *__restrict__ sub = nullptr) {
-    const int nn = nw * nw;
-    for (int e = threadIdx.x; e < nn; e += blockDim.x)
-        T1[(e % nw) + ld * (e / nw)] = conv_c<C>(sub ? csub(src[e], sub[e]) : src[e]);
+    stage_from_global(src, T1, nw, ld, sub);
     __syncthreads();
     mm_xy(T1, U, T2, nw, ld);
     __syncthreads();
@@ -497,7 +527,7 @@ __global__ void __launch_bounds__(WIDE ? 512 : 256, WIDE ? 1 : (sizeof(R) == 8 ?
     for (int64_t b = kb; b < ke; ++b) {
         const double2 *xw = p.xw + b * p.xw_stride;
         const double wk = p.weights ? p.weights[b] * p.scale : p.scale;
-        for (int e = threadIdx.x; e < nn; e += blockDim.x) sU[(e % nw) + ld * (e / nw)] = conv_c<C>(p.U[b * nn + e]);
+        stage_from_global(p.U + b * nn, sU, nw, ld);
         for (int i = threadIdx.x; i < nw; i += blockDim.x) {
             const double e = p.E[b * nw + i];
             sE[i] = e;
