@@ -267,6 +267,9 @@ template <typename C> WNLQG_D void mm_comm(const C *X, const C *Y, C *out, int n
     }
 }
 
+// Prefetch of one 128-byte line into L2 (a hint: no value, no fault on the line's contents).
+WNLQG_D void l2_prefetch(const void *ptr) { asm volatile("prefetch.global.L2 [%0];" ::"l"(ptr)); }
+
 // dst0 = X0 - Y0 (and dst1 = X1 when X1 is given) for column-major nw x nw matrices in global
 // memory (Y0 optional), into shared matrices of leading dimension ld.  Each thread issues all the
 // loads of four elements per matrix before its first store, so that the global-memory latency is
@@ -527,6 +530,15 @@ __global__ void __launch_bounds__(WIDE ? 512 : 256, WIDE ? 1 : (sizeof(R) == 8 ?
     for (int64_t b = kb; b < ke; ++b) {
         const double2 *xw = p.xw + b * p.xw_stride;
         const double wk = p.weights ? p.weights[b] * p.scale : p.scale;
+        if (!NG && p.xw && b + 1 < ke) {
+            // The next point's channels and eigenvectors into L2 (128-byte lines) while this
+            // point computes: its staging loads then wait on L2 instead of HBM.
+            const char *nx = reinterpret_cast<const char *>(xw + p.xw_stride);
+            const char *nu = reinterpret_cast<const char *>(p.U + (b + 1) * nn);
+            const int64_t lx = p.xw_stride * (int64_t)sizeof(double2) / 128, lu = (int64_t)nn * sizeof(double2) / 128;
+            for (int64_t l = threadIdx.x; l < lx + lu; l += blockDim.x)
+                l2_prefetch(l < lx ? nx + 128 * l : nu + 128 * (l - lx));
+        }
         stage_from_global(p.U + b * nn, sU, nw, ld);
         for (int i = threadIdx.x; i < nw; i += blockDim.x) {
             const double e = p.E[b * nw + i];
