@@ -444,6 +444,48 @@ WNLQG_D void team_column_product(const C *X, const C *Y, C (&out)[Team<TEAM>::RO
     }
 }
 
+// FP64 team of 128 threads (four warps), np <= 32: P = op(X) Y on the FP64 tensor cores (op = X^H
+// when XH), warp w taking the 8 x 32 row block w as four 8 x 8 tiles (one A fragment per K step
+// shared by the four tiles, twelve DMMA chains, dmma.cuh's three-product form); then a team
+// barrier and out[r + ld c] = f(r, c, P[r][c]) for r, c < np.  out may alias X or Y (every
+// operand read precedes the barrier), and f may read out[r + ld c] itself, which only the
+// calling lane writes.  No closing barrier.
+template <bool XH, typename F>
+WNLQG_D void team128_dmma(const double2 *X, const double2 *Y, double2 *out, int np, int ld, F f) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int fr = lane >> 2, fk = lane & 3;
+    const int r = 8 * w + fr;
+    const double2 zero = make_double2(0.0, 0.0);
+    Dmma3 acc[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[q].zero();
+    for (int k0 = 0; k0 < np; k0 += 4) {
+        const int ka = k0 + fk;
+        double2 a = zero;
+        if (r < np && ka < np) {
+            if (XH) {
+                const double2 v = X[ka + ld * r];
+                a = make_double2(v.x, -v.y);
+            } else {
+                a = X[r + ld * ka];
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int c = 8 * q + fr;
+            acc[q].mac(a, (ka < np && c < np) ? Y[ka + ld * c] : zero);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            const int c = 8 * q + 2 * fk + i;
+            if (r < np && c < np) out[r + ld * c] = f(r, c, acc[q].value(i));
+        }
+}
+
 template <int TEAM, typename C>
 WNLQG_D void team_store_column(C *M, const C (&v)[Team<TEAM>::ROWS], int np, int ld) {
     constexpr int ROWS = Team<TEAM>::ROWS;
@@ -622,6 +664,18 @@ WNLQG_D bool team_first_order_completion(double2 *A, double2 *W, int np, int ld,
     Team<TEAM>::sync();
     if (t < np) A[t + ld * t] = make_double2(1.0, 0.0);
     Team<TEAM>::sync();
+    if constexpr (TEAM == 128) {
+        if (tau > 1.4901161193847656e-08) {
+            team128_dmma<false>(A, A, A, np, ld, [](int r, int c, double2 v) {   // A <- I + E + E^2 / 2
+                return make_double2(0.5 * (v.x + (r == c ? 1.0 : 0.0)), 0.5 * v.y);
+            });
+            Team<TEAM>::sync();
+        }
+        team128_dmma<false>(W, A, W, np, ld, [](int, int, double2 v) { return v; });   // W <- W A
+        if (t < np) A[t + ld * t] = make_double2(dnew[t], 0.0);
+        Team<TEAM>::sync();
+        return true;
+    }
     double2 col[Team<TEAM>::ROWS];
     if (tau > 1.4901161193847656e-08) {
         constexpr int ROWS = Team<TEAM>::ROWS;
@@ -665,7 +719,7 @@ struct WarpRefineSmem {
 
 // Blocks of 64 threads holding two teams (TEAM = 32), otherwise blocks of TEAM threads (one team).
 template <int TEAM>
-__global__ void __launch_bounds__(TEAM == 128 ? 128 : 64, TEAM == 32 ? 1 : 6) eigh_refine_f64_team_kernel(const double2 *__restrict__ h_in, int64_t h_stride,
+__global__ void __launch_bounds__(TEAM == 128 ? 128 : 64, TEAM == 32 ? 1 : (TEAM == 128 ? 5 : 6)) eigh_refine_f64_team_kernel(const double2 *__restrict__ h_in, int64_t h_stride,
                                                                   const float2 *__restrict__ V_in, int64_t batch, int nw,
                                                                   double *__restrict__ E_out, double2 *__restrict__ U_out,
                                                                   int converge) {
@@ -695,6 +749,18 @@ __global__ void __launch_bounds__(TEAM == 128 ? 128 : 64, TEAM == 32 ? 1 : 6) ei
         }
         Team<TEAM>::sync();
         // E = V^H V - I into A; then M = I - E/2 + 3 E^2 / 8 into A; W <- V M.
+        if constexpr (TEAM == 128) {
+            team128_dmma<true>(W, W, A, np, ld, [](int r, int c, double2 v) {
+                return make_double2(v.x - (r == c ? 1.0 : 0.0), v.y);
+            });
+            Team<TEAM>::sync();
+            team128_dmma<false>(A, A, A, np, ld, [&](int r, int c, double2 v) {      // (E^2), then M
+                const double2 e = A[r + ld * c];
+                return make_double2((r == c ? 1.0 : 0.0) - 0.5 * e.x + 0.375 * v.x, -0.5 * e.y + 0.375 * v.y);
+            });
+            Team<TEAM>::sync();
+            team128_dmma<false>(W, A, W, np, ld, [](int, int, double2 v) { return v; });   // W <- V M
+        } else {
         team_column_product<TEAM>(W, W, col, np, ld, true);
 #pragma unroll
         for (int i = 0; i < ROWS; ++i)
@@ -715,9 +781,16 @@ __global__ void __launch_bounds__(TEAM == 128 ? 128 : 64, TEAM == 32 ? 1 : 6) ei
         team_column_product<TEAM>(W, A, col, np, ld, false);                 // (V M)[:, c0]
         Team<TEAM>::sync();
         team_store_column<TEAM>(W, col, np, ld);
+        }
         // A <- W^H H W (exactly Hermitian); returns ||H||_F.
         auto project = [&]() {
             const double f = team_load_hermitian<TEAM>(A, h_in + b * h_stride, nw, np, ld, red);   // A <- H
+            if constexpr (TEAM == 128) {
+                team128_dmma<false>(A, W, A, np, ld, [](int, int, double2 v) { return v; });   // A <- H W
+                Team<TEAM>::sync();
+                team128_dmma<true>(W, A, A, np, ld, [](int, int, double2 v) { return v; });    // A <- W^H H W
+                Team<TEAM>::sync();
+            } else {
             team_column_product<TEAM>(A, W, col, np, ld, false);             // (H W)[:, c0]
             Team<TEAM>::sync();
             team_store_column<TEAM>(A, col, np, ld);
@@ -726,6 +799,7 @@ __global__ void __launch_bounds__(TEAM == 128 ? 128 : 64, TEAM == 32 ? 1 : 6) ei
             Team<TEAM>::sync();
             team_store_column<TEAM>(A, col, np, ld);
             Team<TEAM>::sync();
+            }
             const int row = t & 31;
             if (row < np)
                 for (int i = row + (t >> 5); i < np; i += TEAM / 32) {
