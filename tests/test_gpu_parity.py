@@ -207,6 +207,40 @@ def test_mixed_eigensolver_refined_to_fp64(engine_cls, oracle_mod, name, monkeyp
         assert np.max(np.abs(ov - 1.0)) < 1e-8, (i, np.max(np.abs(ov - 1.0)), np.min(np.diff(eo)))
 
 
+@pytest.mark.parametrize("nw", [17, 24, 31])
+@pytest.mark.parametrize("precision", [_abi.PRECISION_FP64, _abi.PRECISION_MIXED])
+def test_team_eigensolver_below_32_orbitals(engine_cls, oracle_mod, nw, precision, monkeypatch):
+    """17 to 31 orbitals run the 128-thread team eigensolver on np = nw or nw + 1 < 32 (the FP64
+    refinement's DMMA row blocks masked at np, a zero-padded row and column for odd nw).  Spectra
+    at arbitrary points against the oracle (eigenvalues to 1e-11 of the largest |E|, eigenvectors
+    of bands 1 meV from their neighbours parallel to 1e-8), point values and a warm-started mesh
+    block to 1e-10 (FP64) or the mixed bound.  The FP64 CUDA-core Fourier sums
+    (WNLQG_B200_DIRECT_FOURIER=1) isolate the eigensolver from the tensor-core Fourier."""
+    monkeypatch.setenv("WNLQG_B200_DIRECT_FOURIER", "1")
+    model = synthetic_orthogonal_model(nw, 1, seed=70 + nw, full_position=True)
+    task = nw32_task(nom=64, precision=precision)
+    k = np.random.default_rng(nw).random((8, 3))
+    mesh = (6, 5, 4)
+    with engine_cls(model, task) as eng:
+        e, u = eng.spectrum(k)
+        pts = eng.point_values(k)
+        got_mesh = eng.integrate_mesh(mesh, 10, 110)
+    for i in range(k.shape[0]):
+        eo, uo, _ = oracle_mod.kpoint_spectrum(model, k[i])
+        assert np.max(np.abs(e[i] - eo)) < 1e-11 * max(1.0, np.abs(eo).max())
+        gaps = np.diff(eo)
+        isolated = np.ones(nw, dtype=bool)
+        isolated[:-1] &= gaps > 1e-3
+        isolated[1:] &= gaps > 1e-3
+        ov = np.abs(np.sum(u[i].conj() * uo, axis=0))
+        assert np.max(np.abs(ov - 1.0)[isolated]) < 1e-8
+    tol = RTOL if precision == _abi.PRECISION_FP64 else MIXED_RTOL
+    for g, r in zip(task.split(pts), task.split(oracle_mod.point_values(model, task, k))):
+        assert rel_err(g, r) < tol
+    for g, r in zip(task.split(got_mesh), task.split(oracle_mod.integrate_mesh(model, task, mesh, 10, 110))):
+        assert rel_err(g, r) < tol
+
+
 @pytest.mark.parametrize("name", ["nw4", "nw32"])
 def test_fp64_warp_eigensolver_matches_cta_jacobi(engine_cls, name, monkeypatch):
     """FP64 path up to 32 orbitals: FP32 warp Jacobi as preconditioner, then FP64 sweeps to the
